@@ -1,0 +1,279 @@
+/*
+ * ys_newton.h -- C ABI of the yasps_b200 Newton inner-loop library.
+ *
+ * One shared library (libys_newton.so) built for sm_100a.  Every entry point
+ * is `extern "C"`, takes plain device/host pointers and sizes, never throws,
+ * and returns an int32 status (YS_OK == 0, negative on error; see below).
+ * All device buffers are owned by the caller.  `stream` is a cudaStream_t
+ * passed as `void*` (NULL = legacy default stream).  Calls on the same
+ * stream are ordered; no call synchronises the device unless stated.
+ *
+ * Citations point at the reference (txstc55/yasps) interface each entry
+ * replaces, relative to the reference project root, PKG = yasps/yasps.
+ */
+#ifndef YS_NEWTON_H
+#define YS_NEWTON_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (mirroring the reference's return codes) ------------- */
+#define YS_OK 0
+#define YS_ERR_CUDA (-1)              /* CUDA failure (hessianKernelHost.pyx:151-155)    */
+#define YS_ERR_INVALID (-2)           /* invalid argument / unsupported shape           */
+#define YS_ERR_CAPACITY (-3)          /* caller buffer or index range too small         */
+#define YS_ERR_NOT_CONVERGED (-4)     /* PCG budget exhausted (solverKernel.pyx:686)     */
+#define YS_ERR_INVALID_RESIDUAL (-5)  /* invalid initial residual (solverKernel.pyx:602) */
+/* A non-positive curvature at PCG iteration `it` returns -(it + 4)
+ * (solverKernel.pyx:670-673); MAS domain inversion failures return
+ * YS_ERR_SINGULAR_DOMAIN with the failing domain count in the result.    */
+#define YS_ERR_SINGULAR_DOMAIN (-6)
+
+/* Last error message of the calling thread ("" if none). */
+const char* ys_last_error(void);
+/* Library ABI version (major * 100 + minor). */
+int32_t ys_version(void);
+
+/* ---- index slots (PKG/kernel/Coordinate/gradientIndicesKernel.pyx) ------ */
+
+/* Slot codes of an energy whose argument list is a JOIN of dimension
+ * `join_dim` through `connectivity` [n x join_dim] into a primitive union of
+ * `num_children` children (num_children == 1: a plain primitive).  Child c
+ * owns union indices [child_prefix[c], child_prefix[c+1]) and resolves to
+ *   child_kind[c] == 2: target leaf, code = child_wrt_start[c] + i*size + 2
+ *   child_kind[c] == 1: non-target DATA leaf, code 1
+ *   child_kind[c] == 0: no differentiated leaf (CONSTANT / not a target of
+ *                       a restricted energy): code 0, the space is padding.
+ * With a union every argument takes two slots [child, pad] (the reference
+ * reserves index_size+1 slots, gradientIndicesKernel.pyx:566-574); the pad
+ * slot carries the size of an argument whose child has no leaf.
+ * Output: codes [n x K], sizes [n x K], K = join_dim * (num_children > 1 ? 2 : 1).
+ * `child_prefix`, `child_kind`, `child_wrt_start` are HOST arrays (<= 8 children).
+ * Replaces the generated `int get_indices(...)`
+ * (gradientIndicesKernel.pyx:869-946).                                      */
+int32_t ys_join_union_indices(const uint32_t* connectivity, uint32_t n, uint32_t join_dim,
+                              uint32_t num_children, const uint32_t* child_prefix,
+                              const int32_t* child_kind, const uint32_t* child_wrt_start,
+                              uint32_t leaf_size, uint32_t* codes, uint16_t* sizes, void* stream);
+
+/* Local permutation + per-instance coordinate counts.  coord_outer has n+1
+ * entries: coord_outer[0] = 0, coord_outer[i+1] = sum_{j<=i} u_j (u_j + 1)/2
+ * with u_j the unique target slots of instance j.  total_sizes may be NULL.
+ * Replaces `int compress_indices(...)` (gradientIndicesKernel.pyx:131-214);
+ * the reference's grouping of instances by compressed size only selects its
+ * per-size kernel templates and has no counterpart here.                   */
+int32_t ys_compress_indices(const uint32_t* codes, const uint16_t* sizes, uint32_t n, uint32_t K,
+                            int16_t* perm, uint16_t* total_sizes, uint32_t* coord_outer,
+                            void* stream);
+
+/* Upper-triangle block coordinates (scalar (row,col) pairs) and dims.
+ * Replaces `int computeCoordinates(...)` (gradientIndicesKernel.pyx:276-318). */
+int32_t ys_compute_coordinates(const uint32_t* codes, const int16_t* perm, const uint16_t* sizes,
+                               const uint32_t* coord_outer, uint32_t n, uint32_t K,
+                               uint32_t* coords, uint16_t* dims, void* stream);
+
+/* ---- sparsity pattern (PKG/kernel/Coordinate/coordinateCompressionKernel.pyx) */
+
+/* Device workspace for ys_pattern_build with `n_coords` occurrences. */
+int32_t ys_pattern_workspace_bytes(uint32_t n_coords, uint64_t* bytes);
+
+typedef struct ys_pattern_out {
+  /* device outputs, capacity n_coords (n_coords + 1 for value_offset) */
+  uint32_t* positions;     /* [2*nu] unique scalar (row, col), order (h, w, row, col) */
+  uint16_t* block_dims;    /* [2*nu] (h, w)                                       */
+  uint32_t* value_offset;  /* [nu+1] exclusive scan of h*w                         */
+  uint32_t* lookup;        /* [n_coords] value offset of each occurrence           */
+  uint32_t* record;        /* [n_coords] record offset of each occurrence          */
+  uint32_t* record_begin;  /* [nu] record offset of each unique block's first record */
+  uint32_t* record_count;  /* [nu] occurrences of each unique block                */
+  /* host outputs */
+  uint32_t num_unique;
+  uint32_t num_categories;     /* <= 16 */
+  uint16_t category_dims[32];  /* (h, w) per category                              */
+  uint32_t category_counts[16];
+  uint32_t category_starts[17];/* value offsets; [num_categories] = total values  */
+  uint64_t total_records;      /* sum of h*w over occurrences                      */
+} ys_pattern_out;
+
+/* Global unique sort of all occurrences by (h, w, row, col), stable in the
+ * occurrence index.  Besides the reference outputs (unique coordinates,
+ * category metadata, lookup) it returns the deterministic assembly plan:
+ * the records of one unique block are contiguous, in occurrence order.
+ * Synchronises `stream` once to read the category metadata.
+ * Replaces `get_unique_coords` + `compress_unique_coords`
+ * (coordinateCompressionKernel.pyx:92-144, 350-419).                       */
+int32_t ys_pattern_build(const uint32_t* coords, const uint16_t* dims, uint32_t n_coords,
+                         void* workspace, uint64_t workspace_bytes, ys_pattern_out* out,
+                         void* stream);
+
+/* ---- element evaluation (PKG/kernel/Hessian) ------------------------------ */
+
+#define YS_MAX_UNION 8
+
+/* A gathered 3-vector attribute: a union of up to 8 children (AoS xyz FP64). */
+typedef struct ys_union3 {
+  const double* child[YS_MAX_UNION];
+  uint32_t prefix[YS_MAX_UNION + 1];
+  uint32_t num_children;
+} ys_union3;
+
+/* Per-term DoF plan produced from the slot codes and the pattern. */
+typedef struct ys_term_plan {
+  const uint32_t* codes;        /* [n x K] slot codes                              */
+  uint32_t K;                   /* slots per instance                              */
+  uint32_t slot_stride;         /* slots per argument (1 plain, 2 union)           */
+  const uint32_t* coord_outer;  /* [n+1] first occurrence of each instance          */
+  const uint32_t* record;       /* pattern record offset of each occurrence (term slice) */
+  const uint32_t* grad_outer;   /* [n+1] first target-argument occurrence           */
+  const uint32_t* grad_record;  /* gradient record offset of each target argument    */
+} ys_term_plan;
+
+typedef struct ys_snh_args {
+  ys_union3 position;           /* current positions (DATA)                         */
+  ys_union3 rest;               /* rest positions (CONSTANT)                        */
+  const uint32_t* tets;         /* [n x 4] union indices                            */
+  uint32_t num_elements;
+  const double* mu;             /* per element, or NULL to use mu_value             */
+  const double* lam;            /* per element, or NULL to use lam_value            */
+  double mu_value, lam_value, dt;
+  int32_t projection_method;    /* -1/0 none, 1 |lambda|, 2 max(lambda, 0)          */
+  ys_term_plan plan;
+  double* block_records;        /* pattern records (FP64)                           */
+  double* grad_records;         /* gradient records (FP64)                          */
+  double* energy;               /* [n] per-element energy, or NULL                  */
+  uint32_t* work_list;          /* [n] scratch: elements needing the eigen-projection */
+  uint32_t* work_count;         /* [1] scratch counter                               */
+} ys_snh_args;
+
+/* Stable Neo-Hookean tetrahedra (examples/dropping_in_container_mixed/helpers.py:102-127):
+ * gradient, Hessian, SPD projection of the full 12x12 local Hessian (the
+ * inner projection of differentiator.pyx:794-799), merge of repeated
+ * vertices and the scatter into pattern/gradient records
+ * (hessianKernelNoProject.pyx:63-264).  Replaces the generated
+ * `compute_hessian_and_gradient_with_compression` for this energy
+ * (hessianKernelHost.pyx:27-161).                                          */
+int32_t ys_snh_eval(const ys_snh_args* args, void* stream);
+
+typedef struct ys_inertia_args {
+  const double* position;       /* [n x 3] (DATA target primitive)                  */
+  const double* x_tilde;        /* [n x 3] inertia target                           */
+  const double* mass;           /* [n]                                              */
+  uint32_t num_vertices;
+  ys_term_plan plan;
+  double* block_records;
+  double* grad_records;
+  double* energy;               /* [n] or NULL                                      */
+} ys_inertia_args;
+
+/* Implicit-Euler inertia 1/2 (x - x~)^T m (x - x~) per vertex
+ * (examples/dropping_in_container_mixed/helpers.py:138-141).               */
+int32_t ys_inertia_eval(const ys_inertia_args* args, void* stream);
+
+/* ---- deterministic assembly --------------------------------------------- */
+
+/* out[offset[u] + e] = sum_{c < count[u]} records[begin[u] + c*hw_u + e] for
+ * e < hw_u, summed in occurrence order (no float atomics).  When out32 is
+ * not NULL an FP32 copy of the sums is written as well.  `dims` gives (h, w)
+ * per unique entry (the gradient uses (size, 1)).                          */
+int32_t ys_assemble(const double* records, const uint32_t* begin, const uint32_t* count,
+                    const uint32_t* offset, const uint16_t* dims, uint32_t nu,
+                    double* out, float* out32, void* stream);
+
+/* Per-variable diagonal blocks and scalar diagonal from assembled block sets.
+ * Variable v of attribute a (count_a instances of size s_a) has scalar
+ * offset seg_start[a] + i*s_a and diagonal block at diag_start[a] + i*s_a^2.
+ * Adds (accumulate != 0) or writes.  Replaces the diagonal / diagonal-block
+ * accumulation of hessianKernelFullProject.pyx:186-212.                    */
+int32_t ys_extract_diagonal(const double* values, const uint32_t* positions,
+                            const uint16_t* block_dims, const uint32_t* value_offset, uint32_t nu,
+                            uint32_t num_attributes, const uint32_t* seg_start /*host*/,
+                            const uint32_t* attr_size /*host*/, const uint32_t* diag_start /*host*/,
+                            double* diag_blocks, double* diagonal, int32_t accumulate, void* stream);
+
+/* Block pseudo-inverse of the diagonal blocks, |lambda| -> |1/lambda|
+ * (|lambda| < 1e-6 -> |lambda|).  Replaces `invert_diagonal_blocks`
+ * (PKG/kernel/Solver/diagonalBlockInverseKernel.pyx:123-176).              */
+int32_t ys_invert_diagonal_blocks(const double* diag_blocks, double* inverse, uint32_t num_attributes,
+                                  const uint32_t* diag_start /*host*/, const uint32_t* count /*host*/,
+                                  const uint32_t* attr_size /*host*/, void* stream);
+
+/* ---- symmetric block SpMV ------------------------------------------------ */
+
+/* Row plan of symmetric upper block storage over 3-DoF variables: for
+ * variable i, the stored blocks with row i (direct) and col i (transposed).
+ * entries: [2*nu] capacity; row_ptr: [num_vars+1].  Requires all blocks 3x3
+ * and positions on 3-aligned scalar offsets.                               */
+int32_t ys_spmv_plan_build(const uint32_t* positions, uint32_t nu, uint32_t num_vars,
+                           void* workspace, uint64_t workspace_bytes, uint32_t* row_ptr,
+                           uint32_t* entry_block, uint32_t* entry_col, void* stream);
+int32_t ys_spmv_plan_workspace_bytes(uint32_t nu, uint32_t num_vars, uint64_t* bytes);
+
+/* y = H x (beta == 0) or y += H x (beta == 1) for a 3x3 symmetric upper
+ * block set with FP64 (values) or FP32 (values32) blocks, one of which is
+ * NULL.  Deterministic (row-gather, fixed order).  Replaces `spmv_blocks`
+ * (PKG/matrixAndVector/matrix/matrix.pyx:21-86) and `spmvOffDiagonalBlocks`
+ * (PKG/kernel/Solver/solverKernel.pyx:156-215).                            */
+int32_t ys_spmv3(const double* values, const float* values32, const uint32_t* row_ptr,
+                 const uint32_t* entry_block, const uint32_t* entry_col, uint32_t num_vars,
+                 const double* x, double* y, int32_t beta, void* stream);
+
+/* ---- preconditioned CG ----------------------------------------------------- */
+
+#define YS_PREC_BLOCK_JACOBI 0
+#define YS_PREC_MAS 1
+
+#define YS_STOP_PRECONDITIONED 0   /* r^T M^-1 r <= tol * r0^T M^-1 r0 (reference rule) */
+#define YS_STOP_RESIDUAL 1         /* ||r||_2 <= tol * ||rhs||_2                        */
+
+typedef struct ys_matrix3 {
+  /* up to two 3x3 block sets (static + dynamic), each with an SpMV row plan */
+  uint32_t num_sets;
+  const double* values[2];
+  const float* values32[2];
+  const uint32_t* row_ptr[2];
+  const uint32_t* entry_block[2];
+  const uint32_t* entry_col[2];
+  uint32_t num_vars;             /* 3-DoF variables; n = 3 * num_vars             */
+} ys_matrix3;
+
+typedef struct ys_pcg_args {
+  ys_matrix3 matrix;
+  int32_t precision;            /* 0: FP64 blocks, 1: FP32 blocks (values32)      */
+  int32_t preconditioner;       /* YS_PREC_*                                      */
+  const double* jacobi_inverse; /* [num_vars * 9] block-Jacobi inverse            */
+  void* mas;                    /* ys_mas handle for YS_PREC_MAS                  */
+  int32_t stop_rule;            /* YS_STOP_*                                      */
+  double tolerance;
+  uint32_t max_iterations;
+  const double* rhs;            /* [n]                                            */
+  double* solution;             /* [n] in: initial guess unless zero_initial_guess */
+  int32_t zero_initial_guess;
+  double* workspace;            /* ys_pcg_workspace_doubles(n) doubles             */
+} ys_pcg_args;
+
+typedef struct ys_pcg_result {
+  int32_t status;        /* reference convention: >=0 iterations (0: converged at start), <0 error */
+  uint32_t iterations;
+  double delta0, delta;  /* preconditioned r^T z at start / end                   */
+  double residual0, residual;  /* recursive ||r||_2 at start / end                  */
+} ys_pcg_result;
+
+uint64_t ys_pcg_workspace_doubles(uint32_t n);
+
+/* Opaque solver: owns the CUDA graph of one PCG configuration (the loop runs
+ * on the device behind a conditional while node; one device->host read of
+ * the status per solve).  Replaces `computeSolution`
+ * (PKG/kernel/Solver/solverKernel.pyx:547-687, block-Jacobi) and the MAS
+ * PCG runtime (PKG/solver/mas/cuda_runtime.py:3549-3751, mas/cuda/pcg.cu). */
+int32_t ys_pcg_create(const ys_pcg_args* args, void** handle);
+int32_t ys_pcg_run(void* handle, void* stream, ys_pcg_result* result);
+int32_t ys_pcg_destroy(void* handle);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YS_NEWTON_H */

@@ -1,0 +1,159 @@
+"""Regenerate the golden fixtures in this folder from the reference itself.
+
+Run in a container where the reference checkout is available::
+
+    python tests/golden/make_golden.py /path/to/yasps-reference
+
+It executes the reference's own Python code and stores its outputs:
+
+* ``snh_torch_single_tet.npz`` -- the reference's float64 PyTorch SNH
+  formulation (``examples/backup/pytorch_energy_hessian_and_gradient/
+  stable_neo_hookean.py``): its rest-invariant and energy functions are
+  extracted from the script's syntax tree (the benchmark part of the script is
+  not run) and differentiated with ``torch.autograd`` on the script's own
+  single-tet rest/current positions and material (mu=2000, lam=1000).
+* ``snh_sympy_six_tets.npz`` -- the reference's SymPy check script
+  (``tests/energy/check_stable_neo_hookean.py``) run as-is; its assembled
+  24x24 Hessian, gradient and energy over the six-tet cube fixture.
+* ``mas_cpu_reference.npz`` -- the reference's NumPy MAS solver
+  (``yasps/yasps/solver/mas``) on a small SNH + inertia system, with pymetis
+  replaced by the chunk-ordering shim documented in ``oracle/mas.py`` (the
+  reference's own BFS component split is used inside the shim).
+
+Nothing in the test suite reads the reference checkout; the tests only read
+the ``.npz`` files written here.
+"""
+
+from __future__ import annotations
+
+import ast
+import os
+import runpy
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+
+def torch_single_tet(ref):
+  import torch
+  path = os.path.join(ref, "examples/backup/pytorch_energy_hessian_and_gradient/stable_neo_hookean.py")
+  tree = ast.parse(open(path).read())
+  keep = []
+  for node in tree.body:
+    if isinstance(node, (ast.Import, ast.ImportFrom)):
+      keep.append(node)
+    elif isinstance(node, ast.FunctionDef) and node.name in ("precompute_rest_invariants",
+                                                              "stable_neo_hookean_energy_precomp"):
+      keep.append(node)
+    elif isinstance(node, ast.Assign) and any(isinstance(t, ast.Name) and t.id in (
+        "rest_position_np", "current_position_np") for t in node.targets):
+      keep.append(node)
+  env = {}
+  exec(compile(ast.Module(body=keep, type_ignores=[]), path, "exec"), env)
+  torch.set_default_dtype(torch.float64)
+  rest = torch.tensor(env["rest_position_np"])[None]
+  cur = torch.tensor(env["current_position_np"])[None]
+  mu, lam = torch.tensor(2000.0), torch.tensor(1000.0)
+  ib, vol = env["precompute_rest_invariants"](rest)
+  f = lambda flat: env["stable_neo_hookean_energy_precomp"](flat.reshape(1, 4, 3), ib, vol, mu, lam).sum()
+  x = cur.reshape(12).clone().requires_grad_(True)
+  e = f(x)
+  (g,) = torch.autograd.grad(e, x)
+  h = torch.autograd.functional.hessian(f, cur.reshape(12).clone())
+  np.savez(os.path.join(HERE, "snh_torch_single_tet.npz"), rest=env["rest_position_np"],
+           current=env["current_position_np"], mu=2000.0, lam=1000.0, energy=e.item(), grad=g.numpy(),
+           hess=h.numpy(), ib=ib[0].numpy(), vol=vol[0].item())
+
+
+def sympy_six_tets(ref):
+  path = os.path.join(ref, "tests/energy/check_stable_neo_hookean.py")
+  out = runpy.run_path(path, run_name="__golden__")
+  np.savez(os.path.join(HERE, "snh_sympy_six_tets.npz"), vols=np.asarray(out["vols"], dtype=np.float64),
+           ibs=np.asarray(out["IBS"], dtype=np.float64).reshape(-1, 3, 3),
+           tet_positions=np.asarray(out["tet_positions"], dtype=np.float64).reshape(-1, 4, 3),
+           indices=np.asarray(out["indices"], dtype=np.int64), mu=2000.0, lam=1000.0,
+           energy=float(out["energy_sum"]), grad=np.asarray(out["gradient_sum"], dtype=np.float64),
+           hess=np.asarray(out["sum_mat"], dtype=np.float64))
+
+
+def mas_reference(ref):
+  sys.path.insert(0, os.path.join(ref, "yasps/yasps/solver"))
+  import mas
+  from mas import hierarchy as mas_hierarchy
+  from mas import metis as mas_metis
+  from mas.matrix_view import BlockSparseMatrixView
+  from oracle import energies, pattern, projection
+
+  def chunk_order(graph, target_nodes_per_partition=16):
+    if graph.node_count <= 1 or not graph.edges:
+      order = np.arange(graph.node_count, dtype=np.int64)
+      return mas_metis.OrderingResult(order, (tuple(map(int, order)),), "trivial", 0.0)
+    groups = []
+    for start in range(0, graph.node_count, target_nodes_per_partition):
+      part = list(range(start, min(graph.node_count, start + target_nodes_per_partition)))
+      groups.extend(mas_metis._component_bfs_groups(graph, part))
+    groups.sort(key=min)
+    order = np.asarray([n for g in groups for n in g], dtype=np.int64)
+    return mas_metis.OrderingResult(order, tuple(tuple(map(int, g)) for g in groups), "chunk", 0.0)
+
+  mas_hierarchy.metis_order = chunk_order
+
+  # A 6x6x6 Morton-numbered cube, Kuhn six-tet split, SNH + inertia, z=0 pinned.
+  from yasps_b200 import scenes
+  sc = scenes.fem_cube(6, spacing=0.1, young=1e5, poisson=0.4, noise=0.01, seed=0)
+  rhs, pat, values, n = _assemble_oracle(sc, energies, pattern, projection)
+  counts = np.asarray(pat.category_counts, dtype=np.int64)
+  view = BlockSparseMatrixView(
+      rows=n, cols=n, variable_scalar_offsets=np.arange(0, n, 3), variable_dimensions=np.full(n // 3, 3),
+      static_values=values, static_positions=pat.positions.astype(np.int64),
+      static_category_starts=pat.category_starts[:-1].astype(np.int64), static_category_counts=counts,
+      static_block_dimensions=pat.category_dims.astype(np.int64), symmetric_storage=True)
+  solver = mas.MASSolver(max_domain_dofs=96, target_nodes_per_partition=32, inverse_backend="cpu_reference")
+  iterations = solver.solve(view, rhs, tolerance=1e-12, max_iterations=500)
+  h = solver.hierarchy
+  np.savez(os.path.join(HERE, "mas_cpu_reference.npz"), rhs=rhs, values=values, positions=pat.positions,
+           solution=solver.solution, iterations=iterations,
+           relative_residual=solver.statistics.relative_residual,
+           domains_per_level=np.asarray(h.domains_per_level), nodes_per_level=np.asarray(h.nodes_per_level),
+           level0_domains=np.concatenate([np.asarray(d) for d in h.levels[0].domains]),
+           level0_domain_sizes=np.asarray([len(d) for d in h.levels[0].domains]),
+           composed_last=h.composed_node_maps[-1])
+
+
+def _assemble_oracle(sc, energies, pattern, projection):
+  """Gradient and upper block storage of the SNH + inertia scene (oracle)."""
+  n = sc.free_count * 3
+  codes, sizes = sc.snh_slots()
+  perm, _, _ = pattern.compress_slots(codes, sizes)
+  c1, d1, o1 = pattern.coordinates(codes, sizes, perm)
+  icodes, isizes = sc.inertia_slots()
+  iperm, _, _ = pattern.compress_slots(icodes, isizes)
+  c2, d2, o2 = pattern.coordinates(icodes, isizes, iperm)
+  pat = pattern.build_pattern([c1, c2], [d1, d2])
+  x = sc.positions_all()[sc.tets]
+  _, g, hh = energies.snh_from_rest(x, sc.rest_all()[sc.tets], sc.mu, sc.lam, sc.dt)
+  hh = projection.project_spd(hh, 1)
+  gl = np.zeros(n)
+  values = np.zeros(pat.total_values)
+  diag = np.zeros(n * 3)
+  pattern.scatter_term(codes, sizes, perm, pat.lookups[0], o1, g, hh, gl, values, diag, [0, n], [0, 3 * n])
+  _, gi, hi = energies.inertia_local(sc.free_positions(), sc.x_tilde(), sc.mass)
+  pattern.scatter_term(icodes, isizes, iperm, pat.lookups[1], o2, gi, hi, gl, values, diag, [0, n], [0, 3 * n])
+  return gl, pat, values, n
+
+
+if __name__ == "__main__":
+  ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YASPS_REFERENCE", "")
+  if not ref or not os.path.isdir(ref):
+    raise SystemExit("usage: make_golden.py <reference checkout>")
+  which = sys.argv[2:] or ["torch", "mas", "sympy"]
+  if "torch" in which:
+    torch_single_tet(ref)
+  if "mas" in which:
+    mas_reference(ref)
+  if "sympy" in which:
+    sympy_six_tets(ref)

@@ -1,0 +1,150 @@
+"""Seeded synthetic workloads (FEM cubes) in the reference's scene idiom.
+
+The cube follows the FEM workloads of this project: an ``n x n x n`` vertex
+grid with spacing ``h``, every hexahedron split into six tetrahedra with the
+reference's cube split (``tests/energy/test_stable_neo_hookean.py:28-30``,
+``[[0,1,3,7],[1,2,3,7],[0,1,4,7],[1,5,4,7],[1,2,6,7],[1,5,6,7]]``, which is
+conforming across hexahedra), tetrahedra oriented to a positive rest volume,
+positions = rest + U(-noise, noise) from ``numpy.random.default_rng(seed)``.
+
+The ``z = 0`` layer is a separate *non-target* DATA primitive stacked before
+the free vertices in a primitive union ``[pinned, free]`` (the reference
+idiom, ``examples/one_bunny_partial_abd``), so pinned vertices take part in
+each element's 12x12 projection but are not unknowns.  Both primitives are
+numbered in Morton (Z-order) of their grid coordinates, which makes chunks of
+32 consecutive free vertices the 32-vertex Morton domains used by MAS, and
+the tetrahedra are ordered by the Morton code of their hexahedron.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+# Reference cube corner numbering: 0 (0,0,0) 1 (1,0,0) 2 (1,1,0) 3 (0,1,0)
+# 4 (0,0,1) 5 (1,0,1) 6 (1,1,1) 7 (0,1,1).
+_CORNERS = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+_SPLIT = np.array([[0, 1, 3, 7], [1, 2, 3, 7], [0, 1, 4, 7], [1, 5, 4, 7], [1, 2, 6, 7], [1, 5, 6, 7]])
+
+
+def morton3(i, j, k):
+  """Interleave the bits of three non-negative integer arrays (x lowest)."""
+  def spread(v):
+    v = np.asarray(v, dtype=np.uint64) & np.uint64(0x1FFFFF)
+    v = (v | (v << np.uint64(32))) & np.uint64(0x1F00000000FFFF)
+    v = (v | (v << np.uint64(16))) & np.uint64(0x1F0000FF0000FF)
+    v = (v | (v << np.uint64(8))) & np.uint64(0x100F00F00F00F00F)
+    v = (v | (v << np.uint64(4))) & np.uint64(0x10C30C30C30C30C3)
+    v = (v | (v << np.uint64(2))) & np.uint64(0x1249249249249249)
+    return v
+  return spread(i) | (spread(j) << np.uint64(1)) | (spread(k) << np.uint64(2))
+
+
+def lame(young, poisson):
+  mu = young / (2.0 * (1.0 + poisson))
+  lam = young * poisson / ((1.0 + poisson) * (1.0 - 2.0 * poisson))
+  return mu, lam
+
+
+@dataclass
+class FemCube:
+  """Arrays of one FEM cube scene (union order: pinned first, then free)."""
+
+  n: int
+  spacing: float
+  pinned_rest: np.ndarray      # (np, 3)
+  free_rest: np.ndarray        # (nf, 3)
+  pinned_position: np.ndarray  # (np, 3)
+  free_position: np.ndarray    # (nf, 3)
+  tets: np.ndarray             # (nt, 4) uint32 union indices
+  mass: np.ndarray             # (nf,) lumped masses of the free vertices
+  velocity: np.ndarray         # (nf, 3)
+  mu: float
+  lam: float
+  density: float
+  dt: float
+  gravity: np.ndarray
+
+  @property
+  def pinned_count(self) -> int:
+    return int(self.pinned_rest.shape[0])
+
+  @property
+  def free_count(self) -> int:
+    return int(self.free_rest.shape[0])
+
+  @property
+  def tet_count(self) -> int:
+    return int(self.tets.shape[0])
+
+  @property
+  def dofs(self) -> int:
+    return 3 * self.free_count
+
+  def positions_all(self) -> np.ndarray:
+    return np.concatenate([self.pinned_position, self.free_position])
+
+  def rest_all(self) -> np.ndarray:
+    return np.concatenate([self.pinned_rest, self.free_rest])
+
+  def free_positions(self) -> np.ndarray:
+    return self.free_position
+
+  def x_tilde(self) -> np.ndarray:
+    """Inertia target ``x_before + v dt + g dt^2`` with ``x_before`` the current state."""
+    return self.free_position + self.velocity * self.dt + self.gravity[None] * self.dt * self.dt
+
+  def snh_slots(self):
+    """Per-tet index slots ``[child, pad] x 4`` of the union path (codes, sizes)."""
+    t = self.tets.astype(np.int64)
+    codes = np.zeros((t.shape[0], 8), dtype=np.int64)
+    sizes = np.zeros((t.shape[0], 8), dtype=np.int64)
+    free = t >= self.pinned_count
+    codes[:, 0::2] = np.where(free, 2 + 3 * (t - self.pinned_count), 1)
+    sizes[:, 0::2] = 3
+    return codes, sizes
+
+  def inertia_slots(self):
+    codes = (2 + 3 * np.arange(self.free_count, dtype=np.int64))[:, None]
+    return codes, np.full_like(codes, 3)
+
+
+def fem_cube(n: int, spacing: float = 0.1, young: float = 1e5, poisson: float = 0.4, noise: float = 0.01,
+             seed: int = 0, density: float = 1000.0, dt: float = 0.01,
+             gravity=(0.0, 0.0, -9.8)) -> FemCube:
+  """Build the ``n^3`` FEM cube workload (see module docstring)."""
+  if n < 2:
+    raise ValueError("fem_cube needs at least 2 vertices per side")
+  g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), axis=-1).reshape(-1, 3)
+  lex = g[:, 0] * n * n + g[:, 1] * n + g[:, 2]
+  rng = np.random.default_rng(seed)
+  rest_lex = g.astype(np.float64) * spacing
+  pos_lex = rest_lex + rng.uniform(-noise, noise, size=rest_lex.shape)
+  codes = morton3(g[:, 0], g[:, 1], g[:, 2])
+  pinned = g[:, 2] == 0
+  pin_ids = np.flatnonzero(pinned)[np.argsort(codes[pinned], kind="stable")]
+  free_ids = np.flatnonzero(~pinned)[np.argsort(codes[~pinned], kind="stable")]
+  union_of_lex = np.empty(n ** 3, dtype=np.int64)
+  union_of_lex[lex[pin_ids]] = np.arange(pin_ids.size)
+  union_of_lex[lex[free_ids]] = pin_ids.size + np.arange(free_ids.size)
+  h = np.stack(np.meshgrid(np.arange(n - 1), np.arange(n - 1), np.arange(n - 1), indexing="ij"), axis=-1).reshape(-1, 3)
+  h = h[np.argsort(morton3(h[:, 0], h[:, 1], h[:, 2]), kind="stable")]
+  corner = h[:, None, :] + _CORNERS[None]
+  corner_lex = corner[..., 0] * n * n + corner[..., 1] * n + corner[..., 2]
+  tets_lex = corner_lex[:, _SPLIT].reshape(-1, 4)
+  r = rest_lex[tets_lex]
+  det = np.linalg.det(np.stack([r[:, 1] - r[:, 0], r[:, 2] - r[:, 0], r[:, 3] - r[:, 0]], axis=2))
+  flip = det < 0
+  tets_lex[flip, 2], tets_lex[flip, 3] = tets_lex[flip, 3].copy(), tets_lex[flip, 2].copy()
+  vol = np.abs(det) / 6.0
+  vmass = np.zeros(n ** 3)
+  np.add.at(vmass, tets_lex.ravel(), np.repeat(density * vol / 4.0, 4))
+  mu, lam = lame(young, poisson)
+  return FemCube(
+      n=n, spacing=spacing,
+      pinned_rest=rest_lex[pin_ids], free_rest=rest_lex[free_ids],
+      pinned_position=pos_lex[pin_ids], free_position=pos_lex[free_ids],
+      tets=union_of_lex[tets_lex].astype(np.uint32), mass=vmass[free_ids],
+      velocity=np.zeros((free_ids.size, 3)), mu=mu, lam=lam, density=density, dt=dt,
+      gravity=np.asarray(gravity, dtype=np.float64))
