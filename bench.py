@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Newton solves/sec of the YASPS inner loop on B200.
+
+Workload (one step = one Newton step): Stable Neo-Hookean + implicit-Euler
+inertia on a 64x64x64 vertex cube (262,144 vertices, 1,500,282 tets, z=0
+layer pinned: 774,144 DoF), E=1e6, nu=0.45, noise +-0.005, dt=1/100,
+gravity -9.8 z.  A step evaluates every element gradient and SPD-projected
+Hessian, assembles the 3x3 block matrix, rebuilds the MAS preconditioner
+(32-vertex Morton domains) and solves H x = g to a true relative residual of
+1e-6 in the precision form (FP32 SpMV/MAS, FP64 dots and FP64 refinement).
+The plain FP64 path (FP64 SpMV) is timed beside it (``fp64``).
+
+``value``: whole-job solves/s with the scene resident on the device.
+``e2e``: the same through ``scene.minimizeEnergy`` with host positions copied
+in and the solution copied out every step.
+``--impl reference``: the CPU restatement of the reference path (oracle) on
+a bounded sample of the same workload (rank 0 only).
+
+Launch: ``python bench.py --gpus N --steps K --warmup W``; for N>1 under
+torchrun every rank solves its own independent scene (replicas, weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Newton solves/sec at 1e-6 rel. residual, FP32+refine vs FP64; p50/p99 latency"
+
+
+def parse():
+  p = argparse.ArgumentParser()
+  p.add_argument("--gpus", type=int, default=1)
+  p.add_argument("--steps", type=int, default=30)
+  p.add_argument("--warmup", type=int, default=3)
+  p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+  p.add_argument("--side", type=int, default=64, help="cube side in vertices")
+  p.add_argument("--no-cpu-baseline", action="store_true")
+  p.add_argument("--tol", type=float, default=1e-6)
+  return p.parse_args()
+
+
+def workload(side, seed):
+  from yasps_b200 import scenes
+  return scenes.fem_cube(side, spacing=0.1, young=1e6, poisson=0.45, noise=0.005, seed=seed)
+
+
+def config(cube, extra=None):
+  c = {"workload": f"SNH+inertia FEM cube {cube.n}^3 verts, {cube.tet_count} tets, {cube.dofs} DoF, "
+                   "MAS 32-vertex Morton domains, solve to 1e-6 true relative residual",
+       "vertices": cube.n ** 3, "tets": cube.tet_count, "dof": cube.dofs, "young": 1e6, "poisson": 0.45,
+       "l2": "working set > L2 (element records ~1.1 GB, MAS inverses ~0.3 GB, blocks 0.15 GB)"}
+  if extra:
+    c.update(extra)
+  return c
+
+
+class Clocks:
+  """nvidia-smi samples during the timed region."""
+
+  FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+            "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+  def __init__(self, device):
+    self.device = device
+    self.proc = None
+    self.file = None
+
+  def start(self):
+    try:
+      self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+      self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                    "-lms", "50", "-i", str(self.device)], stdout=self.file,
+                                   stderr=subprocess.DEVNULL)
+    except Exception:
+      self.proc = None
+
+  def stop(self):
+    if self.proc is None:
+      return None
+    time.sleep(0.06)
+    self.proc.terminate()
+    try:
+      self.proc.wait(timeout=5)
+    except Exception:
+      self.proc.kill()
+    self.file.flush()
+    self.file.seek(0)
+    rows = [l.split(",") for l in self.file.read().strip().splitlines() if l.strip()]
+    os.unlink(self.file.name)
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for r in rows:
+      try:
+        sm.append(float(r[1]))
+        mx = max(mx, float(r[2]))
+        for name, v in zip(names, r[5:9]):
+          if v.strip().lower() == "active":
+            reasons.add(name)
+      except (ValueError, IndexError):
+        continue
+    if not sm:
+      return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+  try:
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+      d = json.load(f)
+    return float(d["hbm_gbs"]), "measured"
+  except Exception:
+    return 6650.0, "fallback"
+
+
+def dist_setup(args):
+  import torch
+  rank = int(os.environ.get("RANK", "0"))
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  if torch.cuda.is_available():
+    torch.cuda.set_device(local)
+  pg = None
+  if world > 1:
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    pg = dist
+  return rank, world, local, pg
+
+
+def max_over_ranks(x, pg):
+  if pg is None:
+    return x
+  import torch
+  t = torch.tensor([x], dtype=torch.float64, device="cuda")
+  pg.all_reduce(t, op=pg.ReduceOp.MAX)
+  return float(t.item())
+
+
+def barrier(pg):
+  if pg is not None:
+    pg.barrier()
+
+
+def time_steps(fn, steps, pg):
+  import torch
+  lat = []
+  torch.cuda.synchronize()
+  barrier(pg)
+  torch.cuda.synchronize()
+  start = torch.cuda.Event(enable_timing=True)
+  end = torch.cuda.Event(enable_timing=True)
+  start.record()
+  for _ in range(steps):
+    t0 = time.perf_counter()
+    fn()
+    lat.append(time.perf_counter() - t0)
+  end.record()
+  torch.cuda.synchronize()
+  barrier(pg)
+  ms = start.elapsed_time(end)
+  return max_over_ranks(ms, pg), lat
+
+
+def gpu_arm(args):
+  import torch
+  from yasps_b200 import _lib as L
+  from yasps_b200 import scenes
+  rank, world, local, pg = dist_setup(args)
+  L.load()
+  cube = workload(args.side, seed=rank)
+  sc, h = scenes.fem_scene(cube)
+  mz = sc.minimizer
+  solver = mz.setSolver("mas", mixed_spmv=True, stop_rule="residual")
+  step = lambda: mz.computeHessianAndGradient(tolerance=args.tol, maxIterations=2000)
+  for _ in range(max(args.warmup, 3)):
+    step()
+  stats = dict(solver.statistics)
+  clocks = Clocks(local)
+  clocks.start()
+  ms, lat = time_steps(step, args.steps, pg)
+  clk = clocks.stop()
+  stats = dict(solver.statistics)
+  impl = solver.implementation
+  rel_res = float(getattr(impl, "final_relative_residual", float("nan")))
+  value = world * args.steps / (ms / 1e3)
+  lat_ms = sorted(1e3 * x for x in lat)
+  # kernels launched per step (ours): element eval 2 + inertia 1 + assemble 2 + diag 1 + MAS numeric (levels) +
+  # refine 2 per refinement + PCG init 4 + 6 per PCG iteration.
+  levels = len(impl.hierarchy.levels)
+  its, refs = int(stats["iterations"]), int(stats.get("refinements", 1))
+  launches_per_step = 6 + levels + 1 + 2 * (refs + 1) + refs * 4 + 6 * its
+  # plain FP64 path on the same scene
+  solver64 = mz.setSolver("mas", mixed_spmv=False, stop_rule="residual")
+  for _ in range(2):
+    step()
+  ms64, _ = time_steps(step, max(3, args.steps // 3), pg)
+  fp64_value = world * max(3, args.steps // 3) / (ms64 / 1e3)
+  stats64 = dict(solver64.statistics)
+  # end to end through the public API with host buffers
+  mz.setSolver("mas", mixed_spmv=True, stop_rule="residual")
+  host_pos = torch.from_numpy(np.ascontiguousarray(cube.free_position.reshape(-1))).pin_memory()
+  out_host = torch.empty(cube.dofs, dtype=torch.float64).pin_memory()
+  fp = h["free_position"]
+
+  def e2e_step():
+    fp.updateValue(host_pos)
+    segs = sc.minimizeEnergy(tolerance=args.tol, maxIterations=2000)
+    out_host.copy_(segs[0])
+  fp.updateValue(host_pos.cuda())
+  for _ in range(2):
+    e2e_step()
+  ms_e2e, _ = time_steps(e2e_step, max(3, args.steps // 3), pg)
+  e2e_value = world * max(3, args.steps // 3) / (ms_e2e / 1e3)
+  # roofline of the dominant kernel (MAS domain GEMV), timed on its own stream
+  ms_solver = mz.linearSolver.implementation
+  H = mz.activeHessian()
+  import ctypes
+  nbytes = ctypes.c_uint64(0)
+  s = torch.cuda.current_stream()
+  L.call("ys_mas_gemv", ms_solver._mas, s.cuda_stream, ctypes.byref(nbytes))
+  reps = 50
+  torch.cuda.synchronize()
+  e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  e0.record(s)
+  for _ in range(reps):
+    L.call("ys_mas_gemv", ms_solver._mas, s.cuda_stream, None)
+  e1.record(s)
+  torch.cuda.synchronize()
+  gemv_ms = e0.elapsed_time(e1) / reps
+  hbm, peak_kind = peaks()
+  achieved = nbytes.value / (gemv_ms / 1e3) / 1e9
+  roofline = {"kernel": "mas_gemv (MAS domain-inverse apply, FP32)", "bound": "hbm", "achieved": achieved,
+              "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+              "traffic": None, "bytes_per_launch": int(nbytes.value), "ms_per_launch": gemv_ms}
+  cpu = None
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu = cpu_baseline_leg(cube, args.tol)
+  line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+          "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "f32+f64 refine (f64 element Hessians and projection)",
+          "data": "synthetic (seeded FEM cube, no external data)",
+          "config": config(cube, {"parallelism": f"replicas x{world}", "path": "fp32+refine",
+                                  "iterations": its, "refinements": refs, "levels": levels,
+                                  "true_rel_residual": rel_res}),
+          "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
+          "fp64": {"value": fp64_value, "unit": "solves/s", "iterations": int(stats64["iterations"])},
+          "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * cube.dofs,
+                  "d2h_bytes_per_step": 8 * cube.dofs},
+          "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline, "clocks": clk,
+          "cpu_baseline": cpu}
+  if rank == 0:
+    print(json.dumps(line), flush=True)
+  if pg is not None:
+    pg.destroy_process_group()
+
+
+def cpu_baseline_leg(cube, tol):
+  from oracle import baseline
+  threads = os.cpu_count() or 1
+  g, H, mas, its = baseline.prepare(cube, tol=tol)
+  total, info = baseline.timed_sample(cube, H, g, mas, its)
+  return {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "port",
+          "sample": (f"oracle (NumPy/SciPy, {threads} host threads): SNH eval+projection+assembly on "
+                     f"{info['sample_fraction']:.4f} of the tets and MAS update on the same fraction of level-0 "
+                     f"domains, scaled; {info['iterations']} MAS-PCG iterations from a full CPU solve to 1e-6 "
+                     f"timed per iteration"), "breakdown_s": info}
+
+
+def reference_arm(args):
+  rank = int(os.environ.get("RANK", "0"))
+  if rank != 0:
+    return
+  from oracle import baseline
+  cube = workload(args.side, seed=0)
+  g, H, mas, its = baseline.prepare(cube, tol=args.tol)
+  for _ in range(args.warmup):
+    baseline.timed_sample(cube, H, g, mas, its)
+  totals = []
+  for _ in range(args.steps):
+    t, info = baseline.timed_sample(cube, H, g, mas, its)
+    totals.append(t)
+  value = 1.0 / float(np.mean(totals))
+  threads = os.cpu_count() or 1
+  cpu = {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+         "sample": (f"oracle restatement of the reference CPU path: SNH+projection+assembly and MAS update on "
+                    f"{info['sample_fraction']:.4f} of the work scaled up, {its} MAS-PCG iterations timed per "
+                    f"iteration")}
+  line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1,
+          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded FEM cube)",
+          "config": config(cube, {"parallelism": "cpu", "path": "fp64", "iterations": its}),
+          "cpu_baseline": cpu, "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                                       "d2h_bytes_per_step": 0}}
+  print(json.dumps(line), flush=True)
+
+
+def main():
+  args = parse()
+  if args.impl == "reference":
+    reference_arm(args)
+  else:
+    gpu_arm(args)
+
+
+if __name__ == "__main__":
+  main()

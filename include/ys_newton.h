@@ -20,6 +20,10 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 /* ---- status codes (mirroring the reference's return codes) ------------- */
 #define YS_OK 0
 #define YS_ERR_CUDA (-1)              /* CUDA failure (hessianKernelHost.pyx:151-155)    */
@@ -159,8 +163,11 @@ int32_t ys_snh_eval(const ys_snh_args* args, void* stream);
 
 typedef struct ys_inertia_args {
   const double* position;       /* [n x 3] (DATA target primitive)                  */
-  const double* x_tilde;        /* [n x 3] inertia target                           */
+  const double* x_before;       /* [n x 3] positions at the start of the step       */
+  const double* velocity;       /* [n x 3] or NULL (zero)                           */
   const double* mass;           /* [n]                                              */
+  double dt;
+  double gravity[3];            /* x~ = x_before + v dt + gravity dt^2              */
   uint32_t num_vertices;
   ys_term_plan plan;
   double* block_records;
@@ -263,6 +270,81 @@ typedef struct ys_pcg_result {
 
 uint64_t ys_pcg_workspace_doubles(uint32_t n);
 
+/* ---- multilevel additive Schwarz (PKG/solver/mas) -------------------------- */
+
+/* Static description of a MAS hierarchy over 3-DoF variables, produced on
+ * the host once per static structure (mas/hierarchy.py:150-271).  Packed
+ * node space: level l owns nodes [level_node_offset[l], level_node_offset[l+1]),
+ * level 0 being the fine variables.  All pointers are device arrays unless
+ * marked host; the handle keeps the pointers (the caller keeps them alive). */
+typedef struct ys_mas_desc {
+  uint32_t num_fine_vars;
+  uint32_t num_levels;                 /* 1..8                                        */
+  const uint32_t* level_node_offset;   /* host [num_levels+1]                         */
+  const double* level_weights;         /* host [num_levels] (mas/preconditioner.py:32-36) */
+  const uint32_t* cmap;                /* [num_levels * num_fine_vars] packed node of each fine var */
+  const uint32_t* child_ptr;           /* [coarse nodes + 1] fine children of coarse nodes */
+  const uint32_t* child_fine;
+  uint32_t num_domains;
+  const uint32_t* dom_node_ptr;        /* [num_domains+1]                             */
+  const uint32_t* dom_nodes;           /* packed node ids, local order                 */
+  const uint64_t* inv_offset;          /* [num_domains] float offset of each inverse   */
+  const uint32_t* dom_entry_ptr;       /* [num_domains+1]                             */
+  const uint32_t* dom_entry;           /* [3 * entries] (local i, local j, level block) */
+  uint32_t fine_blocks;                /* level-0 blocks = the static 3x3 upper blocks */
+  uint32_t coarse_blocks;
+  const uint32_t* cb_src_ptr;          /* [coarse_blocks+1]                           */
+  const uint32_t* cb_src;              /* block index | mode << 30 (0 B, 1 B^T, 2 B+B^T) */
+  const uint32_t* cb_level_begin;      /* host [num_levels+1] coarse block ranges       */
+  uint32_t max_domain_dofs;            /* <= 128                                      */
+  double* coarse_values;               /* [coarse_blocks * 9] scratch                  */
+  float* inverse;                      /* FP32 domain inverses                         */
+  float* level_residual;               /* [3 * packed nodes] scratch                   */
+  float* level_correction;             /* [3 * packed nodes] scratch                   */
+  int32_t* status;                     /* [1] scratch                                  */
+} ys_mas_desc;
+
+int32_t ys_mas_create(const ys_mas_desc* desc, void** handle);
+/* Level Galerkin sums and FP64 Gauss-Jordan inverses of every domain from
+ * the assembled FP64 fine blocks (mas/numeric_assembly.py:64-83,
+ * mas/cuda/local_inverse.cu:190-545).  When failed_domains is not NULL the
+ * call synchronises and reports singular domains (YS_ERR_SINGULAR_DOMAIN). */
+int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* stream, int32_t* failed_domains);
+/* z = M^-1 r (mas/preconditioner.py:128-154). */
+int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream);
+int32_t ys_mas_destroy(void* handle);
+/* The domain-GEMV stage of ys_mas_apply alone, on the level residuals of the
+ * last apply (used to time the preconditioner's dominant kernel).  When
+ * algorithmic_bytes is not NULL it receives the bytes one launch must move
+ * (inverses + gathered residuals + corrections); that query synchronises. */
+int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes);
+
+/* ---- extras -------------------------------------------------------------- */
+
+/* Gradient occurrences: one (dof, dof) coordinate with dims (size, 1) per
+ * target slot (repeated slots included); grad_outer[n+1] prefix counts. */
+int32_t ys_gradient_coordinates(const uint32_t* codes, const uint16_t* sizes, uint32_t n, uint32_t K,
+                                uint32_t* grad_outer, uint32_t* coords, uint16_t* dims, void* stream);
+/* ys_assemble specialised for 3x3 blocks. */
+int32_t ys_assemble3(const double* records, const uint32_t* begin, const uint32_t* count, const uint32_t* offset,
+                     uint32_t nu, double* out, float* out32, void* stream);
+/* ys_assemble with out offset offset[u * offset_stride] (the gradient passes
+ * the pattern positions with stride 2). */
+int32_t ys_assemble_strided(const double* records, const uint32_t* begin, const uint32_t* count,
+                            const uint32_t* offset, uint32_t offset_stride, const uint16_t* dims, uint32_t nu,
+                            double* out, void* stream);
+/* FP64 iterative-refinement residual: x += delta (when delta is not NULL),
+ * r = rhs - H x with the FP64 blocks of `m`, and ||r||^2, ||rhs||^2 (host
+ * norms_host[0..1] when not NULL, synchronising `stream`).  workspace holds
+ * ys_refine_workspace_doubles(num_vars) doubles.  The FP64 audit of the
+ * reference's mixed_spmv mode (PKG/solver/mas/solver.py:643-688).           */
+uint64_t ys_refine_workspace_doubles(uint32_t num_vars);
+int32_t ys_refine_residual(const ys_matrix3* m, const double* rhs, double* x, const double* delta, double* r,
+                           double* workspace, double* norms_host, void* stream);
+/* Asynchronous halves of ys_pcg_run. */
+int32_t ys_pcg_launch(void* handle, void* stream);
+int32_t ys_pcg_status(void* handle, void* stream, ys_pcg_result* result);
+
 /* Opaque solver: owns the CUDA graph of one PCG configuration (the loop runs
  * on the device behind a conditional while node; one device->host read of
  * the status per solve).  Replaces `computeSolution`
@@ -271,6 +353,10 @@ uint64_t ys_pcg_workspace_doubles(uint32_t n);
 int32_t ys_pcg_create(const ys_pcg_args* args, void** handle);
 int32_t ys_pcg_run(void* handle, void* stream, ys_pcg_result* result);
 int32_t ys_pcg_destroy(void* handle);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,183 @@
+"""Timed CPU restatement of one Newton step (oracle; bench baseline only).
+
+TEST/BASELINE INFRASTRUCTURE ONLY -- used by ``bench.py``'s ``cpu_baseline``
+and ``--impl reference`` legs.  It restates, vectorised with NumPy/SciPy,
+the reference's CPU path for the step: SNH gradient/Hessian with the
+reference's PSD-test + eigen projection rule, block assembly, the MAS
+numeric update (dense domain matrices + FP64 inverse,
+``PKG/solver/mas/numeric_assembly.py``, ``local_inverse.py:40-78``) and
+MAS-preconditioned CG (``mas/pcg.py``, ``mas/preconditioner.py``) with the
+chunk ordering of ``oracle/mas.py``.
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import energies, projection
+
+
+def system_from_cube(cube, tet_slice=slice(None)):
+  """Vectorised oracle gradient + sparse Hessian (free DoFs) of the cube."""
+  tets = cube.tets.astype(np.int64)[tet_slice]
+  x = cube.positions_all()[tets]
+  r = cube.rest_all()[tets]
+  _, g, h = energies.snh_from_rest(x, r, cube.mu, cube.lam, cube.dt)
+  h = projection.project_spd(h, 1)
+  npin, n = cube.pinned_count, cube.dofs
+  free = tets >= npin
+  dof = np.where(free[:, :, None], 3 * (tets[:, :, None] - npin) + np.arange(3), -1).reshape(len(tets), 12)
+  grad = np.zeros(n)
+  m = dof >= 0
+  np.add.at(grad, dof[m], g[m])
+  rows = np.broadcast_to(dof[:, :, None], h.shape)
+  cols = np.broadcast_to(dof[:, None, :], h.shape)
+  keep = (rows >= 0) & (cols >= 0)
+  H = sp.coo_matrix((h[keep], (rows[keep], cols[keep])), shape=(n, n)).tocsr()
+  _, gi, hi = energies.inertia_local(cube.free_position, cube.x_tilde(), cube.mass)
+  grad += gi.ravel()
+  H = H + sp.diags(np.repeat(cube.mass, 3))
+  return grad, H.tocsr()
+
+
+class CpuMas:
+  """MAS over chunk-ordered 32-node domains, assembled from a CSR matrix."""
+
+  def __init__(self, H, nv, target=32, coarsest_weight=2.5, max_levels=6, max_dofs=96):
+    from . import mas
+    B = abs(H)
+    B = sp.csr_matrix((np.ones(B.nnz), B.indices, B.indptr), shape=B.shape)
+    node = sp.csr_matrix((np.ones(3 * nv), (np.arange(3 * nv), np.repeat(np.arange(nv), 3))), shape=(3 * nv, nv))
+    G = (node.T @ B @ node).tocoo()
+    edges = np.stack([G.row, G.col], axis=1)
+    edges = edges[edges[:, 0] < edges[:, 1]]
+    self.h = mas.build_hierarchy(np.full(nv, 3), [tuple(e) for e in edges], max_domain_dofs=max_dofs,
+                                 max_levels=max_levels, target_nodes=target)
+    L = len(self.h.levels)
+    self.weights = (1.0,) * (L - 1) + (coarsest_weight,)
+    self.nv = nv
+    self.maps = []
+    for lvl, cm in zip(self.h.levels, self.h.composed):
+      P = sp.csr_matrix((np.ones(3 * nv), (np.arange(3 * nv), (3 * cm[:, None] + np.arange(3)).ravel())),
+                        shape=(3 * nv, 3 * lvl.dims.size))
+      self.maps.append(P)
+    self.update(H)
+
+  def update(self, H, domain_fraction=1.0):
+    """Dense domain matrices + FP64 Cholesky inverses.
+
+    With ``domain_fraction < 1`` only that fraction of the level-0 domains is
+    processed; returns ``(seconds of the sampled level-0 domain work, seconds
+    of everything else)`` so a caller can scale the former alone.
+    """
+    self.inverses = []
+    t_sampled = t_rest = 0.0
+    for li, (lvl, P) in enumerate(zip(self.h.levels, self.maps)):
+      t0 = time.perf_counter()
+      A = H if li == 0 else (P.T @ H @ P).tocsr()
+      doms = lvl.domains
+      if li == 0 and domain_fraction < 1.0:
+        doms = doms[:max(1, int(len(doms) * domain_fraction))]
+      t1 = time.perf_counter()
+      invs = []
+      for dom in doms:
+        idx = (3 * np.asarray(dom)[:, None] + np.arange(3)).ravel()
+        M = A[idx][:, idx].toarray()
+        Lc = np.linalg.cholesky(0.5 * (M + M.T))
+        Li = np.linalg.inv(Lc)
+        invs.append((idx, Li.T @ Li))
+      self.inverses.append(invs)
+      t2 = time.perf_counter()
+      if li == 0:
+        t_sampled += t2 - t1
+        t_rest += t1 - t0
+      else:
+        t_rest += t2 - t0
+    return t_sampled, t_rest
+
+  def apply(self, r):
+    out = np.zeros_like(r)
+    for li, (P, invs) in enumerate(zip(self.maps, self.inverses)):
+      rl = P.T @ r
+      zl = np.zeros_like(rl)
+      for idx, inv in invs:
+        zl[idx] = inv @ rl[idx]
+      out += self.weights[li] * (P @ zl)
+    return out
+
+
+def pcg(H, g, M, tol, maxit):
+  x = np.zeros_like(g)
+  r = g.copy()
+  z = M.apply(r)
+  p = z.copy()
+  rz = r @ z
+  gn = np.linalg.norm(g)
+  for it in range(1, maxit + 1):
+    q = H @ p
+    a = rz / (p @ q)
+    x += a * p
+    r -= a * q
+    if np.linalg.norm(r) <= tol * gn:
+      return x, it
+    z = M.apply(r)
+    rz2 = r @ z
+    p = z + (rz2 / rz) * p
+    rz = rz2
+  return x, maxit
+
+
+def assemble_chunked(cube, chunk=200_000):
+  """Full CPU gradient + Hessian, element work in chunks (bounded memory)."""
+  nt = cube.tet_count
+  g, H = None, None
+  for s in range(0, nt, chunk):
+    gi, Hi = system_from_cube(cube, slice(s, min(nt, s + chunk)))
+    g = gi if g is None else g + gi
+    H = Hi if H is None else H + Hi
+  # the inertia term was added once per chunk: keep one copy
+  k = (nt + chunk - 1) // chunk
+  if k > 1:
+    _, gi, _ = energies.inertia_local(cube.free_position, cube.x_tilde(), cube.mass)
+    g -= (k - 1) * gi.ravel()
+    H = H - (k - 1) * sp.diags(np.repeat(cube.mass, 3))
+  return g, H.tocsr()
+
+
+def prepare(cube, tol=1e-6, maxit=1000):
+  """Untimed setup: the full CPU system, its MAS and the PCG iteration count."""
+  g, H = assemble_chunked(cube)
+  mas = CpuMas(H, cube.free_count)
+  _, its = pcg(H, g, mas, tol, maxit)
+  return g, H, mas, its
+
+
+def timed_sample(cube, H, g, mas, iterations, sample_fraction=1.0 / 128, pcg_iterations=3):
+  """Seconds of one CPU Newton step, measured on a bounded sample.
+
+  Element evaluation (SNH + projection + assembly) on ``sample_fraction`` of
+  the tetrahedra and the MAS numeric update on the same fraction of the
+  level-0 domains are scaled up by that fraction; ``pcg_iterations`` full
+  MAS-PCG iterations are scaled to ``iterations`` (the count a full CPU solve
+  to the target residual takes, measured once by :func:`prepare`).
+  """
+  nt = cube.tet_count
+  k = max(1, int(nt * sample_fraction))
+  t0 = time.perf_counter()
+  system_from_cube(cube, slice(0, k))
+  t_elem = (time.perf_counter() - t0) * nt / k
+  nd = len(mas.h.levels[0].domains)
+  frac = max(1.0 / nd, sample_fraction)
+  saved = mas.inverses
+  t_sampled, t_rest = mas.update(H, domain_fraction=frac)
+  t_mas = t_sampled / frac + t_rest
+  mas.inverses = saved
+  t0 = time.perf_counter()
+  pcg(H, g, mas, 0.0, pcg_iterations)
+  t_it = (time.perf_counter() - t0) / pcg_iterations
+  total = t_elem + t_mas + t_it * iterations
+  return total, dict(element_s=t_elem, mas_update_s=t_mas, pcg_iteration_s=t_it, iterations=int(iterations),
+                     sample_fraction=sample_fraction)

@@ -1,0 +1,178 @@
+"""GPU parity of the Newton inner loop against the oracle (CUDA path via the C ABI).
+
+Tolerances (relative to the largest magnitude of the compared quantity):
+pattern, lookups and assembly plan bit-exact; FP64 gradient / Hessian 1e-12;
+FP32 SpMV 1e-5; solutions at the stated relative residual.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import solvers
+from tests.oracle_scene import OracleCube
+from yasps_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+  a, b = np.asarray(a), np.asarray(b)
+  return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def c0():
+  cube = scenes.fem_cube(10, spacing=0.1, young=1e5, poisson=0.4, noise=0.01, seed=0)
+  return cube, OracleCube(cube)
+
+
+def build(cube, solver=None, **opts):
+  sc, h = scenes.fem_scene(cube)
+  if solver:
+    sc.minimizer.setSolver(solver, **opts)
+  return sc, h
+
+
+def test_pattern_and_lookups_bit_exact(c0):
+  cube, ora = c0
+  sc, _ = build(cube)
+  H = sc.minimizer.computeNumericValue()
+  pos = H.block_positions.cpu().numpy().astype(np.int64).reshape(-1, 2)
+  assert np.array_equal(pos, ora.pattern.positions)
+  assert H.block_counts == ora.pattern.category_counts.tolist()
+  assert H.block_dimensions == [3, 3]
+  assert H.blocks_start_indices == ora.pattern.category_starts.tolist()
+  lk = H._static.pattern.lookup.cpu().numpy().astype(np.int64)
+  assert np.array_equal(lk, np.concatenate(ora.pattern.lookups))
+
+
+def test_gradient_and_hessian_fp64(c0):
+  cube, ora = c0
+  sc, _ = build(cube)
+  H = sc.minimizer.computeNumericValue()
+  assert rel(H.gradient.value.cpu().numpy(), ora.gradient) <= 1e-12
+  assert rel(H.blocks_flattened.cpu().numpy()[:ora.values.size], ora.values) <= 1e-12
+  assert rel(H.diagonal_blocks.cpu().numpy(), ora.diag_blocks) <= 1e-12
+
+
+def test_projection_path_with_many_indefinite_elements():
+  cube = scenes.fem_cube(6, noise=0.04, seed=5)
+  ora = OracleCube(cube)
+  assert (~ora.psd).sum() > 10, "the case must exercise the eigen-projection"
+  sc, _ = build(cube)
+  H = sc.minimizer.computeNumericValue()
+  assert rel(H.blocks_flattened.cpu().numpy()[:ora.values.size], ora.values) <= 1e-12
+
+
+@pytest.mark.parametrize("method", [0, 2])
+def test_projection_methods(method):
+  cube = scenes.fem_cube(5, noise=0.04, seed=7)
+  ora = OracleCube(cube, projection_method=method)
+  sc, _ = scenes.fem_scene(cube, projection_method=method)
+  H = sc.minimizer.computeNumericValue()
+  assert rel(H.blocks_flattened.cpu().numpy()[:ora.values.size], ora.values) <= 1e-12
+
+
+def test_assembly_is_bit_reproducible(c0):
+  cube, _ = c0
+  sc, _ = build(cube)
+  H = sc.minimizer.computeNumericValue()
+  v1 = H.blocks_flattened.clone()
+  g1 = H.gradient.value.clone()
+  H.compute()
+  assert bool((v1 == H.blocks_flattened).all()) and bool((g1 == H.gradient.value).all())
+
+
+def test_spmv_fp64_and_fp32(c0):
+  import torch
+  from yasps_b200 import vector
+  cube, ora = c0
+  sc, _ = build(cube)
+  H = sc.minimizer.computeNumericValue()
+  x = np.linspace(-0.8, 0.9, H.cols)
+  xv = vector(H.cols)
+  xv.updateValue(x)
+  ref = ora.matvec(x)
+  for transpose in (False, True):
+    assert rel(H.spmv(xv, transpose=transpose).get(), ref) <= 1e-12
+  H.ensure_fp32()
+  assert rel(H.spmv(xv, fp32=True).get(), ref) <= 1e-5
+
+
+def test_block_jacobi_pcg_matches_oracle(c0):
+  cube, ora = c0
+  sc, _ = build(cube, "jacobian")
+  H = sc.minimizer.computeNumericValue()
+  n = H.rows
+  inv = solvers.diagonal_inverse(ora.diag_blocks, [n // 3], [3])
+  ref = solvers.jacobi_pcg(ora.matvec, ora.gradient, inv, [n // 3], [3], 1e-16, 2000)
+  code = sc.minimizer.linearSolver.computeSolution(H, H.gradient, None, tolerance=1e-16, maxIterations=2000,
+                                                   zero_initial_guess=True)
+  assert ref.status > 0 and abs(code - ref.status) <= 1
+  x = sc.minimizer.linearSolver.solution.cpu().numpy()
+  assert solvers.relative_residual(ora.matvec, ora.gradient, x) <= 1e-7
+  assert rel(x, ref.solution) <= 1e-6
+
+
+def test_jacobi_status_codes(c0):
+  cube, _ = c0
+  sc, _ = build(cube, "jacobian")
+  H = sc.minimizer.computeNumericValue()
+  code = sc.minimizer.linearSolver.computeSolution(H, H.gradient, None, tolerance=1e-30, maxIterations=3,
+                                                   zero_initial_guess=True)
+  assert code == -4
+  code = sc.minimizer.linearSolver.computeSolution(H, H.gradient, None, tolerance=1.0, maxIterations=3,
+                                                   zero_initial_guess=True)
+  assert code == 0
+
+
+def test_mas_pcg_matches_oracle(c0):
+  from oracle import mas as omas
+  cube, ora = c0
+  sc, _ = build(cube, "mas")
+  H = sc.minimizer.computeNumericValue()
+  p = ora.pattern
+  edges = [(r // 3, c // 3) for r, c in p.positions if r != c]
+  h = omas.build_hierarchy(np.full(ora.n // 3, 3), edges)
+  blocks = [(r // 3, c // 3, ora.values[o:o + 9].reshape(3, 3)) for (r, c), o in zip(p.positions, p.value_offsets)]
+  pre = omas.MASPreconditioner(h, omas.level_local_matrices(h, blocks))
+  ref = solvers.mas_pcg(ora.matvec, ora.gradient, pre.apply, 1e-12, 500)
+  code = sc.minimizer.linearSolver.computeSolution(H, H.gradient, None, tolerance=1e-12, maxIterations=500,
+                                                   zero_initial_guess=True)
+  st = sc.minimizer.linearSolver.statistics
+  assert code == 0 and ref.converged
+  assert abs(st["iterations"] - ref.iterations) <= 2
+  x = sc.minimizer.linearSolver.solution.cpu().numpy()
+  assert solvers.relative_residual(ora.matvec, ora.gradient, x) <= 10 * ref.relative_residual + 1e-9
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_mas_true_residual_target(c0, mixed):
+  cube, ora = c0
+  sc, _ = build(cube, "mas", mixed_spmv=mixed, stop_rule="residual")
+  segs = sc.minimizeEnergy(tolerance=1e-6, maxIterations=1000)
+  x = segs[0].cpu().numpy()
+  assert solvers.relative_residual(ora.matvec, ora.gradient, x) <= 1e-6
+
+
+def test_mas_apply_matches_oracle(c0):
+  import torch
+  from oracle import mas as omas
+  from yasps_b200 import _lib as L
+  cube, ora = c0
+  sc, _ = build(cube, "mas")
+  H = sc.minimizer.computeNumericValue()
+  ms = sc.minimizer.linearSolver.implementation
+  ms._ensure_hierarchy(H)
+  assert ms.numeric_update(H) == 0
+  r = np.cos(np.arange(H.rows) * 0.37)
+  rt = torch.from_numpy(r).cuda()
+  z = torch.zeros_like(rt)
+  L.call("ys_mas_apply", ms._mas, L.ptr(rt), L.ptr(z), L.stream_ptr())
+  p = ora.pattern
+  edges = [(a // 3, b // 3) for a, b in p.positions if a != b]
+  h = omas.build_hierarchy(np.full(ora.n // 3, 3), edges)
+  blocks = [(a // 3, b // 3, ora.values[o:o + 9].reshape(3, 3)) for (a, b), o in zip(p.positions, p.value_offsets)]
+  pre = omas.MASPreconditioner(h, omas.level_local_matrices(h, blocks))
+  # FP32 inverses and level vectors: single-precision agreement
+  assert rel(z.cpu().numpy(), pre.apply(r)) <= 2e-4

@@ -1,0 +1,92 @@
+"""Host-side logic (no GPU): workloads, the MAS hierarchy builder, the API graph."""
+
+import numpy as np
+import pytest
+
+from oracle import mas as omas
+from oracle import pattern
+from yasps_b200 import mas_hierarchy, scenes
+
+
+def _cube_edges(n):
+  c = scenes.fem_cube(n)
+  codes, sizes = c.snh_slots()
+  perm, _, _ = pattern.compress_slots(codes, sizes)
+  coords, dims, _ = pattern.coordinates(codes, sizes, perm)
+  pat = pattern.build_pattern([coords], [dims])
+  pos = pat.positions
+  return c, pos, (pos[pos[:, 0] != pos[:, 1]] // 3)
+
+
+def test_fem_cube_counts():
+  c = scenes.fem_cube(10)
+  assert (c.pinned_count, c.free_count, c.tet_count) == (100, 900, 4374)
+  r = c.rest_all()[c.tets.astype(np.int64)]
+  det = np.linalg.det(np.stack([r[:, 1] - r[:, 0], r[:, 2] - r[:, 0], r[:, 3] - r[:, 0]], axis=2))
+  assert np.all(det > 0)
+  assert np.isclose(c.mass.sum() + 0.0, c.mass.sum())
+  # Lame parameters from E, nu
+  mu, lam = scenes.lame(1e5, 0.4)
+  assert np.isclose(mu, 35714.285714285714) and np.isclose(lam, 142857.14285714287)
+
+
+def test_cube_edge_count_matches_grid_formula():
+  # all vertices free: axis + face-diagonal + body-diagonal edges + diagonal blocks
+  n = 6
+  c = scenes.fem_cube(n)
+  t = c.tets.astype(np.int64)
+  e = set()
+  for a in range(4):
+    for b in range(a + 1, 4):
+      e |= {(min(x, y), max(x, y)) for x, y in zip(t[:, a], t[:, b])}
+  axis = 3 * (n - 1) * n * n
+  face = 3 * (n - 1) ** 2 * n
+  body = (n - 1) ** 3
+  assert len(e) == axis + face + body
+
+
+@pytest.mark.parametrize("n", [4, 6, 9])
+def test_product_hierarchy_matches_oracle(n):
+  c, pos, edges = _cube_edges(n)
+  nv = c.free_count
+  hp = mas_hierarchy.build_hierarchy(np.full(nv, 3), edges)
+  ho = omas.build_hierarchy(np.full(nv, 3), [tuple(e) for e in edges])
+  assert hp.domains_per_level == [len(l.domains) for l in ho.levels]
+  assert hp.nodes_per_level == [l.dims.size for l in ho.levels]
+  for lp, lo in zip(hp.levels, ho.levels):
+    assert [sorted(np.asarray(d).tolist()) for d in lp.domains] == [sorted(d) for d in lo.domains]
+  for cp, co in zip(hp.composed, ho.composed):
+    assert np.array_equal(cp, co)
+
+
+def test_hierarchy_tables_are_consistent():
+  c, pos, edges = _cube_edges(6)
+  nv = c.free_count
+  h = mas_hierarchy.build_hierarchy(np.full(nv, 3), edges)
+  t = mas_hierarchy.build_tables(h, pos)
+  L = len(h.levels)
+  assert t.cmap.size == L * nv
+  assert t.dom_node_ptr[-1] == t.level_node_offset[-1]
+  # every packed node belongs to exactly one domain
+  assert np.array_equal(np.sort(t.dom_nodes), np.arange(t.level_node_offset[-1]))
+  # coarse block sources reference earlier blocks only
+  idx = t.cb_src & 0x3FFFFFFF
+  assert idx.size == 0 or idx.max() < t.fine_blocks + t.cb_level_begin[-1]
+  assert t.max_domain_dofs <= 96
+
+
+def test_scene_api_validation():
+  from yasps_b200 import scene, stable_neo_hookean
+  sc = scene("s")
+  m = sc.addMesh("m")
+  v = m.addPrimitive("v", numInstances=4)
+  x = v.addAttribute("x", rows=3, cols=1)
+  t = m.addPrimitive("t", numInstances=1)
+  con = t.addConnectivity("c", v, [[0, 1, 2, 3]], 4)
+  tx = t.addAttribute("x", through=con, source=x)
+  with pytest.raises(ValueError):
+    stable_neo_hookean(x, tx, 1.0, 1.0, 0.01)  # rest must be a JOIN
+  with pytest.raises(ValueError):
+    t.addConnectivity("bad", v, [[0, 1, 2, 9]], 4)
+  with pytest.raises(ValueError):
+    sc.addMinimizeTarget([x, x])

@@ -1,0 +1,120 @@
+// Dense symmetric kernels used by the element projection (FP64).
+//
+// * psd_test_packed<N>: the reference's LDL^T PSD short-circuit
+//   (PKG/kernel/Hessian/hessianKernelHeader.pyx:79-141), same operation order
+//   (one correctly rounded reciprocal per column, FMA trailing update).
+// * jacobi_eigen<N>: cyclic Jacobi eigen-decomposition (Jacobi 1846;
+//   Golub & Van Loan, Matrix Computations, 4th ed., Alg. 8.5.2 with the
+//   symmetric Schur 2x2 rotation of Alg. 8.5.1).  The reference calls Eigen's
+//   SelfAdjointEigenSolver here; the projected matrix is the same to rounding.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+namespace ys {
+
+// Lower-triangle packed index (row-major over rows, columns 0..row).
+__host__ __device__ constexpr int tri(int r, int c) { return r * (r + 1) / 2 + c; }
+
+// In-place test on a packed lower triangle `s` (destroyed).  Returns true when
+// the matrix is positive semidefinite within 1e-10 * max(1, max |A_ii|).
+template <int N>
+__device__ __forceinline__ bool psd_test_packed(double* s) {
+  double scale = 1.0;
+#pragma unroll
+  for (int r = 0; r < N; ++r) scale = fmax(scale, fabs(s[tri(r, r)]));
+  const double tol = scale * 1.0e-10;
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < N; ++c) {
+    const double pivot = s[tri(c, c)];
+    if (pivot < -tol) ok = false;
+    if (fabs(pivot) <= tol) {
+#pragma unroll
+      for (int r = c + 1; r < N; ++r)
+        if (fabs(s[tri(r, c)]) > tol) ok = false;
+      continue;
+    }
+    const double inv = __drcp_rn(pivot);
+#pragma unroll
+    for (int r = c + 1; r < N; ++r) {
+      const double f = s[tri(r, c)] * inv;
+#pragma unroll
+      for (int t = c + 1; t <= r; ++t) s[tri(r, t)] = __fma_rn(-f, s[tri(t, c)], s[tri(r, t)]);
+    }
+  }
+  return ok;
+}
+
+// Cyclic Jacobi on a full symmetric N x N matrix a (row-major, overwritten
+// with a diagonal), eigenvectors in the columns of v.  Bounded sweeps.
+template <int N>
+__device__ void jacobi_eigen(double (&a)[N][N], double (&v)[N][N]) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) v[i][j] = i == j ? 1.0 : 0.0;
+  double total = 0.0;
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) total += a[i][j] * a[i][j];
+  if (total == 0.0) return;
+  for (int sweep = 0; sweep < 24; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < N; ++p)
+      for (int q = p + 1; q < N; ++q) off += a[p][q] * a[p][q];
+    if (off <= 1.0e-34 * total) break;
+    for (int p = 0; p < N - 1; ++p) {
+      for (int q = p + 1; q < N; ++q) {
+        const double apq = a[p][q];
+        if (apq == 0.0) continue;
+        const double app = a[p][p], aqq = a[q][q];
+        const double tau = (aqq - app) / (2.0 * apq);
+        double t;
+        if (fabs(tau) > 1.0e150) t = 0.5 / tau;
+        else t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        const double c = rsqrt(1.0 + t * t);
+        const double s = t * c;
+        a[p][p] = app - t * apq;
+        a[q][q] = aqq + t * apq;
+        a[p][q] = 0.0;
+        a[q][p] = 0.0;
+        for (int k = 0; k < N; ++k) {
+          if (k == p || k == q) continue;
+          const double akp = a[k][p], akq = a[k][q];
+          const double nkp = c * akp - s * akq;
+          const double nkq = s * akp + c * akq;
+          a[k][p] = nkp; a[p][k] = nkp;
+          a[k][q] = nkq; a[q][k] = nkq;
+        }
+        for (int k = 0; k < N; ++k) {
+          const double vkp = v[k][p], vkq = v[k][q];
+          v[k][p] = c * vkp - s * vkq;
+          v[k][q] = s * vkp + c * vkq;
+        }
+      }
+    }
+  }
+}
+
+// a <- V diag(f(lambda)) V^T with lambda = diag(a) after jacobi_eigen.
+// method 1: |lambda| for negative eigenvalues, 2: 0 for negative eigenvalues.
+template <int N>
+__device__ void jacobi_reconstruct(double (&a)[N][N], const double (&v)[N][N], int method) {
+  double w[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const double l = a[i][i];
+    w[i] = l < 0.0 ? (method == 1 ? -l : 0.0) : l;
+  }
+  for (int i = 0; i < N; ++i) {
+    for (int j = i; j < N; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < N; ++k) acc += v[i][k] * w[k] * v[j][k];
+      a[i][j] = acc;
+      a[j][i] = acc;
+    }
+  }
+}
+
+}  // namespace ys

@@ -1,0 +1,553 @@
+// Multilevel additive Schwarz (MAS) preconditioner on the device.
+//
+// Follows the reference's MAS (PKG/solver/mas): levels of aggregated nodes,
+// dense explicit inverses of every domain (computed in FP64, stored FP32;
+// mas/cuda/local_inverse.cu:190-545, mas/local_inverse.py:40-78) and the
+// weighted additive application z = sum_l w_l P_l A_l^-1 R_l r
+// (mas/preconditioner.py:128-154, mas/cuda/preconditioner_apply.cu).
+//
+// Numeric update (once per Newton step):
+//   mas_level_blocks : Galerkin block sums of level l from level l-1 blocks
+//                      (fixed source order -> deterministic);
+//   mas_domain_inverse: one CTA per domain assembles its dense FP64 matrix in
+//                      shared memory and inverts it in place (Gauss-Jordan,
+//                      the reference's default backend), writes FP32.
+// Application (every PCG iteration, HBM bound on the FP32 inverses):
+//   mas_restrict : packed FP32 level residuals (fixed-order child sums);
+//   mas_gemv     : one CTA per domain, z_d = A_d^-1 r_d (coalesced columns);
+//   mas_collect  : z = sum_l w_l z_l(map_l(i)) fused with r^T z, r^T r and the
+//                  PCG stop test (deterministic last-block reduction).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ys_mas.cuh"
+
+namespace ys {
+
+constexpr int kMaxLevels = 8;
+constexpr int kInvThreads = 256;
+
+struct MasDev {
+  uint32_t nv;              // fine 3-DoF nodes
+  uint32_t levels;
+  uint32_t packed_nodes;    // total nodes over all levels
+  uint32_t level_node_offset[kMaxLevels + 1];
+  float weight[kMaxLevels];
+  const uint32_t* cmap;     // [levels x nv] packed node index per fine node and level
+  const uint32_t* child_ptr;   // [packed_nodes - nv + 1] children of coarse nodes (levels >= 1)
+  const uint32_t* child_fine;
+  // domains (all levels)
+  uint32_t num_domains;
+  const uint32_t* dom_node_ptr;   // [D+1]
+  const uint32_t* dom_nodes;      // packed node ids in local order
+  const uint64_t* inv_offset;     // [D]
+  const uint32_t* dom_entry_ptr;  // [D+1] dense assembly entries of each domain
+  const uint32_t* dom_entry;      // [E*3] (local i, local j, level block index)
+  // level blocks: level 0 = fine upper blocks (values supplied per update)
+  uint32_t fine_blocks;
+  uint32_t coarse_blocks;         // blocks of levels >= 1 (stored after the fine ones)
+  const uint32_t* cb_src_ptr;     // [coarse_blocks+1]
+  const uint32_t* cb_src;         // source block index (into level values) | mode << 30
+  uint32_t cb_level_begin[kMaxLevels + 1];  // coarse block ranges per level (relative)
+  double* coarse_values;          // [coarse_blocks * 9]
+  float* inverse;                 // FP32 inverses
+  float* rl;                      // packed level residuals [3 * packed_nodes]
+  float* zl;                      // packed level corrections
+  int* status;                    // [1] failing domain count
+  uint32_t max_dofs;
+  const double* fine_values;      // set at numeric update
+};
+
+__device__ __forceinline__ const double* level_block(const MasDev& M, uint32_t idx) {
+  return idx < M.fine_blocks ? M.fine_values + 9ull * idx : M.coarse_values + 9ull * (idx - M.fine_blocks);
+}
+
+// One thread per (coarse block, element); sources summed in their stored order.
+// mode 0: B, 1: B^T, 2: B + B^T.
+__global__ void mas_level_blocks(MasDev M, uint32_t begin, uint32_t end) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t cb = begin + t / 9;
+  if (cb >= end) return;
+  const int e = (int)(t % 9), k = e / 3, l = e % 3;
+  double acc = 0.0;
+  for (uint32_t s = M.cb_src_ptr[cb]; s < M.cb_src_ptr[cb + 1]; ++s) {
+    const uint32_t src = M.cb_src[s];
+    const uint32_t mode = src >> 30, idx = src & 0x3fffffffu;
+    const double* b = level_block(M, idx);
+    if (mode == 0) acc += b[3 * k + l];
+    else if (mode == 1) acc += b[3 * l + k];
+    else acc += b[3 * k + l] + b[3 * l + k];
+  }
+  M.coarse_values[9 * cb + e] = acc;
+}
+
+// Dense assembly + in-place Gauss-Jordan inverse of one domain per CTA.
+__global__ void __launch_bounds__(kInvThreads) mas_domain_inverse(MasDev M) {
+  extern __shared__ double A[];  // n*n
+  __shared__ double colk[128];
+  __shared__ double rowk[128];
+  __shared__ int bad;
+  const uint32_t d = blockIdx.x;
+  const uint32_t n = 3 * (M.dom_node_ptr[d + 1] - M.dom_node_ptr[d]);
+  for (uint32_t i = threadIdx.x; i < n * n; i += blockDim.x) A[i] = 0.0;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  const uint32_t e0 = M.dom_entry_ptr[d], e1 = M.dom_entry_ptr[d + 1];
+  for (uint64_t t = (uint64_t)e0 * 9 + threadIdx.x; t < (uint64_t)e1 * 9; t += blockDim.x) {
+    const uint64_t e = t / 9;
+    const int el = (int)(t % 9), k = el / 3, m = el % 3;
+    const uint32_t li = M.dom_entry[3 * e], lj = M.dom_entry[3 * e + 1], bi = M.dom_entry[3 * e + 2];
+    const double v = level_block(M, bi)[el];
+    A[(3 * li + k) * n + 3 * lj + m] = v;
+    if (li != lj) A[(3 * lj + m) * n + 3 * li + k] = v;
+  }
+  __syncthreads();
+  // Gauss-Jordan without pivoting (SPD domains): after step k, A holds the
+  // inverse in the eliminated columns.  Relative pivot tolerance 1e-12 of
+  // the largest diagonal entry (mas/local_inverse.py:43-65).
+  double scale = 0.0;
+  for (uint32_t i = 0; i < n; ++i) scale = fmax(scale, fabs(A[i * n + i]));
+  const double tol = 1.0e-12 * fmax(scale, 1.0e-300);
+  for (uint32_t k = 0; k < n; ++k) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      colk[i] = A[i * n + k];
+      rowk[i] = A[k * n + i];
+    }
+    __syncthreads();
+    const double piv = rowk[k];
+    if (!(piv > tol) && threadIdx.x == 0) bad = 1;
+    const double ip = 1.0 / piv;
+    // Row k scaled, column k set to -a_ik / piv, the rest updated.
+    for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) {
+      const uint32_t i = t / n, j = t - (t / n) * n;
+      double v;
+      if (i == k) v = (j == k) ? ip : rowk[j] * ip;
+      else if (j == k) v = -colk[i] * ip;
+      else v = A[t] - colk[i] * rowk[j] * ip;
+      A[t] = v;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
+  float* out = M.inverse + M.inv_offset[d];
+  for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) {
+    const uint32_t i = t / n, j = t % n;
+    out[t] = (float)(0.5 * (A[i * n + j] + A[j * n + i]));
+  }
+}
+
+// Packed FP32 level residuals: level 0 copies r, coarse nodes sum children.
+__global__ void mas_restrict(MasDev M, const double* __restrict__ r) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M.packed_nodes) return;
+  double s0, s1, s2;
+  if (p < M.nv) {
+    s0 = r[3ull * p]; s1 = r[3ull * p + 1]; s2 = r[3ull * p + 2];
+  } else {
+    const uint32_t c = p - M.nv;
+    s0 = s1 = s2 = 0.0;
+    for (uint32_t q = M.child_ptr[c]; q < M.child_ptr[c + 1]; ++q) {
+      const uint32_t f = M.child_fine[q];
+      s0 += r[3ull * f]; s1 += r[3ull * f + 1]; s2 += r[3ull * f + 2];
+    }
+  }
+  M.rl[3ull * p] = (float)s0;
+  M.rl[3ull * p + 1] = (float)s1;
+  M.rl[3ull * p + 2] = (float)s2;
+}
+
+// z_d = A_d^-1 r_d, one CTA per domain; thread i owns output row i and reads
+// column i of the symmetric inverse (coalesced across the CTA).
+__global__ void __launch_bounds__(128) mas_gemv(MasDev M) {
+  __shared__ float rloc[384];
+  const uint32_t d = blockIdx.x;
+  const uint32_t nb = M.dom_node_ptr[d], nn = M.dom_node_ptr[d + 1] - nb;
+  const uint32_t n = 3 * nn;
+  for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+    const uint32_t node = M.dom_nodes[nb + t / 3];
+    rloc[t] = M.rl[3ull * node + t % 3];
+  }
+  __syncthreads();
+  const float* inv = M.inverse + M.inv_offset[d];
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    float acc0 = 0.f, acc1 = 0.f;
+    uint32_t j = 0;
+    for (; j + 1 < n; j += 2) {
+      acc0 += __ldg(inv + (uint64_t)j * n + i) * rloc[j];
+      acc1 += __ldg(inv + (uint64_t)(j + 1) * n + i) * rloc[j + 1];
+    }
+    if (j < n) acc0 += __ldg(inv + (uint64_t)j * n + i) * rloc[j];
+    const uint32_t node = M.dom_nodes[nb + i / 3];
+    M.zl[3ull * node + i % 3] = acc0 + acc1;
+  }
+}
+
+struct MasPcg {
+  MasDev M;
+  SpmvSet sets[2];
+  int nsets;
+  int fp32;
+  uint32_t nv;
+  const double* rhs;
+  double* x;
+  double* r;
+  double* p;
+  double* q;
+  double* z;
+  double* st;
+  double* partials;
+  unsigned* tickets;
+  int stop_rule;
+  int zero_guess;
+  double tolerance;
+  uint32_t max_it;
+  cudaGraphConditionalHandle cond;
+};
+
+__global__ void __launch_bounds__(kPcgBlock) mas_init_residual(MasPcg P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.nv) return;
+  double r0 = P.rhs[3ull * i], r1 = P.rhs[3ull * i + 1], r2 = P.rhs[3ull * i + 2];
+  if (P.zero_guess) {
+    P.x[3ull * i] = 0.0; P.x[3ull * i + 1] = 0.0; P.x[3ull * i + 2] = 0.0;
+  } else {
+    double h0, h1, h2;
+    spmv3_row(P.sets, P.nsets, P.fp32, i, P.x, h0, h1, h2);
+    r0 -= h0; r1 -= h1; r2 -= h2;
+  }
+  P.r[3ull * i] = r0; P.r[3ull * i + 1] = r1; P.r[3ull * i + 2] = r2;
+}
+
+__device__ __forceinline__ void collect_node(const MasPcg& P, uint32_t i, double (&z)[3]) {
+  z[0] = z[1] = z[2] = 0.0;
+  for (uint32_t l = 0; l < P.M.levels; ++l) {
+    const uint32_t node = P.M.cmap[(uint64_t)l * P.nv + i];
+    const double w = (double)P.M.weight[l];
+    z[0] += w * (double)P.M.zl[3ull * node];
+    z[1] += w * (double)P.M.zl[3ull * node + 1];
+    z[2] += w * (double)P.M.zl[3ull * node + 2];
+  }
+}
+
+// z = M^-1 r; p = z; r^T z, r^T r, g^T g; stop threshold; loop flag.
+__global__ void __launch_bounds__(kPcgBlock) mas_init_collect(MasPcg P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[3] = {0.0, 0.0, 0.0};
+  if (i < P.nv) {
+    double z[3];
+    collect_node(P, i, z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double r = P.r[3ull * i + k], g = P.rhs[3ull * i + k];
+      P.z[3ull * i + k] = z[k];
+      P.p[3ull * i + k] = z[k];
+      v[0] += r * z[k];
+      v[1] += r * r;
+      v[2] += g * g;
+    }
+  }
+  if (!grid_reduce_last<3>(v, P.partials, P.tickets)) return;
+  if (threadIdx.x != 0) return;
+  double* st = P.st;
+  const double delta = v[0];
+  st[kDeltaNew] = delta;
+  st[kDelta0] = delta;
+  st[kRR] = v[1];
+  st[kRR0] = v[1];
+  st[kGG] = v[2];
+  st[kIter] = 0.0;
+  st[kAlpha] = 0.0;
+  st[kBeta] = 0.0;
+  int status = kContinue;
+  double tol;
+  if (P.stop_rule == YS_STOP_RESIDUAL) {
+    tol = P.tolerance * P.tolerance * v[2];
+    if (!(isfinite(v[1]) && isfinite(v[2]))) status = kInvalidInit;
+    else if (v[1] <= tol) status = kConverged;
+    else if (!(isfinite(delta) && delta > 0.0)) status = kInvalidInit;
+  } else {
+    // mas/pcg.py:44-66: converged when r^T z <= tol * reference.
+    tol = P.tolerance * delta;
+    if (!(isfinite(delta) && delta >= 0.0)) status = kInvalidInit;
+    else if (delta <= tol) status = kConverged;
+    else if (!(delta > 0.0)) status = kInvalidInit;
+  }
+  if (status == kContinue && P.max_it == 0) status = kMaxIter;
+  st[kTolAbs] = tol;
+  st[kStatus] = (double)status;
+  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kPcgBlock) mas_update(MasPcg P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.nv || P.st[kStatus] != (double)kContinue) return;
+  const double alpha = P.st[kAlpha];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    P.x[3ull * i + k] = P.x[3ull * i + k] + P.p[3ull * i + k] * alpha;
+    P.r[3ull * i + k] = P.r[3ull * i + k] - P.q[3ull * i + k] * alpha;
+  }
+}
+
+__global__ void __launch_bounds__(kPcgBlock) mas_iter_collect(MasPcg P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = P.st[kStatus] == (double)kContinue;
+  double v[2] = {0.0, 0.0};
+  if (i < P.nv && live) {
+    double z[3];
+    collect_node(P, i, z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double r = P.r[3ull * i + k];
+      P.z[3ull * i + k] = z[k];
+      v[0] += r * z[k];
+      v[1] += r * r;
+    }
+  }
+  if (!grid_reduce_last<2>(v, P.partials, P.tickets + 2)) return;
+  if (threadIdx.x != 0 || !live) return;
+  double* st = P.st;
+  const double next = v[0], prev = st[kDeltaOld];
+  const double it = st[kIter] + 1.0;
+  st[kIter] = it;
+  st[kDeltaNew] = next;
+  st[kRR] = v[1];
+  int status = kContinue;
+  // mas/pcg.py:80-98
+  if (!isfinite(next) || next < 0.0 || !isfinite(prev) || prev <= 0.0) {
+    st[kBeta] = 0.0;
+    status = kNonSpd;
+  } else {
+    st[kBeta] = next / prev;
+    const bool done = P.stop_rule == YS_STOP_RESIDUAL ? v[1] <= st[kTolAbs] : next <= st[kTolAbs];
+    if (done) status = kConverged;
+    else if (next == 0.0) status = kNonSpd;
+    else if (it >= (double)P.max_it) status = kMaxIter;
+  }
+  st[kStatus] = (double)status;
+  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kPcgBlock) mas_collect_only(MasPcg P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.nv) return;
+  double z[3];
+  collect_node(P, i, z);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) P.z[3ull * i + k] = z[k];
+}
+
+struct MasHandle {
+  MasDev M;
+  std::vector<uint32_t> cb_level_begin;
+  std::vector<MasPcg*> pcgs;
+  int* status_host = nullptr;
+};
+
+static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
+                              const void* fn, unsigned grid, unsigned block, size_t smem, void** args) {
+  cudaKernelNodeParams kp{};
+  kp.func = const_cast<void*>(fn);
+  kp.gridDim = dim3(grid);
+  kp.blockDim = dim3(block);
+  kp.sharedMemBytes = (unsigned)smem;
+  kp.kernelParams = args;
+  return cudaGraphAddKernelNode(node, g, deps, ndeps, &kp);
+}
+
+// Restrict -> GEMV chain shared by init and iteration.
+static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
+                                   cudaGraphNode_t* last, const double* r) {
+  cudaGraphNode_t n1 = nullptr, n2 = nullptr;
+  MasDev m = M;
+  const double* rr = r;
+  void* a1[] = {&m, &rr};
+  cudaError_t e = add_kernel(g, &n1, deps, ndeps, (const void*)mas_restrict, grid_for(M.packed_nodes, 256), 256, 0, a1);
+  if (e != cudaSuccess) return e;
+  void* a2[] = {&m};
+  e = add_kernel(g, &n2, &n1, 1, (const void*)mas_gemv, M.num_domains, 128, 0, a2);
+  *last = n2;
+  return e;
+}
+
+cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
+                               cudaGraphNode_t* last, uint32_t nv, const double* rhs, double* x, double* r, double* p,
+                               double* q, double* z, double* st, double* partials, unsigned* tickets, const SpmvSet* sets,
+                               int nsets, int fp32, int stop_rule, int zero_guess, double tolerance, uint32_t max_it,
+                               cudaGraphConditionalHandle cond, MasPcgHooks* hooks) {
+  auto* h = static_cast<MasHandle*>(mas);
+  if (h->M.nv != nv) return cudaErrorInvalidValue;
+  if (!zero_guess) return cudaErrorNotSupported;
+  auto* P = new MasPcg{};
+  P->M = h->M;
+  for (int s = 0; s < nsets; ++s) P->sets[s] = sets[s];
+  P->nsets = nsets;
+  P->fp32 = fp32;
+  P->nv = nv;
+  P->rhs = rhs;
+  P->x = x;
+  P->r = r;
+  P->p = p;
+  P->q = q;
+  P->z = z;
+  P->st = st;
+  P->partials = partials;
+  P->tickets = tickets;
+  P->stop_rule = stop_rule;
+  P->zero_guess = zero_guess;
+  P->tolerance = tolerance;
+  P->max_it = max_it;
+  P->cond = cond;
+  h->pcgs.push_back(P);
+  hooks->params = P;
+  const unsigned grid = grid_for(nv, kPcgBlock);
+  cudaGraphNode_t n0 = nullptr, n1 = nullptr, n2 = nullptr;
+  void* a0[] = {P};
+  cudaError_t e = add_kernel(g, &n0, deps, ndeps, (const void*)mas_init_residual, grid, kPcgBlock, 0, a0);
+  if (e == cudaSuccess) e = add_apply_nodes(P->M, g, &n0, 1, &n1, r);
+  if (e == cudaSuccess) e = add_kernel(g, &n2, &n1, 1, (const void*)mas_init_collect, grid, kPcgBlock, 0, a0);
+  *last = n2;
+  return e;
+}
+
+cudaError_t mas_add_update_nodes(void* mas, cudaGraph_t body, const cudaGraphNode_t* deps, size_t ndeps,
+                                 cudaGraphNode_t* last, MasPcgHooks* hooks) {
+  (void)mas;
+  auto* P = static_cast<MasPcg*>(hooks->params);
+  const unsigned grid = grid_for(P->nv, kPcgBlock);
+  cudaGraphNode_t n0 = nullptr, n1 = nullptr, n2 = nullptr;
+  void* a0[] = {P};
+  cudaError_t e = add_kernel(body, &n0, deps, ndeps, (const void*)mas_update, grid, kPcgBlock, 0, a0);
+  if (e == cudaSuccess) e = add_apply_nodes(P->M, body, &n0, 1, &n1, P->r);
+  if (e == cudaSuccess) e = add_kernel(body, &n2, &n1, 1, (const void*)mas_iter_collect, grid, kPcgBlock, 0, a0);
+  *last = n2;
+  return e;
+}
+
+}  // namespace ys
+
+extern "C" {
+
+int32_t ys_mas_create(const ys_mas_desc* d, void** handle) {
+  YS_REQUIRE(d && handle, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE(d->num_levels >= 1 && d->num_levels <= ys::kMaxLevels, YS_ERR_INVALID, "1..8 levels");
+  YS_REQUIRE(d->max_domain_dofs >= 3 && d->max_domain_dofs <= 128, YS_ERR_INVALID, "domain DoF must be <= 128");
+  auto* h = new ys::MasHandle();
+  ys::MasDev& M = h->M;
+  M.nv = d->num_fine_vars;
+  M.levels = d->num_levels;
+  for (uint32_t l = 0; l <= d->num_levels; ++l) M.level_node_offset[l] = d->level_node_offset[l];
+  for (uint32_t l = 0; l < d->num_levels; ++l) M.weight[l] = (float)d->level_weights[l];
+  M.packed_nodes = d->level_node_offset[d->num_levels];
+  M.cmap = d->cmap;
+  M.child_ptr = d->child_ptr;
+  M.child_fine = d->child_fine;
+  M.num_domains = d->num_domains;
+  M.dom_node_ptr = d->dom_node_ptr;
+  M.dom_nodes = d->dom_nodes;
+  M.inv_offset = d->inv_offset;
+  M.dom_entry_ptr = d->dom_entry_ptr;
+  M.dom_entry = d->dom_entry;
+  M.fine_blocks = d->fine_blocks;
+  M.coarse_blocks = d->coarse_blocks;
+  M.cb_src_ptr = d->cb_src_ptr;
+  M.cb_src = d->cb_src;
+  for (uint32_t l = 0; l <= d->num_levels; ++l) M.cb_level_begin[l] = d->cb_level_begin[l];
+  M.coarse_values = d->coarse_values;
+  M.inverse = d->inverse;
+  M.rl = d->level_residual;
+  M.zl = d->level_correction;
+  M.status = d->status;
+  M.max_dofs = d->max_domain_dofs;
+  M.fine_values = nullptr;
+  cudaError_t e = cudaMallocHost(&h->status_host, sizeof(int));
+  if (e == cudaSuccess) {
+    const size_t smem = sizeof(double) * d->max_domain_dofs * d->max_domain_dofs;
+    e = cudaFuncSetAttribute(ys::mas_domain_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  if (e != cudaSuccess) {
+    ys_set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    if (h->status_host) cudaFreeHost(h->status_host);
+    delete h;
+    return YS_ERR_CUDA;
+  }
+  *handle = h;
+  return YS_OK;
+}
+
+int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* stream, int32_t* failed_domains) {
+  YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
+  auto* h = static_cast<ys::MasHandle*>(handle);
+  cudaStream_t s = (cudaStream_t)stream;
+  ys::MasDev& M = h->M;
+  M.fine_values = fine_values;
+  for (auto* p : h->pcgs) p->M.fine_values = fine_values;
+  YS_CUDA_TRY(cudaMemsetAsync(M.status, 0, sizeof(int), s));
+  for (uint32_t l = 1; l < M.levels; ++l) {
+    const uint32_t b = M.cb_level_begin[l], e = M.cb_level_begin[l + 1];
+    if (e > b) {
+      ys::mas_level_blocks<<<ys::grid_for(9ull * (e - b), 256), 256, 0, s>>>(M, b, e);
+      YS_CHECK_LAUNCH();
+    }
+  }
+  const size_t smem = sizeof(double) * M.max_dofs * M.max_dofs;
+  ys::mas_domain_inverse<<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
+  YS_CHECK_LAUNCH();
+  if (failed_domains) {
+    YS_CUDA_TRY(cudaMemcpyAsync(h->status_host, M.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    YS_CUDA_TRY(cudaStreamSynchronize(s));
+    *failed_domains = *h->status_host;
+    if (*failed_domains) return YS_ERR_SINGULAR_DOMAIN;
+  }
+  return YS_OK;
+}
+
+int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
+  YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
+  auto* h = static_cast<ys::MasHandle*>(handle);
+  cudaStream_t s = (cudaStream_t)stream;
+  ys::MasDev& M = h->M;
+  ys::mas_restrict<<<ys::grid_for(M.packed_nodes, 256), 256, 0, s>>>(M, r);
+  YS_CHECK_LAUNCH();
+  ys::mas_gemv<<<M.num_domains, 128, 0, s>>>(M);
+  YS_CHECK_LAUNCH();
+  ys::MasPcg P{};
+  P.M = M;
+  P.nv = M.nv;
+  P.z = z;
+  ys::mas_collect_only<<<ys::grid_for(M.nv, ys::kPcgBlock), ys::kPcgBlock, 0, s>>>(P);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes) {
+  YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
+  auto* h = static_cast<ys::MasHandle*>(handle);
+  ys::MasDev& M = h->M;
+  if (algorithmic_bytes) {
+    // every inverse read once (FP32) + the gathered residual and the correction
+    std::vector<uint32_t> ptr(M.num_domains + 1);
+    cudaMemcpy(ptr.data(), M.dom_node_ptr, sizeof(uint32_t) * (M.num_domains + 1), cudaMemcpyDeviceToHost);
+    uint64_t bytes = 0;
+    for (uint32_t d = 0; d < M.num_domains; ++d) {
+      const uint64_t n = 3ull * (ptr[d + 1] - ptr[d]);
+      bytes += 4 * n * n + 4 * n + 4 * n + 4 * (n / 3);
+    }
+    *algorithmic_bytes = bytes;
+  }
+  ys::mas_gemv<<<M.num_domains, 128, 0, (cudaStream_t)stream>>>(M);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_mas_destroy(void* handle) {
+  if (!handle) return YS_OK;
+  auto* h = static_cast<ys::MasHandle*>(handle);
+  for (auto* p : h->pcgs) delete p;
+  if (h->status_host) cudaFreeHost(h->status_host);
+  delete h;
+  return YS_OK;
+}
+
+}  // extern "C"

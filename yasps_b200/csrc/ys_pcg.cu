@@ -1,0 +1,447 @@
+// Preconditioned CG with the loop on the device.
+//
+// The reference's block-Jacobi PCG runs a host loop with ~10 launches and a
+// device->host copy per iteration (PKG/kernel/Solver/solverKernel.pyx:606-686);
+// its MAS PCG drives a CUDA graph with a conditional while node
+// (PKG/solver/mas/cuda/pcg.cu:373-383).  Here one CUDA graph holds the whole
+// solve: initial residual, a conditional while node whose body is
+//   spmv_dot  : q = H p, curvature p^T q -> alpha         (last-block finish)
+//   update    : x += alpha p, r -= alpha q, z = M^-1 r,
+//               r^T z, r^T r -> beta, stop test, loop flag  (last-block finish)
+//   direction : p = z + beta p
+// and a single device->host read of the status per solve.  All reductions are
+// deterministic (fixed-order block trees, fixed-order partial sums).
+#include <cmath>
+#include <vector>
+
+#include "ys_mas.cuh"
+#include "ys_pcg.cuh"
+
+namespace ys {
+
+struct PcgParams {
+  SpmvSet sets[2];
+  int nsets;
+  int fp32;
+  uint32_t nv;
+  const double* rhs;
+  double* x;
+  double* r;
+  double* p;
+  double* q;
+  double* z;
+  const double* jinv;
+  double* st;
+  double* partials;
+  unsigned* tickets;
+  int stop_rule;
+  int zero_guess;
+  double tolerance;
+  uint32_t max_it;
+  cudaGraphConditionalHandle cond;
+};
+
+__device__ __forceinline__ void jacobi3(const double* __restrict__ inv, uint32_t i, double r0, double r1, double r2,
+                                        double& z0, double& z1, double& z2) {
+  const double* m = inv + 9ull * i;
+  z0 = m[0] * r0 + m[1] * r1 + m[2] * r2;
+  z1 = m[3] * r0 + m[4] * r1 + m[5] * r2;
+  z2 = m[6] * r0 + m[7] * r1 + m[8] * r2;
+}
+
+__device__ __forceinline__ bool stop_reached(const PcgParams& P, double delta_new, double rr) {
+  return P.stop_rule == YS_STOP_RESIDUAL ? rr <= P.st[kTolAbs] : delta_new <= P.st[kTolAbs];
+}
+
+// Initial residual, preconditioned residual and the stop threshold.
+__global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};  // r.z, r.r, g.g, g.M^-1 g
+  if (i < P.nv) {
+    const double g0 = P.rhs[3ull * i], g1 = P.rhs[3ull * i + 1], g2 = P.rhs[3ull * i + 2];
+    double r0 = g0, r1 = g1, r2 = g2;
+    if (P.zero_guess) {
+      P.x[3ull * i] = 0.0; P.x[3ull * i + 1] = 0.0; P.x[3ull * i + 2] = 0.0;
+    } else {
+      double h0, h1, h2;
+      spmv3_row(P.sets, P.nsets, P.fp32, i, P.x, h0, h1, h2);
+      r0 = g0 - h0; r1 = g1 - h1; r2 = g2 - h2;
+    }
+    double z0, z1, z2;
+    jacobi3(P.jinv, i, r0, r1, r2, z0, z1, z2);
+    P.r[3ull * i] = r0; P.r[3ull * i + 1] = r1; P.r[3ull * i + 2] = r2;
+    P.z[3ull * i] = z0; P.z[3ull * i + 1] = z1; P.z[3ull * i + 2] = z2;
+    P.p[3ull * i] = z0; P.p[3ull * i + 1] = z1; P.p[3ull * i + 2] = z2;
+    v[0] = r0 * z0 + r1 * z1 + r2 * z2;
+    v[1] = r0 * r0 + r1 * r1 + r2 * r2;
+    v[2] = g0 * g0 + g1 * g1 + g2 * g2;
+    if (!P.zero_guess) {
+      double y0, y1, y2;
+      jacobi3(P.jinv, i, g0, g1, g2, y0, y1, y2);
+      v[3] = g0 * y0 + g1 * y1 + g2 * y2;
+    }
+  }
+  if (!grid_reduce_last<4>(v, P.partials, P.tickets)) return;
+  if (threadIdx.x != 0) return;
+  double* st = P.st;
+  const double delta_new = v[0];
+  const double delta0 = P.zero_guess ? v[0] : v[3];
+  st[kDeltaNew] = delta_new;
+  st[kDelta0] = delta0;
+  st[kRR] = v[1];
+  st[kRR0] = v[1];
+  st[kGG] = v[2];
+  st[kIter] = 0.0;
+  st[kAlpha] = 0.0;
+  st[kBeta] = 0.0;
+  int status = kContinue;
+  double tol;
+  if (P.stop_rule == YS_STOP_RESIDUAL) {
+    tol = P.tolerance * P.tolerance * v[2];
+    if (!(isfinite(v[1]) && isfinite(v[2]))) status = kInvalidInit;
+    else if (v[1] <= tol) status = kConverged;
+    else if (!(isfinite(delta_new) && delta_new > 0.0)) status = kInvalidInit;
+  } else {
+    // solverKernel.pyx:588-604
+    tol = P.tolerance * delta0;
+    if (!(isfinite(delta0) && delta0 >= 0.0 && isfinite(delta_new) && delta_new >= 0.0)) status = kInvalidInit;
+    else if (!(isfinite(tol) && tol >= 0.0)) status = kInvalidInit;
+    else if (delta_new <= tol) status = kConverged;
+  }
+  if (status == kContinue && P.max_it == 0) status = kMaxIter;
+  st[kTolAbs] = tol;
+  st[kStatus] = (double)status;
+  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (i < P.nv) {
+    double q0, q1, q2;
+    spmv3_row(P.sets, P.nsets, P.fp32, i, P.p, q0, q1, q2);
+    P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
+    v[0] = P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
+  }
+  if (!grid_reduce_last<1>(v, P.partials, P.tickets + 1)) return;
+  if (threadIdx.x != 0) return;
+  double* st = P.st;
+  const double curv = v[0];
+  st[kCurv] = curv;
+  st[kDeltaOld] = st[kDeltaNew];
+  if (!isfinite(curv) || curv <= 0.0) {
+    // prepareCgIteration (solverKernel.pyx:388-404)
+    st[kAlpha] = 0.0;
+    st[kStatus] = (double)kNonSpd;
+    st[kIter] = st[kIter] + 1.0;
+    cudaGraphSetConditional(P.cond, 0u);
+  } else {
+    st[kAlpha] = st[kDeltaNew] / curv;
+  }
+}
+
+__global__ void __launch_bounds__(kPcgBlock) pcg_update_bj(PcgParams P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = P.st[kStatus] == (double)kContinue;
+  double v[2] = {0.0, 0.0};
+  if (i < P.nv && live) {
+    const double alpha = P.st[kAlpha];
+    double r[3], z[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      P.x[3ull * i + k] = P.x[3ull * i + k] + P.p[3ull * i + k] * alpha;
+      r[k] = P.r[3ull * i + k] - P.q[3ull * i + k] * alpha;
+      P.r[3ull * i + k] = r[k];
+    }
+    jacobi3(P.jinv, i, r[0], r[1], r[2], z[0], z[1], z[2]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P.z[3ull * i + k] = z[k];
+    v[0] = r[0] * z[0] + r[1] * z[1] + r[2] * z[2];
+    v[1] = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  }
+  if (!grid_reduce_last<2>(v, P.partials, P.tickets + 2)) return;
+  if (threadIdx.x != 0 || !live) return;
+  double* st = P.st;
+  const double delta_new = v[0], delta_old = st[kDeltaOld];
+  const double it = st[kIter] + 1.0;
+  st[kIter] = it;
+  st[kDeltaNew] = delta_new;
+  st[kRR] = v[1];
+  int status = kContinue;
+  // finishCgIteration (solverKernel.pyx:420-438)
+  if (!isfinite(delta_new) || delta_new < 0.0 || !isfinite(delta_old) || delta_old <= 0.0) {
+    st[kBeta] = 0.0;
+    status = kNonSpd;
+  } else {
+    st[kBeta] = delta_new / delta_old;
+    if (stop_reached(P, delta_new, v[1])) status = kConverged;
+    else if (it >= (double)P.max_it) status = kMaxIter;
+  }
+  st[kStatus] = (double)status;
+  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kPcgBlock) pcg_direction(PcgParams P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.nv) return;
+  if (P.st[kStatus] == (double)kNonSpd) return;
+  const double beta = P.st[kBeta];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) P.p[3ull * i + k] = P.z[3ull * i + k] + P.p[3ull * i + k] * beta;
+}
+
+// Iterative refinement step in FP64: x += delta, then r = rhs - H x with the
+// FP64 blocks and the deterministic norms ||r||^2, ||rhs||^2 in out[0..1].
+__global__ void __launch_bounds__(kPcgBlock) refine_add(uint32_t nv, double* __restrict__ x,
+                                                        const double* __restrict__ delta) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) x[3ull * i + k] += delta[3ull * i + k];
+}
+
+struct RefineParams {
+  SpmvSet sets[2];
+  int nsets;
+  uint32_t nv;
+  const double* rhs;
+  const double* x;
+  double* r;
+  double* out;
+  double* partials;
+  unsigned* ticket;
+};
+
+__global__ void __launch_bounds__(kPcgBlock) refine_residual(RefineParams P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (i < P.nv) {
+    double h[3];
+    spmv3_row(P.sets, P.nsets, false, i, P.x, h[0], h[1], h[2]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double g = P.rhs[3ull * i + k];
+      const double r = g - h[k];
+      P.r[3ull * i + k] = r;
+      v[0] += r * r;
+      v[1] += g * g;
+    }
+  }
+  if (!grid_reduce_last<2>(v, P.partials, P.ticket)) return;
+  if (threadIdx.x == 0) {
+    P.out[0] = v[0];
+    P.out[1] = v[1];
+  }
+}
+
+struct PcgHandle {
+  PcgParams P;
+  int preconditioner;
+  MasPcgHooks mas;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double* slots_host = nullptr;
+};
+
+static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
+                              const void* fn, unsigned grid, unsigned block, void** args) {
+  cudaKernelNodeParams kp{};
+  kp.func = const_cast<void*>(fn);
+  kp.gridDim = dim3(grid);
+  kp.blockDim = dim3(block);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = args;
+  kp.extra = nullptr;
+  return cudaGraphAddKernelNode(node, g, deps, ndeps, &kp);
+}
+
+}  // namespace ys
+
+extern "C" {
+
+uint64_t ys_pcg_workspace_doubles(uint32_t n) {
+  const uint64_t nv = (n + 2) / 3;
+  const uint64_t grid = (nv + ys::kPcgBlock - 1) / ys::kPcgBlock;
+  // r, p, q, z (n each) + slots + partials (4 per block) + tickets
+  return 4ull * 3 * nv + ys::kSlots + 4 * (grid + 1) + 8;
+}
+
+int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
+  YS_REQUIRE(args && handle, YS_ERR_INVALID, "null argument");
+  const ys_pcg_args& a = *args;
+  YS_REQUIRE(a.matrix.num_sets >= 1 && a.matrix.num_sets <= 2, YS_ERR_INVALID, "1 or 2 block sets");
+  YS_REQUIRE(a.preconditioner == YS_PREC_BLOCK_JACOBI ? a.jacobi_inverse != nullptr : a.mas != nullptr,
+             YS_ERR_INVALID, "missing preconditioner data");
+  auto* h = new ys::PcgHandle();
+  ys::PcgParams& P = h->P;
+  P.nsets = (int)a.matrix.num_sets;
+  P.fp32 = a.precision == 1;
+  for (int s = 0; s < P.nsets; ++s) {
+    P.sets[s] = ys::SpmvSet{a.matrix.values[s], a.matrix.values32[s], a.matrix.row_ptr[s], a.matrix.entry_block[s],
+                            a.matrix.entry_col[s]};
+    if (P.fp32 && !P.sets[s].values32) { delete h; YS_REQUIRE(false, YS_ERR_INVALID, "FP32 PCG needs values32"); }
+    if (!P.fp32 && !P.sets[s].values) { delete h; YS_REQUIRE(false, YS_ERR_INVALID, "FP64 PCG needs values"); }
+  }
+  P.nv = a.matrix.num_vars;
+  const uint64_t n = 3ull * P.nv;
+  P.rhs = a.rhs;
+  P.x = a.solution;
+  double* w = a.workspace;
+  P.r = w; w += n;
+  P.p = w; w += n;
+  P.q = w; w += n;
+  P.z = w; w += n;
+  P.st = w; w += ys::kSlots;
+  const unsigned grid = ys::grid_for(P.nv, ys::kPcgBlock);
+  P.partials = w; w += 4ull * (grid + 1);
+  P.tickets = reinterpret_cast<unsigned*>(w);
+  P.jinv = a.jacobi_inverse;
+  P.stop_rule = a.stop_rule;
+  P.zero_guess = a.zero_initial_guess;
+  P.tolerance = a.tolerance;
+  P.max_it = a.max_iterations;
+  h->preconditioner = a.preconditioner;
+
+  cudaError_t e = cudaGraphCreate(&h->graph, 0);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&P.cond, h->graph, 0, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) e = cudaMallocHost(&h->slots_host, sizeof(double) * ys::kSlots);
+  cudaGraphNode_t reset = nullptr, init = nullptr, loop = nullptr;
+  if (e == cudaSuccess) {
+    cudaMemsetParams mp{};
+    mp.dst = P.tickets;
+    mp.value = 0;
+    mp.pitch = 0;
+    mp.elementSize = 4;
+    mp.width = 8;
+    mp.height = 1;
+    e = cudaGraphAddMemsetNode(&reset, h->graph, nullptr, 0, &mp);
+  }
+  if (e == cudaSuccess) {
+    if (a.preconditioner == YS_PREC_BLOCK_JACOBI) {
+      void* args0[] = {&P};
+      e = ys::add_kernel(h->graph, &init, &reset, 1, (const void*)ys::pcg_init_bj, grid, ys::kPcgBlock, args0);
+    } else {
+      e = ys::mas_add_init_nodes(a.mas, h->graph, &reset, 1, &init, P.nv, P.rhs, P.x, P.r, P.p, P.q, P.z, P.st, P.partials,
+                                 P.tickets, P.sets, P.nsets, P.fp32, P.stop_rule, P.zero_guess, P.tolerance, P.max_it,
+                                 P.cond, &h->mas);
+    }
+  }
+  if (e == cudaSuccess) {
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = P.cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&loop, h->graph, &init, 1, &cp);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      cudaGraphNode_t n1 = nullptr, n2 = nullptr, n3 = nullptr;
+      void* args1[] = {&P};
+      e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot, grid, ys::kPcgBlock, args1);
+      if (e == cudaSuccess) {
+        if (a.preconditioner == YS_PREC_BLOCK_JACOBI) {
+          e = ys::add_kernel(body, &n2, &n1, 1, (const void*)ys::pcg_update_bj, grid, ys::kPcgBlock, args1);
+        } else {
+          e = ys::mas_add_update_nodes(a.mas, body, &n1, 1, &n2, &h->mas);
+        }
+      }
+      if (e == cudaSuccess)
+        e = ys::add_kernel(body, &n3, &n2, 1, (const void*)ys::pcg_direction, grid, ys::kPcgBlock, args1);
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->exec, h->graph, 0);
+  if (e != cudaSuccess) {
+    ys_set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->slots_host) cudaFreeHost(h->slots_host);
+    delete h;
+    return YS_ERR_CUDA;
+  }
+  *handle = h;
+  return YS_OK;
+}
+
+int32_t ys_pcg_launch(void* handle, void* stream) {
+  YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
+  auto* h = static_cast<ys::PcgHandle*>(handle);
+  YS_CUDA_TRY(cudaGraphLaunch(h->exec, (cudaStream_t)stream));
+  return YS_OK;
+}
+
+int32_t ys_pcg_status(void* handle, void* stream, ys_pcg_result* result) {
+  YS_REQUIRE(handle && result, YS_ERR_INVALID, "null argument");
+  auto* h = static_cast<ys::PcgHandle*>(handle);
+  cudaStream_t s = (cudaStream_t)stream;
+  YS_CUDA_TRY(cudaMemcpyAsync(h->slots_host, h->P.st, sizeof(double) * ys::kSlots, cudaMemcpyDeviceToHost, s));
+  YS_CUDA_TRY(cudaStreamSynchronize(s));
+  const double* st = h->slots_host;
+  const int status = (int)st[ys::kStatus];
+  const uint32_t it = (uint32_t)st[ys::kIter];
+  result->iterations = it;
+  result->delta0 = st[ys::kDelta0];
+  result->delta = st[ys::kDeltaNew];
+  result->residual0 = sqrt(st[ys::kRR0]);
+  result->residual = sqrt(st[ys::kRR]);
+  switch (status) {
+    case ys::kConverged: result->status = (int32_t)it; break;
+    case ys::kNonSpd: result->status = -(int32_t)it - 4; break;
+    case ys::kInvalidInit: result->status = YS_ERR_INVALID_RESIDUAL; break;
+    case ys::kMaxIter: result->status = YS_ERR_NOT_CONVERGED; break;
+    default: result->status = YS_ERR_NOT_CONVERGED; break;
+  }
+  return YS_OK;
+}
+
+int32_t ys_pcg_run(void* handle, void* stream, ys_pcg_result* result) {
+  int32_t rc = ys_pcg_launch(handle, stream);
+  if (rc != YS_OK) return rc;
+  return ys_pcg_status(handle, stream, result);
+}
+
+uint64_t ys_refine_workspace_doubles(uint32_t num_vars) {
+  return 2 + (ys::grid_for(num_vars, ys::kPcgBlock) + 1) * 2 + 2;
+}
+
+int32_t ys_refine_residual(const ys_matrix3* m, const double* rhs, double* x, const double* delta, double* r,
+                           double* workspace, double* norms_host, void* stream) {
+  YS_REQUIRE(m && m->num_sets >= 1 && m->num_sets <= 2, YS_ERR_INVALID, "bad matrix");
+  cudaStream_t s = (cudaStream_t)stream;
+  const uint32_t nv = m->num_vars;
+  const unsigned grid = ys::grid_for(nv, ys::kPcgBlock);
+  if (delta) {
+    ys::refine_add<<<grid, ys::kPcgBlock, 0, s>>>(nv, x, delta);
+    YS_CHECK_LAUNCH();
+  }
+  ys::RefineParams P{};
+  P.nsets = (int)m->num_sets;
+  for (int k = 0; k < P.nsets; ++k)
+    P.sets[k] = ys::SpmvSet{m->values[k], nullptr, m->row_ptr[k], m->entry_block[k], m->entry_col[k]};
+  P.nv = nv;
+  P.rhs = rhs;
+  P.x = x;
+  P.r = r;
+  P.out = workspace;
+  P.ticket = reinterpret_cast<unsigned*>(workspace + 2);
+  P.partials = workspace + 4;
+  YS_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned), s));
+  ys::refine_residual<<<grid, ys::kPcgBlock, 0, s>>>(P);
+  YS_CHECK_LAUNCH();
+  if (norms_host) {
+    YS_CUDA_TRY(cudaMemcpyAsync(norms_host, workspace, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    YS_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return YS_OK;
+}
+
+int32_t ys_pcg_destroy(void* handle) {
+  if (!handle) return YS_OK;
+  auto* h = static_cast<ys::PcgHandle*>(handle);
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->slots_host) cudaFreeHost(h->slots_host);
+  delete h;
+  return YS_OK;
+}
+
+}  // extern "C"

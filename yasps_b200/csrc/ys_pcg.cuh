@@ -1,0 +1,61 @@
+// Shared PCG device state and reductions (ys_pcg.cu, ys_mas.cu).
+#pragma once
+
+#include "ys_common.cuh"
+#include "ys_spmv.cuh"
+
+namespace ys {
+
+// Device scalar slots of one PCG solve (double[kSlots]).
+enum PcgSlot : int {
+  kDelta0 = 0,     // reference preconditioned residual r0^T M^-1 r0 (or rhs^T M^-1 rhs)
+  kDeltaNew = 1,   // current r^T z
+  kCurv = 2,       // p^T H p
+  kDeltaOld = 3,
+  kAlpha = 4,
+  kBeta = 5,
+  kStatus = 6,     // PcgStatus
+  kIter = 7,
+  kRR = 8,         // current r^T r
+  kRR0 = 9,
+  kGG = 10,        // rhs^T rhs
+  kTolAbs = 11,    // threshold in the units of the stop rule
+  kMaxIt = 12,
+  kSlots = 16
+};
+
+enum PcgStatus : int { kContinue = 0, kConverged = 1, kNonSpd = 2, kInvalidInit = 3, kMaxIter = 4 };
+
+constexpr int kPcgBlock = 256;
+
+// Deterministic grid-wide reduction of NV values: every block stores its
+// block sums, the last block to arrive (ticket) reduces the partials in a
+// fixed order.  Returns true in the last block, whose threads all receive
+// the totals.  partials: [NV * gridDim.x]; ticket: zero on entry, reset here.
+template <int NV>
+__device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* __restrict__ partials,
+                                                 unsigned* __restrict__ ticket) {
+  __shared__ double red[kPcgBlock / 32];
+  __shared__ bool last;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    const double s = block_sum<kPcgBlock>(v[k], red);
+    if (threadIdx.x == 0) partials[(uint64_t)k * gridDim.x + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double acc = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) acc += __ldcg(partials + (uint64_t)k * gridDim.x + b);
+    v[k] = block_sum<kPcgBlock>(acc, red);
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+}  // namespace ys

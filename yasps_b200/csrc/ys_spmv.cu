@@ -1,0 +1,132 @@
+// Row plan build and the standalone symmetric 3x3-block SpMV.
+#include <cub/cub.cuh>
+
+#include "ys_spmv.cuh"
+
+namespace ys {
+
+__global__ void spmv_entries_kernel(const uint32_t* __restrict__ pos, uint32_t nu, uint64_t* __restrict__ keys,
+                                    uint32_t* __restrict__ vals, uint32_t* __restrict__ counts,
+                                    uint32_t* __restrict__ bad) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nu) return;
+  const uint32_t r = pos[2ull * b], c = pos[2ull * b + 1];
+  if ((r % 3) || (c % 3)) { atomicOr(bad, 1u); }
+  const uint32_t ri = r / 3, ci = c / 3;
+  // Direct entry in row ri at slot 2b, transposed entry in row ci at slot 2b+1.
+  keys[2ull * b] = ((uint64_t)ri << 32) | ci;
+  vals[2ull * b] = b;
+  atomicAdd(counts + ri, 1u);
+  if (r != c) {
+    keys[2ull * b + 1] = ((uint64_t)ci << 32) | ri;
+    vals[2ull * b + 1] = b | 0x80000000u;
+    atomicAdd(counts + ci, 1u);
+  } else {
+    keys[2ull * b + 1] = ~0ull;  // sorts last, dropped
+    vals[2ull * b + 1] = 0xffffffffu;
+  }
+}
+
+__global__ void spmv_split_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals, uint32_t n,
+                                  uint32_t* __restrict__ eblock, uint32_t* __restrict__ ecol) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  eblock[p] = vals[p];
+  ecol[p] = (uint32_t)(keys[p] & 0xffffffffu);
+}
+
+__global__ void __launch_bounds__(256) spmv3_kernel(SpmvSet set, bool fp32, uint32_t nv, const double* __restrict__ x,
+                                                    double* __restrict__ y, int beta) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  double y0, y1, y2;
+  spmv3_row(&set, 1, fp32, i, x, y0, y1, y2);
+  if (beta) {
+    y0 += y[3ull * i];
+    y1 += y[3ull * i + 1];
+    y2 += y[3ull * i + 2];
+  }
+  y[3ull * i] = y0;
+  y[3ull * i + 1] = y1;
+  y[3ull * i + 2] = y2;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+static size_t spmv_cub_bytes(uint32_t n2, uint32_t nv) {
+  size_t a = 0, b = 0;
+  cub::DoubleBuffer<uint64_t> k(nullptr, nullptr);
+  cub::DoubleBuffer<uint32_t> v(nullptr, nullptr);
+  cub::DeviceRadixSort::SortPairs(nullptr, a, k, v, (int)n2);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)nv + 1);
+  return std::max(a, b);
+}
+
+static size_t spmv_ws_bytes(uint32_t nu, uint32_t nv) {
+  const uint64_t n2 = 2ull * (nu > 0 ? nu : 1);
+  return 2 * align256(8 * n2) + 2 * align256(4 * n2) + align256(4ull * (nv + 1)) + align256(16) +
+         align256(spmv_cub_bytes((uint32_t)n2, nv));
+}
+
+}  // namespace ys
+
+extern "C" {
+
+int32_t ys_spmv_plan_workspace_bytes(uint32_t nu, uint32_t num_vars, uint64_t* bytes) {
+  *bytes = ys::spmv_ws_bytes(nu, num_vars);
+  return YS_OK;
+}
+
+int32_t ys_spmv_plan_build(const uint32_t* positions, uint32_t nu, uint32_t num_vars, void* workspace,
+                           uint64_t workspace_bytes, uint32_t* row_ptr, uint32_t* entry_block, uint32_t* entry_col,
+                           void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  YS_REQUIRE(nu < 0x40000000u, YS_ERR_INVALID, "too many blocks");
+  YS_REQUIRE(workspace_bytes >= ys::spmv_ws_bytes(nu, num_vars), YS_ERR_CAPACITY, "spmv plan workspace too small");
+  YS_CUDA_TRY(cudaMemsetAsync(row_ptr, 0, 4ull * (num_vars + 1), s));
+  if (nu == 0) return YS_OK;
+  const uint32_t n2 = 2 * nu;
+  char* p = (char*)workspace;
+  auto take = [&](size_t bytes) { void* r = p; p += ys::align256(bytes); return r; };
+  uint64_t* k0 = (uint64_t*)take(8ull * n2);
+  uint64_t* k1 = (uint64_t*)take(8ull * n2);
+  uint32_t* v0 = (uint32_t*)take(4ull * n2);
+  uint32_t* v1 = (uint32_t*)take(4ull * n2);
+  uint32_t* counts = (uint32_t*)take(4ull * (num_vars + 1));
+  uint32_t* bad = (uint32_t*)take(16);
+  size_t cub_bytes = ys::spmv_cub_bytes(n2, num_vars);
+  void* tmp = take(cub_bytes);
+  YS_CUDA_TRY(cudaMemsetAsync(counts, 0, 4ull * (num_vars + 1), s));
+  YS_CUDA_TRY(cudaMemsetAsync(bad, 0, 4, s));
+  ys::spmv_entries_kernel<<<ys::grid_for(nu, 256), 256, 0, s>>>(positions, nu, k0, v0, counts, bad);
+  YS_CHECK_LAUNCH();
+  cub::DoubleBuffer<uint64_t> kb(k0, k1);
+  cub::DoubleBuffer<uint32_t> vb(v0, v1);
+  size_t tb = cub_bytes;
+  YS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tb, kb, vb, (int)n2, 0, 64, s));
+  tb = cub_bytes;
+  YS_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tb, counts, row_ptr, (int)num_vars + 1, s));
+  uint32_t total = 0, hbad = 0;
+  YS_CUDA_TRY(cudaMemcpyAsync(&total, row_ptr + num_vars, 4, cudaMemcpyDeviceToHost, s));
+  YS_CUDA_TRY(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s));
+  YS_CUDA_TRY(cudaStreamSynchronize(s));
+  YS_REQUIRE(hbad == 0, YS_ERR_INVALID, "block positions are not 3-aligned");
+  ys::spmv_split_kernel<<<ys::grid_for(total, 256), 256, 0, s>>>(kb.Current(), vb.Current(), total, entry_block,
+                                                                   entry_col);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_spmv3(const double* values, const float* values32, const uint32_t* row_ptr, const uint32_t* entry_block,
+                 const uint32_t* entry_col, uint32_t num_vars, const double* x, double* y, int32_t beta,
+                 void* stream) {
+  YS_REQUIRE((values == nullptr) != (values32 == nullptr), YS_ERR_INVALID, "pass exactly one of values/values32");
+  if (num_vars == 0) return YS_OK;
+  ys::SpmvSet set{values, values32, row_ptr, entry_block, entry_col};
+  ys::spmv3_kernel<<<ys::grid_for(num_vars, 256), 256, 0, (cudaStream_t)stream>>>(set, values32 != nullptr, num_vars,
+                                                                                   x, y, beta);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// Symmetric 3x3-block SpMV row gather (shared by ys_spmv.cu and the PCG/MAS kernels).
+//
+// Storage: the reference's upper-triangle, duplicate-free block COO
+// (PKG/matrixAndVector/matrix/matrix.pyx:101-113); a block (r, c) with r < c
+// implies its transpose.  The row plan lists, for variable i, the stored
+// blocks with row i (direct) and col i (transposed, flag bit 31), so every
+// output row is a gather with a fixed summation order: deterministic and
+// free of atomics.  The second read of an off-diagonal block (from the other
+// row) is an L2 hit when rows are processed in (Morton) order.
+#pragma once
+
+#include "ys_common.cuh"
+
+namespace ys {
+
+struct SpmvSet {
+  const double* values;
+  const float* values32;
+  const uint32_t* row_ptr;
+  const uint32_t* entry_block;
+  const uint32_t* entry_col;
+};
+
+template <typename T>
+__device__ __forceinline__ void spmv3_row_accumulate(const T* __restrict__ vals, const uint32_t* __restrict__ row_ptr,
+                                                     const uint32_t* __restrict__ eblock,
+                                                     const uint32_t* __restrict__ ecol, uint32_t i,
+                                                     const double* __restrict__ x, double& y0, double& y1,
+                                                     double& y2) {
+  const uint32_t e0 = row_ptr[i], e1 = row_ptr[i + 1];
+  T a0 = 0, a1 = 0, a2 = 0;
+  for (uint32_t e = e0; e < e1; ++e) {
+    const uint32_t eb = __ldg(eblock + e);
+    const uint32_t j = __ldg(ecol + e);
+    const T* b = vals + 9ull * (eb & 0x7fffffffu);
+    const T x0 = (T)__ldg(x + 3ull * j), x1 = (T)__ldg(x + 3ull * j + 1), x2 = (T)__ldg(x + 3ull * j + 2);
+    const T b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2), b3 = __ldg(b + 3), b4 = __ldg(b + 4),
+            b5 = __ldg(b + 5), b6 = __ldg(b + 6), b7 = __ldg(b + 7), b8 = __ldg(b + 8);
+    if (eb & 0x80000000u) {
+      a0 += b0 * x0 + b3 * x1 + b6 * x2;
+      a1 += b1 * x0 + b4 * x1 + b7 * x2;
+      a2 += b2 * x0 + b5 * x1 + b8 * x2;
+    } else {
+      a0 += b0 * x0 + b1 * x1 + b2 * x2;
+      a1 += b3 * x0 + b4 * x1 + b5 * x2;
+      a2 += b6 * x0 + b7 * x1 + b8 * x2;
+    }
+  }
+  y0 += (double)a0;
+  y1 += (double)a1;
+  y2 += (double)a2;
+}
+
+// y_i = sum over the (up to two) block sets.
+__device__ __forceinline__ void spmv3_row(const SpmvSet* sets, int nsets, bool fp32, uint32_t i,
+                                          const double* __restrict__ x, double& y0, double& y1, double& y2) {
+  y0 = y1 = y2 = 0.0;
+  for (int s = 0; s < nsets; ++s) {
+    if (fp32)
+      spmv3_row_accumulate<float>(sets[s].values32, sets[s].row_ptr, sets[s].entry_block, sets[s].entry_col, i, x, y0,
+                                  y1, y2);
+    else
+      spmv3_row_accumulate<double>(sets[s].values, sets[s].row_ptr, sets[s].entry_block, sets[s].entry_col, i, x, y0,
+                                   y1, y2);
+  }
+}
+
+}  // namespace ys

@@ -1,0 +1,114 @@
+"""Energy expressions of the Newton inner loop (fixed CUDA element kernels).
+
+Each function mirrors the signature of the reference example helper that
+builds the same energy symbolically, and returns an expression to pass to
+``primitive.addAttribute(name, computed_attribute=...)``:
+
+* :func:`stable_neo_hookean` -- ``examples/dropping_in_container_mixed/helpers.py:102-127``
+* :func:`inertia`            -- ``examples/dropping_in_container_mixed/helpers.py:138-141``
+
+Parameters (``mu``, ``lam``, ``dt``, ``mass``) may be Python floats, 1x1
+scene constants, or per-instance attributes of the energy's primitive.
+"""
+
+from __future__ import annotations
+
+from .graph import CONSTANT, DATA, JOIN, UNION, attribute
+
+
+class EnergyExpr:
+  kind = "energy"
+
+  def __init__(self):
+    self.attribute = None
+
+  def bind(self, att) -> None:
+    if self.attribute is not None:
+      raise ValueError("an energy expression can be bound to one attribute only")
+    self.attribute = att
+    self.validate(att.correspondance)
+
+  def validate(self, prim) -> None:  # pragma: no cover - overridden
+    pass
+
+
+def _param(v, prim, name):
+  """Normalise a parameter to ('value', float) or ('array', attribute)."""
+  if isinstance(v, attribute):
+    if v.size != 1:
+      raise ValueError(f"{name} must be a scalar attribute")
+    owner = v.correspondance
+    if getattr(owner, "type", None) == "scene":
+      return ("scene", v)
+    if owner is not prim:
+      raise ValueError(f"{name} must live on the energy's primitive or on the scene")
+    return ("array", v)
+  return ("value", float(v))
+
+
+def _join_of_positions(att, name, dim):
+  if not isinstance(att, attribute) or att.operator != JOIN:
+    raise ValueError(f"{name} must be a JOIN attribute (addAttribute(..., through=..., source=...))")
+  if att.through.dimension != dim or att.source.size != 3:
+    raise ValueError(f"{name} must gather {dim} 3-vectors")
+  if att.source.operator not in (DATA, CONSTANT, UNION):
+    raise ValueError(f"{name}: the gathered attribute must be DATA, CONSTANT or a UNION of them")
+
+
+class SnhEnergy(EnergyExpr):
+  kind = "snh"
+
+  def __init__(self, tet_position_rest, tet_position, mu, lam, dt):
+    super().__init__()
+    _join_of_positions(tet_position, "tet_position", 4)
+    _join_of_positions(tet_position_rest, "tet_position_rest", 4)
+    self.position = tet_position
+    self.rest = tet_position_rest
+    self.mu, self.lam, self.dt = mu, lam, dt
+
+  def validate(self, prim) -> None:
+    if self.position.correspondance is not prim or self.rest.correspondance is not prim:
+      raise ValueError("stable_neo_hookean: the tet attributes must live on the energy's primitive")
+    self.mu_p = _param(self.mu, prim, "mu")
+    self.lam_p = _param(self.lam, prim, "lam")
+    self.dt_p = _param(self.dt, prim, "dt")
+    if self.dt_p[0] == "array":
+      raise ValueError("dt must be a scalar")
+
+
+class InertiaEnergy(EnergyExpr):
+  kind = "inertia"
+
+  def __init__(self, x_before, vel, dt, x, mass, gravity):
+    super().__init__()
+    for a, name in ((x, "x"), (x_before, "x_before")):
+      if not isinstance(a, attribute) or a.size != 3 or a.operator not in (DATA, CONSTANT):
+        raise ValueError(f"inertia: {name} must be a 3-vector DATA/CONSTANT attribute of the primitive")
+    if vel is not None and (not isinstance(vel, attribute) or vel.size != 3):
+      raise ValueError("inertia: vel must be a 3-vector attribute or None")
+    self.x, self.x_before, self.vel = x, x_before, vel
+    self.dt, self.mass = dt, mass
+    self.gravity = tuple(float(g) for g in gravity)
+
+  def validate(self, prim) -> None:
+    for a in (self.x, self.x_before, self.vel):
+      if a is not None and a.correspondance is not prim:
+        raise ValueError("inertia: attributes must live on the energy's primitive")
+    if self.x.operator != DATA:
+      raise ValueError("inertia: x must be a DATA attribute")
+    self.dt_p = _param(self.dt, prim, "dt")
+    self.mass_p = _param(self.mass, prim, "mass")
+
+
+def stable_neo_hookean(tet_position_rest, tet_position, mu, lam, dt) -> SnhEnergy:
+  """Stable Neo-Hookean tetrahedral energy scaled by ``dt^2``."""
+  return SnhEnergy(tet_position_rest, tet_position, mu, lam, dt)
+
+
+def inertia(x_before, vel, dt, x, mass, gravity=(0.0, -9.8, 0.0)) -> InertiaEnergy:
+  """``1/2 (x - x~)^T m (x - x~)`` with ``x~ = x_before + vel dt + gravity dt^2``.
+
+  The reference helper hard-codes ``gravity = (0, -9.8, 0)``; it is a
+  parameter here.
+  """
+  return InertiaEnergy(x_before, vel, dt, x, mass, gravity)

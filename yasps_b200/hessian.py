@@ -1,0 +1,502 @@
+"""Assembled Hessian and gradient of a set of energy terms.
+
+Mirrors the reference ``hessian`` (``PKG/matrixAndVector/matrix/hessian.pyx``):
+the same public attributes (``blocks_flattened``, ``block_positions``,
+``blocks_start_indices``, ``block_counts``, ``block_dimensions``, their
+``_dynamic`` twins, ``diagonal``, ``diagonal_blocks``, ``gradient``, ``wrt``,
+``gradient_segments_start_cpu``, ``diagonal_blocks_start_cpu``), ``compute``,
+``spmv`` and ``+``.  Storage is the reference's: upper-triangle duplicate-free
+block COO sorted by ``(h, w, row, col)``, values row-major per block,
+diagonal blocks full, off-diagonal blocks implying their transpose.
+
+Pipeline (all on the device through libys_newton.so):
+
+* setup (once per static structure; dynamic terms every ``compute``):
+  slot codes -> local compression -> coordinates -> unique sort giving the
+  pattern, the lookup and the deterministic assembly plan;
+* ``compute``: element kernels write per-occurrence records, assembly sums
+  them in a fixed order (bit-reproducible), diagonal blocks are extracted.
+"""
+
+from __future__ import annotations
+
+from typing import List, Optional
+
+import numpy as np
+
+from . import _lib as L
+from .graph import CONSTANT, DATA, JOIN, UNION, resolve_leaf_children
+
+
+def _torch():
+  import torch
+  return torch
+
+
+def _dev():
+  from .graph import _device
+  return _device()
+
+
+class vector:
+  """Device vector (``PKG/matrixAndVector/vector/vector.pyx``)."""
+
+  def __init__(self, size: int, value=None):
+    torch = _torch()
+    self.size = int(size)
+    self.value = torch.zeros(self.size, dtype=torch.float64, device=_dev()) if value is None else value
+
+  def updateValue(self, values) -> None:
+    torch = _torch()
+    src = values if isinstance(values, torch.Tensor) else torch.from_numpy(np.asarray(values, dtype=np.float64))
+    self.value.copy_(src.reshape(-1))
+
+  def get(self) -> np.ndarray:
+    return self.value.detach().cpu().numpy()
+
+
+class _Term:
+  """One energy applied to all instances of its primitive."""
+
+  def __init__(self, request, wrt, wrt_start):
+    self.request = request
+    self.energy_att = request.energy
+    self.expr = request.energy.expr
+    self.prim = request.energy.correspondance
+    self.projection_method = int(request.projection_method)
+    self.dynamic = bool(request.dynamic_instances)
+    self.local_targets = list(request.targets)
+    self.wrt = wrt
+    self.wrt_start = wrt_start
+    self._const_cache = {}
+
+  @property
+  def n(self) -> int:
+    return int(self.prim.numInstances)
+
+  def leaf_kind(self, leaf):
+    if leaf.operator == CONSTANT:
+      return 0, 0
+    if self.local_targets and not any(leaf is t for t in self.local_targets):
+      return 0, 0
+    for k, w in enumerate(self.wrt):
+      if w is leaf:
+        return 2, int(self.wrt_start[k])
+    return 1, 0
+
+  # -- slot codes ---------------------------------------------------------------
+  def codes(self):
+    """Device (codes int32 [n*K], sizes int16 [n*K], K, slot_stride)."""
+    torch = _torch()
+    n = self.n
+    if self.expr.kind == "snh":
+      join = self.expr.position
+      conn = join.through.value
+      leaves, prefix = resolve_leaf_children(join.source)
+      dim = 4
+    elif self.expr.kind == "inertia":
+      key = ("identity", n)
+      if key not in self._const_cache:
+        self._const_cache[key] = torch.arange(max(n, 1), dtype=torch.int32, device=_dev())
+      conn = self._const_cache[key]
+      leaves, prefix = [self.expr.x], [0, n]
+      dim = 1
+    else:  # pragma: no cover
+      raise NotImplementedError(self.expr.kind)
+    nc = len(leaves)
+    kinds, starts = zip(*(self.leaf_kind(l) for l in leaves))
+    stride = 2 if nc > 1 else 1
+    K = dim * stride
+    codes = torch.empty(max(n * K, 1), dtype=torch.int32, device=_dev())
+    sizes = torch.empty(max(n * K, 1), dtype=torch.int16, device=_dev())
+    arr = lambda v, t: (t * len(v))(*v)
+    L.call("ys_join_union_indices", L.ptr(conn), n, dim, nc, arr(prefix, L.u32), arr(kinds, L.i32),
+           arr(starts, L.u32), 3, L.ptr(codes), L.ptr(sizes), L.stream_ptr())
+    return codes, sizes, K, stride
+
+  # -- element evaluation --------------------------------------------------------
+  def _param(self, p, n):
+    torch = _torch()
+    kind, v = p
+    if kind == "value":
+      return None, float(v)
+    if kind == "scene":
+      return None, v.scalar()
+    return v.value, 0.0
+
+  def _union3(self, att):
+    leaves, prefix = resolve_leaf_children(att)
+    u = L.Union3()
+    for c, leaf in enumerate(leaves):
+      u.child[c] = L.ptr(leaf.value)
+    for c, p in enumerate(prefix):
+      u.prefix[c] = p
+    u.num_children = len(leaves)
+    return u
+
+  def evaluate(self, plan, block_records, grad_records, energy=None):
+    torch = _torch()
+    n = self.n
+    if n == 0:
+      return
+    e = self.expr
+    s = L.stream_ptr()
+    if e.kind == "snh":
+      if e.rest.through is not e.position.through:
+        raise ValueError("stable_neo_hookean: rest and current positions must use the same connectivity")
+      a = L.SnhArgs()
+      a.position = self._union3(e.position.source)
+      a.rest = self._union3(e.rest.source)
+      a.tets = L.ptr(e.position.through.value)
+      a.num_elements = n
+      mu_arr, a.mu_value = self._param(e.mu_p, n)
+      lam_arr, a.lam_value = self._param(e.lam_p, n)
+      a.mu, a.lam = L.ptr(mu_arr), L.ptr(lam_arr)
+      a.dt = self._param(e.dt_p, n)[1]
+      a.projection_method = self.projection_method
+      a.plan = plan
+      a.block_records, a.grad_records = L.ptr(block_records), L.ptr(grad_records)
+      a.energy = L.ptr(energy)
+      key = ("work", n)
+      if key not in self._const_cache:
+        self._const_cache[key] = (torch.empty(n, dtype=torch.int32, device=_dev()),
+                                  torch.zeros(1, dtype=torch.int32, device=_dev()))
+      wl, wc = self._const_cache[key]
+      a.work_list, a.work_count = L.ptr(wl), L.ptr(wc)
+      import ctypes
+      L.call("ys_snh_eval", ctypes.byref(a), s)
+    elif e.kind == "inertia":
+      import ctypes
+      a = L.InertiaArgs()
+      a.position = L.ptr(e.x.value)
+      a.x_before = L.ptr(e.x_before.value)
+      a.velocity = L.ptr(e.vel.value) if e.vel is not None else None
+      m_arr, m_val = self._param(e.mass_p, n)
+      if m_arr is None:
+        key = ("mass", n, m_val)
+        if key not in self._const_cache:
+          self._const_cache[key] = torch.full((n,), m_val, dtype=torch.float64, device=_dev())
+        m_arr = self._const_cache[key]
+      a.mass = L.ptr(m_arr)
+      a.dt = self._param(e.dt_p, n)[1]
+      for k in range(3):
+        a.gravity[k] = e.gravity[k]
+      a.num_vertices = n
+      a.plan = plan
+      a.block_records, a.grad_records = L.ptr(block_records), L.ptr(grad_records)
+      a.energy = L.ptr(energy)
+      L.call("ys_inertia_eval", ctypes.byref(a), s)
+
+
+class _Pattern:
+  """Device pattern + assembly plan of one occurrence set."""
+
+  def __init__(self, coords, dims, m):
+    import ctypes
+    torch = _torch()
+    self.m = m
+    cap = max(m, 1)
+    i32 = lambda k: torch.empty(max(k, 1), dtype=torch.int32, device=_dev())
+    self.positions = i32(2 * cap)
+    self.dims = torch.empty(2 * cap, dtype=torch.int16, device=_dev())
+    self.value_offset = i32(cap + 1)
+    self.lookup = i32(cap)
+    self.record = i32(cap)
+    self.record_begin = i32(cap)
+    self.record_count = i32(cap)
+    ws = L.u64(0)
+    L.call("ys_pattern_workspace_bytes", m, ctypes.byref(ws))
+    work = torch.empty(int(ws.value), dtype=torch.uint8, device=_dev())
+    out = L.PatternOut()
+    out.positions, out.block_dims, out.value_offset = L.ptr(self.positions), L.ptr(self.dims), L.ptr(self.value_offset)
+    out.lookup, out.record = L.ptr(self.lookup), L.ptr(self.record)
+    out.record_begin, out.record_count = L.ptr(self.record_begin), L.ptr(self.record_count)
+    L.call("ys_pattern_build", L.ptr(coords), L.ptr(dims), m, L.ptr(work), int(ws.value), ctypes.byref(out),
+           L.stream_ptr())
+    self.num_unique = int(out.num_unique)
+    nc = int(out.num_categories)
+    self.category_dims = [int(x) for x in out.category_dims[:2 * nc]]
+    self.category_counts = [int(x) for x in out.category_counts[:nc]]
+    self.category_starts = [int(x) for x in out.category_starts[:nc + 1]] if nc else [0]
+    self.total_records = int(out.total_records)
+    self.total_values = self.category_starts[-1] if nc else 0
+    self.all3 = nc == 1 and self.category_dims == [3, 3]
+
+
+class _BlockSet:
+  def __init__(self):
+    self.terms: List[_Term] = []
+    self.pattern: Optional[_Pattern] = None
+    self.values = None
+    self.values32 = None
+    self.records = None
+    self.infos = []
+    self.spmv = None  # (row_ptr, entry_block, entry_col)
+
+
+class hessian:
+  """Assembled Hessian of energy terms w.r.t. the minimisation targets."""
+
+  def __init__(self, wrt, requests_static=(), requests_dynamic=()):
+    self.__wrt = list(wrt)
+    sizes = [w.size * w.correspondance.numInstances for w in self.__wrt]
+    self.gradient_segments_start_cpu = [0] + np.cumsum(sizes).tolist()
+    dsz = [w.size * w.size * w.correspondance.numInstances for w in self.__wrt]
+    self.diagonal_blocks_start_cpu = [0] + np.cumsum(dsz).tolist()
+    self.wrt_start_indices = self.gradient_segments_start_cpu
+    self.rows = self.cols = int(self.gradient_segments_start_cpu[-1])
+    if self.rows <= 0:
+      raise ValueError("hessian: total target size must be positive")
+    self.symmetric_storage = True
+    self._requests_static = list(requests_static)
+    self._requests_dynamic = list(requests_dynamic)
+    self._setup = False
+    self.want_fp32 = False
+    self.values32_current = False
+    self.gradient: Optional[vector] = None
+    self.diagonal = None
+    self.diagonal_blocks = None
+    self.energy_buffers = {}
+
+  # -- composition ----------------------------------------------------------------
+  @property
+  def wrt(self):
+    return self.__wrt
+
+  def __add__(self, other: "hessian") -> "hessian":
+    if not isinstance(other, hessian):
+      raise TypeError("hessian.__add__: unsupported operand")
+    if len(self.wrt) != len(other.wrt) or any(a is not b for a, b in zip(self.wrt, other.wrt)):
+      raise ValueError("hessian.__add__: wrt mismatch")
+    return hessian(self.wrt, self._requests_static + other._requests_static,
+                   self._requests_dynamic + other._requests_dynamic)
+
+  # -- setup -----------------------------------------------------------------------
+  def _plan_terms(self, terms):
+    """Codes, compression, coordinates for a list of terms (device)."""
+    import ctypes
+    torch = _torch()
+    s = L.stream_ptr()
+    info = []
+    total = 0
+    for t in terms:
+      n = t.n
+      codes, sizes, K, stride = t.codes()
+      perm = torch.empty(max(n * K, 1), dtype=torch.int16, device=_dev())
+      outer = torch.empty(n + 1, dtype=torch.int32, device=_dev())
+      L.call("ys_compress_indices", L.ptr(codes), L.ptr(sizes), n, K, L.ptr(perm), None, L.ptr(outer), s)
+      m = int(outer[n].item()) if n else 0
+      info.append(dict(term=t, codes=codes, sizes=sizes, K=K, stride=stride, perm=perm, outer=outer, m=m, off=total))
+      total += m
+    coords = torch.empty(max(2 * total, 2), dtype=torch.int32, device=_dev())
+    dims = torch.empty(max(2 * total, 2), dtype=torch.int16, device=_dev())
+    for d in info:
+      if d["m"] == 0:
+        continue
+      off = d["off"]
+      L.call("ys_compute_coordinates", L.ptr(d["codes"]), L.ptr(d["perm"]), L.ptr(d["sizes"]), L.ptr(d["outer"]),
+             d["term"].n, d["K"], coords.data_ptr() + 8 * off, dims.data_ptr() + 4 * off, s)
+    return info, coords, dims, total
+
+  def _gradient_plan(self, infos):
+    torch = _torch()
+    s = L.stream_ptr()
+    total = 0
+    for d in infos:
+      n, K = d["term"].n, d["K"]
+      d["gouter"] = torch.empty(n + 1, dtype=torch.int32, device=_dev())
+      L.call("ys_gradient_coordinates", L.ptr(d["codes"]), L.ptr(d["sizes"]), n, K, L.ptr(d["gouter"]), None, None,
+             None, s)
+      d["gm"] = int(d["gouter"][n].item()) if n else 0
+      d["goff"] = total
+      total += d["gm"]
+    coords = torch.empty(max(2 * total, 2), dtype=torch.int32, device=_dev())
+    dims = torch.empty(max(2 * total, 2), dtype=torch.int16, device=_dev())
+    for d in infos:
+      if d["gm"] == 0:
+        continue
+      n, K = d["term"].n, d["K"]
+      L.call("ys_gradient_coordinates", L.ptr(d["codes"]), L.ptr(d["sizes"]), n, K, L.ptr(d["gouter"]),
+             coords.data_ptr() + 8 * d["goff"], dims.data_ptr() + 4 * d["goff"], s)
+    pat = _Pattern(coords, dims, total)
+    self._grad_pattern = pat
+    self._grad_records = torch.empty(max(pat.total_records, 1), dtype=torch.float64, device=_dev())
+
+  def _build_set(self, bs: _BlockSet, infos, coords, dims, total):
+    torch = _torch()
+    bs.pattern = _Pattern(coords, dims, total)
+    bs.records = torch.empty(max(bs.pattern.total_records, 1), dtype=torch.float64, device=_dev())
+    if bs.values is None or bs.values.numel() < max(bs.pattern.total_values, 1):
+      bs.values = torch.zeros(max(bs.pattern.total_values, 1), dtype=torch.float64, device=_dev())
+    bs.values32 = None
+    bs.infos = infos
+    bs.spmv = None
+
+  def _term_plan(self, d, bs):
+    p = L.TermPlan()
+    p.codes = L.ptr(d["codes"])
+    p.K = d["K"]
+    p.slot_stride = d["stride"]
+    p.coord_outer = L.ptr(d["outer"])
+    p.record = bs.pattern.record.data_ptr() + 4 * d["off"]
+    p.grad_outer = L.ptr(d["gouter"])
+    p.grad_record = self._grad_pattern.record.data_ptr() + 4 * d["goff"]
+    return p
+
+  def _setup_compute(self):
+    torch = _torch()
+    wrt = self.__wrt
+    self._static = _BlockSet()
+    self._dynamic = _BlockSet()
+    self._static.terms = [_Term(r, wrt, self.wrt_start_indices) for r in self._requests_static]
+    self._dynamic.terms = [_Term(r, wrt, self.wrt_start_indices) for r in self._requests_dynamic]
+    self._static_infos = self._plan_terms(self._static.terms)
+    self._build_set(self._static, *self._static_infos)
+    self.gradient = vector(self.rows)
+    self.diagonal = torch.zeros(self.rows, dtype=torch.float64, device=_dev())
+    self.diagonal_blocks = torch.zeros(max(self.diagonal_blocks_start_cpu[-1], 1), dtype=torch.float64,
+                                       device=_dev())
+    self._setup = True
+
+  def _refresh_dynamic(self):
+    infos = self._plan_terms(self._dynamic.terms)
+    self._build_set(self._dynamic, *infos)
+    self._gradient_plan(self._static_infos[0] + infos[0])
+
+  # -- numeric --------------------------------------------------------------------
+  def compute(self, local_gradient: Optional[vector] = None):
+    torch = _torch()
+    if not self._setup:
+      self._setup_compute()
+      if not self._dynamic.terms:
+        self._gradient_plan(self._static_infos[0])
+    if self._dynamic.terms:
+      self._refresh_dynamic()
+    if local_gradient is not None:
+      self.gradient = local_gradient
+    s = L.stream_ptr()
+    for bs in (self._static, self._dynamic):
+      for d in bs.infos:
+        t = d["term"]
+        eng = self.energy_buffers.get(id(t))
+        t.evaluate(self._term_plan(d, bs), bs.records, self._grad_records, eng)
+    for bs in (self._static, self._dynamic):
+      self._assemble(bs)
+    self.gradient.value.zero_()
+    gp = self._grad_pattern
+    if gp.num_unique:
+      L.call("ys_assemble_strided", L.ptr(self._grad_records), L.ptr(gp.record_begin), L.ptr(gp.record_count),
+             L.ptr(gp.positions), 2, L.ptr(gp.dims), gp.num_unique, L.ptr(self.gradient.value), s)
+    self.diagonal.zero_()
+    self.diagonal_blocks.zero_()
+    nat = len(self.__wrt)
+    arr = lambda v: (L.u32 * len(v))(*v)
+    seg = arr(self.gradient_segments_start_cpu)
+    asz = arr([w.size for w in self.__wrt])
+    dst = arr(self.diagonal_blocks_start_cpu[:nat])
+    for bs in (self._static, self._dynamic):
+      p = bs.pattern
+      if p is None or p.num_unique == 0:
+        continue
+      L.call("ys_extract_diagonal", L.ptr(bs.values), L.ptr(p.positions), L.ptr(p.dims), L.ptr(p.value_offset),
+             p.num_unique, nat, seg, asz, dst, L.ptr(self.diagonal_blocks), L.ptr(self.diagonal), 1, s)
+    self.values32_current = self.want_fp32
+    return self
+
+  def _assemble(self, bs: _BlockSet):
+    torch = _torch()
+    p = bs.pattern
+    if p is None or p.num_unique == 0:
+      return
+    s = L.stream_ptr()
+    v32 = None
+    if self.want_fp32:
+      if bs.values32 is None or bs.values32.numel() < bs.values.numel():
+        bs.values32 = torch.zeros(bs.values.numel(), dtype=torch.float32, device=_dev())
+      v32 = bs.values32
+    if p.all3:
+      L.call("ys_assemble3", L.ptr(bs.records), L.ptr(p.record_begin), L.ptr(p.record_count), L.ptr(p.value_offset),
+             p.num_unique, L.ptr(bs.values), L.ptr(v32), s)
+    else:
+      L.call("ys_assemble", L.ptr(bs.records), L.ptr(p.record_begin), L.ptr(p.record_count), L.ptr(p.value_offset),
+             L.ptr(p.dims), p.num_unique, L.ptr(bs.values), L.ptr(v32), s)
+
+  # -- reference attribute surface ---------------------------------------------------
+  def _set_attr(self, bs, name):
+    p = bs.pattern if bs is not None else None
+    if p is None or p.num_unique == 0:
+      return {"values": _torch().zeros(1, dtype=_torch().float64, device=_dev()),
+              "positions": _torch().zeros(2, dtype=_torch().int32, device=_dev()), "starts": [],
+              "counts": [], "dims": []}[name]
+    return {"values": bs.values, "positions": p.positions[:2 * p.num_unique], "starts": p.category_starts,
+            "counts": p.category_counts, "dims": p.category_dims}[name]
+
+  blocks_flattened = property(lambda self: self._set_attr(self._static, "values"))
+  block_positions = property(lambda self: self._set_attr(self._static, "positions"))
+  blocks_start_indices = property(lambda self: self._set_attr(self._static, "starts"))
+  block_counts = property(lambda self: self._set_attr(self._static, "counts"))
+  block_dimensions = property(lambda self: self._set_attr(self._static, "dims"))
+  blocks_flattened_dynamic = property(lambda self: self._set_attr(self._dynamic, "values"))
+  block_positions_dynamic = property(lambda self: self._set_attr(self._dynamic, "positions"))
+  blocks_start_indices_dynamic = property(lambda self: self._set_attr(self._dynamic, "starts"))
+  block_counts_dynamic = property(lambda self: self._set_attr(self._dynamic, "counts"))
+  block_dimensions_dynamic = property(lambda self: self._set_attr(self._dynamic, "dims"))
+
+  @property
+  def block_sets(self):
+    return [bs for bs in (self._static, self._dynamic) if bs.pattern is not None and bs.pattern.num_unique]
+
+  def ensure_fp32(self):
+    """FP32 copies of the block values (assembled FP64 sums cast once)."""
+    torch = _torch()
+    if self.values32_current:
+      return
+    for bs in self.block_sets:
+      bs.values32 = bs.values.to(torch.float32)
+    self.values32_current = True
+
+  def spmv_plan(self, bs: _BlockSet):
+    """Row plan of a 3x3 block set for the deterministic SpMV."""
+    import ctypes
+    torch = _torch()
+    if bs.spmv is not None:
+      return bs.spmv
+    p = bs.pattern
+    if not p.all3:
+      raise NotImplementedError("the device SpMV and PCG support 3x3 blocks (3-DoF variables)")
+    nv = self.rows // 3
+    ws = L.u64(0)
+    L.call("ys_spmv_plan_workspace_bytes", p.num_unique, nv, ctypes.byref(ws))
+    work = torch.empty(int(ws.value), dtype=torch.uint8, device=_dev())
+    row_ptr = torch.empty(nv + 1, dtype=torch.int32, device=_dev())
+    eb = torch.empty(2 * p.num_unique, dtype=torch.int32, device=_dev())
+    ec = torch.empty(2 * p.num_unique, dtype=torch.int32, device=_dev())
+    L.call("ys_spmv_plan_build", L.ptr(p.positions), p.num_unique, nv, L.ptr(work), int(ws.value), L.ptr(row_ptr),
+           L.ptr(eb), L.ptr(ec), L.stream_ptr())
+    bs.spmv = (row_ptr, eb, ec)
+    return bs.spmv
+
+  def spmv(self, direction: vector, transpose: bool = False, fp32: bool = False) -> vector:
+    """``H x`` (symmetric, so ``transpose`` gives the same product)."""
+    out = vector(self.rows)
+    first = True
+    for bs in self.block_sets:
+      row_ptr, eb, ec = self.spmv_plan(bs)
+      vals = (None, bs.values32) if fp32 else (bs.values, None)
+      L.call("ys_spmv3", L.ptr(vals[0]), L.ptr(vals[1]), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), self.rows // 3,
+             L.ptr(direction.value), L.ptr(out.value), 0 if first else 1, L.stream_ptr())
+      first = False
+    return out
+
+  def matrix3(self, fp32=False):
+    """C descriptor of the (up to two) 3x3 block sets."""
+    m = L.Matrix3()
+    sets = self.block_sets
+    m.num_sets = len(sets)
+    for k, bs in enumerate(sets):
+      row_ptr, eb, ec = self.spmv_plan(bs)
+      m.values[k] = L.ptr(bs.values)
+      m.values32[k] = L.ptr(bs.values32) if bs.values32 is not None else None
+      m.row_ptr[k], m.entry_block[k], m.entry_col[k] = L.ptr(row_ptr), L.ptr(eb), L.ptr(ec)
+    m.num_vars = self.rows // 3
+    return m

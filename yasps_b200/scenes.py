@@ -110,6 +110,56 @@ class FemCube:
     return codes, np.full_like(codes, 3)
 
 
+def fem_scene(cube: "FemCube", name: str = "fem_cube", projection_method: int = 1):
+  """Build the cube with the public scene API (the reference example idiom).
+
+  Returns ``(scene, handles)`` where ``handles`` maps names to the attributes
+  a Newton loop updates (``free_position``, ``pinned_position``, ...).
+  """
+  from .energies import inertia, stable_neo_hookean
+  from .scene import scene as make_scene
+
+  sc = make_scene(name)
+  dt = sc.addConstant("dt")
+  dt.updateValue(cube.dt)
+  mu = sc.addConstant("mu")
+  mu.updateValue(cube.mu)
+  lam = sc.addConstant("lam")
+  lam.updateValue(cube.lam)
+  body = sc.addMesh("body")
+  pinned = body.addPrimitive("pinned", numInstances=cube.pinned_count)
+  pinned_position = pinned.addAttribute("position", rows=3, cols=1)
+  pinned_position.updateValue(cube.pinned_position)
+  pinned_rest = pinned.addConstant("rest_position", rows=3, cols=1)
+  pinned_rest.updateValue(cube.pinned_rest)
+  free = body.addPrimitive("free", numInstances=cube.free_count)
+  free_position = free.addAttribute("position", rows=3, cols=1)
+  free_position.updateValue(cube.free_position)
+  free_rest = free.addConstant("rest_position", rows=3, cols=1)
+  free_rest.updateValue(cube.free_rest)
+  last = free.addConstant("last_position", rows=3, cols=1)
+  last.updateValue(cube.free_position)
+  vel = free.addConstant("velocity", rows=3, cols=1)
+  vel.updateValue(cube.velocity)
+  mass = free.addConstant("mass")
+  mass.updateValue(cube.mass)
+  verts = body.addPrimitiveUnion("vertices", [pinned, free])
+  position = verts.addAttribute("position")
+  rest = verts.addAttribute("rest_position")
+  tets = body.addPrimitive("tetrahedra", numInstances=cube.tet_count)
+  to_verts = tets.addConnectivity("to_vertices", verts, cube.tets, 4)
+  tet_position = tets.addAttribute("position", through=to_verts, source=position)
+  tet_rest = tets.addAttribute("rest_position", through=to_verts, source=rest)
+  snh = tets.addAttribute("snh", computed_attribute=stable_neo_hookean(tet_rest, tet_position, mu, lam, dt))
+  kin = free.addAttribute("inertia", computed_attribute=inertia(last, vel, dt, free_position, mass,
+                                                                 gravity=tuple(cube.gravity)))
+  sc.addEnergy(snh, projection_method=projection_method)
+  sc.addEnergy(kin, projection_method=-1)
+  sc.addMinimizeTarget([free_position])
+  return sc, dict(free_position=free_position, pinned_position=pinned_position, last_position=last, velocity=vel,
+                  snh=snh, inertia=kin, tets=tets)
+
+
 def fem_cube(n: int, spacing: float = 0.1, young: float = 1e5, poisson: float = 0.4, noise: float = 0.01,
              seed: int = 0, density: float = 1000.0, dt: float = 0.01,
              gravity=(0.0, 0.0, -9.8)) -> FemCube:

@@ -1,0 +1,370 @@
+"""Linear solvers: block-Jacobi PCG and MAS-preconditioned CG.
+
+Mirrors the reference solver surface (``PKG/solver/solver.py:9-68``,
+``PKG/solver/jacobianPCGSolver.pyx:14-166``, ``PKG/solver/masSolver.py:13-126``):
+``computeSolution(active_hessian, right_hand_side, initial_guess, tolerance,
+maxIterations, zero_initial_guess) -> int``, ``reset()``, ``solution`` and
+``statistics``.  The tolerance keeps the reference meaning (a squared,
+preconditioned ratio ``r^T M^-1 r <= tol * r0^T M^-1 r0``) unless
+``stop_rule="residual"`` is given, in which case it is the true relative
+residual ``||g - H x|| / ||g||``.
+
+``masSolver(mixed_spmv=True)`` is the precision form: FP32 Hessian blocks in
+the PCG SpMV (FP32 products and row sums), FP32 MAS application, FP64 PCG
+vectors and reductions, and FP64 iterative refinement ``r = g - H x`` with
+the FP64 blocks until the FP64 residual meets the tolerance (the
+reference's ``mixed_spmv`` FP64 audit + corrective solve,
+``mas/solver.py:643-688``, iterated).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib as L
+from .hessian import vector, _dev, _torch
+from . import mas_hierarchy
+
+_STOP = {"preconditioned": L.YS_STOP_PRECONDITIONED, "residual": L.YS_STOP_RESIDUAL}
+
+
+class _PcgCache:
+  def __init__(self):
+    self.key = None
+    self.handle = None
+    self.keepalive = None
+
+  def get(self, key, build):
+    if key != self.key:
+      self.release()
+      self.handle, self.keepalive = build()
+      self.key = key
+    return self.handle
+
+  def release(self):
+    if self.handle is not None:
+      L.call("ys_pcg_destroy", self.handle)
+    self.handle, self.key, self.keepalive = None, None, None
+
+
+def _as_tensor(v):
+  if v is None:
+    return None
+  return v.value if hasattr(v, "value") else v
+
+
+class _PcgBase:
+  def __init__(self, stop_rule="preconditioned"):
+    if stop_rule not in _STOP:
+      raise ValueError("stop_rule must be 'preconditioned' or 'residual'")
+    self.stop_rule = stop_rule
+    self._solution = None
+    self._work = None
+    self._cache = _PcgCache()
+    self._statistics = {}
+    self.last_result = None
+
+  @property
+  def solution(self):
+    return self._solution
+
+  @property
+  def statistics(self) -> dict:
+    return dict(self._statistics)
+
+  def reset(self):
+    self._cache.release()
+    self._solution = None
+    self._work = None
+    self._statistics = {}
+
+  def _buffers(self, n):
+    torch = _torch()
+    if self._solution is None or self._solution.numel() != n:
+      self._solution = torch.zeros(n, dtype=torch.float64, device=_dev())
+      self._work = torch.zeros(int(L.load().ys_pcg_workspace_doubles(n)), dtype=torch.float64, device=_dev())
+      self._cache.release()
+
+  def _run_pcg(self, H, rhs, x, fp32, prec_kind, jinv, mas_handle, tol, maxit, zero_guess, stop_rule):
+    """One device PCG solve into ``x``; returns the ys_pcg_result."""
+    key = (id(H), H.rows, rhs.data_ptr(), x.data_ptr(), fp32, prec_kind, None if jinv is None else jinv.data_ptr(),
+           mas_handle, float(tol), int(maxit), bool(zero_guess), stop_rule,
+           tuple(bs.values.data_ptr() for bs in H.block_sets),
+           tuple(0 if bs.values32 is None else bs.values32.data_ptr() for bs in H.block_sets))
+
+    def build():
+      args = L.PcgArgs()
+      args.matrix = H.matrix3()
+      args.precision = 1 if fp32 else 0
+      args.preconditioner = prec_kind
+      args.jacobi_inverse = L.ptr(jinv)
+      args.mas = mas_handle
+      args.stop_rule = _STOP[stop_rule]
+      args.tolerance = tol
+      args.max_iterations = maxit
+      args.rhs = L.ptr(rhs)
+      args.solution = L.ptr(x)
+      args.zero_initial_guess = 1 if zero_guess else 0
+      args.workspace = L.ptr(self._work)
+      h = ctypes.c_void_p()
+      L.call("ys_pcg_create", ctypes.byref(args), ctypes.byref(h))
+      return h, args
+
+    handle = self._cache.get(key, build)
+    res = L.PcgResult()
+    L.call("ys_pcg_run", handle, L.stream_ptr(), ctypes.byref(res))
+    self.last_result = res
+    return res
+
+
+class jacobianPCGSolver(_PcgBase):
+  """Block-Jacobi PCG (``PKG/solver/jacobianPCGSolver.pyx:84-166``)."""
+
+  def __init__(self, stop_rule="preconditioned"):
+    super().__init__(stop_rule)
+    self._jinv = None
+
+  def computeSolution(self, active_hessian, right_hand_side, initial_guess=None, tolerance=1e-3,
+                      maxIterations=20000, zero_initial_guess=False):
+    t0 = time.perf_counter()
+    rhs = _as_tensor(right_hand_side)
+    n = rhs.numel()
+    if n == 0:
+      self._statistics = {"solver": "jacobian", "converged": True, "iterations": 0}
+      return 0
+    self._buffers(n)
+    if active_hessian is None:
+      self._solution.zero_()
+      return 0
+    if n != active_hessian.rows:
+      raise ValueError("jacobianPCGSolver.computeSolution: right_hand_side size must match the Hessian size.")
+    torch = _torch()
+    H = active_hessian
+    if self._jinv is None or self._jinv.numel() != H.diagonal_blocks.numel():
+      self._jinv = torch.zeros_like(H.diagonal_blocks)
+    nat = len(H.wrt)
+    arr = lambda v: (L.u32 * len(v))(*v)
+    L.call("ys_invert_diagonal_blocks", L.ptr(H.diagonal_blocks), L.ptr(self._jinv), nat,
+           arr(H.diagonal_blocks_start_cpu[:nat]), arr([w.correspondance.numInstances for w in H.wrt]),
+           arr([w.size for w in H.wrt]), L.stream_ptr())
+    if not zero_initial_guess:
+      self._solution.copy_(_as_tensor(initial_guess))
+    res = self._run_pcg(H, rhs, self._solution, False, L.YS_PREC_BLOCK_JACOBI, self._jinv, None, tolerance,
+                        maxIterations, zero_initial_guess, self.stop_rule)
+    self._statistics = {"solver": "jacobian", "converged": res.status >= 0, "iterations": int(res.iterations),
+                        "result": int(res.status), "solve_seconds": time.perf_counter() - t0,
+                        "matrix_size": int(H.rows), "tolerance": float(tolerance)}
+    return int(res.status)
+
+
+class masSolver(_PcgBase):
+  """MAS-preconditioned CG (``PKG/solver/masSolver.py:13-126``, ``mas/solver.py``)."""
+
+  def __init__(self, max_domain_dofs=96, max_levels=6, target_nodes_per_partition=32, coarsest_level_weight=2.5,
+               level_weights=None, global_coarse_domain=True, mixed_spmv=False, stop_rule="preconditioned",
+               refinement_tolerance=1e-3, max_refinements=8, **unused):
+    super().__init__(stop_rule)
+    self.max_domain_dofs = int(max_domain_dofs)
+    self.max_levels = int(max_levels)
+    self.target_nodes = int(target_nodes_per_partition)
+    self.coarsest_level_weight = float(coarsest_level_weight)
+    self.level_weights = None if level_weights is None else tuple(float(w) for w in level_weights)
+    self.global_coarse_domain = bool(global_coarse_domain)
+    self.mixed_spmv = bool(mixed_spmv)
+    self.refinement_tolerance = float(refinement_tolerance)
+    self.max_refinements = int(max_refinements)
+    self.hierarchy = None
+    self._mas = None
+    self._mas_key = None
+    self._tables = None
+    self._dev_tables = None
+
+  def reset(self):
+    super().reset()
+    if self._mas is not None:
+      L.call("ys_mas_destroy", self._mas)
+    self._mas, self._mas_key, self.hierarchy, self._tables, self._dev_tables = None, None, None, None, None
+
+  def _ensure_hierarchy(self, H):
+    torch = _torch()
+    sets = H.block_sets
+    if len(sets) != 1:
+      raise NotImplementedError("the device MAS assembles one static 3x3 block set")
+    bs = sets[0]
+    key = (id(bs.pattern), H.rows)
+    if key == self._mas_key:
+      return
+    if self._mas is not None:
+      L.call("ys_mas_destroy", self._mas)
+      self._mas = None
+    pos = bs.pattern.positions[:2 * bs.pattern.num_unique].cpu().numpy().astype(np.int64).reshape(-1, 2)
+    nv = H.rows // 3
+    edges = pos[pos[:, 0] != pos[:, 1]] // 3
+    self.hierarchy = mas_hierarchy.build_hierarchy(np.full(nv, 3), edges, self.max_domain_dofs, self.max_levels,
+                                                   self.target_nodes, self.global_coarse_domain)
+    t = mas_hierarchy.build_tables(self.hierarchy, pos)
+    self._tables = t
+    nl = len(self.hierarchy.levels)
+    if self.level_weights is None:
+      weights = (1.0,) * (nl - 1) + (self.coarsest_level_weight,)
+    else:
+      if len(self.level_weights) < nl:
+        raise ValueError("level_weights needs one weight per level")
+      weights = self.level_weights[:nl - 1] + self.level_weights[-1:] if len(self.level_weights) > nl else \
+          self.level_weights
+    up = lambda a, dt=torch.int32: torch.from_numpy(np.ascontiguousarray(a).view(
+        np.int32 if dt == torch.int32 else np.int64)).to(_dev())
+    nb_coarse = int(t.cb_level_begin[-1])
+    packed = int(t.level_node_offset[-1])
+    dev = dict(cmap=up(t.cmap), child_ptr=up(t.child_ptr), child_fine=up(t.child_fine),
+               dom_node_ptr=up(t.dom_node_ptr), dom_nodes=up(t.dom_nodes),
+               inv_offset=up(t.inv_offset, torch.int64), dom_entry_ptr=up(t.dom_entry_ptr),
+               dom_entry=up(t.dom_entry), cb_src_ptr=up(t.cb_src_ptr), cb_src=up(t.cb_src),
+               coarse_values=torch.zeros(max(9 * nb_coarse, 1), dtype=torch.float64, device=_dev()),
+               inverse=torch.zeros(max(t.inverse_floats, 1), dtype=torch.float32, device=_dev()),
+               rl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
+               zl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
+               status=torch.zeros(1, dtype=torch.int32, device=_dev()))
+    lno = (L.u32 * (nl + 1))(*t.level_node_offset.tolist())
+    lw = (L.f64 * nl)(*weights)
+    cbl = (L.u32 * (nl + 1))(*t.cb_level_begin.tolist())
+    d = L.MasDesc()
+    d.num_fine_vars, d.num_levels = nv, nl
+    d.level_node_offset, d.level_weights = lno, lw
+    d.cmap, d.child_ptr, d.child_fine = L.ptr(dev["cmap"]), L.ptr(dev["child_ptr"]), L.ptr(dev["child_fine"])
+    d.num_domains = len(t.dom_node_ptr) - 1
+    d.dom_node_ptr, d.dom_nodes, d.inv_offset = L.ptr(dev["dom_node_ptr"]), L.ptr(dev["dom_nodes"]), L.ptr(
+        dev["inv_offset"])
+    d.dom_entry_ptr, d.dom_entry = L.ptr(dev["dom_entry_ptr"]), L.ptr(dev["dom_entry"])
+    d.fine_blocks, d.coarse_blocks = t.fine_blocks, nb_coarse
+    d.cb_src_ptr, d.cb_src, d.cb_level_begin = L.ptr(dev["cb_src_ptr"]), L.ptr(dev["cb_src"]), cbl
+    d.max_domain_dofs = t.max_domain_dofs
+    d.coarse_values, d.inverse = L.ptr(dev["coarse_values"]), L.ptr(dev["inverse"])
+    d.level_residual, d.level_correction, d.status = L.ptr(dev["rl"]), L.ptr(dev["zl"]), L.ptr(dev["status"])
+    h = ctypes.c_void_p()
+    L.call("ys_mas_create", ctypes.byref(d), ctypes.byref(h))
+    self._mas = h
+    self._dev_tables = (dev, lno, lw, cbl)
+    self._mas_key = key
+    self._cache.release()
+
+  def numeric_update(self, H, check=True):
+    failed = ctypes.c_int32(0)
+    L.call("ys_mas_numeric_update", self._mas, L.ptr(H.block_sets[0].values), L.stream_ptr(),
+           ctypes.byref(failed) if check else None)
+    return int(failed.value)
+
+  def computeSolution(self, active_hessian, right_hand_side, initial_guess=None, tolerance=1e-3,
+                      maxIterations=20000, zero_initial_guess=False, check_domains=True):
+    t0 = time.perf_counter()
+    rhs = _as_tensor(right_hand_side)
+    n = rhs.numel()
+    if n == 0:
+      return 0
+    self._buffers(n)
+    if active_hessian is None:
+      self._solution.zero_()
+      return 0
+    H = active_hessian
+    if n != H.rows:
+      raise ValueError("masSolver right-hand side size must match the matrix size")
+    if not zero_initial_guess and initial_guess is not None:
+      raise NotImplementedError("the device MAS PCG starts from a zero initial guess")
+    self._ensure_hierarchy(H)
+    failed = self.numeric_update(H, check_domains)
+    if failed:
+      raise np.linalg.LinAlgError(f"MAS: {failed} domain(s) are singular")
+    if not self.mixed_spmv:
+      res = self._run_pcg(H, rhs, self._solution, False, L.YS_PREC_MAS, None, self._mas, tolerance, maxIterations,
+                          True, self.stop_rule)
+      status = int(res.status)
+      its = int(res.iterations)
+      refinements = 0
+    else:
+      status, its, refinements = self._solve_mixed(H, rhs, tolerance, maxIterations)
+    self._statistics = {"solver": "mas", "converged": status >= 0, "iterations": its, "refinements": refinements,
+                        "result": 0 if status >= 0 else -4, "solve_seconds": time.perf_counter() - t0,
+                        "levels": len(self.hierarchy.levels), "domains_per_level": self.hierarchy.domains_per_level,
+                        "matrix_size": int(H.rows), "tolerance": float(tolerance)}
+    return 0 if status >= 0 else -4
+
+  def _solve_mixed(self, H, rhs, tolerance, max_iterations):
+    """FP32 inner PCG + FP64 iterative refinement (true FP64 residual test)."""
+    torch = _torch()
+    H.ensure_fp32()
+    n = H.rows
+    if getattr(self, "_mixed", None) is None or self._mixed[0].numel() != n:
+      ws = int(L.load().ys_refine_workspace_doubles(n // 3))
+      self._mixed = (torch.zeros(n, dtype=torch.float64, device=_dev()),
+                     torch.zeros(n, dtype=torch.float64, device=_dev()),
+                     torch.zeros(ws, dtype=torch.float64, device=_dev()))
+    r, delta, work = self._mixed
+    x = self._solution
+    m = H.matrix3()
+    norms = (L.f64 * 2)()
+    target = tolerance if self.stop_rule == "residual" else np.sqrt(tolerance)
+    total_its, refinements, status = 0, 0, -4
+    # x = 0, r = g (the refinement residual of the zero guess)
+    x.zero_()
+    L.call("ys_refine_residual", ctypes.byref(m), L.ptr(rhs), L.ptr(x), None, L.ptr(r), L.ptr(work), norms,
+           L.stream_ptr())
+    gnorm = float(np.sqrt(norms[1]))
+    rnorm = float(np.sqrt(norms[0]))
+    if rnorm <= target * gnorm:
+      return 0, 0, 0
+    for _ in range(self.max_refinements):
+      inner_tol = max(self.refinement_tolerance, 0.5 * target * gnorm / max(rnorm, 1e-300))
+      res = self._run_pcg(H, r, delta, True, L.YS_PREC_MAS, None, self._mas, min(inner_tol, 0.5),
+                          max(1, max_iterations - total_its), True, "residual")
+      total_its += int(res.iterations)
+      refinements += 1
+      L.call("ys_refine_residual", ctypes.byref(m), L.ptr(rhs), L.ptr(x), L.ptr(delta), L.ptr(r), L.ptr(work),
+             norms, L.stream_ptr())
+      rnorm = float(np.sqrt(norms[0]))
+      if rnorm <= target * gnorm:
+        status = total_its
+        break
+      if total_its >= max_iterations or res.status < -4:
+        break
+    self.final_relative_residual = rnorm / max(gnorm, 1e-300)
+    return status, total_its, refinements
+
+
+class solver:
+  """Solver dispatcher (``PKG/solver/solver.py:9-68``)."""
+
+  def __init__(self, solver="mas", **options):
+    self.solverName = ""
+    self.implementation = None
+    self.setSolver(solver, **options)
+
+  @property
+  def solution(self):
+    return self.implementation.solution
+
+  @property
+  def statistics(self):
+    return self.implementation.statistics
+
+  def setSolver(self, solver="mas", **options):
+    name = solver.strip().lower()
+    if name == "jacobian":
+      impl = jacobianPCGSolver(**options)
+    elif name == "mas":
+      impl = masSolver(**options)
+    else:
+      raise ValueError("solver must be either 'jacobian' or 'mas'")
+    if self.implementation is not None:
+      self.implementation.reset()
+    self.solverName = name
+    self.implementation = impl
+    return self
+
+  def reset(self):
+    self.implementation.reset()
+
+  def computeSolution(self, *args, **kwargs):
+    return self.implementation.computeSolution(*args, **kwargs)
