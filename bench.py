@@ -199,11 +199,12 @@ def gpu_arm(args):
   rel_res = float(getattr(impl, "final_relative_residual", float("nan")))
   value = world * args.steps / (ms / 1e3)
   lat_ms = sorted(1e3 * x for x in lat)
-  # kernels launched per step (ours): element eval 2 + inertia 1 + assemble 2 + diag 1 + MAS numeric (levels) +
-  # refine 2 per refinement + PCG init 4 + 6 per PCG iteration.
+  # kernels of this library launched per step: SNH eval + projection, inertia, block + gradient assembly,
+  # diagonal extraction (6); MAS numeric update (levels - 1 Galerkin sums + 1 inverse); refinement residual
+  # (1 + 2 per refinement); per PCG solve an init of (3 + levels) and (5 + levels) per iteration.
   levels = len(impl.hierarchy.levels)
   its, refs = int(stats["iterations"]), int(stats.get("refinements", 1))
-  launches_per_step = 6 + levels + 1 + 2 * (refs + 1) + refs * 4 + 6 * its
+  launches_per_step = 6 + levels + 1 + 2 * refs + refs * (3 + levels) + its * (5 + levels)
   # plain FP64 path on the same scene
   solver64 = mz.setSolver("mas", mixed_spmv=False, stop_rule="residual")
   for _ in range(2):

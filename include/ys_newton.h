@@ -283,8 +283,8 @@ typedef struct ys_mas_desc {
   const uint32_t* level_node_offset;   /* host [num_levels+1]                         */
   const double* level_weights;         /* host [num_levels] (mas/preconditioner.py:32-36) */
   const uint32_t* cmap;                /* [num_levels * num_fine_vars] packed node of each fine var */
-  const uint32_t* child_ptr;           /* [coarse nodes + 1] fine children of coarse nodes */
-  const uint32_t* child_fine;
+  const uint32_t* child_ptr;           /* [coarse nodes + 1] children of every coarse node:  */
+  const uint32_t* child_fine;          /* packed ids of its nodes on the level below          */
   uint32_t num_domains;
   const uint32_t* dom_node_ptr;        /* [num_domains+1]                             */
   const uint32_t* dom_nodes;           /* packed node ids, local order                 */
@@ -302,6 +302,7 @@ typedef struct ys_mas_desc {
   float* level_residual;               /* [3 * packed nodes] scratch                   */
   float* level_correction;             /* [3 * packed nodes] scratch                   */
   int32_t* status;                     /* [1] scratch                                  */
+  double* level_residual64;            /* [3 * packed nodes] scratch (FP64 restriction) */
 } ys_mas_desc;
 
 int32_t ys_mas_create(const ys_mas_desc* desc, void** handle);
@@ -341,6 +342,9 @@ int32_t ys_assemble_strided(const double* records, const uint32_t* begin, const 
 uint64_t ys_refine_workspace_doubles(uint32_t num_vars);
 int32_t ys_refine_residual(const ys_matrix3* m, const double* rhs, double* x, const double* delta, double* r,
                            double* workspace, double* norms_host, void* stream);
+/* Change the tolerance / iteration budget of an existing solver (the graph
+ * reads them from device memory, so no rebuild). */
+int32_t ys_pcg_set_params(void* handle, double tolerance, uint32_t max_iterations);
 /* Asynchronous halves of ys_pcg_run. */
 int32_t ys_pcg_launch(void* handle, void* stream);
 int32_t ys_pcg_status(void* handle, void* stream, ys_pcg_result* result);

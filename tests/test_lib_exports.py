@@ -34,6 +34,32 @@ def test_version_and_error_string_without_gpu():
   assert isinstance(lib.ys_last_error(), bytes)
 
 
+def _header_structs():
+  text = open(os.path.join(ROOT, "include", "ys_newton.h")).read()
+  text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+  out = {}
+  for body, name in re.findall(r"typedef struct \w+ \{(.*?)\} (\w+);", text, flags=re.S):
+    fields = []
+    for decl in body.split(";"):
+      decl = decl.strip()
+      if not decl:
+        continue
+      for part in decl.split(","):
+        m = re.search(r"(\w+)\s*(\[[^\]]*\])?\s*$", part.strip())
+        fields.append(m.group(1))
+    out[name] = fields
+  return out
+
+
+def test_ctypes_structs_follow_header_field_order():
+  structs = _header_structs()
+  pairs = {"ys_pattern_out": _lib.PatternOut, "ys_union3": _lib.Union3, "ys_term_plan": _lib.TermPlan,
+           "ys_snh_args": _lib.SnhArgs, "ys_inertia_args": _lib.InertiaArgs, "ys_matrix3": _lib.Matrix3,
+           "ys_pcg_args": _lib.PcgArgs, "ys_pcg_result": _lib.PcgResult, "ys_mas_desc": _lib.MasDesc}
+  for cname, cls in pairs.items():
+    assert structs[cname] == [f[0] for f in cls._fields_], cname
+
+
 def test_struct_layouts_match_header_sizes():
   # pointers 8 bytes, the union descriptor is 8 pointers + 9 u32 + u32 (+pad)
   assert ctypes.sizeof(_lib.Union3) == 8 * 8 + 10 * 4

@@ -79,7 +79,7 @@ class MasDesc(C.Structure):
               ("dom_nodes", vp), ("inv_offset", vp), ("dom_entry_ptr", vp), ("dom_entry", vp),
               ("fine_blocks", u32), ("coarse_blocks", u32), ("cb_src_ptr", vp), ("cb_src", vp),
               ("cb_level_begin", P(u32)), ("max_domain_dofs", u32), ("coarse_values", vp), ("inverse", vp),
-              ("level_residual", vp), ("level_correction", vp), ("status", vp)]
+              ("level_residual", vp), ("level_correction", vp), ("status", vp), ("level_residual64", vp)]
 
 
 # name: (restype, argtypes)
@@ -105,6 +105,7 @@ SIGNATURES = {
     "ys_pcg_create": (i32, [P(PcgArgs), P(vp)]),
     "ys_pcg_run": (i32, [vp, vp, P(PcgResult)]),
     "ys_pcg_launch": (i32, [vp, vp]),
+    "ys_pcg_set_params": (i32, [vp, f64, u32]),
     "ys_pcg_status": (i32, [vp, vp, P(PcgResult)]),
     "ys_pcg_destroy": (i32, [vp]),
     "ys_mas_create": (i32, [P(MasDesc), P(vp)]),

@@ -35,7 +35,7 @@ struct MasDev {
   uint32_t level_node_offset[kMaxLevels + 1];
   float weight[kMaxLevels];
   const uint32_t* cmap;     // [levels x nv] packed node index per fine node and level
-  const uint32_t* child_ptr;   // [packed_nodes - nv + 1] children of coarse nodes (levels >= 1)
+  const uint32_t* child_ptr;   // [packed_nodes - nv + 1] children (packed ids of level l-1) of coarse nodes
   const uint32_t* child_fine;
   // domains (all levels)
   uint32_t num_domains;
@@ -53,6 +53,7 @@ struct MasDev {
   double* coarse_values;          // [coarse_blocks * 9]
   float* inverse;                 // FP32 inverses
   float* rl;                      // packed level residuals [3 * packed_nodes]
+  double* rl64;                   // FP64 restriction chain (levels >= 1)
   float* zl;                      // packed level corrections
   int* status;                    // [1] failing domain count
   uint32_t max_dofs;
@@ -137,20 +138,27 @@ __global__ void __launch_bounds__(kInvThreads) mas_domain_inverse(MasDev M) {
   }
 }
 
-// Packed FP32 level residuals: level 0 copies r, coarse nodes sum children.
-__global__ void mas_restrict(MasDev M, const double* __restrict__ r) {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= M.packed_nodes) return;
+// Packed level residuals, one level per launch: level 0 is r itself (FP32
+// copy); a node of level l >= 1 sums its children of level l-1 (FP64, fixed
+// order; children of level 1 are read from r, deeper ones from rl64).
+__global__ void mas_restrict(MasDev M, const double* __restrict__ r, uint32_t level) {
+  const uint32_t begin = M.level_node_offset[level], end = M.level_node_offset[level + 1];
+  const uint32_t p = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= end) return;
   double s0, s1, s2;
-  if (p < M.nv) {
+  if (level == 0) {
     s0 = r[3ull * p]; s1 = r[3ull * p + 1]; s2 = r[3ull * p + 2];
   } else {
+    const double* src = level == 1 ? r : M.rl64;
     const uint32_t c = p - M.nv;
     s0 = s1 = s2 = 0.0;
     for (uint32_t q = M.child_ptr[c]; q < M.child_ptr[c + 1]; ++q) {
       const uint32_t f = M.child_fine[q];
-      s0 += r[3ull * f]; s1 += r[3ull * f + 1]; s2 += r[3ull * f + 2];
+      s0 += src[3ull * f]; s1 += src[3ull * f + 1]; s2 += src[3ull * f + 2];
     }
+    M.rl64[3ull * p] = s0;
+    M.rl64[3ull * p + 1] = s1;
+    M.rl64[3ull * p + 2] = s2;
   }
   M.rl[3ull * p] = (float)s0;
   M.rl[3ull * p + 1] = (float)s1;
@@ -262,18 +270,18 @@ __global__ void __launch_bounds__(kPcgBlock) mas_init_collect(MasPcg P) {
   int status = kContinue;
   double tol;
   if (P.stop_rule == YS_STOP_RESIDUAL) {
-    tol = P.tolerance * P.tolerance * v[2];
+    tol = P.st[kTolParam] * P.st[kTolParam] * v[2];
     if (!(isfinite(v[1]) && isfinite(v[2]))) status = kInvalidInit;
     else if (v[1] <= tol) status = kConverged;
     else if (!(isfinite(delta) && delta > 0.0)) status = kInvalidInit;
   } else {
     // mas/pcg.py:44-66: converged when r^T z <= tol * reference.
-    tol = P.tolerance * delta;
+    tol = P.st[kTolParam] * delta;
     if (!(isfinite(delta) && delta >= 0.0)) status = kInvalidInit;
     else if (delta <= tol) status = kConverged;
     else if (!(delta > 0.0)) status = kInvalidInit;
   }
-  if (status == kContinue && P.max_it == 0) status = kMaxIter;
+  if (status == kContinue && P.st[kMaxItParam] < 1.0) status = kMaxIter;
   st[kTolAbs] = tol;
   st[kStatus] = (double)status;
   cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(kPcgBlock) mas_iter_collect(MasPcg P) {
     const bool done = P.stop_rule == YS_STOP_RESIDUAL ? v[1] <= st[kTolAbs] : next <= st[kTolAbs];
     if (done) status = kConverged;
     else if (next == 0.0) status = kNonSpd;
-    else if (it >= (double)P.max_it) status = kMaxIter;
+    else if (it >= P.st[kMaxItParam]) status = kMaxIter;
   }
   st[kStatus] = (double)status;
   cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
@@ -359,14 +367,23 @@ static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGr
 // Restrict -> GEMV chain shared by init and iteration.
 static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
                                    cudaGraphNode_t* last, const double* r) {
-  cudaGraphNode_t n1 = nullptr, n2 = nullptr;
   MasDev m = M;
   const double* rr = r;
-  void* a1[] = {&m, &rr};
-  cudaError_t e = add_kernel(g, &n1, deps, ndeps, (const void*)mas_restrict, grid_for(M.packed_nodes, 256), 256, 0, a1);
+  cudaGraphNode_t prev = nullptr;
+  cudaError_t e = cudaSuccess;
+  for (uint32_t l = 0; l < M.levels && e == cudaSuccess; ++l) {
+    uint32_t level = l;
+    void* a1[] = {&m, &rr, &level};
+    const uint32_t cnt = M.level_node_offset[l + 1] - M.level_node_offset[l];
+    cudaGraphNode_t n = nullptr;
+    if (l == 0) e = add_kernel(g, &n, deps, ndeps, (const void*)mas_restrict, grid_for(cnt, 256), 256, 0, a1);
+    else e = add_kernel(g, &n, &prev, 1, (const void*)mas_restrict, grid_for(cnt, 256), 256, 0, a1);
+    prev = n;
+  }
   if (e != cudaSuccess) return e;
+  cudaGraphNode_t n2 = nullptr;
   void* a2[] = {&m};
-  e = add_kernel(g, &n2, &n1, 1, (const void*)mas_gemv, M.num_domains, 128, 0, a2);
+  e = add_kernel(g, &n2, &prev, 1, (const void*)mas_gemv, M.num_domains, 128, 0, a2);
   *last = n2;
   return e;
 }
@@ -457,6 +474,7 @@ int32_t ys_mas_create(const ys_mas_desc* d, void** handle) {
   M.coarse_values = d->coarse_values;
   M.inverse = d->inverse;
   M.rl = d->level_residual;
+  M.rl64 = d->level_residual64;
   M.zl = d->level_correction;
   M.status = d->status;
   M.max_dofs = d->max_domain_dofs;
@@ -508,8 +526,11 @@ int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
   auto* h = static_cast<ys::MasHandle*>(handle);
   cudaStream_t s = (cudaStream_t)stream;
   ys::MasDev& M = h->M;
-  ys::mas_restrict<<<ys::grid_for(M.packed_nodes, 256), 256, 0, s>>>(M, r);
-  YS_CHECK_LAUNCH();
+  for (uint32_t l = 0; l < M.levels; ++l) {
+    const uint32_t cnt = M.level_node_offset[l + 1] - M.level_node_offset[l];
+    ys::mas_restrict<<<ys::grid_for(cnt, 256), 256, 0, s>>>(M, r, l);
+    YS_CHECK_LAUNCH();
+  }
   ys::mas_gemv<<<M.num_domains, 128, 0, s>>>(M);
   YS_CHECK_LAUNCH();
   ys::MasPcg P{};

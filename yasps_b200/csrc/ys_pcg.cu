@@ -97,18 +97,18 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
   int status = kContinue;
   double tol;
   if (P.stop_rule == YS_STOP_RESIDUAL) {
-    tol = P.tolerance * P.tolerance * v[2];
+    tol = P.st[kTolParam] * P.st[kTolParam] * v[2];
     if (!(isfinite(v[1]) && isfinite(v[2]))) status = kInvalidInit;
     else if (v[1] <= tol) status = kConverged;
     else if (!(isfinite(delta_new) && delta_new > 0.0)) status = kInvalidInit;
   } else {
     // solverKernel.pyx:588-604
-    tol = P.tolerance * delta0;
+    tol = P.st[kTolParam] * delta0;
     if (!(isfinite(delta0) && delta0 >= 0.0 && isfinite(delta_new) && delta_new >= 0.0)) status = kInvalidInit;
     else if (!(isfinite(tol) && tol >= 0.0)) status = kInvalidInit;
     else if (delta_new <= tol) status = kConverged;
   }
-  if (status == kContinue && P.max_it == 0) status = kMaxIter;
+  if (status == kContinue && P.st[kMaxItParam] < 1.0) status = kMaxIter;
   st[kTolAbs] = tol;
   st[kStatus] = (double)status;
   cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_update_bj(PcgParams P) {
   } else {
     st[kBeta] = delta_new / delta_old;
     if (stop_reached(P, delta_new, v[1])) status = kConverged;
-    else if (it >= (double)P.max_it) status = kMaxIter;
+    else if (it >= P.st[kMaxItParam]) status = kMaxIter;
   }
   st[kStatus] = (double)status;
   cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
@@ -241,6 +241,7 @@ struct PcgHandle {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double* slots_host = nullptr;
+  double params[2] = {0.0, 0.0};  // tolerance, iteration budget (copied to the device per launch)
 };
 
 static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
@@ -300,6 +301,8 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   P.zero_guess = a.zero_initial_guess;
   P.tolerance = a.tolerance;
   P.max_it = a.max_iterations;
+  h->params[0] = a.tolerance;
+  h->params[1] = (double)a.max_iterations;
   h->preconditioner = a.preconditioner;
 
   cudaError_t e = cudaGraphCreate(&h->graph, 0);
@@ -365,7 +368,20 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
 int32_t ys_pcg_launch(void* handle, void* stream) {
   YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
   auto* h = static_cast<ys::PcgHandle*>(handle);
+  // Pageable source: the copy is staged before the call returns, so the
+  // parameters may change for the next launch right away.
+  const double params[2] = {h->params[0], h->params[1]};
+  YS_CUDA_TRY(cudaMemcpyAsync(h->P.st + ys::kTolParam, params, sizeof(params), cudaMemcpyHostToDevice,
+                              (cudaStream_t)stream));
   YS_CUDA_TRY(cudaGraphLaunch(h->exec, (cudaStream_t)stream));
+  return YS_OK;
+}
+
+int32_t ys_pcg_set_params(void* handle, double tolerance, uint32_t max_iterations) {
+  YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
+  auto* h = static_cast<ys::PcgHandle*>(handle);
+  h->params[0] = tolerance;
+  h->params[1] = (double)max_iterations;
   return YS_OK;
 }
 

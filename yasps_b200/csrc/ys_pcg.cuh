@@ -20,7 +20,8 @@ enum PcgSlot : int {
   kRR0 = 9,
   kGG = 10,        // rhs^T rhs
   kTolAbs = 11,    // threshold in the units of the stop rule
-  kMaxIt = 12,
+  kTolParam = 13,  // solve parameters, written by the host before each launch
+  kMaxItParam = 14,
   kSlots = 16
 };
 

@@ -175,6 +175,15 @@ class MasTables:
   inverse_floats: int
 
 
+def _step_map(h: Hierarchy, l: int, counts, nv) -> np.ndarray:
+  """Map of level l-1 node ids to level l node ids (composed[l] = step o composed[l-1])."""
+  if l == 1:
+    return h.composed[1]
+  rep = np.zeros(counts[l - 1], dtype=np.int64)
+  rep[h.composed[l - 1]] = np.arange(nv)
+  return h.composed[l][rep]
+
+
 def build_tables(h: Hierarchy, fine_positions: np.ndarray) -> MasTables:
   """Device tables for 3-DoF variables and one 3x3 upper block set.
 
@@ -188,12 +197,14 @@ def build_tables(h: Hierarchy, fine_positions: np.ndarray) -> MasTables:
   counts = [l.dims.size for l in h.levels]
   offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
   cmap = np.stack([offs[l] + h.composed[l] for l in range(L)]).astype(np.uint32)
-  # children of coarse packed nodes (levels >= 1), fine ids ascending
+  # children of coarse packed nodes: the packed ids of their nodes one level
+  # below, ascending (the restriction runs level by level)
   child_ptr, child_fine, base = [0], [], 0
   for l in range(1, L):
-    order = np.argsort(h.composed[l], kind="stable")
-    cnt = np.bincount(h.composed[l], minlength=counts[l])
-    child_fine.append(order)
+    step = _step_map(h, l, counts, nv)
+    order = np.argsort(step, kind="stable")
+    cnt = np.bincount(step, minlength=counts[l])
+    child_fine.append(offs[l - 1] + order)
     child_ptr.extend((base + np.cumsum(cnt)).tolist())
     base += int(cnt.sum())
   child_ptr = np.asarray(child_ptr, dtype=np.uint32)
@@ -225,15 +236,7 @@ def build_tables(h: Hierarchy, fine_positions: np.ndarray) -> MasTables:
   next_index = nb0
   for l in range(1, L):
     prev = level_pairs[-1]
-    m = h.composed[l] if l == 1 else None
-    # map level l-1 node ids to level l ids
-    if l == 1:
-      to_l = h.composed[1]
-    else:
-      # composed[l] = step o composed[l-1]; recover the step map from one fine rep per node
-      rep = np.zeros(counts[l - 1], dtype=np.int64)
-      rep[h.composed[l - 1]] = np.arange(nv)
-      to_l = h.composed[l][rep]
+    to_l = _step_map(h, l, counts, nv)
     A, B = to_l[prev[:, 0]], to_l[prev[:, 1]]
     lo, hi = np.minimum(A, B), np.maximum(A, B)
     mode = np.where(A < B, 0, np.where(A > B, 1, np.where(prev[:, 0] == prev[:, 1], 0, 2)))

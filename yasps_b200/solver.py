@@ -91,7 +91,7 @@ class _PcgBase:
   def _run_pcg(self, H, rhs, x, fp32, prec_kind, jinv, mas_handle, tol, maxit, zero_guess, stop_rule):
     """One device PCG solve into ``x``; returns the ys_pcg_result."""
     key = (id(H), H.rows, rhs.data_ptr(), x.data_ptr(), fp32, prec_kind, None if jinv is None else jinv.data_ptr(),
-           mas_handle, float(tol), int(maxit), bool(zero_guess), stop_rule,
+           mas_handle, bool(zero_guess), stop_rule,
            tuple(bs.values.data_ptr() for bs in H.block_sets),
            tuple(0 if bs.values32 is None else bs.values32.data_ptr() for bs in H.block_sets))
 
@@ -114,6 +114,7 @@ class _PcgBase:
       return h, args
 
     handle = self._cache.get(key, build)
+    L.call("ys_pcg_set_params", handle, float(tol), int(maxit))
     res = L.PcgResult()
     L.call("ys_pcg_run", handle, L.stream_ptr(), ctypes.byref(res))
     self.last_result = res
@@ -227,6 +228,7 @@ class masSolver(_PcgBase):
                inverse=torch.zeros(max(t.inverse_floats, 1), dtype=torch.float32, device=_dev()),
                rl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
                zl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
+               rl64=torch.zeros(3 * packed, dtype=torch.float64, device=_dev()),
                status=torch.zeros(1, dtype=torch.int32, device=_dev()))
     lno = (L.u32 * (nl + 1))(*t.level_node_offset.tolist())
     lw = (L.f64 * nl)(*weights)
@@ -244,6 +246,7 @@ class masSolver(_PcgBase):
     d.max_domain_dofs = t.max_domain_dofs
     d.coarse_values, d.inverse = L.ptr(dev["coarse_values"]), L.ptr(dev["inverse"])
     d.level_residual, d.level_correction, d.status = L.ptr(dev["rl"]), L.ptr(dev["zl"]), L.ptr(dev["status"])
+    d.level_residual64 = L.ptr(dev["rl64"])
     h = ctypes.c_void_p()
     L.call("ys_mas_create", ctypes.byref(d), ctypes.byref(h))
     self._mas = h
