@@ -117,4 +117,92 @@ __device__ void jacobi_reconstruct(double (&a)[N][N], const double (&v)[N][N], i
   }
 }
 
+// Upper-triangle packed index for an N x N symmetric matrix (row <= col).
+template <int N>
+__host__ __device__ constexpr int utri(int r, int c) {
+  return r <= c ? r * N - r * (r - 1) / 2 + (c - r) : c * N - c * (c - 1) / 2 + (r - c);
+}
+
+// Cyclic Jacobi with the matrix in registers (packed upper triangle `a`,
+// fully unrolled so every index is a compile-time constant) and the
+// eigenvectors in shared memory, thread-interleaved: v[(i*N + j) * stride].
+// After return, a holds the eigenvalues on its diagonal.
+template <int N>
+__device__ __forceinline__ void jacobi_eigen_reg(double (&a)[N * (N + 1) / 2], double* __restrict__ v, int stride) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) v[(i * N + j) * stride] = i == j ? 1.0 : 0.0;
+  double total = 0.0;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = i; j < N; ++j) total += (i == j ? 1.0 : 2.0) * a[utri<N>(i, j)] * a[utri<N>(i, j)];
+  if (total == 0.0) return;
+  for (int sweep = 0; sweep < 24; ++sweep) {
+    double off = 0.0;
+#pragma unroll
+    for (int p = 0; p < N; ++p)
+#pragma unroll
+      for (int q = p + 1; q < N; ++q) off += a[utri<N>(p, q)] * a[utri<N>(p, q)];
+    if (off <= 0.5e-34 * total) break;
+#pragma unroll
+    for (int p = 0; p < N - 1; ++p) {
+#pragma unroll
+      for (int q = p + 1; q < N; ++q) {
+        const double apq = a[utri<N>(p, q)];
+        if (apq != 0.0) {
+          const double app = a[utri<N>(p, p)], aqq = a[utri<N>(q, q)];
+          const double tau = (aqq - app) / (2.0 * apq);
+          const double t = fabs(tau) > 1.0e150 ? 0.5 / tau
+                                                : (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          const double c = rsqrt(1.0 + t * t);
+          const double s = t * c;
+          a[utri<N>(p, p)] = app - t * apq;
+          a[utri<N>(q, q)] = aqq + t * apq;
+          a[utri<N>(p, q)] = 0.0;
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            if (k == p || k == q) continue;
+            const double akp = a[utri<N>(k, p)], akq = a[utri<N>(k, q)];
+            a[utri<N>(k, p)] = c * akp - s * akq;
+            a[utri<N>(k, q)] = s * akp + c * akq;
+          }
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            const double vkp = v[(k * N + p) * stride], vkq = v[(k * N + q) * stride];
+            v[(k * N + p) * stride] = c * vkp - s * vkq;
+            v[(k * N + q) * stride] = s * vkp + c * vkq;
+          }
+        }
+      }
+    }
+  }
+}
+
+// a <- V diag(f(lambda)) V^T in place (packed upper), V in shared memory.
+template <int N>
+__device__ __forceinline__ void jacobi_reconstruct_reg(double (&a)[N * (N + 1) / 2], const double* __restrict__ v,
+                                                       int stride, int method) {
+  double w[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const double l = a[utri<N>(i, i)];
+    w[i] = l < 0.0 ? (method == 1 ? -l : 0.0) : l;
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    double vi[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) vi[k] = v[(i * N + k) * stride] * w[k];
+#pragma unroll
+    for (int j = i; j < N; ++j) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < N; ++k) acc += vi[k] * v[(j * N + k) * stride];
+      a[utri<N>(i, j)] = acc;
+    }
+  }
+}
+
 }  // namespace ys

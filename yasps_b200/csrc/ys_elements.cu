@@ -295,7 +295,8 @@ __device__ __forceinline__ bool chol3(double w00, double w01, double w02, double
   return true;
 }
 
-__device__ __noinline__ void snh_project_one(const ys_snh_args& a, uint32_t t) {
+__device__ __forceinline__ void snh_project_one(const ys_snh_args& a, uint32_t t, double* __restrict__ vsh,
+                                                int vstride) {
   SnhState st;
   snh_state(a, t, st);
   uint32_t code[4];
@@ -331,21 +332,22 @@ __device__ __noinline__ void snh_project_one(const ys_snh_args& a, uint32_t t) {
     lu[p] = mul(st.f, lc[p]);
     lv[p] = mul(st.cof, lc[p]);
   }
-  double kmat[9][9];
+  // K (9x9, packed upper triangle in registers), eigenvectors in shared memory.
+  double kmat[45];
 #pragma unroll
   for (int p = 0; p < 3; ++p)
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
+    for (int q = p; q < 3; ++q) {
       double blk[3][3];
       hess_block(st, lc[p], lc[q], lu[p], lu[q], lv[p], lv[q], blk);
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int m = 0; m < 3; ++m) kmat[3 * p + k][3 * q + m] = blk[k][m];
+        for (int m = 0; m < 3; ++m)
+          if (3 * p + k <= 3 * q + m) kmat[utri<9>(3 * p + k, 3 * q + m)] = blk[k][m];
     }
-  double vec[9][9];
-  jacobi_eigen<9>(kmat, vec);
-  jacobi_reconstruct<9>(kmat, vec, a.projection_method);
+  jacobi_eigen_reg<9>(kmat, vsh, vstride);
+  jacobi_reconstruct_reg<9>(kmat, vsh, vstride, a.projection_method);
   // Q = G L^-T: Q[a][p] = sum_j G[a][j] (L^-1)[p][j]; solve L y = G_a per vertex.
   double qm[4][3];
 #pragma unroll
@@ -357,21 +359,29 @@ __device__ __noinline__ void snh_project_one(const ys_snh_args& a, uint32_t t) {
     qm[k][0] = y0; qm[k][1] = y1; qm[k][2] = y2;
   }
   auto block = [&](int ai, int bi, double (&blk)[3][3]) {
+#pragma unroll
     for (int k = 0; k < 3; ++k)
+#pragma unroll
       for (int m = 0; m < 3; ++m) {
         double acc = 0.0;
+#pragma unroll
         for (int p = 0; p < 3; ++p)
-          for (int q = 0; q < 3; ++q) acc += qm[ai][p] * qm[bi][q] * kmat[3 * p + k][3 * q + m];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) acc += qm[ai][p] * qm[bi][q] * kmat[utri<9>(3 * p + k, 3 * q + m)];
         blk[k][m] = acc;
       }
   };
   write_hessian_records(code, a.plan.coord_outer[t], a.plan.record, a.block_records, block);
 }
 
-__global__ void __launch_bounds__(128) snh_project_kernel(const ys_snh_args a) {
+constexpr int kProjThreads = 64;
+
+__global__ void __launch_bounds__(kProjThreads) snh_project_kernel(const ys_snh_args a) {
+  extern __shared__ double vshared[];  // 81 doubles per thread, thread-interleaved
+  double* vsh = vshared + threadIdx.x;
   const uint32_t count = *a.work_count;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-    snh_project_one(a, a.work_list[i]);
+    snh_project_one(a, a.work_list[i], vsh, blockDim.x);
 }
 
 __global__ void inertia_kernel(const ys_inertia_args a) {
@@ -422,8 +432,9 @@ int32_t ys_snh_eval(const ys_snh_args* args, void* stream) {
   if (a.projection_method >= 1) {
     // The work count stays on the device: a grid-stride launch sized to the
     // SMs covers any count without a host round trip.
-    const unsigned pgrid = std::min<unsigned>(grid, ys::kSMs * 16);
-    ys::snh_project_kernel<<<pgrid, 128, 0, s>>>(a);
+    const unsigned pgrid = std::min<unsigned>(ys::grid_for(a.num_elements, ys::kProjThreads), ys::kSMs * 16);
+    const size_t smem = sizeof(double) * 81 * ys::kProjThreads;
+    ys::snh_project_kernel<<<pgrid, ys::kProjThreads, smem, s>>>(a);
     YS_CHECK_LAUNCH();
   }
   return YS_OK;

@@ -84,7 +84,9 @@ __global__ void mas_level_blocks(MasDev M, uint32_t begin, uint32_t end) {
 }
 
 // Dense assembly + in-place Gauss-Jordan inverse of one domain per CTA.
-__global__ void __launch_bounds__(kInvThreads) mas_domain_inverse(MasDev M) {
+// T: register tile edge (domain size <= 16 T).
+template <int T>
+__global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_inverse(MasDev M) {
   extern __shared__ double A[];  // n*n
   __shared__ double colk[128];
   __shared__ double rowk[128];
@@ -107,29 +109,73 @@ __global__ void __launch_bounds__(kInvThreads) mas_domain_inverse(MasDev M) {
   // Gauss-Jordan without pivoting (SPD domains): after step k, A holds the
   // inverse in the eliminated columns.  Relative pivot tolerance 1e-12 of
   // the largest diagonal entry (mas/local_inverse.py:43-65).
+  // Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns tx + 16b
+  // (a, b < 8) in registers; each step only broadcasts the pivot row and
+  // column through shared memory.
   double scale = 0.0;
   for (uint32_t i = 0; i < n; ++i) scale = fmax(scale, fabs(A[i * n + i]));
   const double tol = 1.0e-12 * fmax(scale, 1.0e-300);
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+  double R[T][T];
+#pragma unroll
+  for (int a = 0; a < T; ++a)
+#pragma unroll
+    for (int b = 0; b < T; ++b) {
+      const uint32_t i = ty + 16 * a, j = tx + 16 * b;
+      R[a][b] = (i < n && j < n) ? A[i * n + j] : 0.0;
+    }
   for (uint32_t k = 0; k < n; ++k) {
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-      colk[i] = A[i * n + k];
-      rowk[i] = A[k * n + i];
+    const int kb = (int)(k >> 4), kr = (int)(k & 15);
+    if (tx == kr) {
+#pragma unroll
+      for (int a = 0; a < T; ++a) {
+        double v = 0.0;
+#pragma unroll
+        for (int b = 0; b < T; ++b) v = (b == kb) ? R[a][b] : v;
+        colk[ty + 16 * a] = v;
+      }
+    }
+    if (ty == kr) {
+#pragma unroll
+      for (int b = 0; b < T; ++b) {
+        double v = 0.0;
+#pragma unroll
+        for (int a = 0; a < T; ++a) v = (a == kb) ? R[a][b] : v;
+        rowk[tx + 16 * b] = v;
+      }
     }
     __syncthreads();
     const double piv = rowk[k];
     if (!(piv > tol) && threadIdx.x == 0) bad = 1;
     const double ip = 1.0 / piv;
+    double ci[T], rj[T];
+#pragma unroll
+    for (int a = 0; a < T; ++a) ci[a] = colk[ty + 16 * a];
+#pragma unroll
+    for (int b = 0; b < T; ++b) rj[b] = rowk[tx + 16 * b];
     // Row k scaled, column k set to -a_ik / piv, the rest updated.
-    for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) {
-      const uint32_t i = t / n, j = t - (t / n) * n;
-      double v;
-      if (i == k) v = (j == k) ? ip : rowk[j] * ip;
-      else if (j == k) v = -colk[i] * ip;
-      else v = A[t] - colk[i] * rowk[j] * ip;
-      A[t] = v;
+#pragma unroll
+    for (int a = 0; a < T; ++a) {
+      const bool on_row = (ty + 16 * a) == (int)k;
+      const double cip = ci[a] * ip;
+#pragma unroll
+      for (int b = 0; b < T; ++b) {
+        const bool on_col = (tx + 16 * b) == (int)k;
+        const double upd = R[a][b] - cip * rj[b];
+        const double v = on_row ? (on_col ? ip : rj[b] * ip) : (on_col ? -cip : upd);
+        R[a][b] = v;
+      }
     }
     __syncthreads();
   }
+#pragma unroll
+  for (int a = 0; a < T; ++a)
+#pragma unroll
+    for (int b = 0; b < T; ++b) {
+      const uint32_t i = ty + 16 * a, j = tx + 16 * b;
+      if (i < n && j < n) A[i * n + j] = R[a][b];
+    }
+  __syncthreads();
   if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
   float* out = M.inverse + M.inv_offset[d];
   for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) {
@@ -179,15 +225,17 @@ __global__ void __launch_bounds__(128) mas_gemv(MasDev M) {
   __syncthreads();
   const float* inv = M.inverse + M.inv_offset[d];
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    float acc0 = 0.f, acc1 = 0.f;
+    // 8 independent partial sums keep 8 column loads in flight per thread.
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t j = 0;
-    for (; j + 1 < n; j += 2) {
-      acc0 += __ldg(inv + (uint64_t)j * n + i) * rloc[j];
-      acc1 += __ldg(inv + (uint64_t)(j + 1) * n + i) * rloc[j + 1];
+    for (; j + 8 <= n; j += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] += __ldg(inv + (uint64_t)(j + u) * n + i) * rloc[j + u];
     }
-    if (j < n) acc0 += __ldg(inv + (uint64_t)j * n + i) * rloc[j];
+    for (; j < n; ++j) acc[0] += __ldg(inv + (uint64_t)j * n + i) * rloc[j];
+    const float s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
     const uint32_t node = M.dom_nodes[nb + i / 3];
-    M.zl[3ull * node + i % 3] = acc0 + acc1;
+    M.zl[3ull * node + i % 3] = s;
   }
 }
 
@@ -482,7 +530,9 @@ int32_t ys_mas_create(const ys_mas_desc* d, void** handle) {
   cudaError_t e = cudaMallocHost(&h->status_host, sizeof(int));
   if (e == cudaSuccess) {
     const size_t smem = sizeof(double) * d->max_domain_dofs * d->max_domain_dofs;
-    e = cudaFuncSetAttribute(ys::mas_domain_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(ys::mas_domain_inverse<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ys::mas_domain_inverse<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
   if (e != cudaSuccess) {
     ys_set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
@@ -510,7 +560,10 @@ int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* str
     }
   }
   const size_t smem = sizeof(double) * M.max_dofs * M.max_dofs;
-  ys::mas_domain_inverse<<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
+  if (M.max_dofs <= 96)
+    ys::mas_domain_inverse<6><<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
+  else
+    ys::mas_domain_inverse<8><<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
   YS_CHECK_LAUNCH();
   if (failed_domains) {
     YS_CUDA_TRY(cudaMemcpyAsync(h->status_host, M.status, sizeof(int), cudaMemcpyDeviceToHost, s));
