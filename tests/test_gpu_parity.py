@@ -129,7 +129,7 @@ def test_jacobi_status_codes(c0):
 def test_mas_pcg_matches_oracle(c0):
   from oracle import mas as omas
   cube, ora = c0
-  sc, _ = build(cube, "mas")
+  sc, _ = build(cube, "mas", fine_level_weight=1.0)  # the CPU reference's level weights
   H = sc.minimizer.computeNumericValue()
   p = ora.pattern
   edges = [(r // 3, c // 3) for r, c in p.positions if r != c]
@@ -160,7 +160,7 @@ def test_mas_apply_matches_oracle(c0):
   from oracle import mas as omas
   from yasps_b200 import _lib as L
   cube, ora = c0
-  sc, _ = build(cube, "mas")
+  sc, _ = build(cube, "mas", fine_level_weight=1.0)  # the CPU reference's level weights
   H = sc.minimizer.computeNumericValue()
   ms = sc.minimizer.linearSolver.implementation
   ms._ensure_hierarchy(H)

@@ -90,6 +90,8 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
   extern __shared__ double A[];  // n*n
   __shared__ double colk[128];
   __shared__ double rowk[128];
+  __shared__ double dinv[128];
+  __shared__ double piv_sh[1];
   __shared__ int bad;
   const uint32_t d = blockIdx.x;
   const uint32_t n = 3 * (M.dom_node_ptr[d + 1] - M.dom_node_ptr[d]);
@@ -112,9 +114,20 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
   // Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns tx + 16b
   // (a, b < 8) in registers; each step only broadcasts the pivot row and
   // column through shared memory.
-  double scale = 0.0;
-  for (uint32_t i = 0; i < n; ++i) scale = fmax(scale, fabs(A[i * n + i]));
-  const double tol = 1.0e-12 * fmax(scale, 1.0e-300);
+  // The matrix is first scaled to unit diagonal, S = D^-1/2 A D^-1/2 (pivots
+  // of S lie in (0, 1]); the inverse is D^-1/2 S^-1 D^-1/2.  A pivot of S
+  // below 1e-12 (or a non-positive diagonal) marks the domain singular.
+  // GJ step k as one uniform update S_ij -= c_i r_j / s_kk with c = column k
+  // except c_k = s_kk - 1 and r = row k except r_k = s_kk + 1: this yields
+  // the scaled row k, the column -s_ik / s_kk and the pivot 1 / s_kk exactly,
+  // so the update is pure FMAs (no per-element selects).
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double dii = A[i * n + i];
+    if (!(dii > 0.0)) bad = 1;
+    dinv[i] = dii > 0.0 ? rsqrt(dii) : 1.0;
+  }
+  __syncthreads();
+  const double tol = 1.0e-12;
   const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
   double R[T][T];
 #pragma unroll
@@ -122,7 +135,7 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
 #pragma unroll
     for (int b = 0; b < T; ++b) {
       const uint32_t i = ty + 16 * a, j = tx + 16 * b;
-      R[a][b] = (i < n && j < n) ? A[i * n + j] : 0.0;
+      R[a][b] = (i < n && j < n) ? A[i * n + j] * dinv[i] * dinv[j] : 0.0;
     }
   for (uint32_t k = 0; k < n; ++k) {
     const int kb = (int)(k >> 4), kr = (int)(k & 15);
@@ -132,7 +145,9 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
         double v = 0.0;
 #pragma unroll
         for (int b = 0; b < T; ++b) v = (b == kb) ? R[a][b] : v;
-        colk[ty + 16 * a] = v;
+        const bool diag = (ty + 16 * a) == (int)k;
+        if (diag) piv_sh[0] = v;
+        colk[ty + 16 * a] = diag ? v - 1.0 : v;
       }
     }
     if (ty == kr) {
@@ -141,30 +156,21 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
         double v = 0.0;
 #pragma unroll
         for (int a = 0; a < T; ++a) v = (a == kb) ? R[a][b] : v;
-        rowk[tx + 16 * b] = v;
+        rowk[tx + 16 * b] = ((tx + 16 * b) == (int)k) ? v + 1.0 : v;
       }
     }
     __syncthreads();
-    const double piv = rowk[k];
+    const double piv = piv_sh[0];
     if (!(piv > tol) && threadIdx.x == 0) bad = 1;
     const double ip = 1.0 / piv;
-    double ci[T], rj[T];
-#pragma unroll
-    for (int a = 0; a < T; ++a) ci[a] = colk[ty + 16 * a];
+    double rj[T];
 #pragma unroll
     for (int b = 0; b < T; ++b) rj[b] = rowk[tx + 16 * b];
-    // Row k scaled, column k set to -a_ik / piv, the rest updated.
 #pragma unroll
     for (int a = 0; a < T; ++a) {
-      const bool on_row = (ty + 16 * a) == (int)k;
-      const double cip = ci[a] * ip;
+      const double cip = colk[ty + 16 * a] * ip;
 #pragma unroll
-      for (int b = 0; b < T; ++b) {
-        const bool on_col = (tx + 16 * b) == (int)k;
-        const double upd = R[a][b] - cip * rj[b];
-        const double v = on_row ? (on_col ? ip : rj[b] * ip) : (on_col ? -cip : upd);
-        R[a][b] = v;
-      }
+      for (int b = 0; b < T; ++b) R[a][b] = fma(-cip, rj[b], R[a][b]);
     }
     __syncthreads();
   }
@@ -173,7 +179,7 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
 #pragma unroll
     for (int b = 0; b < T; ++b) {
       const uint32_t i = ty + 16 * a, j = tx + 16 * b;
-      if (i < n && j < n) A[i * n + j] = R[a][b];
+      if (i < n && j < n) A[i * n + j] = R[a][b] * dinv[i] * dinv[j];
     }
   __syncthreads();
   if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
@@ -209,6 +215,40 @@ __global__ void mas_restrict(MasDev M, const double* __restrict__ r, uint32_t le
   M.rl[3ull * p] = (float)s0;
   M.rl[3ull * p + 1] = (float)s1;
   M.rl[3ull * p + 2] = (float)s2;
+}
+
+// All levels from `first` to the coarsest in one CTA (small levels: the
+// launch would cost more than the work), level by level.
+__global__ void __launch_bounds__(1024) mas_restrict_tail(MasDev M, const double* __restrict__ r, uint32_t first) {
+  for (uint32_t level = first; level < M.levels; ++level) {
+    const uint32_t begin = M.level_node_offset[level], end = M.level_node_offset[level + 1];
+    const double* src = level == 1 ? r : M.rl64;
+    for (uint32_t p = begin + threadIdx.x; p < end; p += blockDim.x) {
+      const uint32_t c = p - M.nv;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      for (uint32_t q = M.child_ptr[c]; q < M.child_ptr[c + 1]; ++q) {
+        const uint32_t f = M.child_fine[q];
+        s0 += src[3ull * f]; s1 += src[3ull * f + 1]; s2 += src[3ull * f + 2];
+      }
+      M.rl64[3ull * p] = s0;
+      M.rl64[3ull * p + 1] = s1;
+      M.rl64[3ull * p + 2] = s2;
+      M.rl[3ull * p] = (float)s0;
+      M.rl[3ull * p + 1] = (float)s1;
+      M.rl[3ull * p + 2] = (float)s2;
+    }
+    __syncthreads();
+  }
+}
+
+// First level handled by mas_restrict_tail: every level from there on has at
+// most kTailNodes nodes.
+constexpr uint32_t kTailNodes = 4096;
+
+__host__ __device__ inline uint32_t restrict_tail_first(const MasDev& M) {
+  uint32_t first = M.levels;
+  while (first > 1 && M.level_node_offset[first] - M.level_node_offset[first - 1] <= kTailNodes) --first;
+  return first;
 }
 
 // z_d = A_d^-1 r_d, one CTA per domain; thread i owns output row i and reads
@@ -273,6 +313,7 @@ __global__ void __launch_bounds__(kPcgBlock) mas_init_residual(MasPcg P) {
     r0 -= h0; r1 -= h1; r2 -= h2;
   }
   P.r[3ull * i] = r0; P.r[3ull * i + 1] = r1; P.r[3ull * i + 2] = r2;
+  P.M.rl[3ull * i] = (float)r0; P.M.rl[3ull * i + 1] = (float)r1; P.M.rl[3ull * i + 2] = (float)r2;
 }
 
 __device__ __forceinline__ void collect_node(const MasPcg& P, uint32_t i, double (&z)[3]) {
@@ -342,7 +383,9 @@ __global__ void __launch_bounds__(kPcgBlock) mas_update(MasPcg P) {
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     P.x[3ull * i + k] = P.x[3ull * i + k] + P.p[3ull * i + k] * alpha;
-    P.r[3ull * i + k] = P.r[3ull * i + k] - P.q[3ull * i + k] * alpha;
+    const double r = P.r[3ull * i + k] - P.q[3ull * i + k] * alpha;
+    P.r[3ull * i + k] = r;
+    P.M.rl[3ull * i + k] = (float)r;  // level-0 restriction fused
   }
 }
 
@@ -415,23 +458,37 @@ static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGr
 // Restrict -> GEMV chain shared by init and iteration.
 static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
                                    cudaGraphNode_t* last, const double* r) {
+  // Level 0 (the FP32 copy of r) is written by the kernel that produces r.
   MasDev m = M;
   const double* rr = r;
+  const uint32_t first = restrict_tail_first(M);
+  const cudaGraphNode_t* dp = deps;
+  size_t nd = ndeps;
   cudaGraphNode_t prev = nullptr;
   cudaError_t e = cudaSuccess;
-  for (uint32_t l = 0; l < M.levels && e == cudaSuccess; ++l) {
+  for (uint32_t l = 1; l < first && e == cudaSuccess; ++l) {
     uint32_t level = l;
     void* a1[] = {&m, &rr, &level};
     const uint32_t cnt = M.level_node_offset[l + 1] - M.level_node_offset[l];
     cudaGraphNode_t n = nullptr;
-    if (l == 0) e = add_kernel(g, &n, deps, ndeps, (const void*)mas_restrict, grid_for(cnt, 256), 256, 0, a1);
-    else e = add_kernel(g, &n, &prev, 1, (const void*)mas_restrict, grid_for(cnt, 256), 256, 0, a1);
+    e = add_kernel(g, &n, dp, nd, (const void*)mas_restrict, grid_for(cnt, 256), 256, 0, a1);
     prev = n;
+    dp = &prev;
+    nd = 1;
+  }
+  if (e == cudaSuccess && first < M.levels) {
+    uint32_t f = first;
+    void* a1[] = {&m, &rr, &f};
+    cudaGraphNode_t n = nullptr;
+    e = add_kernel(g, &n, dp, nd, (const void*)mas_restrict_tail, 1, 1024, 0, a1);
+    prev = n;
+    dp = &prev;
+    nd = 1;
   }
   if (e != cudaSuccess) return e;
   cudaGraphNode_t n2 = nullptr;
   void* a2[] = {&m};
-  e = add_kernel(g, &n2, &prev, 1, (const void*)mas_gemv, M.num_domains, 128, 0, a2);
+  e = add_kernel(g, &n2, dp, nd, (const void*)mas_gemv, M.num_domains, 128, 0, a2);
   *last = n2;
   return e;
 }
@@ -533,6 +590,11 @@ int32_t ys_mas_create(const ys_mas_desc* d, void** handle) {
     e = cudaFuncSetAttribute(ys::mas_domain_inverse<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(ys::mas_domain_inverse<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // prefer the largest shared-memory carveout so two 96-DoF domains fit per SM
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ys::mas_domain_inverse<6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ys::mas_domain_inverse<8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   }
   if (e != cudaSuccess) {
     ys_set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);

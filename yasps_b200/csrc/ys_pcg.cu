@@ -114,12 +114,15 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
   cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
 }
 
+// kRowLanes threads per row (see spmv3_group).
 __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = t / kRowLanes;
+  const int lane = (int)(t % kRowLanes);
   double v[1] = {0.0};
-  if (i < P.nv) {
-    double q0, q1, q2;
-    spmv3_row(P.sets, P.nsets, P.fp32, i, P.p, q0, q1, q2);
+  double q0, q1, q2;
+  spmv3_group(P.sets, P.nsets, P.fp32, i, i < P.nv, lane, P.p, q0, q1, q2);
+  if (i < P.nv && lane == 0) {
     P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
     v[0] = P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
   }
@@ -264,7 +267,9 @@ uint64_t ys_pcg_workspace_doubles(uint32_t n) {
   const uint64_t nv = (n + 2) / 3;
   const uint64_t grid = (nv + ys::kPcgBlock - 1) / ys::kPcgBlock;
   // r, p, q, z (n each) + slots + partials (4 per block) + tickets
-  return 4ull * 3 * nv + ys::kSlots + 4 * (grid + 1) + 8;
+  // partials: up to 4 values per block of the row kernels, or 1 per block of
+  // the kRowLanes-per-row SpMV (kRowLanes times more blocks)
+  return 4ull * 3 * nv + ys::kSlots + (uint64_t)ys::kRowLanes * (grid + 2) + 8;
 }
 
 int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
@@ -294,7 +299,8 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   P.z = w; w += n;
   P.st = w; w += ys::kSlots;
   const unsigned grid = ys::grid_for(P.nv, ys::kPcgBlock);
-  P.partials = w; w += 4ull * (grid + 1);
+  const unsigned grid_rows = ys::grid_for((uint64_t)P.nv * ys::kRowLanes, ys::kPcgBlock);
+  P.partials = w; w += (uint64_t)ys::kRowLanes * (grid + 2);
   P.tickets = reinterpret_cast<unsigned*>(w);
   P.jinv = a.jacobi_inverse;
   P.stop_rule = a.stop_rule;
@@ -340,7 +346,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       cudaGraph_t body = cp.conditional.phGraph_out[0];
       cudaGraphNode_t n1 = nullptr, n2 = nullptr, n3 = nullptr;
       void* args1[] = {&P};
-      e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot, grid, ys::kPcgBlock, args1);
+      e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot, grid_rows, ys::kPcgBlock, args1);
       if (e == cudaSuccess) {
         if (a.preconditioner == YS_PREC_BLOCK_JACOBI) {
           e = ys::add_kernel(body, &n2, &n1, 1, (const void*)ys::pcg_update_bj, grid, ys::kPcgBlock, args1);

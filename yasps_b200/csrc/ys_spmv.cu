@@ -37,10 +37,12 @@ __global__ void spmv_split_kernel(const uint64_t* __restrict__ keys, const uint3
 
 __global__ void __launch_bounds__(256) spmv3_kernel(SpmvSet set, bool fp32, uint32_t nv, const double* __restrict__ x,
                                                     double* __restrict__ y, int beta) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = t / kRowLanes;
+  const int lane = (int)(t % kRowLanes);
   double y0, y1, y2;
-  spmv3_row(&set, 1, fp32, i, x, y0, y1, y2);
+  spmv3_group(&set, 1, fp32, i, i < nv, lane, x, y0, y1, y2);
+  if (i >= nv || lane != 0) return;
   if (beta) {
     y0 += y[3ull * i];
     y1 += y[3ull * i + 1];
@@ -123,8 +125,8 @@ int32_t ys_spmv3(const double* values, const float* values32, const uint32_t* ro
   YS_REQUIRE((values == nullptr) != (values32 == nullptr), YS_ERR_INVALID, "pass exactly one of values/values32");
   if (num_vars == 0) return YS_OK;
   ys::SpmvSet set{values, values32, row_ptr, entry_block, entry_col};
-  ys::spmv3_kernel<<<ys::grid_for(num_vars, 256), 256, 0, (cudaStream_t)stream>>>(set, values32 != nullptr, num_vars,
-                                                                                   x, y, beta);
+  ys::spmv3_kernel<<<ys::grid_for((uint64_t)num_vars * ys::kRowLanes, 256), 256, 0, (cudaStream_t)stream>>>(
+      set, values32 != nullptr, num_vars, x, y, beta);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

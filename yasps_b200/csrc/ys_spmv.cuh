@@ -51,6 +51,65 @@ __device__ __forceinline__ void spmv3_row_accumulate(const T* __restrict__ vals,
   y2 += (double)a2;
 }
 
+// Row gather by a group of kRowLanes lanes: lane l handles entries l, l+8, ...
+// of the row; the partial sums are combined by a fixed shuffle tree, so the
+// result is deterministic.  Every lane of the warp executes the same
+// shuffles: a row beyond the matrix passes an empty entry range.
+constexpr int kRowLanes = 8;
+
+template <typename T>
+__device__ __forceinline__ void spmv3_group_accumulate(const T* __restrict__ vals, uint32_t e0, uint32_t e1,
+                                                       const uint32_t* __restrict__ eblock,
+                                                       const uint32_t* __restrict__ ecol, int lane,
+                                                       const double* __restrict__ x, double& y0, double& y1,
+                                                       double& y2) {
+  T a0 = 0, a1 = 0, a2 = 0;
+  for (uint32_t e = e0 + lane; e < e1; e += kRowLanes) {
+    const uint32_t eb = __ldg(eblock + e);
+    const uint32_t j = __ldg(ecol + e);
+    const T* b = vals + 9ull * (eb & 0x7fffffffu);
+    const T x0 = (T)__ldg(x + 3ull * j), x1 = (T)__ldg(x + 3ull * j + 1), x2 = (T)__ldg(x + 3ull * j + 2);
+    const T b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2), b3 = __ldg(b + 3), b4 = __ldg(b + 4),
+            b5 = __ldg(b + 5), b6 = __ldg(b + 6), b7 = __ldg(b + 7), b8 = __ldg(b + 8);
+    if (eb & 0x80000000u) {
+      a0 += b0 * x0 + b3 * x1 + b6 * x2;
+      a1 += b1 * x0 + b4 * x1 + b7 * x2;
+      a2 += b2 * x0 + b5 * x1 + b8 * x2;
+    } else {
+      a0 += b0 * x0 + b1 * x1 + b2 * x2;
+      a1 += b3 * x0 + b4 * x1 + b5 * x2;
+      a2 += b6 * x0 + b7 * x1 + b8 * x2;
+    }
+  }
+#pragma unroll
+  for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o, kRowLanes);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o, kRowLanes);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o, kRowLanes);
+  }
+  y0 += (double)a0;
+  y1 += (double)a1;
+  y2 += (double)a2;
+}
+
+// Group version over the (up to two) block sets; every lane of the warp must
+// call it, rows beyond the matrix with valid == false.
+__device__ __forceinline__ void spmv3_group(const SpmvSet* sets, int nsets, bool fp32, uint32_t i, bool valid,
+                                            int lane, const double* __restrict__ x, double& y0, double& y1,
+                                            double& y2) {
+  y0 = y1 = y2 = 0.0;
+  for (int s = 0; s < nsets; ++s) {
+    const uint32_t e0 = valid ? sets[s].row_ptr[i] : 0u;
+    const uint32_t e1 = valid ? sets[s].row_ptr[i + 1] : 0u;
+    if (fp32)
+      spmv3_group_accumulate<float>(sets[s].values32, e0, e1, sets[s].entry_block, sets[s].entry_col, lane, x, y0,
+                                    y1, y2);
+    else
+      spmv3_group_accumulate<double>(sets[s].values, e0, e1, sets[s].entry_block, sets[s].entry_col, lane, x, y0,
+                                     y1, y2);
+  }
+}
+
 // y_i = sum over the (up to two) block sets.
 __device__ __forceinline__ void spmv3_row(const SpmvSet* sets, int nsets, bool fp32, uint32_t i,
                                           const double* __restrict__ x, double& y0, double& y1, double& y2) {

@@ -1,0 +1,90 @@
+"""Per-kernel timing of the Newton inner loop on one FEM cube.
+
+``python -m yasps_b200.kernelbench --side 64 [--kernel all|gemv|spmv|...] [--reps 20]``
+
+Builds the cube workload, runs one Newton step (``masSolver(mixed_spmv=True)``)
+and then launches each kernel stage again ``--reps`` times, timing it with
+CUDA events on the launching stream.  Also the case driver for ncu captures
+(``--kernel gemv --reps 3`` launches the GEMV stage three times).
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+
+import torch
+
+from . import _lib as L
+from . import scenes
+
+
+def _time(fn, reps):
+  s = torch.cuda.current_stream()
+  fn()
+  torch.cuda.synchronize()
+  e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  e0.record(s)
+  for _ in range(reps):
+    fn()
+  e1.record(s)
+  torch.cuda.synchronize()
+  return e0.elapsed_time(e1) / reps
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument("--side", type=int, default=64)
+  ap.add_argument("--kernel", default="all")
+  ap.add_argument("--reps", type=int, default=20)
+  args = ap.parse_args()
+  cube = scenes.fem_cube(args.side, young=1e6, poisson=0.45, noise=0.005)
+  sc, _ = scenes.fem_scene(cube)
+  mz = sc.minimizer
+  mz.setSolver("mas", mixed_spmv=True, stop_rule="residual")
+  mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000)
+  torch.cuda.synchronize()
+  H = mz.activeHessian()
+  mas = mz.linearSolver.implementation
+  bs = H._static
+  d = bs.infos[0]
+  snh = d["term"]
+  plan = H._term_plan(d, bs)
+  p = bs.pattern
+  st = L.stream_ptr()
+  row_ptr, eb, ec = H.spmv_plan(bs)
+  x = torch.cos(torch.arange(H.rows, dtype=torch.float64, device="cuda") * 0.37)
+  y = torch.zeros_like(x)
+  z = torch.zeros_like(x)
+  nv = H.rows // 3
+
+  def snh_eval(method):
+    snh.projection_method = method
+    snh.evaluate(plan, bs.records, H._grad_records)
+    snh.projection_method = 1
+
+  cases = {
+      "snh_eval_only": lambda: snh_eval(0),
+      "snh_eval_project": lambda: snh_eval(1),
+      "assemble3": lambda: L.call("ys_assemble3", L.ptr(bs.records), L.ptr(p.record_begin), L.ptr(p.record_count),
+                                  L.ptr(p.value_offset), p.num_unique, L.ptr(bs.values), L.ptr(bs.values32), st),
+      "mas_numeric": lambda: mas.numeric_update(H, check=False),
+      "spmv_fp64": lambda: L.call("ys_spmv3", L.ptr(bs.values), None, L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv,
+                                  L.ptr(x), L.ptr(y), 0, st),
+      "spmv_fp32": lambda: L.call("ys_spmv3", None, L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv,
+                                  L.ptr(x), L.ptr(y), 0, st),
+      "mas_apply": lambda: L.call("ys_mas_apply", mas._mas, L.ptr(x), L.ptr(z), st),
+      "gemv": lambda: L.call("ys_mas_gemv", mas._mas, st, None),
+      "newton_step": lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
+  }
+  out = {"side": args.side, "tets": cube.tet_count, "dof": cube.dofs, "blocks": p.num_unique,
+         "non_psd": int(snh._const_cache[("work", snh.n)][1].item()), "pcg": mz.linearSolver.statistics}
+  for name, fn in cases.items():
+    if args.kernel in ("all", name):
+      out[name + "_ms"] = _time(fn, args.reps if name != "newton_step" else max(2, args.reps // 5))
+  print(json.dumps(out))
+
+
+if __name__ == "__main__":
+  main()

@@ -165,13 +165,22 @@ class masSolver(_PcgBase):
   """MAS-preconditioned CG (``PKG/solver/masSolver.py:13-126``, ``mas/solver.py``)."""
 
   def __init__(self, max_domain_dofs=96, max_levels=6, target_nodes_per_partition=32, coarsest_level_weight=2.5,
-               level_weights=None, global_coarse_domain=True, mixed_spmv=False, stop_rule="preconditioned",
-               refinement_tolerance=1e-3, max_refinements=8, **unused):
+               fine_level_weight=1.5, level_weights=None, global_coarse_domain=True, mixed_spmv=False,
+               stop_rule="preconditioned", refinement_tolerance=1e-3, max_refinements=8, **unused):
+    """Options follow ``MASSolver`` (``PKG/solver/mas/solver.py:89-120``).
+
+    Level weights default to the reference's device runtime
+    (``mas/cuda_runtime.py:1238-1243``): ``fine_level_weight`` on level 0, 1 on
+    the intermediate levels and ``coarsest_level_weight`` on the coarsest
+    (``fine_level_weight=1.0`` gives the CPU reference's weights,
+    ``mas/preconditioner.py:32-36``).  ``level_weights`` overrides both.
+    """
     super().__init__(stop_rule)
     self.max_domain_dofs = int(max_domain_dofs)
     self.max_levels = int(max_levels)
     self.target_nodes = int(target_nodes_per_partition)
     self.coarsest_level_weight = float(coarsest_level_weight)
+    self.fine_level_weight = float(fine_level_weight)
     self.level_weights = None if level_weights is None else tuple(float(w) for w in level_weights)
     self.global_coarse_domain = bool(global_coarse_domain)
     self.mixed_spmv = bool(mixed_spmv)
@@ -210,7 +219,8 @@ class masSolver(_PcgBase):
     self._tables = t
     nl = len(self.hierarchy.levels)
     if self.level_weights is None:
-      weights = (1.0,) * (nl - 1) + (self.coarsest_level_weight,)
+      weights = ((self.coarsest_level_weight,) if nl == 1 else
+                 (self.fine_level_weight,) + (1.0,) * (nl - 2) + (self.coarsest_level_weight,))
     else:
       if len(self.level_weights) < nl:
         raise ValueError("level_weights needs one weight per level")
