@@ -14,7 +14,8 @@
 //                      the reference's default backend), writes FP32.
 // Application (every PCG iteration, HBM bound on the FP32 inverses):
 //   mas_restrict : packed FP32 level residuals (fixed-order child sums);
-//   mas_gemv     : one CTA per domain, z_d = A_d^-1 r_d (coalesced columns);
+//   mas_gemv     : one CTA per domain, z_d = A_d^-1 r_d from the packed upper
+//                  triangle staged in shared memory;
 //   mas_collect  : z = sum_l w_l z_l(map_l(i)) fused with r^T z, r^T r and the
 //                  PCG stop test (deterministic last-block reduction).
 #include <cmath>
@@ -183,10 +184,12 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
     }
   __syncthreads();
   if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
+  // FP32 upper triangle, row-major packed (row i holds columns i..n-1).
   float* out = M.inverse + M.inv_offset[d];
-  for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) {
-    const uint32_t i = t / n, j = t % n;
-    out[t] = (float)(0.5 * (A[i * n + j] + A[j * n + i]));
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t i = warp; i < n; i += kInvThreads / 32) {
+    const uint32_t base = i * n - i * (i - 1) / 2;
+    for (uint32_t j = i + lane; j < n; j += 32) out[base + (j - i)] = (float)(0.5 * (A[i * n + j] + A[j * n + i]));
   }
 }
 
@@ -251,29 +254,52 @@ __host__ __device__ inline uint32_t restrict_tail_first(const MasDev& M) {
   return first;
 }
 
-// z_d = A_d^-1 r_d, one CTA per domain; thread i owns output row i and reads
-// column i of the symmetric inverse (coalesced across the CTA).
+// z_d = A_d^-1 r_d, one CTA per domain.  The FP32 inverse is stored as its
+// packed upper triangle (n(n+1)/2 floats from a 16-byte aligned offset): it is
+// staged in shared memory with coalesced 16-byte loads, so every byte crosses
+// HBM once and half as many bytes cross as for a full n x n inverse.  Thread i
+// owns output row i; S(i, j) for j < i is read from column i of the upper
+// triangle (consecutive threads, consecutive words).
+__host__ __device__ inline uint32_t gemv_rloc_offset(uint32_t max_dofs) {
+  return (max_dofs * (max_dofs + 1) / 2 + 3) & ~3u;
+}
+inline size_t gemv_smem_bytes(uint32_t max_dofs) { return 4ull * (gemv_rloc_offset(max_dofs) + max_dofs); }
+
 __global__ void __launch_bounds__(128) mas_gemv(MasDev M) {
-  __shared__ float rloc[384];
+  extern __shared__ float4 gemv_smem[];
+  float* S = reinterpret_cast<float*>(gemv_smem);
+  float* rloc = S + gemv_rloc_offset(M.max_dofs);
   const uint32_t d = blockIdx.x;
   const uint32_t nb = M.dom_node_ptr[d], nn = M.dom_node_ptr[d + 1] - nb;
   const uint32_t n = 3 * nn;
+  const uint32_t packed4 = (n * (n + 1) / 2 + 3) / 4;
+  const float4* src = reinterpret_cast<const float4*>(M.inverse + M.inv_offset[d]);
+  for (uint32_t t = threadIdx.x; t < packed4; t += blockDim.x) gemv_smem[t] = __ldg(src + t);
   for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
     const uint32_t node = M.dom_nodes[nb + t / 3];
     rloc[t] = M.rl[3ull * node + t % 3];
   }
   __syncthreads();
-  const float* inv = M.inverse + M.inv_offset[d];
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    // 8 independent partial sums keep 8 column loads in flight per thread.
-    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const uint32_t bi = i * n - i * (i - 1) / 2 - i;  // S(i, j) = S[bi + j], j >= i
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    uint32_t bj = 0;  // start of packed row j
     uint32_t j = 0;
-    for (; j + 8 <= n; j += 8) {
+    for (; j + 4 <= n; j += 4) {
 #pragma unroll
-      for (int u = 0; u < 8; ++u) acc[u] += __ldg(inv + (uint64_t)(j + u) * n + i) * rloc[j + u];
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t jj = j + u;
+        const uint32_t idx = jj < i ? bj + (i - jj) : bi + jj;
+        acc[u] += S[idx] * rloc[jj];
+        bj += n - jj;
+      }
     }
-    for (; j < n; ++j) acc[0] += __ldg(inv + (uint64_t)j * n + i) * rloc[j];
-    const float s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    for (; j < n; ++j) {
+      const uint32_t idx = j < i ? bj + (i - j) : bi + j;
+      acc[0] += S[idx] * rloc[j];
+      bj += n - j;
+    }
+    const float s = (acc[0] + acc[1]) + (acc[2] + acc[3]);
     const uint32_t node = M.dom_nodes[nb + i / 3];
     M.zl[3ull * node + i % 3] = s;
   }
@@ -488,7 +514,7 @@ static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGra
   if (e != cudaSuccess) return e;
   cudaGraphNode_t n2 = nullptr;
   void* a2[] = {&m};
-  e = add_kernel(g, &n2, dp, nd, (const void*)mas_gemv, M.num_domains, 128, 0, a2);
+  e = add_kernel(g, &n2, dp, nd, (const void*)mas_gemv, M.num_domains, 128, (unsigned)gemv_smem_bytes(M.max_dofs), a2);
   *last = n2;
   return e;
 }
@@ -646,7 +672,7 @@ int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
     ys::mas_restrict<<<ys::grid_for(cnt, 256), 256, 0, s>>>(M, r, l);
     YS_CHECK_LAUNCH();
   }
-  ys::mas_gemv<<<M.num_domains, 128, 0, s>>>(M);
+  ys::mas_gemv<<<M.num_domains, 128, ys::gemv_smem_bytes(M.max_dofs), s>>>(M);
   YS_CHECK_LAUNCH();
   ys::MasPcg P{};
   P.M = M;
@@ -662,17 +688,17 @@ int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes) {
   auto* h = static_cast<ys::MasHandle*>(handle);
   ys::MasDev& M = h->M;
   if (algorithmic_bytes) {
-    // every inverse read once (FP32) + the gathered residual and the correction
+    // every packed FP32 inverse read once + the gathered residual and the correction
     std::vector<uint32_t> ptr(M.num_domains + 1);
     cudaMemcpy(ptr.data(), M.dom_node_ptr, sizeof(uint32_t) * (M.num_domains + 1), cudaMemcpyDeviceToHost);
     uint64_t bytes = 0;
     for (uint32_t d = 0; d < M.num_domains; ++d) {
       const uint64_t n = 3ull * (ptr[d + 1] - ptr[d]);
-      bytes += 4 * n * n + 4 * n + 4 * n + 4 * (n / 3);
+      bytes += 4 * ((n * (n + 1) / 2 + 3) / 4 * 4) + 4 * n + 4 * n + 4 * (n / 3);
     }
     *algorithmic_bytes = bytes;
   }
-  ys::mas_gemv<<<M.num_domains, 128, 0, (cudaStream_t)stream>>>(M);
+  ys::mas_gemv<<<M.num_domains, 128, ys::gemv_smem_bytes(M.max_dofs), (cudaStream_t)stream>>>(M);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

@@ -64,21 +64,46 @@ __device__ __forceinline__ void spmv3_group_accumulate(const T* __restrict__ val
                                                        const double* __restrict__ x, double& y0, double& y1,
                                                        double& y2) {
   T a0 = 0, a1 = 0, a2 = 0;
-  for (uint32_t e = e0 + lane; e < e1; e += kRowLanes) {
-    const uint32_t eb = __ldg(eblock + e);
-    const uint32_t j = __ldg(ecol + e);
-    const T* b = vals + 9ull * (eb & 0x7fffffffu);
-    const T x0 = (T)__ldg(x + 3ull * j), x1 = (T)__ldg(x + 3ull * j + 1), x2 = (T)__ldg(x + 3ull * j + 2);
-    const T b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2), b3 = __ldg(b + 3), b4 = __ldg(b + 4),
-            b5 = __ldg(b + 5), b6 = __ldg(b + 6), b7 = __ldg(b + 7), b8 = __ldg(b + 8);
-    if (eb & 0x80000000u) {
-      a0 += b0 * x0 + b3 * x1 + b6 * x2;
-      a1 += b1 * x0 + b4 * x1 + b7 * x2;
-      a2 += b2 * x0 + b5 * x1 + b8 * x2;
+  // Two entries per iteration (e and e + kRowLanes): both index loads, then
+  // both value/vector gathers are in flight before any use.
+  for (uint32_t e = e0 + lane; e < e1; e += 2 * kRowLanes) {
+    const uint32_t f = e + kRowLanes;
+    const bool two = f < e1;
+    const uint32_t ebA = __ldg(eblock + e), jA = __ldg(ecol + e);
+    const uint32_t ebB = two ? __ldg(eblock + f) : ebA, jB = two ? __ldg(ecol + f) : jA;
+    const T* bA = vals + 9ull * (ebA & 0x7fffffffu);
+    const T* bB = vals + 9ull * (ebB & 0x7fffffffu);
+    T xa[3], xb[3], ba[9], bb[9];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      xa[k] = (T)__ldg(x + 3ull * jA + k);
+      xb[k] = (T)__ldg(x + 3ull * jB + k);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      ba[k] = __ldg(bA + k);
+      bb[k] = __ldg(bB + k);
+    }
+    const T wB = two ? (T)1 : (T)0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) xb[k] *= wB;
+    if (ebA & 0x80000000u) {
+      a0 += ba[0] * xa[0] + ba[3] * xa[1] + ba[6] * xa[2];
+      a1 += ba[1] * xa[0] + ba[4] * xa[1] + ba[7] * xa[2];
+      a2 += ba[2] * xa[0] + ba[5] * xa[1] + ba[8] * xa[2];
     } else {
-      a0 += b0 * x0 + b1 * x1 + b2 * x2;
-      a1 += b3 * x0 + b4 * x1 + b5 * x2;
-      a2 += b6 * x0 + b7 * x1 + b8 * x2;
+      a0 += ba[0] * xa[0] + ba[1] * xa[1] + ba[2] * xa[2];
+      a1 += ba[3] * xa[0] + ba[4] * xa[1] + ba[5] * xa[2];
+      a2 += ba[6] * xa[0] + ba[7] * xa[1] + ba[8] * xa[2];
+    }
+    if (ebB & 0x80000000u) {
+      a0 += bb[0] * xb[0] + bb[3] * xb[1] + bb[6] * xb[2];
+      a1 += bb[1] * xb[0] + bb[4] * xb[1] + bb[7] * xb[2];
+      a2 += bb[2] * xb[0] + bb[5] * xb[1] + bb[8] * xb[2];
+    } else {
+      a0 += bb[0] * xb[0] + bb[1] * xb[1] + bb[2] * xb[2];
+      a1 += bb[3] * xb[0] + bb[4] * xb[1] + bb[5] * xb[2];
+      a2 += bb[6] * xb[0] + bb[7] * xb[1] + bb[8] * xb[2];
     }
   }
 #pragma unroll

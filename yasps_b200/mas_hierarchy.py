@@ -223,7 +223,8 @@ def build_tables(h: Hierarchy, fine_positions: np.ndarray) -> MasTables:
       dom_nodes.append(offs[l] + dom)
       dom_ptr.append(dom_ptr[-1] + dom.size)
       inv_off.append(cursor)
-      cursor += (3 * dom.size) ** 2
+      k = 3 * dom.size
+      cursor += (k * (k + 1) // 2 + 3) // 4 * 4  # packed upper triangle, 16-byte aligned
       max_dofs = max(max_dofs, 3 * dom.size)
     node_dom.append(nd)
     node_loc.append(nl)
