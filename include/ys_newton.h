@@ -73,6 +73,18 @@ int32_t ys_compress_indices(const uint32_t* codes, const uint16_t* sizes, uint32
                             int16_t* perm, uint16_t* total_sizes, uint32_t* coord_outer,
                             void* stream);
 
+/* Same arguments and outputs as ys_compress_indices (bit-identical), but the
+ * call allocates nothing: the count scan keeps its tile sums in a fixed
+ * 128 KiB device array of the library instead of temporary storage from
+ * cudaMallocAsync.  No counterpart in the reference.
+ * Limit: n <= 67,108,864 instances; larger n returns YS_ERR_CAPACITY.
+ * The first call on a device resolves the array's address (set-up), so make
+ * it before any stream capture.  All calls on a device share the array: calls
+ * that overlap in time (other streams or threads) race on it.              */
+int32_t ys_compress_indices_noalloc(const uint32_t* codes, const uint16_t* sizes, uint32_t n,
+                                    uint32_t K, int16_t* perm, uint16_t* total_sizes,
+                                    uint32_t* coord_outer, void* stream);
+
 /* Upper-triangle block coordinates (scalar (row,col) pairs) and dims.
  * Replaces `int computeCoordinates(...)` (gradientIndicesKernel.pyx:276-318). */
 int32_t ys_compute_coordinates(const uint32_t* codes, const int16_t* perm, const uint16_t* sizes,

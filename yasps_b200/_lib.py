@@ -88,6 +88,7 @@ SIGNATURES = {
     "ys_version": (i32, []),
     "ys_join_union_indices": (i32, [vp, u32, u32, u32, P(u32), P(i32), P(u32), u32, vp, vp, vp]),
     "ys_compress_indices": (i32, [vp, vp, u32, u32, vp, vp, vp, vp]),
+    "ys_compress_indices_noalloc": (i32, [vp, vp, u32, u32, vp, vp, vp, vp]),
     "ys_compute_coordinates": (i32, [vp, vp, vp, vp, u32, u32, vp, vp, vp]),
     "ys_pattern_workspace_bytes": (i32, [u32, P(u64)]),
     "ys_pattern_build": (i32, [vp, vp, u32, vp, u64, P(PatternOut), vp]),

@@ -146,6 +146,124 @@ __global__ void grad_coords_kernel(const uint32_t* __restrict__ codes, const uin
   }
 }
 
+// ---- allocation-free compression -----------------------------------------
+//
+// ys_compress_indices_noalloc runs compress_kernel and then scans the counts
+// with a three-pass tiled scan (tile sums, one-block scan of the tile sums,
+// per-tile scan plus offset) instead of the CUB device scan, whose temporary
+// storage comes from cudaMallocAsync.  The tile sums live in a fixed
+// file-scope device array: at most kNoAllocMaxTiles tiles of kScanTile counts,
+// i.e. n <= 67,108,864 instances, 128 KiB of scratch per device.  Each call
+// writes every tile sum it reads before reading it, so nothing has to start
+// at zero; all calls on a device share the array, so two calls that overlap in
+// time (different streams or threads) race on it.  The scan is modulo 2^32
+// like the CUB scan, so the outputs are bit-identical.
+constexpr uint32_t kScanThreads = 256;
+constexpr uint32_t kScanItems = 8;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;
+constexpr uint32_t kNoAllocMaxTiles = 32768;
+constexpr uint64_t kNoAllocMaxInstances = (uint64_t)kNoAllocMaxTiles * kScanTile;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) uint32_t g_noalloc_tile_sums[kNoAllocMaxTiles];
+
+__global__ void __launch_bounds__(kScanThreads) scan_tile_sums(const uint32_t* __restrict__ v, uint32_t n,
+                                                               uint32_t* __restrict__ tile_sums) {
+  using Reduce = cub::BlockReduce<uint32_t, kScanThreads>;
+  __shared__ typename Reduce::TempStorage tmp;
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+  uint32_t s = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kScanItems; ++k) {
+    const uint64_t i = base + k * kScanThreads + threadIdx.x;
+    if (i < n) s += v[i];
+  }
+  s = Reduce(tmp).Sum(s);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = s;
+}
+
+// Exclusive scan of the tile sums in place, one block of 1024 threads; thread
+// t owns a run of ceil(tiles / 1024) consecutive sums.
+__global__ void __launch_bounds__(1024) scan_tile_offsets(uint32_t* __restrict__ tile_sums, uint32_t tiles) {
+  using Scan = cub::BlockScan<uint32_t, 1024>;
+  __shared__ typename Scan::TempStorage tmp;
+  const uint32_t per = (tiles + 1023) / 1024;
+  const uint32_t b = threadIdx.x * per;
+  uint32_t s = 0;
+  for (uint32_t k = 0; k < per; ++k)
+    if (b + k < tiles) s += tile_sums[b + k];
+  uint32_t pre = 0;
+  Scan(tmp).ExclusiveSum(s, pre);
+  for (uint32_t k = 0; k < per; ++k) {
+    if (b + k < tiles) {
+      const uint32_t v = tile_sums[b + k];
+      tile_sums[b + k] = pre;
+      pre += v;
+    }
+  }
+}
+
+// In-place inclusive scan of one tile plus its offset.  The tile is staged in
+// shared memory with one pad word per 32 (conflict-free striped and blocked
+// access).
+__global__ void __launch_bounds__(kScanThreads) scan_tiles(uint32_t* __restrict__ v, uint32_t n,
+                                                           const uint32_t* __restrict__ tile_offsets) {
+  using Scan = cub::BlockScan<uint32_t, kScanThreads>;
+  __shared__ typename Scan::TempStorage tmp;
+  __shared__ uint32_t tile[kScanTile + kScanTile / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+#pragma unroll
+  for (uint32_t k = 0; k < kScanItems; ++k) {
+    const uint32_t x = k * kScanThreads + threadIdx.x;
+    tile[x + (x >> 5)] = base + x < n ? v[base + x] : 0u;
+  }
+  __syncthreads();
+  uint32_t run[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kScanItems; ++k) {
+    const uint32_t x = threadIdx.x * kScanItems + k;
+    s += tile[x + (x >> 5)];
+    run[k] = s;
+  }
+  uint32_t pre = 0;
+  Scan(tmp).ExclusiveSum(s, pre);
+  pre += tile_offsets[blockIdx.x];
+#pragma unroll
+  for (uint32_t k = 0; k < kScanItems; ++k) {
+    const uint32_t x = threadIdx.x * kScanItems + k;
+    tile[x + (x >> 5)] = run[k] + pre;
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t k = 0; k < kScanItems; ++k) {
+    const uint32_t x = k * kScanThreads + threadIdx.x;
+    if (base + x < n) v[base + x] = tile[x + (x >> 5)];
+  }
+}
+
+// Device address of the tile-sum array for the current device, resolved once
+// per device (the first call on a device does this set-up).
+static int32_t noalloc_tile_sums(uint32_t** out) {
+  static std::mutex mu;
+  static void* addr[kNoAllocMaxDevices] = {};
+  int dev = 0;
+  YS_CUDA_TRY(cudaGetDevice(&dev));
+  YS_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, YS_ERR_INVALID, "device ordinal beyond 63");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_tile_sums);
+    if (e != cudaSuccess || !p) {
+      ys_set_last_error(e != cudaSuccess ? cudaGetErrorString(e) : "null scratch address", __FILE__, __LINE__);
+      return YS_ERR_CUDA;
+    }
+    addr[dev] = p;
+  }
+  *out = static_cast<uint32_t*>(addr[dev]);
+  return YS_OK;
+}
+
 }  // namespace ys
 
 extern "C" {
@@ -218,6 +336,29 @@ int32_t ys_compute_coordinates(const uint32_t* codes, const int16_t* perm, const
   if (n == 0) return YS_OK;
   ys::coordinates_kernel<<<ys::grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(codes, perm, sizes, coord_outer, n,
                                                                                    K, coords, dims);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_compress_indices_noalloc(const uint32_t* codes, const uint16_t* sizes, uint32_t n, uint32_t K,
+                                    int16_t* perm, uint16_t* total_sizes, uint32_t* coord_outer, void* stream) {
+  YS_REQUIRE(K >= 1 && K <= 4096, YS_ERR_INVALID, "K must be 1..4096");
+  YS_REQUIRE(n <= ys::kNoAllocMaxInstances, YS_ERR_CAPACITY,
+             "n exceeds the allocation-free scan's fixed scratch (at most 67,108,864 instances)");
+  uint32_t* tile_sums = nullptr;
+  const int32_t rc = ys::noalloc_tile_sums(&tile_sums);
+  if (rc != YS_OK) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  YS_CUDA_TRY(cudaMemsetAsync(coord_outer, 0, sizeof(uint32_t), s));
+  if (n == 0) return YS_OK;
+  ys::compress_kernel<<<ys::grid_for(n, 256), 256, 0, s>>>(codes, sizes, n, K, perm, total_sizes, coord_outer + 1);
+  YS_CHECK_LAUNCH();
+  const uint32_t tiles = (uint32_t)((n + ys::kScanTile - 1) / ys::kScanTile);
+  ys::scan_tile_sums<<<tiles, ys::kScanThreads, 0, s>>>(coord_outer + 1, n, tile_sums);
+  YS_CHECK_LAUNCH();
+  ys::scan_tile_offsets<<<1, 1024, 0, s>>>(tile_sums, tiles);
+  YS_CHECK_LAUNCH();
+  ys::scan_tiles<<<tiles, ys::kScanThreads, 0, s>>>(coord_outer + 1, n, tile_sums);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }
