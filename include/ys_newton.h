@@ -370,6 +370,56 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle);
 int32_t ys_pcg_run(void* handle, void* stream, ys_pcg_result* result);
 int32_t ys_pcg_destroy(void* handle);
 
+/* ---- serving form: batched MAS-PCG over resident solves ------------------
+ * Many Newton-step solves ("slots") advance together: one launch runs
+ * `passes_per_launch` pipeline passes over every attached slot, each pass a
+ * PCG iteration of every live slot (FP32 blocks and MAS inside, FP64
+ * vectors, dots and refinement residuals; the precision form of masSolver
+ * with mixed_spmv).  Converged slots retire on the device; the host attaches
+ * new slots between launches.  A slot's arithmetic does not depend on the
+ * other slots in the launch, so its result is bit-identical alone and in a
+ * mix.  The reference has no serving form (its MAS PCG solves one system,
+ * PKG/solver/mas/cuda_runtime.py:3549-3751).                              */
+#define YS_SERVE_EMPTY 0   /* no solve attached                               */
+#define YS_SERVE_INIT 1    /* attached, not started                           */
+#define YS_SERVE_REFINE 2  /* FP64 residual of x in the next pass             */
+#define YS_SERVE_START 3   /* inner PCG restart in this pass                  */
+#define YS_SERVE_ITER 4    /* inner PCG iterating                             */
+#define YS_SERVE_DONE 5    /* ||g - H x|| <= tolerance ||g|| (FP64 blocks)     */
+#define YS_SERVE_FAILED 6  /* non-SPD curvature / preconditioner, or budget   */
+
+typedef struct ys_serve_slot_desc {
+  void* mas;                   /* ys_mas handle of this solve, numeric update done */
+  ys_matrix3 matrix;           /* one 3x3 block set: values (FP64) + values32 (FP32) */
+  const double* rhs;           /* g [3 * num_vars]                                   */
+  double* solution;            /* x [3 * num_vars] (written)                         */
+  double* workspace;           /* ys_serve_workspace_doubles(num_vars) doubles        */
+  double tolerance;            /* target true relative residual                      */
+  double refinement_tolerance; /* lower bound of every inner relative tolerance      */
+  uint32_t max_iterations;     /* inner iterations over all refinements              */
+} ys_serve_slot_desc;
+
+typedef struct ys_serve_slot_status {
+  int32_t phase;               /* YS_SERVE_*                                         */
+  uint32_t iterations;         /* inner PCG iterations so far                        */
+  uint32_t refinements;        /* FP64 residual evaluations after the first          */
+  double relative_residual;    /* ||g - H x|| / ||g|| at the last FP64 evaluation     */
+} ys_serve_slot_status;
+
+uint64_t ys_serve_workspace_doubles(uint32_t num_vars);
+/* max_slots <= 256; passes_per_launch <= 64. */
+int32_t ys_serve_create(uint32_t max_slots, uint32_t passes_per_launch, void** handle);
+/* Attach a solve to a free slot (takes effect at the next launch). */
+int32_t ys_serve_attach(void* handle, uint32_t slot, const ys_serve_slot_desc* desc);
+/* Detach a slot (its buffers are no longer read after the next launch). */
+int32_t ys_serve_detach(void* handle, uint32_t slot);
+/* Run passes_per_launch passes over the attached slots on `stream`
+ * (asynchronous; one CUDA graph per size bucket of the CTA tables). */
+int32_t ys_serve_launch(void* handle, void* stream);
+/* Synchronise `stream` and report every slot: out[max_slots]. */
+int32_t ys_serve_status(void* handle, void* stream, ys_serve_slot_status* out);
+int32_t ys_serve_destroy(void* handle);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -27,6 +27,7 @@ YS_PREC_MAS = 1
 YS_STOP_PRECONDITIONED = 0
 YS_STOP_RESIDUAL = 1
 YS_MAX_UNION = 8
+YS_SERVE_EMPTY, YS_SERVE_INIT, YS_SERVE_REFINE, YS_SERVE_START, YS_SERVE_ITER, YS_SERVE_DONE, YS_SERVE_FAILED = range(7)
 
 
 class PatternOut(C.Structure):
@@ -82,6 +83,15 @@ class MasDesc(C.Structure):
               ("level_residual", vp), ("level_correction", vp), ("status", vp), ("level_residual64", vp)]
 
 
+
+class ServeSlotDesc(C.Structure):
+  _fields_ = [("mas", vp), ("matrix", Matrix3), ("rhs", vp), ("solution", vp), ("workspace", vp), ("tolerance", f64),
+              ("refinement_tolerance", f64), ("max_iterations", u32)]
+
+
+class ServeSlotStatus(C.Structure):
+  _fields_ = [("phase", i32), ("iterations", u32), ("refinements", u32), ("relative_residual", f64)]
+
 # name: (restype, argtypes)
 SIGNATURES = {
     "ys_last_error": (C.c_char_p, []),
@@ -117,6 +127,13 @@ SIGNATURES = {
     "ys_gradient_coordinates": (i32, [vp, vp, u32, u32, vp, vp, vp, vp]),
     "ys_refine_workspace_doubles": (u64, [u32]),
     "ys_refine_residual": (i32, [P(Matrix3), vp, vp, vp, vp, vp, P(f64), vp]),
+    "ys_serve_workspace_doubles": (u64, [u32]),
+    "ys_serve_create": (i32, [u32, u32, P(vp)]),
+    "ys_serve_attach": (i32, [vp, u32, P(ServeSlotDesc)]),
+    "ys_serve_detach": (i32, [vp, u32]),
+    "ys_serve_launch": (i32, [vp, vp]),
+    "ys_serve_status": (i32, [vp, vp, P(ServeSlotStatus)]),
+    "ys_serve_destroy": (i32, [vp]),
 }
 
 _lib = None
