@@ -121,6 +121,56 @@ class _PcgBase:
     return res
 
 
+def upload_mas_tables(t):
+  """Device copies of the structural MAS tables (shared by every numeric state)."""
+  torch = _torch()
+  up = lambda a, dt=torch.int32: torch.from_numpy(np.ascontiguousarray(a).view(
+      np.int32 if dt == torch.int32 else np.int64)).to(_dev())
+  return dict(cmap=up(t.cmap), child_ptr=up(t.child_ptr), child_fine=up(t.child_fine),
+              dom_node_ptr=up(t.dom_node_ptr), dom_nodes=up(t.dom_nodes),
+              inv_offset=up(t.inv_offset, torch.int64), dom_entry_ptr=up(t.dom_entry_ptr),
+              dom_entry=up(t.dom_entry), cb_src_ptr=up(t.cb_src_ptr), cb_src=up(t.cb_src))
+
+
+def mas_numeric_buffers(t):
+  """Per-solve numeric MAS state: Galerkin blocks, FP32 inverses, level vectors."""
+  torch = _torch()
+  nb_coarse = int(t.cb_level_begin[-1])
+  packed = int(t.level_node_offset[-1])
+  return dict(coarse_values=torch.zeros(max(9 * nb_coarse, 1), dtype=torch.float64, device=_dev()),
+              inverse=torch.zeros(max(t.inverse_floats, 1), dtype=torch.float32, device=_dev()),
+              rl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
+              zl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
+              rl64=torch.zeros(3 * packed, dtype=torch.float64, device=_dev()),
+              status=torch.zeros(1, dtype=torch.int32, device=_dev()))
+
+
+def create_mas_handle(t, nv, weights, dev):
+  """``ys_mas_create`` over tables ``t`` (host) / ``dev`` (device tables and
+  numeric buffers); returns the handle and the host arrays it borrowed."""
+  nl = len(t.level_node_offset) - 1
+  lno = (L.u32 * (nl + 1))(*t.level_node_offset.tolist())
+  lw = (L.f64 * nl)(*weights)
+  cbl = (L.u32 * (nl + 1))(*t.cb_level_begin.tolist())
+  d = L.MasDesc()
+  d.num_fine_vars, d.num_levels = nv, nl
+  d.level_node_offset, d.level_weights = lno, lw
+  d.cmap, d.child_ptr, d.child_fine = L.ptr(dev["cmap"]), L.ptr(dev["child_ptr"]), L.ptr(dev["child_fine"])
+  d.num_domains = len(t.dom_node_ptr) - 1
+  d.dom_node_ptr, d.dom_nodes, d.inv_offset = L.ptr(dev["dom_node_ptr"]), L.ptr(dev["dom_nodes"]), L.ptr(
+      dev["inv_offset"])
+  d.dom_entry_ptr, d.dom_entry = L.ptr(dev["dom_entry_ptr"]), L.ptr(dev["dom_entry"])
+  d.fine_blocks, d.coarse_blocks = t.fine_blocks, int(t.cb_level_begin[-1])
+  d.cb_src_ptr, d.cb_src, d.cb_level_begin = L.ptr(dev["cb_src_ptr"]), L.ptr(dev["cb_src"]), cbl
+  d.max_domain_dofs = t.max_domain_dofs
+  d.coarse_values, d.inverse = L.ptr(dev["coarse_values"]), L.ptr(dev["inverse"])
+  d.level_residual, d.level_correction, d.status = L.ptr(dev["rl"]), L.ptr(dev["zl"]), L.ptr(dev["status"])
+  d.level_residual64 = L.ptr(dev["rl64"])
+  h = ctypes.c_void_p()
+  L.call("ys_mas_create", ctypes.byref(d), ctypes.byref(h))
+  return h, (lno, lw, cbl)
+
+
 class jacobianPCGSolver(_PcgBase):
   """Block-Jacobi PCG (``PKG/solver/jacobianPCGSolver.pyx:84-166``)."""
 
@@ -192,6 +242,16 @@ class masSolver(_PcgBase):
     self._tables = None
     self._dev_tables = None
 
+  def weights_for(self, nl):
+    """Level weights of an ``nl``-level hierarchy."""
+    if self.level_weights is None:
+      return ((self.coarsest_level_weight,) if nl == 1 else
+              (self.fine_level_weight,) + (1.0,) * (nl - 2) + (self.coarsest_level_weight,))
+    if len(self.level_weights) < nl:
+      raise ValueError("level_weights needs one weight per level")
+    return self.level_weights[:nl - 1] + self.level_weights[-1:] if len(self.level_weights) > nl else \
+        self.level_weights
+
   def reset(self):
     super().reset()
     if self._mas is not None:
@@ -217,50 +277,12 @@ class masSolver(_PcgBase):
                                                    self.target_nodes, self.global_coarse_domain)
     t = mas_hierarchy.build_tables(self.hierarchy, pos)
     self._tables = t
-    nl = len(self.hierarchy.levels)
-    if self.level_weights is None:
-      weights = ((self.coarsest_level_weight,) if nl == 1 else
-                 (self.fine_level_weight,) + (1.0,) * (nl - 2) + (self.coarsest_level_weight,))
-    else:
-      if len(self.level_weights) < nl:
-        raise ValueError("level_weights needs one weight per level")
-      weights = self.level_weights[:nl - 1] + self.level_weights[-1:] if len(self.level_weights) > nl else \
-          self.level_weights
-    up = lambda a, dt=torch.int32: torch.from_numpy(np.ascontiguousarray(a).view(
-        np.int32 if dt == torch.int32 else np.int64)).to(_dev())
-    nb_coarse = int(t.cb_level_begin[-1])
-    packed = int(t.level_node_offset[-1])
-    dev = dict(cmap=up(t.cmap), child_ptr=up(t.child_ptr), child_fine=up(t.child_fine),
-               dom_node_ptr=up(t.dom_node_ptr), dom_nodes=up(t.dom_nodes),
-               inv_offset=up(t.inv_offset, torch.int64), dom_entry_ptr=up(t.dom_entry_ptr),
-               dom_entry=up(t.dom_entry), cb_src_ptr=up(t.cb_src_ptr), cb_src=up(t.cb_src),
-               coarse_values=torch.zeros(max(9 * nb_coarse, 1), dtype=torch.float64, device=_dev()),
-               inverse=torch.zeros(max(t.inverse_floats, 1), dtype=torch.float32, device=_dev()),
-               rl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
-               zl=torch.zeros(3 * packed, dtype=torch.float32, device=_dev()),
-               rl64=torch.zeros(3 * packed, dtype=torch.float64, device=_dev()),
-               status=torch.zeros(1, dtype=torch.int32, device=_dev()))
-    lno = (L.u32 * (nl + 1))(*t.level_node_offset.tolist())
-    lw = (L.f64 * nl)(*weights)
-    cbl = (L.u32 * (nl + 1))(*t.cb_level_begin.tolist())
-    d = L.MasDesc()
-    d.num_fine_vars, d.num_levels = nv, nl
-    d.level_node_offset, d.level_weights = lno, lw
-    d.cmap, d.child_ptr, d.child_fine = L.ptr(dev["cmap"]), L.ptr(dev["child_ptr"]), L.ptr(dev["child_fine"])
-    d.num_domains = len(t.dom_node_ptr) - 1
-    d.dom_node_ptr, d.dom_nodes, d.inv_offset = L.ptr(dev["dom_node_ptr"]), L.ptr(dev["dom_nodes"]), L.ptr(
-        dev["inv_offset"])
-    d.dom_entry_ptr, d.dom_entry = L.ptr(dev["dom_entry_ptr"]), L.ptr(dev["dom_entry"])
-    d.fine_blocks, d.coarse_blocks = t.fine_blocks, nb_coarse
-    d.cb_src_ptr, d.cb_src, d.cb_level_begin = L.ptr(dev["cb_src_ptr"]), L.ptr(dev["cb_src"]), cbl
-    d.max_domain_dofs = t.max_domain_dofs
-    d.coarse_values, d.inverse = L.ptr(dev["coarse_values"]), L.ptr(dev["inverse"])
-    d.level_residual, d.level_correction, d.status = L.ptr(dev["rl"]), L.ptr(dev["zl"]), L.ptr(dev["status"])
-    d.level_residual64 = L.ptr(dev["rl64"])
-    h = ctypes.c_void_p()
-    L.call("ys_mas_create", ctypes.byref(d), ctypes.byref(h))
+    weights = self.weights_for(len(self.hierarchy.levels))
+    dev = upload_mas_tables(t)
+    dev.update(mas_numeric_buffers(t))
+    h, keep = create_mas_handle(t, nv, weights, dev)
     self._mas = h
-    self._dev_tables = (dev, lno, lw, cbl)
+    self._dev_tables = (dev, keep)
     self._mas_key = key
     self._cache.release()
 
