@@ -90,3 +90,34 @@ def test_scene_api_validation():
     t.addConnectivity("bad", v, [[0, 1, 2, 9]], 4)
   with pytest.raises(ValueError):
     sc.addMinimizeTarget([x, x])
+
+
+def test_fem_positions_match_fem_cube():
+  from yasps_b200 import scenes
+  c = scenes.fem_cube(6, young=3e4, poisson=0.33, noise=0.02, seed=11)
+  pinned, free = scenes.fem_positions(6, noise=0.02, seed=11)
+  assert np.array_equal(pinned, c.pinned_position) and np.array_equal(free, c.free_position)
+
+
+def test_poisson_stream_shapes_and_ranges():
+  from yasps_b200 import serving
+  reqs = serving.poisson_fem_stream(count=40, mean_spacing=2e-3, side_range=(4, 9), seed=3)
+  arr = np.array([r.arrival for r in reqs])
+  assert arr[0] == 0.0 and np.all(np.diff(arr) >= 0)
+  assert all(4 <= r.side <= 9 for r in reqs)
+  for r in reqs:
+    assert r.free_position.numel() == 3 * r.side ** 2 * (r.side - 1)
+    assert r.pinned_position.numel() == 3 * r.side ** 2
+  mu = np.array([r.mu for r in reqs])
+  assert np.all(mu > 0)
+
+
+def test_serve_entry_points_validate_without_gpu():
+  import ctypes
+  from yasps_b200 import _lib as L
+  lib = L.load()
+  h = ctypes.c_void_p()
+  assert lib.ys_serve_create(0, 4, ctypes.byref(h)) == L.YS_ERR_INVALID
+  assert lib.ys_serve_create(8, 0, ctypes.byref(h)) == L.YS_ERR_INVALID
+  assert lib.ys_serve_attach(None, 0, None) == L.YS_ERR_INVALID
+  assert lib.ys_serve_workspace_doubles(1000) >= 15 * 1000

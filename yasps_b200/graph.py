@@ -106,6 +106,24 @@ class attribute:
         self._dev = None
     self._version += 1
 
+  def setScalar(self, v: float) -> None:
+    """Set a constant's value on the host only (no device copy; a device
+    mirror is rebuilt when ``value`` is next read)."""
+    n = getattr(self.correspondance, "numInstances", 1)
+    self._host = np.full(n * self.size, float(v))
+    self._dev = None
+    self._version += 1
+
+  def copyValueFrom(self, src, non_blocking: bool = True) -> None:
+    """Copy ``src`` (a tensor, e.g. pinned host memory) into the existing
+    device values on the current stream; the host mirror is dropped."""
+    dst = self.value
+    if src.numel() != dst.numel():
+      raise ValueError(f"attribute.copyValueFrom: expected {dst.numel()} values, got {src.numel()}")
+    dst.copy_(src.reshape(-1), non_blocking=non_blocking)
+    self._host = None
+    self._version += 1
+
   @property
   def host_value(self) -> np.ndarray:
     if self._host is None:

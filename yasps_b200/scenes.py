@@ -19,6 +19,7 @@ the tetrahedra are ordered by the Morton code of their hexahedron.
 from __future__ import annotations
 
 from dataclasses import dataclass
+from functools import lru_cache
 
 import numpy as np
 
@@ -158,6 +159,27 @@ def fem_scene(cube: "FemCube", name: str = "fem_cube", projection_method: int = 
   sc.addMinimizeTarget([free_position])
   return sc, dict(free_position=free_position, pinned_position=pinned_position, last_position=last, velocity=vel,
                   snh=snh, inertia=kin, tets=tets)
+
+
+@lru_cache(maxsize=64)
+def _vertex_order(n: int):
+  """Lexicographic grid coordinates and the pinned / free vertex orders of an
+  ``n^3`` cube (Morton order within each primitive, as in ``fem_cube``)."""
+  g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), axis=-1).reshape(-1, 3)
+  codes = morton3(g[:, 0], g[:, 1], g[:, 2])
+  pinned = g[:, 2] == 0
+  pin_ids = np.flatnonzero(pinned)[np.argsort(codes[pinned], kind="stable")]
+  free_ids = np.flatnonzero(~pinned)[np.argsort(codes[~pinned], kind="stable")]
+  return g, pin_ids, free_ids
+
+
+def fem_positions(n: int, spacing: float = 0.1, noise: float = 0.01, seed: int = 0):
+  """``(pinned_position, free_position)`` of ``fem_cube(n, spacing=spacing,
+  noise=noise, seed=seed)`` without rebuilding the mesh (same draws)."""
+  g, pin_ids, free_ids = _vertex_order(n)
+  rng = np.random.default_rng(seed)
+  pos_lex = g.astype(np.float64) * spacing + rng.uniform(-noise, noise, size=g.shape)
+  return pos_lex[pin_ids], pos_lex[free_ids]
 
 
 def fem_cube(n: int, spacing: float = 0.1, young: float = 1e5, poisson: float = 0.4, noise: float = 0.01,
