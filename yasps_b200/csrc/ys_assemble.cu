@@ -34,6 +34,32 @@ __global__ void __launch_bounds__(256) assemble_kernel(const double* __restrict_
   }
 }
 
+// Small entries (gradient segments, hw = 3 for 3-DoF vertices): 3 lanes per
+// unique entry, 10 entries per warp; a group walks elements sub, sub+3, ...
+// of its entry, each summed over the records in order (the same order as
+// assemble_kernel).
+__global__ void __launch_bounds__(256) assemble_small_kernel(const double* __restrict__ rec,
+                                                             const uint32_t* __restrict__ begin,
+                                                             const uint32_t* __restrict__ count,
+                                                             const uint32_t* __restrict__ offset,
+                                                             uint32_t offset_stride,
+                                                             const uint16_t* __restrict__ dims, uint32_t nu,
+                                                             double* __restrict__ out) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (lane >= 30) return;
+  const uint32_t u = warp * 10 + lane / 3, sub = lane % 3;
+  if (u >= nu) return;
+  const uint32_t hw = (uint32_t)dims[2ull * u] * dims[2ull * u + 1];
+  const uint32_t b = begin[u], c = count[u];
+  const uint64_t o = offset[(uint64_t)u * offset_stride];
+  for (uint32_t e = sub; e < hw; e += 3) {
+    double acc = 0.0;
+    for (uint32_t k = 0; k < c; ++k) acc += rec[(uint64_t)b + (uint64_t)k * hw + e];
+    out[o + e] = acc;
+  }
+}
+
 // 3x3 fast path: 9 lanes per unique block (3 blocks per warp, 5 lanes idle).
 __global__ void __launch_bounds__(256) assemble3_kernel(const double* __restrict__ rec,
                                                         const uint32_t* __restrict__ begin,
@@ -138,9 +164,9 @@ int32_t ys_assemble_strided(const double* records, const uint32_t* begin, const 
                             const uint32_t* offset, uint32_t offset_stride, const uint16_t* dims, uint32_t nu,
                             double* out, void* stream) {
   if (nu == 0) return YS_OK;
-  const uint64_t threads = (uint64_t)nu * 32;
-  ys::assemble_kernel<float><<<ys::grid_for(threads, 256), 256, 0, (cudaStream_t)stream>>>(
-      records, begin, count, offset, offset_stride, dims, nu, out, nullptr);
+  const uint64_t threads = ((uint64_t)nu + 9) / 10 * 32;
+  ys::assemble_small_kernel<<<ys::grid_for(threads, 256), 256, 0, (cudaStream_t)stream>>>(
+      records, begin, count, offset, offset_stride, dims, nu, out);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

@@ -29,23 +29,41 @@ namespace ys {
 
 constexpr int kInvThreads = 256;
 
-// One thread per (coarse block, element); sources summed in their stored order.
-// mode 0: B, 1: B^T, 2: B + B^T.
-__global__ void mas_level_blocks(MasDev M, uint32_t begin, uint32_t end) {
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t cb = begin + t / 9;
-  if (cb >= end) return;
-  const int e = (int)(t % 9), k = e / 3, l = e % 3;
-  double acc = 0.0;
-  for (uint32_t s = M.cb_src_ptr[cb]; s < M.cb_src_ptr[cb + 1]; ++s) {
+// One warp per coarse block: lane l sums sources l, l+32, ... (mode 0: B,
+// 1: B^T, 2: B + B^T), then a fixed xor-shuffle tree combines the lanes, so
+// the sum order is fixed (deterministic) and long source lists (the coarse
+// levels) are summed 32-wide instead of serially.
+__global__ void __launch_bounds__(256) mas_level_blocks(MasDev M, uint32_t begin, uint32_t end) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t cb = begin + warp;
+  if (cb >= end) return;  // warp-uniform
+  double acc[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+  for (uint32_t s = M.cb_src_ptr[cb] + lane; s < M.cb_src_ptr[cb + 1]; s += 32) {
     const uint32_t src = M.cb_src[s];
     const uint32_t mode = src >> 30, idx = src & 0x3fffffffu;
     const double* b = level_block(M, idx);
-    if (mode == 0) acc += b[3 * k + l];
-    else if (mode == 1) acc += b[3 * l + k];
-    else acc += b[3 * k + l] + b[3 * l + k];
+    double v[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) v[e] = b[e];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        const double d = v[3 * k + l], t = v[3 * l + k];
+        acc[3 * k + l] += mode == 0 ? d : (mode == 1 ? t : d + t);
+      }
   }
-  M.coarse_values[9 * cb + e] = acc;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], o);
+  if (lane == 0) {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) M.coarse_values[9ull * cb + e] = acc[e];
+  }
 }
 
 // Dense assembly + in-place Gauss-Jordan inverse of one domain per CTA.
@@ -53,10 +71,10 @@ __global__ void mas_level_blocks(MasDev M, uint32_t begin, uint32_t end) {
 template <int T>
 __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_inverse(MasDev M) {
   extern __shared__ double A[];  // n*n
-  __shared__ double colk[128];
-  __shared__ double rowk[128];
+  __shared__ double colk[2][128];
+  __shared__ double rowk[2][128];
   __shared__ double dinv[128];
-  __shared__ double piv_sh[1];
+  __shared__ double piv_sh[2];
   __shared__ int bad;
   const uint32_t d = blockIdx.x;
   const uint32_t n = 3 * (M.dom_node_ptr[d + 1] - M.dom_node_ptr[d]);
@@ -102,8 +120,10 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
       const uint32_t i = ty + 16 * a, j = tx + 16 * b;
       R[a][b] = (i < n && j < n) ? A[i * n + j] * dinv[i] * dinv[j] : 0.0;
     }
-  for (uint32_t k = 0; k < n; ++k) {
-    const int kb = (int)(k >> 4), kr = (int)(k & 15);
+  // Pivot column / row of step k are published in buffer k & 1 by their
+  // owners right after step k-1's update, so each step needs one barrier.
+  auto publish = [&](uint32_t k) {
+    const int kb = (int)(k >> 4), kr = (int)(k & 15), buf = (int)(k & 1);
     if (tx == kr) {
 #pragma unroll
       for (int a = 0; a < T; ++a) {
@@ -111,8 +131,8 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
 #pragma unroll
         for (int b = 0; b < T; ++b) v = (b == kb) ? R[a][b] : v;
         const bool diag = (ty + 16 * a) == (int)k;
-        if (diag) piv_sh[0] = v;
-        colk[ty + 16 * a] = diag ? v - 1.0 : v;
+        if (diag) piv_sh[buf] = v;
+        colk[buf][ty + 16 * a] = diag ? v - 1.0 : v;
       }
     }
     if (ty == kr) {
@@ -121,22 +141,27 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
         double v = 0.0;
 #pragma unroll
         for (int a = 0; a < T; ++a) v = (a == kb) ? R[a][b] : v;
-        rowk[tx + 16 * b] = ((tx + 16 * b) == (int)k) ? v + 1.0 : v;
+        rowk[buf][tx + 16 * b] = ((tx + 16 * b) == (int)k) ? v + 1.0 : v;
       }
     }
-    __syncthreads();
-    const double piv = piv_sh[0];
+  };
+  publish(0);
+  __syncthreads();
+  for (uint32_t k = 0; k < n; ++k) {
+    const int buf = (int)(k & 1);
+    const double piv = piv_sh[buf];
     if (!(piv > tol) && threadIdx.x == 0) bad = 1;
     const double ip = 1.0 / piv;
     double rj[T];
 #pragma unroll
-    for (int b = 0; b < T; ++b) rj[b] = rowk[tx + 16 * b];
+    for (int b = 0; b < T; ++b) rj[b] = rowk[buf][tx + 16 * b];
 #pragma unroll
     for (int a = 0; a < T; ++a) {
-      const double cip = colk[ty + 16 * a] * ip;
+      const double cip = colk[buf][ty + 16 * a] * ip;
 #pragma unroll
       for (int b = 0; b < T; ++b) R[a][b] = fma(-cip, rj[b], R[a][b]);
     }
+    if (k + 1 < n) publish(k + 1);
     __syncthreads();
   }
 #pragma unroll
@@ -516,7 +541,7 @@ int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* str
   for (uint32_t l = 1; l < M.levels; ++l) {
     const uint32_t b = M.cb_level_begin[l], e = M.cb_level_begin[l + 1];
     if (e > b) {
-      ys::mas_level_blocks<<<ys::grid_for(9ull * (e - b), 256), 256, 0, s>>>(M, b, e);
+      ys::mas_level_blocks<<<ys::grid_for(32ull * (e - b), 256), 256, 0, s>>>(M, b, e);
       YS_CHECK_LAUNCH();
     }
   }

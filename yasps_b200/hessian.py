@@ -252,6 +252,7 @@ class hessian:
     self._requests_dynamic = list(requests_dynamic)
     self._setup = False
     self.want_fp32 = False
+    self.want_diagonal = True  # diagonal / diagonal_blocks (block-Jacobi); MAS-only callers may skip them
     self.values32_current = False
     self.gradient: Optional[vector] = None
     self.diagonal = None
@@ -387,6 +388,13 @@ class hessian:
     if gp.num_unique:
       L.call("ys_assemble_strided", L.ptr(self._grad_records), L.ptr(gp.record_begin), L.ptr(gp.record_count),
              L.ptr(gp.positions), 2, L.ptr(gp.dims), gp.num_unique, L.ptr(self.gradient.value), s)
+    if self.want_diagonal:
+      self._extract_diagonal()
+    self.values32_current = self.want_fp32
+    return self
+
+  def _extract_diagonal(self):
+    s = L.stream_ptr()
     self.diagonal.zero_()
     self.diagonal_blocks.zero_()
     nat = len(self.__wrt)
@@ -400,8 +408,6 @@ class hessian:
         continue
       L.call("ys_extract_diagonal", L.ptr(bs.values), L.ptr(p.positions), L.ptr(p.dims), L.ptr(p.value_offset),
              p.num_unique, nat, seg, asz, dst, L.ptr(self.diagonal_blocks), L.ptr(self.diagonal), 1, s)
-    self.values32_current = self.want_fp32
-    return self
 
   def _assemble(self, bs: _BlockSet):
     torch = _torch()

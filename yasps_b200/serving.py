@@ -91,6 +91,7 @@ class FemTopology:
     self.scene.minimizer.setSolver("mas", **opts)
     self.mas_solver = self.scene.minimizer.linearSolver.implementation
     H = self.scene.minimizer.computeNumericValue()
+    H.want_diagonal = False  # the MAS path reads no diagonal blocks
     self.mas_solver._ensure_hierarchy(H)
     self.H = H
     self.tables = self.mas_solver._tables
@@ -209,6 +210,7 @@ class NewtonServer:
     self._active = {}                             # id -> (req, slot)
     self.launches = 0
     self.passes_run = 0
+    self.host_seconds = collections.Counter()    # admit / attach / launch / wait (host time per phase)
 
   # -- resources ------------------------------------------------------------------
   def topology(self, side: int) -> FemTopology:
@@ -273,8 +275,10 @@ class NewtonServer:
       if slot is None:
         break
       req = queue.popleft()
+      t = time.perf_counter()
       with torch.cuda.stream(self.admit_stream):
         slot.admit(req)
+      self.host_seconds["admit"] += time.perf_counter() - t
       req.t_admit = now
       self._pending.append((req, slot, self._free_ids.pop()))
 
@@ -292,7 +296,9 @@ class NewtonServer:
 
   def _retire(self, clock, t0) -> List[NewtonRequest]:
     torch = _torch()
+    t = time.perf_counter()
     L.call("ys_serve_status", self.handle, self.solve_stream.cuda_stream, self._status)
+    self.host_seconds["wait"] += time.perf_counter() - t
     done = [sid for sid in self._active
             if self._status[sid].phase in (L.YS_SERVE_DONE, L.YS_SERVE_FAILED)]
     if not done:
@@ -332,7 +338,9 @@ class NewtonServer:
         i += 1
       self._attach_ready()
       if self._active:
+        t = time.perf_counter()
         L.call("ys_serve_launch", self.handle, self.solve_stream.cuda_stream)
+        self.host_seconds["launch"] += time.perf_counter() - t
         self.launches += 1
         self.passes_run += self.passes
         # admission work of new arrivals overlaps the launch in flight
@@ -345,7 +353,9 @@ class NewtonServer:
         continue
       self._admit_arrivals(queue, now)
       if self._pending:
+        t = time.perf_counter()
         self._pending[0][1].ready.synchronize()
+        self.host_seconds["wait_admission"] += time.perf_counter() - t
       elif queue:
         raise RuntimeError(f"a side-{queue[0].side} request does not fit the memory budget")
       elif i < total:
