@@ -295,8 +295,8 @@ __device__ __forceinline__ bool chol3(double w00, double w01, double w02, double
   return true;
 }
 
-__device__ __forceinline__ void snh_project_one(const ys_snh_args& a, uint32_t t, double* __restrict__ vsh,
-                                                int vstride) {
+__device__ __forceinline__ void snh_project_one(const ys_snh_args& a, uint32_t t, double* __restrict__ stash,
+                                                int stride) {
   SnhState st;
   snh_state(a, t, st);
   uint32_t code[4];
@@ -332,7 +332,19 @@ __device__ __forceinline__ void snh_project_one(const ys_snh_args& a, uint32_t t
     lu[p] = mul(st.f, lc[p]);
     lv[p] = mul(st.cof, lc[p]);
   }
-  // K (9x9, packed upper triangle in registers), eigenvectors in shared memory.
+  // Q = G L^-T: Q[a][p] = sum_j G[a][j] (L^-1)[p][j]; solve L y = G_a per vertex.
+  constexpr int QS = project_stash_doubles<9>();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double g0 = st.g[k].x, g1 = st.g[k].y, g2 = st.g[k].z;
+    const double y0 = g0 / l[0][0];
+    const double y1 = (g1 - l[1][0] * y0) / l[1][1];
+    const double y2 = (g2 - l[2][0] * y0 - l[2][1] * y1) / l[2][2];
+    stash[(QS + 3 * k) * stride] = y0;
+    stash[(QS + 3 * k + 1) * stride] = y1;
+    stash[(QS + 3 * k + 2) * stride] = y2;
+  }
+  // K (9x9, packed upper triangle in registers), projected in place.
   double kmat[45];
 #pragma unroll
   for (int p = 0; p < 3; ++p)
@@ -346,18 +358,12 @@ __device__ __forceinline__ void snh_project_one(const ys_snh_args& a, uint32_t t
         for (int m = 0; m < 3; ++m)
           if (3 * p + k <= 3 * q + m) kmat[utri<9>(3 * p + k, 3 * q + m)] = blk[k][m];
     }
-  jacobi_eigen_reg<9>(kmat, vsh, vstride);
-  jacobi_reconstruct_reg<9>(kmat, vsh, vstride, a.projection_method);
-  // Q = G L^-T: Q[a][p] = sum_j G[a][j] (L^-1)[p][j]; solve L y = G_a per vertex.
+  project_negative_modes<9>(kmat, a.projection_method, stash, stride);
   double qm[4][3];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const double g0 = st.g[k].x, g1 = st.g[k].y, g2 = st.g[k].z;
-    const double y0 = g0 / l[0][0];
-    const double y1 = (g1 - l[1][0] * y0) / l[1][1];
-    const double y2 = (g2 - l[2][0] * y0 - l[2][1] * y1) / l[2][2];
-    qm[k][0] = y0; qm[k][1] = y1; qm[k][2] = y2;
-  }
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int p = 0; p < 3; ++p) qm[k][p] = stash[(QS + 3 * k + p) * stride];
   auto block = [&](int ai, int bi, double (&blk)[3][3]) {
 #pragma unroll
     for (int k = 0; k < 3; ++k)
@@ -376,12 +382,16 @@ __device__ __forceinline__ void snh_project_one(const ys_snh_args& a, uint32_t t
 
 constexpr int kProjThreads = 64;
 
+// Per-thread shared-memory stash of the projection (original K, reflectors,
+// Q), thread-interleaved.
+constexpr int kProjStash = project_stash_doubles<9>() + 12;
+
 __global__ void __launch_bounds__(kProjThreads) snh_project_kernel(const ys_snh_args a) {
-  extern __shared__ double vshared[];  // 81 doubles per thread, thread-interleaved
-  double* vsh = vshared + threadIdx.x;
+  extern __shared__ double proj_stash[];
+  double* stash = proj_stash + threadIdx.x;
   const uint32_t count = *a.work_count;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-    snh_project_one(a, a.work_list[i], vsh, blockDim.x);
+    snh_project_one(a, a.work_list[i], stash, blockDim.x);
 }
 
 __global__ void inertia_kernel(const ys_inertia_args a) {
@@ -433,7 +443,8 @@ int32_t ys_snh_eval(const ys_snh_args* args, void* stream) {
     // The work count stays on the device: a grid-stride launch sized to the
     // SMs covers any count without a host round trip.
     const unsigned pgrid = std::min<unsigned>(ys::grid_for(a.num_elements, ys::kProjThreads), ys::kSMs * 16);
-    const size_t smem = sizeof(double) * 81 * ys::kProjThreads;
+    const size_t smem = sizeof(double) * ys::kProjStash * ys::kProjThreads;  // above the 48 KB default
+    YS_CUDA_TRY(cudaFuncSetAttribute(ys::snh_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ys::snh_project_kernel<<<pgrid, ys::kProjThreads, smem, s>>>(a);
     YS_CHECK_LAUNCH();
   }
