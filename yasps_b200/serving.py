@@ -181,12 +181,13 @@ class NewtonServer:
 
   ``max_slots`` solves are in flight at most; ``memory_budget`` bounds the
   bytes of the pooled per-request buffers (admission by HBM footprint);
-  ``passes`` PCG passes run per launch between two host checks.
+  ``passes`` PCG passes run per launch between two host checks;
+  ``admission_streams`` streams carry the admission work of different sides.
   """
 
   def __init__(self, max_slots: int = 64, passes: int = 8, memory_budget: float = 40e9, tolerance: float = 1e-6,
                refinement_tolerance: float = 1e-3, max_iterations: int = 2000, spacing: float = 0.1,
-               solver_options: Optional[dict] = None):
+               solver_options: Optional[dict] = None, admission_streams: int = 4):
     torch = _torch()
     self.max_slots = int(max_slots)
     self.passes = int(passes)
@@ -200,7 +201,9 @@ class NewtonServer:
     L.call("ys_serve_create", self.max_slots, self.passes, ctypes.byref(h))
     self.handle = h
     self._status = (L.ServeSlotStatus * self.max_slots)()
-    self.admit_stream = torch.cuda.Stream()
+    # admission work of different sides overlaps on several streams; one side
+    # always uses the same stream (its requests share the template buffers)
+    self.admit_streams = [torch.cuda.Stream() for _ in range(int(admission_streams))]
     self.solve_stream = torch.cuda.Stream()
     self.topologies: Dict[int, FemTopology] = {}
     self._idle = collections.defaultdict(list)   # side -> idle slots
@@ -276,7 +279,7 @@ class NewtonServer:
         break
       req = queue.popleft()
       t = time.perf_counter()
-      with torch.cuda.stream(self.admit_stream):
+      with torch.cuda.stream(self.admit_streams[req.side % len(self.admit_streams)]):
         slot.admit(req)
       self.host_seconds["admit"] += time.perf_counter() - t
       req.t_admit = now
