@@ -13,6 +13,9 @@ The plain FP64 path (FP64 SpMV) is timed beside it (``fp64``).
 ``value``: whole-job solves/s with the scene resident on the device.
 ``e2e``: the same through ``scene.minimizeEnergy`` with host positions copied
 in and the solution copied out every step.
+``serving``: the serving form on a seeded stream of 512 FEM Newton steps
+(Poisson arrivals, sides 8..48): continuous batching in the precision form
+beside the serial plain FP64 path, solves/s and p50/p99 latency (rank 0, N=1).
 ``--impl reference``: the CPU restatement of the reference path (oracle) on
 a bounded sample of the same workload (rank 0 only).
 
@@ -48,6 +51,8 @@ def parse():
   p.add_argument("--side", type=int, default=64, help="cube side in vertices")
   p.add_argument("--no-cpu-baseline", action="store_true")
   p.add_argument("--tol", type=float, default=1e-6)
+  p.add_argument("--serving-requests", type=int, default=512,
+                 help="requests of the serving stream (0: skip the serving leg)")
   return p.parse_args()
 
 
@@ -199,12 +204,9 @@ def gpu_arm(args):
   rel_res = float(getattr(impl, "final_relative_residual", float("nan")))
   value = world * args.steps / (ms / 1e3)
   lat_ms = sorted(1e3 * x for x in lat)
-  # kernels of this library launched per step: SNH eval + projection, inertia, block + gradient assembly,
-  # diagonal extraction (6); MAS numeric update (levels - 1 Galerkin sums + 1 inverse); refinement residual
-  # (1 + 2 per refinement); per PCG solve an init of (3 + levels) and (5 + levels) per iteration.
   levels = len(impl.hierarchy.levels)
   its, refs = int(stats["iterations"]), int(stats.get("refinements", 1))
-  launches_per_step = 6 + levels + 1 + 2 * refs + refs * (3 + levels) + its * (5 + levels)
+  launches_per_step = launches_per_newton_step(impl, its, refs)
   # plain FP64 path on the same scene
   solver64 = mz.setSolver("mas", mixed_spmv=False, stop_rule="residual")
   for _ in range(2):
@@ -251,6 +253,9 @@ def gpu_arm(args):
   cpu = None
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     cpu = cpu_baseline_leg(cube, args.tol)
+  serve = None
+  if rank == 0 and world == 1 and args.serving_requests > 0:
+    serve = serving_leg(args)
   line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
           "vs_baseline": None, "dtype": "f32+f64 refine (f64 element Hessians and projection)",
@@ -263,11 +268,67 @@ def gpu_arm(args):
           "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * cube.dofs,
                   "d2h_bytes_per_step": 8 * cube.dofs},
           "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline, "clocks": clk,
-          "cpu_baseline": cpu}
+          "cpu_baseline": cpu, "serving": serve}
   if rank == 0:
     print(json.dumps(line), flush=True)
   if pg is not None:
     pg.destroy_process_group()
+
+
+def launches_per_newton_step(impl, its, refs):
+  """Kernels of this library launched in one Newton step of the precision form.
+
+  Element stage: SNH eval + projection, inertia, block and gradient assembly,
+  diagonal extraction (6).  MAS numeric update: one Galerkin sum per coarse
+  level and the domain inverses.  Refinement: the initial residual (1) and per
+  refinement x += d and r = g - H x (2).  Each PCG solve: init = residual, the
+  grid restrictions of the large levels, the one-CTA tail, GEMV, collect;
+  every iteration = SpMV+dot, update, large-level restrictions, tail, GEMV,
+  collect, direction.
+  """
+  t = impl._tables
+  offs = [int(v) for v in t.level_node_offset]
+  levels = len(offs) - 1
+  first = levels
+  while first > 1 and offs[first] - offs[first - 1] <= 4096:
+    first -= 1
+  tail = 1 if first < levels else 0
+  init = 1 + (first - 1) + tail + 2
+  per_it = 2 + (first - 1) + tail + 3
+  return 6 + (levels - 1) + 1 + 1 + 2 * refs + refs * init + its * per_it
+
+
+def serving_leg(args):
+  """Serving form on a seeded Poisson stream of FEM Newton steps (one GPU):
+  continuous batching (FP32+refine) beside the serial plain FP64 path."""
+  import torch
+  from yasps_b200 import serving
+  n = args.serving_requests
+  srv = serving.NewtonServer(max_slots=64, passes=8, memory_budget=40e9, tolerance=args.tol)
+  t0 = time.perf_counter()
+  srv.register(range(8, 49))
+  t_register = time.perf_counter() - t0
+  srv.run(serving.poisson_fem_stream(count=82, mean_spacing=0.0, seed=99))
+  srv.solve_serial_fp64(serving.poisson_fem_stream(count=41, mean_spacing=0.0, seed=98))
+  out = {"workload": (f"{n} FEM Newton-step requests, Poisson arrivals (mean gap 2 ms), cube side U{{8..48}}, "
+                      "E log-uniform [1e4, 1e6], nu U[0.3, 0.45], noise +-0.01, 40 GB admission budget, "
+                      "solve to 1e-6 true relative residual"),
+         "register_topologies_s": t_register}
+  clocks = Clocks(torch.cuda.current_device())
+  clocks.start()
+  done = srv.run(serving.poisson_fem_stream(count=n, mean_spacing=2e-3, seed=0))
+  out["served"] = serving.stream_stats(done)
+  out["served"]["max_rel_residual"] = max(r.relative_residual for r in done)
+  out["served_saturated"] = serving.stream_stats(
+      srv.run(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=0)))
+  out["serial_fp64"] = serving.stream_stats(
+      srv.solve_serial_fp64(serving.poisson_fem_stream(count=n, mean_spacing=2e-3, seed=0)))
+  out["serial_fp64_saturated"] = serving.stream_stats(
+      srv.solve_serial_fp64(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=0)))
+  out["clocks"] = clocks.stop()
+  out["resident_gb"] = srv.resident_bytes / 1e9
+  srv.close()
+  return out
 
 
 def cpu_baseline_leg(cube, tol):
