@@ -191,6 +191,54 @@ typedef struct ys_inertia_args {
  * (examples/dropping_in_container_mixed/helpers.py:138-141).               */
 int32_t ys_inertia_eval(const ys_inertia_args* args, void* stream);
 
+/* ---- vertex-tuple energies (cloth, contact, friction) --------------------
+ * Energies over a JOIN of `arity` 3-DoF vertices (examples/
+ * dropping_in_container_mixed/helpers.py, friction_helpers.py): gradient and
+ * Hessian by second-order forward-mode differentiation of the formula, the
+ * local Hessian projected like SNH (LDL^T PSD test, then |lambda| or
+ * max(lambda, 0) of the negative modes), merged and scattered into records.
+ * values[] by kind:
+ *   barriers (PP/PE/PT/EE, helpers.py:143-199): dHat, kappa; d is the
+ *     squared distance, E = kappa (d - dHat)^2 log^2(d / dHat);
+ *   BENDING (helpers.py:213-234): bendStiff, dt; rest = x_init;
+ *   BARAFF_WITKIN (helpers.py:272-292): stretchS, shearS, thickness, dt;
+ *     rest = x_init;
+ *   STVK_MEMBRANE: mu, lam, thickness, dt; rest = x_init, the Baraff-Witkin
+ *     rest frame (no counterpart in the reference);
+ *   FRICTION_PT (friction_helpers.py:12-66, :73-182): fDhat, dt,
+ *     frictionRate; rest = positions at the start of the step; params per
+ *     element (stride >= 9): beta1, beta2, tangent0[3], tangent1[3],
+ *     lambda_last_h.                                                       */
+#define YS_ENERGY_POINT_POINT 1
+#define YS_ENERGY_POINT_EDGE 2
+#define YS_ENERGY_POINT_TRIANGLE 3
+#define YS_ENERGY_EDGE_EDGE 4
+#define YS_ENERGY_BENDING 5
+#define YS_ENERGY_BARAFF_WITKIN 6
+#define YS_ENERGY_STVK_MEMBRANE 7
+#define YS_ENERGY_FRICTION_PT 8
+
+typedef struct ys_energy_args {
+  int32_t kind;                 /* YS_ENERGY_*                                      */
+  ys_union3 position;           /* current positions (DATA)                         */
+  ys_union3 rest;               /* rest / initial / previous positions by kind      */
+  const uint32_t* conn;         /* [n x arity] union indices                        */
+  uint32_t arity;               /* 2 (PP), 3 (PE, membranes), 4 (PT, EE, bending, friction) */
+  uint32_t num_elements;
+  const double* params;         /* [n x param_stride] per-element parameters or NULL */
+  uint32_t param_stride;
+  double values[8];             /* scalar parameters by kind (above)                */
+  int32_t projection_method;    /* -1/0 none, 1 |lambda|, 2 max(lambda, 0)          */
+  ys_term_plan plan;
+  double* block_records;
+  double* grad_records;
+  double* energy;               /* [n] or NULL                                      */
+} ys_energy_args;
+
+/* Replaces the generated `compute_hessian_and_gradient_with_compression` of
+ * these energies (hessianKernelHost.pyx:27-161).                           */
+int32_t ys_energy_eval(const ys_energy_args* args, void* stream);
+
 /* ---- deterministic assembly --------------------------------------------- */
 
 /* out[offset[u] + e] = sum_{c < count[u]} records[begin[u] + c*hw_u + e] for

@@ -15,6 +15,9 @@ It executes the reference's own Python code and stores its outputs:
 * ``snh_sympy_six_tets.npz`` -- the reference's SymPy check script
   (``tests/energy/check_stable_neo_hookean.py``) run as-is; its assembled
   24x24 Hessian, gradient and energy over the six-tet cube fixture.
+* ``cloth_torch.npz`` -- bending and Baraff-Witkin energies and gradients
+  from the reference's float64 PyTorch scripts (``bending.py``,
+  ``baraff_witkin.py`` in the same folder), see :func:`torch_cloth`.
 * ``mas_cpu_reference.npz`` -- the reference's NumPy MAS solver
   (``yasps/yasps/solver/mas``) on a small SNH + inertia system, with pymetis
   replaced by the chunk-ordering shim documented in ``oracle/mas.py`` (the
@@ -67,6 +70,50 @@ def torch_single_tet(ref):
   np.savez(os.path.join(HERE, "snh_torch_single_tet.npz"), rest=env["rest_position_np"],
            current=env["current_position_np"], mu=2000.0, lam=1000.0, energy=e.item(), grad=g.numpy(),
            hess=h.numpy(), ib=ib[0].numpy(), vol=vol[0].item())
+
+
+def _extract(path, names, assigns=()):
+  tree = ast.parse(open(path).read())
+  keep = [n for n in tree.body if isinstance(n, (ast.Import, ast.ImportFrom)) or
+          (isinstance(n, ast.FunctionDef) and n.name in names) or
+          (isinstance(n, ast.Assign) and any(isinstance(t, ast.Name) and t.id in assigns for t in n.targets))]
+  env = {}
+  exec(compile(ast.Module(body=keep, type_ignores=[]), path, "exec"), env)
+  return env
+
+
+def torch_cloth(ref):
+  """Bending and Baraff-Witkin from the reference's float64 PyTorch scripts
+  (functions extracted from their syntax trees) on the scripts' own base
+  element scaled by 1.54 plus seeded noise (stretched, so every stretch
+  coefficient of the helper formula is 1).  The scripts add 1e-8 guards
+  (axis norm, normal norm, 1 + cos), so they pin the formulas to ~1e-7."""
+  import torch
+  torch.set_default_dtype(torch.float64)
+  base = os.path.join(ref, "examples/backup/pytorch_energy_hessian_and_gradient")
+  gen = torch.Generator().manual_seed(7)
+  out = {}
+  env = _extract(os.path.join(base, "bending.py"), ("angle", "edgeTheta_from_x", "bending_energy_precomp"))
+  pos = np.array([[0, 0, 1], [1, 0, 2], [0, 0, 0], [0, 2, 0]], dtype=np.float64)
+  pos -= pos.mean(axis=0)
+  rest = torch.tensor(pos)[None].expand(6, -1, -1).contiguous()
+  x = (rest * 1.54 + 1e-2 * torch.randn((6, 4, 3), generator=gen)).requires_grad_(True)
+  t0 = env["edgeTheta_from_x"](rest).detach()
+  len0 = torch.norm(rest[:, 1, :] - rest[:, 0, :], dim=1)
+  e = env["bending_energy_precomp"](x, t0, len0, torch.tensor(1000.0))
+  (g,) = torch.autograd.grad(e.sum(), x)
+  out.update(bend_rest=rest.numpy(), bend_x=x.detach().numpy(), bend_energy=e.detach().numpy(),
+             bend_grad=g.numpy(), bend_stiff=1000.0)
+  env = _extract(os.path.join(base, "baraff_witkin.py"), ("compute_rest_shape", "baraff_witkin_energy"))
+  pos = np.array([[0, 0, 1], [1, 0, 2], [0, 0, 0]], dtype=np.float64)
+  pos -= pos.mean(axis=0)
+  rest = torch.tensor(pos)[None].expand(6, -1, -1).contiguous()
+  x = (rest * 1.54 + 1e-2 * torch.randn((6, 3, 3), generator=gen)).requires_grad_(True)
+  e = env["baraff_witkin_energy"](rest, x, torch.tensor(2000.0), torch.tensor(1000.0), 0.01, 1.0)
+  (g,) = torch.autograd.grad(e.sum(), x)
+  out.update(bw_rest=rest.numpy(), bw_x=x.detach().numpy(), bw_energy=e.detach().numpy(), bw_grad=g.numpy(),
+             bw_params=np.array([2000.0, 1000.0, 0.01, 1.0]))
+  np.savez(os.path.join(HERE, "cloth_torch.npz"), **out)
 
 
 def sympy_six_tets(ref):
@@ -150,10 +197,12 @@ if __name__ == "__main__":
   ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YASPS_REFERENCE", "")
   if not ref or not os.path.isdir(ref):
     raise SystemExit("usage: make_golden.py <reference checkout>")
-  which = sys.argv[2:] or ["torch", "mas", "sympy"]
+  which = sys.argv[2:] or ["torch", "mas", "sympy", "cloth"]
   if "torch" in which:
     torch_single_tet(ref)
   if "mas" in which:
     mas_reference(ref)
   if "sympy" in which:
     sympy_six_tets(ref)
+  if "cloth" in which:
+    torch_cloth(ref)

@@ -1,0 +1,71 @@
+"""Oracle vertex-tuple energies: pinned to the reference's float64 PyTorch
+scripts (bending, Baraff-Witkin) and checked for derivative consistency.
+
+The reference scripts guard norms with +1e-8 terms, which move these
+values by up to ~5e-7 relative, so the pin tolerance is 2e-6 relative; the barriers, StVK and friction have no runnable reference
+(parity unpinned), their Hessians are checked against finite differences of
+the autograd gradients.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import vertex_energies as ve
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def cloth():
+  return np.load(os.path.join(HERE, "cloth_torch.npz"))
+
+
+def test_bending_matches_reference_torch(cloth):
+  e, g, _ = ve.energy_grad_hess(5, cloth["bend_x"], cloth["bend_rest"], (float(cloth["bend_stiff"]), 1.0))
+  assert np.allclose(e, cloth["bend_energy"], rtol=2e-6, atol=0)
+  ref = cloth["bend_grad"].reshape(len(e), -1)
+  assert np.abs(g - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+def test_baraff_witkin_matches_reference_torch(cloth):
+  e, g, _ = ve.energy_grad_hess(6, cloth["bw_x"], cloth["bw_rest"], tuple(cloth["bw_params"]))
+  assert np.allclose(e, cloth["bw_energy"], rtol=2e-6, atol=0)
+  ref = cloth["bw_grad"].reshape(len(e), -1)
+  assert np.abs(g - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+def _elements(kind, rng):
+  arity = {1: 2, 2: 3, 3: 4, 4: 4, 5: 4, 6: 3, 7: 3, 8: 4}[kind]
+  base = np.array([[0.0, 0.0, 0.0], [0.1, 0.0, 0.01], [0.02, 0.0, 0.1], [0.05, 0.03, 0.04]])[:arity]
+  rest = base[None] + rng.uniform(-1e-3, 1e-3, size=(3, arity, 3))
+  x = rest * 1.1 + rng.uniform(-2e-3, 2e-3, size=rest.shape)
+  if kind in (1, 2, 3, 4):
+    x[:, 0] += np.array([0.0, 0.02, 0.0])  # keep the pair apart
+  return x, rest
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_hessian_is_the_derivative_of_the_gradient(kind):
+  rng = np.random.default_rng(kind)
+  x, rest = _elements(kind, rng)
+  params = {1: (1e-3, 1e3), 2: (1e-3, 1e3), 3: (1e-3, 1e3), 4: (1e-3, 1e3), 5: (1e-3, 0.01),
+            6: (2000.0, 1000.0, 1e-3, 0.01), 7: (5e3, 2e3, 1e-3, 0.01), 8: (1e-6, 0.01, 0.3)}[kind]
+  lagged = None
+  if kind == 8:
+    lagged = np.stack([ve.lagged_friction_pt(x[t] + 1e-4, 1e-3, 1e3) for t in range(len(x))])
+    rest = x - rng.uniform(-1e-3, 1e-3, size=x.shape)  # previous positions: a sliding step
+  _, g, h = ve.energy_grad_hess(kind, x, rest, params, lagged)
+  step = 1e-7
+  for t in range(len(x)):
+    for i in range(x.shape[1] * 3):
+      xp, xm = x.copy(), x.copy()
+      xp[t].reshape(-1)[i] += step
+      xm[t].reshape(-1)[i] -= step
+      _, gp, _ = ve.energy_grad_hess(kind, xp[t:t + 1], rest[t:t + 1], params,
+                                     None if lagged is None else lagged[t:t + 1])
+      _, gm, _ = ve.energy_grad_hess(kind, xm[t:t + 1], rest[t:t + 1], params,
+                                     None if lagged is None else lagged[t:t + 1])
+      fd = (gp[0] - gm[0]) / (2 * step)
+      assert np.abs(fd - h[t, i]).max() <= 1e-5 * max(np.abs(h[t]).max(), 1e-300)

@@ -27,6 +27,8 @@ YS_PREC_MAS = 1
 YS_STOP_PRECONDITIONED = 0
 YS_STOP_RESIDUAL = 1
 YS_MAX_UNION = 8
+(YS_ENERGY_POINT_POINT, YS_ENERGY_POINT_EDGE, YS_ENERGY_POINT_TRIANGLE, YS_ENERGY_EDGE_EDGE, YS_ENERGY_BENDING,
+ YS_ENERGY_BARAFF_WITKIN, YS_ENERGY_STVK_MEMBRANE, YS_ENERGY_FRICTION_PT) = range(1, 9)
 YS_SERVE_EMPTY, YS_SERVE_INIT, YS_SERVE_REFINE, YS_SERVE_START, YS_SERVE_ITER, YS_SERVE_DONE, YS_SERVE_FAILED = range(7)
 
 
@@ -55,6 +57,13 @@ class SnhArgs(C.Structure):
 class InertiaArgs(C.Structure):
   _fields_ = [("position", vp), ("x_before", vp), ("velocity", vp), ("mass", vp), ("dt", f64), ("gravity", f64 * 3),
               ("num_vertices", u32), ("plan", TermPlan), ("block_records", vp), ("grad_records", vp),
+              ("energy", vp)]
+
+
+class EnergyArgs(C.Structure):
+  _fields_ = [("kind", i32), ("position", Union3), ("rest", Union3), ("conn", vp), ("arity", u32),
+              ("num_elements", u32), ("params", vp), ("param_stride", u32), ("values", f64 * 8),
+              ("projection_method", i32), ("plan", TermPlan), ("block_records", vp), ("grad_records", vp),
               ("energy", vp)]
 
 
@@ -104,6 +113,7 @@ SIGNATURES = {
     "ys_pattern_build": (i32, [vp, vp, u32, vp, u64, P(PatternOut), vp]),
     "ys_snh_eval": (i32, [P(SnhArgs), vp]),
     "ys_inertia_eval": (i32, [P(InertiaArgs), vp]),
+    "ys_energy_eval": (i32, [P(EnergyArgs), vp]),
     "ys_assemble": (i32, [vp, vp, vp, vp, vp, u32, vp, vp, vp]),
     "ys_assemble3": (i32, [vp, vp, vp, vp, u32, vp, vp, vp]),
     "ys_assemble_strided": (i32, [vp, vp, vp, vp, u32, vp, u32, vp, vp]),

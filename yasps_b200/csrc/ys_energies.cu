@@ -1,0 +1,390 @@
+// Vertex-tuple energies of the mixed (cloth + contact) scenes.
+//
+// Energy formulas follow the reference example helpers
+// (examples/dropping_in_container_mixed/helpers.py):
+//   point_point / point_edge / point_triangle / edge_edge (:143-199): IPC
+//     log-barrier kappa (d - dHat)^2 log^2(d / dHat) on the SQUARED
+//     distance d of the pair type;
+//   bending (:213-234): kb (theta - theta0)^2 |x1_0 - x0_0| dt^2, theta the
+//     dihedral angle 2 atan2(((n0 x n1).axis)/|axis|, n0.n1 + |n0||n1|);
+//   baraff_witkin (:272-292): stretch / shear of the rest-frame deformation
+//     gradient (compute_rest_shape, :240-270), area-weighted, dt^2;
+// the lagged friction of examples/dropping_in_container/friction_helpers.py
+// (:12-66 smoothing, :73-182 point-triangle), and a StVK membrane on the same
+// rest frame (the reference ships no StVK).  Gradients and Hessians come from
+// second-order forward-mode differentiation (ys_ad.cuh); the local Hessian
+// is projected like the SNH one (LDL^T PSD test, then the negative modes) and
+// scattered with the NoProject merge rules into pattern records.
+#include "ys_ad.cuh"
+#include "ys_common.cuh"
+
+namespace ys {
+
+template <int A>
+struct Pts {
+  double p[A][3];
+};
+
+__device__ __forceinline__ void load_point(const ys_union3& u, uint32_t idx, double (&p)[3]) {
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 1; k < YS_MAX_UNION; ++k)
+    if (k < (int)u.num_children && idx >= u.prefix[k]) c = k;
+  const double* s = u.child[c] + 3ull * (idx - u.prefix[c]);
+  p[0] = __ldg(s);
+  p[1] = __ldg(s + 1);
+  p[2] = __ldg(s + 2);
+}
+
+// kappa u^2 L^2 with u = d - dHat, L = log(d / dHat), as f(d), f', f''.
+template <int N>
+__device__ __forceinline__ HD<N> barrier_of(const HD<N>& d, double dhat, double kappa) {
+  const double x = d.v, u = x - dhat, L = log(x / dhat), ix = 1.0 / x;
+  const double f = kappa * u * u * L * L;
+  const double df = kappa * (2.0 * u * L * L + 2.0 * u * u * L * ix);
+  const double d2f = kappa * (2.0 * L * L + 8.0 * u * L * ix + 2.0 * u * u * ix * ix - 2.0 * u * u * L * ix * ix);
+  return hd_apply(d, f, df, d2f);
+}
+
+struct PointPoint {
+  static constexpr int A = 2;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t, const Pts<A>& x, const Pts<A>&) {
+    const HV<N> p0 = hv_var<N>(x.p[0], 0), p1 = hv_var<N>(x.p[1], 3);
+    const HV<N> e = p1 - p0;
+    return barrier_of(dot(e, e), a.values[0], a.values[1]);
+  }
+};
+
+struct PointEdge {
+  static constexpr int A = 3;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t, const Pts<A>& x, const Pts<A>&) {
+    const HV<N> p0 = hv_var<N>(x.p[0], 0), p1 = hv_var<N>(x.p[1], 3), p2 = hv_var<N>(x.p[2], 6);
+    const HV<N> c = cross(p1 - p0, p2 - p0);
+    const HV<N> e = p2 - p1;
+    return barrier_of(dot(c, c) / dot(e, e), a.values[0], a.values[1]);
+  }
+};
+
+struct PointTriangle {
+  static constexpr int A = 4;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t, const Pts<A>& x, const Pts<A>&) {
+    const HV<N> p0 = hv_var<N>(x.p[0], 0), p1 = hv_var<N>(x.p[1], 3), p2 = hv_var<N>(x.p[2], 6),
+                p3 = hv_var<N>(x.p[3], 9);
+    const HV<N> b = cross(p2 - p1, p3 - p1);
+    const HD<N> atb = dot(p0 - p1, b);
+    return barrier_of(sq(atb) / dot(b, b), a.values[0], a.values[1]);
+  }
+};
+
+struct EdgeEdge {
+  static constexpr int A = 4;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t, const Pts<A>& x, const Pts<A>&) {
+    const HV<N> p0 = hv_var<N>(x.p[0], 0), p1 = hv_var<N>(x.p[1], 3), p2 = hv_var<N>(x.p[2], 6),
+                p3 = hv_var<N>(x.p[3], 9);
+    const HV<N> b = cross(p1 - p0, p3 - p2);
+    const HD<N> atb = dot(p2 - p0, b);
+    return barrier_of(sq(atb) / dot(b, b), a.values[0], a.values[1]);
+  }
+};
+
+// Plain-double dihedral angle of the same formula (rest state).
+__device__ __forceinline__ double dihedral(const double (&q0)[3], const double (&q1)[3], const double (&q2)[3],
+                                          const double (&q3)[3]) {
+  auto sub = [](const double (&u)[3], const double (&v)[3], double (&o)[3]) {
+    o[0] = u[0] - v[0]; o[1] = u[1] - v[1]; o[2] = u[2] - v[2];
+  };
+  auto crs = [](const double (&u)[3], const double (&v)[3], double (&o)[3]) {
+    o[0] = u[1] * v[2] - u[2] * v[1]; o[1] = u[2] * v[0] - u[0] * v[2]; o[2] = u[0] * v[1] - u[1] * v[0];
+  };
+  auto dt = [](const double (&u)[3], const double (&v)[3]) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+  double a[3], b[3], n0[3], n1[3], axis[3], c[3];
+  sub(q0, q2, a); sub(q1, q2, b); crs(a, b, n0);
+  sub(q1, q3, a); sub(q0, q3, b); crs(a, b, n1);
+  sub(q1, q0, axis);
+  crs(n0, n1, c);
+  const double num = dt(c, axis) / sqrt(dt(axis, axis));
+  const double den = dt(n0, n1) + sqrt(dt(n0, n0)) * sqrt(dt(n1, n1));
+  return 2.0 * atan2(num, den);
+}
+
+struct Bending {
+  static constexpr int A = 4;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t, const Pts<A>& x, const Pts<A>& r) {
+    const HV<N> q0 = hv_var<N>(x.p[0], 0), q1 = hv_var<N>(x.p[1], 3), q2 = hv_var<N>(x.p[2], 6),
+                q3 = hv_var<N>(x.p[3], 9);
+    const HV<N> n0 = cross(q0 - q2, q1 - q2);
+    const HV<N> n1 = cross(q1 - q3, q0 - q3);
+    const HV<N> axis = q1 - q0;
+    const HD<N> num = dot(cross(n0, n1), axis) / norm(axis);
+    const HD<N> den = dot(n0, n1) + norm(n0) * norm(n1);
+    const HD<N> theta = 2.0 * hd_atan2(num, den);
+    const double theta0 = dihedral(r.p[0], r.p[1], r.p[2], r.p[3]);
+    const double e0 = r.p[1][0] - r.p[0][0], e1 = r.p[1][1] - r.p[0][1], e2 = r.p[1][2] - r.p[0][2];
+    const double len = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+    const double dt = a.values[1];
+    return (a.values[0] * len * dt * dt) * sq(theta - theta0);
+  }
+};
+
+// Rest-frame inverse shape matrix of a triangle (compute_rest_shape,
+// helpers.py:240-270: rotate the normal onto +y, keep (x, z)) and the rest
+// area |v01 x v02| / 2.
+__device__ __forceinline__ void rest_frame(const Pts<3>& r, double (&minv)[2][2], double& area) {
+  double v01[3], v02[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { v01[k] = r.p[1][k] - r.p[0][k]; v02[k] = r.p[2][k] - r.p[0][k]; }
+  double n[3] = {v01[1] * v02[2] - v01[2] * v02[1], v01[2] * v02[0] - v01[0] * v02[2],
+                 v01[0] * v02[1] - v01[1] * v02[0]};
+  const double nl = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  area = 0.5 * nl;
+  n[0] /= nl; n[1] /= nl; n[2] /= nl;
+  // vec = n x (0, 1, 0), cos = n.(0, 1, 0)
+  const double v[3] = {-n[2], 0.0, n[0]};
+  const double c = n[1];
+  const double vx[3][3] = {{0.0, -v[2], v[1]}, {v[2], 0.0, -v[0]}, {-v[1], v[0], 0.0}};
+  double rot[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s += vx[i][k] * vx[k][j];
+      rot[i][j] = (i == j ? 1.0 : 0.0) + vx[i][j] + s / (1.0 + c);
+    }
+  double uv[3][2];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    uv[p][0] = rot[0][0] * r.p[p][0] + rot[0][1] * r.p[p][1] + rot[0][2] * r.p[p][2];
+    uv[p][1] = rot[2][0] * r.p[p][0] + rot[2][1] * r.p[p][1] + rot[2][2] * r.p[p][2];
+  }
+  const double m00 = uv[1][0] - uv[0][0], m01 = uv[2][0] - uv[0][0];
+  const double m10 = uv[1][1] - uv[0][1], m11 = uv[2][1] - uv[0][1];
+  const double idet = 1.0 / (m00 * m11 - m01 * m10);
+  minv[0][0] = m11 * idet;
+  minv[0][1] = -m01 * idet;
+  minv[1][0] = -m10 * idet;
+  minv[1][1] = m00 * idet;
+}
+
+// Columns of F = [x1 - x0, x2 - x0] M^-1 (3x2).
+template <int N>
+__device__ __forceinline__ void membrane_f(const Pts<3>& x, const double (&minv)[2][2], HV<N>& f0, HV<N>& f1) {
+  const HV<N> p0 = hv_var<N>(x.p[0], 0), p1 = hv_var<N>(x.p[1], 3), p2 = hv_var<N>(x.p[2], 6);
+  const HV<N> x10 = p1 - p0, x20 = p2 - p0;
+  f0 = minv[0][0] * x10 + minv[1][0] * x20;
+  f1 = minv[0][1] * x10 + minv[1][1] * x20;
+}
+
+struct BaraffWitkin {
+  static constexpr int A = 3;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t, const Pts<A>& x, const Pts<A>& r) {
+    double minv[2][2], area;
+    rest_frame(r, minv, area);
+    HV<N> f0, f1;
+    membrane_f<N>(x, minv, f0, f1);
+    const HD<N> shear = sq(dot(f0, f1));
+    const HD<N> i5u = norm(f0), i5v = norm(f1);
+    const double uc = i5u.v < 1.0 ? 0.01 : 1.0, vc = i5v.v < 1.0 ? 0.01 : 1.0;
+    const HD<N> stretch = uc * sq(i5u - 1.0) + vc * sq(i5v - 1.0);
+    const double dt = a.values[3];
+    const double w = a.values[2] * area * dt * dt;  // thickness * area * dt^2
+    return w * (a.values[0] * stretch + a.values[1] * shear);
+  }
+};
+
+// psi = mu tr(E^2) + lam/2 tr(E)^2, E = (F^T F - I) / 2, on the same rest frame.
+struct StvkMembrane {
+  static constexpr int A = 3;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t, const Pts<A>& x, const Pts<A>& r) {
+    double minv[2][2], area;
+    rest_frame(r, minv, area);
+    HV<N> f0, f1;
+    membrane_f<N>(x, minv, f0, f1);
+    const HD<N> e00 = 0.5 * (dot(f0, f0) - 1.0), e11 = 0.5 * (dot(f1, f1) - 1.0), e01 = 0.5 * dot(f0, f1);
+    const HD<N> tr = e00 + e11;
+    const HD<N> psi = a.values[0] * (sq(e00) + sq(e11) + 2.0 * sq(e01)) + (0.5 * a.values[1]) * sq(tr);
+    const double dt = a.values[3];
+    return (a.values[2] * area * dt * dt) * psi;
+  }
+};
+
+// Lagged point-triangle friction (friction_helpers.py:12-66, :73-182).
+// Per element params: beta1, beta2, tangent0 (3), tangent1 (3), lambda_last_h;
+// `rest` holds the positions at the start of the step.
+struct FrictionPT {
+  static constexpr int A = 4;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t t, const Pts<A>& x, const Pts<A>& r) {
+    const double* q = a.params + (uint64_t)t * a.param_stride;
+    const double b1 = q[0], b2 = q[1];
+    HV<N> dx[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double d[3] = {x.p[k][0] - r.p[k][0], x.p[k][1] - r.p[k][1], x.p[k][2] - r.p[k][2]};
+      dx[k] = hv_var<N>(d, 3 * k);  // d(x - x_old)/dx = I
+    }
+    const HV<N> rel = dx[0] - (dx[1] + b1 * (dx[2] - dx[1]) + b2 * (dx[3] - dx[1]));
+    const HD<N> u0 = q[2] * rel.x + q[3] * rel.y + q[4] * rel.z;
+    const HD<N> u1 = q[5] * rel.x + q[6] * rel.y + q[7] * rel.z;
+    const HD<N> y2 = sq(u0) + sq(u1);
+    const double fdhat = a.values[0], dt = a.values[1], rate = a.values[2];
+    const double eps = sqrt(fdhat) * dt, fric_dhat = fdhat * dt * dt;
+    const HD<N> y = hd_sqrt(y2 + 1e-16);
+    HD<N> phi;
+    if (y2.v > fric_dhat) phi = y;
+    else phi = ((1.0 / eps) * y2 + eps / 3.0) - (1.0 / (3.0 * eps * eps)) * (y2 * y);
+    return (rate * q[8]) * phi;
+  }
+};
+
+// ---- scatter into records --------------------------------------------------
+
+template <int A>
+__device__ __forceinline__ void load_arg_codes(const ys_term_plan& p, uint32_t t, uint32_t (&code)[A]) {
+#pragma unroll
+  for (int k = 0; k < A; ++k) code[k] = p.codes[(uint64_t)t * p.K + (uint64_t)k * p.slot_stride];
+}
+
+// Records of the (projected) local Hessian h (packed upper, N = 3A): merged
+// per distinct target argument, blocks transposed when the row DoF exceeds
+// the column DoF (hessianKernelNoProject.pyx:94-264), in the slot order of
+// the coordinates (first occurrence i <= j).
+template <int A>
+__device__ __forceinline__ void write_records(const uint32_t (&code)[A], uint32_t occ0, const uint32_t* record,
+                                              double* out, const double (&h)[3 * A * (3 * A + 1) / 2]) {
+  constexpr int N = 3 * A;
+  int group[A], first[A];
+  int nfirst = 0;
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    group[k] = -1;
+    if (code[k] < 2) continue;
+    int g = -1;
+    for (int q = 0; q < nfirst; ++q)
+      if (code[first[q]] == code[k]) g = q;
+    if (g < 0) { first[nfirst] = k; g = nfirst++; }
+    group[k] = g;
+  }
+  uint32_t occ = occ0;
+  for (int gi = 0; gi < nfirst; ++gi)
+    for (int gj = gi; gj < nfirst; ++gj) {
+      double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+      for (int ai = 0; ai < A; ++ai) {
+        if (group[ai] != gi) continue;
+#pragma unroll
+        for (int bi = 0; bi < A; ++bi) {
+          if (group[bi] != gj) continue;
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int l = 0; l < 3; ++l) acc[k][l] += h[utri<N>(3 * ai + k, 3 * bi + l)];
+        }
+      }
+      double* dst = out + record[occ++];
+      const bool upper = code[first[gi]] < code[first[gj]];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) dst[3 * k + l] = upper ? acc[k][l] : acc[l][k];
+    }
+}
+
+// Threads per CTA of the energy kernels (the projection stash is per thread).
+constexpr int kEnergyThreads = 32;
+
+template <class E>
+__global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const ys_energy_args a) {
+  constexpr int A = E::A, N = 3 * A;
+  extern __shared__ double energy_stash[];
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  Pts<A> x, r;
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    const uint32_t id = a.conn[(uint64_t)t * A + k];
+    load_point(a.position, id, x.p[k]);
+    if (a.rest.num_children) load_point(a.rest, id, r.p[k]);
+    else r.p[k][0] = r.p[k][1] = r.p[k][2] = 0.0;
+  }
+  const HD<N> e = E::template eval<N>(a, t, x, r);
+  if (a.energy) a.energy[t] = e.v;
+  uint32_t code[A];
+  load_arg_codes<A>(a.plan, t, code);
+  uint32_t q = a.plan.grad_outer[t];
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    if (code[k] < 2) continue;
+    double* dst = a.grad_records + a.plan.grad_record[q++];
+    dst[0] = e.g[3 * k];
+    dst[1] = e.g[3 * k + 1];
+    dst[2] = e.g[3 * k + 2];
+  }
+  double h[HD<N>::H];
+#pragma unroll
+  for (int i = 0; i < HD<N>::H; ++i) h[i] = e.h[i];
+  if (a.projection_method >= 1) {
+    double s[HD<N>::H];  // packed lower copy for the PSD test
+#pragma unroll
+    for (int rr = 0; rr < N; ++rr)
+#pragma unroll
+      for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = h[utri<N>(c, rr)];
+    if (!psd_test_packed<N>(s))
+      project_negative_modes<N>(h, a.projection_method, energy_stash + threadIdx.x, blockDim.x);
+  }
+  write_records<A>(code, a.plan.coord_outer[t], a.plan.record, a.block_records, h);
+}
+
+template <class E>
+static int32_t launch_energy(const ys_energy_args& a, cudaStream_t s) {
+  YS_REQUIRE(a.arity == (uint32_t)E::A, YS_ERR_INVALID, "arity does not match the energy kind");
+  constexpr int N = 3 * E::A;
+  const size_t smem = sizeof(double) * project_stash_doubles<N>() * kEnergyThreads;
+  YS_CUDA_TRY(cudaFuncSetAttribute(energy_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  energy_kernel<E><<<grid_for(a.num_elements, kEnergyThreads), kEnergyThreads, smem, s>>>(a);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+}  // namespace ys
+
+extern "C" {
+
+int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
+  YS_REQUIRE(args != nullptr, YS_ERR_INVALID, "null args");
+  const ys_energy_args& a = *args;
+  YS_REQUIRE(a.plan.slot_stride >= 1 && a.plan.K == a.arity * a.plan.slot_stride, YS_ERR_INVALID,
+             "K must be arity * slot_stride");
+  YS_REQUIRE(a.position.num_children >= 1 && a.position.num_children <= YS_MAX_UNION, YS_ERR_INVALID,
+             "bad position union");
+  YS_REQUIRE(a.rest.num_children <= YS_MAX_UNION, YS_ERR_INVALID, "bad rest union");
+  if (a.num_elements == 0) return YS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool needs_rest = a.kind == YS_ENERGY_BENDING || a.kind == YS_ENERGY_BARAFF_WITKIN ||
+                          a.kind == YS_ENERGY_STVK_MEMBRANE || a.kind == YS_ENERGY_FRICTION_PT;
+  YS_REQUIRE(!needs_rest || a.rest.num_children >= 1, YS_ERR_INVALID, "this energy needs rest positions");
+  YS_REQUIRE(a.kind != YS_ENERGY_FRICTION_PT || (a.params && a.param_stride >= 9), YS_ERR_INVALID,
+             "friction needs 9 lagged parameters per element");
+  switch (a.kind) {
+    case YS_ENERGY_POINT_POINT: return ys::launch_energy<ys::PointPoint>(a, s);
+    case YS_ENERGY_POINT_EDGE: return ys::launch_energy<ys::PointEdge>(a, s);
+    case YS_ENERGY_POINT_TRIANGLE: return ys::launch_energy<ys::PointTriangle>(a, s);
+    case YS_ENERGY_EDGE_EDGE: return ys::launch_energy<ys::EdgeEdge>(a, s);
+    case YS_ENERGY_BENDING: return ys::launch_energy<ys::Bending>(a, s);
+    case YS_ENERGY_BARAFF_WITKIN: return ys::launch_energy<ys::BaraffWitkin>(a, s);
+    case YS_ENERGY_STVK_MEMBRANE: return ys::launch_energy<ys::StvkMembrane>(a, s);
+    case YS_ENERGY_FRICTION_PT: return ys::launch_energy<ys::FrictionPT>(a, s);
+    default: break;
+  }
+  YS_REQUIRE(false, YS_ERR_INVALID, "unknown energy kind");
+}
+
+}  // extern "C"

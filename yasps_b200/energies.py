@@ -112,3 +112,97 @@ def inertia(x_before, vel, dt, x, mass, gravity=(0.0, -9.8, 0.0)) -> InertiaEner
   parameter here.
   """
   return InertiaEnergy(x_before, vel, dt, x, mass, gravity)
+
+
+# ---- vertex-tuple energies (cloth, contact, friction) -----------------------------
+
+class VertexEnergy(EnergyExpr):
+  """An energy over a JOIN of ``arity`` 3-vectors, evaluated by ``ys_energy_eval``."""
+
+  kind = "vertex"
+  code = 0
+  arity = 0
+  param_names = ()
+
+  def __init__(self, position, rest=None, params=(), per_element=None):
+    super().__init__()
+    _join_of_positions(position, "position", self.arity)
+    if rest is not None:
+      _join_of_positions(rest, "rest", self.arity)
+      if rest.through is not position.through:
+        raise ValueError(f"{type(self).__name__}: rest and current positions must use the same connectivity")
+    self.position, self.rest = position, rest
+    self.params = tuple(params)
+    self.per_element = per_element
+
+  def validate(self, prim) -> None:
+    if self.position.correspondance is not prim:
+      raise ValueError(f"{type(self).__name__}: the position JOIN must live on the energy's primitive")
+    self.params_p = [_param(v, prim, n) for v, n in zip(self.params, self.param_names)]
+    for p, n in zip(self.params_p, self.param_names):
+      if p[0] == "array":
+        raise ValueError(f"{n} must be a scalar")
+    if self.per_element is not None:
+      if self.per_element.correspondance is not prim:
+        raise ValueError("per-element parameters must live on the energy's primitive")
+
+
+def _vertex_energy(name, code, arity, names, needs_rest):
+  cls = type(name, (VertexEnergy,), {"code": code, "arity": arity, "param_names": names})
+  cls.needs_rest = needs_rest
+  return cls
+
+
+PointPointBarrier = _vertex_energy("PointPointBarrier", 1, 2, ("dHat", "kappa"), False)
+PointEdgeBarrier = _vertex_energy("PointEdgeBarrier", 2, 3, ("dHat", "kappa"), False)
+PointTriangleBarrier = _vertex_energy("PointTriangleBarrier", 3, 4, ("dHat", "kappa"), False)
+EdgeEdgeBarrier = _vertex_energy("EdgeEdgeBarrier", 4, 4, ("dHat", "kappa"), False)
+BendingEnergy = _vertex_energy("BendingEnergy", 5, 4, ("bendStiff", "dt"), True)
+BaraffWitkinEnergy = _vertex_energy("BaraffWitkinEnergy", 6, 3, ("stretchS", "shearS", "thickness", "dt"), True)
+StvkMembraneEnergy = _vertex_energy("StvkMembraneEnergy", 7, 3, ("mu", "lam", "thickness", "dt"), True)
+FrictionPointTriangle = _vertex_energy("FrictionPointTriangle", 8, 4, ("fDhat", "dt", "frictionRate"), True)
+
+
+def point_point(position, dHat, kappa):
+  """IPC barrier on the squared point-point distance (``helpers.py:143-152``)."""
+  return PointPointBarrier(position, None, (dHat, kappa))
+
+
+def point_edge(position, dHat, kappa):
+  """IPC barrier on the squared point-edge distance (``helpers.py:154-165``)."""
+  return PointEdgeBarrier(position, None, (dHat, kappa))
+
+
+def point_triangle(position, dHat, kappa):
+  """IPC barrier on the squared point-triangle distance (``helpers.py:167-180``)."""
+  return PointTriangleBarrier(position, None, (dHat, kappa))
+
+
+def edge_edge(position, dHat, kappa):
+  """IPC barrier on the squared edge-edge distance (``helpers.py:182-195``)."""
+  return EdgeEdgeBarrier(position, None, (dHat, kappa))
+
+
+def bending(x, x_init, bendStiff, dt):
+  """Dihedral bending ``kb (theta - theta0)^2 |e0| dt^2`` (``helpers.py:213-234``)."""
+  return BendingEnergy(x, x_init, (bendStiff, dt))
+
+
+def baraff_witkin(x_init, x, stretchS, shearS, thickness, dt):
+  """Baraff-Witkin cloth stretch + shear (``helpers.py:272-292``)."""
+  return BaraffWitkinEnergy(x, x_init, (stretchS, shearS, thickness, dt))
+
+
+def stvk_membrane(x_init, x, mu, lam, thickness, dt):
+  """StVK membrane on the Baraff-Witkin rest frame (no counterpart in the reference)."""
+  return StvkMembraneEnergy(x, x_init, (mu, lam, thickness, dt))
+
+
+def friction_point_triangle(position, old_position, fDhat, dt, frictionRate, lagged):
+  """Lagged point-triangle friction (``friction_helpers.py:12-66, 73-182``).
+
+  ``lagged`` is a 9-vector attribute of the energy's primitive per pair:
+  ``beta1, beta2, tangent0 (3), tangent1 (3), lambda_last_h``, fixed over the
+  Newton step as in the reference.
+  """
+  return FrictionPointTriangle(position, old_position, (fDhat, dt, frictionRate), per_element=lagged)

@@ -94,6 +94,11 @@ class _Term:
       conn = join.through.value
       leaves, prefix = resolve_leaf_children(join.source)
       dim = 4
+    elif self.expr.kind == "vertex":
+      join = self.expr.position
+      conn = join.through.value
+      leaves, prefix = resolve_leaf_children(join.source)
+      dim = self.expr.arity
     elif self.expr.kind == "inertia":
       key = ("identity", n)
       if key not in self._const_cache:
@@ -165,6 +170,30 @@ class _Term:
       a.work_list, a.work_count = L.ptr(wl), L.ptr(wc)
       import ctypes
       L.call("ys_snh_eval", ctypes.byref(a), s)
+    elif e.kind == "vertex":
+      import ctypes
+      a = L.EnergyArgs()
+      a.kind = e.code
+      a.position = self._union3(e.position.source)
+      if e.rest is not None:
+        a.rest = self._union3(e.rest.source)
+      else:
+        a.rest.num_children = 0
+      if e.needs_rest and e.rest is None:
+        raise ValueError(f"{type(e).__name__} needs rest positions")
+      a.conn = L.ptr(e.position.through.value)
+      a.arity = e.arity
+      a.num_elements = n
+      if e.per_element is not None:
+        a.params = L.ptr(e.per_element.value)
+        a.param_stride = e.per_element.size
+      for k, p in enumerate(e.params_p):
+        a.values[k] = self._param(p, n)[1]
+      a.projection_method = self.projection_method
+      a.plan = plan
+      a.block_records, a.grad_records = L.ptr(block_records), L.ptr(grad_records)
+      a.energy = L.ptr(energy)
+      L.call("ys_energy_eval", ctypes.byref(a), s)
     elif e.kind == "inertia":
       import ctypes
       a = L.InertiaArgs()
