@@ -16,6 +16,8 @@ in and the solution copied out every step.
 ``serving``: the serving form on a seeded stream of 512 FEM Newton steps
 (Poisson arrivals, sides 8..48): continuous batching in the precision form
 beside the serial plain FP64 path, solves/s and p50/p99 latency (rank 0, N=1).
+``cloth_contact``: Newton steps of the mixed cloth + contact scene (StVK,
+bending, 200k barrier pairs, friction) in both precision forms (rank 0, N=1).
 ``--impl reference``: the CPU restatement of the reference path (oracle) on
 a bounded sample of the same workload (rank 0 only).
 
@@ -51,6 +53,7 @@ def parse():
   p.add_argument("--side", type=int, default=64, help="cube side in vertices")
   p.add_argument("--no-cpu-baseline", action="store_true")
   p.add_argument("--tol", type=float, default=1e-6)
+  p.add_argument("--no-cloth", action="store_true", help="skip the cloth + contact leg")
   p.add_argument("--serving-requests", type=int, default=512,
                  help="requests of the serving stream (0: skip the serving leg)")
   return p.parse_args()
@@ -256,6 +259,9 @@ def gpu_arm(args):
   serve = None
   if rank == 0 and world == 1 and args.serving_requests > 0:
     serve = serving_leg(args)
+  cloth = None
+  if rank == 0 and world == 1 and not args.no_cloth:
+    cloth = cloth_leg(args)
   line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
           "vs_baseline": None, "dtype": "f32+f64 refine (f64 element Hessians and projection)",
@@ -268,7 +274,7 @@ def gpu_arm(args):
           "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * cube.dofs,
                   "d2h_bytes_per_step": 8 * cube.dofs},
           "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline, "clocks": clk,
-          "cpu_baseline": cpu, "serving": serve}
+          "cpu_baseline": cpu, "serving": serve, "cloth_contact": cloth}
   if rank == 0:
     print(json.dumps(line), flush=True)
   if pg is not None:
@@ -296,6 +302,34 @@ def launches_per_newton_step(impl, its, refs):
   init = 1 + (first - 1) + tail + 2
   per_it = 2 + (first - 1) + tail + 3
   return 6 + (levels - 1) + 1 + 1 + 2 * refs + refs * init + its * per_it
+
+
+def cloth_leg(args):
+  """Mixed cloth + contact Newton steps (StVK membrane, bending, 100k PT + 100k
+  EE barriers, PT friction, inertia; 256^2 cloth over a static obstacle):
+  precision form and plain FP64, CUDA-event timed."""
+  import torch
+  from yasps_b200 import scenes
+  cc = scenes.cloth_contact(256, 200_000)
+  sc, _ = scenes.cloth_contact_scene(cc)
+  mz = sc.minimizer
+  out = {"workload": ("256x256 cloth (65,536 verts, 130,050 tris) StVK E=1e4 nu=0.3 h=1e-3, bending kb=1e-3, "
+                      "100k point-triangle + 100k edge-edge log-barrier pairs (d-hat 1e-3, squared distances "
+                      "in (0.1, 1) d-hat) against a static obstacle, lagged PT friction mu=0.3, inertia; "
+                      "solve to 1e-6 true relative residual")}
+  for name, mixed in (("fp32_refine", True), ("fp64", False)):
+    solver = mz.setSolver("mas", mixed_spmv=mixed, stop_rule="residual")
+    step = lambda: mz.computeHessianAndGradient(tolerance=args.tol, maxIterations=5000)
+    for _ in range(2):
+      step()
+    ms, _ = time_steps(step, 5, None)
+    st = solver.statistics
+    out[name] = {"solves_per_s": 5 / (ms / 1e3), "ms_per_step": ms / 5, "iterations": int(st["iterations"]),
+                 "refinements": int(st.get("refinements", 0))}
+  impl = mz.linearSolver.implementation
+  out["dof"] = mz.activeHessian().rows
+  out["blocks"] = int(mz.activeHessian()._static.pattern.num_unique)
+  return out
 
 
 def serving_leg(args):

@@ -33,12 +33,40 @@ def _time(fn, reps):
   return e0.elapsed_time(e1) / reps
 
 
+def cloth_main(args):
+  """Cloth + contact scene (StVK, bending, PT/EE barriers, PT friction)."""
+  cc = scenes.cloth_contact(args.side, args.pairs)
+  sc, _ = scenes.cloth_contact_scene(cc)
+  mz = sc.minimizer
+  mz.setSolver("mas", mixed_spmv=True, stop_rule="residual")
+  mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000)
+  torch.cuda.synchronize()
+  H = mz.activeHessian()
+  bs = H._static
+  out = {"scene": "cloth_contact", "side": args.side, "pairs": args.pairs, "dof": H.rows,
+         "blocks": bs.pattern.num_unique, "pcg": mz.linearSolver.statistics}
+  for d in bs.infos:
+    t = d["term"]
+    plan = H._term_plan(d, bs)
+    name = type(t.expr).__name__
+    out[name + "_ms"] = _time(lambda: t.evaluate(plan, bs.records, H._grad_records), args.reps)
+    out[name + "_elements"] = t.n
+  out["compute_ms"] = _time(lambda: H.compute(), max(2, args.reps // 4))
+  out["newton_step_ms"] = _time(lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
+                                max(2, args.reps // 5))
+  print(json.dumps(out))
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument("--side", type=int, default=64)
   ap.add_argument("--kernel", default="all")
   ap.add_argument("--reps", type=int, default=20)
+  ap.add_argument("--scene", default="fem", choices=["fem", "cloth"])
+  ap.add_argument("--pairs", type=int, default=200_000)
   args = ap.parse_args()
+  if args.scene == "cloth":
+    return cloth_main(args)
   cube = scenes.fem_cube(args.side, young=1e6, poisson=0.45, noise=0.005)
   sc, _ = scenes.fem_scene(cube)
   mz = sc.minimizer

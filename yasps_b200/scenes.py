@@ -220,3 +220,174 @@ def fem_cube(n: int, spacing: float = 0.1, young: float = 1e5, poisson: float = 
       tets=union_of_lex[tets_lex].astype(np.uint32), mass=vmass[free_ids],
       velocity=np.zeros((free_ids.size, 3)), mu=mu, lam=lam, density=density, dt=dt,
       gravity=np.asarray(gravity, dtype=np.float64))
+
+
+# ---- cloth over a static obstacle with synthetic contacts ------------------------------
+
+def lagged_friction_pt(x_old, dhat, kappa):
+  """Lagged point-triangle friction data for pairs ``x_old`` [n, 4, 3] (point,
+  triangle) at the start of the step, vectorised: the closest-point
+  coordinates, the tangent basis and the contact force magnitude
+  (``friction_helpers.py:12-27, 73-141``); returns [n, 9]
+  (beta1, beta2, tangent0, tangent1, lambda_last_h)."""
+  x = np.asarray(x_old, dtype=np.float64)
+  p, t0, t1, t2 = x[:, 0], x[:, 1], x[:, 2], x[:, 3]
+  e01, e02 = t1 - t0, t2 - t0
+  B = np.stack([e01, e02], axis=2)                       # [n, 3, 2]
+  btb = np.einsum("nki,nkj->nij", B, B)
+  beta = np.einsum("nij,nj->ni", np.linalg.inv(btb), np.einsum("nki,nk->ni", B, p - t0))
+  tan0 = e01 / np.linalg.norm(e01, axis=1, keepdims=True)
+  c = np.cross(np.cross(e01, e02), e01)
+  tan1 = c / np.linalg.norm(c, axis=1, keepdims=True)
+  q = t0 + beta[:, :1] * e01 + beta[:, 1:] * e02
+  d2 = np.einsum("ni,ni->n", p - q, p - q)
+  lg = np.log(d2 / dhat)
+  lenE = d2 - dhat
+  inner = lg * lg * (2.0 * d2 - 2.0 * dhat) + 2.0 * lg * lenE * lenE / d2
+  lam = -kappa * 2.0 * np.sqrt(d2) * inner
+  return np.concatenate([beta, tan0, tan1, lam[:, None]], axis=1)
+
+
+@dataclass
+class ClothContact:
+  """Arrays of the cloth-over-obstacle scene (union order: obstacle, cloth)."""
+
+  side: int
+  cloth_rest: np.ndarray      # (nc, 3)
+  cloth_position: np.ndarray  # (nc, 3)
+  obstacle: np.ndarray        # (no, 3) static, non-target
+  tris: np.ndarray            # (nt, 3) cloth triangles (cloth-local ids)
+  bend: np.ndarray            # (nb, 4) interior edges + opposite vertices (cloth-local)
+  pt: np.ndarray              # (npt, 4) union ids: cloth point, obstacle triangle
+  ee: np.ndarray              # (nee, 4) union ids: cloth edge, obstacle edge
+  lagged: np.ndarray          # (npt, 9) friction data of the PT pairs
+  mass: np.ndarray            # (nc,)
+  mu: float
+  lam: float
+  thickness: float
+  bend_stiff: float
+  dhat: float
+  kappa: float
+  friction: float
+  fdhat: float
+  dt: float
+
+
+def cloth_contact(side: int = 256, pairs: int = 200_000, spacing: float = 0.05, young: float = 1e4,
+                  poisson: float = 0.3, thickness: float = 1e-3, bend_stiff: float = 1e-3, dhat: float = 1e-3,
+                  kappa: float = 1e3, friction: float = 0.3, eps_v: float = 1e-3, density: float = 200.0,
+                  dt: float = 0.01, seed: int = 0) -> ClothContact:
+  """A ``side x side`` cloth sheet (xz plane, triangles wound to +y normals)
+  over a static obstacle grid offset by half a cell, with ``pairs`` synthetic
+  contacts split between point-triangle and edge-edge pairs whose squared
+  distances spread over (0.1, 1.0) d-hat (obstacle heights drawn per vertex)."""
+  rng = np.random.default_rng(seed)
+  n = side
+  gi, gk = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+  rest = np.stack([gi.ravel() * spacing, np.zeros(n * n), gk.ravel() * spacing], axis=1)
+  pos = rest + rng.uniform(-0.01, 0.01, size=rest.shape) * spacing
+  pos[:, 1] = 0.0
+  a = (gi[:-1, :-1] * n + gk[:-1, :-1]).ravel()
+  b, c, d = a + n, a + n + 1, a + 1
+  tris = np.concatenate([np.stack([a, c, b], axis=1), np.stack([a, d, c], axis=1)])
+  # interior edges with their two opposite vertices
+  e = np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]])
+  opp = np.concatenate([tris[:, 2], tris[:, 0], tris[:, 1]])
+  key = np.sort(e, axis=1)
+  order = np.lexsort((key[:, 1], key[:, 0]))
+  key, e, opp = key[order], e[order], opp[order]
+  same = np.all(key[1:] == key[:-1], axis=1)
+  i = np.flatnonzero(same)
+  bend = np.stack([e[i, 0], e[i, 1], opp[i], opp[i + 1]], axis=1)
+  # obstacle: (n-1) x (n-1) grid at the cell centres, below the cloth
+  m = n - 1
+  oi, ok = np.meshgrid(np.arange(m), np.arange(m), indexing="ij")
+  obstacle = np.stack([(oi.ravel() + 0.5) * spacing, np.zeros(m * m), (ok.ravel() + 0.5) * spacing], axis=1)
+  obstacle[:, 1] = -np.sqrt(rng.uniform(0.1, 1.0, size=m * m) * dhat)
+  no = m * m
+  oa = (oi[:-1, :-1] * m + ok[:-1, :-1]).ravel()
+  otris = np.stack([oa, oa + m + 1, oa + m], axis=1)
+  npt = pairs // 2
+  nee = pairs - npt
+  # PT: a cloth vertex above an obstacle triangle (cloth vertex (i+1, k+1) lies over cell (i, k))
+  tri_pick = rng.integers(0, len(otris), size=npt)
+  ti, tk = tri_pick // (m - 1), tri_pick % (m - 1)
+  cloth_v = (ti + 1) * n + (tk + 1)
+  pt = np.stack([no + cloth_v, otris[tri_pick, 0], otris[tri_pick, 1], otris[tri_pick, 2]], axis=1)
+  # EE: a cloth x-edge crossing an obstacle z-edge below it
+  ei = rng.integers(0, m - 1, size=nee)
+  ek = rng.integers(1, m, size=nee)
+  c0 = ei * n + ek
+  c1 = (ei + 1) * n + ek
+  o0 = ei * m + (ek - 1)
+  o1 = ei * m + ek
+  ee = np.stack([no + c0, no + c1, o0, o1], axis=1)
+  allpos = np.concatenate([obstacle, pos])
+  lagged = lagged_friction_pt(allpos[pt], dhat, kappa)
+  areas = np.zeros(n * n)
+  cr = np.cross(rest[tris[:, 1]] - rest[tris[:, 0]], rest[tris[:, 2]] - rest[tris[:, 0]])
+  tri_area = 0.5 * np.linalg.norm(cr, axis=1)
+  np.add.at(areas, tris.ravel(), np.repeat(tri_area / 3.0, 3))
+  mu, lam = lame(young, poisson)
+  return ClothContact(side=n, cloth_rest=rest, cloth_position=pos, obstacle=obstacle, tris=tris, bend=bend,
+                      pt=pt.astype(np.uint32), ee=ee.astype(np.uint32), lagged=lagged,
+                      mass=density * thickness * areas, mu=mu, lam=lam, thickness=thickness,
+                      bend_stiff=bend_stiff, dhat=dhat, kappa=kappa, friction=friction, fdhat=eps_v * eps_v,
+                      dt=dt)
+
+
+def cloth_contact_scene(cc: ClothContact, projection_method: int = 1):
+  """The cloth scene with the public API: StVK membrane and bending on the
+  cloth, PT/EE barriers and PT friction through a union [obstacle, cloth]
+  (the obstacle is DATA but not a minimisation target), inertia."""
+  from .energies import (edge_edge, friction_point_triangle, inertia, point_triangle, bending as bend_energy,
+                         stvk_membrane)
+  from .scene import scene as make_scene
+  sc = make_scene("cloth_contact")
+  body = sc.addMesh("cloth")
+  obst = body.addPrimitive("obstacle", numInstances=len(cc.obstacle))
+  opos = obst.addAttribute("position", rows=3, cols=1)
+  opos.updateValue(cc.obstacle)
+  orest = obst.addConstant("old_position", rows=3, cols=1)
+  orest.updateValue(cc.obstacle)
+  cloth = body.addPrimitive("cloth", numInstances=len(cc.cloth_position))
+  pos = cloth.addAttribute("position", rows=3, cols=1)
+  pos.updateValue(cc.cloth_position)
+  rest = cloth.addConstant("rest_position", rows=3, cols=1)
+  rest.updateValue(cc.cloth_rest)
+  old = cloth.addConstant("old_position", rows=3, cols=1)
+  old.updateValue(cc.cloth_position)
+  mass = cloth.addConstant("mass")
+  mass.updateValue(cc.mass)
+  tri = body.addPrimitive("triangles", numInstances=len(cc.tris))
+  tc = tri.addConnectivity("to_cloth", cloth, cc.tris.astype(np.uint32), 3)
+  mem = tri.addAttribute("stvk", computed_attribute=stvk_membrane(
+      tri.addAttribute("rest", through=tc, source=rest), tri.addAttribute("x", through=tc, source=pos),
+      cc.mu, cc.lam, cc.thickness, cc.dt))
+  be = body.addPrimitive("bending_edges", numInstances=len(cc.bend))
+  bc = be.addConnectivity("to_cloth", cloth, cc.bend.astype(np.uint32), 4)
+  ben = be.addAttribute("bending", computed_attribute=bend_energy(
+      be.addAttribute("x", through=bc, source=pos), be.addAttribute("rest", through=bc, source=rest),
+      cc.bend_stiff, cc.dt))
+  allv = body.addPrimitiveUnion("all_vertices", [obst, cloth])
+  apos = allv.addAttribute("position")
+  aold = allv.addAttribute("old_position")
+  ptp = body.addPrimitive("pt_pairs", numInstances=len(cc.pt))
+  ptc = ptp.addConnectivity("to_vertices", allv, cc.pt, 4)
+  ptx = ptp.addAttribute("x", through=ptc, source=apos)
+  pte = ptp.addAttribute("barrier", computed_attribute=point_triangle(ptx, cc.dhat, cc.kappa))
+  lag = ptp.addConstant("lagged", rows=9, cols=1)
+  lag.updateValue(cc.lagged)
+  ptf = ptp.addAttribute("friction", computed_attribute=friction_point_triangle(
+      ptx, ptp.addAttribute("x_old", through=ptc, source=aold), cc.fdhat, cc.dt, cc.friction, lag))
+  eep = body.addPrimitive("ee_pairs", numInstances=len(cc.ee))
+  eec = eep.addConnectivity("to_vertices", allv, cc.ee, 4)
+  eee = eep.addAttribute("barrier", computed_attribute=edge_edge(
+      eep.addAttribute("x", through=eec, source=apos), cc.dhat, cc.kappa))
+  kin = cloth.addAttribute("inertia", computed_attribute=inertia(old, None, cc.dt, pos, mass,
+                                                                 gravity=(0.0, -9.8, 0.0)))
+  for e in (mem, ben, pte, eee, ptf):
+    sc.addEnergy(e, projection_method=projection_method)
+  sc.addEnergy(kin, projection_method=-1)
+  sc.addMinimizeTarget([pos])
+  return sc, dict(position=pos, old_position=old)
