@@ -172,6 +172,10 @@ typedef struct ys_snh_args {
  * `compute_hessian_and_gradient_with_compression` for this energy
  * (hessianKernelHost.pyx:27-161).                                          */
 int32_t ys_snh_eval(const ys_snh_args* args, void* stream);
+/* With block_records and grad_records NULL, ys_snh_eval, ys_inertia_eval and
+ * ys_energy_eval write only the per-element energies to `energy` (the
+ * reference's per-instance energy kernel, PKG/kernel/globalKernel.pyx:35-434,
+ * used by minimizer.computeTotalEnergy, minimizer.pyx:396-407).           */
 
 typedef struct ys_inertia_args {
   const double* position;       /* [n x 3] (DATA target primitive)                  */
@@ -238,6 +242,11 @@ typedef struct ys_energy_args {
 /* Replaces the generated `compute_hessian_and_gradient_with_compression` of
  * these energies (hessianKernelHost.pyx:27-161).                           */
 int32_t ys_energy_eval(const ys_energy_args* args, void* stream);
+
+/* Deterministic sum of n doubles into out[0] (device), fixed reduction order
+ * for a given n; workspace: ys_sum_workspace_doubles() doubles.            */
+uint64_t ys_sum_workspace_doubles(void);
+int32_t ys_sum(const double* values, uint32_t n, double* out, double* workspace, void* stream);
 
 /* ---- deterministic assembly --------------------------------------------- */
 

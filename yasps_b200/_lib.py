@@ -114,6 +114,8 @@ SIGNATURES = {
     "ys_snh_eval": (i32, [P(SnhArgs), vp]),
     "ys_inertia_eval": (i32, [P(InertiaArgs), vp]),
     "ys_energy_eval": (i32, [P(EnergyArgs), vp]),
+    "ys_sum_workspace_doubles": (u64, []),
+    "ys_sum": (i32, [vp, u32, vp, vp, vp]),
     "ys_assemble": (i32, [vp, vp, vp, vp, vp, u32, vp, vp, vp]),
     "ys_assemble3": (i32, [vp, vp, vp, vp, u32, vp, vp, vp]),
     "ys_assemble_strided": (i32, [vp, vp, vp, vp, u32, vp, u32, vp, vp]),

@@ -32,6 +32,16 @@ struct HD {
   double h[H];
 };
 
+// Value only (energy evaluation without derivatives): the loops over N = 0
+// inputs are empty; the one-element arrays are never touched.
+template <>
+struct HD<0> {
+  static constexpr int H = 0;
+  double v;
+  double g[1];
+  double h[1];
+};
+
 template <int N>
 __device__ __forceinline__ HD<N> hd_const(double c) {
   HD<N> r;

@@ -6,6 +6,8 @@
 // occurrence index.  Assembly is a segmented sum over contiguous memory in
 // that order: no float atomics, bit-reproducible, HBM bound (read records
 // once, write the assembled values once).
+#include <algorithm>
+
 #include "ys_common.cuh"
 #include "ys_eigen.cuh"
 
@@ -135,6 +137,36 @@ __global__ void invert_blocks_kernel(const double* __restrict__ in, double* __re
     }
 }
 
+// Deterministic sum: block sums of a fixed grid, then the last block adds
+// them in index order.
+constexpr int kSumThreads = 256;
+constexpr unsigned kSumBlocks = 1024;
+
+__global__ void __launch_bounds__(kSumThreads) sum_kernel(const double* __restrict__ x, uint32_t n,
+                                                          double* __restrict__ partials, unsigned* __restrict__ ticket,
+                                                          double* __restrict__ out) {
+  __shared__ double red[kSumThreads / 32];
+  __shared__ bool last;
+  double v = 0.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v += x[i];
+  const double sb = block_sum<kSumThreads>(v, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = sb;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double acc = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) acc += __ldcg(partials + b);
+  acc = block_sum<kSumThreads>(acc, red);
+  if (threadIdx.x == 0) {
+    *out = acc;
+    *ticket = 0u;
+  }
+}
+
 }  // namespace ys
 
 extern "C" {
@@ -209,6 +241,22 @@ int32_t ys_invert_diagonal_blocks(const double* diag_blocks, double* inverse, ui
     }
     YS_CHECK_LAUNCH();
   }
+  return YS_OK;
+}
+
+uint64_t ys_sum_workspace_doubles(void) { return ys::kSumBlocks + 1; }
+
+int32_t ys_sum(const double* values, uint32_t n, double* out, double* workspace, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned* ticket = reinterpret_cast<unsigned*>(workspace + ys::kSumBlocks);
+  YS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
+  if (n == 0) {
+    YS_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double), s));
+    return YS_OK;
+  }
+  const unsigned grid = std::min<unsigned>(ys::grid_for(n, ys::kSumThreads), ys::kSumBlocks);
+  ys::sum_kernel<<<grid, ys::kSumThreads, 0, s>>>(values, n, workspace, ticket, out);
+  YS_CHECK_LAUNCH();
   return YS_OK;
 }
 

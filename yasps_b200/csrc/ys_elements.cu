@@ -406,6 +406,7 @@ __global__ void inertia_kernel(const ys_inertia_args a) {
   for (int k = 0; k < 3; ++k) xt[k] = xb[k] + (a.velocity ? a.velocity[3ull * i + k] * a.dt : 0.0) + a.gravity[k] * h2;
   const double d0 = x[0] - xt[0], d1 = x[1] - xt[1], d2 = x[2] - xt[2];
   if (a.energy) a.energy[i] = 0.5 * m * (d0 * d0 + d1 * d1 + d2 * d2);
+  if (!a.block_records) return;  // energy only
   const uint32_t code = a.plan.codes[(uint64_t)i * a.plan.K];
   if (code < 2) return;
   double* g = a.grad_records + a.plan.grad_record[a.plan.grad_outer[i]];
@@ -417,6 +418,15 @@ __global__ void inertia_kernel(const ys_inertia_args a) {
   for (int k = 0; k < 9; ++k) h[k] = (k % 4 == 0) ? m : 0.0;
 }
 
+// Per-tet energy only (line search).
+__global__ void __launch_bounds__(128) snh_energy_kernel(const ys_snh_args a) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  SnhState st;
+  snh_state(a, t, st);
+  a.energy[t] = st.energy;
+}
+
 }  // namespace ys
 
 extern "C" {
@@ -424,14 +434,20 @@ extern "C" {
 int32_t ys_snh_eval(const ys_snh_args* args, void* stream) {
   YS_REQUIRE(args != nullptr, YS_ERR_INVALID, "null args");
   const ys_snh_args& a = *args;
-  YS_REQUIRE(a.plan.slot_stride >= 1 && a.plan.K == 4 * a.plan.slot_stride, YS_ERR_INVALID,
-             "SNH needs 4 arguments (K = 4 * slot_stride)");
   YS_REQUIRE(a.position.num_children >= 1 && a.position.num_children <= YS_MAX_UNION, YS_ERR_INVALID,
              "bad position union");
   YS_REQUIRE(a.rest.num_children >= 1 && a.rest.num_children <= YS_MAX_UNION, YS_ERR_INVALID, "bad rest union");
   YS_REQUIRE(((uintptr_t)a.tets & 15u) == 0, YS_ERR_INVALID, "tets must be 16-byte aligned");
   if (a.num_elements == 0) return YS_OK;
   cudaStream_t s = (cudaStream_t)stream;
+  if (a.block_records == nullptr && a.grad_records == nullptr) {
+    YS_REQUIRE(a.energy, YS_ERR_INVALID, "energy-only evaluation needs the energy output");
+    ys::snh_energy_kernel<<<ys::grid_for(a.num_elements, 128), 128, 0, s>>>(a);
+    YS_CHECK_LAUNCH();
+    return YS_OK;
+  }
+  YS_REQUIRE(a.plan.slot_stride >= 1 && a.plan.K == 4 * a.plan.slot_stride, YS_ERR_INVALID,
+             "SNH needs 4 arguments (K = 4 * slot_stride)");
   if (a.projection_method >= 1) {
     YS_REQUIRE(a.work_list && a.work_count, YS_ERR_INVALID, "projection needs work_list/work_count");
     YS_CUDA_TRY(cudaMemsetAsync(a.work_count, 0, sizeof(uint32_t), s));

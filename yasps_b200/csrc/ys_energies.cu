@@ -343,6 +343,31 @@ __global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const ys_energy_
   write_records<A>(code, a.plan.coord_outer[t], a.plan.record, a.block_records, h);
 }
 
+// Per-element energy only (line search): the same formulas on HD<0> numbers.
+template <class E>
+__global__ void __launch_bounds__(128) energy_value_kernel(const ys_energy_args a) {
+  constexpr int A = E::A;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  Pts<A> x, r;
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    const uint32_t id = a.conn[(uint64_t)t * A + k];
+    load_point(a.position, id, x.p[k]);
+    if (a.rest.num_children) load_point(a.rest, id, r.p[k]);
+    else r.p[k][0] = r.p[k][1] = r.p[k][2] = 0.0;
+  }
+  a.energy[t] = E::template eval<0>(a, t, x, r).v;
+}
+
+template <class E>
+static int32_t launch_energy_value(const ys_energy_args& a, cudaStream_t s) {
+  YS_REQUIRE(a.arity == (uint32_t)E::A, YS_ERR_INVALID, "arity does not match the energy kind");
+  energy_value_kernel<E><<<grid_for(a.num_elements, 128), 128, 0, s>>>(a);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
 template <class E>
 static int32_t launch_energy(const ys_energy_args& a, cudaStream_t s) {
   YS_REQUIRE(a.arity == (uint32_t)E::A, YS_ERR_INVALID, "arity does not match the energy kind");
@@ -361,8 +386,6 @@ extern "C" {
 int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
   YS_REQUIRE(args != nullptr, YS_ERR_INVALID, "null args");
   const ys_energy_args& a = *args;
-  YS_REQUIRE(a.plan.slot_stride >= 1 && a.plan.K == a.arity * a.plan.slot_stride, YS_ERR_INVALID,
-             "K must be arity * slot_stride");
   YS_REQUIRE(a.position.num_children >= 1 && a.position.num_children <= YS_MAX_UNION, YS_ERR_INVALID,
              "bad position union");
   YS_REQUIRE(a.rest.num_children <= YS_MAX_UNION, YS_ERR_INVALID, "bad rest union");
@@ -373,6 +396,24 @@ int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
   YS_REQUIRE(!needs_rest || a.rest.num_children >= 1, YS_ERR_INVALID, "this energy needs rest positions");
   YS_REQUIRE(a.kind != YS_ENERGY_FRICTION_PT || (a.params && a.param_stride >= 9), YS_ERR_INVALID,
              "friction needs 9 lagged parameters per element");
+  if (a.block_records == nullptr && a.grad_records == nullptr) {
+    // energy only
+    YS_REQUIRE(a.energy, YS_ERR_INVALID, "energy-only evaluation needs the energy output");
+    switch (a.kind) {
+      case YS_ENERGY_POINT_POINT: return ys::launch_energy_value<ys::PointPoint>(a, s);
+      case YS_ENERGY_POINT_EDGE: return ys::launch_energy_value<ys::PointEdge>(a, s);
+      case YS_ENERGY_POINT_TRIANGLE: return ys::launch_energy_value<ys::PointTriangle>(a, s);
+      case YS_ENERGY_EDGE_EDGE: return ys::launch_energy_value<ys::EdgeEdge>(a, s);
+      case YS_ENERGY_BENDING: return ys::launch_energy_value<ys::Bending>(a, s);
+      case YS_ENERGY_BARAFF_WITKIN: return ys::launch_energy_value<ys::BaraffWitkin>(a, s);
+      case YS_ENERGY_STVK_MEMBRANE: return ys::launch_energy_value<ys::StvkMembrane>(a, s);
+      case YS_ENERGY_FRICTION_PT: return ys::launch_energy_value<ys::FrictionPT>(a, s);
+      default: break;
+    }
+    YS_REQUIRE(false, YS_ERR_INVALID, "unknown energy kind");
+  }
+  YS_REQUIRE(a.plan.slot_stride >= 1 && a.plan.K == a.arity * a.plan.slot_stride, YS_ERR_INVALID,
+             "K must be arity * slot_stride");
   switch (a.kind) {
     case YS_ENERGY_POINT_POINT: return ys::launch_energy<ys::PointPoint>(a, s);
     case YS_ENERGY_POINT_EDGE: return ys::launch_energy<ys::PointEdge>(a, s);

@@ -422,6 +422,43 @@ class hessian:
     self.values32_current = self.want_fp32
     return self
 
+  def term_energies(self):
+    """Per-element energies of every term (device tensors), energy kernels only."""
+    torch = _torch()
+    if not self._setup:
+      self._setup_compute()
+      if not self._dynamic.terms:
+        self._gradient_plan(self._static_infos[0])
+    out = []
+    plan = L.TermPlan()
+    for bs in (self._static, self._dynamic):
+      for t in bs.terms:
+        key = ("energy_values", t.n)
+        if key not in t._const_cache:
+          t._const_cache[key] = torch.empty(max(t.n, 1), dtype=torch.float64, device=_dev())
+        e = t._const_cache[key]
+        if t.n:
+          t.evaluate(plan, None, None, e)
+        out.append((t, e[:t.n]))
+    return out
+
+  def computeTotalEnergy(self) -> float:
+    """Sum of all terms' energies: each term summed on the device in a fixed
+    order (``ys_sum``), the terms added on the host in request order
+    (``minimizer.pyx:396-407``)."""
+    torch = _torch()
+    terms = self.term_energies()
+    if getattr(self, "_sum_work", None) is None:
+      self._sum_work = torch.empty(int(L.load().ys_sum_workspace_doubles()), dtype=torch.float64, device=_dev())
+    sums = torch.zeros(max(len(terms), 1), dtype=torch.float64, device=_dev())
+    s = L.stream_ptr()
+    for k, (t, e) in enumerate(terms):
+      L.call("ys_sum", L.ptr(e), t.n, sums.data_ptr() + 8 * k, L.ptr(self._sum_work), s)
+    total = 0.0
+    for v in sums[:len(terms)].cpu().tolist():
+      total += v
+    return total
+
   def _extract_diagonal(self):
     s = L.stream_ptr()
     self.diagonal.zero_()

@@ -99,6 +99,34 @@ class minimizer:
   def gradient(self):
     return self.activeHessian().gradient.value
 
+  def computeTotalEnergy(self) -> float:
+    """Total energy of the active (not ignored) energies (``minimizer.pyx:396-407``)."""
+    return self.activeHessian().computeTotalEnergy()
+
+  def backtrackingLineSearch(self, direction=None, step=1.0, shrink=0.5, max_steps=8):
+    """Move the targets to ``x - alpha d`` with the largest ``alpha = step *
+    shrink^k`` (k < max_steps) that does not increase the total energy, as the
+    reference examples' substep loop does after their CCD step bound
+    (``examples/dropping_in_container/dropping_in_container.py:486-560``).
+    ``direction`` defaults to the last solution segments.  Returns the
+    accepted alpha (0.0 when no step decreased the energy: targets restored).
+    """
+    segs = self.solutionSegments if direction is None else direction
+    if len(segs) != len(self.wrt):
+      raise ValueError("minimizer.backtrackingLineSearch: one direction segment per target")
+    before = self.computeTotalEnergy()
+    saved = [w.value.clone() for w in self.wrt]
+    alpha = float(step)
+    for _ in range(int(max_steps)):
+      for w, x0, d in zip(self.wrt, saved, segs):
+        w.copyValueFrom(x0 - alpha * d.reshape(x0.shape), non_blocking=False)
+      if self.computeTotalEnergy() <= before:
+        return alpha
+      alpha *= shrink
+    for w, x0 in zip(self.wrt, saved):
+      w.copyValueFrom(x0, non_blocking=False)
+    return 0.0
+
   def computeHessianAndGradient(self, tolerance=1e-3, maxIterations=20000):
     H = self.computeNumericValue()
     code = self.linearSolver.computeSolution(H, H.gradient, None, tolerance=tolerance, maxIterations=maxIterations,
@@ -168,6 +196,12 @@ class scene:
   @property
   def gradient(self):
     return self.minimizer.gradient
+
+  def computeTotalEnergy(self) -> float:
+    return self.minimizer.computeTotalEnergy()
+
+  def backtrackingLineSearch(self, direction=None, step=1.0, shrink=0.5, max_steps=8):
+    return self.minimizer.backtrackingLineSearch(direction, step, shrink, max_steps)
 
   def ignoreEnergies(self, energies):
     self.minimizer.ignoreEnergies(energies)
