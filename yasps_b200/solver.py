@@ -90,10 +90,13 @@ class _PcgBase:
 
   def _run_pcg(self, H, rhs, x, fp32, prec_kind, jinv, mas_handle, tol, maxit, zero_guess, stop_rule):
     """One device PCG solve into ``x``; returns the ys_pcg_result."""
+    # the graph holds every device pointer of the matrix: a rebuilt pattern
+    # (dynamic terms) gives new row plans and must give a new graph
+    plans = tuple(tuple(t.data_ptr() for t in H.spmv_plan(bs)) + (bs.pattern.num_unique,) for bs in H.block_sets)
     key = (id(H), H.rows, rhs.data_ptr(), x.data_ptr(), fp32, prec_kind, None if jinv is None else jinv.data_ptr(),
            mas_handle, bool(zero_guess), stop_rule,
            tuple(bs.values.data_ptr() for bs in H.block_sets),
-           tuple(0 if bs.values32 is None else bs.values32.data_ptr() for bs in H.block_sets))
+           tuple(0 if bs.values32 is None else bs.values32.data_ptr() for bs in H.block_sets), plans)
 
     def build():
       args = L.PcgArgs()
