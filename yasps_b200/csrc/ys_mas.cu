@@ -184,17 +184,25 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
 
 // Packed level residuals, one level per launch: level 0 is r itself (FP32
 // copy); a node of level l >= 1 sums its children of level l-1.
+// Level 0: a thread per node; levels >= 1: a warp per node.
 __global__ void mas_restrict(MasDev M, const double* __restrict__ r, uint32_t level) {
   const uint32_t begin = M.level_node_offset[level], end = M.level_node_offset[level + 1];
-  const uint32_t p = begin + blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= end) return;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (level == 0) {
+    const uint32_t p = begin + t;
+    if (p >= end) return;
     M.rl[3ull * p] = (float)r[3ull * p];
     M.rl[3ull * p + 1] = (float)r[3ull * p + 1];
     M.rl[3ull * p + 2] = (float)r[3ull * p + 2];
-  } else {
-    restrict_node(M, r, level, p);
+    return;
   }
+  const uint32_t p = begin + (t >> 5);
+  if (p >= end) return;  // warp-uniform
+  restrict_node_warp(M, r, level, p, (int)(t & 31));
+}
+
+__host__ inline unsigned restrict_grid(uint32_t level, uint32_t cnt) {
+  return grid_for(level == 0 ? (uint64_t)cnt : 32ull * cnt, 256);
 }
 
 // All levels from `first` to the coarsest in one CTA (small levels: the
@@ -395,7 +403,7 @@ static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGra
     void* a1[] = {&m, &rr, &level};
     const uint32_t cnt = M.level_node_offset[l + 1] - M.level_node_offset[l];
     cudaGraphNode_t n = nullptr;
-    e = add_kernel(g, &n, dp, nd, (const void*)mas_restrict, grid_for(cnt, 256), 256, 0, a1);
+    e = add_kernel(g, &n, dp, nd, (const void*)mas_restrict, restrict_grid(l, cnt), 256, 0, a1);
     prev = n;
     dp = &prev;
     nd = 1;
@@ -567,7 +575,7 @@ int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
   ys::MasDev& M = h->M;
   for (uint32_t l = 0; l < M.levels; ++l) {
     const uint32_t cnt = M.level_node_offset[l + 1] - M.level_node_offset[l];
-    ys::mas_restrict<<<ys::grid_for(cnt, 256), 256, 0, s>>>(M, r, l);
+    ys::mas_restrict<<<ys::restrict_grid(l, cnt), 256, 0, s>>>(M, r, l);
     YS_CHECK_LAUNCH();
   }
   ys::mas_gemv<<<M.num_domains, 128, ys::gemv_smem_bytes(M.max_dofs), s>>>(M);

@@ -51,30 +51,41 @@ __device__ __forceinline__ const double* level_block(const MasDev& M, uint32_t i
   return idx < M.fine_blocks ? M.fine_values + 9ull * idx : M.coarse_values + 9ull * (idx - M.fine_blocks);
 }
 
-// Level-l (l >= 1) node p: fixed-order sum of its children of level l-1.
-__device__ __forceinline__ void restrict_node(const MasDev& M, const double* __restrict__ r, uint32_t level,
-                                              uint32_t p) {
+// Level-l (l >= 1) node p by one warp (p warp-uniform): lane k sums children
+// k, k+32, ... of level l-1 (FP64), a fixed xor-shuffle tree adds the lanes.
+__device__ __forceinline__ void restrict_node_warp(const MasDev& M, const double* __restrict__ r, uint32_t level,
+                                                   uint32_t p, int lane) {
   const double* src = level == 1 ? r : M.rl64;
   const uint32_t c = p - M.nv;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (uint32_t q = M.child_ptr[c]; q < M.child_ptr[c + 1]; ++q) {
+  for (uint32_t q = M.child_ptr[c] + lane; q < M.child_ptr[c + 1]; q += 32) {
     const uint32_t f = M.child_fine[q];
     s0 += src[3ull * f]; s1 += src[3ull * f + 1]; s2 += src[3ull * f + 2];
   }
-  M.rl64[3ull * p] = s0;
-  M.rl64[3ull * p + 1] = s1;
-  M.rl64[3ull * p + 2] = s2;
-  M.rl[3ull * p] = (float)s0;
-  M.rl[3ull * p + 1] = (float)s1;
-  M.rl[3ull * p + 2] = (float)s2;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (lane == 0) {
+    M.rl64[3ull * p] = s0;
+    M.rl64[3ull * p + 1] = s1;
+    M.rl64[3ull * p + 2] = s2;
+    M.rl[3ull * p] = (float)s0;
+    M.rl[3ull * p + 1] = (float)s1;
+    M.rl[3ull * p + 2] = (float)s2;
+  }
 }
 
-// Levels first..coarsest by one CTA, level by level (block-strided nodes).
+// Levels first..coarsest by one CTA, level by level (a warp per node).
 __device__ __forceinline__ void restrict_tail_levels(const MasDev& M, const double* __restrict__ r,
                                                      uint32_t first) {
+  const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
   for (uint32_t level = first; level < M.levels; ++level) {
     const uint32_t begin = M.level_node_offset[level], end = M.level_node_offset[level + 1];
-    for (uint32_t p = begin + threadIdx.x; p < end; p += blockDim.x) restrict_node(M, r, level, p);
+    for (uint32_t p = begin + warp; p < end; p += nwarps) restrict_node_warp(M, r, level, p, lane);
     __syncthreads();
   }
 }

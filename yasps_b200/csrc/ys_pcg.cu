@@ -115,13 +115,16 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
 }
 
 // kRowLanes threads per row (see spmv3_group).
+// One instantiation per precision of the block values (the FP32 one keeps
+// fewer registers: higher occupancy for the latency-bound gathers).
+template <bool FP32>
 __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t i = t / kRowLanes;
   const int lane = (int)(t % kRowLanes);
   double v[1] = {0.0};
   double q0, q1, q2;
-  spmv3_group(P.sets, P.nsets, P.fp32, i, i < P.nv, lane, P.p, q0, q1, q2);
+  spmv3_group(P.sets, P.nsets, FP32, i, i < P.nv, lane, P.p, q0, q1, q2);
   if (i < P.nv && lane == 0) {
     P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
     v[0] = P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
@@ -346,7 +349,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       cudaGraph_t body = cp.conditional.phGraph_out[0];
       cudaGraphNode_t n1 = nullptr, n2 = nullptr, n3 = nullptr;
       void* args1[] = {&P};
-      e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot, grid_rows, ys::kPcgBlock, args1);
+      e = ys::add_kernel(body, &n1, nullptr, 0, P.fp32 ? (const void*)ys::pcg_spmv_dot<true> : (const void*)ys::pcg_spmv_dot<false>, grid_rows, ys::kPcgBlock, args1);
       if (e == cudaSuccess) {
         if (a.preconditioner == YS_PREC_BLOCK_JACOBI) {
           e = ys::add_kernel(body, &n2, &n1, 1, (const void*)ys::pcg_update_bj, grid, ys::kPcgBlock, args1);

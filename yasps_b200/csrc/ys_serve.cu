@@ -9,7 +9,8 @@
 //                     (INIT/REFINE: done when ||r|| <= tol ||g||, else START)
 //   serve_update    : ITER   d += alpha p, r -= alpha q;  START  d = 0
 //                     (both write the FP32 level-0 residual)
-//   serve_restrict  : MAS restriction of the large levels (one launch each)
+//   serve_restrict  : MAS restriction of the large levels (one launch each,
+//                     a warp per node)
 //   serve_tail      : MAS restriction of the small levels (one CTA a slot)
 //   serve_gemv      : MAS domain inverses (one CTA a domain)
 //   serve_collect   : z = M^-1 r, r^T z, r^T r -> beta; inner stop -> REFINE
@@ -242,8 +243,8 @@ __global__ void __launch_bounds__(kPcgBlock) serve_restrict(const ServeDev* __re
   uint32_t s, b;
   if (!map_entry(S->map_restrict[level], S->n_restrict[level], s, b) || !mas_live(S, s)) return;
   const ServeSlot& T = S->slots[s];
-  const uint32_t p = T.M.level_node_offset[level] + b * blockDim.x + threadIdx.x;
-  if (p < T.M.level_node_offset[level + 1]) restrict_node(T.M, T.r, level, p);
+  const uint32_t p = T.M.level_node_offset[level] + ((b * blockDim.x + threadIdx.x) >> 5);
+  if (p < T.M.level_node_offset[level + 1]) restrict_node_warp(T.M, T.r, level, p, (int)(threadIdx.x & 31));
 }
 
 __global__ void __launch_bounds__(1024) serve_tail(const ServeDev* __restrict__ S) {
@@ -423,7 +424,8 @@ static int32_t stage_maps(ServeHandle* h, cudaStream_t s) {
     tail.push_back(tag);
     for (uint32_t l = 1; l < T.first_tail; ++l) {
       const uint32_t cnt = T.M.level_node_offset[l + 1] - T.M.level_node_offset[l];
-      for (uint32_t b = 0; b < (cnt + kPcgBlock - 1) / kPcgBlock; ++b) res[l].push_back(tag | b);
+      // a warp per node
+      for (uint32_t b = 0; b < (32 * cnt + kPcgBlock - 1) / kPcgBlock; ++b) res[l].push_back(tag | b);
     }
     smem_dofs = std::max(smem_dofs, T.M.max_dofs);
   }
