@@ -69,12 +69,11 @@ __global__ void __launch_bounds__(256) mas_level_blocks(MasDev M, uint32_t begin
 // Dense assembly + in-place Gauss-Jordan inverse of one domain per CTA.
 // T: register tile edge (domain size <= 16 T).
 template <int T>
-__global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_inverse(MasDev M) {
+__global__ void __launch_bounds__(kInvThreads, 1) mas_domain_inverse(MasDev M) {
   extern __shared__ double A[];  // n*n
-  __shared__ double colk[2][128];
-  __shared__ double rowk[2][128];
+  __shared__ double colb[2][128 * 4];
+  __shared__ double rowb[2][4 * 128];
   __shared__ double dinv[128];
-  __shared__ double piv_sh[2];
   __shared__ int bad;
   const uint32_t d = blockIdx.x;
   const uint32_t n = 3 * (M.dom_node_ptr[d + 1] - M.dom_node_ptr[d]);
@@ -91,19 +90,21 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
     if (li != lj) A[(3 * lj + m) * n + 3 * li + k] = v;
   }
   __syncthreads();
-  // Gauss-Jordan without pivoting (SPD domains): after step k, A holds the
+  // Gauss-Jordan without pivoting (SPD domains): after a step, A holds the
   // inverse in the eliminated columns.  Relative pivot tolerance 1e-12 of
   // the largest diagonal entry (mas/local_inverse.py:43-65).
   // Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns tx + 16b
-  // (a, b < 8) in registers; each step only broadcasts the pivot row and
-  // column through shared memory.
-  // The matrix is first scaled to unit diagonal, S = D^-1/2 A D^-1/2 (pivots
-  // of S lie in (0, 1]); the inverse is D^-1/2 S^-1 D^-1/2.  A pivot of S
-  // below 1e-12 (or a non-positive diagonal) marks the domain singular.
-  // GJ step k as one uniform update S_ij -= c_i r_j / s_kk with c = column k
-  // except c_k = s_kk - 1 and r = row k except r_k = s_kk + 1: this yields
-  // the scaled row k, the column -s_ik / s_kk and the pivot 1 / s_kk exactly,
-  // so the update is pure FMAs (no per-element selects).
+  // (a, b < T) in registers.  The matrix is first scaled to unit diagonal,
+  // S = D^-1/2 A D^-1/2 (pivots in (0, 1]); the inverse is D^-1/2 S^-1 D^-1/2;
+  // a scalar pivot below 1e-12 (or a non-positive diagonal) marks the domain
+  // singular.  The order is padded to a multiple of 4 with identity rows.
+  // Blocked steps of 4 pivots K: with P = S[K,K], C = S[:,K] except
+  // C[K,:] = P - I and R = S[K,:] except R[:,K] = P + I, the one update
+  //   S -= (C P^-1) R
+  // gives the scaled rows P^-1 S[K,:], the columns -S[:,K] P^-1 and P^-1 in
+  // place, so the update is pure FMAs; the owners of the next block's rows and
+  // columns publish them to double-buffered shared memory, one barrier a step.
+  const uint32_t np = (n + 3) & ~3u;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
     const double dii = A[i * n + i];
     if (!(dii > 0.0)) bad = 1;
@@ -118,72 +119,108 @@ __global__ void __launch_bounds__(kInvThreads, T <= 6 ? 2 : 1) mas_domain_invers
 #pragma unroll
     for (int b = 0; b < T; ++b) {
       const uint32_t i = ty + 16 * a, j = tx + 16 * b;
-      R[a][b] = (i < n && j < n) ? A[i * n + j] * dinv[i] * dinv[j] : 0.0;
+      R[a][b] = (i < n && j < n) ? A[i * n + j] * dinv[i] * dinv[j] : (i == j && i < np ? 1.0 : 0.0);
     }
-  // Pivot column / row of step k are published in buffer k & 1 by their
-  // owners right after step k-1's update, so each step needs one barrier.
+  // publish block k: colb[buf][i][m] = C[i][m], rowb[buf][m][j] = R[m][j]
   auto publish = [&](uint32_t k) {
-    const int kb = (int)(k >> 4), kr = (int)(k & 15), buf = (int)(k & 1);
-    if (tx == kr) {
+    const int kb = (int)((4 * k) >> 4), base = (int)((4 * k) & 15), buf = (int)(k & 1);
+    if (tx >= base && tx < base + 4) {
+      const int m = tx - base;
 #pragma unroll
       for (int a = 0; a < T; ++a) {
         double v = 0.0;
 #pragma unroll
         for (int b = 0; b < T; ++b) v = (b == kb) ? R[a][b] : v;
-        const bool diag = (ty + 16 * a) == (int)k;
-        if (diag) piv_sh[buf] = v;
-        colk[buf][ty + 16 * a] = diag ? v - 1.0 : v;
+        const bool diag = (ty + 16 * a) == (int)(4 * k) + m;
+        colb[buf][(ty + 16 * a) * 4 + m] = diag ? v - 1.0 : v;
       }
     }
-    if (ty == kr) {
+    if (ty >= base && ty < base + 4) {
+      const int m = ty - base;
 #pragma unroll
       for (int b = 0; b < T; ++b) {
         double v = 0.0;
 #pragma unroll
         for (int a = 0; a < T; ++a) v = (a == kb) ? R[a][b] : v;
-        rowk[buf][tx + 16 * b] = ((tx + 16 * b) == (int)k) ? v + 1.0 : v;
+        const bool diag = (tx + 16 * b) == (int)(4 * k) + m;
+        rowb[buf][m * 128 + tx + 16 * b] = diag ? v + 1.0 : v;
       }
     }
   };
   publish(0);
   __syncthreads();
-  for (uint32_t k = 0; k < n; ++k) {
+  const uint32_t nblk = np / 4;
+  for (uint32_t k = 0; k < nblk; ++k) {
     const int buf = (int)(k & 1);
-    const double piv = piv_sh[buf];
-    if (!(piv > tol) && threadIdx.x == 0) bad = 1;
-    const double ip = 1.0 / piv;
-    double rj[T];
+    // P^-1 of the 4x4 pivot block (every thread alike) by 2x2 blocks:
+    // P = [A B; B' D], S = D - B' A^-1 B, P^-1 = [A^-1 + E S^-1 E', -E S^-1;
+    // -S^-1 E', S^-1] with E = A^-1 B (P is symmetric up to rounding; the
+    // blocks are read as stored).  The leading pivot and the Schur
+    // determinant carry the singularity test.
+    double P[4][4];
+    {
+      double q[4][4];
 #pragma unroll
-    for (int b = 0; b < T; ++b) rj[b] = rowk[buf][tx + 16 * b];
+      for (int l = 0; l < 4; ++l)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) q[l][m] = colb[buf][(4 * k + l) * 4 + m] + (l == m ? 1.0 : 0.0);
+      const double da = q[0][0] * q[1][1] - q[0][1] * q[1][0];
+      const double ida = 1.0 / da;
+      const double ai00 = q[1][1] * ida, ai01 = -q[0][1] * ida, ai10 = -q[1][0] * ida, ai11 = q[0][0] * ida;
+      // E = A^-1 B (2x2), F = C A^-1 (2x2), S = D - C A^-1 B
+      const double e00 = ai00 * q[0][2] + ai01 * q[1][2], e01 = ai00 * q[0][3] + ai01 * q[1][3];
+      const double e10 = ai10 * q[0][2] + ai11 * q[1][2], e11 = ai10 * q[0][3] + ai11 * q[1][3];
+      const double f00 = q[2][0] * ai00 + q[2][1] * ai10, f01 = q[2][0] * ai01 + q[2][1] * ai11;
+      const double f10 = q[3][0] * ai00 + q[3][1] * ai10, f11 = q[3][0] * ai01 + q[3][1] * ai11;
+      const double s00 = q[2][2] - (q[2][0] * e00 + q[2][1] * e10), s01 = q[2][3] - (q[2][0] * e01 + q[2][1] * e11);
+      const double s10 = q[3][2] - (q[3][0] * e00 + q[3][1] * e10), s11 = q[3][3] - (q[3][0] * e01 + q[3][1] * e11);
+      const double ds = s00 * s11 - s01 * s10;
+      const double ids = 1.0 / ds;
+      const double si00 = s11 * ids, si01 = -s01 * ids, si10 = -s10 * ids, si11 = s00 * ids;
+      // bottom right S^-1, top right -E S^-1, bottom left -S^-1 F, top left A^-1 + E S^-1 F
+      P[2][2] = si00; P[2][3] = si01; P[3][2] = si10; P[3][3] = si11;
+      P[0][2] = -(e00 * si00 + e01 * si10); P[0][3] = -(e00 * si01 + e01 * si11);
+      P[1][2] = -(e10 * si00 + e11 * si10); P[1][3] = -(e10 * si01 + e11 * si11);
+      P[2][0] = -(si00 * f00 + si01 * f10); P[2][1] = -(si00 * f01 + si01 * f11);
+      P[3][0] = -(si10 * f00 + si11 * f10); P[3][1] = -(si10 * f01 + si11 * f11);
+      P[0][0] = ai00 - (P[0][2] * f00 + P[0][3] * f10); P[0][1] = ai01 - (P[0][2] * f01 + P[0][3] * f11);
+      P[1][0] = ai10 - (P[1][2] * f00 + P[1][3] * f10); P[1][1] = ai11 - (P[1][2] * f01 + P[1][3] * f11);
+      // scalar pivots of the same elimination: q00, da / q00, and the two of S
+      const bool ok = q[0][0] > tol && da > tol * q[0][0] && s00 > tol && ds > tol * s00;
+      if (!ok && threadIdx.x == 0) bad = 1;
+    }
+    double rj[4][T];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int b = 0; b < T; ++b) rj[m][b] = rowb[buf][m * 128 + tx + 16 * b];
 #pragma unroll
     for (int a = 0; a < T; ++a) {
-      const double cip = colk[buf][ty + 16 * a] * ip;
+      const double* c = &colb[buf][(ty + 16 * a) * 4];
+      const double c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+      double w[4];
 #pragma unroll
-      for (int b = 0; b < T; ++b) R[a][b] = fma(-cip, rj[b], R[a][b]);
+      for (int m = 0; m < 4; ++m) w[m] = c0 * P[0][m] + c1 * P[1][m] + c2 * P[2][m] + c3 * P[3][m];
+#pragma unroll
+      for (int b = 0; b < T; ++b)
+        R[a][b] = fma(-w[3], rj[3][b], fma(-w[2], rj[2][b], fma(-w[1], rj[1][b], fma(-w[0], rj[0][b], R[a][b]))));
     }
-    if (k + 1 < n) publish(k + 1);
+    if (k + 1 < nblk) publish(k + 1);
     __syncthreads();
   }
+  if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
+  // FP32 upper triangle, row-major packed (row i holds columns i..n-1),
+  // straight from the register tiles (the upper entries of the inverse).
+  float* out = M.inverse + M.inv_offset[d];
 #pragma unroll
   for (int a = 0; a < T; ++a)
 #pragma unroll
     for (int b = 0; b < T; ++b) {
       const uint32_t i = ty + 16 * a, j = tx + 16 * b;
-      if (i < n && j < n) A[i * n + j] = R[a][b] * dinv[i] * dinv[j];
+      if (i < n && j < n && j >= i) out[i * n - i * (i - 1) / 2 + (j - i)] = (float)(R[a][b] * dinv[i] * dinv[j]);
     }
-  __syncthreads();
-  if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
-  // FP32 upper triangle, row-major packed (row i holds columns i..n-1).
-  float* out = M.inverse + M.inv_offset[d];
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t i = warp; i < n; i += kInvThreads / 32) {
-    const uint32_t base = i * n - i * (i - 1) / 2;
-    for (uint32_t j = i + lane; j < n; j += 32) out[base + (j - i)] = (float)(0.5 * (A[i * n + j] + A[j * n + i]));
-  }
 }
 
-// Packed level residuals, one level per launch: level 0 is r itself (FP32
-// copy); a node of level l >= 1 sums its children of level l-1.
 // Level 0: a thread per node; levels >= 1: a warp per node.
 __global__ void mas_restrict(MasDev M, const double* __restrict__ r, uint32_t level) {
   const uint32_t begin = M.level_node_offset[level], end = M.level_node_offset[level + 1];
