@@ -55,6 +55,11 @@ class vector:
     return self.value.detach().cpu().numpy()
 
 
+def fp32_slots(num_blocks: int) -> int:
+  """Floats of the FP32 copy of a 3x3 block set (16-byte aligned 12-float slots)."""
+  return max(12 * int(num_blocks), 12)
+
+
 class _Term:
   """One energy applied to all instances of its primitive."""
 
@@ -482,9 +487,10 @@ class hessian:
       return
     s = L.stream_ptr()
     v32 = None
-    if self.want_fp32:
-      if bs.values32 is None or bs.values32.numel() < bs.values.numel():
-        bs.values32 = torch.zeros(bs.values.numel(), dtype=torch.float32, device=_dev())
+    if self.want_fp32 and p.all3:
+      n32 = fp32_slots(p.num_unique)
+      if bs.values32 is None or bs.values32.numel() < n32:
+        bs.values32 = torch.zeros(n32, dtype=torch.float32, device=_dev())
       v32 = bs.values32
     if p.all3:
       L.call("ys_assemble3", L.ptr(bs.records), L.ptr(p.record_begin), L.ptr(p.record_count), L.ptr(p.value_offset),
@@ -524,7 +530,10 @@ class hessian:
     if self.values32_current:
       return
     for bs in self.block_sets:
-      bs.values32 = bs.values.to(torch.float32)
+      nu = bs.pattern.num_unique
+      v = torch.zeros((nu, 12), dtype=torch.float32, device=_dev())
+      v[:, :9] = bs.values[:9 * nu].view(nu, 9).to(torch.float32)
+      bs.values32 = v.reshape(-1)
     self.values32_current = True
 
   def spmv_plan(self, bs: _BlockSet):

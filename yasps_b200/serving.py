@@ -101,6 +101,7 @@ class FemTopology:
     bs = H.block_sets[0]
     self.plan = H.spmv_plan(bs)
     self.nvalues = int(bs.values.numel())
+    self.nvalues32 = int(bs.values32.numel())
     self.n = int(H.rows)
     self.nv = self.n // 3
     self.mu_att = self.scene["mu"]
@@ -128,7 +129,7 @@ class _Slot:
     dev = torch.device("cuda")
     self.topo = topo
     self.values = torch.zeros(topo.nvalues, dtype=torch.float64, device=dev)
-    self.values32 = torch.zeros(topo.nvalues, dtype=torch.float32, device=dev)
+    self.values32 = torch.zeros(topo.nvalues32, dtype=torch.float32, device=dev)
     self.g = torch.zeros(topo.n, dtype=torch.float64, device=dev)
     self.x = torch.zeros(topo.n, dtype=torch.float64, device=dev)
     self.work = torch.zeros(int(L.load().ys_serve_workspace_doubles(topo.nv)), dtype=torch.float64, device=dev)
