@@ -296,7 +296,7 @@ def launches_per_newton_step(impl, its, refs):
   offs = [int(v) for v in t.level_node_offset]
   levels = len(offs) - 1
   first = levels
-  while first > 1 and offs[first] - offs[first - 1] <= 4096:
+  while first > 1 and offs[first] - offs[first - 1] <= 512:
     first -= 1
   tail = 1 if first < levels else 0
   init = 1 + (first - 1) + tail + 2
@@ -340,7 +340,7 @@ def serving_leg(args):
   n = args.serving_requests
   srv = serving.NewtonServer(max_slots=64, passes=8, memory_budget=40e9, tolerance=args.tol)
   t0 = time.perf_counter()
-  srv.register(range(8, 49))
+  srv.register(range(8, 49), slots_per_side=2)
   t_register = time.perf_counter() - t0
   srv.run(serving.poisson_fem_stream(count=82, mean_spacing=0.0, seed=99))
   srv.solve_serial_fp64(serving.poisson_fem_stream(count=41, mean_spacing=0.0, seed=98))

@@ -68,8 +68,10 @@ __global__ void __launch_bounds__(256) mas_level_blocks(MasDev M, uint32_t begin
 
 // Dense assembly + in-place Gauss-Jordan inverse of one domain per CTA.
 // T: register tile edge (domain size <= 16 T).
-template <int T>
-__global__ void __launch_bounds__(kInvThreads, 1) mas_domain_inverse(MasDev M) {
+// PB pivots per blocked step (2: fits 128 registers, two CTAs per SM for the
+// 96-DoF domains; 4: the 128-DoF tile, one CTA per SM).
+template <int T, int PB>
+__global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inverse(MasDev M) {
   extern __shared__ double A[];  // n*n
   __shared__ double colb[2][128 * 4];
   __shared__ double rowb[2][4 * 128];
@@ -97,14 +99,14 @@ __global__ void __launch_bounds__(kInvThreads, 1) mas_domain_inverse(MasDev M) {
   // (a, b < T) in registers.  The matrix is first scaled to unit diagonal,
   // S = D^-1/2 A D^-1/2 (pivots in (0, 1]); the inverse is D^-1/2 S^-1 D^-1/2;
   // a scalar pivot below 1e-12 (or a non-positive diagonal) marks the domain
-  // singular.  The order is padded to a multiple of 4 with identity rows.
-  // Blocked steps of 4 pivots K: with P = S[K,K], C = S[:,K] except
+  // singular.  The order is padded to a multiple of PB with identity rows.
+  // Blocked steps of PB pivots K: with P = S[K,K], C = S[:,K] except
   // C[K,:] = P - I and R = S[K,:] except R[:,K] = P + I, the one update
   //   S -= (C P^-1) R
   // gives the scaled rows P^-1 S[K,:], the columns -S[:,K] P^-1 and P^-1 in
   // place, so the update is pure FMAs; the owners of the next block's rows and
   // columns publish them to double-buffered shared memory, one barrier a step.
-  const uint32_t np = (n + 3) & ~3u;
+  const uint32_t np = (n + PB - 1) / PB * PB;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
     const double dii = A[i * n + i];
     if (!(dii > 0.0)) bad = 1;
@@ -123,42 +125,49 @@ __global__ void __launch_bounds__(kInvThreads, 1) mas_domain_inverse(MasDev M) {
     }
   // publish block k: colb[buf][i][m] = C[i][m], rowb[buf][m][j] = R[m][j]
   auto publish = [&](uint32_t k) {
-    const int kb = (int)((4 * k) >> 4), base = (int)((4 * k) & 15), buf = (int)(k & 1);
-    if (tx >= base && tx < base + 4) {
+    const int kb = (int)((PB * k) >> 4), base = (int)((PB * k) & 15), buf = (int)(k & 1);
+    if (tx >= base && tx < base + PB) {
       const int m = tx - base;
 #pragma unroll
       for (int a = 0; a < T; ++a) {
         double v = 0.0;
 #pragma unroll
         for (int b = 0; b < T; ++b) v = (b == kb) ? R[a][b] : v;
-        const bool diag = (ty + 16 * a) == (int)(4 * k) + m;
-        colb[buf][(ty + 16 * a) * 4 + m] = diag ? v - 1.0 : v;
+        const bool diag = (ty + 16 * a) == (int)(PB * k) + m;
+        colb[buf][(ty + 16 * a) * PB + m] = diag ? v - 1.0 : v;
       }
     }
-    if (ty >= base && ty < base + 4) {
+    if (ty >= base && ty < base + PB) {
       const int m = ty - base;
 #pragma unroll
       for (int b = 0; b < T; ++b) {
         double v = 0.0;
 #pragma unroll
         for (int a = 0; a < T; ++a) v = (a == kb) ? R[a][b] : v;
-        const bool diag = (tx + 16 * b) == (int)(4 * k) + m;
+        const bool diag = (tx + 16 * b) == (int)(PB * k) + m;
         rowb[buf][m * 128 + tx + 16 * b] = diag ? v + 1.0 : v;
       }
     }
   };
   publish(0);
   __syncthreads();
-  const uint32_t nblk = np / 4;
+  const uint32_t nblk = np / PB;
   for (uint32_t k = 0; k < nblk; ++k) {
     const int buf = (int)(k & 1);
+    double P[PB][PB];
+    if constexpr (PB == 2) {
+      const double q00 = colb[buf][(2 * k) * 2] + 1.0, q01 = colb[buf][(2 * k) * 2 + 1];
+      const double q10 = colb[buf][(2 * k + 1) * 2], q11 = colb[buf][(2 * k + 1) * 2 + 1] + 1.0;
+      const double da = q00 * q11 - q01 * q10;
+      const double ida = 1.0 / da;
+      P[0][0] = q11 * ida; P[0][1] = -q01 * ida; P[1][0] = -q10 * ida; P[1][1] = q00 * ida;
+      if (!(q00 > tol && da > tol * q00) && threadIdx.x == 0) bad = 1;
+    } else {
     // P^-1 of the 4x4 pivot block (every thread alike) by 2x2 blocks:
     // P = [A B; B' D], S = D - B' A^-1 B, P^-1 = [A^-1 + E S^-1 E', -E S^-1;
     // -S^-1 E', S^-1] with E = A^-1 B (P is symmetric up to rounding; the
     // blocks are read as stored).  The leading pivot and the Schur
     // determinant carry the singularity test.
-    double P[4][4];
-    {
       double q[4][4];
 #pragma unroll
       for (int l = 0; l < 4; ++l)
@@ -189,21 +198,29 @@ __global__ void __launch_bounds__(kInvThreads, 1) mas_domain_inverse(MasDev M) {
       const bool ok = q[0][0] > tol && da > tol * q[0][0] && s00 > tol && ds > tol * s00;
       if (!ok && threadIdx.x == 0) bad = 1;
     }
-    double rj[4][T];
+    double rj[PB][T];
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < PB; ++m)
 #pragma unroll
       for (int b = 0; b < T; ++b) rj[m][b] = rowb[buf][m * 128 + tx + 16 * b];
 #pragma unroll
     for (int a = 0; a < T; ++a) {
-      const double* c = &colb[buf][(ty + 16 * a) * 4];
-      const double c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
-      double w[4];
+      const double* c = &colb[buf][(ty + 16 * a) * PB];
+      double w[PB];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) w[m] = c0 * P[0][m] + c1 * P[1][m] + c2 * P[2][m] + c3 * P[3][m];
+      for (int m = 0; m < PB; ++m) {
+        double acc = 0.0;
 #pragma unroll
-      for (int b = 0; b < T; ++b)
-        R[a][b] = fma(-w[3], rj[3][b], fma(-w[2], rj[2][b], fma(-w[1], rj[1][b], fma(-w[0], rj[0][b], R[a][b]))));
+        for (int l = 0; l < PB; ++l) acc += c[l] * P[l][m];
+        w[m] = acc;
+      }
+#pragma unroll
+      for (int b = 0; b < T; ++b) {
+        double v = R[a][b];
+#pragma unroll
+        for (int m = 0; m < PB; ++m) v = fma(-w[m], rj[m][b], v);
+        R[a][b] = v;
+      }
     }
     if (k + 1 < nblk) publish(k + 1);
     __syncthreads();
@@ -553,17 +570,17 @@ int32_t ys_mas_create(const ys_mas_desc* d, void** handle) {
   M.status = d->status;
   M.max_dofs = d->max_domain_dofs;
   M.fine_values = nullptr;
-  cudaError_t e = cudaMallocHost(&h->status_host, sizeof(int));
-  if (e == cudaSuccess) {
+  cudaError_t e = cudaSuccess;
+  {
     const size_t smem = sizeof(double) * d->max_domain_dofs * d->max_domain_dofs;
-    e = cudaFuncSetAttribute(ys::mas_domain_inverse<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(ys::mas_domain_inverse<6, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(ys::mas_domain_inverse<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(ys::mas_domain_inverse<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // prefer the largest shared-memory carveout so two 96-DoF domains fit per SM
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(ys::mas_domain_inverse<6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      e = cudaFuncSetAttribute(ys::mas_domain_inverse<6, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(ys::mas_domain_inverse<8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      e = cudaFuncSetAttribute(ys::mas_domain_inverse<8, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   }
   if (e != cudaSuccess) {
     ys_set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
@@ -592,11 +609,14 @@ int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* str
   }
   const size_t smem = sizeof(double) * M.max_dofs * M.max_dofs;
   if (M.max_dofs <= 96)
-    ys::mas_domain_inverse<6><<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
+    ys::mas_domain_inverse<6, 2><<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
   else
-    ys::mas_domain_inverse<8><<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
+    ys::mas_domain_inverse<8, 4><<<M.num_domains, ys::kInvThreads, smem, s>>>(M);
   YS_CHECK_LAUNCH();
   if (failed_domains) {
+    // pinned status word, allocated on first use (callers that never ask,
+    // such as the serving loop, never synchronise on a host allocation)
+    if (!h->status_host) YS_CUDA_TRY(cudaMallocHost(&h->status_host, sizeof(int)));
     YS_CUDA_TRY(cudaMemcpyAsync(h->status_host, M.status, sizeof(int), cudaMemcpyDeviceToHost, s));
     YS_CUDA_TRY(cudaStreamSynchronize(s));
     *failed_domains = *h->status_host;

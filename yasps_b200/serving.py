@@ -137,7 +137,6 @@ class _Slot:
     tables = dict(topo.dev_tables)
     tables.update(self.numeric)
     self.mas, self._keep = create_mas_handle(topo.tables, topo.nv, topo.weights, tables)
-    self.host_x = torch.empty(topo.n, dtype=torch.float64).pin_memory()
     self.ready = torch.cuda.Event()
     owned = [self.values, self.values32, self.g, self.x, self.work, *self.numeric.values()]
     self.nbytes = int(sum(t.numel() * t.element_size() for t in owned))
@@ -215,6 +214,8 @@ class NewtonServer:
     self.launches = 0
     self.passes_run = 0
     self.host_seconds = collections.Counter()    # admit / attach / launch / wait (host time per phase)
+    self.gpu_ms = collections.Counter()          # device time of the PCG launches (CUDA events)
+    self._launch_events = []
 
   # -- resources ------------------------------------------------------------------
   def topology(self, side: int) -> FemTopology:
@@ -303,15 +304,20 @@ class NewtonServer:
     t = time.perf_counter()
     L.call("ys_serve_status", self.handle, self.solve_stream.cuda_stream, self._status)
     self.host_seconds["wait"] += time.perf_counter() - t
+    for e0, e1 in self._launch_events:
+      self.gpu_ms["launch"] += e0.elapsed_time(e1)
+    self._launch_events.clear()
     done = [sid for sid in self._active
             if self._status[sid].phase in (L.YS_SERVE_DONE, L.YS_SERVE_FAILED)]
     if not done:
       return []
+    # the status read synchronised the solve stream: plain copies of the
+    # solutions (no pinned buffers, whose allocation would synchronise the
+    # device while other solves are in flight)
+    sols = {}
     with torch.cuda.stream(self.solve_stream):
       for sid in done:
-        slot = self._active[sid][1]
-        slot.host_x.copy_(slot.x, non_blocking=True)
-    self.solve_stream.synchronize()
+        sols[sid] = self._active[sid][1].x.cpu().numpy()
     t = clock() - t0
     out = []
     for sid in done:
@@ -319,7 +325,7 @@ class NewtonServer:
       st = self._status[sid]
       req.phase, req.iterations, req.refinements = int(st.phase), int(st.iterations), int(st.refinements)
       req.relative_residual = float(st.relative_residual)
-      req.solution = slot.host_x.numpy().copy()
+      req.solution = sols[sid]
       req.t_done = t
       L.call("ys_serve_detach", self.handle, sid)
       self._free_ids.append(sid)
@@ -343,7 +349,11 @@ class NewtonServer:
       self._attach_ready()
       if self._active:
         t = time.perf_counter()
+        e0, e1 = _torch().cuda.Event(enable_timing=True), _torch().cuda.Event(enable_timing=True)
+        e0.record(self.solve_stream)
         L.call("ys_serve_launch", self.handle, self.solve_stream.cuda_stream)
+        e1.record(self.solve_stream)
+        self._launch_events.append((e0, e1))
         self.host_seconds["launch"] += time.perf_counter() - t
         self.launches += 1
         self.passes_run += self.passes
