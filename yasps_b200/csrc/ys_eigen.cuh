@@ -248,12 +248,18 @@ __device__ __forceinline__ void project_negative_modes(double (&a)[N * (N + 1) /
   double vecs[N][N];  // eigenvectors of T for the negative modes (local memory)
   double vout[N][N];  // the same mapped back by Q
   double wts[N];
-  for (int m = 0; m < nneg; ++m) {
+  // The loop runs warp-uniformly to the warp's largest count (lanes past
+  // their own count compute a masked dummy mode): every local-memory access
+  // of an iteration is then at the same offset in all lanes (coalesced).
+  const int mmax = __reduce_max_sync(__activemask(), nneg);
+  for (int m = 0; m < mmax; ++m) {
+    const bool live = m < nneg;
     double lo = -1.0 - 1e-12, hi = 0.0;
     for (int it = 0; it < 56; ++it) {
       const double mid = 0.5 * (lo + hi);
-      if (sturm_count<N>(d, e2, mid) > m) hi = mid;
-      else lo = mid;
+      const bool up = sturm_count<N>(d, e2, mid) > m;
+      hi = up ? mid : hi;
+      lo = up ? lo : mid;
     }
     const double lam = 0.5 * (lo + hi);
     // -- 3. inverse iteration on T - lam I ---------------------------------------
@@ -321,14 +327,14 @@ __device__ __forceinline__ void project_negative_modes(double (&a)[N * (N + 1) /
       for (int i = k + 1; i < N; ++i) y[i] -= t * stash[(RS + refl(k, i)) * stride];
     }
 #pragma unroll
-    for (int i = 0; i < N; ++i) vout[m][i] = y[i];
+    for (int i = 0; i < N; ++i) vout[m][i] = live ? y[i] : 0.0;
     const double l = lam * g;  // original scale
-    wts[m] = method == 1 ? -2.0 * l : -l;
+    wts[m] = live ? (method == 1 ? -2.0 * l : -l) : 0.0;
   }
   // -- 4. A + sum w v v^T ----------------------------------------------------------
 #pragma unroll
   for (int i = 0; i < KS; ++i) a[i] = stash[i * stride];
-  for (int m = 0; m < nneg; ++m) {
+  for (int m = 0; m < mmax; ++m) {
     double y[N];
 #pragma unroll
     for (int i = 0; i < N; ++i) y[i] = vout[m][i];
