@@ -296,6 +296,18 @@ int32_t ys_spmv3(const double* values, const float* values32, const uint32_t* ro
                  const uint32_t* entry_block, const uint32_t* entry_col, uint32_t num_vars,
                  const double* x, double* y, int32_t beta, void* stream);
 
+/* FP32 copy of a 3-vector per variable in 16-byte slots (x, y, z, 0):
+ * x32[4 i + k] = (float)x[3 i + k].  x32 16-byte aligned.  The FP32 PCG keeps
+ * its search direction in this form next to the FP64 one.               */
+int32_t ys_pack_x32(const double* x, uint32_t num_vars, float* x32, void* stream);
+
+/* ys_spmv3 with FP32 blocks reading x from its ys_pack_x32 copy (one 16-byte
+ * load per neighbour instead of three 8-byte ones); the same products as
+ * ys_spmv3 with values32 and the FP64 x.  The SpMV of the FP32 PCG loop. */
+int32_t ys_spmv3_x32(const float* values32, const uint32_t* row_ptr, const uint32_t* entry_block,
+                     const uint32_t* entry_col, uint32_t num_vars, const float* x32, double* y,
+                     int32_t beta, void* stream);
+
 /* ---- preconditioned CG ----------------------------------------------------- */
 
 #define YS_PREC_BLOCK_JACOBI 0

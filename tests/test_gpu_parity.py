@@ -96,7 +96,21 @@ def test_spmv_fp64_and_fp32(c0):
   for transpose in (False, True):
     assert rel(H.spmv(xv, transpose=transpose).get(), ref) <= 1e-12
   H.ensure_fp32()
-  assert rel(H.spmv(xv, fp32=True).get(), ref) <= 1e-5
+  y32 = H.spmv(xv, fp32=True).get()
+  assert rel(y32, ref) <= 1e-5
+  # the float4 copy of x gives the same products in the same order: bit-exact
+  from yasps_b200 import _lib as L
+  nv = H.rows // 3
+  xd = torch.from_numpy(x).cuda()
+  x32 = torch.empty(4 * nv, dtype=torch.float32, device="cuda")
+  y = torch.empty(H.rows, dtype=torch.float64, device="cuda")
+  L.call("ys_pack_x32", L.ptr(xd), nv, L.ptr(x32), L.stream_ptr())
+  assert torch.equal(x32.view(nv, 4)[:, :3], xd.view(nv, 3).float())
+  for k, bs in enumerate(H.block_sets):
+    row_ptr, eb, ec = H.spmv_plan(bs)
+    L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32), L.ptr(y),
+           1 if k else 0, L.stream_ptr())
+  assert np.array_equal(y.cpu().numpy(), y32)
 
 
 def test_block_jacobi_pcg_matches_oracle(c0):

@@ -280,6 +280,7 @@ struct MasPcg {
   double* x;
   double* r;
   double* p;
+  float4* p32;  // FP32 copy of p for the FP32 SpMV, else null
   double* q;
   double* z;
   double* st;
@@ -327,6 +328,7 @@ __global__ void __launch_bounds__(kPcgBlock) mas_init_collect(MasPcg P) {
       v[1] += r * r;
       v[2] += g * g;
     }
+    if (P.p32) P.p32[i] = make_float4((float)z[0], (float)z[1], (float)z[2], 0.0f);
   }
   if (!grid_reduce_last<3>(v, P.partials, P.tickets)) return;
   if (threadIdx.x != 0) return;
@@ -481,7 +483,7 @@ static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGra
 
 cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
                                cudaGraphNode_t* last, uint32_t nv, const double* rhs, double* x, double* r, double* p,
-                               double* q, double* z, double* st, double* partials, unsigned* tickets, const SpmvSet* sets,
+                               float4* p32, double* q, double* z, double* st, double* partials, unsigned* tickets, const SpmvSet* sets,
                                int nsets, int fp32, int stop_rule, int zero_guess, double tolerance, uint32_t max_it,
                                cudaGraphConditionalHandle cond, MasPcgHooks* hooks) {
   auto* h = static_cast<MasHandle*>(mas);
@@ -497,6 +499,7 @@ cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* 
   P->x = x;
   P->r = r;
   P->p = p;
+  P->p32 = p32;
   P->q = q;
   P->z = z;
   P->st = st;

@@ -14,7 +14,7 @@ struct MasPcgHooks {
 // final node.
 cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
                                cudaGraphNode_t* last, uint32_t nv, const double* rhs, double* x, double* r, double* p,
-                               double* q, double* z, double* st, double* partials, unsigned* tickets, const SpmvSet* sets,
+                               float4* p32, double* q, double* z, double* st, double* partials, unsigned* tickets, const SpmvSet* sets,
                                int nsets, int fp32, int stop_rule, int zero_guess, double tolerance, uint32_t max_it,
                                cudaGraphConditionalHandle cond, MasPcgHooks* hooks);
 

@@ -28,6 +28,7 @@ struct PcgParams {
   double* x;
   double* r;
   double* p;
+  float4* p32;  // FP32 copy of p (x, y, z, 0) for the FP32 SpMV, else null
   double* q;
   double* z;
   const double* jinv;
@@ -72,6 +73,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
     P.r[3ull * i] = r0; P.r[3ull * i + 1] = r1; P.r[3ull * i + 2] = r2;
     P.z[3ull * i] = z0; P.z[3ull * i + 1] = z1; P.z[3ull * i + 2] = z2;
     P.p[3ull * i] = z0; P.p[3ull * i + 1] = z1; P.p[3ull * i + 2] = z2;
+    if (P.p32) P.p32[i] = make_float4((float)z0, (float)z1, (float)z2, 0.0f);
     v[0] = r0 * z0 + r1 * z1 + r2 * z2;
     v[1] = r0 * r0 + r1 * r1 + r2 * r2;
     v[2] = g0 * g0 + g1 * g1 + g2 * g2;
@@ -124,7 +126,8 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
   const int lane = (int)(t % kRowLanes);
   double v[1] = {0.0};
   double q0, q1, q2;
-  spmv3_group(P.sets, P.nsets, FP32, i, i < P.nv, lane, P.p, q0, q1, q2);
+  if (FP32) spmv3_group_x32(P.sets, P.nsets, i, i < P.nv, lane, P.p32, q0, q1, q2);
+  else spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.p, q0, q1, q2);
   if (i < P.nv && lane == 0) {
     P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
     v[0] = P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
@@ -192,8 +195,13 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_direction(PcgParams P) {
   if (i >= P.nv) return;
   if (P.st[kStatus] == (double)kNonSpd) return;
   const double beta = P.st[kBeta];
+  double p[3];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) P.p[3ull * i + k] = P.z[3ull * i + k] + P.p[3ull * i + k] * beta;
+  for (int k = 0; k < 3; ++k) {
+    p[k] = P.z[3ull * i + k] + P.p[3ull * i + k] * beta;
+    P.p[3ull * i + k] = p[k];
+  }
+  if (P.p32) P.p32[i] = make_float4((float)p[0], (float)p[1], (float)p[2], 0.0f);
 }
 
 // Iterative refinement step in FP64: x += delta, then r = rhs - H x with the
@@ -269,10 +277,11 @@ extern "C" {
 uint64_t ys_pcg_workspace_doubles(uint32_t n) {
   const uint64_t nv = (n + 2) / 3;
   const uint64_t grid = (nv + ys::kPcgBlock - 1) / ys::kPcgBlock;
-  // r, p, q, z (n each) + slots + partials (4 per block) + tickets
+  // r, p, q, z (n each) + the FP32 copy of p (4 floats per variable) +
+  // slots + partials + tickets
   // partials: up to 4 values per block of the row kernels, or 1 per block of
   // the kRowLanes-per-row SpMV (kRowLanes times more blocks)
-  return 4ull * 3 * nv + ys::kSlots + (uint64_t)ys::kRowLanes * (grid + 2) + 8;
+  return 4ull * 3 * nv + 2 * nv + ys::kSlots + (uint64_t)ys::kRowLanes * (grid + 2) + 8;
 }
 
 int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
@@ -300,6 +309,9 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   P.p = w; w += n;
   P.q = w; w += n;
   P.z = w; w += n;
+  // 12 doubles per variable before it: 16-byte aligned with the workspace
+  P.p32 = P.fp32 ? reinterpret_cast<float4*>(w) : nullptr;
+  w += 2ull * P.nv;
   P.st = w; w += ys::kSlots;
   const unsigned grid = ys::grid_for(P.nv, ys::kPcgBlock);
   const unsigned grid_rows = ys::grid_for((uint64_t)P.nv * ys::kRowLanes, ys::kPcgBlock);
@@ -333,7 +345,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       void* args0[] = {&P};
       e = ys::add_kernel(h->graph, &init, &reset, 1, (const void*)ys::pcg_init_bj, grid, ys::kPcgBlock, args0);
     } else {
-      e = ys::mas_add_init_nodes(a.mas, h->graph, &reset, 1, &init, P.nv, P.rhs, P.x, P.r, P.p, P.q, P.z, P.st, P.partials,
+      e = ys::mas_add_init_nodes(a.mas, h->graph, &reset, 1, &init, P.nv, P.rhs, P.x, P.r, P.p, P.p32, P.q, P.z, P.st, P.partials,
                                  P.tickets, P.sets, P.nsets, P.fp32, P.stop_rule, P.zero_guess, P.tolerance, P.max_it,
                                  P.cond, &h->mas);
     }

@@ -53,6 +53,31 @@ __global__ void __launch_bounds__(256) spmv3_kernel(SpmvSet set, bool fp32, uint
   y[3ull * i + 2] = y2;
 }
 
+// FP32 block values with the float4 copy of x (the layout of the FP32 PCG loop).
+__global__ void __launch_bounds__(256) spmv3_x32_kernel(SpmvSet set, uint32_t nv, const float4* __restrict__ x32,
+                                                        double* __restrict__ y, int beta) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = t / kRowLanes;
+  const int lane = (int)(t % kRowLanes);
+  double y0, y1, y2;
+  spmv3_group_x32(&set, 1, i, i < nv, lane, x32, y0, y1, y2);
+  if (i >= nv || lane != 0) return;
+  if (beta) {
+    y0 += y[3ull * i];
+    y1 += y[3ull * i + 1];
+    y2 += y[3ull * i + 2];
+  }
+  y[3ull * i] = y0;
+  y[3ull * i + 1] = y1;
+  y[3ull * i + 2] = y2;
+}
+
+__global__ void pack_x32_kernel(const double* __restrict__ x, uint32_t nv, float4* __restrict__ x32) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  x32[i] = make_float4((float)x[3ull * i], (float)x[3ull * i + 1], (float)x[3ull * i + 2], 0.0f);
+}
+
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 static size_t spmv_cub_bytes(uint32_t n2, uint32_t nv) {
@@ -127,6 +152,29 @@ int32_t ys_spmv3(const double* values, const float* values32, const uint32_t* ro
   ys::SpmvSet set{values, values32, row_ptr, entry_block, entry_col};
   ys::spmv3_kernel<<<ys::grid_for((uint64_t)num_vars * ys::kRowLanes, 256), 256, 0, (cudaStream_t)stream>>>(
       set, values32 != nullptr, num_vars, x, y, beta);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_pack_x32(const double* x, uint32_t num_vars, float* x32, void* stream) {
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(x32) & 15) == 0, YS_ERR_INVALID, "x32 must be 16-byte aligned");
+  if (num_vars == 0) return YS_OK;
+  ys::pack_x32_kernel<<<ys::grid_for(num_vars, 256), 256, 0, (cudaStream_t)stream>>>(
+      x, num_vars, reinterpret_cast<float4*>(x32));
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_spmv3_x32(const float* values32, const uint32_t* row_ptr, const uint32_t* entry_block,
+                     const uint32_t* entry_col, uint32_t num_vars, const float* x32, double* y, int32_t beta,
+                     void* stream) {
+  YS_REQUIRE(values32 && x32, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(x32) & 15) == 0 && (reinterpret_cast<uintptr_t>(values32) & 15) == 0,
+             YS_ERR_INVALID, "values32 and x32 must be 16-byte aligned");
+  if (num_vars == 0) return YS_OK;
+  ys::SpmvSet set{nullptr, values32, row_ptr, entry_block, entry_col};
+  ys::spmv3_x32_kernel<<<ys::grid_for((uint64_t)num_vars * ys::kRowLanes, 256), 256, 0, (cudaStream_t)stream>>>(
+      set, num_vars, reinterpret_cast<const float4*>(x32), y, beta);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

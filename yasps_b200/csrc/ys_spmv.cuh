@@ -40,6 +40,39 @@ __device__ __forceinline__ void load_block(const float* __restrict__ vals, uint3
   b[8] = v2.x;
 }
 
+// Neighbour vector gather: FP64 x (three scalar loads, rounded to T), or the
+// FP32 copy in 16-byte slots (x, y, z, 0) per variable (one float4 load; the
+// copy holds the same roundings, so both give the same products).
+template <typename T>
+__device__ __forceinline__ void load_x(const double* __restrict__ x, uint32_t j, T (&v)[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = (T)__ldg(x + 3ull * j + k);
+}
+
+__device__ __forceinline__ void load_x(const float4* __restrict__ x, uint32_t j, float (&v)[3]) {
+  const float4 t = __ldg(x + j);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z;
+}
+
+__device__ __forceinline__ float mac(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double mac(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// a += B x (or B^T x for a transposed entry) as explicit fused multiply-add
+// chains: the rounding is fixed by the source, not by how the compiler
+// contracts, so every kernel that gathers a row gets the same bits.
+template <typename T>
+__device__ __forceinline__ void block_mac(const T (&b)[9], const T (&x)[3], bool transposed, T& a0, T& a1, T& a2) {
+  if (transposed) {
+    a0 = mac(b[6], x[2], mac(b[3], x[1], mac(b[0], x[0], a0)));
+    a1 = mac(b[7], x[2], mac(b[4], x[1], mac(b[1], x[0], a1)));
+    a2 = mac(b[8], x[2], mac(b[5], x[1], mac(b[2], x[0], a2)));
+  } else {
+    a0 = mac(b[2], x[2], mac(b[1], x[1], mac(b[0], x[0], a0)));
+    a1 = mac(b[5], x[2], mac(b[4], x[1], mac(b[3], x[0], a1)));
+    a2 = mac(b[8], x[2], mac(b[7], x[1], mac(b[6], x[0], a2)));
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void spmv3_row_accumulate(const T* __restrict__ vals, const uint32_t* __restrict__ row_ptr,
                                                      const uint32_t* __restrict__ eblock,
@@ -51,20 +84,10 @@ __device__ __forceinline__ void spmv3_row_accumulate(const T* __restrict__ vals,
   for (uint32_t e = e0; e < e1; ++e) {
     const uint32_t eb = __ldg(eblock + e);
     const uint32_t j = __ldg(ecol + e);
-    T bv[9];
+    T bv[9], xv[3];
     load_block(vals, eb & 0x7fffffffu, bv);
-    const T x0 = (T)__ldg(x + 3ull * j), x1 = (T)__ldg(x + 3ull * j + 1), x2 = (T)__ldg(x + 3ull * j + 2);
-    const T b0 = bv[0], b1 = bv[1], b2 = bv[2], b3 = bv[3], b4 = bv[4], b5 = bv[5], b6 = bv[6], b7 = bv[7],
-            b8 = bv[8];
-    if (eb & 0x80000000u) {
-      a0 += b0 * x0 + b3 * x1 + b6 * x2;
-      a1 += b1 * x0 + b4 * x1 + b7 * x2;
-      a2 += b2 * x0 + b5 * x1 + b8 * x2;
-    } else {
-      a0 += b0 * x0 + b1 * x1 + b2 * x2;
-      a1 += b3 * x0 + b4 * x1 + b5 * x2;
-      a2 += b6 * x0 + b7 * x1 + b8 * x2;
-    }
+    load_x(x, j, xv);
+    block_mac(bv, xv, (eb & 0x80000000u) != 0, a0, a1, a2);
   }
   y0 += (double)a0;
   y1 += (double)a1;
@@ -77,11 +100,11 @@ __device__ __forceinline__ void spmv3_row_accumulate(const T* __restrict__ vals,
 // shuffles: a row beyond the matrix passes an empty entry range.
 constexpr int kRowLanes = 8;
 
-template <typename T>
+template <typename T, typename X>
 __device__ __forceinline__ void spmv3_group_accumulate(const T* __restrict__ vals, uint32_t e0, uint32_t e1,
                                                        const uint32_t* __restrict__ eblock,
                                                        const uint32_t* __restrict__ ecol, int lane,
-                                                       const double* __restrict__ x, double& y0, double& y1,
+                                                       const X* __restrict__ x, double& y0, double& y1,
                                                        double& y2) {
   T a0 = 0, a1 = 0, a2 = 0;
   // Two entries per iteration (e and e + kRowLanes): both index loads, then
@@ -92,34 +115,15 @@ __device__ __forceinline__ void spmv3_group_accumulate(const T* __restrict__ val
     const uint32_t ebA = __ldg(eblock + e), jA = __ldg(ecol + e);
     const uint32_t ebB = two ? __ldg(eblock + f) : ebA, jB = two ? __ldg(ecol + f) : jA;
     T xa[3], xb[3], ba[9], bb[9];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      xa[k] = (T)__ldg(x + 3ull * jA + k);
-      xb[k] = (T)__ldg(x + 3ull * jB + k);
-    }
+    load_x(x, jA, xa);
+    load_x(x, jB, xb);
     load_block(vals, ebA & 0x7fffffffu, ba);
     load_block(vals, ebB & 0x7fffffffu, bb);
     const T wB = two ? (T)1 : (T)0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) xb[k] *= wB;
-    if (ebA & 0x80000000u) {
-      a0 += ba[0] * xa[0] + ba[3] * xa[1] + ba[6] * xa[2];
-      a1 += ba[1] * xa[0] + ba[4] * xa[1] + ba[7] * xa[2];
-      a2 += ba[2] * xa[0] + ba[5] * xa[1] + ba[8] * xa[2];
-    } else {
-      a0 += ba[0] * xa[0] + ba[1] * xa[1] + ba[2] * xa[2];
-      a1 += ba[3] * xa[0] + ba[4] * xa[1] + ba[5] * xa[2];
-      a2 += ba[6] * xa[0] + ba[7] * xa[1] + ba[8] * xa[2];
-    }
-    if (ebB & 0x80000000u) {
-      a0 += bb[0] * xb[0] + bb[3] * xb[1] + bb[6] * xb[2];
-      a1 += bb[1] * xb[0] + bb[4] * xb[1] + bb[7] * xb[2];
-      a2 += bb[2] * xb[0] + bb[5] * xb[1] + bb[8] * xb[2];
-    } else {
-      a0 += bb[0] * xb[0] + bb[1] * xb[1] + bb[2] * xb[2];
-      a1 += bb[3] * xb[0] + bb[4] * xb[1] + bb[5] * xb[2];
-      a2 += bb[6] * xb[0] + bb[7] * xb[1] + bb[8] * xb[2];
-    }
+    block_mac(ba, xa, (ebA & 0x80000000u) != 0, a0, a1, a2);
+    block_mac(bb, xb, (ebB & 0x80000000u) != 0, a0, a1, a2);
   }
 #pragma unroll
   for (int o = kRowLanes / 2; o > 0; o >>= 1) {
@@ -147,6 +151,18 @@ __device__ __forceinline__ void spmv3_group(const SpmvSet* sets, int nsets, bool
     else
       spmv3_group_accumulate<double>(sets[s].values, e0, e1, sets[s].entry_block, sets[s].entry_col, lane, x, y0,
                                      y1, y2);
+  }
+}
+
+// FP32 group version reading the float4 copy of x.
+__device__ __forceinline__ void spmv3_group_x32(const SpmvSet* sets, int nsets, uint32_t i, bool valid, int lane,
+                                                const float4* __restrict__ x32, double& y0, double& y1, double& y2) {
+  y0 = y1 = y2 = 0.0;
+  for (int s = 0; s < nsets; ++s) {
+    const uint32_t e0 = valid ? sets[s].row_ptr[i] : 0u;
+    const uint32_t e1 = valid ? sets[s].row_ptr[i + 1] : 0u;
+    spmv3_group_accumulate<float>(sets[s].values32, e0, e1, sets[s].entry_block, sets[s].entry_col, lane, x32, y0, y1,
+                                  y2);
   }
 }
 

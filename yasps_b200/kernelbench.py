@@ -86,6 +86,8 @@ def main():
   y = torch.zeros_like(x)
   z = torch.zeros_like(x)
   nv = H.rows // 3
+  x32 = torch.empty(4 * nv, dtype=torch.float32, device="cuda")
+  L.call("ys_pack_x32", L.ptr(x), nv, L.ptr(x32), st)
 
   def snh_eval(method):
     snh.projection_method = method
@@ -102,6 +104,8 @@ def main():
                                   L.ptr(x), L.ptr(y), 0, st),
       "spmv_fp32": lambda: L.call("ys_spmv3", None, L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv,
                                   L.ptr(x), L.ptr(y), 0, st),
+      "spmv_fp32_x32": lambda: L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv,
+                                      L.ptr(x32), L.ptr(y), 0, st),
       "mas_apply": lambda: L.call("ys_mas_apply", mas._mas, L.ptr(x), L.ptr(z), st),
       "gemv": lambda: L.call("ys_mas_gemv", mas._mas, st, None),
       "newton_step": lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
