@@ -369,7 +369,9 @@ typedef struct ys_mas_desc {
   uint32_t num_domains;
   const uint32_t* dom_node_ptr;        /* [num_domains+1]                             */
   const uint32_t* dom_nodes;           /* packed node ids, local order                 */
-  const uint64_t* inv_offset;          /* [num_domains] float offset of each inverse   */
+  const uint64_t* inv_offset;          /* [num_domains] float offset of each inverse,  */
+                                       /* a multiple of 4; ys_mas_inverse_floats(3 * */
+                                       /* domain nodes) floats each                    */
   const uint32_t* dom_entry_ptr;       /* [num_domains+1]                             */
   const uint32_t* dom_entry;           /* [3 * entries] (local i, local j, level block) */
   uint32_t fine_blocks;                /* level-0 blocks = the static 3x3 upper blocks */
@@ -379,12 +381,20 @@ typedef struct ys_mas_desc {
   const uint32_t* cb_level_begin;      /* host [num_levels+1] coarse block ranges       */
   uint32_t max_domain_dofs;            /* <= 128                                      */
   double* coarse_values;               /* [coarse_blocks * 9] scratch                  */
-  float* inverse;                      /* FP32 domain inverses                         */
+  float* inverse;                      /* FP32 domain inverses (4x4 tile layout below) */
   float* level_residual;               /* [3 * packed nodes] scratch                   */
   float* level_correction;             /* [3 * packed nodes] scratch                   */
   int32_t* status;                     /* [1] scratch                                  */
   double* level_residual64;            /* [3 * packed nodes] scratch (FP64 restriction) */
 } ys_mas_desc;
+
+/* Floats of one domain's FP32 inverse: the n x n inverse padded to 4T rows
+ * (T = ceil(n/4) rounded up to even; zero padding) stored as its upper 4x4
+ * tiles (A <= B, diagonal tiles in full), 16 floats a tile, row-major in the
+ * tile; tile (A, B) at slot A (T+1) + B - A for A < T/2, else at
+ * q (T+1) + T - q + B - A with q = T-1-A (the triangle folded into a
+ * T/2 x (T+1) rectangle).  Equals 8 T (T+1).  Host function.             */
+uint64_t ys_mas_inverse_floats(uint32_t dofs);
 
 int32_t ys_mas_create(const ys_mas_desc* desc, void** handle);
 /* Level Galerkin sums and FP64 Gauss-Jordan inverses of every domain from

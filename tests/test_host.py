@@ -121,3 +121,40 @@ def test_serve_entry_points_validate_without_gpu():
   assert lib.ys_serve_create(8, 0, ctypes.byref(h)) == L.YS_ERR_INVALID
   assert lib.ys_serve_attach(None, 0, None) == L.YS_ERR_INVALID
   assert lib.ys_serve_workspace_doubles(1000) >= 15 * 1000
+
+
+def test_mas_tile_layout_host_math():
+  """The tiled FP32 inverse layout: the Python size formula equals the
+  library's, the folded tile order is a bijection onto [0, T(T+1)/2) that the
+  GEMV inverts with its float quotient, and its partial grid rows are read
+  without shared-memory bank conflicts."""
+  from yasps_b200 import _lib
+  from yasps_b200.mas_hierarchy import inverse_floats
+  lib = _lib.load()
+  for n in range(3, 129, 3):
+    t = (n + 3) // 4
+    t += t & 1
+    assert inverse_floats(n) == lib.ys_mas_inverse_floats(n) == 16 * t * (t + 1) // 2
+    assert 4 * t <= (96 if n <= 96 else 128)  # inside the inverse kernel's register tile
+
+    def slot(a, b):
+      if a < t // 2:
+        return a * (t + 1) + (b - a)
+      q = t - 1 - a
+      return q * (t + 1) + (t - q) + (b - a)
+
+    slots = sorted(slot(a, b) for a in range(t) for b in range(a, t))
+    assert slots == list(range(t * (t + 1) // 2))
+    inv_w = np.float32(1.0) / np.float32(t + 1)
+    for a in range(t):
+      for b in range(a, t):
+        s = slot(a, b)
+        q = int((np.float32(s) + np.float32(0.5)) * inv_w)
+        c = s - q * (t + 1)
+        first = c < t - q
+        assert (q if first else t - 1 - q) == a
+        assert ((q + c) if first else a + (c - (t - q))) == b
+    ld = (t + 6) // 8 * 8 + 1
+    assert ld >= t and ld % 8 == 1
+    banks = {((i // 4) * ld * 4 + i % 4) % 32 for i in range(32)}
+    assert len(banks) == 32

@@ -124,6 +124,7 @@ SIGNATURES = {
     "ys_spmv_plan_workspace_bytes": (i32, [u32, u32, P(u64)]),
     "ys_spmv_plan_build": (i32, [vp, u32, u32, vp, u64, vp, vp, vp, vp]),
     "ys_spmv3": (i32, [vp, vp, vp, vp, vp, u32, vp, vp, i32, vp]),
+    "ys_mas_inverse_floats": (u64, [u32]),
     "ys_pack_x32": (i32, [vp, u32, vp, vp]),
     "ys_spmv3_x32": (i32, [vp, vp, vp, vp, u32, vp, vp, i32, vp]),
     "ys_pcg_workspace_doubles": (u64, [u32]),

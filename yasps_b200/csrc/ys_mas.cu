@@ -226,16 +226,23 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
     __syncthreads();
   }
   if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
-  // FP32 upper triangle, row-major packed (row i holds columns i..n-1),
-  // straight from the register tiles (the upper entries of the inverse).
+  // FP32 upper 4x4 tiles (inv_tile_slot order), straight from the register
+  // tiles; the padding rows and columns up to 4 * inv_tiles(n) are zero.
   float* out = M.inverse + M.inv_offset[d];
+  const uint32_t nt = inv_tiles(n);
 #pragma unroll
-  for (int a = 0; a < T; ++a)
+  for (int a = 0; a < T; ++a) {
+    const uint32_t i = ty + 16 * a;
+    const uint32_t rb = inv_tile_rowbase(nt, i >> 2);
 #pragma unroll
     for (int b = 0; b < T; ++b) {
-      const uint32_t i = ty + 16 * a, j = tx + 16 * b;
-      if (i < n && j < n && j >= i) out[i * n - i * (i - 1) / 2 + (j - i)] = (float)(R[a][b] * dinv[i] * dinv[j]);
+      const uint32_t j = tx + 16 * b;
+      if (i < 4 * nt && j < 4 * nt && (i >> 2) <= (j >> 2)) {
+        const float v = (i < n && j < n) ? (float)(R[a][b] * dinv[i] * dinv[j]) : 0.0f;
+        out[16u * (rb + (j >> 2)) + 4 * (i & 3) + (j & 3)] = v;
+      }
     }
+  }
 }
 
 // Level 0: a thread per node; levels >= 1: a warp per node.
@@ -649,18 +656,21 @@ int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
   return YS_OK;
 }
 
+uint64_t ys_mas_inverse_floats(uint32_t dofs) { return ys::inv_floats(dofs); }
+
 int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes) {
   YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
   auto* h = static_cast<ys::MasHandle*>(handle);
   ys::MasDev& M = h->M;
   if (algorithmic_bytes) {
-    // every packed FP32 inverse read once + the gathered residual and the correction
+    // every tiled FP32 inverse read once + the gathered residual, the node
+    // ids and the correction
     std::vector<uint32_t> ptr(M.num_domains + 1);
     cudaMemcpy(ptr.data(), M.dom_node_ptr, sizeof(uint32_t) * (M.num_domains + 1), cudaMemcpyDeviceToHost);
     uint64_t bytes = 0;
     for (uint32_t d = 0; d < M.num_domains; ++d) {
-      const uint64_t n = 3ull * (ptr[d + 1] - ptr[d]);
-      bytes += 4 * ((n * (n + 1) / 2 + 3) / 4 * 4) + 4 * n + 4 * n + 4 * (n / 3);
+      const uint32_t n = 3u * (ptr[d + 1] - ptr[d]);
+      bytes += 4 * ys::inv_floats(n) + 4ull * n + 4ull * n + 4ull * (n / 3);
     }
     *algorithmic_bytes = bytes;
   }

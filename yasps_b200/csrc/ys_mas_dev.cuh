@@ -100,52 +100,122 @@ __host__ __device__ inline uint32_t restrict_tail_first(const MasDev& M) {
   return first;
 }
 
-// z_d = A_d^-1 r_d for domain d by one CTA.  The FP32 inverse is stored as
-// its packed upper triangle (n(n+1)/2 floats from a 16-byte aligned offset):
-// it is staged in shared memory with coalesced 16-byte loads, so every byte
-// crosses HBM once and half as many bytes cross as for a full n x n inverse.
-// Thread i owns output row i; S(i, j) for j < i is read from column i of the
-// upper triangle (consecutive threads, consecutive words).
-__host__ __device__ inline uint32_t gemv_rloc_offset(uint32_t max_dofs) {
-  return (max_dofs * (max_dofs + 1) / 2 + 3) & ~3u;
+// FP32 domain inverses are stored as 4x4 tiles: the n x n inverse is padded
+// to 4T rows (T = ceil(n / 4) rounded up to even, zero padding) and its upper
+// tiles (A <= B, diagonal tiles in full) are kept, 16 floats a tile, row-major
+// inside the tile.  Tile order folds the triangle into a T/2 x (T+1)
+// rectangle: rectangle row q holds tile row q (B = q..T-1) followed by tile
+// row T-1-q, so a tile's slot and its (A, B) convert with one division.
+__host__ __device__ inline uint32_t inv_tiles(uint32_t n) {
+  const uint32_t t = (n + 3) / 4;
+  return t + (t & 1u);
 }
-inline size_t gemv_smem_bytes(uint32_t max_dofs) { return 4ull * (gemv_rloc_offset(max_dofs) + max_dofs); }
+__host__ __device__ inline uint64_t inv_floats(uint32_t n) {
+  const uint64_t t = inv_tiles(n);
+  return 8ull * t * (t + 1);
+}
+// slot of tile (A, B) = inv_tile_rowbase(T, A) + B
+__host__ __device__ inline uint32_t inv_tile_rowbase(uint32_t T, uint32_t A) {
+  if (A < T / 2) return A * T;
+  const uint32_t q = T - 1 - A;
+  return q * (T + 1) + (T - q) - A;
+}
+__host__ __device__ inline uint32_t inv_tile_slot(uint32_t T, uint32_t A, uint32_t B) {
+  return inv_tile_rowbase(T, A) + B;
+}
+// Row stride (in float4) of the partial-product grid: >= T and 1 mod 8, so
+// the reads of the final row sums and the transposed writes are free of
+// shared-memory bank conflicts.
+__host__ __device__ inline uint32_t gemv_partial_ld(uint32_t T) { return (T + 6) / 8 * 8 + 1; }
+inline size_t gemv_smem_bytes(uint32_t max_dofs) {
+  const uint32_t T = inv_tiles(max_dofs);
+  return 16ull * (T * gemv_partial_ld(T) + T);
+}
 
+// Products of one tile (A, B) (slot `slot`, rows t0..t3) with the staged
+// residual: T_AB r_B into cell (A, B) and, off the diagonal, T_AB^T r_A into
+// cell (B, A) of the partial grid.
+__device__ __forceinline__ void gemv_tile(uint32_t T, uint32_t ld, uint32_t slot, const float4 (&t)[4],
+                                          const float4* r4, float4* part) {
+  // slot = q (T + 1) + c; the +0.5 keeps the float quotient off integers
+  const uint32_t q = (uint32_t)(((float)slot + 0.5f) * (1.0f / (float)(T + 1)));
+  const uint32_t c = slot - q * (T + 1);
+  const bool first = c < T - q;
+  const uint32_t A = first ? q : T - 1 - q;
+  const uint32_t B = first ? q + c : A + (c - (T - q));
+  const float4 rb = r4[B];
+  float4 u;
+  u.x = fmaf(t[0].w, rb.w, fmaf(t[0].z, rb.z, fmaf(t[0].y, rb.y, t[0].x * rb.x)));
+  u.y = fmaf(t[1].w, rb.w, fmaf(t[1].z, rb.z, fmaf(t[1].y, rb.y, t[1].x * rb.x)));
+  u.z = fmaf(t[2].w, rb.w, fmaf(t[2].z, rb.z, fmaf(t[2].y, rb.y, t[2].x * rb.x)));
+  u.w = fmaf(t[3].w, rb.w, fmaf(t[3].z, rb.z, fmaf(t[3].y, rb.y, t[3].x * rb.x)));
+  part[A * ld + B] = u;
+  if (A != B) {
+    const float4 ra = r4[A];
+    float4 v;
+    v.x = fmaf(t[3].x, ra.w, fmaf(t[2].x, ra.z, fmaf(t[1].x, ra.y, t[0].x * ra.x)));
+    v.y = fmaf(t[3].y, ra.w, fmaf(t[2].y, ra.z, fmaf(t[1].y, ra.y, t[0].y * ra.x)));
+    v.z = fmaf(t[3].z, ra.w, fmaf(t[2].z, ra.z, fmaf(t[1].z, ra.y, t[0].z * ra.x)));
+    v.w = fmaf(t[3].w, ra.w, fmaf(t[2].w, ra.z, fmaf(t[1].w, ra.y, t[0].w * ra.x)));
+    part[B * ld + A] = v;
+  }
+}
+
+// Tiles a thread loads before the residual is staged (their HBM reads
+// overlap the residual gather).
+constexpr int kGemvPrefetch = 3;
+
+// z_d = A_d^-1 r_d for domain d by one CTA.  A thread takes whole tiles
+// (four coalesced 16-byte loads straight from HBM, every byte read once):
+// tile (A, B) gives T_AB r_B for output tile row A and, off the diagonal,
+// T_AB^T r_A for output tile row B.  Every (output row, source tile) pair is
+// produced by exactly one tile, into its own cell of a shared-memory grid,
+// and each output entry sums its grid row in a fixed order: deterministic.
 __device__ __forceinline__ void gemv_domain(const MasDev& M, uint32_t d, float4* smem) {
-  float* S = reinterpret_cast<float*>(smem);
-  float* rloc = S + gemv_rloc_offset(M.max_dofs);
   const uint32_t nb = M.dom_node_ptr[d], nn = M.dom_node_ptr[d + 1] - nb;
   const uint32_t n = 3 * nn;
-  const uint32_t packed4 = (n * (n + 1) / 2 + 3) / 4;
+  const uint32_t T = inv_tiles(n);
+  const uint32_t ld = gemv_partial_ld(T);
+  const uint32_t tiles = T * (T + 1) / 2;
+  float4* part = smem;         // [T][ld] partial products
+  float4* r4 = smem + T * ld;  // r_d, zero beyond n
   const float4* src = reinterpret_cast<const float4*>(M.inverse + M.inv_offset[d]);
-  for (uint32_t t = threadIdx.x; t < packed4; t += blockDim.x) smem[t] = __ldg(src + t);
-  for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
-    const uint32_t node = M.dom_nodes[nb + t / 3];
-    rloc[t] = M.rl[3ull * node + t % 3];
+  float4 pre[kGemvPrefetch][4];
+#pragma unroll
+  for (int k = 0; k < kGemvPrefetch; ++k) {
+    const uint32_t slot = threadIdx.x + k * blockDim.x;
+    if (slot < tiles) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) pre[k][m] = __ldg(src + 4ull * slot + m);
+    }
+  }
+  float* rloc = reinterpret_cast<float*>(r4);
+  for (uint32_t t = threadIdx.x; t < 4 * T; t += blockDim.x) {
+    float v = 0.0f;
+    if (t < n) v = M.rl[3ull * M.dom_nodes[nb + t / 3] + t % 3];
+    rloc[t] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kGemvPrefetch; ++k) {
+    const uint32_t slot = threadIdx.x + k * blockDim.x;
+    if (slot < tiles) gemv_tile(T, ld, slot, pre[k], r4, part);
+  }
+  for (uint32_t slot = threadIdx.x + kGemvPrefetch * blockDim.x; slot < tiles; slot += blockDim.x) {
+    float4 t[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) t[m] = __ldg(src + 4ull * slot + m);
+    gemv_tile(T, ld, slot, t, r4, part);
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    const uint32_t bi = i * n - i * (i - 1) / 2 - i;  // S(i, j) = S[bi + j], j >= i
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    uint32_t bj = 0;  // start of packed row j
-    uint32_t j = 0;
-    for (; j + 4 <= n; j += 4) {
-#pragma unroll
-      for (uint32_t u = 0; u < 4; ++u) {
-        const uint32_t jj = j + u;
-        const uint32_t idx = jj < i ? bj + (i - jj) : bi + jj;
-        acc[u] += S[idx] * rloc[jj];
-        bj += n - jj;
-      }
+    const float* row = reinterpret_cast<const float*>(part + (i / 4) * ld) + (i % 4);
+    float s0 = 0.0f, s1 = 0.0f;
+    for (uint32_t y = 0; y < T; y += 2) {  // T is even
+      s0 += row[4 * y];
+      s1 += row[4 * y + 4];
     }
-    for (; j < n; ++j) {
-      const uint32_t idx = j < i ? bj + (i - j) : bi + j;
-      acc[0] += S[idx] * rloc[j];
-      bj += n - j;
-    }
-    const float s = (acc[0] + acc[1]) + (acc[2] + acc[3]);
-    const uint32_t node = M.dom_nodes[nb + i / 3];
-    M.zl[3ull * node + i % 3] = s;
+    M.zl[3ull * M.dom_nodes[nb + i / 3] + i % 3] = s0 + s1;
   }
 }
 

@@ -175,6 +175,15 @@ class MasTables:
   inverse_floats: int
 
 
+def inverse_floats(dofs: int) -> int:
+  """FP32 floats of one domain's tiled inverse: the upper 4x4 tiles of the
+  inverse padded to T = ceil(dofs / 4) (rounded up to even) tile rows,
+  16 floats a tile (``ys_mas_inverse_floats``)."""
+  t = (dofs + 3) // 4
+  t += t & 1
+  return 8 * t * (t + 1)
+
+
 def _step_map(h: Hierarchy, l: int, counts, nv) -> np.ndarray:
   """Map of level l-1 node ids to level l node ids (composed[l] = step o composed[l-1])."""
   if l == 1:
@@ -224,7 +233,7 @@ def build_tables(h: Hierarchy, fine_positions: np.ndarray) -> MasTables:
       dom_ptr.append(dom_ptr[-1] + dom.size)
       inv_off.append(cursor)
       k = 3 * dom.size
-      cursor += (k * (k + 1) // 2 + 3) // 4 * 4  # packed upper triangle, 16-byte aligned
+      cursor += inverse_floats(k)
       max_dofs = max(max_dofs, 3 * dom.size)
     node_dom.append(nd)
     node_loc.append(nl)
