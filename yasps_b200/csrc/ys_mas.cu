@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(1024) mas_restrict_tail(MasDev M, const double
   restrict_tail_levels(M, r, first);
 }
 
-__global__ void __launch_bounds__(128) mas_gemv(MasDev M) {
+__global__ void __launch_bounds__(kGemvThreads) mas_gemv(MasDev M) {
   extern __shared__ float4 gemv_smem[];
   gemv_domain(M, blockIdx.x, gemv_smem);
 }
@@ -483,7 +483,7 @@ static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGra
   if (e != cudaSuccess) return e;
   cudaGraphNode_t n2 = nullptr;
   void* a2[] = {&m};
-  e = add_kernel(g, &n2, dp, nd, (const void*)mas_gemv, M.num_domains, 128, (unsigned)gemv_smem_bytes(M.max_dofs), a2);
+  e = add_kernel(g, &n2, dp, nd, (const void*)mas_gemv, M.num_domains, kGemvThreads, (unsigned)gemv_smem_bytes(M.max_dofs), a2);
   *last = n2;
   return e;
 }
@@ -645,7 +645,7 @@ int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
     ys::mas_restrict<<<ys::restrict_grid(l, cnt), 256, 0, s>>>(M, r, l);
     YS_CHECK_LAUNCH();
   }
-  ys::mas_gemv<<<M.num_domains, 128, ys::gemv_smem_bytes(M.max_dofs), s>>>(M);
+  ys::mas_gemv<<<M.num_domains, ys::kGemvThreads, ys::gemv_smem_bytes(M.max_dofs), s>>>(M);
   YS_CHECK_LAUNCH();
   ys::MasPcg P{};
   P.M = M;
@@ -674,7 +674,7 @@ int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes) {
     }
     *algorithmic_bytes = bytes;
   }
-  ys::mas_gemv<<<M.num_domains, 128, ys::gemv_smem_bytes(M.max_dofs), (cudaStream_t)stream>>>(M);
+  ys::mas_gemv<<<M.num_domains, ys::kGemvThreads, ys::gemv_smem_bytes(M.max_dofs), (cudaStream_t)stream>>>(M);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

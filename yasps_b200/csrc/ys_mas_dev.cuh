@@ -161,9 +161,11 @@ __device__ __forceinline__ void gemv_tile(uint32_t T, uint32_t ld, uint32_t slot
   }
 }
 
-// Tiles a thread loads before the residual is staged (their HBM reads
-// overlap the residual gather).
-constexpr int kGemvPrefetch = 3;
+// Threads of a domain-GEMV CTA, and the tiles a thread loads before the
+// residual is staged (their HBM reads overlap the residual gather); 160 x 2
+// covers the 300 tiles of a 96-DoF domain.
+constexpr int kGemvThreads = 160;
+constexpr int kGemvPrefetch = 2;
 
 // z_d = A_d^-1 r_d for domain d by one CTA.  A thread takes whole tiles
 // (four coalesced 16-byte loads straight from HBM, every byte read once):

@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(1024) serve_tail(const ServeDev* __restrict__ 
   restrict_tail_levels(T.M, T.r, T.first_tail);
 }
 
-__global__ void __launch_bounds__(128) serve_gemv(const ServeDev* __restrict__ S) {
+__global__ void __launch_bounds__(kGemvThreads) serve_gemv(const ServeDev* __restrict__ S) {
   extern __shared__ float4 serve_smem[];
   uint32_t s, d;
   if (!map_entry(S->map_gemv, S->n_gemv, s, d) || !mas_live(S, s)) return;
@@ -400,7 +400,7 @@ static cudaError_t build_graph(ServeHandle* h, const Bucket& k, cudaGraphExec_t*
       if (k.restrict_cap[l])
         e = add_node(g, &n, &prev, (const void*)serve_restrict, k.restrict_cap[l], kPcgBlock, 0, al[l]);
     if (e == cudaSuccess) e = add_node(g, &n, &prev, (const void*)serve_tail, k.tail, 1024, 0, a);
-    if (e == cudaSuccess) e = add_node(g, &n, &prev, (const void*)serve_gemv, k.gemv, 128, k.smem, a);
+    if (e == cudaSuccess) e = add_node(g, &n, &prev, (const void*)serve_gemv, k.gemv, kGemvThreads, k.smem, a);
     if (e == cudaSuccess) e = add_node(g, &n, &prev, (const void*)serve_collect, k.rows, kPcgBlock, 0, a);
     if (e == cudaSuccess) e = add_node(g, &n, &prev, (const void*)serve_direction, k.rows, kPcgBlock, 0, a);
   }
