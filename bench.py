@@ -250,9 +250,15 @@ def gpu_arm(args):
   gemv_ms = e0.elapsed_time(e1) / reps
   hbm, peak_kind = peaks()
   achieved = nbytes.value / (gemv_ms / 1e3) / 1e9
+  # DRAM traffic per launch from an ncu capture of the 56^3 cube (109.60 MB
+  # read + 4.24 MB written; its tiled layout holds GEMV_LAYOUT_56 bytes),
+  # scaled by this launch's layout bytes (traffic grows with the domains)
+  from yasps_b200.kernelbench import gemv_layout_bytes
+  traffic = (109.60e6 + 4.24e6) / GEMV_LAYOUT_56 * gemv_layout_bytes(ms_solver._tables)
   roofline = {"kernel": "mas_gemv (MAS domain-inverse apply, FP32)", "bound": "hbm", "achieved": achieved,
               "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-              "traffic": None, "bytes_per_launch": int(nbytes.value), "ms_per_launch": gemv_ms}
+              "traffic": traffic, "bytes_per_launch": int(nbytes.value), "ms_per_launch": gemv_ms}
+  roofline_spmv = spmv_roofline(mz.activeHessian(), hbm, peak_kind)
   cpu = None
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
     cpu = cpu_baseline_leg(cube, args.tol)
@@ -273,12 +279,52 @@ def gpu_arm(args):
           "fp64": {"value": fp64_value, "unit": "solves/s", "iterations": int(stats64["iterations"])},
           "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * cube.dofs,
                   "d2h_bytes_per_step": 8 * cube.dofs},
-          "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline, "clocks": clk,
+          "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
+          "roofline_spmv": roofline_spmv, "clocks": clk,
           "cpu_baseline": cpu, "serving": serve, "cloth_contact": cloth}
   if rank == 0:
     print(json.dumps(line), flush=True)
   if pg is not None:
     pg.destroy_process_group()
+
+
+GEMV_LAYOUT_56 = 111_651_744  # tiled-layout bytes of one domain-GEMV launch on the 56^3 cube
+
+
+def spmv_roofline(H, hbm, peak_kind, reps=50):
+  """The FP32 block SpMV of the PCG loop (FP32 blocks, float4 copy of the
+  direction) timed alone with CUDA events.  Algorithmic bytes: 9 floats per
+  stored upper block, (block, column) indices and the row pointer, x read
+  once (3 floats a variable) and y written once (3 doubles)."""
+  import torch
+  from yasps_b200 import _lib as L
+  bs = H.block_sets[0]
+  row_ptr, eb, ec = H.spmv_plan(bs)
+  nv = H.rows // 3
+  entries = int(row_ptr[-1].item())
+  x = torch.cos(torch.arange(H.rows, dtype=torch.float64, device="cuda") * 0.37)
+  x32 = torch.empty(4 * nv, dtype=torch.float32, device="cuda")
+  y = torch.empty_like(x)
+  s = torch.cuda.current_stream()
+  L.call("ys_pack_x32", L.ptr(x), nv, L.ptr(x32), s.cuda_stream)
+  call = lambda: L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32),
+                        L.ptr(y), 0, s.cuda_stream)
+  for _ in range(3):
+    call()
+  torch.cuda.synchronize()
+  e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  e0.record(s)
+  for _ in range(reps):
+    call()
+  e1.record(s)
+  torch.cuda.synchronize()
+  ms = e0.elapsed_time(e1) / reps
+  nbytes = 36 * bs.pattern.num_unique + 8 * entries + 4 * (nv + 1) + 12 * nv + 24 * nv
+  achieved = nbytes / (ms / 1e3) / 1e9
+  return {"kernel": "spmv3_x32 (symmetric 3x3 block SpMV, FP32 blocks)", "bound": "hbm", "achieved": achieved,
+          "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+          "bytes_per_launch": nbytes, "ms_per_launch": ms, "stored_blocks": bs.pattern.num_unique,
+          "entries": entries}
 
 
 def launches_per_newton_step(impl, its, refs):

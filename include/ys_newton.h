@@ -408,7 +408,8 @@ int32_t ys_mas_destroy(void* handle);
 /* The domain-GEMV stage of ys_mas_apply alone, on the level residuals of the
  * last apply (used to time the preconditioner's dominant kernel).  When
  * algorithmic_bytes is not NULL it receives the bytes one launch must move
- * (inverses + gathered residuals + corrections); that query synchronises. */
+ * (the n(n+1)/2 distinct FP32 entries of every inverse + gathered residuals,
+ * node ids and corrections); that query synchronises.                     */
 int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes);
 
 /* ---- extras -------------------------------------------------------------- */

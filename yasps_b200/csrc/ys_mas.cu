@@ -663,14 +663,15 @@ int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes) {
   auto* h = static_cast<ys::MasHandle*>(handle);
   ys::MasDev& M = h->M;
   if (algorithmic_bytes) {
-    // every tiled FP32 inverse read once + the gathered residual, the node
-    // ids and the correction
+    // the distinct entries of every FP32 inverse (its upper triangle, read
+    // once) + the gathered residual, the node ids and the correction; the
+    // tile layout reads ~3 % more (padding, full diagonal tiles)
     std::vector<uint32_t> ptr(M.num_domains + 1);
     cudaMemcpy(ptr.data(), M.dom_node_ptr, sizeof(uint32_t) * (M.num_domains + 1), cudaMemcpyDeviceToHost);
     uint64_t bytes = 0;
     for (uint32_t d = 0; d < M.num_domains; ++d) {
-      const uint32_t n = 3u * (ptr[d + 1] - ptr[d]);
-      bytes += 4 * ys::inv_floats(n) + 4ull * n + 4ull * n + 4ull * (n / 3);
+      const uint64_t n = 3ull * (ptr[d + 1] - ptr[d]);
+      bytes += 4 * (n * (n + 1) / 2) + 4 * n + 4 * n + 4 * (n / 3);
     }
     *algorithmic_bytes = bytes;
   }

@@ -14,6 +14,8 @@ import argparse
 import ctypes
 import json
 
+import numpy as np
+
 import torch
 
 from . import _lib as L
@@ -55,6 +57,15 @@ def cloth_main(args):
   out["newton_step_ms"] = _time(lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
                                 max(2, args.reps // 5))
   print(json.dumps(out))
+
+
+def gemv_layout_bytes(tables) -> int:
+  """Bytes one domain-GEMV launch reads and writes in the tiled inverse
+  layout: every tile of every inverse, the gathered residual, node ids and
+  the correction."""
+  from yasps_b200.mas_hierarchy import inverse_floats
+  sizes = np.diff(np.asarray(tables.dom_node_ptr, dtype=np.int64))
+  return int(sum(4 * inverse_floats(3 * int(k)) + 28 * int(k) for k in sizes))
 
 
 def main():
@@ -110,7 +121,10 @@ def main():
       "gemv": lambda: L.call("ys_mas_gemv", mas._mas, st, None),
       "newton_step": lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
   }
+  nbytes = ctypes.c_uint64(0)
+  L.call("ys_mas_gemv", mas._mas, st, ctypes.byref(nbytes))
   out = {"side": args.side, "tets": cube.tet_count, "dof": cube.dofs, "blocks": p.num_unique,
+         "gemv_alg_bytes": int(nbytes.value), "gemv_layout_bytes": gemv_layout_bytes(mas._tables),
          "non_psd": int(snh._const_cache[("work", snh.n)][1].item()), "pcg": mz.linearSolver.statistics}
   for name, fn in cases.items():
     if args.kernel in ("all", name):
