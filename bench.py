@@ -94,6 +94,14 @@ class Clocks:
                                    stderr=subprocess.DEVNULL)
     except Exception:
       self.proc = None
+      return
+    # nvidia-smi takes a moment to start: hold the timed region until the
+    # first sample is written (at most 5 s)
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+      if os.path.getsize(self.file.name) > 0:
+        break
+      time.sleep(0.02)
 
   def stop(self):
     if self.proc is None:
@@ -389,6 +397,9 @@ def serving_leg(args):
   srv.register(range(8, 49), slots_per_side=2)
   t_register = time.perf_counter() - t0
   srv.run(serving.poisson_fem_stream(count=82, mean_spacing=0.0, seed=99))
+  # steady state: a saturated warm-up stream grows the per-side slot pools to
+  # what a burst needs, so no slot is created inside the timed streams
+  srv.run(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=97))
   srv.solve_serial_fp64(serving.poisson_fem_stream(count=41, mean_spacing=0.0, seed=98))
   out = {"workload": (f"{n} FEM Newton-step requests, Poisson arrivals (mean gap 2 ms), cube side U{{8..48}}, "
                       "E log-uniform [1e4, 1e6], nu U[0.3, 0.45], noise +-0.01, 40 GB admission budget, "
@@ -396,6 +407,7 @@ def serving_leg(args):
          "register_topologies_s": t_register}
   clocks = Clocks(torch.cuda.current_device())
   clocks.start()
+  created = srv.slots_created
   done = srv.run(serving.poisson_fem_stream(count=n, mean_spacing=2e-3, seed=0))
   out["served"] = serving.stream_stats(done)
   out["served"]["max_rel_residual"] = max(r.relative_residual for r in done)
@@ -407,6 +419,7 @@ def serving_leg(args):
       srv.solve_serial_fp64(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=0)))
   out["clocks"] = clocks.stop()
   out["resident_gb"] = srv.resident_bytes / 1e9
+  out["slots_created_while_timed"] = srv.slots_created - created
   srv.close()
   return out
 

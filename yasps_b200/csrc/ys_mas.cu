@@ -20,6 +20,7 @@
 //                  PCG stop test (deterministic last-block reduction).
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "ys_mas.cuh"
@@ -63,6 +64,16 @@ __global__ void __launch_bounds__(256) mas_level_blocks(MasDev M, uint32_t begin
   if (lane == 0) {
 #pragma unroll
     for (int e = 0; e < 9; ++e) M.coarse_values[9ull * cb + e] = acc[e];
+  }
+}
+
+// f(integral_constant<int, I>) for I = B .. E-1 (a loop whose index is a
+// compile-time constant in its body).
+template <int B, int E, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(f);
   }
 }
 
@@ -123,16 +134,18 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
       const uint32_t i = ty + 16 * a, j = tx + 16 * b;
       R[a][b] = (i < n && j < n) ? A[i * n + j] * dinv[i] * dinv[j] : (i == j && i < np ? 1.0 : 0.0);
     }
-  // publish block k: colb[buf][i][m] = C[i][m], rowb[buf][m][j] = R[m][j]
-  auto publish = [&](uint32_t k) {
-    const int kb = (int)((PB * k) >> 4), base = (int)((PB * k) & 15), buf = (int)(k & 1);
+  // publish block k: colb[buf][i][m] = C[i][m], rowb[buf][m][j] = R[m][j].
+  // Block k lies in register column/row KB = PB k / 16 of its owners; KB is a
+  // compile-time constant (the step loop is unrolled over it), so the owners
+  // read their tile entries directly.
+  auto publish = [&](auto kb_c, uint32_t k) {
+    constexpr int KB = decltype(kb_c)::value;
+    const int base = (int)((PB * k) & 15), buf = (int)(k & 1);
     if (tx >= base && tx < base + PB) {
       const int m = tx - base;
 #pragma unroll
       for (int a = 0; a < T; ++a) {
-        double v = 0.0;
-#pragma unroll
-        for (int b = 0; b < T; ++b) v = (b == kb) ? R[a][b] : v;
+        const double v = R[a][KB];
         const bool diag = (ty + 16 * a) == (int)(PB * k) + m;
         colb[buf][(ty + 16 * a) * PB + m] = diag ? v - 1.0 : v;
       }
@@ -141,18 +154,21 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
       const int m = ty - base;
 #pragma unroll
       for (int b = 0; b < T; ++b) {
-        double v = 0.0;
-#pragma unroll
-        for (int a = 0; a < T; ++a) v = (a == kb) ? R[a][b] : v;
+        const double v = R[KB][b];
         const bool diag = (tx + 16 * b) == (int)(PB * k) + m;
         rowb[buf][m * 128 + tx + 16 * b] = diag ? v + 1.0 : v;
       }
     }
   };
-  publish(0);
+  constexpr int kSteps = 16 / PB;  // blocked steps per register column
+  publish(std::integral_constant<int, 0>{}, 0u);
   __syncthreads();
   const uint32_t nblk = np / PB;
-  for (uint32_t k = 0; k < nblk; ++k) {
+  static_for<0, T>([&](auto kb_c) {
+  constexpr int KB = decltype(kb_c)::value;
+  for (int sub = 0; sub < kSteps; ++sub) {
+    const uint32_t k = (uint32_t)(KB * kSteps + sub);
+    if (k >= nblk) break;
     const int buf = (int)(k & 1);
     double P[PB][PB];
     if constexpr (PB == 2) {
@@ -222,9 +238,16 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
         R[a][b] = v;
       }
     }
-    if (k + 1 < nblk) publish(k + 1);
+    if (k + 1 < nblk) {
+      if (sub + 1 < kSteps) {
+        publish(kb_c, k + 1);
+      } else {
+        if constexpr (KB + 1 < T) publish(std::integral_constant<int, KB + 1>{}, k + 1);
+      }
+    }
     __syncthreads();
   }
+  });
   if (threadIdx.x == 0 && bad) atomicAdd(M.status, 1);
   // FP32 upper 4x4 tiles (inv_tile_slot order), straight from the register
   // tiles; the padding rows and columns up to 4 * inv_tiles(n) are zero.

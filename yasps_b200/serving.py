@@ -213,6 +213,7 @@ class NewtonServer:
     self._active = {}                             # id -> (req, slot)
     self.launches = 0
     self.passes_run = 0
+    self.slots_created = 0
     self.host_seconds = collections.Counter()    # admit / attach / launch / wait (host time per phase)
     self.gpu_ms = collections.Counter()          # device time of the PCG launches (CUDA events)
     self._launch_events = []
@@ -237,6 +238,7 @@ class NewtonServer:
     _torch().cuda.synchronize()
 
   def _new_slot(self, topo: FemTopology) -> Optional[_Slot]:
+    self.slots_created += 1
     slot = _Slot(topo)
     if self.resident_bytes + slot.nbytes > self.memory_budget:
       # evict idle slots of other sides until it fits
