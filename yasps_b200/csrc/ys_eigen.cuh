@@ -263,6 +263,31 @@ __device__ __forceinline__ void project_negative_modes(double (&a)[N * (N + 1) /
     }
     const double lam = 0.5 * (lo + hi);
     // -- 3. inverse iteration on T - lam I ---------------------------------------
+    // LU of T - lam I with partial pivoting (rows i, i+1 swapped when the
+    // subdiagonal entry is larger), once for both solves; U rows hold
+    // (pivot, u1, u2) at columns (i, i+1, i+2), kept as pivot reciprocals.
+    // Pivots below eps (unit scale) are raised to eps: every member of a
+    // cluster is amplified alike, so Gram-Schmidt can separate them.
+    double mlt[N], u1[N], u2[N], ipiv[N];
+    bool swp[N];
+    {
+      double pb = d[0] - lam, pc = e[0], pf = 0.0;
+#pragma unroll
+      for (int i = 0; i < N - 1; ++i) {
+        const double na = e[i], nb = d[i + 1] - lam, nc = i + 1 < N - 1 ? e[i + 1] : 0.0;
+        const bool sw = fabs(na) > fabs(pb);
+        const double r0 = sw ? na : pb, r1 = sw ? nb : pc, r2 = sw ? nc : pf;
+        const double o0 = sw ? pb : na, o1 = sw ? pc : nb, o2 = sw ? pf : nc;
+        const double piv = fabs(r0) >= 2.2e-16 ? r0 : (r0 >= 0.0 ? 2.2e-16 : -2.2e-16);
+        const double ip = 1.0 / piv;
+        const double ml = o0 * ip;
+        swp[i] = sw; mlt[i] = ml; u1[i] = r1; u2[i] = r2; ipiv[i] = ip;
+        pb = o1 - ml * r1;
+        pc = o2 - ml * r2;
+        pf = 0.0;
+      }
+      ipiv[N - 1] = 1.0 / (fabs(pb) >= 2.2e-16 ? pb : (pb >= 0.0 ? 2.2e-16 : -2.2e-16));
+    }
     double y[N];
 #pragma unroll
     for (int i = 0; i < N; ++i) y[i] = 1.0 + 0.125 * (double)((i * 7 + m * 3) % 5);
@@ -283,35 +308,23 @@ __device__ __forceinline__ void project_negative_modes(double (&a)[N * (N + 1) /
 #pragma unroll
       for (int i = 0; i < N; ++i) y[i] *= inv;
       if (pass == 2) break;
-      // solve (T - lam I) y' = y: elimination with partial pivoting applied
-      // to the right-hand side as it goes; U rows (u0, u1, u2) at columns
-      // (i, i+1, i+2)
-      double u0[N], u1[N], u2[N];
-      double pb = d[0] - lam, pc = e[0], pf = 0.0, py = y[0];
+      // solve (T - lam I) y' = y with the factors: the row swaps and
+      // eliminations on y, then back substitution
+      double py = y[0];
 #pragma unroll
       for (int i = 0; i < N - 1; ++i) {
-        const double na = e[i], nb = d[i + 1] - lam, nc = i + 1 < N - 1 ? e[i + 1] : 0.0, ny = y[i + 1];
-        const bool s = fabs(na) > fabs(pb);
-        const double r0 = s ? na : pb, r1 = s ? nb : pc, r2 = s ? nc : pf, ry = s ? ny : py;
-        const double o0 = s ? pb : na, o1 = s ? pc : nb, o2 = s ? pf : nc, oy = s ? py : ny;
-        // pivots below eps (unit scale) are raised to eps: every member of a
-        // cluster is amplified alike, so Gram-Schmidt can separate them
-        const double piv = fabs(r0) >= 2.2e-16 ? r0 : (r0 >= 0.0 ? 2.2e-16 : -2.2e-16);
-        const double mlt = o0 / piv;
-        u0[i] = piv; u1[i] = r1; u2[i] = r2; y[i] = ry;
-        pb = o1 - mlt * r1;
-        pc = o2 - mlt * r2;
-        pf = 0.0;
-        py = oy - mlt * ry;
+        const double ny = y[i + 1];
+        const double ry = swp[i] ? ny : py, oy = swp[i] ? py : ny;
+        y[i] = ry;
+        py = oy - mlt[i] * ry;
       }
-      u0[N - 1] = fabs(pb) >= 2.2e-16 ? pb : (pb >= 0.0 ? 2.2e-16 : -2.2e-16);
       y[N - 1] = py;
 #pragma unroll
       for (int i = N - 1; i >= 0; --i) {
         double t = y[i];
         if (i + 1 < N) t -= u1[i] * y[i + 1];
         if (i + 2 < N) t -= u2[i] * y[i + 2];
-        y[i] = t / u0[i];
+        y[i] = t * ipiv[i];
       }
     }
     // map back, v = H_0 H_1 ... H_{N-3} y
