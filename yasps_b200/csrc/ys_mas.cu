@@ -18,6 +18,7 @@
 //                  triangle staged in shared memory;
 //   mas_collect  : z = sum_l w_l z_l(map_l(i)) fused with r^T z, r^T r and the
 //                  PCG stop test (deterministic last-block reduction).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
@@ -295,9 +296,10 @@ __global__ void __launch_bounds__(1024) mas_restrict_tail(MasDev M, const double
   restrict_tail_levels(M, r, first);
 }
 
-__global__ void __launch_bounds__(kGemvThreads) mas_gemv(MasDev M) {
+// Domains d0 .. d0 + gridDim.x - 1.
+__global__ void __launch_bounds__(kGemvThreads) mas_gemv(MasDev M, uint32_t d0) {
   extern __shared__ float4 gemv_smem[];
-  gemv_domain(M, blockIdx.x, gemv_smem);
+  gemv_domain(M, d0 + blockIdx.x, gemv_smem);
 }
 
 struct MasPcg {
@@ -458,7 +460,24 @@ struct MasHandle {
   std::vector<uint32_t> cb_level_begin;
   std::vector<MasPcg*> pcgs;
   int* status_host = nullptr;
+  int64_t fine_domains = -1;  // level-0 domains (the first ones), looked up once
 };
+
+// Number of level-0 domains: domains are numbered level by level, so they
+// are the first ones and cover exactly the level-0 nodes.
+static cudaError_t fine_domain_count(MasHandle* h, uint32_t* out) {
+  if (h->fine_domains < 0) {
+    const MasDev& M = h->M;
+    std::vector<uint32_t> ptr(M.num_domains + 1);
+    const cudaError_t e =
+        cudaMemcpy(ptr.data(), M.dom_node_ptr, sizeof(uint32_t) * ptr.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return e;
+    const uint32_t end = M.levels > 1 ? M.level_node_offset[1] : ptr.back();
+    h->fine_domains = std::lower_bound(ptr.begin(), ptr.end(), end) - ptr.begin();
+  }
+  *out = (uint32_t)h->fine_domains;
+  return cudaSuccess;
+}
 
 const MasDev* mas_device_state(void* handle) { return handle ? &static_cast<MasHandle*>(handle)->M : nullptr; }
 
@@ -473,17 +492,31 @@ static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGr
   return cudaGraphAddKernelNode(node, g, deps, ndeps, &kp);
 }
 
-// Restrict -> GEMV chain shared by init and iteration.
-static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
-                                   cudaGraphNode_t* last, const double* r) {
-  // Level 0 (the FP32 copy of r) is written by the kernel that produces r.
+// z_l = A_l^-1 r_l for every domain, as two branches joined by an empty
+// node: the level-0 domains need only the level-0 residual (written by the
+// kernel that produces r), so their GEMV runs beside the restriction chain
+// of the coarse levels (grid restrictions, the one-CTA tail) and the GEMV of
+// the coarse domains that follows it.
+static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g, const cudaGraphNode_t* deps,
+                                   size_t ndeps, cudaGraphNode_t* last, const double* r) {
   MasDev m = M;
   const double* rr = r;
+  uint32_t fine = 0;
+  cudaError_t e = fine_domain_count(h, &fine);
+  if (e != cudaSuccess) return e;
+  const unsigned smem = (unsigned)gemv_smem_bytes(M.max_dofs);
+  cudaGraphNode_t fine_gemv = nullptr;
+  uint32_t d0 = 0;
+  void* af[] = {&m, &d0};
+  e = add_kernel(g, &fine_gemv, deps, ndeps, (const void*)mas_gemv, fine, kGemvThreads, smem, af);
+  if (e != cudaSuccess || fine == M.num_domains) {
+    *last = fine_gemv;
+    return e;
+  }
   const uint32_t first = restrict_tail_first(M);
   const cudaGraphNode_t* dp = deps;
   size_t nd = ndeps;
   cudaGraphNode_t prev = nullptr;
-  cudaError_t e = cudaSuccess;
   for (uint32_t l = 1; l < first && e == cudaSuccess; ++l) {
     uint32_t level = l;
     void* a1[] = {&m, &rr, &level};
@@ -504,11 +537,13 @@ static cudaError_t add_apply_nodes(const MasDev& M, cudaGraph_t g, const cudaGra
     nd = 1;
   }
   if (e != cudaSuccess) return e;
-  cudaGraphNode_t n2 = nullptr;
-  void* a2[] = {&m};
-  e = add_kernel(g, &n2, dp, nd, (const void*)mas_gemv, M.num_domains, kGemvThreads, (unsigned)gemv_smem_bytes(M.max_dofs), a2);
-  *last = n2;
-  return e;
+  cudaGraphNode_t coarse_gemv = nullptr;
+  uint32_t d1 = fine;
+  void* ac[] = {&m, &d1};
+  e = add_kernel(g, &coarse_gemv, dp, nd, (const void*)mas_gemv, M.num_domains - fine, kGemvThreads, smem, ac);
+  if (e != cudaSuccess) return e;
+  const cudaGraphNode_t both[2] = {fine_gemv, coarse_gemv};
+  return cudaGraphAddEmptyNode(last, g, both, 2);
 }
 
 cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps,
@@ -546,7 +581,7 @@ cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* 
   cudaGraphNode_t n0 = nullptr, n1 = nullptr, n2 = nullptr;
   void* a0[] = {P};
   cudaError_t e = add_kernel(g, &n0, deps, ndeps, (const void*)mas_init_residual, grid, kPcgBlock, 0, a0);
-  if (e == cudaSuccess) e = add_apply_nodes(P->M, g, &n0, 1, &n1, r);
+  if (e == cudaSuccess) e = add_apply_nodes(h, P->M, g, &n0, 1, &n1, r);
   if (e == cudaSuccess) e = add_kernel(g, &n2, &n1, 1, (const void*)mas_init_collect, grid, kPcgBlock, 0, a0);
   *last = n2;
   return e;
@@ -554,13 +589,13 @@ cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* 
 
 cudaError_t mas_add_update_nodes(void* mas, cudaGraph_t body, const cudaGraphNode_t* deps, size_t ndeps,
                                  cudaGraphNode_t* last, MasPcgHooks* hooks) {
-  (void)mas;
+  auto* h = static_cast<MasHandle*>(mas);
   auto* P = static_cast<MasPcg*>(hooks->params);
   const unsigned grid = grid_for(P->nv, kPcgBlock);
   cudaGraphNode_t n0 = nullptr, n1 = nullptr, n2 = nullptr;
   void* a0[] = {P};
   cudaError_t e = add_kernel(body, &n0, deps, ndeps, (const void*)mas_update, grid, kPcgBlock, 0, a0);
-  if (e == cudaSuccess) e = add_apply_nodes(P->M, body, &n0, 1, &n1, P->r);
+  if (e == cudaSuccess) e = add_apply_nodes(h, P->M, body, &n0, 1, &n1, P->r);
   if (e == cudaSuccess) e = add_kernel(body, &n2, &n1, 1, (const void*)mas_iter_collect, grid, kPcgBlock, 0, a0);
   *last = n2;
   return e;
@@ -668,7 +703,7 @@ int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
     ys::mas_restrict<<<ys::restrict_grid(l, cnt), 256, 0, s>>>(M, r, l);
     YS_CHECK_LAUNCH();
   }
-  ys::mas_gemv<<<M.num_domains, ys::kGemvThreads, ys::gemv_smem_bytes(M.max_dofs), s>>>(M);
+  ys::mas_gemv<<<M.num_domains, ys::kGemvThreads, ys::gemv_smem_bytes(M.max_dofs), s>>>(M, 0u);
   YS_CHECK_LAUNCH();
   ys::MasPcg P{};
   P.M = M;
@@ -698,7 +733,7 @@ int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes) {
     }
     *algorithmic_bytes = bytes;
   }
-  ys::mas_gemv<<<M.num_domains, ys::kGemvThreads, ys::gemv_smem_bytes(M.max_dofs), (cudaStream_t)stream>>>(M);
+  ys::mas_gemv<<<M.num_domains, ys::kGemvThreads, ys::gemv_smem_bytes(M.max_dofs), (cudaStream_t)stream>>>(M, 0u);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

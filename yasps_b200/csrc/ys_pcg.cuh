@@ -33,6 +33,22 @@ constexpr int kPcgBlock = 256;
 // block sums, the last block to arrive (ticket) reduces the partials in a
 // fixed order.  Returns true in the last block, whose threads all receive
 // the totals.  partials: [NV * gridDim.x]; ticket: zero on entry, reset here.
+// This thread's share (entries threadIdx.x + j blockDim.x) of the sum of n
+// block partials, in four independent chains so four loads are in flight;
+// the order is fixed by n and the block size.
+__device__ __forceinline__ double thread_partial_sum(const double* __restrict__ p, unsigned n) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  unsigned b = threadIdx.x;
+  for (; b + 3 * blockDim.x < n; b += 4 * blockDim.x) {
+    a0 += __ldcg(p + b);
+    a1 += __ldcg(p + b + blockDim.x);
+    a2 += __ldcg(p + b + 2 * blockDim.x);
+    a3 += __ldcg(p + b + 3 * blockDim.x);
+  }
+  for (; b < n; b += blockDim.x) a0 += __ldcg(p + b);
+  return (a0 + a1) + (a2 + a3);
+}
+
 template <int NV>
 __device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* __restrict__ partials,
                                                  unsigned* __restrict__ ticket) {
@@ -51,9 +67,7 @@ __device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* __rest
   __threadfence();
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
-    double acc = 0.0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) acc += __ldcg(partials + (uint64_t)k * gridDim.x + b);
-    v[k] = block_sum<kPcgBlock>(acc, red);
+    v[k] = block_sum<kPcgBlock>(thread_partial_sum(partials + (uint64_t)k * gridDim.x, gridDim.x), red);
   }
   if (threadIdx.x == 0) *ticket = 0u;
   return true;

@@ -127,9 +127,7 @@ __device__ __forceinline__ bool slot_reduce_last(double (&v)[NV], double* __rest
   __threadfence();
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
-    double acc = 0.0;
-    for (unsigned b = threadIdx.x; b < nblk; b += blockDim.x) acc += __ldcg(partials + (uint64_t)k * nblk + b);
-    v[k] = block_sum<kPcgBlock>(acc, red);
+    v[k] = block_sum<kPcgBlock>(thread_partial_sum(partials + (uint64_t)k * nblk, nblk), red);
   }
   if (threadIdx.x == 0) *ticket = 0u;
   return true;

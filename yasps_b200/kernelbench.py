@@ -120,6 +120,11 @@ def main():
       "mas_apply": lambda: L.call("ys_mas_apply", mas._mas, L.ptr(x), L.ptr(z), st),
       "gemv": lambda: L.call("ys_mas_gemv", mas._mas, st, None),
       "newton_step": lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
+      # 50 MAS-PCG iterations (unreachable tolerance) from one graph launch
+      "pcg50_fp32": lambda: mas._run_pcg(H, H.gradient.value, z, True, L.YS_PREC_MAS, None, mas._mas, 1e-30, 50,
+                                         True, "residual"),
+      "pcg50_fp64": lambda: mas._run_pcg(H, H.gradient.value, z, False, L.YS_PREC_MAS, None, mas._mas, 1e-30, 50,
+                                         True, "residual"),
   }
   nbytes = ctypes.c_uint64(0)
   L.call("ys_mas_gemv", mas._mas, st, ctypes.byref(nbytes))
