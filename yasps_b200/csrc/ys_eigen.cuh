@@ -246,8 +246,6 @@ __device__ __forceinline__ void project_negative_modes(double (&a)[N * (N + 1) /
   // -- 2. negative eigenvalues ---------------------------------------------------
   const int nneg = sturm_count<N>(d, e2, 0.0);
   double vecs[N][N];  // eigenvectors of T for the negative modes (local memory)
-  double vout[N][N];  // the same mapped back by Q
-  double wts[N];
   // The loop runs warp-uniformly to the warp's largest count (lanes past
   // their own count compute a masked dummy mode): every local-memory access
   // of an iteration is then at the same offset in all lanes (coalesced).
@@ -339,24 +337,18 @@ __device__ __forceinline__ void project_negative_modes(double (&a)[N * (N + 1) /
 #pragma unroll
       for (int i = k + 1; i < N; ++i) y[i] -= t * stash[(RS + refl(k, i)) * stride];
     }
+    // -- 4. A += w v v^T on the stashed original, mode by mode -----------------
+    if (live) {
+      const double l = lam * g;  // original scale
+      const double w = method == 1 ? -2.0 * l : -l;
 #pragma unroll
-    for (int i = 0; i < N; ++i) vout[m][i] = live ? y[i] : 0.0;
-    const double l = lam * g;  // original scale
-    wts[m] = live ? (method == 1 ? -2.0 * l : -l) : 0.0;
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = i; j < N; ++j) stash[utri<N>(i, j) * stride] += w * y[i] * y[j];
+    }
   }
-  // -- 4. A + sum w v v^T ----------------------------------------------------------
 #pragma unroll
   for (int i = 0; i < KS; ++i) a[i] = stash[i * stride];
-  for (int m = 0; m < mmax; ++m) {
-    double y[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i) y[i] = vout[m][i];
-    const double w = wts[m];
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-#pragma unroll
-      for (int j = i; j < N; ++j) a[utri<N>(i, j)] += w * y[i] * y[j];
-  }
 }
 
 }  // namespace ys
