@@ -350,7 +350,7 @@ def launches_per_newton_step(impl, its, refs):
   offs = [int(v) for v in t.level_node_offset]
   levels = len(offs) - 1
   first = levels
-  while first > 1 and offs[first] - offs[first - 1] <= 512:
+  while first > 1 and offs[first] - offs[first - 1] <= 64:
     first -= 1
   tail = 1 if first < levels else 0
   init = 1 + (first - 1) + tail + 2

@@ -513,6 +513,14 @@ static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g,
     *last = fine_gemv;
     return e;
   }
+  // The coarse chain is a string of small launches: at the greatest
+  // priority its CTAs are dispatched ahead of the waiting level-0 GEMV CTAs,
+  // so it finishes under the GEMV instead of after it.
+  int least = 0, greatest = 0;
+  e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (e != cudaSuccess) return e;
+  cudaKernelNodeAttrValue prio{};
+  prio.priority = greatest;
   const uint32_t first = restrict_tail_first(M);
   const cudaGraphNode_t* dp = deps;
   size_t nd = ndeps;
@@ -523,6 +531,7 @@ static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g,
     const uint32_t cnt = M.level_node_offset[l + 1] - M.level_node_offset[l];
     cudaGraphNode_t n = nullptr;
     e = add_kernel(g, &n, dp, nd, (const void*)mas_restrict, restrict_grid(l, cnt), 256, 0, a1);
+    if (e == cudaSuccess) e = cudaGraphKernelNodeSetAttribute(n, cudaKernelNodeAttributePriority, &prio);
     prev = n;
     dp = &prev;
     nd = 1;
@@ -532,6 +541,7 @@ static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g,
     void* a1[] = {&m, &rr, &f};
     cudaGraphNode_t n = nullptr;
     e = add_kernel(g, &n, dp, nd, (const void*)mas_restrict_tail, 1, 1024, 0, a1);
+    if (e == cudaSuccess) e = cudaGraphKernelNodeSetAttribute(n, cudaKernelNodeAttributePriority, &prio);
     prev = n;
     dp = &prev;
     nd = 1;
@@ -541,6 +551,7 @@ static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g,
   uint32_t d1 = fine;
   void* ac[] = {&m, &d1};
   e = add_kernel(g, &coarse_gemv, dp, nd, (const void*)mas_gemv, M.num_domains - fine, kGemvThreads, smem, ac);
+  if (e == cudaSuccess) e = cudaGraphKernelNodeSetAttribute(coarse_gemv, cudaKernelNodeAttributePriority, &prio);
   if (e != cudaSuccess) return e;
   const cudaGraphNode_t both[2] = {fine_gemv, coarse_gemv};
   return cudaGraphAddEmptyNode(last, g, both, 2);

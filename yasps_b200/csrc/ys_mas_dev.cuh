@@ -92,7 +92,7 @@ __device__ __forceinline__ void restrict_tail_levels(const MasDev& M, const doub
 
 // First level handled by the one-CTA tail restriction: every level from
 // there on has at most kTailNodes nodes.
-constexpr uint32_t kTailNodes = 512;
+constexpr uint32_t kTailNodes = 64;
 
 __host__ __device__ inline uint32_t restrict_tail_first(const MasDev& M) {
   uint32_t first = M.levels;
