@@ -341,10 +341,11 @@ def launches_per_newton_step(impl, its, refs):
   Element stage: SNH eval + projection, inertia, block and gradient assembly,
   diagonal extraction (6).  MAS numeric update: one Galerkin sum per coarse
   level and the domain inverses.  Refinement: the initial residual (1) and per
-  refinement x += d and r = g - H x (2).  Each PCG solve: init = residual, the
-  grid restrictions of the large levels, the one-CTA tail, GEMV, collect;
-  every iteration = SpMV+dot, update, large-level restrictions, tail, GEMV,
-  collect, direction.
+  refinement x += d and r = g - H x (2).  Each PCG solve: init = residual,
+  the grid restrictions of the levels above 64 nodes, the one-CTA tail of the
+  rest, the level-0 and the coarse domain GEMVs, collect; every iteration =
+  SpMV+dot, update (+ level-1 restriction), grid restrictions from level 2,
+  tail, the two GEMVs, collect, direction.
   """
   t = impl._tables
   offs = [int(v) for v in t.level_node_offset]
@@ -352,9 +353,14 @@ def launches_per_newton_step(impl, its, refs):
   first = levels
   while first > 1 and offs[first] - offs[first - 1] <= 64:
     first -= 1
-  tail = 1 if first < levels else 0
-  init = 1 + (first - 1) + tail + 2
-  per_it = 2 + (first - 1) + tail + 3
+  coarse = 1 if levels > 1 else 0
+  tail_init = 1 if first < levels else 0
+  init = 1 + (first - 1) + tail_init + 1 + coarse + 1
+  if levels > 1:
+    f_it = max(first, 2)
+    per_it = 2 + (first - 2 if first > 2 else 0) + (1 if f_it < levels else 0) + 1 + coarse + 2
+  else:
+    per_it = 2 + 1 + 2
   return 6 + (levels - 1) + 1 + 1 + 2 * refs + refs * init + its * per_it
 
 

@@ -73,6 +73,12 @@ def test_hierarchy_tables_are_consistent():
   idx = t.cb_src & 0x3FFFFFFF
   assert idx.size == 0 or idx.max() < t.fine_blocks + t.cb_level_begin[-1]
   assert t.max_domain_dofs <= 96
+  # the children of the level-1 nodes are every fine variable exactly once
+  # (the PCG update writes the level-1 residuals from this partition)
+  ptr = np.asarray(t.child_ptr, dtype=np.int64)
+  lo, hi = int(t.level_node_offset[1]) - nv, int(t.level_node_offset[2]) - nv
+  kids = np.asarray(t.child_fine, dtype=np.int64)[ptr[lo]:ptr[hi]]
+  assert np.array_equal(np.sort(kids), np.arange(nv))
 
 
 def test_scene_api_validation():

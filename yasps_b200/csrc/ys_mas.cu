@@ -407,6 +407,47 @@ __global__ void __launch_bounds__(kPcgBlock) mas_update(MasPcg P) {
   }
 }
 
+// mas_update fused with the level-1 restriction: a warp per level-1 node
+// updates the node's children (lanes stride them as restrict_node_warp does)
+// and sums their new residuals in the same order, so the level-1 values are
+// bit-identical to a separate restriction pass.  Every fine variable is the
+// child of exactly one level-1 node.
+__global__ void __launch_bounds__(kPcgBlock) mas_update_restrict(MasPcg P) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t p = P.M.level_node_offset[1] + (t >> 5);
+  if (p >= P.M.level_node_offset[2] || P.st[kStatus] != (double)kContinue) return;  // warp-uniform
+  const int lane = (int)(t & 31);
+  const double alpha = P.st[kAlpha];
+  const uint32_t c = p - P.M.nv;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (uint32_t q = P.M.child_ptr[c] + lane; q < P.M.child_ptr[c + 1]; q += 32) {
+    const uint32_t i = P.M.child_fine[q];
+    double r[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      P.x[3ull * i + k] = P.x[3ull * i + k] + P.p[3ull * i + k] * alpha;
+      r[k] = P.r[3ull * i + k] - P.q[3ull * i + k] * alpha;
+      P.r[3ull * i + k] = r[k];
+      P.M.rl[3ull * i + k] = (float)r[k];
+    }
+    s0 += r[0]; s1 += r[1]; s2 += r[2];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (lane == 0) {
+    P.M.rl64[3ull * p] = s0;
+    P.M.rl64[3ull * p + 1] = s1;
+    P.M.rl64[3ull * p + 2] = s2;
+    P.M.rl[3ull * p] = (float)s0;
+    P.M.rl[3ull * p + 1] = (float)s1;
+    P.M.rl[3ull * p + 2] = (float)s2;
+  }
+}
+
 __global__ void __launch_bounds__(kPcgBlock) mas_iter_collect(MasPcg P) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = P.st[kStatus] == (double)kContinue;
@@ -498,7 +539,7 @@ static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGr
 // of the coarse levels (grid restrictions, the one-CTA tail) and the GEMV of
 // the coarse domains that follows it.
 static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g, const cudaGraphNode_t* deps,
-                                   size_t ndeps, cudaGraphNode_t* last, const double* r) {
+                                   size_t ndeps, cudaGraphNode_t* last, const double* r, uint32_t restricted) {
   MasDev m = M;
   const double* rr = r;
   uint32_t fine = 0;
@@ -525,7 +566,8 @@ static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g,
   const cudaGraphNode_t* dp = deps;
   size_t nd = ndeps;
   cudaGraphNode_t prev = nullptr;
-  for (uint32_t l = 1; l < first && e == cudaSuccess; ++l) {
+  // levels up to `restricted` are written by the kernel that produces r
+  for (uint32_t l = restricted + 1; l < first && e == cudaSuccess; ++l) {
     uint32_t level = l;
     void* a1[] = {&m, &rr, &level};
     const uint32_t cnt = M.level_node_offset[l + 1] - M.level_node_offset[l];
@@ -536,8 +578,8 @@ static cudaError_t add_apply_nodes(MasHandle* h, const MasDev& M, cudaGraph_t g,
     dp = &prev;
     nd = 1;
   }
-  if (e == cudaSuccess && first < M.levels) {
-    uint32_t f = first;
+  uint32_t f = first > restricted ? first : restricted + 1;
+  if (e == cudaSuccess && f < M.levels) {
     void* a1[] = {&m, &rr, &f};
     cudaGraphNode_t n = nullptr;
     e = add_kernel(g, &n, dp, nd, (const void*)mas_restrict_tail, 1, 1024, 0, a1);
@@ -592,7 +634,7 @@ cudaError_t mas_add_init_nodes(void* mas, cudaGraph_t g, const cudaGraphNode_t* 
   cudaGraphNode_t n0 = nullptr, n1 = nullptr, n2 = nullptr;
   void* a0[] = {P};
   cudaError_t e = add_kernel(g, &n0, deps, ndeps, (const void*)mas_init_residual, grid, kPcgBlock, 0, a0);
-  if (e == cudaSuccess) e = add_apply_nodes(h, P->M, g, &n0, 1, &n1, r);
+  if (e == cudaSuccess) e = add_apply_nodes(h, P->M, g, &n0, 1, &n1, r, 0u);
   if (e == cudaSuccess) e = add_kernel(g, &n2, &n1, 1, (const void*)mas_init_collect, grid, kPcgBlock, 0, a0);
   *last = n2;
   return e;
@@ -605,8 +647,12 @@ cudaError_t mas_add_update_nodes(void* mas, cudaGraph_t body, const cudaGraphNod
   const unsigned grid = grid_for(P->nv, kPcgBlock);
   cudaGraphNode_t n0 = nullptr, n1 = nullptr, n2 = nullptr;
   void* a0[] = {P};
-  cudaError_t e = add_kernel(body, &n0, deps, ndeps, (const void*)mas_update, grid, kPcgBlock, 0, a0);
-  if (e == cudaSuccess) e = add_apply_nodes(h, P->M, body, &n0, 1, &n1, P->r);
+  // with a level 1, the update writes the level-1 residuals too
+  const bool fused = P->M.levels > 1;
+  const unsigned grid1 = fused ? grid_for(32ull * (P->M.level_node_offset[2] - P->M.level_node_offset[1]), kPcgBlock) : grid;
+  cudaError_t e = add_kernel(body, &n0, deps, ndeps, fused ? (const void*)mas_update_restrict : (const void*)mas_update,
+                             grid1, kPcgBlock, 0, a0);
+  if (e == cudaSuccess) e = add_apply_nodes(h, P->M, body, &n0, 1, &n1, P->r, fused ? 1u : 0u);
   if (e == cudaSuccess) e = add_kernel(body, &n2, &n1, 1, (const void*)mas_iter_collect, grid, kPcgBlock, 0, a0);
   *last = n2;
   return e;
