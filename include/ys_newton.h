@@ -476,7 +476,7 @@ typedef struct ys_serve_slot_desc {
   ys_matrix3 matrix;           /* one 3x3 block set: values (FP64) + values32 (FP32) */
   const double* rhs;           /* g [3 * num_vars]                                   */
   double* solution;            /* x [3 * num_vars] (written)                         */
-  double* workspace;           /* ys_serve_workspace_doubles(num_vars) doubles        */
+  double* workspace;           /* ys_serve_workspace_doubles(num_vars), 16-B aligned */
   double tolerance;            /* target true relative residual                      */
   double refinement_tolerance; /* lower bound of every inner relative tolerance      */
   uint32_t max_iterations;     /* inner iterations over all refinements              */

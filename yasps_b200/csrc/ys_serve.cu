@@ -60,6 +60,7 @@ struct ServeSlot {
   double* d;
   double* r;
   double* p;
+  float4* p32;            // FP32 copy of p (x, y, z, 0) for the FP32 SpMV
   double* q;
   double* z;
   double* partials;       // [2 * spmv_blocks]
@@ -147,7 +148,7 @@ __global__ void __launch_bounds__(kPcgBlock) serve_spmv(const ServeDev* __restri
   double v[2] = {0.0, 0.0};
   if (phase == kServeIter) {
     double q0, q1, q2;
-    spmv3_group(&T.A, 1, true, i, valid, lane, T.p, q0, q1, q2);
+    spmv3_group_x32(&T.A, 1, i, valid, lane, T.p32, q0, q1, q2);
     if (valid && lane == 0) {
       T.q[3ull * i] = q0; T.q[3ull * i + 1] = q1; T.q[3ull * i + 2] = q2;
       v[0] = T.p[3ull * i] * q0 + T.p[3ull * i + 1] * q1 + T.p[3ull * i + 2] * q2;
@@ -314,14 +315,18 @@ __global__ void __launch_bounds__(kPcgBlock) serve_direction(const ServeDev* __r
   const uint32_t i = b * blockDim.x + threadIdx.x;
   if (i >= T.nv) return;
   if (phase == kServeIter) {
+    double p[3];
     if (st.fresh) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) T.p[3ull * i + k] = T.z[3ull * i + k];
+      for (int k = 0; k < 3; ++k) p[k] = T.z[3ull * i + k];
     } else {
       const double beta = st.beta;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) T.p[3ull * i + k] = T.z[3ull * i + k] + T.p[3ull * i + k] * beta;
+      for (int k = 0; k < 3; ++k) p[k] = T.z[3ull * i + k] + T.p[3ull * i + k] * beta;
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) T.p[3ull * i + k] = p[k];
+    T.p32[i] = make_float4((float)p[0], (float)p[1], (float)p[2], 0.0f);
   } else if (phase == kServeRefine) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) T.x[3ull * i + k] += T.d[3ull * i + k];
@@ -489,8 +494,9 @@ extern "C" {
 
 uint64_t ys_serve_workspace_doubles(uint32_t num_vars) {
   const uint64_t spmv_blocks = ((uint64_t)num_vars * ys::kRowLanes + ys::kPcgBlock - 1) / ys::kPcgBlock;
-  // d, r, p, q, z + partials + tickets
-  return 15ull * num_vars + 2 * spmv_blocks + 2;
+  // FP32 copy of p (4 floats a variable, first: 16-byte aligned) + d, r, p,
+  // q, z + partials + tickets
+  return 2ull * num_vars + 15ull * num_vars + 2 * spmv_blocks + 2;
 }
 
 int32_t ys_serve_create(uint32_t max_slots, uint32_t passes_per_launch, void** handle) {
@@ -543,6 +549,8 @@ int32_t ys_serve_attach(void* handle, uint32_t slot, const ys_serve_slot_desc* d
   YS_REQUIRE(M->nv <= (ys::kLocalMask / ys::kRowLanes) * (uint32_t)ys::kPcgBlock && M->num_domains <= ys::kLocalMask,
              YS_ERR_CAPACITY, "slot too large for the CTA tables");
   YS_REQUIRE(d->rhs && d->solution && d->workspace, YS_ERR_INVALID, "null vector");
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(d->workspace) & 15) == 0, YS_ERR_INVALID,
+             "workspace must be 16-byte aligned");
   YS_REQUIRE(d->tolerance > 0.0 && d->max_iterations >= 1, YS_ERR_INVALID, "bad tolerance / iteration budget");
   // the staging entry of this slot may still be the source of a pending copy
   YS_CUDA_TRY(cudaEventSynchronize(h->staged));
@@ -559,6 +567,7 @@ int32_t ys_serve_attach(void* handle, uint32_t slot, const ys_serve_slot_desc* d
   T.x = d->solution;
   const uint64_t n = 3ull * T.nv;
   double* w = d->workspace;
+  T.p32 = reinterpret_cast<float4*>(w); w += 2ull * T.nv;
   T.d = w; w += n;
   T.r = w; w += n;
   T.p = w; w += n;
