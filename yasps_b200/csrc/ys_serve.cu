@@ -4,9 +4,9 @@
 // and numeric inverses, its right-hand side and PCG vectors.  One launch runs
 // `passes` pipeline passes over every attached slot; a pass is
 //   serve_spmv      : ITER   q = A32 p, p^T q -> alpha
-//                     INIT   x = 0, r = g            -> ||r||, ||g||
+//   serve_residual  : INIT   x = 0, r = g            -> ||r||, ||g||
 //                     REFINE r = g - A64 x (FP64)    -> ||r||, ||g||
-//                     (INIT/REFINE: done when ||r|| <= tol ||g||, else START)
+//                     (done when ||r|| <= tol ||g||, else START)
 //   serve_update    : ITER   d += alpha p, r -= alpha q;  START  d = 0
 //                     (both write the FP32 level-0 residual)
 //   serve_restrict  : MAS restriction of the large levels (one launch each,
@@ -134,26 +134,54 @@ __device__ __forceinline__ bool slot_reduce_last(double (&v)[NV], double* __rest
   return true;
 }
 
+// ITER: q = A32 p (FP32 blocks, float4 copy of p), p^T q -> alpha.  Kept
+// apart from the FP64 residual kernel so it runs at the FP32 gather's
+// register count (occupancy).
 __global__ void __launch_bounds__(kPcgBlock) serve_spmv(const ServeDev* __restrict__ S) {
   uint32_t s, b;
   if (!map_entry(S->map_spmv, S->n_spmv, s, b)) return;
   const ServeSlot& T = S->slots[s];
   SlotState& st = S->state[s];
+  if (st.phase != kServeIter) return;
+  const uint32_t t = b * blockDim.x + threadIdx.x;
+  const uint32_t i = t / kRowLanes;
+  const int lane = (int)(t % kRowLanes);
+  const bool valid = i < T.nv;
+  double v[1] = {0.0};
+  double q0, q1, q2;
+  spmv3_group_x32(&T.A, 1, i, valid, lane, T.p32, q0, q1, q2);
+  if (valid && lane == 0) {
+    T.q[3ull * i] = q0; T.q[3ull * i + 1] = q1; T.q[3ull * i + 2] = q2;
+    v[0] = T.p[3ull * i] * q0 + T.p[3ull * i + 1] * q1 + T.p[3ull * i + 2] * q2;
+  }
+  if (!slot_reduce_last<1>(v, T.partials, T.tickets, b, T.spmv_blocks)) return;
+  if (threadIdx.x != 0) return;
+  const double curv = v[0];
+  st.delta_old = st.delta_new;
+  if (!isfinite(curv) || curv <= 0.0) {
+    st.alpha = 0.0;
+    st.phase = kServeFailed;
+  } else {
+    st.alpha = st.delta_new / curv;
+  }
+}
+
+// INIT: x = 0, r = g; REFINE: r = g - A64 x (FP64 blocks); both -> ||r||,
+// ||g||, then DONE when ||r|| <= tol ||g||, else START with the next inner
+// tolerance.
+__global__ void __launch_bounds__(kPcgBlock) serve_residual(const ServeDev* __restrict__ S) {
+  uint32_t s, b;
+  if (!map_entry(S->map_spmv, S->n_spmv, s, b)) return;
+  const ServeSlot& T = S->slots[s];
+  SlotState& st = S->state[s];
   const int phase = st.phase;
-  if (phase != kServeInit && phase != kServeRefine && phase != kServeIter) return;
+  if (phase != kServeInit && phase != kServeRefine) return;
   const uint32_t t = b * blockDim.x + threadIdx.x;
   const uint32_t i = t / kRowLanes;
   const int lane = (int)(t % kRowLanes);
   const bool valid = i < T.nv;
   double v[2] = {0.0, 0.0};
-  if (phase == kServeIter) {
-    double q0, q1, q2;
-    spmv3_group_x32(&T.A, 1, i, valid, lane, T.p32, q0, q1, q2);
-    if (valid && lane == 0) {
-      T.q[3ull * i] = q0; T.q[3ull * i + 1] = q1; T.q[3ull * i + 2] = q2;
-      v[0] = T.p[3ull * i] * q0 + T.p[3ull * i + 1] * q1 + T.p[3ull * i + 2] * q2;
-    }
-  } else if (phase == kServeRefine) {
+  if (phase == kServeRefine) {
     double h[3];
     spmv3_group(&T.A, 1, false, i, valid, lane, T.x, h[0], h[1], h[2]);
     if (valid && lane == 0) {
@@ -177,17 +205,6 @@ __global__ void __launch_bounds__(kPcgBlock) serve_spmv(const ServeDev* __restri
   }
   if (!slot_reduce_last<2>(v, T.partials, T.tickets, b, T.spmv_blocks)) return;
   if (threadIdx.x != 0) return;
-  if (phase == kServeIter) {
-    const double curv = v[0];
-    st.delta_old = st.delta_new;
-    if (!isfinite(curv) || curv <= 0.0) {
-      st.alpha = 0.0;
-      st.phase = kServeFailed;
-    } else {
-      st.alpha = st.delta_new / curv;
-    }
-    return;
-  }
   const double rr = v[0], gg = v[1];
   if (phase == kServeRefine) st.refinements += 1;
   st.rr = rr;
@@ -398,6 +415,7 @@ static cudaError_t build_graph(ServeHandle* h, const Bucket& k, cudaGraphExec_t*
   cudaGraphNode_t prev = nullptr, n = nullptr;
   for (uint32_t pass = 0; pass < h->passes && e == cudaSuccess; ++pass) {
     e = add_node(g, &n, &prev, (const void*)serve_spmv, k.spmv, kPcgBlock, 0, a);
+    if (e == cudaSuccess) e = add_node(g, &n, &prev, (const void*)serve_residual, k.spmv, kPcgBlock, 0, a);
     if (e == cudaSuccess) e = add_node(g, &n, &prev, (const void*)serve_update, k.rows, kPcgBlock, 0, a);
     for (uint32_t l = 1; l < k.levels && e == cudaSuccess; ++l)
       if (k.restrict_cap[l])
