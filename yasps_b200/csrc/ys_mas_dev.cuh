@@ -192,9 +192,21 @@ __device__ __forceinline__ void gemv_domain(const MasDev& M, uint32_t d, float4*
     }
   }
   float* rloc = reinterpret_cast<float*>(r4);
+  // A domain's node list is normally the consecutive packed ids from nb
+  // (domains are numbered level by level over the packed node order): the
+  // residual is read there at once, beside the list entry that confirms it
+  // (a mismatch takes the listed node), so the gather is not a chain of two
+  // dependent loads.  The first entry's node is kept for the store below.
+  uint32_t own_node = 0;
   for (uint32_t t = threadIdx.x; t < 4 * T; t += blockDim.x) {
     float v = 0.0f;
-    if (t < n) v = M.rl[3ull * M.dom_nodes[nb + t / 3] + t % 3];
+    if (t < n) {
+      const uint32_t guess = nb + t / 3;
+      const float vs = M.rl[3ull * guess + t % 3];
+      const uint32_t node = M.dom_nodes[nb + t / 3];
+      v = node == guess ? vs : M.rl[3ull * node + t % 3];
+      if (t == threadIdx.x) own_node = node;
+    }
     rloc[t] = v;
   }
   __syncthreads();
@@ -217,7 +229,8 @@ __device__ __forceinline__ void gemv_domain(const MasDev& M, uint32_t d, float4*
       s0 += row[4 * y];
       s1 += row[4 * y + 4];
     }
-    M.zl[3ull * M.dom_nodes[nb + i / 3] + i % 3] = s0 + s1;
+    const uint32_t node = i == threadIdx.x ? own_node : M.dom_nodes[nb + i / 3];
+    M.zl[3ull * node + i % 3] = s0 + s1;
   }
 }
 
