@@ -286,11 +286,15 @@ class hessian:
     self._requests_dynamic = list(requests_dynamic)
     self._setup = False
     self.want_fp32 = False
-    self.want_diagonal = True  # diagonal / diagonal_blocks (block-Jacobi); MAS-only callers may skip them
+    # diagonal / diagonal_blocks are extracted from the assembled blocks when
+    # first read after a compute (block-Jacobi reads them, MAS does not);
+    # want_diagonal = True extracts them with every compute
+    self.want_diagonal = False
+    self._diag_stale = True
     self.values32_current = False
     self.gradient: Optional[vector] = None
-    self.diagonal = None
-    self.diagonal_blocks = None
+    self._diagonal = None
+    self._diagonal_blocks = None
     self.energy_buffers = {}
 
   # -- composition ----------------------------------------------------------------
@@ -388,8 +392,8 @@ class hessian:
     self._static_infos = self._plan_terms(self._static.terms)
     self._build_set(self._static, *self._static_infos)
     self.gradient = vector(self.rows)
-    self.diagonal = torch.zeros(self.rows, dtype=torch.float64, device=_dev())
-    self.diagonal_blocks = torch.zeros(max(self.diagonal_blocks_start_cpu[-1], 1), dtype=torch.float64,
+    self._diagonal = torch.zeros(self.rows, dtype=torch.float64, device=_dev())
+    self._diagonal_blocks = torch.zeros(max(self.diagonal_blocks_start_cpu[-1], 1), dtype=torch.float64,
                                        device=_dev())
     self._setup = True
 
@@ -422,6 +426,7 @@ class hessian:
     if gp.num_unique:
       L.call("ys_assemble_strided", L.ptr(self._grad_records), L.ptr(gp.record_begin), L.ptr(gp.record_count),
              L.ptr(gp.positions), 2, L.ptr(gp.dims), gp.num_unique, L.ptr(self.gradient.value), s)
+    self._diag_stale = True
     if self.want_diagonal:
       self._extract_diagonal()
     self.values32_current = self.want_fp32
@@ -464,10 +469,25 @@ class hessian:
       total += v
     return total
 
+  @property
+  def diagonal(self):
+    """Diagonal entries of the assembled matrix (``hessian.pyx`` ``diagonal``)."""
+    if self._diag_stale and self._setup:
+      self._extract_diagonal()
+    return self._diagonal
+
+  @property
+  def diagonal_blocks(self):
+    """Per-variable diagonal blocks (``hessian.pyx`` ``diagonal_blocks``)."""
+    if self._diag_stale and self._setup:
+      self._extract_diagonal()
+    return self._diagonal_blocks
+
   def _extract_diagonal(self):
     s = L.stream_ptr()
-    self.diagonal.zero_()
-    self.diagonal_blocks.zero_()
+    self._diag_stale = False
+    self._diagonal.zero_()
+    self._diagonal_blocks.zero_()
     nat = len(self.__wrt)
     arr = lambda v: (L.u32 * len(v))(*v)
     seg = arr(self.gradient_segments_start_cpu)
@@ -478,7 +498,7 @@ class hessian:
       if p is None or p.num_unique == 0:
         continue
       L.call("ys_extract_diagonal", L.ptr(bs.values), L.ptr(p.positions), L.ptr(p.dims), L.ptr(p.value_offset),
-             p.num_unique, nat, seg, asz, dst, L.ptr(self.diagonal_blocks), L.ptr(self.diagonal), 1, s)
+             p.num_unique, nat, seg, asz, dst, L.ptr(self._diagonal_blocks), L.ptr(self._diagonal), 1, s)
 
   def _assemble(self, bs: _BlockSet):
     torch = _torch()
