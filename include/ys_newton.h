@@ -402,6 +402,11 @@ int32_t ys_mas_create(const ys_mas_desc* desc, void** handle);
  * mas/cuda/local_inverse.cu:190-545).  When failed_domains is not NULL the
  * call synchronises and reports singular domains (YS_ERR_SINGULAR_DOMAIN). */
 int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* stream, int32_t* failed_domains);
+/* Singular domains of the last ys_mas_numeric_update on `stream` (which may
+ * have been called without failed_domains, so the check can wait for a
+ * later synchronisation); synchronises the stream; YS_ERR_SINGULAR_DOMAIN
+ * when any.                                                              */
+int32_t ys_mas_failed_domains(void* handle, void* stream, int32_t* failed_domains);
 /* z = M^-1 r (mas/preconditioner.py:128-154). */
 int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream);
 int32_t ys_mas_destroy(void* handle);

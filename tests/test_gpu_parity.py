@@ -190,3 +190,21 @@ def test_mas_apply_matches_oracle(c0):
   pre = omas.MASPreconditioner(h, omas.level_local_matrices(h, blocks))
   # FP32 inverses and level vectors: single-precision agreement
   assert rel(z.cpu().numpy(), pre.apply(r)) <= 2e-4
+
+
+def test_mas_singular_domain_is_reported(c0):
+  """A domain whose scaled diagonal is not positive voids the solve: the
+  check runs after the solve (no extra synchronisation before it) and
+  raises, as the reference's pivot test does (mas/local_inverse.py:43-65)."""
+  import torch
+  cube, _ = c0
+  sc, _ = build(cube, "mas", mixed_spmv=True, stop_rule="residual")
+  H = sc.minimizer.computeNumericValue()
+  bs = H.block_sets[0]
+  pos = bs.pattern.positions[:2 * bs.pattern.num_unique].cpu().numpy().reshape(-1, 2)
+  k = int(np.nonzero((pos[:, 0] == 0) & (pos[:, 1] == 0))[0][0])
+  off = int(bs.pattern.value_offset[k].item())
+  bs.values[off:off + 9] = torch.tensor([-1.0, 0, 0, 0, -1.0, 0, 0, 0, -1.0], dtype=torch.float64, device="cuda")
+  solver = sc.minimizer.linearSolver
+  with pytest.raises(np.linalg.LinAlgError):
+    solver.computeSolution(H, H.gradient, None, tolerance=1e-6, maxIterations=50, zero_initial_guess=True)

@@ -125,6 +125,7 @@ SIGNATURES = {
     "ys_spmv_plan_build": (i32, [vp, u32, u32, vp, u64, vp, vp, vp, vp]),
     "ys_spmv3": (i32, [vp, vp, vp, vp, vp, u32, vp, vp, i32, vp]),
     "ys_mas_inverse_floats": (u64, [u32]),
+    "ys_mas_failed_domains": (i32, [vp, vp, P(i32)]),
     "ys_pack_x32": (i32, [vp, u32, vp, vp]),
     "ys_spmv3_x32": (i32, [vp, vp, vp, vp, u32, vp, vp, i32, vp]),
     "ys_pcg_workspace_doubles": (u64, [u32]),

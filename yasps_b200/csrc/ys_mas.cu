@@ -750,6 +750,17 @@ int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* str
   return YS_OK;
 }
 
+int32_t ys_mas_failed_domains(void* handle, void* stream, int32_t* failed_domains) {
+  YS_REQUIRE(handle && failed_domains, YS_ERR_INVALID, "null argument");
+  auto* h = static_cast<ys::MasHandle*>(handle);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h->status_host) YS_CUDA_TRY(cudaMallocHost(&h->status_host, sizeof(int)));
+  YS_CUDA_TRY(cudaMemcpyAsync(h->status_host, h->M.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  YS_CUDA_TRY(cudaStreamSynchronize(s));
+  *failed_domains = *h->status_host;
+  return *failed_domains ? YS_ERR_SINGULAR_DOMAIN : YS_OK;
+}
+
 int32_t ys_mas_apply(void* handle, const double* r, double* z, void* stream) {
   YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
   auto* h = static_cast<ys::MasHandle*>(handle);

@@ -312,9 +312,9 @@ class masSolver(_PcgBase):
     if not zero_initial_guess and initial_guess is not None:
       raise NotImplementedError("the device MAS PCG starts from a zero initial guess")
     self._ensure_hierarchy(H)
-    failed = self.numeric_update(H, check_domains)
-    if failed:
-      raise np.linalg.LinAlgError(f"MAS: {failed} domain(s) are singular")
+    # the singular-domain check is read after the solve (its status read
+    # synchronises anyway); a failed domain voids the solve
+    self.numeric_update(H, check=False)
     if not self.mixed_spmv:
       res = self._run_pcg(H, rhs, self._solution, False, L.YS_PREC_MAS, None, self._mas, tolerance, maxIterations,
                           True, self.stop_rule)
@@ -323,6 +323,11 @@ class masSolver(_PcgBase):
       refinements = 0
     else:
       status, its, refinements = self._solve_mixed(H, rhs, tolerance, maxIterations)
+    if check_domains:
+      failed = L.i32(0)
+      L.call("ys_mas_failed_domains", self._mas, L.stream_ptr(), ctypes.byref(failed), ok=(L.YS_OK, L.YS_ERR_SINGULAR_DOMAIN))
+      if failed.value:
+        raise np.linalg.LinAlgError(f"MAS: {failed.value} domain(s) are singular")
     self._statistics = {"solver": "mas", "converged": status >= 0, "iterations": its, "refinements": refinements,
                         "result": 0 if status >= 0 else -4, "solve_seconds": time.perf_counter() - t0,
                         "levels": len(self.hierarchy.levels), "domains_per_level": self.hierarchy.domains_per_level,
