@@ -11,6 +11,7 @@
 //   direction : p = z + beta p
 // and a single device->host read of the status per solve.  All reductions are
 // deterministic (fixed-order block trees, fixed-order partial sums).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -119,18 +120,25 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
 // kRowLanes threads per row (see spmv3_group).
 // One instantiation per precision of the block values (the FP32 one keeps
 // fewer registers: higher occupancy for the latency-bound gathers).
+// A grid of resident size strides over the groups of kPcgBlock / kRowLanes
+// rows: the dot product then ends in a few hundred block partials (each
+// block's fence and ticket, and the last block's sum, are per block, so a
+// CTA per row group would pay them thousands of times).
 template <bool FP32>
 __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t i = t / kRowLanes;
-  const int lane = (int)(t % kRowLanes);
+  constexpr uint32_t kRows = kPcgBlock / kRowLanes;
+  const uint32_t groups = (P.nv + kRows - 1) / kRows;
+  const int lane = (int)(threadIdx.x % kRowLanes);
   double v[1] = {0.0};
-  double q0, q1, q2;
-  if (FP32) spmv3_group_x32(P.sets, P.nsets, i, i < P.nv, lane, P.p32, q0, q1, q2);
-  else spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.p, q0, q1, q2);
-  if (i < P.nv && lane == 0) {
-    P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
-    v[0] = P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
+  for (uint32_t gb = blockIdx.x; gb < groups; gb += gridDim.x) {  // block-uniform
+    const uint32_t i = gb * kRows + threadIdx.x / kRowLanes;
+    double q0, q1, q2;
+    if (FP32) spmv3_group_x32(P.sets, P.nsets, i, i < P.nv, lane, P.p32, q0, q1, q2);
+    else spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.p, q0, q1, q2);
+    if (i < P.nv && lane == 0) {
+      P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
+      v[0] += P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
+    }
   }
   if (!grid_reduce_last<1>(v, P.partials, P.tickets + 1)) return;
   if (threadIdx.x != 0) return;
@@ -314,7 +322,17 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   w += 2ull * P.nv;
   P.st = w; w += ys::kSlots;
   const unsigned grid = ys::grid_for(P.nv, ys::kPcgBlock);
-  const unsigned grid_rows = ys::grid_for((uint64_t)P.nv * ys::kRowLanes, ys::kPcgBlock);
+  unsigned grid_rows = ys::grid_for((uint64_t)P.nv * ys::kRowLanes, ys::kPcgBlock);
+  {
+    // resident-size grid for the SpMV + dot (see pcg_spmv_dot)
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, P.fp32 ? (const void*)ys::pcg_spmv_dot<true> : (const void*)ys::pcg_spmv_dot<false>, ys::kPcgBlock,
+            0) == cudaSuccess &&
+        sms > 0 && per_sm > 0)
+      grid_rows = std::min<unsigned>(grid_rows, (unsigned)(sms * per_sm));
+  }
   P.partials = w; w += (uint64_t)ys::kRowLanes * (grid + 2);
   P.tickets = reinterpret_cast<unsigned*>(w);
   P.jinv = a.jacobi_inverse;
