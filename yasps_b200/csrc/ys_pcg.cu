@@ -391,7 +391,8 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
         e = ys::add_kernel(body, &n3, &n2, 1, (const void*)ys::pcg_direction, grid, ys::kPcgBlock, args1);
     }
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->exec, h->graph, 0);
+  // per-node priorities (the MAS coarse chain) take effect only with this flag
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->exec, h->graph, cudaGraphInstantiateFlagUseNodePriority);
   if (e != cudaSuccess) {
     ys_set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
     if (h->exec) cudaGraphExecDestroy(h->exec);
