@@ -259,10 +259,10 @@ def gpu_arm(args):
   hbm, peak_kind = peaks()
   achieved = nbytes.value / (gemv_ms / 1e3) / 1e9
   # DRAM traffic per launch from an ncu capture of the 56^3 cube (109.60 MB
-  # read + 4.24 MB written; its tiled layout holds GEMV_LAYOUT_56 bytes),
+  # read + 7.08 MB written; its tiled layout holds GEMV_LAYOUT_56 bytes),
   # scaled by this launch's layout bytes (traffic grows with the domains)
   from yasps_b200.kernelbench import gemv_layout_bytes
-  traffic = (109.60e6 + 4.24e6) / GEMV_LAYOUT_56 * gemv_layout_bytes(ms_solver._tables)
+  traffic = (109.60e6 + 7.08e6) / GEMV_LAYOUT_56 * gemv_layout_bytes(ms_solver._tables)
   roofline = {"kernel": "mas_gemv (MAS domain-inverse apply, FP32)", "bound": "hbm", "achieved": achieved,
               "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
               "traffic": traffic, "bytes_per_launch": int(nbytes.value), "ms_per_launch": gemv_ms}
