@@ -135,6 +135,13 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
       const uint32_t i = ty + 16 * a, j = tx + 16 * b;
       R[a][b] = (i < n && j < n) ? A[i * n + j] * dinv[i] * dinv[j] : (i == j && i < np ? 1.0 : 0.0);
     }
+  // PB == 2 runs the symmetric form (the sweep operator): with v = S[:,K]
+  // except v[K,:] = P - I, the update S -= (v P^-1) v^T and then S[k,k] -= 2
+  // on the pivots sweeps K; after every pivot S holds -S_0^-1.  The update is
+  // symmetric, so only the upper register tiles (a <= b) are kept: v is read
+  // from the published column K for rows in tiles up to the pivot's and from
+  // the published row K beyond it, never from a lower tile.
+  constexpr bool kSweep = PB == 2;
   // publish block k: colb[buf][i][m] = C[i][m], rowb[buf][m][j] = R[m][j].
   // Block k lies in register column/row KB = PB k / 16 of its owners; KB is a
   // compile-time constant (the step loop is unrolled over it), so the owners
@@ -146,6 +153,7 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
       const int m = tx - base;
 #pragma unroll
       for (int a = 0; a < T; ++a) {
+        if (kSweep && a > KB) continue;  // lower tile: not kept (consumers read row K there)
         const double v = R[a][KB];
         const bool diag = (ty + 16 * a) == (int)(PB * k) + m;
         colb[buf][(ty + 16 * a) * PB + m] = diag ? v - 1.0 : v;
@@ -155,9 +163,10 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
       const int m = ty - base;
 #pragma unroll
       for (int b = 0; b < T; ++b) {
+        if (kSweep && b < KB) continue;  // lower tile: not kept (consumers read column K there)
         const double v = R[KB][b];
         const bool diag = (tx + 16 * b) == (int)(PB * k) + m;
-        rowb[buf][m * 128 + tx + 16 * b] = diag ? v + 1.0 : v;
+        rowb[buf][m * 128 + tx + 16 * b] = diag ? (kSweep ? v - 1.0 : v + 1.0) : v;
       }
     }
   };
@@ -219,10 +228,14 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
 #pragma unroll
     for (int m = 0; m < PB; ++m)
 #pragma unroll
-      for (int b = 0; b < T; ++b) rj[m][b] = rowb[buf][m * 128 + tx + 16 * b];
+      for (int b = 0; b < T; ++b)
+        rj[m][b] = (!kSweep || b >= KB) ? rowb[buf][m * 128 + tx + 16 * b] : colb[buf][(tx + 16 * b) * PB + m];
 #pragma unroll
     for (int a = 0; a < T; ++a) {
-      const double* c = &colb[buf][(ty + 16 * a) * PB];
+      double c[PB];
+#pragma unroll
+      for (int l = 0; l < PB; ++l)
+        c[l] = (!kSweep || a <= KB) ? colb[buf][(ty + 16 * a) * PB + l] : rowb[buf][l * 128 + ty + 16 * a];
       double w[PB];
 #pragma unroll
       for (int m = 0; m < PB; ++m) {
@@ -233,11 +246,17 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
       }
 #pragma unroll
       for (int b = 0; b < T; ++b) {
+        if (kSweep && a > b) continue;  // lower tile: never read
         double v = R[a][b];
 #pragma unroll
         for (int m = 0; m < PB; ++m) v = fma(-w[m], rj[m][b], v);
         R[a][b] = v;
       }
+    }
+    if constexpr (kSweep) {
+      // the swept pivots' diagonal: 2 I - P^-1 -> -P^-1
+      const int base = (int)((PB * k) & 15);
+      if (ty == tx && ty >= base && ty < base + PB) R[KB][KB] -= 2.0;
     }
     if (k + 1 < nblk) {
       if (sub + 1 < kSteps) {
@@ -260,9 +279,11 @@ __global__ void __launch_bounds__(kInvThreads, PB == 2 ? 2 : 1) mas_domain_inver
     const uint32_t rb = inv_tile_rowbase(nt, i >> 2);
 #pragma unroll
     for (int b = 0; b < T; ++b) {
+      if (kSweep && a > b) continue;  // strictly lower: no upper 4x4 tile there
       const uint32_t j = tx + 16 * b;
       if (i < 4 * nt && j < 4 * nt && (i >> 2) <= (j >> 2)) {
-        const float v = (i < n && j < n) ? (float)(R[a][b] * dinv[i] * dinv[j]) : 0.0f;
+        const double r = kSweep ? -R[a][b] : R[a][b];  // the sweep leaves -S^-1
+        const float v = (i < n && j < n) ? (float)(r * dinv[i] * dinv[j]) : 0.0f;
         out[16u * (rb + (j >> 2)) + 4 * (i & 3) + (j & 3)] = v;
       }
     }
