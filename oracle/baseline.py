@@ -1,6 +1,6 @@
 """Timed CPU restatement of one Newton step (oracle; bench baseline only).
 
-TEST/BASELINE INFRASTRUCTURE ONLY -- used by ``bench.py``'s ``cpu_baseline``
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY -- used by ``bench.py``'s ``cpu_baseline``
 and ``--impl reference`` legs.  It restates, vectorised with NumPy/SciPy,
 the reference's CPU path for the step: SNH gradient/Hessian with the
 reference's PSD-test + eigen projection rule, block assembly, the MAS
