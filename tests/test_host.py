@@ -164,3 +164,50 @@ def test_mas_tile_layout_host_math():
     assert ld >= t and ld % 8 == 1
     banks = {((i // 4) * ld * 4 + i % 4) % 32 for i in range(32)}
     assert len(banks) == 32
+
+
+def _tiled_sweep(s, tiles=6):
+  """Model of the domain-inverse kernel's symmetric 2-pivot sweep on a
+  16-row tile grid: only upper tiles are updated, lower tiles hold NaN, the
+  pivot column is read from column K for rows up to the pivot's tile and
+  from row K beyond it (the kernel's publish / read rule)."""
+  n = s.shape[0]
+  size = 16 * tiles
+  x = np.zeros((size, size))
+  x[:n, :n] = s
+  x[np.arange(n, size), np.arange(n, size)] = 1.0
+  tile = np.arange(size) // 16
+  upper = tile[:, None] <= tile[None, :]
+  x[~upper] = np.nan
+  for k in range(0, n, 2):
+    kb = k // 16
+    kk = [k, k + 1]
+    colb, rowb = x[:, kk].copy(), x[kk, :].copy()
+    for m in range(2):
+      colb[kk[m], m] -= 1.0
+      rowb[m, kk[m]] -= 1.0
+    pinv = np.linalg.inv(colb[kk, :] + np.eye(2))
+    vi = np.where((tile <= kb)[:, None], colb, rowb.T)
+    vj = np.where((tile >= kb)[:, None], rowb.T, colb)
+    x = np.where(upper, x - (vi @ pinv) @ vj.T, x)
+    x[k, k] -= 2.0
+    x[k + 1, k + 1] -= 2.0
+  return x
+
+
+def test_symmetric_sweep_model_reads_upper_tiles_only():
+  """The upper-tile sweep gives -S^-1 on every upper tile and never reads a
+  lower one (NaN there would spread)."""
+  rng = np.random.default_rng(3)
+  for n in (2, 18, 48, 96):
+    b = rng.normal(size=(n, n))
+    a = b @ b.T + n * np.eye(n)
+    d = 1.0 / np.sqrt(np.diag(a))
+    s = a * d[:, None] * d[None, :]
+    x = _tiled_sweep(s)
+    tile = np.arange(n) // 16
+    up = tile[:, None] <= tile[None, :]
+    got = -x[:n, :n]
+    assert not np.isnan(got[up]).any()
+    inv = np.linalg.inv(s)
+    assert np.abs(np.where(up, got - inv, 0.0)).max() <= 1e-12 * np.abs(inv).max()
