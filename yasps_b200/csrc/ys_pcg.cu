@@ -234,19 +234,26 @@ struct RefineParams {
   unsigned* ticket;
 };
 
+// kRowLanes threads a row on a resident-size grid striding over the row
+// groups (as pcg_spmv_dot), FP64 blocks.
 __global__ void __launch_bounds__(kPcgBlock) refine_residual(RefineParams P) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr uint32_t kRows = kPcgBlock / kRowLanes;
+  const uint32_t groups = (P.nv + kRows - 1) / kRows;
+  const int lane = (int)(threadIdx.x % kRowLanes);
   double v[2] = {0.0, 0.0};
-  if (i < P.nv) {
+  for (uint32_t gb = blockIdx.x; gb < groups; gb += gridDim.x) {  // block-uniform
+    const uint32_t i = gb * kRows + threadIdx.x / kRowLanes;
     double h[3];
-    spmv3_row(P.sets, P.nsets, false, i, P.x, h[0], h[1], h[2]);
+    spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.x, h[0], h[1], h[2]);
+    if (i < P.nv && lane == 0) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const double g = P.rhs[3ull * i + k];
-      const double r = g - h[k];
-      P.r[3ull * i + k] = r;
-      v[0] += r * r;
-      v[1] += g * g;
+      for (int k = 0; k < 3; ++k) {
+        const double g = P.rhs[3ull * i + k];
+        const double r = g - h[k];
+        P.r[3ull * i + k] = r;
+        v[0] += r * r;
+        v[1] += g * g;
+      }
     }
   }
   if (!grid_reduce_last<2>(v, P.partials, P.ticket)) return;
@@ -456,7 +463,9 @@ int32_t ys_pcg_run(void* handle, void* stream, ys_pcg_result* result) {
 }
 
 uint64_t ys_refine_workspace_doubles(uint32_t num_vars) {
-  return 2 + (ys::grid_for(num_vars, ys::kPcgBlock) + 1) * 2 + 2;
+  // norms (2) + ticket (2) + 2 partials per block, at most one block a row group
+  const uint64_t groups = (num_vars + ys::kPcgBlock / ys::kRowLanes - 1) / (ys::kPcgBlock / ys::kRowLanes);
+  return 4 + 2 * (groups + 1);
 }
 
 int32_t ys_refine_residual(const ys_matrix3* m, const double* rhs, double* x, const double* delta, double* r,
@@ -480,8 +489,16 @@ int32_t ys_refine_residual(const ys_matrix3* m, const double* rhs, double* x, co
   P.out = workspace;
   P.ticket = reinterpret_cast<unsigned*>(workspace + 2);
   P.partials = workspace + 4;
+  unsigned rgrid = ys::grid_for((uint64_t)nv * ys::kRowLanes, ys::kPcgBlock);
+  {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ys::refine_residual, ys::kPcgBlock, 0) == cudaSuccess &&
+        sms > 0 && per_sm > 0)
+      rgrid = std::min<unsigned>(rgrid, (unsigned)(sms * per_sm));
+  }
   YS_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned), s));
-  ys::refine_residual<<<grid, ys::kPcgBlock, 0, s>>>(P);
+  ys::refine_residual<<<rgrid, ys::kPcgBlock, 0, s>>>(P);
   YS_CHECK_LAUNCH();
   if (norms_host) {
     YS_CUDA_TRY(cudaMemcpyAsync(norms_host, workspace, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
