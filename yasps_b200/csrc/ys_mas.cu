@@ -395,6 +395,7 @@ __global__ void __launch_bounds__(kPcgBlock) mas_init_collect(MasPcg P) {
   st[kIter] = 0.0;
   st[kAlpha] = 0.0;
   st[kBeta] = 0.0;
+  st[kBarrierFail] = 0.0;
   int status = kContinue;
   double tol;
   if (P.stop_rule == YS_STOP_RESIDUAL) {
@@ -506,6 +507,132 @@ __global__ void __launch_bounds__(kPcgBlock) mas_iter_collect(MasPcg P) {
   }
   st[kStatus] = (double)status;
   cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+}
+
+// mas_iter_collect and pcg_direction in one cooperative (co-resident) grid:
+// each thread collects z for its nodes (the first two kept in registers,
+// further ones through P.z), the blocks meet at a grid barrier whose last
+// arriving block finishes the reductions and the iteration bookkeeping (the
+// code of mas_iter_collect, same order), then every thread sets p = z +
+// beta p for its nodes.  The barrier wait is bounded: a block that gives up
+// marks the solve void (kBarrierFail) and skips the direction.
+__global__ void __launch_bounds__(kPcgBlock) mas_iter_collect_direction(MasPcg P) {
+  __shared__ double red[kPcgBlock / 32];
+  __shared__ int last;
+  __shared__ int ok;
+  double* st = P.st;
+  const bool live = st[kStatus] == (double)kContinue;
+  if (!live) return;  // grid-uniform: nobody writes the status before the barrier
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  double z0[3] = {0.0, 0.0, 0.0}, z1[3] = {0.0, 0.0, 0.0};
+  double v[2] = {0.0, 0.0};
+  uint32_t kk = 0;
+  for (uint32_t i = i0; i < P.nv; i += stride, ++kk) {
+    double z[3];
+    collect_node(P, i, z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double r = P.r[3ull * i + k];
+      v[0] += r * z[k];
+      v[1] += r * r;
+    }
+    if (kk == 0) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) z0[k] = z[k];
+    } else if (kk == 1) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) z1[k] = z[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) P.z[3ull * i + k] = z[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const double sk = block_sum<kPcgBlock>(v[k], red);
+    if (threadIdx.x == 0) P.partials[(uint64_t)k * gridDim.x + blockIdx.x] = sk;
+  }
+  unsigned* count = P.tickets + 4;
+  unsigned* gen = P.tickets + 5;
+  __syncthreads();
+  unsigned g0 = 0;
+  if (threadIdx.x == 0) {
+    g0 = atomicAdd(gen, 0u);
+    __threadfence();
+    last = atomicAdd(count, 1u) == gridDim.x - 1;
+    ok = 1;
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+      v[k] = block_sum<kPcgBlock>(thread_partial_sum(P.partials + (uint64_t)k * gridDim.x, gridDim.x), red);
+    if (threadIdx.x == 0) {
+      const double next = v[0], prev = st[kDeltaOld];
+      const double it = st[kIter] + 1.0;
+      st[kIter] = it;
+      st[kDeltaNew] = next;
+      st[kRR] = v[1];
+      int status = kContinue;
+      // mas/pcg.py:80-98
+      if (!isfinite(next) || next < 0.0 || !isfinite(prev) || prev <= 0.0) {
+        st[kBeta] = 0.0;
+        status = kNonSpd;
+      } else {
+        st[kBeta] = next / prev;
+        const bool done = P.stop_rule == YS_STOP_RESIDUAL ? v[1] <= st[kTolAbs] : next <= st[kTolAbs];
+        if (done) status = kConverged;
+        else if (next == 0.0) status = kNonSpd;
+        else if (it >= st[kMaxItParam]) status = kMaxIter;
+      }
+      st[kStatus] = (double)status;
+      cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+      *count = 0u;
+      __threadfence();
+      atomicAdd(gen, 1u);  // release
+    }
+  } else if (threadIdx.x == 0) {
+    // bounded wait for the release (the grid is co-resident, so the last
+    // block always arrives; the bound only keeps a failure from hanging)
+    uint32_t spins = 0;
+    while (atomicAdd(gen, 0u) == g0) {
+      if (++spins > (1u << 24)) {
+        ok = 0;
+        st[kBarrierFail] = 1.0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (!ok) return;
+  const double st_status = *(volatile double*)&st[kStatus];
+  if (st_status == (double)kNonSpd) return;
+  const double beta = *(volatile double*)&st[kBeta];
+  kk = 0;
+  for (uint32_t i = i0; i < P.nv; i += stride, ++kk) {
+    double z[3];
+    if (kk == 0) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) z[k] = z0[k];
+    } else if (kk == 1) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) z[k] = z1[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) z[k] = P.z[3ull * i + k];
+    }
+    double p[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      p[k] = z[k] + P.p[3ull * i + k] * beta;
+      P.p[3ull * i + k] = p[k];
+    }
+    if (P.p32) P.p32[i] = make_float4((float)p[0], (float)p[1], (float)p[2], 0.0f);
+  }
 }
 
 __global__ void __launch_bounds__(kPcgBlock) mas_collect_only(MasPcg P) {
@@ -674,7 +801,26 @@ cudaError_t mas_add_update_nodes(void* mas, cudaGraph_t body, const cudaGraphNod
   cudaError_t e = add_kernel(body, &n0, deps, ndeps, fused ? (const void*)mas_update_restrict : (const void*)mas_update,
                              grid1, kPcgBlock, 0, a0);
   if (e == cudaSuccess) e = add_apply_nodes(h, P->M, body, &n0, 1, &n1, P->r, fused ? 1u : 0u);
-  if (e == cudaSuccess) e = add_kernel(body, &n2, &n1, 1, (const void*)mas_iter_collect, grid, kPcgBlock, 0, a0);
+  // collect + direction as one cooperative kernel when the device takes it
+  // (co-resident grid); otherwise mas_iter_collect and pcg_direction
+  if (e == cudaSuccess) {
+    int dev = 0, sms = 0, per_sm = 0, coop = 0;
+    const void* fn = (const void*)mas_iter_collect_direction;
+    bool fused = cudaGetDevice(&dev) == cudaSuccess &&
+                 cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+                 cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPcgBlock, 0) == cudaSuccess && per_sm > 0;
+    if (fused) {
+      const unsigned cgrid = std::min<unsigned>(grid, (unsigned)(sms * per_sm));
+      e = add_kernel(body, &n2, &n1, 1, fn, cgrid, kPcgBlock, 0, a0);
+      cudaKernelNodeAttrValue cv{};
+      cv.cooperative = 1;
+      if (e == cudaSuccess) e = cudaGraphKernelNodeSetAttribute(n2, cudaKernelNodeAttributeCooperative, &cv);
+      if (e == cudaSuccess) hooks->fused_direction = true;
+    } else {
+      e = add_kernel(body, &n2, &n1, 1, (const void*)mas_iter_collect, grid, kPcgBlock, 0, a0);
+    }
+  }
   *last = n2;
   return e;
 }

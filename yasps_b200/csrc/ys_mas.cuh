@@ -7,6 +7,7 @@ namespace ys {
 
 struct MasPcgHooks {
   void* params = nullptr;  // owned by the MAS handle
+  bool fused_direction = false;  // the loop body's last MAS node also updates p
 };
 
 // Nodes computing r = g - H x (or r = g), z = M^-1 r, p = z and the initial

@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
   st[kIter] = 0.0;
   st[kAlpha] = 0.0;
   st[kBeta] = 0.0;
+  st[kBarrierFail] = 0.0;
   int status = kContinue;
   double tol;
   if (P.stop_rule == YS_STOP_RESIDUAL) {
@@ -394,7 +395,9 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
           e = ys::mas_add_update_nodes(a.mas, body, &n1, 1, &n2, &h->mas);
         }
       }
-      if (e == cudaSuccess)
+      if (e == cudaSuccess && a.preconditioner != YS_PREC_BLOCK_JACOBI && h->mas.fused_direction)
+        n3 = n2;  // the MAS collect kernel updated p already
+      else if (e == cudaSuccess)
         e = ys::add_kernel(body, &n3, &n2, 1, (const void*)ys::pcg_direction, grid, ys::kPcgBlock, args1);
     }
   }
@@ -446,6 +449,13 @@ int32_t ys_pcg_status(void* handle, void* stream, ys_pcg_result* result) {
   result->delta = st[ys::kDeltaNew];
   result->residual0 = sqrt(st[ys::kRR0]);
   result->residual = sqrt(st[ys::kRR]);
+  if (st[ys::kBarrierFail] != 0.0) {
+    // a grid barrier of the loop gave up waiting (it never does when the
+    // grid is co-resident); nothing of the solve is valid
+    result->status = YS_ERR_CUDA;
+    ys_set_last_error("PCG grid barrier wait ran out", __FILE__, __LINE__);
+    return YS_ERR_CUDA;
+  }
   switch (status) {
     case ys::kConverged: result->status = (int32_t)it; break;
     case ys::kNonSpd: result->status = -(int32_t)it - 4; break;

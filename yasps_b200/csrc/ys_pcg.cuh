@@ -20,6 +20,7 @@ enum PcgSlot : int {
   kRR0 = 9,
   kGG = 10,        // rhs^T rhs
   kTolAbs = 11,    // threshold in the units of the stop rule
+  kBarrierFail = 12,  // nonzero: a grid barrier wait ran out (the solve is void)
   kTolParam = 13,  // solve parameters, written by the host before each launch
   kMaxItParam = 14,
   kSlots = 16
