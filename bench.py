@@ -345,7 +345,7 @@ def launches_per_newton_step(impl, its, refs):
   the grid restrictions of the levels above 64 nodes, the one-CTA tail of the
   rest, the level-0 and the coarse domain GEMVs, collect; every iteration =
   SpMV+dot, update (+ level-1 restriction), grid restrictions from level 2,
-  tail, the two GEMVs, collect, direction.
+  tail, the two GEMVs, collect + direction (one cooperative kernel).
   """
   t = impl._tables
   offs = [int(v) for v in t.level_node_offset]
@@ -358,7 +358,7 @@ def launches_per_newton_step(impl, its, refs):
   init = 1 + (first - 1) + tail_init + 1 + coarse + 1
   if levels > 1:
     f_it = max(first, 2)
-    per_it = 2 + (first - 2 if first > 2 else 0) + (1 if f_it < levels else 0) + 1 + coarse + 2
+    per_it = 2 + (first - 2 if first > 2 else 0) + (1 if f_it < levels else 0) + 1 + coarse + 1
   else:
     per_it = 2 + 1 + 2
   return 6 + (levels - 1) + 1 + 1 + 2 * refs + refs * init + its * per_it
@@ -400,7 +400,7 @@ def serving_leg(args):
   n = args.serving_requests
   srv = serving.NewtonServer(max_slots=64, passes=8, memory_budget=40e9, tolerance=args.tol)
   t0 = time.perf_counter()
-  srv.register(range(8, 49), slots_per_side=2)
+  srv.register(range(8, 49), slots_per_side=3)
   t_register = time.perf_counter() - t0
   srv.run(serving.poisson_fem_stream(count=82, mean_spacing=0.0, seed=99))
   # steady state: a saturated warm-up stream grows the per-side slot pools to
