@@ -267,15 +267,17 @@ def gpu_arm(args):
               "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
               "traffic": traffic, "bytes_per_launch": int(nbytes.value), "ms_per_launch": gemv_ms}
   roofline_spmv = spmv_roofline(mz.activeHessian(), hbm, peak_kind)
-  cpu = None
-  if rank == 0 and world == 1 and not args.no_cpu_baseline:
-    cpu = cpu_baseline_leg(cube, args.tol)
+  # the host-bound serving loop runs before the CPU baseline, whose worker
+  # threads would otherwise compete with it for the host cores
   serve = None
   if rank == 0 and world == 1 and args.serving_requests > 0:
     serve = serving_leg(args)
   cloth = None
   if rank == 0 and world == 1 and not args.no_cloth:
     cloth = cloth_leg(args)
+  cpu = None
+  if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu = cpu_baseline_leg(cube, args.tol)
   line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
           "vs_baseline": None, "dtype": "f32+f64 refine (f64 element Hessians and projection)",
