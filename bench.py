@@ -405,9 +405,11 @@ def serving_leg(args):
   srv.register(range(8, 49), slots_per_side=3)
   t_register = time.perf_counter() - t0
   srv.run(serving.poisson_fem_stream(count=82, mean_spacing=0.0, seed=99))
-  # steady state: a saturated warm-up stream grows the per-side slot pools to
-  # what a burst needs, so no slot is created inside the timed streams
-  srv.run(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=97))
+  # steady state: an untimed pass of the two timed streams grows the
+  # per-side slot pools to what they need, so no slot (device allocations,
+  # which synchronise) is created inside the timed streams
+  srv.run(serving.poisson_fem_stream(count=n, mean_spacing=2e-3, seed=0))
+  srv.run(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=0))
   srv.solve_serial_fp64(serving.poisson_fem_stream(count=41, mean_spacing=0.0, seed=98))
   out = {"workload": (f"{n} FEM Newton-step requests, Poisson arrivals (mean gap 2 ms), cube side U{{8..48}}, "
                       "E log-uniform [1e4, 1e6], nu U[0.3, 0.45], noise +-0.01, 40 GB admission budget, "
