@@ -68,6 +68,26 @@ def gemv_layout_bytes(tables) -> int:
   return int(sum(4 * inverse_floats(3 * int(k)) + 28 * int(k) for k in sizes))
 
 
+def trace_pcg(run):
+  """Kernels of one PCG graph launch with their device durations, from the
+  CUDA activity torch.profiler records (the kernels of the conditional loop
+  body are reported for one iteration)."""
+  from torch.profiler import ProfilerActivity, profile
+  run()
+  torch.cuda.synchronize()
+  with profile(activities=[ProfilerActivity.CUDA]) as prof:
+    run()
+    torch.cuda.synchronize()
+  events = [e for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA]
+  events.sort(key=lambda e: e.time_range.start)
+  rows = [{"kernel": e.name, "start_us": e.time_range.start, "us": e.time_range.elapsed_us()} for e in events]
+  t0 = rows[0]["start_us"] if rows else 0
+  for r in rows:
+    r["start_us"] = round(r["start_us"] - t0, 1)
+    r["us"] = round(r["us"], 1)
+  print(json.dumps(rows, indent=1))
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument("--side", type=int, default=64)
@@ -75,6 +95,8 @@ def main():
   ap.add_argument("--reps", type=int, default=20)
   ap.add_argument("--scene", default="fem", choices=["fem", "cloth"])
   ap.add_argument("--pairs", type=int, default=200_000)
+  ap.add_argument("--trace-pcg", action="store_true",
+                  help="print the kernels of one MAS-PCG launch (torch.profiler CUDA activity)")
   args = ap.parse_args()
   if args.scene == "cloth":
     return cloth_main(args)
@@ -128,6 +150,8 @@ def main():
   }
   nbytes = ctypes.c_uint64(0)
   L.call("ys_mas_gemv", mas._mas, st, ctypes.byref(nbytes))
+  if args.trace_pcg:
+    return trace_pcg(cases["pcg50_fp32"])
   out = {"side": args.side, "tets": cube.tet_count, "dof": cube.dofs, "blocks": p.num_unique,
          "gemv_alg_bytes": int(nbytes.value), "gemv_layout_bytes": gemv_layout_bytes(mas._tables),
          "non_psd": int(snh._const_cache[("work", snh.n)][1].item()), "pcg": mz.linearSolver.statistics}
