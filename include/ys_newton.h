@@ -243,6 +243,62 @@ typedef struct ys_energy_args {
  * these energies (hessianKernelHost.pyx:27-161).                           */
 int32_t ys_energy_eval(const ys_energy_args* args, void* stream);
 
+/* ---- affine (ABD) bodies ------------------------------------------------
+ * A body carries a 3x3 affine matrix A (9 DoF, row-major, the reference's
+ * `affine_matrices` attribute, examples/dropping_in_container_mixed/
+ * dropping_in_container.py:241-245) and a translation t (3 DoF); its
+ * vertices sit at x = A xbar + t (:261-270, xbar the body-frame rest
+ * position).  The 9 DoF of A are stored as three 3-DoF rows, so every block
+ * of the assembled matrix stays 3x3: an element's arguments are the rows
+ * a0, a1, a2 of its body's A and t (K = 3 or 4 arguments of size 3, codes
+ * from ys_join_union_indices over the rows-view [A rows (3 per body), t]).
+ * Kinds:
+ *   ORTHOGONALITY (helpers.py:201-211): stiffness * 1/2 |A^T A - I|_F^2 per
+ *     body, 3 arguments;
+ *   INERTIA (helpers.py:138-141 with x = A xbar + t, dropping_in_container.py:
+ *     378): 1/2 m |x - x~|^2 per vertex, x~ = x_before + v dt +
+ *     gravity dt^2, 4 arguments;
+ *   SNH (helpers.py:129-136 on the tet positions xbar A^T + t,
+ *     dropping_in_container.py:280-320, 370): Stable Neo-Hookean of one
+ *     single-body tetrahedron, 4 arguments.
+ * Gradients and Hessians by second-order forward-mode differentiation in
+ * the (A, t) coordinates, local Hessian projected (PSD test, then the
+ * negative modes) over the full 9x9 / 12x12, merged and scattered like
+ * ys_energy_eval.  No counterpart of the split rows in the reference, whose
+ * pattern keeps 9x9 / 9x3 blocks: the assembled matrix is the same.       */
+#define YS_AFFINE_ORTHOGONALITY 1
+#define YS_AFFINE_INERTIA 2
+#define YS_AFFINE_SNH 3
+
+typedef struct ys_affine_args {
+  int32_t kind;                 /* YS_AFFINE_*                                      */
+  const double* affine;         /* [num_bodies x 9] A per body, row-major           */
+  const double* translation;    /* [num_bodies x 3] t per body (INERTIA, SNH)       */
+  uint32_t num_bodies;
+  uint32_t num_elements;
+  const uint32_t* body;         /* [n] body of each element; NULL: element i is body i */
+  const double* rest;           /* INERTIA: [n x 3] xbar per vertex;                */
+                                /* SNH: [num_rest x 3] body-frame rest positions    */
+  const uint32_t* tets;         /* SNH: [n x 4] indices into rest                   */
+  uint32_t num_rest;
+  const double* x_before;       /* INERTIA: [n x 3]                                 */
+  const double* velocity;       /* INERTIA: [n x 3] or NULL (zero)                  */
+  const double* mass;           /* INERTIA: [n]                                     */
+  const double* mu;             /* SNH: per element, or NULL to use mu_value        */
+  const double* lam;            /* SNH: per element, or NULL to use lam_value       */
+  double mu_value, lam_value;
+  double dt;                    /* INERTIA, SNH                                     */
+  double gravity[3];            /* INERTIA                                          */
+  double stiffness;             /* ORTHOGONALITY                                    */
+  int32_t projection_method;    /* -1/0 none, 1 |lambda|, 2 max(lambda, 0)          */
+  ys_term_plan plan;
+  double* block_records;
+  double* grad_records;
+  double* energy;               /* [n] or NULL; records NULL: energies only         */
+} ys_affine_args;
+
+int32_t ys_affine_eval(const ys_affine_args* args, void* stream);
+
 /* Deterministic sum of n doubles into out[0] (device), fixed reduction order
  * for a given n; workspace: ys_sum_workspace_doubles() doubles.            */
 uint64_t ys_sum_workspace_doubles(void);
@@ -261,6 +317,8 @@ int32_t ys_assemble(const double* records, const uint32_t* begin, const uint32_t
 /* Per-variable diagonal blocks and scalar diagonal from assembled block sets.
  * Variable v of attribute a (count_a instances of size s_a) has scalar
  * offset seg_start[a] + i*s_a and diagonal block at diag_start[a] + i*s_a^2.
+ * Stored blocks smaller than s_a inside one variable (the 3x3 row blocks of
+ * an affine matrix) are placed at their offsets, off-diagonal ones mirrored.
  * Adds (accumulate != 0) or writes.  Replaces the diagonal / diagonal-block
  * accumulation of hessianKernelFullProject.pyx:186-212.                    */
 int32_t ys_extract_diagonal(const double* values, const uint32_t* positions,

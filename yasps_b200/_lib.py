@@ -67,6 +67,17 @@ class EnergyArgs(C.Structure):
               ("energy", vp)]
 
 
+class AffineArgs(C.Structure):
+  _fields_ = [("kind", i32), ("affine", vp), ("translation", vp), ("num_bodies", u32), ("num_elements", u32),
+              ("body", vp), ("rest", vp), ("tets", vp), ("num_rest", u32), ("x_before", vp), ("velocity", vp),
+              ("mass", vp), ("mu", vp), ("lam", vp), ("mu_value", f64), ("lam_value", f64), ("dt", f64),
+              ("gravity", f64 * 3), ("stiffness", f64), ("projection_method", i32), ("plan", TermPlan),
+              ("block_records", vp), ("grad_records", vp), ("energy", vp)]
+
+
+YS_AFFINE_ORTHOGONALITY, YS_AFFINE_INERTIA, YS_AFFINE_SNH = 1, 2, 3
+
+
 class Matrix3(C.Structure):
   _fields_ = [("num_sets", u32), ("values", vp * 2), ("values32", vp * 2), ("row_ptr", vp * 2),
               ("entry_block", vp * 2), ("entry_col", vp * 2), ("num_vars", u32)]
@@ -114,6 +125,7 @@ SIGNATURES = {
     "ys_snh_eval": (i32, [P(SnhArgs), vp]),
     "ys_inertia_eval": (i32, [P(InertiaArgs), vp]),
     "ys_energy_eval": (i32, [P(EnergyArgs), vp]),
+    "ys_affine_eval": (i32, [P(AffineArgs), vp]),
     "ys_sum_workspace_doubles": (u64, []),
     "ys_sum": (i32, [vp, u32, vp, vp, vp]),
     "ys_assemble": (i32, [vp, vp, vp, vp, vp, u32, vp, vp, vp]),

@@ -95,19 +95,42 @@ __global__ void extract_diag_kernel(const double* __restrict__ values, const uin
   const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nu) return;
   const uint32_t r = positions[2ull * u], c = positions[2ull * u + 1];
-  if (r != c) return;
   int a = 0;
   while (a + 1 < (int)L.n && r >= L.seg[a + 1]) ++a;
   const uint32_t s = L.size[a];
-  if (bdims[2ull * u] != s) return;
+  const uint32_t h = bdims[2ull * u], w = bdims[2ull * u + 1];
+  if (c < L.seg[a] || c >= L.seg[a + 1]) return;
   const uint32_t inst = (r - L.seg[a]) / s;
+  if ((c - L.seg[a]) / s != inst) return;
   const double* v = values + voff[u];
   double* d = dblocks ? dblocks + L.dstart[a] + (uint64_t)inst * s * s : nullptr;
-  for (uint32_t k = 0; k < s * s; ++k) {
-    if (d) d[k] = accumulate ? d[k] + v[k] : v[k];
+  if (r == c && h == s) {
+    for (uint32_t k = 0; k < s * s; ++k) {
+      if (d) d[k] = accumulate ? d[k] + v[k] : v[k];
+    }
+    if (diagonal)
+      for (uint32_t k = 0; k < s; ++k) diagonal[r + k] = accumulate ? diagonal[r + k] + v[k * s + k] : v[k * s + k];
+    return;
   }
-  if (diagonal)
-    for (uint32_t k = 0; k < s; ++k) diagonal[r + k] = accumulate ? diagonal[r + k] + v[k * s + k] : v[k * s + k];
+  // A block inside one instance of a larger attribute (the rows of an affine
+  // matrix are stored as 3x3 blocks): placed at its offset, mirrored when it
+  // lies off the diagonal.
+  const uint32_t base = L.seg[a] + inst * s, ro = r - base, co = c - base;
+  if (ro + h > s || co + w > s) return;
+  if (d)
+    for (uint32_t k = 0; k < h; ++k)
+      for (uint32_t l = 0; l < w; ++l) {
+        const double x = v[k * w + l];
+        double& e0 = d[(ro + k) * s + co + l];
+        e0 = accumulate ? e0 + x : x;
+        if (r != c) {
+          double& e1 = d[(co + l) * s + ro + k];
+          e1 = accumulate ? e1 + x : x;
+        }
+      }
+  if (diagonal && r == c)
+    for (uint32_t k = 0; k < h && k < w; ++k)
+      diagonal[r + k] = accumulate ? diagonal[r + k] + v[k * w + k] : v[k * w + k];
 }
 
 // |lambda| -> |1/lambda| (|lambda| < 1e-6 -> |lambda|), diagonalBlockInverseKernel.pyx:69,91.

@@ -301,21 +301,11 @@ __device__ __forceinline__ void write_records(const uint32_t (&code)[A], uint32_
 // Threads per CTA of the energy kernels (the projection stash is per thread).
 constexpr int kEnergyThreads = 32;
 
-template <class E>
-__global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const ys_energy_args a) {
-  constexpr int A = E::A, N = 3 * A;
-  extern __shared__ double energy_stash[];
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.num_elements) return;
-  Pts<A> x, r;
-#pragma unroll
-  for (int k = 0; k < A; ++k) {
-    const uint32_t id = a.conn[(uint64_t)t * A + k];
-    load_point(a.position, id, x.p[k]);
-    if (a.rest.num_children) load_point(a.rest, id, r.p[k]);
-    else r.p[k][0] = r.p[k][1] = r.p[k][2] = 0.0;
-  }
-  const HD<N> e = E::template eval<N>(a, t, x, r);
+// Energy, gradient records, projection and Hessian records of one element
+// from its HD<3A> energy (shared by the vertex-tuple and affine kernels).
+template <int A, class Args>
+__device__ __forceinline__ void finish_element(const Args& a, uint32_t t, const HD<3 * A>& e, double* stash) {
+  constexpr int N = 3 * A;
   if (a.energy) a.energy[t] = e.v;
   uint32_t code[A];
   load_arg_codes<A>(a.plan, t, code);
@@ -337,10 +327,27 @@ __global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const ys_energy_
     for (int rr = 0; rr < N; ++rr)
 #pragma unroll
       for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = h[utri<N>(c, rr)];
-    if (!psd_test_packed<N>(s))
-      project_negative_modes<N>(h, a.projection_method, energy_stash + threadIdx.x, blockDim.x);
+    if (!psd_test_packed<N>(s)) project_negative_modes<N>(h, a.projection_method, stash, blockDim.x);
   }
   write_records<A>(code, a.plan.coord_outer[t], a.plan.record, a.block_records, h);
+}
+
+template <class E>
+__global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const ys_energy_args a) {
+  constexpr int A = E::A, N = 3 * A;
+  extern __shared__ double energy_stash[];
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  Pts<A> x, r;
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    const uint32_t id = a.conn[(uint64_t)t * A + k];
+    load_point(a.position, id, x.p[k]);
+    if (a.rest.num_children) load_point(a.rest, id, r.p[k]);
+    else r.p[k][0] = r.p[k][1] = r.p[k][2] = 0.0;
+  }
+  const HD<N> e = E::template eval<N>(a, t, x, r);
+  finish_element<A>(a, t, e, energy_stash + threadIdx.x);
 }
 
 // Per-element energy only (line search): the same formulas on HD<0> numbers.
@@ -375,6 +382,205 @@ static int32_t launch_energy(const ys_energy_args& a, cudaStream_t s) {
   const size_t smem = sizeof(double) * project_stash_doubles<N>() * kEnergyThreads;
   YS_CUDA_TRY(cudaFuncSetAttribute(energy_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   energy_kernel<E><<<grid_for(a.num_elements, kEnergyThreads), kEnergyThreads, smem, s>>>(a);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+// ---- affine (ABD) bodies -------------------------------------------------
+// Inputs of an element: the rows of its body's A (inputs 3r + c = A[r][c],
+// row-major like the reference attribute) and t (inputs 9 + r).
+
+struct AffineBody {
+  double a[3][3];
+  double t[3];
+};
+
+// x_r = A[r] . xbar + t_r as an HD number: linear in the inputs, so its
+// gradient is (xbar at 3r .. 3r+2, 1 at 9 + r) and its Hessian zero.
+template <int N>
+__device__ __forceinline__ HD<N> affine_coord(const AffineBody& b, const double (&xb)[3], int r) {
+  HD<N> x = hd_const<N>(b.a[r][0] * xb[0] + b.a[r][1] * xb[1] + b.a[r][2] * xb[2] + b.t[r]);
+  if constexpr (N >= 12) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x.g[3 * r + c] = xb[c];
+    x.g[9 + r] = 1.0;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void load_rest3(const double* p, uint64_t i, double (&v)[3]) {
+  v[0] = __ldg(p + 3 * i);
+  v[1] = __ldg(p + 3 * i + 1);
+  v[2] = __ldg(p + 3 * i + 2);
+}
+
+// stiffness * 1/2 sum_rows |row(A^T A - I)|^2 (helpers.py:201-211).
+struct AffineOrthogonality {
+  static constexpr int A = 3;
+  template <int N>
+  __device__ static HD<N> eval(const ys_affine_args& a, uint32_t, const AffineBody& b) {
+    HD<N> m[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m[r][c] = hd_var<N>(b.a[r][c], 3 * r + c);
+    HD<N> acc = hd_const<N>(0.0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        // (A^T A)_ij = sum_k A_ki A_kj
+        HD<N> d = m[0][i] * m[0][j] + m[1][i] * m[1][j] + m[2][i] * m[2][j];
+        if (i == j) d = d - 1.0;
+        acc = acc + sq(d);
+      }
+    return (0.5 * a.stiffness) * acc;
+  }
+};
+
+// 1/2 m |A xbar + t - x~|^2, x~ = x_before + v dt + gravity dt^2.
+struct AffineInertia {
+  static constexpr int A = 4;
+  template <int N>
+  __device__ static HD<N> eval(const ys_affine_args& a, uint32_t e, const AffineBody& b) {
+    double xb[3], x0[3];
+    load_rest3(a.rest, e, xb);
+    load_rest3(a.x_before, e, x0);
+    const double h2 = a.dt * a.dt;
+    HD<N> acc = hd_const<N>(0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const double v = a.velocity ? __ldg(a.velocity + 3ull * e + r) : 0.0;
+      const double xt = x0[r] + v * a.dt + a.gravity[r] * h2;
+      acc = acc + sq(affine_coord<N>(b, xb, r) - xt);
+    }
+    return (0.5 * __ldg(a.mass + e)) * acc;
+  }
+};
+
+// Stable Neo-Hookean (helpers.py:129-136) of a tetrahedron of one body:
+// positions xbar_k A^T + t, F rows x_{k} - x_0, TB rows xbar_k - xbar_0,
+// IB = (TB^T)^-1, vol = det(TB^T) / 6, FI = F^T IB.
+struct AffineSnh {
+  static constexpr int A = 4;
+  template <int N>
+  __device__ static HD<N> eval(const ys_affine_args& a, uint32_t e, const AffineBody& b) {
+    const uint4 tv = reinterpret_cast<const uint4*>(a.tets)[e];
+    double xb[4][3];
+    load_rest3(a.rest, tv.x, xb[0]);
+    load_rest3(a.rest, tv.y, xb[1]);
+    load_rest3(a.rest, tv.z, xb[2]);
+    load_rest3(a.rest, tv.w, xb[3]);
+    double ed[3][3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ed[m][c] = xb[m + 1][c] - xb[0][c];
+    // (TB^T)^-1 rows: (e1 x e2, e2 x e0, e0 x e1) / det
+    double ib[3][3];
+    const double k0[3] = {ed[1][1] * ed[2][2] - ed[1][2] * ed[2][1], ed[1][2] * ed[2][0] - ed[1][0] * ed[2][2],
+                          ed[1][0] * ed[2][1] - ed[1][1] * ed[2][0]};
+    const double k1[3] = {ed[2][1] * ed[0][2] - ed[2][2] * ed[0][1], ed[2][2] * ed[0][0] - ed[2][0] * ed[0][2],
+                          ed[2][0] * ed[0][1] - ed[2][1] * ed[0][0]};
+    const double k2[3] = {ed[0][1] * ed[1][2] - ed[0][2] * ed[1][1], ed[0][2] * ed[1][0] - ed[0][0] * ed[1][2],
+                          ed[0][0] * ed[1][1] - ed[0][1] * ed[1][0]};
+    const double det = ed[0][0] * k0[0] + ed[0][1] * k0[1] + ed[0][2] * k0[2];
+    const double inv = 1.0 / det;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ib[0][c] = k0[c] * inv;
+      ib[1][c] = k1[c] * inv;
+      ib[2][c] = k2[c] * inv;
+    }
+    // Positions, then FI = F^T IB.  FI is linear in A: dFI_ij / dA_ic = M_cj
+    // with M = TB^T IB (the identity up to rounding) and dFI / dt = 0, so
+    // its entries are built as linear HD numbers.
+    double xs[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) xs[k][r] = b.a[r][0] * xb[k][0] + b.a[r][1] * xb[k][1] + b.a[r][2] * xb[k][2] + b.t[r];
+    HD<N> fi[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        fi[i][j] = hd_const<N>(ib[0][j] * (xs[1][i] - xs[0][i]) + ib[1][j] * (xs[2][i] - xs[0][i]) +
+                               ib[2][j] * (xs[3][i] - xs[0][i]));
+        if constexpr (N >= 12) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) fi[i][j].g[3 * i + c] = ed[0][c] * ib[0][j] + ed[1][c] * ib[1][j] + ed[2][c] * ib[2][j];
+        }
+      }
+    HD<N> ic = hd_const<N>(0.0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) ic = ic + sq(fi[i][j]);
+    const HD<N> J = fi[0][0] * (fi[1][1] * fi[2][2] - fi[1][2] * fi[2][1]) -
+                    fi[0][1] * (fi[1][0] * fi[2][2] - fi[1][2] * fi[2][0]) +
+                    fi[0][2] * (fi[1][0] * fi[2][1] - fi[1][1] * fi[2][0]);
+    const double mu = a.mu ? __ldg(a.mu + e) : a.mu_value;
+    const double lam = a.lam ? __ldg(a.lam + e) : a.lam_value;
+    const double alpha = 1.0 + 0.75 * mu / lam;
+    const HD<N> psi = (0.5 * mu) * (ic - 3.0) - (0.5 * mu) * hd_log(ic + 1.0) + (0.5 * lam) * sq(J - alpha);
+    return (det / 6.0 * a.dt * a.dt) * psi;
+  }
+};
+
+// Body of element e; false (element skipped) when an index is out of range.
+__device__ __forceinline__ bool load_affine_body(const ys_affine_args& a, uint32_t e, AffineBody& b) {
+  const uint32_t id = a.body ? __ldg(a.body + e) : e;
+  if (id >= a.num_bodies) return false;
+  if (a.tets) {
+    const uint4 tv = reinterpret_cast<const uint4*>(a.tets)[e];
+    if (tv.x >= a.num_rest || tv.y >= a.num_rest || tv.z >= a.num_rest || tv.w >= a.num_rest) return false;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b.a[r][c] = __ldg(a.affine + 9ull * id + 3 * r + c);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) b.t[r] = a.translation ? __ldg(a.translation + 3ull * id + r) : 0.0;
+  return true;
+}
+
+template <class E>
+__global__ void __launch_bounds__(kEnergyThreads) affine_kernel(const ys_affine_args a) {
+  constexpr int A = E::A, N = 3 * A;
+  extern __shared__ double energy_stash[];
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.num_elements) return;
+  AffineBody b;
+  if (!load_affine_body(a, e, b)) return;
+  const HD<N> en = E::template eval<N>(a, e, b);
+  finish_element<A>(a, e, en, energy_stash + threadIdx.x);
+}
+
+template <class E>
+__global__ void __launch_bounds__(128) affine_value_kernel(const ys_affine_args a) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.num_elements) return;
+  AffineBody b;
+  if (!load_affine_body(a, e, b)) return;
+  a.energy[e] = E::template eval<0>(a, e, b).v;
+}
+
+template <class E>
+static int32_t launch_affine(const ys_affine_args& a, cudaStream_t s) {
+  if (a.block_records == nullptr && a.grad_records == nullptr) {
+    YS_REQUIRE(a.energy, YS_ERR_INVALID, "energy-only evaluation needs the energy output");
+    affine_value_kernel<E><<<grid_for(a.num_elements, 128), 128, 0, s>>>(a);
+    YS_CHECK_LAUNCH();
+    return YS_OK;
+  }
+  YS_REQUIRE(a.block_records && a.grad_records, YS_ERR_INVALID, "block and gradient records go together");
+  YS_REQUIRE(a.plan.slot_stride >= 1 && a.plan.K == (uint32_t)E::A * a.plan.slot_stride, YS_ERR_INVALID,
+             "K must be the argument count * slot_stride");
+  constexpr int N = 3 * E::A;
+  const size_t smem = sizeof(double) * project_stash_doubles<N>() * kEnergyThreads;
+  YS_CUDA_TRY(cudaFuncSetAttribute(affine_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  affine_kernel<E><<<grid_for(a.num_elements, kEnergyThreads), kEnergyThreads, smem, s>>>(a);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }
@@ -426,6 +632,31 @@ int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
     default: break;
   }
   YS_REQUIRE(false, YS_ERR_INVALID, "unknown energy kind");
+}
+
+int32_t ys_affine_eval(const ys_affine_args* args, void* stream) {
+  YS_REQUIRE(args != nullptr, YS_ERR_INVALID, "null args");
+  const ys_affine_args& a = *args;
+  YS_REQUIRE(a.affine != nullptr && a.num_bodies > 0, YS_ERR_INVALID, "affine bodies needed");
+  if (a.num_elements == 0) return YS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (a.kind) {
+    case YS_AFFINE_ORTHOGONALITY:
+      YS_REQUIRE(a.tets == nullptr, YS_ERR_INVALID, "orthogonality takes no tets");
+      return ys::launch_affine<ys::AffineOrthogonality>(a, s);
+    case YS_AFFINE_INERTIA:
+      YS_REQUIRE(a.translation && a.rest && a.x_before && a.mass && a.tets == nullptr, YS_ERR_INVALID,
+                 "affine inertia needs translation, rest, x_before and mass");
+      return ys::launch_affine<ys::AffineInertia>(a, s);
+    case YS_AFFINE_SNH:
+      YS_REQUIRE(a.translation && a.rest && a.tets && a.num_rest > 0, YS_ERR_INVALID,
+                 "affine SNH needs translation, rest and tets");
+      YS_REQUIRE(((uintptr_t)a.tets & 15u) == 0, YS_ERR_INVALID, "tets must be 16-byte aligned");
+      YS_REQUIRE(a.lam || a.lam_value != 0.0, YS_ERR_INVALID, "affine SNH needs lambda (per element or a value)");
+      return ys::launch_affine<ys::AffineSnh>(a, s);
+    default: break;
+  }
+  YS_REQUIRE(false, YS_ERR_INVALID, "unknown affine kind");
 }
 
 }  // extern "C"

@@ -13,7 +13,7 @@ scene constants, or per-instance attributes of the energy's primitive.
 
 from __future__ import annotations
 
-from .graph import CONSTANT, DATA, JOIN, UNION, attribute
+from .graph import AFFINE, CONSTANT, DATA, JOIN, UNION, attribute
 
 
 class EnergyExpr:
@@ -46,13 +46,15 @@ def _param(v, prim, name):
   return ("value", float(v))
 
 
-def _join_of_positions(att, name, dim):
+def _join_of_positions(att, name, dim, affine=False):
   if not isinstance(att, attribute) or att.operator != JOIN:
     raise ValueError(f"{name} must be a JOIN attribute (addAttribute(..., through=..., source=...))")
   if att.through.dimension != dim or att.source.size != 3:
     raise ValueError(f"{name} must gather {dim} 3-vectors")
-  if att.source.operator not in (DATA, CONSTANT, UNION):
-    raise ValueError(f"{name}: the gathered attribute must be DATA, CONSTANT or a UNION of them")
+  allowed = (DATA, CONSTANT, UNION, AFFINE) if affine else (DATA, CONSTANT, UNION)
+  if att.source.operator not in allowed:
+    raise ValueError(f"{name}: the gathered attribute must be DATA, CONSTANT or a UNION of them"
+                     + (" (or affine body positions)" if affine else ""))
 
 
 class SnhEnergy(EnergyExpr):
@@ -60,11 +62,21 @@ class SnhEnergy(EnergyExpr):
 
   def __init__(self, tet_position_rest, tet_position, mu, lam, dt):
     super().__init__()
-    _join_of_positions(tet_position, "tet_position", 4)
+    _join_of_positions(tet_position, "tet_position", 4, affine=True)
     _join_of_positions(tet_position_rest, "tet_position_rest", 4)
     self.position = tet_position
     self.rest = tet_position_rest
     self.mu, self.lam, self.dt = mu, lam, dt
+    if tet_position.source.operator == AFFINE:
+      # tetrahedra of affine bodies: the element's arguments are its body's
+      # A rows and t (ys_affine_eval, YS_AFFINE_SNH)
+      if tet_position_rest.through is not tet_position.through:
+        raise ValueError("stable_neo_hookean: rest and current positions must use the same connectivity")
+      if tet_position_rest.source.operator not in (DATA, CONSTANT) or \
+          tet_position_rest.source.correspondance is not tet_position.source.correspondance:
+        raise ValueError("stable_neo_hookean: the rest positions of affine-body tets must be a DATA/CONSTANT "
+                         "attribute of the body vertices")
+      self.kind = "affine_snh"
 
   def validate(self, prim) -> None:
     if self.position.correspondance is not prim or self.rest.correspondance is not prim:
@@ -82,8 +94,13 @@ class InertiaEnergy(EnergyExpr):
   def __init__(self, x_before, vel, dt, x, mass, gravity):
     super().__init__()
     for a, name in ((x, "x"), (x_before, "x_before")):
-      if not isinstance(a, attribute) or a.size != 3 or a.operator not in (DATA, CONSTANT):
+      ok = (DATA, CONSTANT, AFFINE) if name == "x" else (DATA, CONSTANT)
+      if not isinstance(a, attribute) or a.size != 3 or a.operator not in ok:
         raise ValueError(f"inertia: {name} must be a 3-vector DATA/CONSTANT attribute of the primitive")
+    if x.operator == AFFINE:
+      # vertices of affine bodies: 1/2 m |A xbar + t - x~|^2 over the body's
+      # A rows and t (ys_affine_eval, YS_AFFINE_INERTIA)
+      self.kind = "affine_inertia"
     if vel is not None and (not isinstance(vel, attribute) or vel.size != 3):
       raise ValueError("inertia: vel must be a 3-vector attribute or None")
     self.x, self.x_before, self.vel = x, x_before, vel
@@ -94,8 +111,8 @@ class InertiaEnergy(EnergyExpr):
     for a in (self.x, self.x_before, self.vel):
       if a is not None and a.correspondance is not prim:
         raise ValueError("inertia: attributes must live on the energy's primitive")
-    if self.x.operator != DATA:
-      raise ValueError("inertia: x must be a DATA attribute")
+    if self.x.operator not in (DATA, AFFINE):
+      raise ValueError("inertia: x must be a DATA attribute or affine body positions")
     self.dt_p = _param(self.dt, prim, "dt")
     self.mass_p = _param(self.mass, prim, "mass")
 
@@ -206,3 +223,78 @@ def friction_point_triangle(position, old_position, fDhat, dt, frictionRate, lag
   Newton step as in the reference.
   """
   return FrictionPointTriangle(position, old_position, (fDhat, dt, frictionRate), per_element=lagged)
+
+
+# ---- affine (ABD) bodies ------------------------------------------------------------
+
+class AffinePosition:
+  """``x = A xbar + t`` of the vertices of affine bodies, the computed position
+  of ``examples/dropping_in_container_mixed/dropping_in_container.py:261-270``.
+
+  ``affine_matrix`` and ``translation`` are JOINs of dimension 1 through one
+  vertex-to-body connectivity of the bodies' 3x3 (row-major) and 3-vector
+  DATA attributes; ``rest_position`` is the body-frame rest position of the
+  vertices.  Bound with ``vertices.addAttribute("position",
+  computed_attribute=affine_position(...))``; :func:`inertia` and
+  :func:`stable_neo_hookean` accept the result (directly, or gathered by a
+  JOIN of tetrahedra) and differentiate with respect to A and t.
+  """
+
+  kind = "affine_position"
+
+  def __init__(self, affine_matrix, rest_position, translation):
+    for a, name, size in ((affine_matrix, "affine_matrix", 9), (translation, "translation", 3)):
+      if not isinstance(a, attribute) or a.operator != JOIN or a.through.dimension != 1 or a.source.size != size:
+        raise ValueError(f"affine_position: {name} must be a JOIN (dimension 1) of a {size}-entry body attribute")
+      if a.source.operator != DATA:
+        raise ValueError(f"affine_position: {name} must gather a DATA attribute of the bodies")
+    if affine_matrix.through is not translation.through:
+      raise ValueError("affine_position: affine_matrix and translation must use the same connectivity")
+    if affine_matrix.source.correspondance is not translation.source.correspondance:
+      raise ValueError("affine_position: A and t must live on the same body primitive")
+    if not isinstance(rest_position, attribute) or rest_position.size != 3 or \
+        rest_position.operator not in (DATA, CONSTANT):
+      raise ValueError("affine_position: rest_position must be a 3-vector DATA/CONSTANT attribute")
+    self.affine = affine_matrix.source
+    self.translation = translation.source
+    self.conn = affine_matrix.through
+    self.rest = rest_position
+    self.attribute = None
+
+  @property
+  def bodies(self):
+    return self.affine.correspondance
+
+  def bind(self, att) -> None:
+    if self.attribute is not None:
+      raise ValueError("affine_position can be bound to one attribute only")
+    prim = att.correspondance
+    if self.conn.correspondance is not prim or self.rest.correspondance is not prim:
+      raise ValueError("affine_position: the JOINs and the rest position must live on the vertex primitive")
+    self.attribute = att
+
+
+def affine_position(affine_matrix, rest_position, translation) -> AffinePosition:
+  """``affine_matrix * rest_position + translation`` for affine-body vertices."""
+  return AffinePosition(affine_matrix, rest_position, translation)
+
+
+class AffineOrthogonalityEnergy(EnergyExpr):
+  kind = "affine_ortho"
+
+  def __init__(self, rotation, stiffness):
+    super().__init__()
+    if not isinstance(rotation, attribute) or rotation.size != 9 or rotation.operator != DATA:
+      raise ValueError("affine_energy: rotation must be the bodies' 3x3 DATA attribute")
+    self.rotation = rotation
+    self.stiffness = float(stiffness)
+
+  def validate(self, prim) -> None:
+    if self.rotation.correspondance is not prim:
+      raise ValueError("affine_energy: the energy must live on the bodies' primitive")
+
+
+def affine_energy(rotation, stiffness=1.0) -> AffineOrthogonalityEnergy:
+  """``stiffness * 1/2 |A^T A - I|_F^2`` per body (``helpers.py:201-211``; the
+  reference helper has no stiffness, i.e. 1)."""
+  return AffineOrthogonalityEnergy(rotation, stiffness)

@@ -13,7 +13,10 @@ Newton inner loop consumes:
 * ``UNION``     -- ``primitiveUnion.addAttribute(name)``: the same-named attribute
   of every child, stacked in child order;
 * ``ENERGY``    -- ``primitive.addAttribute(name, computed_attribute=expr)`` with an
-  energy expression from :mod:`yasps_b200.energies`.
+  energy expression from :mod:`yasps_b200.energies`;
+* ``AFFINE``    -- ``primitive.addAttribute(name, computed_attribute=affine_position(...))``:
+  the positions ``A xbar + t`` of the vertices of affine bodies
+  (``examples/dropping_in_container_mixed/dropping_in_container.py:261-270``).
 
 The symbolic expression language of the reference (its ``attribute``
 arithmetic, autodiff and code generator) is not part of this library: the
@@ -30,7 +33,7 @@ from typing import List, Optional
 
 import numpy as np
 
-DATA, CONSTANT, JOIN, UNION, ENERGY = "DATA", "CONSTANT", "JOIN", "UNION", "ENERGY"
+DATA, CONSTANT, JOIN, UNION, ENERGY, AFFINE = "DATA", "CONSTANT", "JOIN", "UNION", "ENERGY", "AFFINE"
 
 _ids = itertools.count()
 
@@ -75,6 +78,17 @@ class attribute:
 
   def __repr__(self):
     return f"attribute({self.fullName}, {self.operator}, {self.rows}x{self.cols})"
+
+  def resize(self, rows: int, cols: int) -> "attribute":
+    """The same attribute seen as ``rows x cols`` (``PKG/attribute/attribute.pyx:250-255``);
+    a JOIN keeps its connectivity and source."""
+    if int(rows) * int(cols) != self.size:
+      raise ValueError(f"attribute.resize: {self.fullName} has {self.size} entries, not {rows}x{cols}")
+    view = attribute(self.name, self.correspondance, self.operator, rows, cols, through=self.through,
+                     source=self.source, children=self.children, expr=self.expr)
+    view._host, view._dev = self._host, self._dev
+    view.hash = self.hash
+    return view
 
   # -- values -----------------------------------------------------------------
   def updateValue(self, values) -> None:
@@ -221,11 +235,14 @@ class primitive:
         raise ValueError("primitive.addAttribute: the source must live on the connectivity target")
       att = attribute(name, self, JOIN, through.dimension, source.size, through=through, source=source)
     elif computed_attribute is not None:
-      from .energies import EnergyExpr
-      if not isinstance(computed_attribute, EnergyExpr):
+      from .energies import AffinePosition, EnergyExpr
+      if isinstance(computed_attribute, AffinePosition):
+        att = attribute(name, self, AFFINE, 3, 1, expr=computed_attribute)
+      elif isinstance(computed_attribute, EnergyExpr):
+        att = attribute(name, self, ENERGY, 1, 1, expr=computed_attribute)
+      else:
         raise TypeError("primitive.addAttribute: computed attributes must be energy expressions "
-                        "from yasps_b200.energies")
-      att = attribute(name, self, ENERGY, 1, 1, expr=computed_attribute)
+                        "or affine_position from yasps_b200.energies")
       computed_attribute.bind(att)
     else:
       att = attribute(name, self, DATA, rows, cols)

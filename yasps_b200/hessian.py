@@ -89,6 +89,34 @@ class _Term:
         return 2, int(self.wrt_start[k])
     return 1, 0
 
+  # -- affine bodies --------------------------------------------------------------
+  def _affine_position(self):
+    e = self.expr
+    return e.x.expr if e.kind == "affine_inertia" else e.position.source.expr
+
+  def affine_bodies(self):
+    """Device body index of every element (int32): the vertex-to-body
+    connectivity, through the tets for SNH (all four vertices of a tet must
+    belong to one body)."""
+    torch = _torch()
+    key = ("affine_body", self.n)
+    if key in self._const_cache:
+      return self._const_cache[key]
+    ap = self._affine_position()
+    vb = ap.conn.value.reshape(-1)
+    if self.expr.kind == "affine_inertia":
+      body = vb
+    else:
+      tets = self.expr.position.through.value.reshape(-1, 4).to(torch.int64)
+      tb = vb.to(torch.int64)[tets] if self.n else torch.zeros((0, 4), dtype=torch.int64, device=_dev())
+      if self.n and not bool((tb == tb[:, :1]).all().item()):
+        raise ValueError("stable_neo_hookean: every tetrahedron of affine bodies must lie in one body")
+      body = tb[:, 0].to(torch.int32).contiguous() if self.n else torch.zeros(1, dtype=torch.int32, device=_dev())
+    if self.n and int(body[:self.n].max().item()) >= ap.bodies.numInstances:
+      raise ValueError("affine bodies: a vertex refers to a body beyond the body primitive")
+    self._const_cache[key] = body
+    return body
+
   # -- slot codes ---------------------------------------------------------------
   def codes(self):
     """Device (codes int32 [n*K], sizes int16 [n*K], K, slot_stride)."""
@@ -111,6 +139,26 @@ class _Term:
       conn = self._const_cache[key]
       leaves, prefix = [self.expr.x], [0, n]
       dim = 1
+    elif self.expr.kind == "affine_ortho":
+      # arguments: the rows of A, gathered from A seen as 3 row-vectors a body
+      key = ("rows", n)
+      if key not in self._const_cache:
+        self._const_cache[key] = torch.arange(max(3 * n, 1), dtype=torch.int32, device=_dev())
+      conn = self._const_cache[key]
+      leaves, prefix = [self.expr.rotation], [0, 3 * n]
+      dim = 3
+    elif self.expr.kind in ("affine_inertia", "affine_snh"):
+      ap = self._affine_position()
+      nb = ap.bodies.numInstances
+      body = self.affine_bodies()
+      key = ("affine_conn", n, nb)
+      if key not in self._const_cache:
+        b = body[:n].to(torch.int64)
+        c = torch.stack([3 * b, 3 * b + 1, 3 * b + 2, 3 * nb + b], dim=1) if n else torch.zeros((1, 4), dtype=torch.int64, device=_dev())
+        self._const_cache[key] = c.to(torch.int32).contiguous()
+      conn = self._const_cache[key]
+      leaves, prefix = [ap.affine, ap.translation], [0, 3 * nb, 4 * nb]
+      dim = 4
     else:  # pragma: no cover
       raise NotImplementedError(self.expr.kind)
     nc = len(leaves)
@@ -199,6 +247,48 @@ class _Term:
       a.block_records, a.grad_records = L.ptr(block_records), L.ptr(grad_records)
       a.energy = L.ptr(energy)
       L.call("ys_energy_eval", ctypes.byref(a), s)
+    elif e.kind in ("affine_ortho", "affine_inertia", "affine_snh"):
+      import ctypes
+      a = L.AffineArgs()
+      a.num_elements = n
+      a.projection_method = self.projection_method
+      a.plan = plan
+      a.block_records, a.grad_records = L.ptr(block_records), L.ptr(grad_records)
+      a.energy = L.ptr(energy)
+      if e.kind == "affine_ortho":
+        a.kind = L.YS_AFFINE_ORTHOGONALITY
+        a.affine = L.ptr(e.rotation.value)
+        a.num_bodies = n
+        a.stiffness = e.stiffness
+      else:
+        ap = self._affine_position()
+        a.affine, a.translation = L.ptr(ap.affine.value), L.ptr(ap.translation.value)
+        a.num_bodies = ap.bodies.numInstances
+        a.body = L.ptr(self.affine_bodies())
+        a.dt = self._param(e.dt_p, n)[1]
+        if e.kind == "affine_inertia":
+          a.kind = L.YS_AFFINE_INERTIA
+          a.rest = L.ptr(ap.rest.value)
+          a.x_before = L.ptr(e.x_before.value)
+          a.velocity = L.ptr(e.vel.value) if e.vel is not None else None
+          m_arr, m_val = self._param(e.mass_p, n)
+          if m_arr is None:
+            key = ("mass", n, m_val)
+            if key not in self._const_cache:
+              self._const_cache[key] = torch.full((n,), m_val, dtype=torch.float64, device=_dev())
+            m_arr = self._const_cache[key]
+          a.mass = L.ptr(m_arr)
+          for k in range(3):
+            a.gravity[k] = e.gravity[k]
+        else:
+          a.kind = L.YS_AFFINE_SNH
+          a.rest = L.ptr(e.rest.source.value)
+          a.num_rest = e.rest.source.correspondance.numInstances
+          a.tets = L.ptr(e.position.through.value)
+          mu_arr, a.mu_value = self._param(e.mu_p, n)
+          lam_arr, a.lam_value = self._param(e.lam_p, n)
+          a.mu, a.lam = L.ptr(mu_arr), L.ptr(lam_arr)
+      L.call("ys_affine_eval", ctypes.byref(a), s)
     elif e.kind == "inertia":
       import ctypes
       a = L.InertiaArgs()

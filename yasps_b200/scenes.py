@@ -222,6 +222,119 @@ def fem_cube(n: int, spacing: float = 0.1, young: float = 1e5, poisson: float = 
       gravity=np.asarray(gravity, dtype=np.float64))
 
 
+# ---- affine (ABD) bodies beside a soft cube ---------------------------------------------
+
+@dataclass
+class AffineBodies:
+  """Arrays of ``num_bodies`` affine bodies: each an ``m^3`` lattice of tets
+  (the cube split above) in its body frame, placed by ``A xbar + t``."""
+
+  rest: np.ndarray          # (nv, 3) body-frame rest positions xbar
+  vertex_body: np.ndarray   # (nv,) body of each vertex
+  tets: np.ndarray          # (nt, 4) uint32 vertex indices (one body each)
+  affine: np.ndarray        # (nb, 9) A per body, row-major
+  translation: np.ndarray   # (nb, 3)
+  mass: np.ndarray          # (nv,) lumped masses
+  velocity: np.ndarray      # (nv, 3)
+  mu: float
+  lam: float
+  stiffness: float          # orthogonality scale
+  dt: float
+  gravity: np.ndarray
+
+  @property
+  def num_bodies(self) -> int:
+    return int(self.affine.shape[0])
+
+  def positions(self) -> np.ndarray:
+    a = self.affine.reshape(-1, 3, 3)[self.vertex_body]
+    return np.einsum("vrc,vc->vr", a, self.rest) + self.translation[self.vertex_body]
+
+
+def affine_bodies(num_bodies: int = 4, m: int = 3, spacing: float = 0.1, young: float = 1e7, poisson: float = 0.3,
+                  stiffness: float = 1e5, deform: float = 0.02, seed: int = 0, density: float = 1000.0,
+                  dt: float = 0.01, gravity=(0.0, 0.0, -9.8)) -> AffineBodies:
+  """Seeded affine bodies: A = R (I + S), R a random rotation, S symmetric with
+  entries U(-deform, deform); t spaced along x above the soft cube."""
+  rng = np.random.default_rng(seed)
+  g = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), axis=-1).reshape(-1, 3)
+  xbar = (g - (m - 1) / 2.0) * spacing
+  h = np.stack(np.meshgrid(np.arange(m - 1), np.arange(m - 1), np.arange(m - 1), indexing="ij"), axis=-1).reshape(-1, 3)
+  corner = h[:, None, :] + _CORNERS[None]
+  lex = corner[..., 0] * m * m + corner[..., 1] * m + corner[..., 2]
+  tl = lex[:, _SPLIT].reshape(-1, 4)
+  r = xbar[tl]
+  det = np.linalg.det(np.stack([r[:, 1] - r[:, 0], r[:, 2] - r[:, 0], r[:, 3] - r[:, 0]], axis=2))
+  flip = det < 0
+  tl[flip, 2], tl[flip, 3] = tl[flip, 3].copy(), tl[flip, 2].copy()
+  vmass = np.zeros(m ** 3)
+  np.add.at(vmass, tl.ravel(), np.repeat(density * np.abs(det) / 24.0, 4))
+  nv = m ** 3
+  affine, trans = [], []
+  for b in range(num_bodies):
+    q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+    if np.linalg.det(q) < 0:
+      q[:, 0] = -q[:, 0]
+    sym = rng.uniform(-deform, deform, size=(3, 3))
+    affine.append((q @ (np.eye(3) + 0.5 * (sym + sym.T))).ravel())
+    trans.append([0.4 * b, 0.0, 1.0] + rng.uniform(-0.01, 0.01, size=3))
+  mu, lam = lame(young, poisson)
+  return AffineBodies(
+      rest=np.tile(xbar, (num_bodies, 1)), vertex_body=np.repeat(np.arange(num_bodies), nv),
+      tets=(tl[None] + nv * np.arange(num_bodies)[:, None, None]).reshape(-1, 4).astype(np.uint32),
+      affine=np.asarray(affine), translation=np.asarray(trans), mass=np.tile(vmass, num_bodies),
+      velocity=rng.uniform(-0.01, 0.01, size=(num_bodies * nv, 3)), mu=mu, lam=lam, stiffness=stiffness, dt=dt,
+      gravity=np.asarray(gravity, dtype=np.float64))
+
+
+def affine_scene(cube: "FemCube", bodies: AffineBodies, name: str = "soft_and_affine", projection_method: int = 1):
+  """The soft cube of :func:`fem_scene` plus affine bodies, built the way
+  ``examples/dropping_in_container_mixed/dropping_in_container.py:235-405``
+  builds its ABD bunnies: body attributes ``affine_matrices`` (3x3) and
+  ``translations``, vertex positions ``A xbar + t`` through a vertex-to-body
+  connectivity, inertia of the body vertices, Stable Neo-Hookean of the body
+  tets, the orthogonality energy of the bodies, and the targets
+  ``[soft positions, affine_matrices, translations]``.
+  """
+  from .energies import affine_energy, affine_position, inertia, stable_neo_hookean
+  sc, hd = fem_scene(cube, name, projection_method)
+  dt = sc["dt"]
+  abd = sc.addMesh("bodies_abd")
+  prims = abd.addPrimitive("affine_bodies", numInstances=bodies.num_bodies)
+  affine_matrices = prims.addAttribute("affine_matrices", rows=3, cols=3)
+  affine_matrices.updateValue(bodies.affine)
+  translations = prims.addAttribute("translations", rows=3, cols=1)
+  translations.updateValue(bodies.translation)
+  nv = bodies.rest.shape[0]
+  verts = abd.addPrimitive("vertices_abd", numInstances=nv)
+  rest = verts.addConstant("rest_position", rows=3, cols=1)
+  rest.updateValue(bodies.rest)
+  last = verts.addConstant("last_position", rows=3, cols=1)
+  last.updateValue(bodies.positions())
+  vel = verts.addConstant("velocity", rows=3, cols=1)
+  vel.updateValue(bodies.velocity)
+  mass = verts.addConstant("mass")
+  mass.updateValue(bodies.mass)
+  v2b = verts.addConnectivity("v_abd2_abd", prims, bodies.vertex_body[:, None].astype(np.uint32), 1)
+  va = verts.addAttribute("affine_matrix", through=v2b, source=affine_matrices).resize(3, 3)
+  vt = verts.addAttribute("translation", through=v2b, source=translations).resize(3, 1)
+  vpos = verts.addAttribute("position", computed_attribute=affine_position(va, rest, vt))
+  tets = abd.addPrimitive("tets_abd", numInstances=bodies.tets.shape[0])
+  t2v = tets.addConnectivity("tets_abds2_vertices", verts, bodies.tets, 4)
+  tpos = tets.addAttribute("positions", through=t2v, source=vpos)
+  trest = tets.addAttribute("rest_positions", through=t2v, source=rest)
+  snh = tets.addAttribute("snh_abds", computed_attribute=stable_neo_hookean(trest, tpos, bodies.mu, bodies.lam, dt))
+  kin = verts.addAttribute("inertia_abds", computed_attribute=inertia(last, vel, dt, vpos, mass,
+                                                                       gravity=tuple(bodies.gravity)))
+  ortho = prims.addAttribute("affine_energy", computed_attribute=affine_energy(affine_matrices, bodies.stiffness))
+  sc.addEnergy(snh, projection_method=projection_method)
+  sc.addEnergy(kin, projection_method=-1)
+  sc.addEnergy(ortho, projection_method=2)
+  sc.addMinimizeTarget([hd["free_position"], affine_matrices, translations])
+  hd.update(affine_matrices=affine_matrices, translations=translations, vertices_abd=verts)
+  return sc, hd
+
+
 # ---- cloth over a static obstacle with synthetic contacts ------------------------------
 
 def lagged_friction_pt(x_old, dhat, kappa):

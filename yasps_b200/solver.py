@@ -197,6 +197,9 @@ class jacobianPCGSolver(_PcgBase):
       raise ValueError("jacobianPCGSolver.computeSolution: right_hand_side size must match the Hessian size.")
     torch = _torch()
     H = active_hessian
+    if any(w.size != 3 for w in H.wrt):
+      raise NotImplementedError("the device block-Jacobi PCG inverts 3x3 variable blocks; scenes with 9-DoF "
+                                "affine attributes are solved with the MAS solver")
     if self._jinv is None or self._jinv.numel() != H.diagonal_blocks.numel():
       self._jinv = torch.zeros_like(H.diagonal_blocks)
     nat = len(H.wrt)
