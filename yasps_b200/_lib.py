@@ -78,6 +78,11 @@ class AffineArgs(C.Structure):
 YS_AFFINE_ORTHOGONALITY, YS_AFFINE_INERTIA, YS_AFFINE_SNH = 1, 2, 3
 
 
+class CoupledArgs(C.Structure):
+  _fields_ = [("base", EnergyArgs), ("affine_child", u32), ("vertex_body", vp), ("rest", vp), ("affine", vp),
+              ("translation", vp), ("num_bodies", u32), ("status", vp)]
+
+
 class Matrix3(C.Structure):
   _fields_ = [("num_sets", u32), ("values", vp * 2), ("values32", vp * 2), ("row_ptr", vp * 2),
               ("entry_block", vp * 2), ("entry_col", vp * 2), ("num_vars", u32)]
@@ -126,6 +131,9 @@ SIGNATURES = {
     "ys_inertia_eval": (i32, [P(InertiaArgs), vp]),
     "ys_energy_eval": (i32, [P(EnergyArgs), vp]),
     "ys_affine_eval": (i32, [P(AffineArgs), vp]),
+    "ys_coupled_indices": (i32, [vp, u32, u32, u32, P(u32), P(i32), P(u32), u32, vp, u32, i32, u32, i32, u32, vp, vp,
+                                 vp]),
+    "ys_coupled_energy_eval": (i32, [P(CoupledArgs), vp]),
     "ys_sum_workspace_doubles": (u64, []),
     "ys_sum": (i32, [vp, u32, vp, vp, vp]),
     "ys_assemble": (i32, [vp, vp, vp, vp, vp, u32, vp, vp, vp]),

@@ -585,6 +585,352 @@ static int32_t launch_affine(const ys_affine_args& a, cudaStream_t s) {
   return YS_OK;
 }
 
+// ---- contact through affine-body vertices ----------------------------------
+// A barrier element over V union vertices, some of them affine-body vertices
+// x = A_b xbar + t_b.  Leaves per vertex: slot 0 the position of a plain
+// vertex; slots 0..2 the rows of A and slot 3 t for an affine vertex.  The
+// Jacobian block of slot s of vertex v (3 rows of x_v, 3 leaf entries) is
+// I3 for a plain position or t, and e_s xbar^T for row s of A.
+
+constexpr uint32_t kNoBody = 0xffffffffu;
+
+struct CoupledVertex {
+  double xbar[3];
+  uint32_t body;  // kNoBody: plain (free or DATA) vertex
+};
+
+struct UnionCodes {
+  uint32_t prefix[YS_MAX_UNION + 1];
+  int32_t kind[YS_MAX_UNION];
+  uint32_t wrt_start[YS_MAX_UNION];
+  uint32_t num_children;
+};
+
+// Union child of index idx (the last child whose range starts at or before it).
+__device__ __forceinline__ uint32_t union_child(const uint32_t* prefix, uint32_t num_children, uint32_t idx) {
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 1; k < YS_MAX_UNION; ++k)
+    if (k < (int)num_children && idx >= prefix[k]) c = k;
+  return c;
+}
+
+__device__ __forceinline__ uint32_t leaf_code(int32_t kind, uint32_t wrt_start, uint32_t local) {
+  return kind == 2 ? wrt_start + 3u * local + 2u : (kind == 1 ? 1u : 0u);
+}
+
+__global__ void coupled_codes_kernel(const uint32_t* __restrict__ conn, uint32_t n, uint32_t V, UnionCodes u,
+                                     uint32_t affine_child, const uint32_t* __restrict__ vertex_body,
+                                     uint32_t num_bodies, int32_t a_kind, uint32_t a_wrt, int32_t t_kind,
+                                     uint32_t t_wrt, uint32_t* __restrict__ codes, uint16_t* __restrict__ sizes) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  for (uint32_t v = 0; v < V; ++v) {
+    const uint32_t idx = conn[(uint64_t)t * V + v];
+    const uint64_t base = (uint64_t)t * 4 * V + 4 * v;
+    uint32_t c4[4] = {0u, 0u, 0u, 0u};
+    if (idx < u.prefix[u.num_children]) {
+      const uint32_t c = union_child(u.prefix, u.num_children, idx);
+      const uint32_t local = idx - u.prefix[c];
+      if (c == affine_child) {
+        const uint32_t b = vertex_body[local];
+        if (b < num_bodies) {
+#pragma unroll
+          for (int r = 0; r < 3; ++r) c4[r] = leaf_code(a_kind, a_wrt, 3u * b + r);
+          c4[3] = leaf_code(t_kind, t_wrt, b);
+        }
+      } else {
+        c4[0] = leaf_code(u.kind[c], u.wrt_start[c], local);
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      codes[base + s] = c4[s];
+      sizes[base + s] = c4[s] ? (uint16_t)3 : (uint16_t)0;
+    }
+  }
+}
+
+__device__ __forceinline__ bool load_coupled_point(const ys_coupled_args& a, uint32_t idx, double (&p)[3],
+                                                   CoupledVertex& cv) {
+  const ys_union3& u = a.base.position;
+  if (idx >= u.prefix[u.num_children]) return false;
+  const uint32_t c = union_child(u.prefix, u.num_children, idx);
+  const uint32_t local = idx - u.prefix[c];
+  if (c != a.affine_child) {
+    const double* s = u.child[c] + 3ull * local;
+    p[0] = __ldg(s);
+    p[1] = __ldg(s + 1);
+    p[2] = __ldg(s + 2);
+    cv.body = kNoBody;
+    cv.xbar[0] = cv.xbar[1] = cv.xbar[2] = 0.0;
+    return true;
+  }
+  const uint32_t b = __ldg(a.vertex_body + local);
+  if (b >= a.num_bodies) return false;
+  load_rest3(a.rest, local, cv.xbar);
+  cv.body = b;
+  const double* A = a.affine + 9ull * b;
+  const double* tr = a.translation + 3ull * b;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    p[r] = __ldg(A + 3 * r) * cv.xbar[0] + __ldg(A + 3 * r + 1) * cv.xbar[1] + __ldg(A + 3 * r + 2) * cv.xbar[2] +
+           __ldg(tr + r);
+  return true;
+}
+
+// J^T g for slot s of vertex cv.
+__device__ __forceinline__ void coupled_jt_vec(const CoupledVertex& cv, int s, const double* g, double (&out)[3]) {
+  if (cv.body != kNoBody && s < 3) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = cv.xbar[c] * g[s];
+  } else {
+    out[0] = g[0];
+    out[1] = g[1];
+    out[2] = g[2];
+  }
+}
+
+// Projection of the compressed Hessian through S = L^T H L (see the header):
+// h (packed upper, vertex coordinates) becomes H + L^-T (S' - S) L^-1.
+// Returns false when the body vertices' Gram matrix is not positive definite.
+template <int V>
+__device__ __forceinline__ bool coupled_project(double (&h)[3 * V * (3 * V + 1) / 2], const CoupledVertex (&cv)[V],
+                                                int method, double* stash) {
+  constexpr int N = 3 * V, H = N * (N + 1) / 2;
+  double L[V][V], Li[V][V];
+#pragma unroll
+  for (int i = 0; i < V; ++i)
+#pragma unroll
+    for (int j = 0; j < V; ++j) L[i][j] = Li[i][j] = 0.0;
+  // Cholesky of the Gram matrix m (m_ij = xbar_i . xbar_j + 1 within one body)
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+#pragma unroll
+    for (int i = j; i < V; ++i) {
+      double m;
+      if (i == j)
+        m = cv[i].body == kNoBody ? 1.0
+                                  : cv[i].xbar[0] * cv[i].xbar[0] + cv[i].xbar[1] * cv[i].xbar[1] +
+                                        cv[i].xbar[2] * cv[i].xbar[2] + 1.0;
+      else
+        m = (cv[i].body != kNoBody && cv[i].body == cv[j].body)
+                ? cv[i].xbar[0] * cv[j].xbar[0] + cv[i].xbar[1] * cv[j].xbar[1] + cv[i].xbar[2] * cv[j].xbar[2] + 1.0
+                : 0.0;
+      const double m0 = m;
+#pragma unroll
+      for (int k = 0; k < j; ++k) m -= L[i][k] * L[j][k];
+      if (i == j) {
+        if (!(m > 1e-12 * m0)) return false;
+        L[j][j] = sqrt(m);
+      } else {
+        L[i][j] = m / L[j][j];
+      }
+    }
+  }
+  // L^-1 (lower triangular)
+#pragma unroll
+  for (int i = 0; i < V; ++i) {
+    Li[i][i] = 1.0 / L[i][i];
+#pragma unroll
+    for (int j = 0; j < i; ++j) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = j; k < i; ++k) acc += L[i][k] * Li[k][j];
+      Li[i][j] = -acc * Li[i][i];
+    }
+  }
+  // S = L^T H L, entry (3v+k, 3w+l) = sum_{p>=v, q>=w} L[p][v] L[q][w] H(3p+k, 3q+l)
+  double sm[H];
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = i; j < N; ++j) {
+      const int v = i / 3, k = i % 3, w = j / 3, l = j % 3;
+      double acc = 0.0;
+#pragma unroll
+      for (int p = v; p < V; ++p)
+#pragma unroll
+        for (int q = w; q < V; ++q) acc += L[p][v] * L[q][w] * h[sym<N>(3 * p + k, 3 * q + l)];
+      sm[utri<N>(i, j)] = acc;
+    }
+  double s[H];  // packed lower copy for the PSD test
+#pragma unroll
+  for (int rr = 0; rr < N; ++rr)
+#pragma unroll
+    for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = sm[utri<N>(c, rr)];
+  if (psd_test_packed<N>(s)) return true;
+  double d[H];
+#pragma unroll
+  for (int i = 0; i < H; ++i) d[i] = sm[i];
+  project_negative_modes<N>(sm, method, stash, blockDim.x);
+#pragma unroll
+  for (int i = 0; i < H; ++i) d[i] = sm[i] - d[i];
+  // H += L^-T D L^-1, entry (3p+k, 3q+l) += sum_{v>=p, w>=q} Li[v][p] Li[w][q] D(3v+k, 3w+l)
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = i; j < N; ++j) {
+      const int p = i / 3, k = i % 3, q = j / 3, l = j % 3;
+      double acc = 0.0;
+#pragma unroll
+      for (int v = p; v < V; ++v)
+#pragma unroll
+        for (int w = q; w < V; ++w) acc += Li[v][p] * Li[w][q] * d[sym<N>(3 * v + k, 3 * w + l)];
+      h[utri<N>(i, j)] += acc;
+    }
+  return true;
+}
+
+// Records of the compressed Hessian: target slots merged by code in
+// first-occurrence order (the coordinates' order), block (gi, gj) =
+// sum over slots k in gi, l in gj of J_k^T H(v_k, v_l) J_l, transposed when
+// the row leaf's code exceeds the column leaf's.
+template <int V>
+__device__ __forceinline__ void coupled_records(const uint32_t (&code)[4 * V], const CoupledVertex (&cv)[V],
+                                                uint32_t occ0, const uint32_t* record, double* out,
+                                                const double (&h)[3 * V * (3 * V + 1) / 2]) {
+  constexpr int N = 3 * V, K = 4 * V;
+  int group[K], first[K];
+  int nfirst = 0;
+  for (int k = 0; k < K; ++k) {
+    group[k] = -1;
+    if (code[k] < 2) continue;
+    int g = -1;
+    for (int q = 0; q < nfirst; ++q)
+      if (code[first[q]] == code[k]) g = q;
+    if (g < 0) { first[nfirst] = k; g = nfirst++; }
+    group[k] = g;
+  }
+  uint32_t occ = occ0;
+  for (int gi = 0; gi < nfirst; ++gi)
+    for (int gj = gi; gj < nfirst; ++gj) {
+      double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int ka = 0; ka < K; ++ka) {
+        if (group[ka] != gi) continue;
+        const int v = ka >> 2, s = ka & 3;
+        const bool rowA = cv[v].body != kNoBody && s < 3;
+        for (int kb = 0; kb < K; ++kb) {
+          if (group[kb] != gj) continue;
+          const int w = kb >> 2, u = kb & 3;
+          const bool rowB = cv[w].body != kNoBody && u < 3;
+          double hb[3][3], lt[3][3];
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) hb[r][c] = h[sym<N>(3 * v + r, 3 * w + c)];
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) lt[r][c] = rowA ? cv[v].xbar[r] * hb[s][c] : hb[r][c];
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[r][c] += rowB ? lt[r][u] * cv[w].xbar[c] : lt[r][c];
+        }
+      }
+      double* dst = out + record[occ++];
+      const bool upper = code[first[gi]] < code[first[gj]];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[3 * r + c] = upper ? acc[r][c] : acc[c][r];
+    }
+}
+
+template <class E>
+__global__ void __launch_bounds__(kEnergyThreads) coupled_kernel(const ys_coupled_args a) {
+  constexpr int V = E::A, N = 3 * V, K = 4 * V;
+  extern __shared__ double energy_stash[];
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.base.num_elements) return;
+  Pts<V> x, r;
+  CoupledVertex cv[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    if (!load_coupled_point(a, a.base.conn[(uint64_t)t * V + v], x.p[v], cv[v])) {
+      if (a.status) atomicCAS(a.status, 0, (int32_t)(t + 1));
+      return;
+    }
+    r.p[v][0] = r.p[v][1] = r.p[v][2] = 0.0;
+  }
+  const HD<N> e = E::template eval<N>(a.base, t, x, r);
+  if (a.base.energy) a.base.energy[t] = e.v;
+  uint32_t code[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) code[k] = a.base.plan.codes[(uint64_t)t * K + k];
+  uint32_t q = a.base.plan.grad_outer[t];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (code[k] < 2) continue;
+    double gq[3];
+    coupled_jt_vec(cv[k >> 2], k & 3, &e.g[3 * (k >> 2)], gq);
+    double* dst = a.base.grad_records + a.base.plan.grad_record[q++];
+    dst[0] = gq[0];
+    dst[1] = gq[1];
+    dst[2] = gq[2];
+  }
+  double h[HD<N>::H];
+#pragma unroll
+  for (int i = 0; i < HD<N>::H; ++i) h[i] = e.h[i];
+  if (a.base.projection_method >= 1) {
+    bool any = false;
+#pragma unroll
+    for (int v = 0; v < V; ++v) any |= cv[v].body != kNoBody;
+    if (!any) {
+      double s[HD<N>::H];
+#pragma unroll
+      for (int rr = 0; rr < N; ++rr)
+#pragma unroll
+        for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = h[utri<N>(c, rr)];
+      if (!psd_test_packed<N>(s))
+        project_negative_modes<N>(h, a.base.projection_method, energy_stash + threadIdx.x, blockDim.x);
+    } else if (!coupled_project<V>(h, cv, a.base.projection_method, energy_stash + threadIdx.x)) {
+      if (a.status) atomicCAS(a.status, 0, (int32_t)(t + 1));
+    }
+  }
+  coupled_records<V>(code, cv, a.base.plan.coord_outer[t], a.base.plan.record, a.base.block_records, h);
+}
+
+template <class E>
+__global__ void __launch_bounds__(128) coupled_value_kernel(const ys_coupled_args a) {
+  constexpr int V = E::A;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.base.num_elements) return;
+  Pts<V> x, r;
+  CoupledVertex cv[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    if (!load_coupled_point(a, a.base.conn[(uint64_t)t * V + v], x.p[v], cv[v])) {
+      if (a.status) atomicCAS(a.status, 0, (int32_t)(t + 1));
+      a.base.energy[t] = 0.0;
+      return;
+    }
+    r.p[v][0] = r.p[v][1] = r.p[v][2] = 0.0;
+  }
+  a.base.energy[t] = E::template eval<0>(a.base, t, x, r).v;
+}
+
+template <class E>
+static int32_t launch_coupled(const ys_coupled_args& a, cudaStream_t s) {
+  YS_REQUIRE(a.base.arity == (uint32_t)E::A, YS_ERR_INVALID, "arity does not match the energy kind");
+  if (a.base.block_records == nullptr && a.base.grad_records == nullptr) {
+    YS_REQUIRE(a.base.energy, YS_ERR_INVALID, "energy-only evaluation needs the energy output");
+    coupled_value_kernel<E><<<grid_for(a.base.num_elements, 128), 128, 0, s>>>(a);
+    YS_CHECK_LAUNCH();
+    return YS_OK;
+  }
+  YS_REQUIRE(a.base.block_records && a.base.grad_records, YS_ERR_INVALID, "block and gradient records go together");
+  YS_REQUIRE(a.base.plan.slot_stride == 1 && a.base.plan.K == 4u * E::A, YS_ERR_INVALID,
+             "coupled codes take K = 4 * arity slots, stride 1");
+  constexpr int N = 3 * E::A;
+  const size_t smem = sizeof(double) * project_stash_doubles<N>() * kEnergyThreads;
+  YS_CUDA_TRY(cudaFuncSetAttribute(coupled_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  coupled_kernel<E><<<grid_for(a.base.num_elements, kEnergyThreads), kEnergyThreads, smem, s>>>(a);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
 }  // namespace ys
 
 extern "C" {
@@ -657,6 +1003,50 @@ int32_t ys_affine_eval(const ys_affine_args* args, void* stream) {
     default: break;
   }
   YS_REQUIRE(false, YS_ERR_INVALID, "unknown affine kind");
+}
+
+int32_t ys_coupled_indices(const uint32_t* connectivity, uint32_t n, uint32_t arity, uint32_t num_children,
+                           const uint32_t* child_prefix, const int32_t* child_kind,
+                           const uint32_t* child_wrt_start, uint32_t affine_child,
+                           const uint32_t* vertex_body, uint32_t num_bodies, int32_t affine_kind,
+                           uint32_t affine_wrt_start, int32_t translation_kind,
+                           uint32_t translation_wrt_start, uint32_t* codes, uint16_t* sizes,
+                           void* stream) {
+  YS_REQUIRE(arity >= 2 && arity <= 4, YS_ERR_INVALID, "coupled barriers take 2 to 4 vertices");
+  YS_REQUIRE(num_children >= 1 && num_children <= YS_MAX_UNION && affine_child < num_children, YS_ERR_INVALID,
+             "bad union or affine child");
+  YS_REQUIRE(child_prefix && child_kind && child_wrt_start, YS_ERR_INVALID, "union description needed");
+  if (n == 0) return YS_OK;
+  YS_REQUIRE(connectivity && vertex_body && codes && sizes, YS_ERR_INVALID, "null pointer");
+  ys::UnionCodes u{};
+  for (uint32_t c = 0; c <= num_children; ++c) u.prefix[c] = child_prefix[c];
+  for (uint32_t c = 0; c < num_children; ++c) { u.kind[c] = child_kind[c]; u.wrt_start[c] = child_wrt_start[c]; }
+  u.num_children = num_children;
+  ys::coupled_codes_kernel<<<ys::grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(
+      connectivity, n, arity, u, affine_child, vertex_body, num_bodies, affine_kind, affine_wrt_start,
+      translation_kind, translation_wrt_start, codes, sizes);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_coupled_energy_eval(const ys_coupled_args* args, void* stream) {
+  YS_REQUIRE(args != nullptr, YS_ERR_INVALID, "null args");
+  const ys_coupled_args& a = *args;
+  YS_REQUIRE(a.base.position.num_children >= 1 && a.base.position.num_children <= YS_MAX_UNION, YS_ERR_INVALID,
+             "bad position union");
+  YS_REQUIRE(a.affine_child < a.base.position.num_children, YS_ERR_INVALID, "affine child outside the union");
+  YS_REQUIRE(a.vertex_body && a.rest && a.affine && a.translation && a.num_bodies > 0, YS_ERR_INVALID,
+             "affine bodies needed");
+  if (a.base.num_elements == 0) return YS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (a.base.kind) {
+    case YS_ENERGY_POINT_POINT: return ys::launch_coupled<ys::PointPoint>(a, s);
+    case YS_ENERGY_POINT_EDGE: return ys::launch_coupled<ys::PointEdge>(a, s);
+    case YS_ENERGY_POINT_TRIANGLE: return ys::launch_coupled<ys::PointTriangle>(a, s);
+    case YS_ENERGY_EDGE_EDGE: return ys::launch_coupled<ys::EdgeEdge>(a, s);
+    default: break;
+  }
+  YS_REQUIRE(false, YS_ERR_INVALID, "coupled evaluation takes the PP, PE, PT and EE barriers");
 }
 
 }  // extern "C"

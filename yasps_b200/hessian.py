@@ -25,7 +25,7 @@ from typing import List, Optional
 import numpy as np
 
 from . import _lib as L
-from .graph import CONSTANT, DATA, JOIN, UNION, resolve_leaf_children
+from .graph import AFFINE, CONSTANT, DATA, JOIN, UNION, resolve_leaf_children
 
 
 def _torch():
@@ -117,11 +117,49 @@ class _Term:
     self._const_cache[key] = body
     return body
 
+  def coupled(self):
+    """``(leaves, prefix, affine child, AffinePosition)`` when the barrier's
+    position union holds the vertices of affine bodies (``x = A xbar + t``,
+    the collision union of ``dropping_in_container.py:344``), else None."""
+    key = ("coupled",)
+    if key in self._const_cache:
+      return self._const_cache[key]
+    out = None
+    if self.expr.kind == "vertex":
+      leaves, prefix = resolve_leaf_children(self.expr.position.source)
+      idx = [i for i, l in enumerate(leaves) if l.operator == AFFINE]
+      if len(idx) > 1:
+        raise ValueError("a position union may hold one primitive of affine-body vertices")
+      if idx:
+        if self.expr.code not in (1, 2, 3, 4):
+          raise ValueError(f"{type(self.expr).__name__}: only the PP/PE/PT/EE barriers take affine-body vertices")
+        ap = leaves[idx[0]].expr
+        vb = ap.conn.value.reshape(-1)
+        if vb.numel() and int(vb.max().item()) >= ap.bodies.numInstances:
+          raise ValueError("affine bodies: a vertex refers to a body beyond the body primitive")
+        out = (leaves, prefix, idx[0], ap)
+    self._const_cache[key] = out
+    return out
+
   # -- slot codes ---------------------------------------------------------------
   def codes(self):
     """Device (codes int32 [n*K], sizes int16 [n*K], K, slot_stride)."""
     torch = _torch()
     n = self.n
+    cp = self.coupled()
+    if cp is not None:
+      leaves, prefix, ac, ap = cp
+      kinds, starts = zip(*((0, 0) if i == ac else self.leaf_kind(l) for i, l in enumerate(leaves)))
+      ak, aw = self.leaf_kind(ap.affine)
+      tk, tw = self.leaf_kind(ap.translation)
+      K = 4 * self.expr.arity
+      codes = torch.empty(max(n * K, 1), dtype=torch.int32, device=_dev())
+      sizes = torch.empty(max(n * K, 1), dtype=torch.int16, device=_dev())
+      arr = lambda v, t: (t * len(v))(*v)
+      L.call("ys_coupled_indices", L.ptr(self.expr.position.through.value), n, self.expr.arity, len(leaves),
+             arr(prefix, L.u32), arr(kinds, L.i32), arr(starts, L.u32), ac, L.ptr(ap.conn.value),
+             ap.bodies.numInstances, ak, aw, tk, tw, L.ptr(codes), L.ptr(sizes), L.stream_ptr())
+      return codes, sizes, K, 1
     if self.expr.kind == "snh":
       join = self.expr.position
       conn = join.through.value
@@ -186,7 +224,7 @@ class _Term:
     leaves, prefix = resolve_leaf_children(att)
     u = L.Union3()
     for c, leaf in enumerate(leaves):
-      u.child[c] = L.ptr(leaf.value)
+      u.child[c] = None if leaf.operator == AFFINE else L.ptr(leaf.value)
     for c, p in enumerate(prefix):
       u.prefix[c] = p
     u.num_children = len(leaves)
@@ -246,7 +284,24 @@ class _Term:
       a.plan = plan
       a.block_records, a.grad_records = L.ptr(block_records), L.ptr(grad_records)
       a.energy = L.ptr(energy)
-      L.call("ys_energy_eval", ctypes.byref(a), s)
+      cp = self.coupled()
+      if cp is None:
+        L.call("ys_energy_eval", ctypes.byref(a), s)
+      else:
+        ap = cp[3]
+        c = L.CoupledArgs()
+        c.base = a
+        c.affine_child = cp[2]
+        c.vertex_body = L.ptr(ap.conn.value)
+        c.rest = L.ptr(ap.rest.value)
+        c.affine, c.translation = L.ptr(ap.affine.value), L.ptr(ap.translation.value)
+        c.num_bodies = ap.bodies.numInstances
+        if "status" not in self._const_cache:
+          self._const_cache["status"] = torch.zeros(1, dtype=torch.int32, device=_dev())
+        st = self._const_cache["status"]
+        st.zero_()
+        c.status = L.ptr(st)
+        L.call("ys_coupled_energy_eval", ctypes.byref(c), s)
     elif e.kind in ("affine_ortho", "affine_inertia", "affine_snh"):
       import ctypes
       a = L.AffineArgs()
@@ -509,6 +564,14 @@ class hessian:
         t = d["term"]
         eng = self.energy_buffers.get(id(t))
         t.evaluate(self._term_plan(d, bs), bs.records, self._grad_records, eng)
+    statuses = [d["term"]._const_cache["status"] for bs in (self._static, self._dynamic) for d in bs.infos
+                if "status" in d["term"]._const_cache]
+    if statuses:
+      st = torch.cat(statuses).cpu()
+      if bool((st != 0).any()):
+        k = int((st != 0).nonzero()[0, 0])
+        raise ValueError(f"contact with affine bodies: element {int(st[k]) - 1} of a barrier term has affinely "
+                         "dependent body vertices (degenerate Gram matrix)")
     for bs in (self._static, self._dynamic):
       self._assemble(bs)
     self.gradient.value.zero_()

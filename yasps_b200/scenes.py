@@ -504,3 +504,75 @@ def cloth_contact_scene(cc: ClothContact, projection_method: int = 1):
   sc.addEnergy(kin, projection_method=-1)
   sc.addMinimizeTarget([pos])
   return sc, dict(position=pos, old_position=old)
+
+
+# ---- contact between cloth, affine bodies and a container ------------------------------
+
+BARRIER_PAIRS = (("pp", 2), ("pe", 3), ("pt", 4), ("ee", 4))
+
+
+def contact_with_bodies_scene(cloth_position, bodies: AffineBodies, container, pairs, dhat: float, kappa: float,
+                              projection_method: int = 2, cloth_mass=None, dt: float = 0.01,
+                              name: str = "contact_with_bodies"):
+  """Barrier pairs over the collision union ``[cloth, abd vertices, container]``
+  (``examples/dropping_in_container_mixed/dropping_in_container.py:344-405``):
+  the abd vertices sit at ``A xbar + t`` of their bodies, the container is
+  DATA, the targets are ``[cloth position, affine_matrices, translations]``.
+  ``pairs`` maps ``pp/pe/pt/ee`` to union-index connectivities.  With
+  ``cloth_mass`` the scene also carries the inertia of the cloth and body
+  vertices and the bodies' orthogonality energy (a solvable system)."""
+  from .energies import affine_energy, affine_position, edge_edge, inertia, point_edge, point_point, point_triangle
+  from .scene import scene as make_scene
+  sc = make_scene(name)
+  m = sc.addMesh("collision_mesh")
+  cloth = m.addPrimitive("cloth", numInstances=len(cloth_position))
+  cpos = cloth.addAttribute("position", rows=3, cols=1)
+  cpos.updateValue(cloth_position)
+  prims = m.addPrimitive("affine_bodies", numInstances=bodies.num_bodies)
+  amat = prims.addAttribute("affine_matrices", rows=3, cols=3)
+  amat.updateValue(bodies.affine)
+  trans = prims.addAttribute("translations", rows=3, cols=1)
+  trans.updateValue(bodies.translation)
+  verts = m.addPrimitive("vertices_abd", numInstances=len(bodies.rest))
+  rest = verts.addConstant("rest_position", rows=3, cols=1)
+  rest.updateValue(bodies.rest)
+  v2b = verts.addConnectivity("v_abd2_abd", prims, bodies.vertex_body[:, None].astype(np.uint32), 1)
+  va = verts.addAttribute("affine_matrix", through=v2b, source=amat).resize(3, 3)
+  vt = verts.addAttribute("translation", through=v2b, source=trans).resize(3, 1)
+  vpos = verts.addAttribute("position", computed_attribute=affine_position(va, rest, vt))
+  cont = m.addPrimitive("container", numInstances=len(container))
+  opos = cont.addAttribute("position", rows=3, cols=1)
+  opos.updateValue(container)
+  allv = m.addPrimitiveUnion("vertices", [cloth, verts, cont])
+  apos = allv.addAttribute("position")
+  makers = {"pp": point_point, "pe": point_edge, "pt": point_triangle, "ee": edge_edge}
+  for key, arity in BARRIER_PAIRS:
+    conn = pairs.get(key)
+    if conn is None or len(conn) == 0:
+      continue
+    p = m.addPrimitive(key, numInstances=len(conn))
+    c = p.addConnectivity(key + "2v", allv, np.asarray(conn, dtype=np.uint32), arity)
+    x = p.addAttribute("positions", through=c, source=apos)
+    sc.addEnergy(p.addAttribute("barrier", computed_attribute=makers[key](x, dhat, kappa)),
+                 projection_method=projection_method)
+  if cloth_mass is not None:
+    old = cloth.addConstant("old_position", rows=3, cols=1)
+    old.updateValue(cloth_position)
+    cm = cloth.addConstant("mass")
+    cm.updateValue(cloth_mass)
+    sc.addEnergy(cloth.addAttribute("inertia", computed_attribute=inertia(old, None, dt, cpos, cm,
+                                                                         gravity=tuple(bodies.gravity))),
+                 projection_method=-1)
+    last = verts.addConstant("last_position", rows=3, cols=1)
+    last.updateValue(bodies.positions())
+    vel = verts.addConstant("velocity", rows=3, cols=1)
+    vel.updateValue(bodies.velocity)
+    vm = verts.addConstant("mass")
+    vm.updateValue(bodies.mass)
+    sc.addEnergy(verts.addAttribute("inertia_abds", computed_attribute=inertia(last, vel, dt, vpos, vm,
+                                                                                gravity=tuple(bodies.gravity))),
+                 projection_method=-1)
+    sc.addEnergy(prims.addAttribute("affine_energy", computed_attribute=affine_energy(amat, bodies.stiffness)),
+                 projection_method=2)
+  sc.addMinimizeTarget([cpos, amat, trans])
+  return sc, dict(position=cpos, affine_matrices=amat, translations=trans, vertices=allv)
