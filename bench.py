@@ -16,8 +16,9 @@ in and the solution copied out every step.
 ``serving``: the serving form on a seeded stream of 512 FEM Newton steps
 (Poisson arrivals, sides 8..48): continuous batching in the precision form
 beside the serial plain FP64 path, solves/s and p50/p99 latency (rank 0, N=1).
-``cloth_contact``: Newton steps of the mixed cloth + contact scene (StVK,
-bending, 200k barrier pairs, friction) in both precision forms (rank 0, N=1).
+``cloth_contact``: Newton steps of the mixed cloth + affine bodies + contact
+scene (StVK, bending, 16 icosphere bodies, 200k barrier pairs, friction) in
+both precision forms (rank 0, N=1).
 ``--impl reference``: the CPU restatement of the reference path (oracle) on
 a bounded sample of the same workload (rank 0 only).
 
@@ -378,17 +379,21 @@ def launches_per_newton_step(impl, its, refs):
 
 def cloth_leg(args):
   """Mixed cloth + contact Newton steps (StVK membrane, bending, 100k PT + 100k
-  EE barriers, PT friction, inertia; 256^2 cloth over a static obstacle):
+  EE barriers, PT friction, inertia; 256^2 cloth over a static obstacle, 16
+  icosphere affine bodies resting on it through body-cloth PT pairs):
   precision form and plain FP64, CUDA-event timed."""
   import torch
   from yasps_b200 import scenes
-  cc = scenes.cloth_contact(256, 200_000)
+  cc = scenes.cloth_contact(256, 200_000, num_bodies=16)
   sc, _ = scenes.cloth_contact_scene(cc)
   mz = sc.minimizer
+  nbp = len(cc.body_pt)
   out = {"workload": ("256x256 cloth (65,536 verts, 130,050 tris) StVK E=1e4 nu=0.3 h=1e-3, bending kb=1e-3, "
-                      "100k point-triangle + 100k edge-edge log-barrier pairs (d-hat 1e-3, squared distances "
-                      "in (0.1, 1) d-hat) against a static obstacle, lagged PT friction mu=0.3, inertia; "
-                      "solve to 1e-6 true relative residual")}
+                      "16 affine bodies (icospheres of 2,562 verts, 12 DoF each, orthogonality 1e5, inertia), "
+                      f"{nbp} body-cloth + {100_000 - nbp} cloth-obstacle point-triangle and 100k edge-edge "
+                      "log-barrier pairs (d-hat 1e-3, squared distances in (0.1, 1) d-hat), lagged PT friction "
+                      "mu=0.3, cloth inertia; solve to 1e-6 true relative residual"),
+         "body_cloth_pairs": nbp}
   for name, mixed in (("fp32_refine", True), ("fp64", False)):
     solver = mz.setSolver("mas", mixed_spmv=mixed, stop_rule="residual")
     step = lambda: mz.computeHessianAndGradient(tolerance=args.tol, maxIterations=5000)

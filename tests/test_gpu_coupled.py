@@ -71,3 +71,23 @@ def test_coupled_scene_mas_solve():
   assert np.linalg.norm(g - dense @ x) <= 1e-8 * np.linalg.norm(g)
   assert [v.numel() for v in segs] == [3 * len(s["cloth"]), 9 * s["bodies"].num_bodies,
                                         3 * s["bodies"].num_bodies]
+
+
+def test_cloth_with_bodies_newton_step():
+  """The mixed scene (cloth membrane, bending, barriers and friction against
+  an obstacle, icosphere affine bodies coupled to the cloth by PT pairs)
+  in both precision forms: the solution meets the true relative residual of
+  the assembled FP64 system."""
+  from yasps_b200 import scenes
+  cc = scenes.cloth_contact(24, 2_000, num_bodies=2, body_subdivisions=2, body_radius=0.25)
+  assert len(cc.body_pt) > 0
+  sc, _ = scenes.cloth_contact_scene(cc)
+  mz = sc.minimizer
+  for mixed in (True, False):
+    mz.setSolver("mas", mixed_spmv=mixed, stop_rule="residual")
+    segs = sc.minimizeEnergy(tolerance=1e-6, maxIterations=5000)
+    x = np.concatenate([v.cpu().numpy().reshape(-1) for v in segs])
+    H = mz.computeNumericValue()
+    g = H.gradient.value.cpu().numpy()
+    assert np.linalg.norm(g - _dense(H) @ x) <= 1e-6 * np.linalg.norm(g)
+    assert [v.numel() for v in segs] == [3 * 24 * 24, 18, 6]

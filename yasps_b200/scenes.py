@@ -384,16 +384,110 @@ class ClothContact:
   friction: float
   fdhat: float
   dt: float
+  bodies: "AffineBodies" = None   # affine bodies over the cloth (icospheres), or None
+  body_pt: np.ndarray = None      # (nbp, 4) PT pairs in the union [cloth, abd, obstacle]
+
+
+def icosphere(subdivisions: int):
+  """Unit icosphere: vertices (10 * 4^s + 2, 3) and triangles (20 * 4^s, 3),
+  each face split into four with the edge midpoints pushed to the sphere."""
+  t = (1.0 + 5.0 ** 0.5) / 2.0
+  v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+  f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11],
+                [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+  v /= np.linalg.norm(v, axis=1, keepdims=True)
+  for _ in range(subdivisions):
+    e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+    key = np.sort(e, axis=1)
+    uniq, inv = np.unique(key, axis=0, return_inverse=True)
+    mid = v[uniq[:, 0]] + v[uniq[:, 1]]
+    mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+    m = len(v) + inv.reshape(3, -1)  # midpoint of edges (0,1), (1,2), (2,0) per face
+    a, b, c = f[:, 0], f[:, 1], f[:, 2]
+    f = np.concatenate([np.stack([a, m[0], m[2]], 1), np.stack([b, m[1], m[0]], 1), np.stack([c, m[2], m[1]], 1),
+                        np.stack([m[0], m[1], m[2]], 1)])
+    v = np.concatenate([v, mid])
+  return v, f
+
+
+def _bodies_over_cloth(rng, side, spacing, dhat, num_bodies, subdivisions, radius, stiffness, dt):
+  """Icosphere affine bodies on a grid over the cloth, each lowered until its
+  lowest vertex is just above sqrt(0.1 d-hat) (the cloth lies at y = 0)."""
+  unit, faces = icosphere(subdivisions)
+  xbar = unit * radius
+  nv = len(xbar)
+  g = int(np.ceil(np.sqrt(num_bodies)))
+  extent = (side - 1) * spacing
+  affine, trans = [], []
+  for b in range(num_bodies):
+    q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+    if np.linalg.det(q) < 0:
+      q[:, 0] = -q[:, 0]
+    sym = rng.uniform(-1e-3, 1e-3, size=(3, 3))
+    a = q @ (np.eye(3) + 0.5 * (sym + sym.T))
+    low = float((xbar @ a.T)[:, 1].min())
+    cx, cz = ((b % g) + 0.5) * extent / g, ((b // g) + 0.5) * extent / g
+    affine.append(a.ravel())
+    trans.append([cx, 1.02 * np.sqrt(0.1 * dhat) - low, cz])
+  return AffineBodies(
+      rest=np.tile(xbar, (num_bodies, 1)), vertex_body=np.repeat(np.arange(num_bodies), nv),
+      tets=np.zeros((0, 4), dtype=np.uint32), affine=np.asarray(affine), translation=np.asarray(trans),
+      mass=np.full(num_bodies * nv, 2.0 / nv), velocity=np.zeros((num_bodies * nv, 3)), mu=0.0, lam=0.0,
+      stiffness=stiffness, dt=dt, gravity=np.array([0.0, -9.8, 0.0])), faces
+
+
+def _body_cloth_pairs(bodies, faces, cloth_pos, side, spacing, dhat):
+  """PT pairs between the bodies and the flat cloth (y = 0), in the union
+  [cloth, abd, obstacle]: (a) a body vertex over the cloth triangle below
+  it, (b) a cloth vertex below a body triangle; kept when the squared
+  plane distance lies in (0.1, 1) d-hat."""
+  n, nc = side, len(cloth_pos)
+  x = bodies.positions()
+  lo, hi = 0.1 * dhat, dhat
+  out = []
+  # (a) body vertex -> cloth triangle (plane y = 0: squared distance y^2)
+  y2 = x[:, 1] ** 2
+  i = np.floor(x[:, 0] / spacing).astype(np.int64)
+  k = np.floor(x[:, 2] / spacing).astype(np.int64)
+  ok = (y2 > lo) & (y2 < hi) & (i >= 0) & (i < n - 1) & (k >= 0) & (k < n - 1)
+  for v in np.flatnonzero(ok):
+    a = i[v] * n + k[v]
+    u, w = x[v, 0] / spacing - i[v], x[v, 2] / spacing - k[v]
+    tri = (a, a + n + 1, a + n) if u > w else (a, a + 1, a + n + 1)
+    out.append((nc + v, *tri))
+  # (b) cloth vertex nearest below a body triangle's centroid
+  nv = bodies.rest.shape[0] // bodies.num_bodies
+  for b in range(bodies.num_bodies):
+    f = faces + b * nv
+    p = x[f]
+    low = np.all(p[:, :, 1] < np.sqrt(hi) * 1.5, axis=1)
+    for tri, q in zip(f[low], p[low]):
+      c = q.mean(axis=0)
+      ci, ck = int(round(c[0] / spacing)), int(round(c[2] / spacing))
+      if not (0 <= ci < n and 0 <= ck < n):
+        continue
+      cv = ci * n + ck
+      nrm = np.cross(q[1] - q[0], q[2] - q[0])
+      d = float(np.dot(cloth_pos[cv] - q[0], nrm) ** 2 / np.dot(nrm, nrm))
+      if lo < d < hi:
+        out.append((cv, nc + tri[0], nc + tri[1], nc + tri[2]))
+  return np.asarray(out, dtype=np.uint32).reshape(-1, 4)
 
 
 def cloth_contact(side: int = 256, pairs: int = 200_000, spacing: float = 0.05, young: float = 1e4,
                   poisson: float = 0.3, thickness: float = 1e-3, bend_stiff: float = 1e-3, dhat: float = 1e-3,
                   kappa: float = 1e3, friction: float = 0.3, eps_v: float = 1e-3, density: float = 200.0,
-                  dt: float = 0.01, seed: int = 0) -> ClothContact:
+                  dt: float = 0.01, seed: int = 0, num_bodies: int = 0, body_subdivisions: int = 4,
+                  body_radius: float = 0.5, body_stiffness: float = 1e5) -> ClothContact:
   """A ``side x side`` cloth sheet (xz plane, triangles wound to +y normals)
   over a static obstacle grid offset by half a cell, with ``pairs`` synthetic
   contacts split between point-triangle and edge-edge pairs whose squared
-  distances spread over (0.1, 1.0) d-hat (obstacle heights drawn per vertex)."""
+  distances spread over (0.1, 1.0) d-hat (obstacle heights drawn per vertex).
+  With ``num_bodies``, icosphere affine bodies (10 * 4^s + 2 vertices each)
+  rest on the cloth, coupled to it by point-triangle pairs in the same
+  distance window; they take their share of the point-triangle pairs."""
   rng = np.random.default_rng(seed)
   n = side
   gi, gk = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
@@ -420,8 +514,13 @@ def cloth_contact(side: int = 256, pairs: int = 200_000, spacing: float = 0.05, 
   no = m * m
   oa = (oi[:-1, :-1] * m + ok[:-1, :-1]).ravel()
   otris = np.stack([oa, oa + m + 1, oa + m], axis=1)
-  npt = pairs // 2
-  nee = pairs - npt
+  bodies, body_pt = None, None
+  if num_bodies:
+    bodies, faces = _bodies_over_cloth(rng, n, spacing, dhat, num_bodies, body_subdivisions, body_radius,
+                                       body_stiffness, dt)
+    body_pt = _body_cloth_pairs(bodies, faces, pos, n, spacing, dhat)
+  npt = pairs // 2 - (0 if body_pt is None else len(body_pt))
+  nee = pairs - pairs // 2
   # PT: a cloth vertex above an obstacle triangle (cloth vertex (i+1, k+1) lies over cell (i, k))
   tri_pick = rng.integers(0, len(otris), size=npt)
   ti, tk = tri_pick // (m - 1), tri_pick % (m - 1)
@@ -446,7 +545,7 @@ def cloth_contact(side: int = 256, pairs: int = 200_000, spacing: float = 0.05, 
                       pt=pt.astype(np.uint32), ee=ee.astype(np.uint32), lagged=lagged,
                       mass=density * thickness * areas, mu=mu, lam=lam, thickness=thickness,
                       bend_stiff=bend_stiff, dhat=dhat, kappa=kappa, friction=friction, fdhat=eps_v * eps_v,
-                      dt=dt)
+                      dt=dt, bodies=bodies, body_pt=body_pt)
 
 
 def cloth_contact_scene(cc: ClothContact, projection_method: int = 1):
@@ -502,11 +601,60 @@ def cloth_contact_scene(cc: ClothContact, projection_method: int = 1):
   for e in (mem, ben, pte, eee, ptf):
     sc.addEnergy(e, projection_method=projection_method)
   sc.addEnergy(kin, projection_method=-1)
-  sc.addMinimizeTarget([pos])
-  return sc, dict(position=pos, old_position=old)
+  if cc.bodies is None:
+    sc.addMinimizeTarget([pos])
+    return sc, dict(position=pos, old_position=old)
+  # affine bodies on the cloth: the collision union [cloth, abd, obstacle]
+  # (dropping_in_container.py:344) carries the body-cloth point-triangle pairs
+  prims, amat, trans, verts, vpos = _affine_body_attributes(body, cc.bodies)
+  coll = body.addPrimitiveUnion("collision_vertices", [cloth, verts, obst])
+  cpos = coll.addAttribute("position")
+  bpp = body.addPrimitive("body_pt_pairs", numInstances=len(cc.body_pt))
+  bpc = bpp.addConnectivity("to_collision_vertices", coll, cc.body_pt, 4)
+  sc.addEnergy(bpp.addAttribute("barrier", computed_attribute=point_triangle(
+      bpp.addAttribute("x", through=bpc, source=cpos), cc.dhat, cc.kappa)), projection_method=projection_method)
+  _affine_body_energies(sc, cc.bodies, prims, amat, verts, vpos, cc.dt)
+  sc.addMinimizeTarget([pos, amat, trans])
+  return sc, dict(position=pos, old_position=old, affine_matrices=amat, translations=trans)
 
 
 # ---- contact between cloth, affine bodies and a container ------------------------------
+
+def _affine_body_attributes(m, bodies: AffineBodies):
+  """Bodies (``affine_matrices``, ``translations``) and their vertices at
+  ``A xbar + t`` on mesh ``m``, as ``dropping_in_container.py:241-270``."""
+  from .energies import affine_position
+  prims = m.addPrimitive("affine_bodies", numInstances=bodies.num_bodies)
+  amat = prims.addAttribute("affine_matrices", rows=3, cols=3)
+  amat.updateValue(bodies.affine)
+  trans = prims.addAttribute("translations", rows=3, cols=1)
+  trans.updateValue(bodies.translation)
+  verts = m.addPrimitive("vertices_abd", numInstances=len(bodies.rest))
+  rest = verts.addConstant("rest_position", rows=3, cols=1)
+  rest.updateValue(bodies.rest)
+  v2b = verts.addConnectivity("v_abd2_abd", prims, bodies.vertex_body[:, None].astype(np.uint32), 1)
+  va = verts.addAttribute("affine_matrix", through=v2b, source=amat).resize(3, 3)
+  vt = verts.addAttribute("translation", through=v2b, source=trans).resize(3, 1)
+  vpos = verts.addAttribute("position", computed_attribute=affine_position(va, rest, vt))
+  return prims, amat, trans, verts, vpos
+
+
+def _affine_body_energies(sc, bodies: AffineBodies, prims, amat, verts, vpos, dt):
+  """Inertia of the body vertices (no projection) and the bodies'
+  orthogonality energy (projection 2), as ``dropping_in_container.py:377-395``."""
+  from .energies import affine_energy, inertia
+  last = verts.addConstant("last_position", rows=3, cols=1)
+  last.updateValue(bodies.positions())
+  vel = verts.addConstant("velocity", rows=3, cols=1)
+  vel.updateValue(bodies.velocity)
+  vm = verts.addConstant("mass")
+  vm.updateValue(bodies.mass)
+  sc.addEnergy(verts.addAttribute("inertia_abds", computed_attribute=inertia(last, vel, dt, vpos, vm,
+                                                                              gravity=tuple(bodies.gravity))),
+               projection_method=-1)
+  sc.addEnergy(prims.addAttribute("affine_energy", computed_attribute=affine_energy(amat, bodies.stiffness)),
+               projection_method=2)
+
 
 BARRIER_PAIRS = (("pp", 2), ("pe", 3), ("pt", 4), ("ee", 4))
 
@@ -521,25 +669,14 @@ def contact_with_bodies_scene(cloth_position, bodies: AffineBodies, container, p
   ``pairs`` maps ``pp/pe/pt/ee`` to union-index connectivities.  With
   ``cloth_mass`` the scene also carries the inertia of the cloth and body
   vertices and the bodies' orthogonality energy (a solvable system)."""
-  from .energies import affine_energy, affine_position, edge_edge, inertia, point_edge, point_point, point_triangle
+  from .energies import edge_edge, inertia, point_edge, point_point, point_triangle
   from .scene import scene as make_scene
   sc = make_scene(name)
   m = sc.addMesh("collision_mesh")
   cloth = m.addPrimitive("cloth", numInstances=len(cloth_position))
   cpos = cloth.addAttribute("position", rows=3, cols=1)
   cpos.updateValue(cloth_position)
-  prims = m.addPrimitive("affine_bodies", numInstances=bodies.num_bodies)
-  amat = prims.addAttribute("affine_matrices", rows=3, cols=3)
-  amat.updateValue(bodies.affine)
-  trans = prims.addAttribute("translations", rows=3, cols=1)
-  trans.updateValue(bodies.translation)
-  verts = m.addPrimitive("vertices_abd", numInstances=len(bodies.rest))
-  rest = verts.addConstant("rest_position", rows=3, cols=1)
-  rest.updateValue(bodies.rest)
-  v2b = verts.addConnectivity("v_abd2_abd", prims, bodies.vertex_body[:, None].astype(np.uint32), 1)
-  va = verts.addAttribute("affine_matrix", through=v2b, source=amat).resize(3, 3)
-  vt = verts.addAttribute("translation", through=v2b, source=trans).resize(3, 1)
-  vpos = verts.addAttribute("position", computed_attribute=affine_position(va, rest, vt))
+  prims, amat, trans, verts, vpos = _affine_body_attributes(m, bodies)
   cont = m.addPrimitive("container", numInstances=len(container))
   opos = cont.addAttribute("position", rows=3, cols=1)
   opos.updateValue(container)
@@ -563,16 +700,6 @@ def contact_with_bodies_scene(cloth_position, bodies: AffineBodies, container, p
     sc.addEnergy(cloth.addAttribute("inertia", computed_attribute=inertia(old, None, dt, cpos, cm,
                                                                          gravity=tuple(bodies.gravity))),
                  projection_method=-1)
-    last = verts.addConstant("last_position", rows=3, cols=1)
-    last.updateValue(bodies.positions())
-    vel = verts.addConstant("velocity", rows=3, cols=1)
-    vel.updateValue(bodies.velocity)
-    vm = verts.addConstant("mass")
-    vm.updateValue(bodies.mass)
-    sc.addEnergy(verts.addAttribute("inertia_abds", computed_attribute=inertia(last, vel, dt, vpos, vm,
-                                                                                gravity=tuple(bodies.gravity))),
-                 projection_method=-1)
-    sc.addEnergy(prims.addAttribute("affine_energy", computed_attribute=affine_energy(amat, bodies.stiffness)),
-                 projection_method=2)
+    _affine_body_energies(sc, bodies, prims, amat, verts, vpos, dt)
   sc.addMinimizeTarget([cpos, amat, trans])
   return sc, dict(position=cpos, affine_matrices=amat, translations=trans, vertices=allv)
