@@ -16,9 +16,6 @@ import pytest
 from oracle import coupled_contact as cc
 from oracle import vertex_energies as ve
 
-ARITY = {1: 2, 2: 3, 3: 4, 4: 4}
-
-
 def rel(a, b):
   return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
