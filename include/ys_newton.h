@@ -79,8 +79,11 @@ int32_t ys_compress_indices(const uint32_t* codes, const uint16_t* sizes, uint32
  * cudaMallocAsync.  No counterpart in the reference.
  * Limit: n <= 67,108,864 instances; larger n returns YS_ERR_CAPACITY.
  * The first call on a device resolves the array's address (set-up), so make
- * it before any stream capture.  All calls on a device share the array: calls
- * that overlap in time (other streams or threads) race on it.              */
+ * it before any stream capture.  The address is kept for the life of the
+ * process: after cudaDeviceReset (or any other teardown of the device's
+ * primary context) it is stale, so do not call this entry point on that
+ * device again in the same process.  All calls on a device share the array:
+ * calls that overlap in time (other streams or threads) race on it.        */
 int32_t ys_compress_indices_noalloc(const uint32_t* codes, const uint16_t* sizes, uint32_t n,
                                     uint32_t K, int16_t* perm, uint16_t* total_sizes,
                                     uint32_t* coord_outer, void* stream);
@@ -454,6 +457,10 @@ typedef struct ys_pcg_args {
   double* workspace;            /* ys_pcg_workspace_doubles(n) doubles             */
 } ys_pcg_args;
 
+/* With YS_PREC_MAS a finite non-positive curvature p^T H p (rounding on an
+ * ill-conditioned SPD system) takes a zero step and restarts the direction
+ * from M^-1 r, as the reference's MAS PCG does (mas/cuda/pcg.cu:183-189);
+ * block-Jacobi ends the solve with -(it+4) as solverKernel.pyx:388-404. */
 typedef struct ys_pcg_result {
   int32_t status;        /* reference convention: >=0 iterations (0: converged at start), <0 error */
   uint32_t iterations;
@@ -557,6 +564,15 @@ int32_t ys_refine_residual(const ys_matrix3* m, const double* rhs, double* x, co
 /* Change the tolerance / iteration budget of an existing solver (the graph
  * reads them from device memory, so no rebuild). */
 int32_t ys_pcg_set_params(void* handle, double tolerance, uint32_t max_iterations);
+/* Polls a block of the MAS loop makes at its grid barrier (the cooperative
+ * collect + direction kernel) before it gives up; default 2^24.  A block that
+ * gives up marks the solve void and ys_pcg_status returns YS_ERR_CUDA; the
+ * loop then ends at its iteration budget.  The waiting grid is co-resident,
+ * so the default bound is never reached in a healthy run; a small bound
+ * exercises the failure path without hanging the device.  Applies from the
+ * next launch.  No counterpart in the reference (its loop has no grid-wide
+ * wait).                                                                    */
+int32_t ys_pcg_set_barrier_poll_limit(void* handle, uint32_t polls);
 /* Asynchronous halves of ys_pcg_run. */
 int32_t ys_pcg_launch(void* handle, void* stream);
 int32_t ys_pcg_status(void* handle, void* stream, ys_pcg_result* result);

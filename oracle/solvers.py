@@ -103,11 +103,17 @@ class PCGResult:
   breakdown: str | None = None
 
 
-def mas_pcg(matvec, rhs, precondition, tolerance, max_iterations, initial_guess=None) -> PCGResult:
+def mas_pcg(matvec, rhs, precondition, tolerance, max_iterations, initial_guess=None,
+            restart=False) -> PCGResult:
   """MAS-preconditioned CG (``PKG/solver/mas/pcg.py:23-102``).
 
   Stops when ``r^T z <= tolerance * reference`` with ``reference = r_0^T z_0``
   for a zero initial guess (``rhs^T M^-1 rhs`` otherwise).
+
+  ``restart=True`` follows the reference's device loop instead of its NumPy
+  one on a finite non-positive curvature (``mas/cuda/pcg.cu:183-189,
+  236-240``): a zero step, then the direction restarts from ``M^-1 r``
+  (beta = 0); the iteration counts.  The NumPy loop ends the solve there.
   """
   rhs = np.asarray(rhs, dtype=np.float64).reshape(-1)
   x = np.zeros_like(rhs) if initial_guess is None else np.asarray(initial_guess, dtype=np.float64).copy()
@@ -126,9 +132,10 @@ def mas_pcg(matvec, rhs, precondition, tolerance, max_iterations, initial_guess=
   for it in range(1, max_iterations + 1):
     product = matvec(direction)
     curvature = float(direction @ product)
-    if not np.isfinite(curvature) or curvature <= 0:
+    restarted = restart and np.isfinite(curvature) and curvature <= 0
+    if not restarted and (not np.isfinite(curvature) or curvature <= 0):
       return PCGResult(x, it - 1, float(np.linalg.norm(residual)) / denom, False, "matrix is not positive definite")
-    alpha = rz / curvature
+    alpha = 0.0 if restarted else rz / curvature
     x += alpha * direction
     residual -= alpha * product
     z = precondition(residual)
@@ -140,7 +147,7 @@ def mas_pcg(matvec, rhs, precondition, tolerance, max_iterations, initial_guess=
       return PCGResult(x, it, rel, True)
     if next_rz == 0.0:
       return PCGResult(x, it, rel, False, "preconditioner is not positive definite")
-    direction = z + (next_rz / rz) * direction
+    direction = z + (0.0 if restarted else next_rz / rz) * direction
     rz = next_rz
   return PCGResult(x, max_iterations, float(np.linalg.norm(residual)) / denom, False)
 

@@ -3,8 +3,13 @@ ys_compress_indices, both through the C ABI.
 
 The outputs are integers: the tolerance is bit-exact.  Several calls in a row
 on inputs of different sizes check that the shared scratch, which keeps the
-previous call's contents, does not leak into a later result.
+previous call's contents, does not leak into a later result.  The device's
+memory pool (the one cudaMallocAsync draws from) shows that the entry point
+really allocates nothing: its used-memory high-water mark stays at zero over
+the calls, while the allocating entry point raises it.
 """
+
+import ctypes
 
 import numpy as np
 import pytest
@@ -62,3 +67,41 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
   rc = lib.ys_compress_indices_noalloc(None, None, MAX_INSTANCES + 1, 4, None, None, None, None)
   assert rc == -3  # YS_ERR_CAPACITY
   assert b"67,108,864" in lib.ys_last_error()
+
+
+CU_MEMPOOL_ATTR_USED_MEM_HIGH = 8
+
+
+def pool_high_water(fn):
+  """Bytes of the current device's memory pool in use at its peak while
+  ``fn`` runs (the high-water mark is reset to zero before, read after)."""
+  import torch
+  cu = ctypes.CDLL("libcuda.so.1")
+  dev = ctypes.c_int()
+  assert cu.cuCtxGetDevice(ctypes.byref(dev)) == 0
+  pool = ctypes.c_void_p()
+  assert cu.cuDeviceGetMemPool(ctypes.byref(pool), dev) == 0
+  torch.cuda.synchronize()
+  zero = ctypes.c_uint64(0)
+  assert cu.cuMemPoolSetAttribute(pool, CU_MEMPOOL_ATTR_USED_MEM_HIGH, ctypes.byref(zero)) == 0
+  fn()
+  torch.cuda.synchronize()
+  high = ctypes.c_uint64(1)
+  assert cu.cuMemPoolGetAttribute(pool, CU_MEMPOOL_ATTR_USED_MEM_HIGH, ctypes.byref(high)) == 0
+  return high.value
+
+
+def test_noalloc_allocates_nothing():
+  import torch
+  n, K = 2_500_000, 4
+  codes, sizes = make_codes(n, K, 5)
+  c = torch.from_numpy(codes.reshape(-1)).cuda()
+  sz = torch.from_numpy(sizes.reshape(-1)).cuda()
+  perm = torch.empty(n * K, dtype=torch.int16, device="cuda")
+  total = torch.empty(n, dtype=torch.int16, device="cuda")
+  outer = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+  args = (L.ptr(c), L.ptr(sz), n, K, L.ptr(perm), L.ptr(total), L.ptr(outer), L.stream_ptr())
+  L.call("ys_compress_indices_noalloc", *args)  # the first call on the device does the set-up
+  assert pool_high_water(lambda: [L.call("ys_compress_indices_noalloc", *args) for _ in range(2)]) == 0
+  # the check sees allocations: the allocating entry point's scan storage
+  assert pool_high_water(lambda: L.call("ys_compress_indices", *args)) > 0

@@ -153,6 +153,7 @@ SIGNATURES = {
     "ys_pcg_run": (i32, [vp, vp, P(PcgResult)]),
     "ys_pcg_launch": (i32, [vp, vp]),
     "ys_pcg_set_params": (i32, [vp, f64, u32]),
+    "ys_pcg_set_barrier_poll_limit": (i32, [vp, u32]),
     "ys_pcg_status": (i32, [vp, vp, P(PcgResult)]),
     "ys_pcg_destroy": (i32, [vp]),
     "ys_mas_create": (i32, [P(MasDesc), P(vp)]),

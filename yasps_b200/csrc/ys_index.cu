@@ -5,6 +5,7 @@
 // every thread walks its own K slots, so the launch is HBM/latency bound.
 #include <cub/cub.cuh>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -243,24 +244,33 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(uint32_t* __restrict_
 }
 
 // Device address of the tile-sum array for the current device, resolved once
-// per device (the first call on a device does this set-up).
+// per device (the first call on a device does this set-up) and then read
+// without a lock.  The address belongs to the device's primary context: after
+// a cudaDeviceReset (or anything else that destroys and recreates that
+// context) the module is loaded again, possibly elsewhere, and the cached
+// address is stale: the entry point must not be called on that device after
+// such a reset in the same process.
+static std::atomic<void*> g_noalloc_addr[kNoAllocMaxDevices];
+
 static int32_t noalloc_tile_sums(uint32_t** out) {
-  static std::mutex mu;
-  static void* addr[kNoAllocMaxDevices] = {};
   int dev = 0;
   YS_CUDA_TRY(cudaGetDevice(&dev));
   YS_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, YS_ERR_INVALID, "device ordinal beyond 63");
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_tile_sums);
-    if (e != cudaSuccess || !p) {
-      ys_set_last_error(e != cudaSuccess ? cudaGetErrorString(e) : "null scratch address", __FILE__, __LINE__);
-      return YS_ERR_CUDA;
+  void* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    static std::mutex mu;  // taken only to resolve a device's address
+    std::lock_guard<std::mutex> lock(mu);
+    p = g_noalloc_addr[dev].load(std::memory_order_relaxed);
+    if (!p) {
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_tile_sums);
+      if (e != cudaSuccess || !p) {
+        ys_set_last_error(e != cudaSuccess ? cudaGetErrorString(e) : "null scratch address", __FILE__, __LINE__);
+        return YS_ERR_CUDA;
+      }
+      g_noalloc_addr[dev].store(p, std::memory_order_release);
     }
-    addr[dev] = p;
   }
-  *out = static_cast<uint32_t*>(addr[dev]);
+  *out = static_cast<uint32_t*>(p);
   return YS_OK;
 }
 

@@ -396,6 +396,7 @@ __global__ void __launch_bounds__(kPcgBlock) mas_init_collect(MasPcg P) {
   st[kAlpha] = 0.0;
   st[kBeta] = 0.0;
   st[kBarrierFail] = 0.0;
+  st[kRestart] = 0.0;
   int status = kContinue;
   double tol;
   if (P.stop_rule == YS_STOP_RESIDUAL) {
@@ -499,7 +500,10 @@ __global__ void __launch_bounds__(kPcgBlock) mas_iter_collect(MasPcg P) {
     st[kBeta] = 0.0;
     status = kNonSpd;
   } else {
-    st[kBeta] = next / prev;
+    // after a zero step (non-positive curvature) the direction restarts
+    // from z = M^-1 r (mas/cuda/pcg.cu:240)
+    st[kBeta] = st[kRestart] != 0.0 ? 0.0 : next / prev;
+    st[kRestart] = 0.0;
     const bool done = P.stop_rule == YS_STOP_RESIDUAL ? v[1] <= st[kTolAbs] : next <= st[kTolAbs];
     if (done) status = kConverged;
     else if (next == 0.0) status = kNonSpd;
@@ -581,7 +585,8 @@ __global__ void __launch_bounds__(kPcgBlock) mas_iter_collect_direction(MasPcg P
         st[kBeta] = 0.0;
         status = kNonSpd;
       } else {
-        st[kBeta] = next / prev;
+        st[kBeta] = st[kRestart] != 0.0 ? 0.0 : next / prev;  // restart: see mas_iter_collect
+        st[kRestart] = 0.0;
         const bool done = P.stop_rule == YS_STOP_RESIDUAL ? v[1] <= st[kTolAbs] : next <= st[kTolAbs];
         if (done) status = kConverged;
         else if (next == 0.0) status = kNonSpd;
@@ -595,14 +600,17 @@ __global__ void __launch_bounds__(kPcgBlock) mas_iter_collect_direction(MasPcg P
     }
   } else if (threadIdx.x == 0) {
     // bounded wait for the release (the grid is co-resident, so the last
-    // block always arrives; the bound only keeps a failure from hanging)
+    // block always arrives; the bound, kPollLimitParam polls, only keeps a
+    // failure from hanging: a block that gives up voids the solve)
+    const double limit = *(volatile double*)&st[kPollLimitParam];
     uint32_t spins = 0;
     while (atomicAdd(gen, 0u) == g0) {
-      if (++spins > (1u << 24)) {
+      if ((double)spins >= limit) {
         ok = 0;
         st[kBarrierFail] = 1.0;
         break;
       }
+      ++spins;
       __nanosleep(64);
     }
     __threadfence();

@@ -38,6 +38,7 @@ struct PcgParams {
   unsigned* tickets;
   int stop_rule;
   int zero_guess;
+  int restart_on_curvature;  // MAS: a non-positive curvature restarts from M^-1 r (zero step, beta = 0)
   double tolerance;
   uint32_t max_it;
   cudaGraphConditionalHandle cond;
@@ -98,6 +99,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
   st[kAlpha] = 0.0;
   st[kBeta] = 0.0;
   st[kBarrierFail] = 0.0;
+  st[kRestart] = 0.0;
   int status = kContinue;
   double tol;
   if (P.stop_rule == YS_STOP_RESIDUAL) {
@@ -147,14 +149,22 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
   const double curv = v[0];
   st[kCurv] = curv;
   st[kDeltaOld] = st[kDeltaNew];
-  if (!isfinite(curv) || curv <= 0.0) {
+  const double rz = st[kDeltaNew];
+  if (P.restart_on_curvature && isfinite(curv) && curv <= 0.0 && isfinite(rz) && rz > 0.0) {
+    // The reference's MAS PCG (mas/cuda/pcg.cu:183-189): rounding can break
+    // conjugacy on an ill-conditioned SPD system, so a finite non-positive
+    // curvature takes a zero step and restarts from M^-1 r (beta = 0 in the
+    // collect kernel) instead of ending the solve as non-SPD.
+    st[kAlpha] = 0.0;
+    st[kRestart] = 1.0;
+  } else if (!isfinite(curv) || curv <= 0.0) {
     // prepareCgIteration (solverKernel.pyx:388-404)
     st[kAlpha] = 0.0;
     st[kStatus] = (double)kNonSpd;
     st[kIter] = st[kIter] + 1.0;
     cudaGraphSetConditional(P.cond, 0u);
   } else {
-    st[kAlpha] = st[kDeltaNew] / curv;
+    st[kAlpha] = rz / curv;
   }
 }
 
@@ -271,7 +281,9 @@ struct PcgHandle {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double* slots_host = nullptr;
-  double params[2] = {0.0, 0.0};  // tolerance, iteration budget (copied to the device per launch)
+  // tolerance, iteration budget, grid-barrier poll limit (copied to the
+  // device per launch)
+  double params[3] = {0.0, 0.0, (double)kDefaultPollLimit};
 };
 
 static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
@@ -346,6 +358,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   P.jinv = a.jacobi_inverse;
   P.stop_rule = a.stop_rule;
   P.zero_guess = a.zero_initial_guess;
+  P.restart_on_curvature = a.preconditioner == YS_PREC_MAS;
   P.tolerance = a.tolerance;
   P.max_it = a.max_iterations;
   h->params[0] = a.tolerance;
@@ -420,7 +433,7 @@ int32_t ys_pcg_launch(void* handle, void* stream) {
   auto* h = static_cast<ys::PcgHandle*>(handle);
   // Pageable source: the copy is staged before the call returns, so the
   // parameters may change for the next launch right away.
-  const double params[2] = {h->params[0], h->params[1]};
+  const double params[3] = {h->params[0], h->params[1], h->params[2]};
   YS_CUDA_TRY(cudaMemcpyAsync(h->P.st + ys::kTolParam, params, sizeof(params), cudaMemcpyHostToDevice,
                               (cudaStream_t)stream));
   YS_CUDA_TRY(cudaGraphLaunch(h->exec, (cudaStream_t)stream));
@@ -432,6 +445,12 @@ int32_t ys_pcg_set_params(void* handle, double tolerance, uint32_t max_iteration
   auto* h = static_cast<ys::PcgHandle*>(handle);
   h->params[0] = tolerance;
   h->params[1] = (double)max_iterations;
+  return YS_OK;
+}
+
+int32_t ys_pcg_set_barrier_poll_limit(void* handle, uint32_t polls) {
+  YS_REQUIRE(handle, YS_ERR_INVALID, "null handle");
+  static_cast<ys::PcgHandle*>(handle)->params[2] = (double)polls;
   return YS_OK;
 }
 

@@ -23,12 +23,20 @@ enum PcgSlot : int {
   kBarrierFail = 12,  // nonzero: a grid barrier wait ran out (the solve is void)
   kTolParam = 13,  // solve parameters, written by the host before each launch
   kMaxItParam = 14,
-  kSlots = 16
+  kPollLimitParam = 15,  // polls a block makes at a grid barrier before it gives up
+  kRestart = 16,   // nonzero: this iteration took a zero step (non-positive curvature), beta = 0 next
+  kSlots = 20
 };
 
 enum PcgStatus : int { kContinue = 0, kConverged = 1, kNonSpd = 2, kInvalidInit = 3, kMaxIter = 4 };
 
 constexpr int kPcgBlock = 256;
+
+// Polls a block makes at a grid barrier of the PCG loop before it gives up
+// and marks the solve void (kBarrierFail).  The grids that wait are
+// co-resident, so the wait always ends well before this; the bound only keeps
+// a failure from hanging the device.
+constexpr uint32_t kDefaultPollLimit = 1u << 24;
 
 // Deterministic grid-wide reduction of NV values: every block stores its
 // block sums, the last block to arrive (ticket) reduces the partials in a
