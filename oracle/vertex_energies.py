@@ -9,8 +9,10 @@ float64 PyTorch and SymPy scripts the same way):
 * ``bending``: ``helpers.py:213-234`` (the half-angle ``atan2`` form);
 * ``baraff_witkin`` and its rest frame ``compute_rest_shape``:
   ``helpers.py:240-292``;
-* lagged point-triangle friction: ``examples/dropping_in_container/
-  friction_helpers.py:12-66`` (smoothing) and ``:73-182`` (point-triangle);
+* lagged friction of the four contact kinds: ``examples/dropping_in_container/
+  friction_helpers.py:12-66`` (smoothing), ``:73-182`` (point-triangle),
+  ``:188-276`` (point-edge), ``:283-405`` (edge-edge), ``:411-500``
+  (point-point);
 * a StVK membrane on the Baraff-Witkin rest frame (the reference ships none:
   parity unpinned for it).
 
@@ -132,14 +134,13 @@ def stvk_membrane(x, rest, p):
   return psi * thickness * _rest_area(rest) * dt * dt
 
 
-def friction_pt(x, rest, p, lagged):
-  """``friction_energy_pt`` with the lagged (beta1, beta2, t0, t1, lambda)."""
+def _friction(rel, p, lagged):
+  """``friction_energy_from_rel_dx`` with ``smooth_friction_phi``
+  (``friction_helpers.py:26-66``): the lagged tangent basis (t0, t1) and
+  lambda are ``lagged[2:5]``, ``lagged[5:8]``, ``lagged[8]``."""
   torch = _t()
   fdhat, dt, rate = p
-  b1, b2 = lagged[0], lagged[1]
   t0, t1, lam = lagged[2:5], lagged[5:8], lagged[8]
-  dx = x - rest
-  rel = dx[0] - (dx[1] + b1 * (dx[2] - dx[1]) + b2 * (dx[3] - dx[1]))
   u0, u1 = t0.dot(rel), t1.dot(rel)
   y2 = u0 * u0 + u1 * u1
   eps = np.sqrt(fdhat) * dt
@@ -150,6 +151,83 @@ def friction_pt(x, rest, p, lagged):
   else:
     phi = eps / 3.0 + y2 / eps - y2 * y / (3.0 * eps * eps)
   return rate * lam * phi
+
+
+def friction_pt(x, rest, p, lagged):
+  """``friction_energy_pt`` (``friction_helpers.py:124-182``) with the lagged
+  (beta1, beta2, t0, t1, lambda); ``rest`` holds the positions of the last step."""
+  b1, b2 = lagged[0], lagged[1]
+  dx = x - rest
+  return _friction(dx[0] - (dx[1] + b1 * (dx[2] - dx[1]) + b2 * (dx[3] - dx[1])), p, lagged)
+
+
+def friction_pe(x, rest, p, lagged):
+  """``friction_energy_pe`` (``friction_helpers.py:235-276``): lagged (eta, 0, t0, t1, lambda)."""
+  eta = lagged[0]
+  dx = x - rest
+  return _friction(dx[0] - (dx[1] + eta * (dx[2] - dx[1])), p, lagged)
+
+
+def friction_ee(x, rest, p, lagged):
+  """``friction_energy_ee`` (``friction_helpers.py:355-405``): lagged (gamma1, gamma2, t0, t1, lambda)."""
+  g1, g2 = lagged[0], lagged[1]
+  dx = x - rest
+  return _friction(dx[0] + g1 * (dx[1] - dx[0]) - dx[2] - g2 * (dx[3] - dx[2]), p, lagged)
+
+
+def friction_pp(x, rest, p, lagged):
+  """``friction_energy_pp`` (``friction_helpers.py:469-500``): lagged (0, 0, t0, t1, lambda)."""
+  dx = x - rest
+  return _friction(dx[0] - dx[1], p, lagged)
+
+
+def _lambda_last_h(d2, dhat, kappa):
+  """``lambda_last_h_rank2`` (``friction_helpers.py:12-23``)."""
+  i5log = np.log(d2 / dhat)
+  lenE = d2 - dhat
+  inner = i5log * i5log * (2.0 * d2 - 2.0 * dhat) + 2.0 * i5log * lenE * lenE / d2
+  return -kappa * 2.0 * np.sqrt(d2) * inner
+
+
+def _unit(v):
+  return v / np.linalg.norm(v)
+
+
+def lagged_friction_pe(x_old, dhat, kappa):
+  """(eta, 0, tangent0, tangent1, lambda) of a point-edge pair
+  (``closest_point_coord_and_tangent_basis_pe``, ``lambda_last_h_pe``,
+  ``friction_helpers.py:188-232``)."""
+  p, e0, e1 = (np.asarray(v, dtype=np.float64) for v in x_old)
+  edge = e1 - e0
+  eta = (p - e0) @ edge / (edge @ edge)
+  q = e0 + eta * edge
+  d2 = (p - q) @ (p - q)
+  return np.concatenate([[eta, 0.0], _unit(edge), _unit(np.cross(edge, p - e0)), [_lambda_last_h(d2, dhat, kappa)]])
+
+
+def lagged_friction_ee(x_old, dhat, kappa):
+  """(gamma1, gamma2, tangent0, tangent1, lambda) of an edge-edge pair
+  (``closest_point_coord_and_tangent_basis_ee``, ``lambda_last_h_ee``,
+  ``friction_helpers.py:283-352``)."""
+  a0, a1, b0, b1 = (np.asarray(v, dtype=np.float64) for v in x_old)
+  e20, e01, e23 = a0 - b0, a1 - a0, b1 - b0
+  A = np.array([[e01 @ e01, -(e23 @ e01)], [-(e23 @ e01), e23 @ e23]])
+  gamma = np.linalg.inv(A) @ np.array([-(e20 @ e01), e20 @ e23])
+  r = (a0 + gamma[0] * e01) - (b0 + gamma[1] * e23)
+  return np.concatenate([gamma, _unit(e01), _unit(np.cross(np.cross(e01, e23), e01)),
+                         [_lambda_last_h(r @ r, dhat, kappa)]])
+
+
+def lagged_friction_pp(x_old, dhat, kappa):
+  """(0, 0, tangent0, tangent1, lambda) of a point-point pair
+  (``closest_point_coord_and_tangent_basis_pp``, ``lambda_last_h_pp``,
+  ``friction_helpers.py:411-466``)."""
+  p0, p1 = (np.asarray(v, dtype=np.float64) for v in x_old)
+  v = p1 - p0
+  xc, yc = np.array([0.0, -v[2], v[1]]), np.array([v[2], 0.0, -v[0]])
+  raw = xc if xc @ xc > yc @ yc else yc
+  r = p0 - p1
+  return np.concatenate([[0.0, 0.0], _unit(raw), _unit(np.cross(v, raw)), [_lambda_last_h(r @ r, dhat, kappa)]])
 
 
 def lagged_friction_pt(x_old, dhat, kappa):
@@ -173,7 +251,9 @@ def lagged_friction_pt(x_old, dhat, kappa):
 
 
 KINDS = {1: point_point, 2: point_edge, 3: point_triangle, 4: edge_edge, 5: bending, 6: baraff_witkin,
-         7: stvk_membrane, 8: friction_pt}
+         7: stvk_membrane, 8: friction_pt, 9: friction_pe, 10: friction_ee, 11: friction_pp}
+FRICTION_KINDS = (8, 9, 10, 11)
+LAGGED = {8: lagged_friction_pt, 9: lagged_friction_pe, 10: lagged_friction_ee, 11: lagged_friction_pp}
 
 
 def energy_grad_hess(kind, x, rest, params, lagged=None):

@@ -18,6 +18,12 @@ It executes the reference's own Python code and stores its outputs:
 * ``cloth_torch.npz`` -- bending and Baraff-Witkin energies and gradients
   from the reference's float64 PyTorch scripts (``bending.py``,
   ``baraff_witkin.py`` in the same folder), see :func:`torch_cloth`.
+* ``helpers_torch.npz`` -- the contact barriers, affine-body terms and the
+  four lagged friction kinds from the reference's own formula code
+  (``examples/dropping_in_container_mixed/helpers.py``,
+  ``examples/dropping_in_container/friction_helpers.py``), run over a float64
+  torch stand-in for the symbolic ``attribute`` class, see
+  :func:`helper_energies`.
 * ``mas_cpu_reference.npz`` -- the reference's NumPy MAS solver
   (``yasps/yasps/solver/mas``) on a small SNH + inertia system, with pymetis
   replaced by the chunk-ordering shim documented in ``oracle/mas.py`` (the
@@ -116,6 +122,265 @@ def torch_cloth(ref):
   np.savez(os.path.join(HERE, "cloth_torch.npz"), **out)
 
 
+class TorchAttribute:
+  """Float64 torch stand-in for the reference's symbolic ``attribute`` class
+  (``yasps/yasps/attribute/attribute.pyx``), covering the operators its
+  example energy helpers use: ``row``, indexing, ``+ - * /`` (``*`` is a
+  matrix product unless one side is a scalar), ``dot``, ``cross``, ``norm``,
+  ``log``, ``sqrt``, ``atan2``, ``transpose``, ``determinant``, ``inverse``,
+  ``trace``, comparisons, and the static ``to_array``, ``identity`` and
+  ``select``.  Values are 2-D tensors (a scalar is 1x1), so autograd
+  differentiates the helpers exactly as written."""
+
+  def __init__(self, value=None, float_value=None):
+    import torch
+    if float_value is not None:
+      value = float(float_value)
+    v = value if isinstance(value, torch.Tensor) else torch.tensor(value, dtype=torch.float64)
+    if v.dim() == 0:
+      v = v.reshape(1, 1)
+    elif v.dim() == 1:
+      v = v.reshape(1, -1)
+    self.v = v
+
+  @classmethod
+  def wrap(cls, x):
+    return x if isinstance(x, cls) else cls(x)
+
+  def scalar(self):
+    return self.v.numel() == 1
+
+  def __add__(self, o):
+    return TorchAttribute(self.v + TorchAttribute.wrap(o).v)
+
+  __radd__ = __add__
+
+  def __sub__(self, o):
+    return TorchAttribute(self.v - TorchAttribute.wrap(o).v)
+
+  def __rsub__(self, o):
+    return TorchAttribute(TorchAttribute.wrap(o).v - self.v)
+
+  def __neg__(self):
+    return TorchAttribute(-self.v)
+
+  def __mul__(self, o):
+    o = TorchAttribute.wrap(o)
+    if self.scalar() or o.scalar():
+      return TorchAttribute(self.v * o.v)
+    return TorchAttribute(self.v @ o.v)
+
+  def __rmul__(self, o):
+    return TorchAttribute.wrap(o) * self
+
+  def __truediv__(self, o):
+    return TorchAttribute(self.v / TorchAttribute.wrap(o).v)
+
+  def __rtruediv__(self, o):
+    return TorchAttribute(TorchAttribute.wrap(o).v / self.v)
+
+  def __lt__(self, o):
+    return TorchAttribute(self.v < TorchAttribute.wrap(o).v)
+
+  def __gt__(self, o):
+    return TorchAttribute(self.v > TorchAttribute.wrap(o).v)
+
+  def row(self, i):
+    return TorchAttribute(self.v[i:i + 1, :])
+
+  def __getitem__(self, i):
+    return TorchAttribute(self.v.reshape(-1)[i])
+
+  def dot(self, o):
+    return TorchAttribute((self.v.reshape(-1) * TorchAttribute.wrap(o).v.reshape(-1)).sum())
+
+  def cross(self, o):
+    import torch
+    c = torch.linalg.cross(self.v.reshape(-1), TorchAttribute.wrap(o).v.reshape(-1))
+    return TorchAttribute(c.reshape(self.v.shape))
+
+  def norm(self):
+    import torch
+    return TorchAttribute(torch.linalg.norm(self.v))
+
+  def log(self):
+    return TorchAttribute(self.v.log())
+
+  def sqrt(self):
+    return TorchAttribute(self.v.sqrt())
+
+  def atan2(self, o):
+    import torch
+    return TorchAttribute(torch.atan2(self.v, TorchAttribute.wrap(o).v))
+
+  def transpose(self):
+    return TorchAttribute(self.v.T)
+
+  def determinant(self):
+    import torch
+    return TorchAttribute(torch.linalg.det(self.v))
+
+  def inverse(self):
+    import torch
+    return TorchAttribute(torch.linalg.inv(self.v))
+
+  def trace(self):
+    return TorchAttribute(self.v.diagonal().sum())
+
+  @staticmethod
+  def to_array(values, rows, cols):
+    import torch
+    vs = [TorchAttribute.wrap(x).v.reshape(()) for x in values]
+    return TorchAttribute(torch.stack(vs).reshape(rows, cols))
+
+  @staticmethod
+  def identity(n):
+    import torch
+    return TorchAttribute(torch.eye(n, dtype=torch.float64))
+
+  @staticmethod
+  def select(cond, a, b):
+    import torch
+    a, b = TorchAttribute.wrap(a), TorchAttribute.wrap(b)
+    return TorchAttribute(torch.where(cond.v, a.v, b.v))
+
+
+def _helpers(path, names):
+  """Functions ``names`` of a reference helper module, run over the stand-in."""
+  tree = ast.parse(open(path).read())
+  keep = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name in names]
+  env = {"attribute": TorchAttribute}
+  exec(compile(ast.Module(body=keep, type_ignores=[]), path, "exec"), env)
+  return env
+
+
+def _ghess(f, flat):
+  """Energy, gradient and Hessian of the scalar ``f`` at the flat input."""
+  import torch
+  x = flat.clone().requires_grad_(True)
+  e = f(x)
+  (g,) = torch.autograd.grad(e, x)
+  h = torch.autograd.functional.hessian(f, flat.clone())
+  return float(e.detach()), g.numpy(), h.numpy()
+
+
+def _contact_configs(rng, kind, n, dhat):
+  """Seeded element positions [n, A, 3] of a contact kind with the squared
+  (line / plane) distance in (0.1, 0.9) dhat."""
+  out = []
+  for _ in range(n):
+    d = np.sqrt(rng.uniform(0.1, 0.9) * dhat)
+    q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+    base = rng.normal(size=3) * 0.1
+    if kind == "pp":
+      x = np.array([[0, 0, 0], [0, 0, d]])
+    elif kind == "pe":
+      x = np.array([[0.3, 0, d], [0, 0, 0], [1.0, 0, 0]])
+    elif kind == "pt":
+      x = np.array([[0.25, 0.3, d], [0, 0, 0], [1.0, 0, 0], [0, 1.0, 0]])
+    else:  # ee
+      x = np.array([[-0.6, 0.1, 0], [0.7, -0.1, 0], [0.05, -0.5, d], [-0.1, 0.8, d]])
+    x = x + rng.normal(size=x.shape) * 1e-3 * np.array([1.0, 1.0, 0.0])
+    out.append(base + x @ q.T)
+  return np.asarray(out)
+
+
+def helper_energies(ref):
+  """Barriers, orthogonality, inertia, SNH and lagged friction from the
+  reference's own formula code, ``examples/dropping_in_container_mixed/
+  helpers.py`` (``inertia``, ``point_point``, ``point_edge``,
+  ``point_triangle``, ``edge_edge``, ``affine_energy``,
+  ``stable_neo_hookean_modified``) and ``examples/dropping_in_container/
+  friction_helpers.py`` (all four friction kinds with their lagged
+  coordinates, tangent bases and ``lambda_last_h``), executed over
+  :class:`TorchAttribute` and differentiated by autograd on seeded inputs.
+  Affine bodies compose their positions as the reference scene does
+  (``dropping_in_container_mixed/dropping_in_container.py:268-270`` for a
+  vertex, ``:288-313`` for a tet)."""
+  import torch
+  torch.set_default_dtype(torch.float64)
+  A = TorchAttribute
+  rng = np.random.default_rng(2024)
+  hp = _helpers(os.path.join(ref, "examples/dropping_in_container_mixed/helpers.py"),
+                ("inertia", "point_point", "point_edge", "point_triangle", "edge_edge", "affine_energy",
+                 "stable_neo_hookean_modified"))
+  fp = _helpers(os.path.join(ref, "examples/dropping_in_container/friction_helpers.py"),
+                {n for n in ("normalize", "scalar_zero", "lambda_last_h_rank2", "smooth_friction_phi",
+                             "friction_energy_from_rel_dx")} |
+                {f"{p}_{k}" for k in ("pp", "pe", "pt", "ee") for p in (
+                    "closest_point_coord_and_tangent_basis", "distance2", "lambda_last_h", "rel_dx",
+                    "friction_energy")} | {f"distance2_{k}_from_coord" for k in ("pp", "pe", "pt", "ee")})
+  out = {}
+  dhat, kappa = 1e-3, 1e4
+  arity = {"pp": 2, "pe": 3, "pt": 4, "ee": 4}
+  fname = {"pp": "point_point", "pe": "point_edge", "pt": "point_triangle", "ee": "edge_edge"}
+  for k, a in arity.items():
+    xs = _contact_configs(rng, k, 4, dhat)
+    es, gs, hs = [], [], []
+    for x in xs:
+      f = lambda v: hp[fname[k]](A(v.reshape(a, 3)), dhat, kappa).v.reshape(())
+      e, g, h = _ghess(f, torch.tensor(x.reshape(-1)))
+      es.append(e); gs.append(g); hs.append(h)
+    out.update({f"barrier_{k}_x": xs, f"barrier_{k}_energy": np.array(es), f"barrier_{k}_grad": np.array(gs),
+                f"barrier_{k}_hess": np.array(hs)})
+    # lagged friction: coordinates, tangent basis and lambda at x_old, energy at x
+    # (tangential moves below and above the smoothing radius sqrt(fDhat) dt)
+    fdt, rate = 0.01, 0.3
+    es, gs, hs, lags, xn = [], [], [], [], []
+    for t, x_old in enumerate(xs):
+      step = (1e-6 if t % 2 == 0 else 1e-3) * rng.normal(size=x_old.shape)
+      x_new = x_old + step
+      old = A(torch.tensor(x_old))
+      coord, basis = fp[f"closest_point_coord_and_tangent_basis_{k}"](old)
+      lam = fp[f"lambda_last_h_{k}"](old, coord, A(dhat), kappa)
+      coord, basis, lam = A(coord.v.detach()), A(basis.v.detach()), A(lam.v.detach())
+      f = lambda v: fp[f"friction_energy_{k}"](A(v.reshape(a, 3)), old, A(dhat), fdt, rate, coord,
+                                               basis.row(0), basis.row(1), lam).v.reshape(())
+      e, g, h = _ghess(f, torch.tensor(x_new.reshape(-1)))
+      es.append(e); gs.append(g); hs.append(h); xn.append(x_new)
+      lags.append(np.concatenate([coord.v.reshape(-1).numpy(), basis.v.reshape(-1).numpy(), lam.v.reshape(-1).numpy()]))
+    out.update({f"friction_{k}_x_old": xs, f"friction_{k}_x": np.array(xn), f"friction_{k}_energy": np.array(es),
+                f"friction_{k}_grad": np.array(gs), f"friction_{k}_hess": np.array(hs),
+                f"friction_{k}_lagged": np.array(lags)})
+  out.update(barrier_params=np.array([dhat, kappa]), friction_params=np.array([dhat, 0.01, 0.3]))
+  # affine bodies: q = (A row-major, t)
+  qs = []
+  for _ in range(4):
+    rot, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+    qs.append(np.concatenate([(rot @ (np.eye(3) + 0.05 * rng.normal(size=(3, 3)))).reshape(-1), rng.normal(size=3)]))
+  qs = np.asarray(qs)
+  ortho = [_ghess(lambda q: hp["affine_energy"](A(q[:9].reshape(3, 3))).v.reshape(()), torch.tensor(q)) for q in qs]
+  xbar, xb, vel = rng.normal(size=(4, 3)), rng.normal(size=(4, 3)), rng.normal(size=(4, 3))
+  mass, dt = 0.37, 0.01
+
+  def inertia_q(q, i):
+    pos = A(q[:9].reshape(3, 3)) * A(torch.tensor(xbar[i]).reshape(3, 1)) + A(q[9:12].reshape(3, 1))
+    return hp["inertia"](A(torch.tensor(xb[i]).reshape(3, 1)), A(torch.tensor(vel[i]).reshape(3, 1)), dt, pos,
+                         mass).v.reshape(())
+  inert = [_ghess(lambda q: inertia_q(q, i), torch.tensor(qs[i])) for i in range(4)]
+  rest = np.array([[0, 0, 0], [1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0]]) * 0.2 + rng.normal(size=(4, 4, 3)) * 0.02
+  mu, lam_ = 2000.0, 1000.0
+
+  def snh_q(q, i):
+    r = A(torch.tensor(rest[i]))
+    t = q[9:12]
+    pos = r * A(q[:9].reshape(3, 3)).transpose() + A(torch.stack([t] * 4))
+
+    def edges(p):
+      x0, x1, x2 = p.row(1) - p.row(0), p.row(2) - p.row(0), p.row(3) - p.row(0)
+      return A.to_array([x0[0], x0[1], x0[2], x1[0], x1[1], x1[2], x2[0], x2[1], x2[2]], rows=3, cols=3)
+    return hp["stable_neo_hookean_modified"](edges(pos), edges(r), mu, lam_, dt).v.reshape(())
+  snh = [_ghess(lambda q: snh_q(q, i), torch.tensor(qs[i])) for i in range(4)]
+  for name, res in (("orthogonality", ortho), ("inertia", inert), ("snh", snh)):
+    out[f"affine_{name}_energy"] = np.array([r[0] for r in res])
+    out[f"affine_{name}_grad"] = np.array([r[1] for r in res])
+    out[f"affine_{name}_hess"] = np.array([r[2] for r in res])
+  out.update(affine_q=qs, affine_xbar=xbar, affine_x_before=xb, affine_velocity=vel,
+             affine_inertia_params=np.array([mass, dt, 0.0, -9.8, 0.0]), affine_rest=rest,
+             affine_snh_params=np.array([mu, lam_, dt]))
+  np.savez(os.path.join(HERE, "helpers_torch.npz"), **out)
+
+
 def sympy_six_tets(ref):
   path = os.path.join(ref, "tests/energy/check_stable_neo_hookean.py")
   out = runpy.run_path(path, run_name="__golden__")
@@ -197,7 +462,7 @@ if __name__ == "__main__":
   ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YASPS_REFERENCE", "")
   if not ref or not os.path.isdir(ref):
     raise SystemExit("usage: make_golden.py <reference checkout>")
-  which = sys.argv[2:] or ["torch", "mas", "sympy", "cloth"]
+  which = sys.argv[2:] or ["torch", "mas", "sympy", "cloth", "helpers"]
   if "torch" in which:
     torch_single_tet(ref)
   if "mas" in which:
@@ -206,3 +471,5 @@ if __name__ == "__main__":
     sympy_six_tets(ref)
   if "cloth" in which:
     torch_cloth(ref)
+  if "helpers" in which:
+    helper_energies(ref)

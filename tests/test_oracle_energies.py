@@ -2,9 +2,11 @@
 scripts (bending, Baraff-Witkin) and checked for derivative consistency.
 
 The reference scripts guard norms with +1e-8 terms, which move these
-values by up to ~5e-7 relative, so the pin tolerance is 2e-6 relative; the barriers, StVK and friction have no runnable reference
-(parity unpinned), their Hessians are checked against finite differences of
-the autograd gradients.
+values by up to ~5e-7 relative, so the pin tolerance is 2e-6 relative.  The
+barriers and the four friction kinds are pinned at 1e-12 to the reference's
+own helper code in ``test_oracle_golden.py``; StVK has no reference
+counterpart (parity unpinned).  Every kind's Hessian is also checked against
+finite differences of its autograd gradient.
 """
 
 import os

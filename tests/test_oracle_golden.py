@@ -92,3 +92,66 @@ def test_diagonal_pseudo_inverse_rule():
   blk = (q * w) @ q.T
   inv = projection.diagonal_block_pseudo_inverse(blk[None])[0]
   np.testing.assert_allclose(inv, (q * np.array([0.5, 0.25, 1e-8])) @ q.T, atol=1e-12)
+
+
+def _close(a, b, tol=1e-12):
+  a, b = np.asarray(a), np.asarray(b)
+  return float(np.abs(a - b).max()) <= tol * max(float(np.abs(b).max()), 1e-300)
+
+
+BARRIERS = {"pp": 1, "pe": 2, "pt": 3, "ee": 4}
+FRICTIONS = {"pt": 8, "pe": 9, "ee": 10, "pp": 11}
+
+
+@pytest.mark.parametrize("kind", sorted(BARRIERS))
+def test_barriers_match_reference_helpers(kind):
+  """``point_point`` / ``point_edge`` / ``point_triangle`` / ``edge_edge`` of
+  ``examples/dropping_in_container_mixed/helpers.py`` (fixtures from the
+  reference's code over a float64 stand-in of its ``attribute`` class)."""
+  from oracle import vertex_energies as ve
+  d = _load("helpers_torch.npz")
+  x = d[f"barrier_{kind}_x"]
+  e, g, h = ve.energy_grad_hess(BARRIERS[kind], x, None, tuple(d["barrier_params"]))
+  assert _close(e, d[f"barrier_{kind}_energy"])
+  assert _close(g, d[f"barrier_{kind}_grad"])
+  assert _close(h, d[f"barrier_{kind}_hess"])
+
+
+@pytest.mark.parametrize("kind", sorted(FRICTIONS))
+def test_lagged_friction_matches_reference_helpers(kind):
+  """The lagged coordinates, tangent basis and lambda at the last positions
+  and the friction energy at the current ones, for the four kinds of
+  ``examples/dropping_in_container/friction_helpers.py``; half of the cases
+  move less than the smoothing radius, half more."""
+  from oracle import vertex_energies as ve
+  d = _load("helpers_torch.npz")
+  dhat, kappa = d["barrier_params"]
+  x_old, x = d[f"friction_{kind}_x_old"], d[f"friction_{kind}_x"]
+  k = FRICTIONS[kind]
+  lagged = np.stack([ve.LAGGED[k](xo, dhat, kappa) for xo in x_old])
+  assert _close(lagged, d[f"friction_{kind}_lagged"])
+  e, g, h = ve.energy_grad_hess(k, x, x_old, tuple(d["friction_params"]), lagged)
+  assert _close(e, d[f"friction_{kind}_energy"])
+  assert _close(g, d[f"friction_{kind}_grad"])
+  assert _close(h, d[f"friction_{kind}_hess"])
+
+
+def test_affine_terms_match_reference_helpers():
+  """``affine_energy``, ``inertia`` of ``A xbar + t`` and
+  ``stable_neo_hookean_modified`` of a tet at ``xbar A^T + t`` (the
+  reference scene's compositions), differentiated in the body coordinates."""
+  from oracle import affine_energies as ae
+  d = _load("helpers_torch.npz")
+  q = d["affine_q"]
+  e, g, h = ae.grad_hess(ae.orthogonality, q, np.zeros((len(q), 1)), 1.0)
+  assert _close(e, d["affine_orthogonality_energy"]) and _close(g, d["affine_orthogonality_grad"])
+  assert _close(h, d["affine_orthogonality_hess"])
+  mass, dt, *grav = d["affine_inertia_params"]
+  data = np.concatenate([d["affine_xbar"], d["affine_x_before"], d["affine_velocity"],
+                         np.full((len(q), 1), mass)], axis=1)
+  e, g, h = ae.grad_hess(ae.inertia, q, data, (dt, *grav))
+  assert _close(e, d["affine_inertia_energy"]) and _close(g, d["affine_inertia_grad"])
+  assert _close(h, d["affine_inertia_hess"])
+  e, g, h = ae.grad_hess(ae.snh, q, d["affine_rest"].reshape(len(q), 12), tuple(d["affine_snh_params"]))
+  assert _close(e, d["affine_snh_energy"]) and _close(g, d["affine_snh_grad"])
+  assert _close(h, d["affine_snh_hess"])
