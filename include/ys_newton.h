@@ -212,10 +212,11 @@ int32_t ys_inertia_eval(const ys_inertia_args* args, void* stream);
  *     rest = x_init;
  *   STVK_MEMBRANE: mu, lam, thickness, dt; rest = x_init, the Baraff-Witkin
  *     rest frame (no counterpart in the reference);
- *   FRICTION_PT (friction_helpers.py:12-66, :73-182): fDhat, dt,
- *     frictionRate; rest = positions at the start of the step; params per
- *     element (stride >= 9): beta1, beta2, tangent0[3], tangent1[3],
- *     lambda_last_h.                                                       */
+ *   FRICTION_PT / _PE / _EE / _PP (friction_helpers.py:12-66; :73-182,
+ *     :188-276, :283-405, :411-500): fDhat, dt, frictionRate; rest =
+ *     positions at the start of the step; params per element (stride >= 9):
+ *     the lagged closest-point coordinates (beta1, beta2 / eta, 0 /
+ *     gamma1, gamma2 / 0, 0), tangent0[3], tangent1[3], lambda_last_h.    */
 #define YS_ENERGY_POINT_POINT 1
 #define YS_ENERGY_POINT_EDGE 2
 #define YS_ENERGY_POINT_TRIANGLE 3
@@ -224,13 +225,16 @@ int32_t ys_inertia_eval(const ys_inertia_args* args, void* stream);
 #define YS_ENERGY_BARAFF_WITKIN 6
 #define YS_ENERGY_STVK_MEMBRANE 7
 #define YS_ENERGY_FRICTION_PT 8
+#define YS_ENERGY_FRICTION_PE 9
+#define YS_ENERGY_FRICTION_EE 10
+#define YS_ENERGY_FRICTION_PP 11
 
 typedef struct ys_energy_args {
   int32_t kind;                 /* YS_ENERGY_*                                      */
   ys_union3 position;           /* current positions (DATA)                         */
   ys_union3 rest;               /* rest / initial / previous positions by kind      */
   const uint32_t* conn;         /* [n x arity] union indices                        */
-  uint32_t arity;               /* 2 (PP), 3 (PE, membranes), 4 (PT, EE, bending, friction) */
+  uint32_t arity;               /* 2 (PP), 3 (PE, membranes), 4 (PT, EE, bending) */
   uint32_t num_elements;
   const double* params;         /* [n x param_stride] per-element parameters or NULL */
   uint32_t param_stride;

@@ -3,8 +3,8 @@
 A sheet of ``m x m`` vertices in the xz plane (two triangles a quad) with a
 membrane and dihedral bending, plus a cloud of free points hovering above it
 at distances inside d-hat, coupled to the sheet by point-triangle,
-edge-edge, point-edge and point-point barriers and by lagged point-triangle
-friction.  Every vertex is a target (one primitive, no union).  ``build``
+edge-edge, point-edge and point-point barriers and by lagged friction of the
+same four kinds.  Every vertex is a target (one primitive, no union).  ``build``
 uses the public scene API; ``oracle_assembly`` assembles the same terms with
 the oracle (same term order, same pattern rules).
 """
@@ -66,6 +66,9 @@ class VertexScene:
     self.bend_params = (1e-3, dt)
     self.fric_params = (1e-6, dt, 0.3)
     self.lagged = np.stack([ve.lagged_friction_pt(self.x_old[q], dhat, kappa) for q in self.pt])
+    self.lagged_pe = np.stack([ve.lagged_friction_pe(self.x_old[q], dhat, kappa) for q in self.pe])
+    self.lagged_ee = np.stack([ve.lagged_friction_ee(self.x_old[q], dhat, kappa) for q in self.ee])
+    self.lagged_pp = np.stack([ve.lagged_friction_pp(self.x_old[q], dhat, kappa) for q in self.pp])
     self.n = 3 * len(self.x)
     self.mass = np.full(len(self.x), 1e-3)
     self.gravity = np.array([0.0, -9.8, 0.0])
@@ -80,7 +83,10 @@ class VertexScene:
             (4, self.ee, b, None, None),
             (2, self.pe, b, None, None),
             (1, self.pp, b, None, None),
-            (8, self.pt, self.fric_params, "old", self.lagged)]
+            (8, self.pt, self.fric_params, "old", self.lagged),
+            (9, self.pe, self.fric_params, "old", self.lagged_pe),
+            (10, self.ee, self.fric_params, "old", self.lagged_ee),
+            (11, self.pp, self.fric_params, "old", self.lagged_pp)]
 
   def build(self, projection_method=1):
     from yasps_b200 import energies as E
@@ -118,7 +124,9 @@ class VertexScene:
       else:
         lagged = prim.addConstant("lagged", rows=9, cols=1)
         lagged.updateValue(lag)
-        e = E.friction_point_triangle(xj, aux_att, *params, lagged)
+        fric = {8: E.friction_point_triangle, 9: E.friction_point_edge, 10: E.friction_edge_edge,
+                11: E.friction_point_point}[kind]
+        e = fric(xj, aux_att, *params, lagged)
       att = prim.addAttribute("energy", computed_attribute=e)
       sc.addEnergy(att, projection_method=projection_method)
     mass = verts.addConstant("mass")

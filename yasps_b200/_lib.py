@@ -28,7 +28,8 @@ YS_STOP_PRECONDITIONED = 0
 YS_STOP_RESIDUAL = 1
 YS_MAX_UNION = 8
 (YS_ENERGY_POINT_POINT, YS_ENERGY_POINT_EDGE, YS_ENERGY_POINT_TRIANGLE, YS_ENERGY_EDGE_EDGE, YS_ENERGY_BENDING,
- YS_ENERGY_BARAFF_WITKIN, YS_ENERGY_STVK_MEMBRANE, YS_ENERGY_FRICTION_PT) = range(1, 9)
+ YS_ENERGY_BARAFF_WITKIN, YS_ENERGY_STVK_MEMBRANE, YS_ENERGY_FRICTION_PT, YS_ENERGY_FRICTION_PE,
+ YS_ENERGY_FRICTION_EE, YS_ENERGY_FRICTION_PP) = range(1, 12)
 YS_SERVE_EMPTY, YS_SERVE_INIT, YS_SERVE_REFINE, YS_SERVE_START, YS_SERVE_ITER, YS_SERVE_DONE, YS_SERVE_FAILED = range(7)
 
 

@@ -10,7 +10,8 @@
 //   baraff_witkin (:272-292): stretch / shear of the rest-frame deformation
 //     gradient (compute_rest_shape, :240-270), area-weighted, dt^2;
 // the lagged friction of examples/dropping_in_container/friction_helpers.py
-// (:12-66 smoothing, :73-182 point-triangle), and a StVK membrane on the same
+// (:12-66 smoothing; point-triangle, point-edge, edge-edge and point-point),
+// and a StVK membrane on the same
 // rest frame (the reference ships no StVK).  Gradients and Hessians come from
 // second-order forward-mode differentiation (ys_ad.cuh); the local Hessian
 // is projected like the SNH one (LDL^T PSD test, then the negative modes) and
@@ -216,32 +217,79 @@ struct StvkMembrane {
   }
 };
 
-// Lagged point-triangle friction (friction_helpers.py:12-66, :73-182).
-// Per element params: beta1, beta2, tangent0 (3), tangent1 (3), lambda_last_h;
-// `rest` holds the positions at the start of the step.
+// Lagged friction (friction_helpers.py:12-66): with the lagged tangent
+// basis (q[2..4], q[5..7]) and lambda_last_h (q[8]), phi of the tangential
+// relative displacement y = |(t0.rel, t1.rel)| (smoothed below sqrt(fDhat) dt)
+// times frictionRate lambda.  `rest` holds the positions at the start of the
+// step, so d(x - x_old)/dx = I.
+template <int N>
+__device__ __forceinline__ HD<N> lagged_friction(const ys_energy_args& a, const double* q, const HV<N>& rel) {
+  const HD<N> u0 = q[2] * rel.x + q[3] * rel.y + q[4] * rel.z;
+  const HD<N> u1 = q[5] * rel.x + q[6] * rel.y + q[7] * rel.z;
+  const HD<N> y2 = sq(u0) + sq(u1);
+  const double fdhat = a.values[0], dt = a.values[1], rate = a.values[2];
+  const double eps = sqrt(fdhat) * dt, fric_dhat = fdhat * dt * dt;
+  const HD<N> y = hd_sqrt(y2 + 1e-16);
+  HD<N> phi;
+  if (y2.v > fric_dhat) phi = y;
+  else phi = ((1.0 / eps) * y2 + eps / 3.0) - (1.0 / (3.0 * eps * eps)) * (y2 * y);
+  return (rate * q[8]) * phi;
+}
+
+template <int N, int A>
+__device__ __forceinline__ void step_inputs(const Pts<A>& x, const Pts<A>& r, HV<N> (&dx)[A]) {
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    const double d[3] = {x.p[k][0] - r.p[k][0], x.p[k][1] - r.p[k][1], x.p[k][2] - r.p[k][2]};
+    dx[k] = hv_var<N>(d, 3 * k);
+  }
+}
+
+// Point-triangle (:73-182): lagged (beta1, beta2) of the closest point.
 struct FrictionPT {
   static constexpr int A = 4;
   template <int N>
   __device__ static HD<N> eval(const ys_energy_args& a, uint32_t t, const Pts<A>& x, const Pts<A>& r) {
     const double* q = a.params + (uint64_t)t * a.param_stride;
-    const double b1 = q[0], b2 = q[1];
-    HV<N> dx[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const double d[3] = {x.p[k][0] - r.p[k][0], x.p[k][1] - r.p[k][1], x.p[k][2] - r.p[k][2]};
-      dx[k] = hv_var<N>(d, 3 * k);  // d(x - x_old)/dx = I
-    }
-    const HV<N> rel = dx[0] - (dx[1] + b1 * (dx[2] - dx[1]) + b2 * (dx[3] - dx[1]));
-    const HD<N> u0 = q[2] * rel.x + q[3] * rel.y + q[4] * rel.z;
-    const HD<N> u1 = q[5] * rel.x + q[6] * rel.y + q[7] * rel.z;
-    const HD<N> y2 = sq(u0) + sq(u1);
-    const double fdhat = a.values[0], dt = a.values[1], rate = a.values[2];
-    const double eps = sqrt(fdhat) * dt, fric_dhat = fdhat * dt * dt;
-    const HD<N> y = hd_sqrt(y2 + 1e-16);
-    HD<N> phi;
-    if (y2.v > fric_dhat) phi = y;
-    else phi = ((1.0 / eps) * y2 + eps / 3.0) - (1.0 / (3.0 * eps * eps)) * (y2 * y);
-    return (rate * q[8]) * phi;
+    HV<N> dx[A];
+    step_inputs<N>(x, r, dx);
+    return lagged_friction<N>(a, q, dx[0] - (dx[1] + q[0] * (dx[2] - dx[1]) + q[1] * (dx[3] - dx[1])));
+  }
+};
+
+// Point-edge (:188-276): lagged eta of the closest point on the edge.
+struct FrictionPE {
+  static constexpr int A = 3;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t t, const Pts<A>& x, const Pts<A>& r) {
+    const double* q = a.params + (uint64_t)t * a.param_stride;
+    HV<N> dx[A];
+    step_inputs<N>(x, r, dx);
+    return lagged_friction<N>(a, q, dx[0] - (dx[1] + q[0] * (dx[2] - dx[1])));
+  }
+};
+
+// Edge-edge (:283-405): lagged (gamma1, gamma2) of the closest points.
+struct FrictionEE {
+  static constexpr int A = 4;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t t, const Pts<A>& x, const Pts<A>& r) {
+    const double* q = a.params + (uint64_t)t * a.param_stride;
+    HV<N> dx[A];
+    step_inputs<N>(x, r, dx);
+    return lagged_friction<N>(a, q, ((dx[0] + q[0] * (dx[1] - dx[0])) - dx[2]) - q[1] * (dx[3] - dx[2]));
+  }
+};
+
+// Point-point (:411-500).
+struct FrictionPP {
+  static constexpr int A = 2;
+  template <int N>
+  __device__ static HD<N> eval(const ys_energy_args& a, uint32_t t, const Pts<A>& x, const Pts<A>& r) {
+    const double* q = a.params + (uint64_t)t * a.param_stride;
+    HV<N> dx[A];
+    step_inputs<N>(x, r, dx);
+    return lagged_friction<N>(a, q, dx[0] - dx[1]);
   }
 };
 
@@ -943,10 +991,12 @@ int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
   YS_REQUIRE(a.rest.num_children <= YS_MAX_UNION, YS_ERR_INVALID, "bad rest union");
   if (a.num_elements == 0) return YS_OK;
   cudaStream_t s = (cudaStream_t)stream;
+  const bool friction = a.kind == YS_ENERGY_FRICTION_PT || a.kind == YS_ENERGY_FRICTION_PE ||
+                        a.kind == YS_ENERGY_FRICTION_EE || a.kind == YS_ENERGY_FRICTION_PP;
   const bool needs_rest = a.kind == YS_ENERGY_BENDING || a.kind == YS_ENERGY_BARAFF_WITKIN ||
-                          a.kind == YS_ENERGY_STVK_MEMBRANE || a.kind == YS_ENERGY_FRICTION_PT;
+                          a.kind == YS_ENERGY_STVK_MEMBRANE || friction;
   YS_REQUIRE(!needs_rest || a.rest.num_children >= 1, YS_ERR_INVALID, "this energy needs rest positions");
-  YS_REQUIRE(a.kind != YS_ENERGY_FRICTION_PT || (a.params && a.param_stride >= 9), YS_ERR_INVALID,
+  YS_REQUIRE(!friction || (a.params && a.param_stride >= 9), YS_ERR_INVALID,
              "friction needs 9 lagged parameters per element");
   if (a.block_records == nullptr && a.grad_records == nullptr) {
     // energy only
@@ -960,6 +1010,9 @@ int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
       case YS_ENERGY_BARAFF_WITKIN: return ys::launch_energy_value<ys::BaraffWitkin>(a, s);
       case YS_ENERGY_STVK_MEMBRANE: return ys::launch_energy_value<ys::StvkMembrane>(a, s);
       case YS_ENERGY_FRICTION_PT: return ys::launch_energy_value<ys::FrictionPT>(a, s);
+      case YS_ENERGY_FRICTION_PE: return ys::launch_energy_value<ys::FrictionPE>(a, s);
+      case YS_ENERGY_FRICTION_EE: return ys::launch_energy_value<ys::FrictionEE>(a, s);
+      case YS_ENERGY_FRICTION_PP: return ys::launch_energy_value<ys::FrictionPP>(a, s);
       default: break;
     }
     YS_REQUIRE(false, YS_ERR_INVALID, "unknown energy kind");
@@ -975,6 +1028,9 @@ int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
     case YS_ENERGY_BARAFF_WITKIN: return ys::launch_energy<ys::BaraffWitkin>(a, s);
     case YS_ENERGY_STVK_MEMBRANE: return ys::launch_energy<ys::StvkMembrane>(a, s);
     case YS_ENERGY_FRICTION_PT: return ys::launch_energy<ys::FrictionPT>(a, s);
+    case YS_ENERGY_FRICTION_PE: return ys::launch_energy<ys::FrictionPE>(a, s);
+    case YS_ENERGY_FRICTION_EE: return ys::launch_energy<ys::FrictionEE>(a, s);
+    case YS_ENERGY_FRICTION_PP: return ys::launch_energy<ys::FrictionPP>(a, s);
     default: break;
   }
   YS_REQUIRE(false, YS_ERR_INVALID, "unknown energy kind");

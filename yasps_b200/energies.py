@@ -178,6 +178,9 @@ BendingEnergy = _vertex_energy("BendingEnergy", 5, 4, ("bendStiff", "dt"), True)
 BaraffWitkinEnergy = _vertex_energy("BaraffWitkinEnergy", 6, 3, ("stretchS", "shearS", "thickness", "dt"), True)
 StvkMembraneEnergy = _vertex_energy("StvkMembraneEnergy", 7, 3, ("mu", "lam", "thickness", "dt"), True)
 FrictionPointTriangle = _vertex_energy("FrictionPointTriangle", 8, 4, ("fDhat", "dt", "frictionRate"), True)
+FrictionPointEdge = _vertex_energy("FrictionPointEdge", 9, 3, ("fDhat", "dt", "frictionRate"), True)
+FrictionEdgeEdge = _vertex_energy("FrictionEdgeEdge", 10, 4, ("fDhat", "dt", "frictionRate"), True)
+FrictionPointPoint = _vertex_energy("FrictionPointPoint", 11, 2, ("fDhat", "dt", "frictionRate"), True)
 
 
 def point_point(position, dHat, kappa):
@@ -223,6 +226,24 @@ def friction_point_triangle(position, old_position, fDhat, dt, frictionRate, lag
   Newton step as in the reference.
   """
   return FrictionPointTriangle(position, old_position, (fDhat, dt, frictionRate), per_element=lagged)
+
+
+def friction_point_edge(position, old_position, fDhat, dt, frictionRate, lagged):
+  """Lagged point-edge friction (``friction_helpers.py:12-66, 188-276``);
+  ``lagged``: ``eta, 0, tangent0 (3), tangent1 (3), lambda_last_h``."""
+  return FrictionPointEdge(position, old_position, (fDhat, dt, frictionRate), per_element=lagged)
+
+
+def friction_edge_edge(position, old_position, fDhat, dt, frictionRate, lagged):
+  """Lagged edge-edge friction (``friction_helpers.py:12-66, 283-405``);
+  ``lagged``: ``gamma1, gamma2, tangent0 (3), tangent1 (3), lambda_last_h``."""
+  return FrictionEdgeEdge(position, old_position, (fDhat, dt, frictionRate), per_element=lagged)
+
+
+def friction_point_point(position, old_position, fDhat, dt, frictionRate, lagged):
+  """Lagged point-point friction (``friction_helpers.py:12-66, 411-500``);
+  ``lagged``: ``0, 0, tangent0 (3), tangent1 (3), lambda_last_h``."""
+  return FrictionPointPoint(position, old_position, (fDhat, dt, frictionRate), per_element=lagged)
 
 
 # ---- affine (ABD) bodies ------------------------------------------------------------
