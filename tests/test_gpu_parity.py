@@ -111,6 +111,55 @@ def test_spmv_fp64_and_fp32(c0):
     L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32), L.ptr(y),
            1 if k else 0, L.stream_ptr())
   assert np.array_equal(y.cpu().numpy(), y32)
+  # the tiled SpMV (shared-memory stages by bulk copies) gives the same bits
+  check_tiled_spmv(H, x32, y.cpu().numpy())
+
+
+def check_tiled_spmv(H, x32, expected):
+  import torch
+  from yasps_b200 import _lib as L
+  nv = H.rows // 3
+  (bs,) = H.block_sets
+  row_ptr, eb, ec = H.spmv_plan(bs)
+  row_block, cap = H.tile_plan(bs)
+  assert cap > 0
+  rb = row_block.cpu().numpy().astype(np.int64)[:nv + 1]
+  pos = bs.pattern.positions[:2 * bs.pattern.num_unique].cpu().numpy().astype(np.int64).reshape(-1, 2)
+  assert np.array_equal(rb, np.searchsorted(pos[:, 0], 3 * np.arange(nv + 1), side="left"))
+  tiles = np.arange(0, nv, L.YS_SPMV_TILE_ROWS)
+  assert cap == int((rb[np.minimum(tiles + L.YS_SPMV_TILE_ROWS, nv)] - rb[tiles]).max())
+  status = torch.zeros(1, dtype=torch.int32, device="cuda")
+  y = torch.full((H.rows,), np.nan, dtype=torch.float64, device="cuda")
+  for _ in range(2):
+    L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block), cap, nv,
+           L.ptr(x32), L.ptr(y), 0, L.ptr(status), L.stream_ptr())
+    assert np.array_equal(y.cpu().numpy(), expected)
+  assert int(status.item()) == 0
+
+
+def test_tiled_spmv_many_tiles_bit_identical():
+  """A 24^3 cube (13,248 free variables, 207 tiles of 64 rows) through the
+  tiled SpMV against the row-plan SpMV, bit for bit, and the FP32 loop that
+  uses it against the oracle."""
+  import torch
+  from yasps_b200 import _lib as L
+  cube = scenes.fem_cube(24, spacing=0.1, young=1e6, poisson=0.45, noise=0.005, seed=1)
+  sc, _ = build(cube, "mas", mixed_spmv=True, stop_rule="residual")
+  H = sc.minimizer.computeNumericValue()
+  H.ensure_fp32()
+  nv = H.rows // 3
+  (bs,) = H.block_sets
+  row_ptr, eb, ec = H.spmv_plan(bs)
+  x = torch.sin(torch.arange(H.rows, dtype=torch.float64, device="cuda") * 0.37)
+  x32 = torch.empty(4 * nv, dtype=torch.float32, device="cuda")
+  L.call("ys_pack_x32", L.ptr(x), nv, L.ptr(x32), L.stream_ptr())
+  y = torch.empty(H.rows, dtype=torch.float64, device="cuda")
+  L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32), L.ptr(y), 0,
+         L.stream_ptr())
+  check_tiled_spmv(H, x32, y.cpu().numpy())
+  ora = OracleCube(cube)
+  segs = sc.minimizeEnergy(tolerance=1e-6, maxIterations=2000)
+  assert solvers.relative_residual(ora.matvec, ora.gradient, segs[0].cpu().numpy()) <= 1e-6
 
 
 def test_block_jacobi_pcg_matches_oracle(c0):

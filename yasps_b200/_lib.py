@@ -30,6 +30,7 @@ YS_MAX_UNION = 8
 (YS_ENERGY_POINT_POINT, YS_ENERGY_POINT_EDGE, YS_ENERGY_POINT_TRIANGLE, YS_ENERGY_EDGE_EDGE, YS_ENERGY_BENDING,
  YS_ENERGY_BARAFF_WITKIN, YS_ENERGY_STVK_MEMBRANE, YS_ENERGY_FRICTION_PT, YS_ENERGY_FRICTION_PE,
  YS_ENERGY_FRICTION_EE, YS_ENERGY_FRICTION_PP) = range(1, 12)
+YS_SPMV_TILE_ROWS = 64
 YS_SERVE_EMPTY, YS_SERVE_INIT, YS_SERVE_REFINE, YS_SERVE_START, YS_SERVE_ITER, YS_SERVE_DONE, YS_SERVE_FAILED = range(7)
 
 
@@ -86,7 +87,8 @@ class CoupledArgs(C.Structure):
 
 class Matrix3(C.Structure):
   _fields_ = [("num_sets", u32), ("values", vp * 2), ("values32", vp * 2), ("row_ptr", vp * 2),
-              ("entry_block", vp * 2), ("entry_col", vp * 2), ("num_vars", u32)]
+              ("entry_block", vp * 2), ("entry_col", vp * 2), ("num_vars", u32), ("row_block", vp * 2),
+              ("tile_cap", u32 * 2)]
 
 
 class PcgArgs(C.Structure):
@@ -149,6 +151,8 @@ SIGNATURES = {
     "ys_mas_failed_domains": (i32, [vp, vp, P(i32)]),
     "ys_pack_x32": (i32, [vp, u32, vp, vp]),
     "ys_spmv3_x32": (i32, [vp, vp, vp, vp, u32, vp, vp, i32, vp]),
+    "ys_spmv_tile_plan": (i32, [vp, u32, vp, vp, u32, vp, P(u32), vp]),
+    "ys_spmv3_x32_tiled": (i32, [vp, vp, vp, vp, vp, u32, u32, vp, vp, i32, vp, vp]),
     "ys_pcg_workspace_doubles": (u64, [u32]),
     "ys_pcg_create": (i32, [P(PcgArgs), P(vp)]),
     "ys_pcg_run": (i32, [vp, vp, P(PcgResult)]),

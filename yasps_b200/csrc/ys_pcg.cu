@@ -17,6 +17,7 @@
 
 #include "ys_mas.cuh"
 #include "ys_pcg.cuh"
+#include "ys_spmv_tiled.cuh"
 
 namespace ys {
 
@@ -39,6 +40,7 @@ struct PcgParams {
   int stop_rule;
   int zero_guess;
   int restart_on_curvature;  // MAS: a non-positive curvature restarts from M^-1 r (zero step, beta = 0)
+  TiledSet tiled;            // tile plan of the FP32 set (pcg_spmv_dot_tiled)
   double tolerance;
   uint32_t max_it;
   cudaGraphConditionalHandle cond;
@@ -120,29 +122,9 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
   cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
 }
 
-// kRowLanes threads per row (see spmv3_group).
-// One instantiation per precision of the block values (the FP32 one keeps
-// fewer registers: higher occupancy for the latency-bound gathers).
-// A grid of resident size strides over the groups of kPcgBlock / kRowLanes
-// rows: the dot product then ends in a few hundred block partials (each
-// block's fence and ticket, and the last block's sum, are per block, so a
-// CTA per row group would pay them thousands of times).
-template <bool FP32>
-__global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
-  constexpr uint32_t kRows = kPcgBlock / kRowLanes;
-  const uint32_t groups = (P.nv + kRows - 1) / kRows;
-  const int lane = (int)(threadIdx.x % kRowLanes);
-  double v[1] = {0.0};
-  for (uint32_t gb = blockIdx.x; gb < groups; gb += gridDim.x) {  // block-uniform
-    const uint32_t i = gb * kRows + threadIdx.x / kRowLanes;
-    double q0, q1, q2;
-    if (FP32) spmv3_group_x32(P.sets, P.nsets, i, i < P.nv, lane, P.p32, q0, q1, q2);
-    else spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.p, q0, q1, q2);
-    if (i < P.nv && lane == 0) {
-      P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
-      v[0] += P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
-    }
-  }
+// Curvature p^T q (grid reduction) and the step length; the last block of
+// the grid decides.
+__device__ __forceinline__ void spmv_dot_finish(const PcgParams& P, double (&v)[1]) {
   if (!grid_reduce_last<1>(v, P.partials, P.tickets + 1)) return;
   if (threadIdx.x != 0) return;
   double* st = P.st;
@@ -166,6 +148,46 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
   } else {
     st[kAlpha] = rz / curv;
   }
+}
+
+// kRowLanes threads per row (see spmv3_group).
+// One instantiation per precision of the block values (the FP32 one keeps
+// fewer registers: higher occupancy for the latency-bound gathers).
+// A grid of resident size strides over the groups of kPcgBlock / kRowLanes
+// rows: the dot product then ends in a few hundred block partials (each
+// block's fence and ticket, and the last block's sum, are per block, so a
+// CTA per row group would pay them thousands of times).
+template <bool FP32>
+__global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
+  constexpr uint32_t kRows = kPcgBlock / kRowLanes;
+  const uint32_t groups = (P.nv + kRows - 1) / kRows;
+  const int lane = (int)(threadIdx.x % kRowLanes);
+  double v[1] = {0.0};
+  for (uint32_t gb = blockIdx.x; gb < groups; gb += gridDim.x) {  // block-uniform
+    const uint32_t i = gb * kRows + threadIdx.x / kRowLanes;
+    double q0, q1, q2;
+    if (FP32) spmv3_group_x32(P.sets, P.nsets, i, i < P.nv, lane, P.p32, q0, q1, q2);
+    else spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.p, q0, q1, q2);
+    if (i < P.nv && lane == 0) {
+      P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
+      v[0] += P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
+    }
+  }
+  spmv_dot_finish(P, v);
+}
+
+// The SpMV + dot of the FP32 loop over the tile plan: each persistent CTA
+// stages its tiles' blocks into shared memory by bulk copies (see
+// ys_spmv_tiled.cuh); lane 0 of a row group writes q and adds p . q.
+__global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot_tiled(PcgParams P) {
+  double v[1] = {0.0};
+  spmv3_tiles_x32(P.tiled, P.p32, P.tickets + 6, [&](uint32_t i, bool valid, int lane, double q0, double q1,
+                                                     double q2) {
+    if (!valid || lane != 0) return;
+    P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
+    v[0] += P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
+  });
+  spmv_dot_finish(P, v);
 }
 
 __global__ void __launch_bounds__(kPcgBlock) pcg_update_bj(PcgParams P) {
@@ -287,12 +309,12 @@ struct PcgHandle {
 };
 
 static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
-                              const void* fn, unsigned grid, unsigned block, void** args) {
+                              const void* fn, unsigned grid, unsigned block, void** args, size_t smem = 0) {
   cudaKernelNodeParams kp{};
   kp.func = const_cast<void*>(fn);
   kp.gridDim = dim3(grid);
   kp.blockDim = dim3(block);
-  kp.sharedMemBytes = 0;
+  kp.sharedMemBytes = (unsigned)smem;
   kp.kernelParams = args;
   kp.extra = nullptr;
   return cudaGraphAddKernelNode(node, g, deps, ndeps, &kp);
@@ -353,6 +375,28 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
         sms > 0 && per_sm > 0)
       grid_rows = std::min<unsigned>(grid_rows, (unsigned)(sms * per_sm));
   }
+  // the FP32 loop of a single block set with a tile plan runs the tiled
+  // SpMV (persistent CTAs, shared-memory stages)
+  bool tiled = false;
+  size_t tile_smem = 0;
+  unsigned grid_tiles = 0;
+  if (P.fp32 && P.nsets == 1 && a.matrix.row_block[0] && a.matrix.tile_cap[0] > 0) {
+    tile_smem = ys::tile_smem_bytes(a.matrix.tile_cap[0]);
+    int dev = 0, sms = 0, per_sm = 0;
+    if (tile_smem <= 200u * 1024u && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaFuncSetAttribute(ys::pcg_spmv_dot_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ys::pcg_spmv_dot_tiled, ys::kPcgBlock, tile_smem) ==
+            cudaSuccess &&
+        sms > 0 && per_sm > 0) {
+      const unsigned ntiles = (P.nv + ys::kTileRows - 1) / ys::kTileRows;
+      grid_tiles = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
+      tiled = true;
+      P.tiled = ys::TiledSet{a.matrix.values32[0], a.matrix.row_ptr[0], a.matrix.entry_block[0],
+                             a.matrix.entry_col[0], a.matrix.row_block[0], P.nv, a.matrix.tile_cap[0]};
+    }
+  }
   P.partials = w; w += (uint64_t)ys::kRowLanes * (grid + 2);
   P.tickets = reinterpret_cast<unsigned*>(w);
   P.jinv = a.jacobi_inverse;
@@ -400,7 +444,13 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       cudaGraph_t body = cp.conditional.phGraph_out[0];
       cudaGraphNode_t n1 = nullptr, n2 = nullptr, n3 = nullptr;
       void* args1[] = {&P};
-      e = ys::add_kernel(body, &n1, nullptr, 0, P.fp32 ? (const void*)ys::pcg_spmv_dot<true> : (const void*)ys::pcg_spmv_dot<false>, grid_rows, ys::kPcgBlock, args1);
+      if (tiled)
+        e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot_tiled, grid_tiles, ys::kPcgBlock,
+                           args1, tile_smem);
+      else
+        e = ys::add_kernel(body, &n1, nullptr, 0,
+                           P.fp32 ? (const void*)ys::pcg_spmv_dot<true> : (const void*)ys::pcg_spmv_dot<false>,
+                           grid_rows, ys::kPcgBlock, args1);
       if (e == cudaSuccess) {
         if (a.preconditioner == YS_PREC_BLOCK_JACOBI) {
           e = ys::add_kernel(body, &n2, &n1, 1, (const void*)ys::pcg_update_bj, grid, ys::kPcgBlock, args1);

@@ -2,6 +2,7 @@
 #include <cub/cub.cuh>
 
 #include "ys_spmv.cuh"
+#include "ys_spmv_tiled.cuh"
 
 namespace ys {
 
@@ -76,6 +77,71 @@ __global__ void pack_x32_kernel(const double* __restrict__ x, uint32_t nv, float
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   x32[i] = make_float4((float)x[3ull * i], (float)x[3ull * i + 1], (float)x[3ull * i + 2], 0.0f);
+}
+
+// row_block[i] = first stored block whose scalar row offset is >= 3 i
+// (i = 0 .. nv): a binary search over the (row, col)-sorted positions.
+__global__ void tile_row_block_kernel(const uint32_t* __restrict__ pos, uint32_t nu, uint32_t nv,
+                                      uint32_t* __restrict__ row_block) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nv) return;
+  const uint64_t key = 3ull * i;
+  uint32_t lo = 0, hi = nu;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if ((uint64_t)pos[2ull * mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  row_block[i] = lo;
+}
+
+// Checks that row i's direct plan entries are the blocks row_block[i] ..
+// row_block[i+1] - 1 in order after its transposed entries, and records the
+// largest tile (scratch[0]: mismatch flag, scratch[1]: tile capacity).
+__global__ void tile_check_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ eblock,
+                                  const uint32_t* __restrict__ row_block, uint32_t nv,
+                                  uint32_t* __restrict__ scratch) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const uint32_t e0 = row_ptr[i], e1 = row_ptr[i + 1];
+  const uint32_t ub = row_block[i], nd = row_block[i + 1] - ub;
+  if (row_block[i + 1] < ub || nd > e1 - e0) {
+    atomicOr(scratch, 1u);
+    return;
+  }
+  const uint32_t nt = (e1 - e0) - nd;
+  for (uint32_t k = 0; k < e1 - e0; ++k) {
+    const uint32_t eb = eblock[e0 + k];
+    const bool ok = k < nt ? (eb & 0x80000000u) != 0 : eb == ub + (k - nt);
+    if (!ok) {
+      atomicOr(scratch, 1u);
+      return;
+    }
+  }
+  if (i % kTileRows == 0) {
+    const uint32_t r1 = min(i + kTileRows, nv);
+    atomicMax(scratch + 1, row_block[r1] - ub);
+  }
+}
+
+// No tile_stage_status given: the flag goes to this word.
+__device__ unsigned g_tile_stage_status;
+
+__global__ void __launch_bounds__(kTileThreads) spmv3_x32_tiled_kernel(TiledSet T, const float4* __restrict__ x32,
+                                                                      double* __restrict__ y, int beta,
+                                                                      unsigned* status) {
+  unsigned* err = status ? status : &g_tile_stage_status;
+  spmv3_tiles_x32(T, x32, err, [&](uint32_t i, bool valid, int lane, double y0, double y1, double y2) {
+    if (!valid || lane != 0) return;
+    if (beta) {
+      y0 += y[3ull * i];
+      y1 += y[3ull * i + 1];
+      y2 += y[3ull * i + 2];
+    }
+    y[3ull * i] = y0;
+    y[3ull * i + 1] = y1;
+    y[3ull * i + 2] = y2;
+  });
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -175,6 +241,59 @@ int32_t ys_spmv3_x32(const float* values32, const uint32_t* row_ptr, const uint3
   ys::SpmvSet set{nullptr, values32, row_ptr, entry_block, entry_col};
   ys::spmv3_x32_kernel<<<ys::grid_for((uint64_t)num_vars * ys::kRowLanes, 256), 256, 0, (cudaStream_t)stream>>>(
       set, num_vars, reinterpret_cast<const float4*>(x32), y, beta);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int32_t ys_spmv_tile_plan(const uint32_t* positions, uint32_t nu, const uint32_t* row_ptr,
+                          const uint32_t* entry_block, uint32_t num_vars, uint32_t* row_block,
+                          uint32_t* tile_cap_host, void* stream) {
+  YS_REQUIRE(row_block && tile_cap_host, YS_ERR_INVALID, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  *tile_cap_host = 0;
+  uint32_t* scratch = row_block + num_vars + 1;
+  YS_CUDA_TRY(cudaMemsetAsync(scratch, 0, 2 * sizeof(uint32_t), s));
+  ys::tile_row_block_kernel<<<ys::grid_for(num_vars + 1ull, 256), 256, 0, s>>>(positions, nu, num_vars, row_block);
+  YS_CHECK_LAUNCH();
+  if (num_vars) {
+    ys::tile_check_kernel<<<ys::grid_for(num_vars, 256), 256, 0, s>>>(row_ptr, entry_block, row_block, num_vars,
+                                                                      scratch);
+    YS_CHECK_LAUNCH();
+  }
+  uint32_t h[2] = {0, 0};
+  YS_CUDA_TRY(cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, s));
+  YS_CUDA_TRY(cudaStreamSynchronize(s));
+  YS_REQUIRE(h[0] == 0, YS_ERR_INVALID, "blocks are not (row, col)-sorted along the row plan");
+  *tile_cap_host = h[1];
+  return YS_OK;
+}
+
+int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr, const uint32_t* entry_block,
+                           const uint32_t* entry_col, const uint32_t* row_block, uint32_t tile_cap,
+                           uint32_t num_vars, const float* x32, double* y, int32_t beta, uint32_t* stage_status,
+                           void* stream) {
+  YS_REQUIRE(values32 && x32 && row_block && tile_cap > 0, YS_ERR_INVALID, "null argument or no tile plan");
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(x32) & 15) == 0 && (reinterpret_cast<uintptr_t>(values32) & 15) == 0,
+             YS_ERR_INVALID, "values32 and x32 must be 16-byte aligned");
+  if (num_vars == 0) return YS_OK;
+  const size_t smem = ys::tile_smem_bytes(tile_cap);
+  YS_REQUIRE(smem <= 200u * 1024u, YS_ERR_CAPACITY, "a tile's blocks exceed the shared-memory stage");
+  YS_CUDA_TRY(cudaFuncSetAttribute(ys::spmv3_x32_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  YS_CUDA_TRY(cudaGetDevice(&dev));
+  YS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  YS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ys::spmv3_x32_tiled_kernel, ys::kTileThreads,
+                                                            smem));
+  YS_REQUIRE(per_sm > 0, YS_ERR_CAPACITY, "tiled SpMV does not fit on an SM");
+  const uint32_t ntiles = (num_vars + ys::kTileRows - 1) / ys::kTileRows;
+  const unsigned grid = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
+  ys::TiledSet T{values32, row_ptr, entry_block, entry_col, row_block, num_vars, tile_cap};
+  ys::spmv3_x32_tiled_kernel<<<grid, ys::kTileThreads, smem, (cudaStream_t)stream>>>(
+      T, reinterpret_cast<const float4*>(x32), y, beta, stage_status);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

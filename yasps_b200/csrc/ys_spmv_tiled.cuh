@@ -1,0 +1,238 @@
+// Tiled symmetric 3x3-block SpMV with FP32 blocks staged in shared memory by
+// bulk copies (cp.async.bulk + mbarrier, double-buffered, persistent CTAs).
+//
+// In the reference's storage every off-diagonal block is stored once (upper)
+// and used twice: by its row (B x_c) and, transposed, by its column
+// (B^T x_r).  The stored blocks are sorted by (row, col), so the blocks whose
+// row lies in a tile of kTileRows consecutive rows form one contiguous range
+// [row_block[r0], row_block[r1]) of the value array.  One bulk copy moves that
+// range into shared memory; every row of the tile then reads its direct
+// blocks and the transposed blocks of rows inside the tile from shared
+// memory, and only the transposed blocks of earlier tiles from global memory
+// (recent, so mostly L2 hits).  A tile's blocks therefore cross HBM once per
+// SpMV instead of once per use, and the scattered 16-byte gathers of the row
+// plan become shared-memory loads.
+//
+// The arithmetic is that of spmv3_group_accumulate (ys_spmv.cuh): kRowLanes
+// lanes a row, lane l takes entries l, l + 8, ... of the row plan in order,
+// the same fused multiply-add chains and the same shuffle tree, so the
+// result is bit-identical to ys_spmv3_x32.
+#pragma once
+
+#include "ys_spmv.cuh"
+
+namespace ys {
+
+constexpr uint32_t kTileRows = YS_SPMV_TILE_ROWS;
+constexpr int kTileThreads = 256;
+constexpr uint32_t kTileSlotBytes = 4 * kFp32BlockStride;  // one FP32 block slot (48 B)
+// try_wait polls before a CTA stops using shared memory (the copies are a
+// few tens of KB and land within microseconds; the bound only keeps a stuck
+// copy from hanging the device)
+constexpr uint32_t kTileWaitPolls = 1u << 22;
+
+struct TiledSet {
+  const float* values32;       // 12-float slots, (row, col)-sorted upper blocks
+  const uint32_t* row_ptr;     // row plan (ys_spmv_plan_build)
+  const uint32_t* entry_block;
+  const uint32_t* entry_col;
+  const uint32_t* row_block;   // [nv + 1] first stored block of each row
+  uint32_t nv;
+  uint32_t tile_cap;           // most blocks in one tile (shared buffer size)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for the phase of the given parity.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t k = 0; k < kTileWaitPolls; ++k)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Order this CTA's earlier generic-proxy reads of shared memory before a bulk
+// copy (async proxy) overwrites it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned) completing on `bar`.  No multicast: the source is this
+// GPU's own memory and only this CTA reads the copy.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void load_slot(const float* __restrict__ p, float (&b)[9]) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+  const float4 v0 = q[0], v1 = q[1], v2 = q[2];
+  b[0] = v0.x; b[1] = v0.y; b[2] = v0.z; b[3] = v0.w;
+  b[4] = v1.x; b[5] = v1.y; b[6] = v1.z; b[7] = v1.w;
+  b[8] = v2.x;
+}
+
+// Block b of the set: from the staged copy of the tile's range [b0, ...) when
+// `staged` and b >= b0, else from global memory.
+__device__ __forceinline__ void tile_block(const TiledSet& T, const float* stage, bool staged, uint32_t b0,
+                                           uint32_t b, float (&v)[9]) {
+  if (staged && b >= b0) load_slot(stage + (uint64_t)kFp32BlockStride * (b - b0), v);
+  else load_block(T.values32, b, v);
+}
+
+// One row of the tile by kRowLanes lanes (see spmv3_group_accumulate); every
+// lane of the warp calls it, rows beyond the matrix with valid == false.
+__device__ __forceinline__ void tile_row(const TiledSet& T, const float4* __restrict__ x32, const float* stage,
+                                         bool staged, uint32_t b0, uint32_t i, bool valid, int lane, double& y0,
+                                         double& y1, double& y2) {
+  uint32_t e0 = 0, e1 = 0, ub = 0, nt = 0;
+  if (valid) {
+    e0 = __ldg(T.row_ptr + i);
+    e1 = __ldg(T.row_ptr + i + 1);
+    ub = __ldg(T.row_block + i);
+    nt = (e1 - e0) - (__ldg(T.row_block + i + 1) - ub);  // transposed entries come first
+  }
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  for (uint32_t e = e0 + lane; e < e1; e += 2 * kRowLanes) {
+    const uint32_t f = e + kRowLanes;
+    const bool two = f < e1;
+    const uint32_t kA = e - e0, kB = two ? f - e0 : kA;
+    const bool tA = kA < nt, tB = kB < nt;
+    const uint32_t jA = __ldg(T.entry_col + e), jB = two ? __ldg(T.entry_col + f) : jA;
+    const uint32_t bA = tA ? (__ldg(T.entry_block + e) & 0x7fffffffu) : ub + (kA - nt);
+    const uint32_t bB = tB ? (__ldg(T.entry_block + e0 + kB) & 0x7fffffffu) : ub + (kB - nt);
+    float xa[3], xb[3], ba[9], bb[9];
+    load_x(x32, jA, xa);
+    load_x(x32, jB, xb);
+    tile_block(T, stage, staged, b0, bA, ba);
+    tile_block(T, stage, staged, b0, bB, bb);
+    const float wB = two ? 1.f : 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) xb[k] *= wB;
+    block_mac(ba, xa, tA, a0, a1, a2);
+    block_mac(bb, xb, tB, a0, a1, a2);
+  }
+#pragma unroll
+  for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o, kRowLanes);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o, kRowLanes);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o, kRowLanes);
+  }
+  y0 = (double)a0;
+  y1 = (double)a1;
+  y2 = (double)a2;
+}
+
+// Shared memory of a tiled launch: two stage buffers of tile_cap slots.
+inline size_t tile_smem_bytes(uint32_t tile_cap) { return 2ull * tile_cap * kTileSlotBytes; }
+
+// Runs every tile t = blockIdx.x + k gridDim.x of the set through the
+// double-buffered stage; out(i, valid, lane, y0, y1, y2) receives each row
+// (all lanes call it, lane 0 of a row group owns the result).  A bulk-copy
+// wait that runs out sets *err and the CTA reads global memory from then on
+// (same values, so the result stays exact).
+template <class Out>
+__device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4* __restrict__ x32,
+                                                unsigned* err, Out&& out) {
+  extern __shared__ float4 tile_stage4[];
+  float* stage_base = reinterpret_cast<float*>(tile_stage4);
+  __shared__ uint64_t bars[2];
+  __shared__ int dead;
+  const uint32_t ntiles = (T.nv + kTileRows - 1) / kTileRows;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+    dead = 0;
+  }
+  __syncthreads();
+  uint32_t issued[2] = {0u, 0u};  // phases issued per buffer (thread 0)
+  // thread 0: stage tile `t` into buffer `buf` (a plain arrive completes the
+  // phase when the tile is empty or larger than the buffer)
+  auto issue = [&](uint32_t t, int buf) {
+    const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
+    const uint32_t b0 = __ldg(T.row_block + r0), b1 = __ldg(T.row_block + r1);
+    const uint32_t nb = b1 - b0;
+    if (nb > 0 && nb <= T.tile_cap) {
+      mbar_arrive_expect_tx(&bars[buf], nb * kTileSlotBytes);
+      bulk_copy_g2s(stage_base + (uint64_t)buf * T.tile_cap * kFp32BlockStride,
+                    T.values32 + (uint64_t)kFp32BlockStride * b0, nb * kTileSlotBytes, &bars[buf]);
+    } else {
+      mbar_arrive(&bars[buf]);
+    }
+    ++issued[buf];
+  };
+  if (threadIdx.x == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  uint32_t k = 0;
+  constexpr uint32_t kPasses = kTileRows / (kTileThreads / kRowLanes);
+  const int lane = (int)(threadIdx.x % kRowLanes);
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+    const int buf = (int)(k & 1);
+    const uint32_t next = t + gridDim.x;
+    if (threadIdx.x == 0 && next < ntiles && !dead) {
+      fence_proxy_async_smem();
+      issue(next, buf ^ 1);
+    }
+    const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
+    const uint32_t b0 = __ldg(T.row_block + r0), nb = __ldg(T.row_block + r1) - b0;
+    bool staged = nb > 0 && nb <= T.tile_cap && !dead;
+    // the k-th tile is the (k >> 1)-th phase of its buffer
+    if (staged && !mbar_wait_bounded(&bars[buf], (k >> 1) & 1u)) {
+      staged = false;
+      dead = 1;  // no further copies into this CTA's buffers
+      atomicOr(err, 1u);
+    }
+    const float* stage = stage_base + (uint64_t)buf * T.tile_cap * kFp32BlockStride;
+#pragma unroll 1
+    for (uint32_t pass = 0; pass < kPasses; ++pass) {
+      const uint32_t i = r0 + pass * (kTileThreads / kRowLanes) + threadIdx.x / kRowLanes;
+      double y0, y1, y2;
+      tile_row(T, x32, stage, staged, b0, i, i < r1, lane, y0, y1, y2);
+      out(i, i < r1, lane, y0, y1, y2);
+    }
+    __syncthreads();
+  }
+  // a CTA that stopped staging waits (bounded) for the last copy it issued
+  // into each buffer before its shared memory goes away
+  if (dead && threadIdx.x == 0) {
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+      if (issued[b]) mbar_wait_bounded(&bars[b], (issued[b] - 1) & 1u);
+  }
+}
+
+}  // namespace ys

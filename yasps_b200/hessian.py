@@ -411,6 +411,7 @@ class _BlockSet:
     self.records = None
     self.infos = []
     self.spmv = None  # (row_ptr, entry_block, entry_col)
+    self.tiles = None  # (row_block, tile capacity) of the tiled SpMV, or (None, 0)
 
 
 class hessian:
@@ -728,7 +729,23 @@ class hessian:
     L.call("ys_spmv_plan_build", L.ptr(p.positions), p.num_unique, nv, L.ptr(work), int(ws.value), L.ptr(row_ptr),
            L.ptr(eb), L.ptr(ec), L.stream_ptr())
     bs.spmv = (row_ptr, eb, ec)
+    bs.tiles = None
     return bs.spmv
+
+  def tile_plan(self, bs: _BlockSet):
+    """``(row_block, tile capacity)`` of the tiled SpMV for a 3x3 block set
+    (``ys_spmv_tile_plan``); ``(None, 0)`` when the set has none."""
+    import ctypes
+    torch = _torch()
+    row_ptr, eb, _ = self.spmv_plan(bs)
+    if bs.tiles is None:
+      nv = self.rows // 3
+      row_block = torch.empty(nv + 3, dtype=torch.int32, device=_dev())
+      cap = L.u32(0)
+      rc = L.call("ys_spmv_tile_plan", L.ptr(bs.pattern.positions), bs.pattern.num_unique, L.ptr(row_ptr), L.ptr(eb),
+                  nv, L.ptr(row_block), ctypes.byref(cap), L.stream_ptr(), ok=(L.YS_OK, L.YS_ERR_INVALID))
+      bs.tiles = (row_block, int(cap.value)) if rc == L.YS_OK else (None, 0)
+    return bs.tiles
 
   def spmv(self, direction: vector, transpose: bool = False, fp32: bool = False) -> vector:
     """``H x`` (symmetric, so ``transpose`` gives the same product)."""
@@ -752,5 +769,7 @@ class hessian:
       m.values[k] = L.ptr(bs.values)
       m.values32[k] = L.ptr(bs.values32) if bs.values32 is not None else None
       m.row_ptr[k], m.entry_block[k], m.entry_col[k] = L.ptr(row_ptr), L.ptr(eb), L.ptr(ec)
+      row_block, cap = self.tile_plan(bs)
+      m.row_block[k], m.tile_cap[k] = L.ptr(row_block), cap
     m.num_vars = self.rows // 3
     return m
