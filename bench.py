@@ -322,7 +322,7 @@ def spmv_roofline(H, hbm, peak_kind, reps=50):
   bs = H.block_sets[0]
   row_ptr, eb, ec = H.spmv_plan(bs)
   nv = H.rows // 3
-  entries = int(row_ptr[-1].item())
+  entries = int(row_ptr[nv].item())
   x = torch.cos(torch.arange(H.rows, dtype=torch.float64, device="cuda") * 0.37)
   x32 = torch.empty(4 * nv, dtype=torch.float32, device="cuda")
   y = torch.empty_like(x)

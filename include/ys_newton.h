@@ -429,31 +429,36 @@ int32_t ys_spmv3_x32(const float* values32, const uint32_t* row_ptr, const uint3
 
 /* Tile plan of a 3x3 block set for the tiled SpMV: rows in tiles of
  * YS_SPMV_TILE_ROWS, row_block[i] = first stored block of row i (the blocks
- * are (row, col)-sorted, so a tile's blocks are one contiguous range), and
- * *tile_cap_host = the most blocks in one tile.  row_block has num_vars + 3
- * entries (the last two are scratch).  Synchronises `stream` (set-up, once
- * per pattern).  YS_ERR_INVALID when the blocks are not (row, col)-sorted or
- * do not match the row plan.  No counterpart in the reference.            */
+ * are (row, col)-sorted, so a tile's blocks are one contiguous range),
+ * *tile_cap_host = the most blocks in one tile and *entry_cap_host = the
+ * most row-plan entries in one tile's 16-byte aligned entry range (a
+ * multiple of 4).  row_block has num_vars + 4 entries (the last three are
+ * scratch here).  Synchronises `stream` (set-up, once per pattern).
+ * YS_ERR_INVALID when the blocks are not (row, col)-sorted or do not match
+ * the row plan.  No counterpart in the reference.                         */
 #define YS_SPMV_TILE_ROWS 64
 int32_t ys_spmv_tile_plan(const uint32_t* positions, uint32_t nu, const uint32_t* row_ptr,
                           const uint32_t* entry_block, uint32_t num_vars, uint32_t* row_block,
-                          uint32_t* tile_cap_host, void* stream);
+                          uint32_t* tile_cap_host, uint32_t* entry_cap_host, void* stream);
 
 /* ys_spmv3_x32 by tiles: persistent CTAs stage each tile's contiguous run of
- * FP32 block slots into shared memory with a bulk copy (cp.async.bulk,
- * mbarrier completion, double-buffered), so every stored block crosses HBM
- * once per product; direct blocks and the transposed blocks of rows in the
- * tile are read from shared memory, the transposed blocks of earlier tiles
- * from global memory.  Bit-identical to ys_spmv3_x32.  `stage_status`
- * (device word or NULL) is OR-ed with 1 when a CTA's wait for a copy ran
- * out (it then reads global memory: the result is the same).  Replaces the
- * reference's `yasps_mas_specialized_fine_block_spmv`
+ * FP32 block slots, its row-plan entries and its row pointers into shared
+ * memory with bulk copies (cp.async.bulk, mbarrier completion,
+ * double-buffered), so every stored block crosses HBM once per product;
+ * direct blocks and the transposed blocks of rows in the tile are read from
+ * shared memory, the transposed blocks of earlier tiles from global memory.
+ * Bit-identical to ys_spmv3_x32.  Padding: row_ptr and row_block hold
+ * num_vars + 4 entries, entry_block and entry_col (row_ptr[num_vars] + 3)
+ * & ~3 (the copies move whole 16-byte words).  `stage_status` (device word
+ * or NULL) is OR-ed with 1 when a CTA's wait for a copy ran out (it then
+ * reads global memory: the result is the same).  Replaces the reference's
+ * `yasps_mas_specialized_fine_block_spmv`
  * (PKG/solver/mas/cuda/block_spmv.cu:279-398).                            */
 int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr,
                            const uint32_t* entry_block, const uint32_t* entry_col,
-                           const uint32_t* row_block, uint32_t tile_cap, uint32_t num_vars,
-                           const float* x32, double* y, int32_t beta, uint32_t* stage_status,
-                           void* stream);
+                           const uint32_t* row_block, uint32_t tile_cap, uint32_t entry_cap,
+                           uint32_t num_vars, const float* x32, double* y, int32_t beta,
+                           uint32_t* stage_status, void* stream);
 
 /* ---- preconditioned CG ----------------------------------------------------- */
 
@@ -474,9 +479,10 @@ typedef struct ys_matrix3 {
   uint32_t num_vars;             /* 3-DoF variables; n = 3 * num_vars             */
   /* optional tile plan of each set (ys_spmv_tile_plan); tile_cap 0: none.
    * With one set, FP32 blocks and a tile plan the PCG loop runs the tiled
-   * SpMV (ys_spmv3_x32_tiled).                                            */
+   * SpMV (ys_spmv3_x32_tiled; its padding rules apply).                   */
   const uint32_t* row_block[2];
   uint32_t tile_cap[2];
+  uint32_t entry_cap[2];
 } ys_matrix3;
 
 typedef struct ys_pcg_args {

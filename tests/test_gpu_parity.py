@@ -121,18 +121,21 @@ def check_tiled_spmv(H, x32, expected):
   nv = H.rows // 3
   (bs,) = H.block_sets
   row_ptr, eb, ec = H.spmv_plan(bs)
-  row_block, cap = H.tile_plan(bs)
-  assert cap > 0
+  row_block, cap, ecap = H.tile_plan(bs)
+  assert cap > 0 and ecap > 0 and ecap % 4 == 0
   rb = row_block.cpu().numpy().astype(np.int64)[:nv + 1]
   pos = bs.pattern.positions[:2 * bs.pattern.num_unique].cpu().numpy().astype(np.int64).reshape(-1, 2)
   assert np.array_equal(rb, np.searchsorted(pos[:, 0], 3 * np.arange(nv + 1), side="left"))
   tiles = np.arange(0, nv, L.YS_SPMV_TILE_ROWS)
-  assert cap == int((rb[np.minimum(tiles + L.YS_SPMV_TILE_ROWS, nv)] - rb[tiles]).max())
+  ends = np.minimum(tiles + L.YS_SPMV_TILE_ROWS, nv)
+  assert cap == int((rb[ends] - rb[tiles]).max())
+  rp = row_ptr.cpu().numpy().astype(np.int64)[:nv + 1]
+  assert ecap == int((((rp[ends] + 3) & ~3) - (rp[tiles] & ~3)).max())
   status = torch.zeros(1, dtype=torch.int32, device="cuda")
   y = torch.full((H.rows,), np.nan, dtype=torch.float64, device="cuda")
   for _ in range(2):
-    L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block), cap, nv,
-           L.ptr(x32), L.ptr(y), 0, L.ptr(status), L.stream_ptr())
+    L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block), cap,
+           ecap, nv, L.ptr(x32), L.ptr(y), 0, L.ptr(status), L.stream_ptr())
     assert np.array_equal(y.cpu().numpy(), expected)
   assert int(status.item()) == 0
 

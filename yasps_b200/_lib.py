@@ -88,7 +88,7 @@ class CoupledArgs(C.Structure):
 class Matrix3(C.Structure):
   _fields_ = [("num_sets", u32), ("values", vp * 2), ("values32", vp * 2), ("row_ptr", vp * 2),
               ("entry_block", vp * 2), ("entry_col", vp * 2), ("num_vars", u32), ("row_block", vp * 2),
-              ("tile_cap", u32 * 2)]
+              ("tile_cap", u32 * 2), ("entry_cap", u32 * 2)]
 
 
 class PcgArgs(C.Structure):
@@ -151,8 +151,8 @@ SIGNATURES = {
     "ys_mas_failed_domains": (i32, [vp, vp, P(i32)]),
     "ys_pack_x32": (i32, [vp, u32, vp, vp]),
     "ys_spmv3_x32": (i32, [vp, vp, vp, vp, u32, vp, vp, i32, vp]),
-    "ys_spmv_tile_plan": (i32, [vp, u32, vp, vp, u32, vp, P(u32), vp]),
-    "ys_spmv3_x32_tiled": (i32, [vp, vp, vp, vp, vp, u32, u32, vp, vp, i32, vp, vp]),
+    "ys_spmv_tile_plan": (i32, [vp, u32, vp, vp, u32, vp, P(u32), P(u32), vp]),
+    "ys_spmv3_x32_tiled": (i32, [vp, vp, vp, vp, vp, u32, u32, u32, vp, vp, i32, vp, vp]),
     "ys_pcg_workspace_doubles": (u64, [u32]),
     "ys_pcg_create": (i32, [P(PcgArgs), P(vp)]),
     "ys_pcg_run": (i32, [vp, vp, P(PcgResult)]),

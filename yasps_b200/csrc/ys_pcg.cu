@@ -380,8 +380,8 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   bool tiled = false;
   size_t tile_smem = 0;
   unsigned grid_tiles = 0;
-  if (P.fp32 && P.nsets == 1 && a.matrix.row_block[0] && a.matrix.tile_cap[0] > 0) {
-    tile_smem = ys::tile_smem_bytes(a.matrix.tile_cap[0]);
+  if (P.fp32 && P.nsets == 1 && a.matrix.row_block[0] && a.matrix.tile_cap[0] > 0 && a.matrix.entry_cap[0] > 0) {
+    tile_smem = ys::tile_smem_bytes(a.matrix.tile_cap[0], a.matrix.entry_cap[0]);
     int dev = 0, sms = 0, per_sm = 0;
     if (tile_smem <= 200u * 1024u && cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
@@ -394,7 +394,8 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       grid_tiles = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
       tiled = true;
       P.tiled = ys::TiledSet{a.matrix.values32[0], a.matrix.row_ptr[0], a.matrix.entry_block[0],
-                             a.matrix.entry_col[0], a.matrix.row_block[0], P.nv, a.matrix.tile_cap[0]};
+                             a.matrix.entry_col[0], a.matrix.row_block[0], P.nv, a.matrix.tile_cap[0],
+                             a.matrix.entry_cap[0]};
     }
   }
   P.partials = w; w += (uint64_t)ys::kRowLanes * (grid + 2);

@@ -97,7 +97,8 @@ __global__ void tile_row_block_kernel(const uint32_t* __restrict__ pos, uint32_t
 
 // Checks that row i's direct plan entries are the blocks row_block[i] ..
 // row_block[i+1] - 1 in order after its transposed entries, and records the
-// largest tile (scratch[0]: mismatch flag, scratch[1]: tile capacity).
+// largest tile (scratch[0]: mismatch flag, scratch[1]: most blocks of a tile,
+// scratch[2]: most plan entries of a tile's 16-byte aligned entry range).
 __global__ void tile_check_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ eblock,
                                   const uint32_t* __restrict__ row_block, uint32_t nv,
                                   uint32_t* __restrict__ scratch) {
@@ -121,6 +122,7 @@ __global__ void tile_check_kernel(const uint32_t* __restrict__ row_ptr, const ui
   if (i % kTileRows == 0) {
     const uint32_t r1 = min(i + kTileRows, nv);
     atomicMax(scratch + 1, row_block[r1] - ub);
+    atomicMax(scratch + 2, ((row_ptr[r1] + 3u) & ~3u) - (e0 & ~3u));
   }
 }
 
@@ -251,12 +253,13 @@ extern "C" {
 
 int32_t ys_spmv_tile_plan(const uint32_t* positions, uint32_t nu, const uint32_t* row_ptr,
                           const uint32_t* entry_block, uint32_t num_vars, uint32_t* row_block,
-                          uint32_t* tile_cap_host, void* stream) {
-  YS_REQUIRE(row_block && tile_cap_host, YS_ERR_INVALID, "null argument");
+                          uint32_t* tile_cap_host, uint32_t* entry_cap_host, void* stream) {
+  YS_REQUIRE(row_block && tile_cap_host && entry_cap_host, YS_ERR_INVALID, "null argument");
   cudaStream_t s = (cudaStream_t)stream;
   *tile_cap_host = 0;
+  *entry_cap_host = 0;
   uint32_t* scratch = row_block + num_vars + 1;
-  YS_CUDA_TRY(cudaMemsetAsync(scratch, 0, 2 * sizeof(uint32_t), s));
+  YS_CUDA_TRY(cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), s));
   ys::tile_row_block_kernel<<<ys::grid_for(num_vars + 1ull, 256), 256, 0, s>>>(positions, nu, num_vars, row_block);
   YS_CHECK_LAUNCH();
   if (num_vars) {
@@ -264,23 +267,25 @@ int32_t ys_spmv_tile_plan(const uint32_t* positions, uint32_t nu, const uint32_t
                                                                       scratch);
     YS_CHECK_LAUNCH();
   }
-  uint32_t h[2] = {0, 0};
+  uint32_t h[3] = {0, 0, 0};
   YS_CUDA_TRY(cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, s));
   YS_CUDA_TRY(cudaStreamSynchronize(s));
   YS_REQUIRE(h[0] == 0, YS_ERR_INVALID, "blocks are not (row, col)-sorted along the row plan");
   *tile_cap_host = h[1];
+  *entry_cap_host = h[2];
   return YS_OK;
 }
 
 int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr, const uint32_t* entry_block,
                            const uint32_t* entry_col, const uint32_t* row_block, uint32_t tile_cap,
-                           uint32_t num_vars, const float* x32, double* y, int32_t beta, uint32_t* stage_status,
-                           void* stream) {
-  YS_REQUIRE(values32 && x32 && row_block && tile_cap > 0, YS_ERR_INVALID, "null argument or no tile plan");
+                           uint32_t entry_cap, uint32_t num_vars, const float* x32, double* y, int32_t beta,
+                           uint32_t* stage_status, void* stream) {
+  YS_REQUIRE(values32 && x32 && row_block && tile_cap > 0 && entry_cap > 0 && (entry_cap & 3u) == 0,
+             YS_ERR_INVALID, "null argument or no tile plan");
   YS_REQUIRE((reinterpret_cast<uintptr_t>(x32) & 15) == 0 && (reinterpret_cast<uintptr_t>(values32) & 15) == 0,
              YS_ERR_INVALID, "values32 and x32 must be 16-byte aligned");
   if (num_vars == 0) return YS_OK;
-  const size_t smem = ys::tile_smem_bytes(tile_cap);
+  const size_t smem = ys::tile_smem_bytes(tile_cap, entry_cap);
   YS_REQUIRE(smem <= 200u * 1024u, YS_ERR_CAPACITY, "a tile's blocks exceed the shared-memory stage");
   YS_CUDA_TRY(cudaFuncSetAttribute(ys::spmv3_x32_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, sms = 0, per_sm = 0;
@@ -291,7 +296,7 @@ int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr, const
   YS_REQUIRE(per_sm > 0, YS_ERR_CAPACITY, "tiled SpMV does not fit on an SM");
   const uint32_t ntiles = (num_vars + ys::kTileRows - 1) / ys::kTileRows;
   const unsigned grid = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
-  ys::TiledSet T{values32, row_ptr, entry_block, entry_col, row_block, num_vars, tile_cap};
+  ys::TiledSet T{values32, row_ptr, entry_block, entry_col, row_block, num_vars, tile_cap, entry_cap};
   ys::spmv3_x32_tiled_kernel<<<grid, ys::kTileThreads, smem, (cudaStream_t)stream>>>(
       T, reinterpret_cast<const float4*>(x32), y, beta, stage_status);
   YS_CHECK_LAUNCH();

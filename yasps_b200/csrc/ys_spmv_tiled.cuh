@@ -33,13 +33,24 @@ constexpr uint32_t kTileWaitPolls = 1u << 22;
 
 struct TiledSet {
   const float* values32;       // 12-float slots, (row, col)-sorted upper blocks
-  const uint32_t* row_ptr;     // row plan (ys_spmv_plan_build)
-  const uint32_t* entry_block;
+  const uint32_t* row_ptr;     // row plan (ys_spmv_plan_build), num_vars + 4 entries
+  const uint32_t* entry_block; // both hold (row_ptr[nv] + 3) & ~3 entries at least
   const uint32_t* entry_col;
-  const uint32_t* row_block;   // [nv + 1] first stored block of each row
+  const uint32_t* row_block;   // [nv + 4] first stored block of each row
   uint32_t nv;
-  uint32_t tile_cap;           // most blocks in one tile (shared buffer size)
+  uint32_t tile_cap;           // most blocks in one tile
+  uint32_t entry_cap;          // most plan entries of one tile, 4-aligned range
 };
+
+// Words of row_ptr / row_block staged per tile: rows r0 .. r0 + kTileRows
+// rounded up to a 16-byte multiple.
+constexpr uint32_t kTileRowWords = (kTileRows + 1 + 3) & ~3u;
+
+// Bytes of one stage buffer: the tile's block slots, its plan entries
+// (columns, then blocks) and its row pointers (row_ptr, then row_block).
+__host__ __device__ inline uint64_t tile_stage_bytes(uint32_t tile_cap, uint32_t entry_cap) {
+  return (uint64_t)tile_cap * kTileSlotBytes + 8ull * entry_cap + 8ull * kTileRowWords;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -106,40 +117,63 @@ __device__ __forceinline__ void load_slot(const float* __restrict__ p, float (&b
   b[8] = v2.x;
 }
 
-// Block b of the set: from the staged copy of the tile's range [b0, ...) when
-// `staged` and b >= b0, else from global memory.
-__device__ __forceinline__ void tile_block(const TiledSet& T, const float* stage, bool staged, uint32_t b0,
-                                           uint32_t b, float (&v)[9]) {
-  if (staged && b >= b0) load_slot(stage + (uint64_t)kFp32BlockStride * (b - b0), v);
-  else load_block(T.values32, b, v);
+// One staged tile: pointers into a stage buffer and the global ranges they
+// hold (blocks [b0, ...), plan entries [e0a, ...), rows [r0, ...]).
+struct TileStage {
+  const float* blocks;
+  const uint32_t* cols;
+  const uint32_t* eblocks;
+  const uint32_t* rptr;
+  const uint32_t* rblock;
+  uint32_t b0, e0a, r0;
+};
+
+__device__ __forceinline__ TileStage stage_view(const TiledSet& T, const float* base, uint32_t r0, uint32_t b0,
+                                                uint32_t e0a) {
+  TileStage S;
+  S.blocks = base;
+  S.cols = reinterpret_cast<const uint32_t*>(base + (uint64_t)kFp32BlockStride * T.tile_cap);
+  S.eblocks = S.cols + T.entry_cap;
+  S.rptr = S.eblocks + T.entry_cap;
+  S.rblock = S.rptr + kTileRowWords;
+  S.b0 = b0;
+  S.e0a = e0a;
+  S.r0 = r0;
+  return S;
 }
 
-// One row of the tile by kRowLanes lanes (see spmv3_group_accumulate); every
-// lane of the warp calls it, rows beyond the matrix with valid == false.
-__device__ __forceinline__ void tile_row(const TiledSet& T, const float4* __restrict__ x32, const float* stage,
-                                         bool staged, uint32_t b0, uint32_t i, bool valid, int lane, double& y0,
-                                         double& y1, double& y2) {
+// One row of a staged tile by kRowLanes lanes (the arithmetic and entry
+// order of spmv3_group_accumulate); every lane of the warp calls it, rows
+// beyond the tile with valid == false.  Only the neighbour vector and the
+// transposed blocks of earlier tiles come from global memory.
+__device__ __forceinline__ void tile_row_staged(const TiledSet& T, const TileStage& S,
+                                                const float4* __restrict__ x32, uint32_t i, bool valid, int lane,
+                                                double& y0, double& y1, double& y2) {
   uint32_t e0 = 0, e1 = 0, ub = 0, nt = 0;
   if (valid) {
-    e0 = __ldg(T.row_ptr + i);
-    e1 = __ldg(T.row_ptr + i + 1);
-    ub = __ldg(T.row_block + i);
-    nt = (e1 - e0) - (__ldg(T.row_block + i + 1) - ub);  // transposed entries come first
+    const uint32_t k = i - S.r0;
+    e0 = S.rptr[k];
+    e1 = S.rptr[k + 1];
+    ub = S.rblock[k];
+    nt = (e1 - e0) - (S.rblock[k + 1] - ub);  // transposed entries come first
   }
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
   for (uint32_t e = e0 + lane; e < e1; e += 2 * kRowLanes) {
     const uint32_t f = e + kRowLanes;
     const bool two = f < e1;
-    const uint32_t kA = e - e0, kB = two ? f - e0 : kA;
+    const uint32_t g = two ? f : e;
+    const uint32_t kA = e - e0, kB = g - e0;
     const bool tA = kA < nt, tB = kB < nt;
-    const uint32_t jA = __ldg(T.entry_col + e), jB = two ? __ldg(T.entry_col + f) : jA;
-    const uint32_t bA = tA ? (__ldg(T.entry_block + e) & 0x7fffffffu) : ub + (kA - nt);
-    const uint32_t bB = tB ? (__ldg(T.entry_block + e0 + kB) & 0x7fffffffu) : ub + (kB - nt);
+    const uint32_t jA = S.cols[e - S.e0a], jB = S.cols[g - S.e0a];
+    const uint32_t bA = tA ? (S.eblocks[e - S.e0a] & 0x7fffffffu) : ub + (kA - nt);
+    const uint32_t bB = tB ? (S.eblocks[g - S.e0a] & 0x7fffffffu) : ub + (kB - nt);
     float xa[3], xb[3], ba[9], bb[9];
     load_x(x32, jA, xa);
     load_x(x32, jB, xb);
-    tile_block(T, stage, staged, b0, bA, ba);
-    tile_block(T, stage, staged, b0, bB, bb);
+    if (bA >= S.b0) load_slot(S.blocks + (uint64_t)kFp32BlockStride * (bA - S.b0), ba);
+    else load_block(T.values32, bA, ba);
+    if (bB >= S.b0) load_slot(S.blocks + (uint64_t)kFp32BlockStride * (bB - S.b0), bb);
+    else load_block(T.values32, bB, bb);
     const float wB = two ? 1.f : 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) xb[k] *= wB;
@@ -157,19 +191,23 @@ __device__ __forceinline__ void tile_row(const TiledSet& T, const float4* __rest
   y2 = (double)a2;
 }
 
-// Shared memory of a tiled launch: two stage buffers of tile_cap slots.
-inline size_t tile_smem_bytes(uint32_t tile_cap) { return 2ull * tile_cap * kTileSlotBytes; }
+// Shared memory of a tiled launch: two stage buffers.
+inline size_t tile_smem_bytes(uint32_t tile_cap, uint32_t entry_cap) {
+  return 2 * tile_stage_bytes(tile_cap, entry_cap);
+}
 
 // Runs every tile t = blockIdx.x + k gridDim.x of the set through the
 // double-buffered stage; out(i, valid, lane, y0, y1, y2) receives each row
 // (all lanes call it, lane 0 of a row group owns the result).  A bulk-copy
 // wait that runs out sets *err and the CTA reads global memory from then on
-// (same values, so the result stays exact).
+// through the row-plan gather (the same values and order: the result stays
+// exact).
 template <class Out>
 __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4* __restrict__ x32,
                                                 unsigned* err, Out&& out) {
   extern __shared__ float4 tile_stage4[];
   float* stage_base = reinterpret_cast<float*>(tile_stage4);
+  const uint64_t buf_floats = tile_stage_bytes(T.tile_cap, T.entry_cap) / 4;
   __shared__ uint64_t bars[2];
   __shared__ int dead;
   const uint32_t ntiles = (T.nv + kTileRows - 1) / kTileRows;
@@ -181,24 +219,31 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
   }
   __syncthreads();
   uint32_t issued[2] = {0u, 0u};  // phases issued per buffer (thread 0)
-  // thread 0: stage tile `t` into buffer `buf` (a plain arrive completes the
-  // phase when the tile is empty or larger than the buffer)
+  // thread 0: stage tile `t` into buffer `buf`: its blocks, its plan entries
+  // (a 16-byte aligned range) and its row pointers, one mbarrier phase
   auto issue = [&](uint32_t t, int buf) {
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
     const uint32_t b0 = __ldg(T.row_block + r0), b1 = __ldg(T.row_block + r1);
-    const uint32_t nb = b1 - b0;
-    if (nb > 0 && nb <= T.tile_cap) {
-      mbar_arrive_expect_tx(&bars[buf], nb * kTileSlotBytes);
-      bulk_copy_g2s(stage_base + (uint64_t)buf * T.tile_cap * kFp32BlockStride,
-                    T.values32 + (uint64_t)kFp32BlockStride * b0, nb * kTileSlotBytes, &bars[buf]);
-    } else {
-      mbar_arrive(&bars[buf]);
+    const uint32_t e0a = __ldg(T.row_ptr + r0) & ~3u, e1a = (__ldg(T.row_ptr + r1) + 3u) & ~3u;
+    // rows r0 .. r1 (inclusive) rounded up to 4 words: at most num_vars + 4
+    const uint32_t vb = (b1 - b0) * kTileSlotBytes, eb = (e1a - e0a) * 4u, rb = ((r1 - r0 + 4u) & ~3u) * 4u;
+    float* dst = stage_base + buf * buf_floats;
+    const TileStage S = stage_view(T, dst, r0, b0, e0a);
+    mbar_arrive_expect_tx(&bars[buf], vb + 2 * eb + 2 * rb);
+    if (vb) bulk_copy_g2s(dst, T.values32 + (uint64_t)kFp32BlockStride * b0, vb, &bars[buf]);
+    if (eb) {
+      bulk_copy_g2s((void*)S.cols, T.entry_col + e0a, eb, &bars[buf]);
+      bulk_copy_g2s((void*)S.eblocks, T.entry_block + e0a, eb, &bars[buf]);
     }
+    bulk_copy_g2s((void*)S.rptr, T.row_ptr + r0, rb, &bars[buf]);
+    bulk_copy_g2s((void*)S.rblock, T.row_block + r0, rb, &bars[buf]);
     ++issued[buf];
   };
   if (threadIdx.x == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
   uint32_t k = 0;
-  constexpr uint32_t kPasses = kTileRows / (kTileThreads / kRowLanes);
+  constexpr uint32_t kRowsPerPass = kTileThreads / kRowLanes;
+  constexpr uint32_t kPasses = kTileRows / kRowsPerPass;
+  static_assert(kPasses == 2, "two rows a thread");
   const int lane = (int)(threadIdx.x % kRowLanes);
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
     const int buf = (int)(k & 1);
@@ -208,22 +253,30 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
       issue(next, buf ^ 1);
     }
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
-    const uint32_t b0 = __ldg(T.row_block + r0), nb = __ldg(T.row_block + r1) - b0;
-    bool staged = nb > 0 && nb <= T.tile_cap && !dead;
+    const uint32_t iA = r0 + threadIdx.x / kRowLanes, iB = iA + kRowsPerPass;
+    double yA[3], yB[3];
     // the k-th tile is the (k >> 1)-th phase of its buffer
+    bool staged = !dead;
     if (staged && !mbar_wait_bounded(&bars[buf], (k >> 1) & 1u)) {
       staged = false;
       dead = 1;  // no further copies into this CTA's buffers
       atomicOr(err, 1u);
     }
-    const float* stage = stage_base + (uint64_t)buf * T.tile_cap * kFp32BlockStride;
-#pragma unroll 1
-    for (uint32_t pass = 0; pass < kPasses; ++pass) {
-      const uint32_t i = r0 + pass * (kTileThreads / kRowLanes) + threadIdx.x / kRowLanes;
-      double y0, y1, y2;
-      tile_row(T, x32, stage, staged, b0, i, i < r1, lane, y0, y1, y2);
-      out(i, i < r1, lane, y0, y1, y2);
+    if (staged) {
+      const float* base = stage_base + buf * buf_floats;
+      const uint32_t* rblk = reinterpret_cast<const uint32_t*>(base + (uint64_t)kFp32BlockStride * T.tile_cap) +
+                             2ull * T.entry_cap + kTileRowWords;
+      const uint32_t* rp = rblk - kTileRowWords;
+      const TileStage S = stage_view(T, base, r0, rblk[0], rp[0] & ~3u);
+      tile_row_staged(T, S, x32, iA, iA < r1, lane, yA[0], yA[1], yA[2]);
+      tile_row_staged(T, S, x32, iB, iB < r1, lane, yB[0], yB[1], yB[2]);
+    } else {
+      SpmvSet g{nullptr, T.values32, T.row_ptr, T.entry_block, T.entry_col};
+      spmv3_group_x32(&g, 1, iA, iA < r1, lane, x32, yA[0], yA[1], yA[2]);
+      spmv3_group_x32(&g, 1, iB, iB < r1, lane, x32, yB[0], yB[1], yB[2]);
     }
+    out(iA, iA < r1, lane, yA[0], yA[1], yA[2]);
+    out(iB, iB < r1, lane, yB[0], yB[1], yB[2]);
     __syncthreads();
   }
   // a CTA that stopped staging waits (bounded) for the last copy it issued

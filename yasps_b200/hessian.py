@@ -723,9 +723,10 @@ class hessian:
     ws = L.u64(0)
     L.call("ys_spmv_plan_workspace_bytes", p.num_unique, nv, ctypes.byref(ws))
     work = torch.empty(int(ws.value), dtype=torch.uint8, device=_dev())
-    row_ptr = torch.empty(nv + 1, dtype=torch.int32, device=_dev())
-    eb = torch.empty(2 * p.num_unique, dtype=torch.int32, device=_dev())
-    ec = torch.empty(2 * p.num_unique, dtype=torch.int32, device=_dev())
+    # padded for the tiled SpMV's 16-byte copies (ys_spmv3_x32_tiled)
+    row_ptr = torch.zeros(nv + 4, dtype=torch.int32, device=_dev())
+    eb = torch.zeros(2 * p.num_unique + 4, dtype=torch.int32, device=_dev())
+    ec = torch.zeros(2 * p.num_unique + 4, dtype=torch.int32, device=_dev())
     L.call("ys_spmv_plan_build", L.ptr(p.positions), p.num_unique, nv, L.ptr(work), int(ws.value), L.ptr(row_ptr),
            L.ptr(eb), L.ptr(ec), L.stream_ptr())
     bs.spmv = (row_ptr, eb, ec)
@@ -733,18 +734,20 @@ class hessian:
     return bs.spmv
 
   def tile_plan(self, bs: _BlockSet):
-    """``(row_block, tile capacity)`` of the tiled SpMV for a 3x3 block set
-    (``ys_spmv_tile_plan``); ``(None, 0)`` when the set has none."""
+    """``(row_block, tile block capacity, tile entry capacity)`` of the tiled
+    SpMV for a 3x3 block set (``ys_spmv_tile_plan``); ``(None, 0, 0)`` when
+    the set has none."""
     import ctypes
     torch = _torch()
     row_ptr, eb, _ = self.spmv_plan(bs)
     if bs.tiles is None:
       nv = self.rows // 3
-      row_block = torch.empty(nv + 3, dtype=torch.int32, device=_dev())
-      cap = L.u32(0)
+      row_block = torch.zeros(nv + 4, dtype=torch.int32, device=_dev())
+      cap, ecap = L.u32(0), L.u32(0)
       rc = L.call("ys_spmv_tile_plan", L.ptr(bs.pattern.positions), bs.pattern.num_unique, L.ptr(row_ptr), L.ptr(eb),
-                  nv, L.ptr(row_block), ctypes.byref(cap), L.stream_ptr(), ok=(L.YS_OK, L.YS_ERR_INVALID))
-      bs.tiles = (row_block, int(cap.value)) if rc == L.YS_OK else (None, 0)
+                  nv, L.ptr(row_block), ctypes.byref(cap), ctypes.byref(ecap), L.stream_ptr(),
+                  ok=(L.YS_OK, L.YS_ERR_INVALID))
+      bs.tiles = (row_block, int(cap.value), int(ecap.value)) if rc == L.YS_OK else (None, 0, 0)
     return bs.tiles
 
   def spmv(self, direction: vector, transpose: bool = False, fp32: bool = False) -> vector:
@@ -769,7 +772,7 @@ class hessian:
       m.values[k] = L.ptr(bs.values)
       m.values32[k] = L.ptr(bs.values32) if bs.values32 is not None else None
       m.row_ptr[k], m.entry_block[k], m.entry_col[k] = L.ptr(row_ptr), L.ptr(eb), L.ptr(ec)
-      row_block, cap = self.tile_plan(bs)
-      m.row_block[k], m.tile_cap[k] = L.ptr(row_block), cap
+      row_block, cap, ecap = self.tile_plan(bs)
+      m.row_block[k], m.tile_cap[k], m.entry_cap[k] = L.ptr(row_block), cap, ecap
     m.num_vars = self.rows // 3
     return m

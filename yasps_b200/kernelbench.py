@@ -115,7 +115,7 @@ def main():
   p = bs.pattern
   st = L.stream_ptr()
   row_ptr, eb, ec = H.spmv_plan(bs)
-  row_block, tile_cap = H.tile_plan(bs)
+  row_block, tile_cap, entry_cap = H.tile_plan(bs)
   x = torch.cos(torch.arange(H.rows, dtype=torch.float64, device="cuda") * 0.37)
   y = torch.zeros_like(x)
   z = torch.zeros_like(x)
@@ -141,7 +141,8 @@ def main():
       "spmv_fp32_x32": lambda: L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv,
                                       L.ptr(x32), L.ptr(y), 0, st),
       "spmv_fp32_tiled": lambda: L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb),
-                                        L.ptr(ec), L.ptr(row_block), tile_cap, nv, L.ptr(x32), L.ptr(y), 0, None,
+                                        L.ptr(ec), L.ptr(row_block), tile_cap, entry_cap, nv, L.ptr(x32), L.ptr(y), 0,
+                                        None,
                                         st),
       "mas_apply": lambda: L.call("ys_mas_apply", mas._mas, L.ptr(x), L.ptr(z), st),
       "gemv": lambda: L.call("ys_mas_gemv", mas._mas, st, None),
@@ -157,7 +158,7 @@ def main():
   if args.trace_pcg:
     return trace_pcg(cases["pcg50_fp32"])
   out = {"side": args.side, "tets": cube.tet_count, "dof": cube.dofs, "blocks": p.num_unique,
-         "plan_entries": int(row_ptr[-1].item()), "tile_cap": tile_cap,
+         "plan_entries": int(row_ptr[nv].item()), "tile_cap": tile_cap, "entry_cap": entry_cap,
          "gemv_alg_bytes": int(nbytes.value), "gemv_layout_bytes": gemv_layout_bytes(mas._tables),
          "non_psd": int(snh._const_cache[("work", snh.n)][1].item()), "pcg": mz.linearSolver.statistics}
   for name, fn in cases.items():
