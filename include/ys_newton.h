@@ -443,8 +443,9 @@ int32_t ys_spmv_tile_plan(const uint32_t* positions, uint32_t nu, const uint32_t
 
 /* ys_spmv3_x32 by tiles: persistent CTAs stage each tile's contiguous run of
  * FP32 block slots, its row-plan entries and its row pointers into shared
- * memory with bulk copies (cp.async.bulk, mbarrier completion,
- * double-buffered), so every stored block crosses HBM once per product;
+ * memory with bulk copies (cp.async.bulk, mbarrier completion, a ring of
+ * `stages` buffers, 2..4, 0 = as many as let two CTAs share an SM), so
+ * every stored block crosses HBM once per product;
  * direct blocks and the transposed blocks of rows in the tile are read from
  * shared memory, the transposed blocks of earlier tiles from global memory.
  * Bit-identical to ys_spmv3_x32.  Padding: row_ptr and row_block hold
@@ -457,8 +458,8 @@ int32_t ys_spmv_tile_plan(const uint32_t* positions, uint32_t nu, const uint32_t
 int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr,
                            const uint32_t* entry_block, const uint32_t* entry_col,
                            const uint32_t* row_block, uint32_t tile_cap, uint32_t entry_cap,
-                           uint32_t num_vars, const float* x32, double* y, int32_t beta,
-                           uint32_t* stage_status, void* stream);
+                           uint32_t stages, uint32_t num_vars, const float* x32, double* y,
+                           int32_t beta, uint32_t* stage_status, void* stream);
 
 /* ---- preconditioned CG ----------------------------------------------------- */
 

@@ -133,9 +133,9 @@ def check_tiled_spmv(H, x32, expected):
   assert ecap == int((((rp[ends] + 3) & ~3) - (rp[tiles] & ~3)).max())
   status = torch.zeros(1, dtype=torch.int32, device="cuda")
   y = torch.full((H.rows,), np.nan, dtype=torch.float64, device="cuda")
-  for _ in range(2):
+  for stages in (0, 2, 3, 4, 0):  # 0: as many stages as let two CTAs share an SM
     L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block), cap,
-           ecap, nv, L.ptr(x32), L.ptr(y), 0, L.ptr(status), L.stream_ptr())
+           ecap, stages, nv, L.ptr(x32), L.ptr(y), 0, L.ptr(status), L.stream_ptr())
     assert np.array_equal(y.cpu().numpy(), expected)
   assert int(status.item()) == 0
 

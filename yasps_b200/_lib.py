@@ -152,7 +152,7 @@ SIGNATURES = {
     "ys_pack_x32": (i32, [vp, u32, vp, vp]),
     "ys_spmv3_x32": (i32, [vp, vp, vp, vp, u32, vp, vp, i32, vp]),
     "ys_spmv_tile_plan": (i32, [vp, u32, vp, vp, u32, vp, P(u32), P(u32), vp]),
-    "ys_spmv3_x32_tiled": (i32, [vp, vp, vp, vp, vp, u32, u32, u32, vp, vp, i32, vp, vp]),
+    "ys_spmv3_x32_tiled": (i32, [vp, vp, vp, vp, vp, u32, u32, u32, u32, vp, vp, i32, vp, vp]),
     "ys_pcg_workspace_doubles": (u64, [u32]),
     "ys_pcg_create": (i32, [P(PcgArgs), P(vp)]),
     "ys_pcg_run": (i32, [vp, vp, P(PcgResult)]),

@@ -381,9 +381,13 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   size_t tile_smem = 0;
   unsigned grid_tiles = 0;
   if (P.fp32 && P.nsets == 1 && a.matrix.row_block[0] && a.matrix.tile_cap[0] > 0 && a.matrix.entry_cap[0] > 0) {
-    tile_smem = ys::tile_smem_bytes(a.matrix.tile_cap[0], a.matrix.entry_cap[0]);
-    int dev = 0, sms = 0, per_sm = 0;
-    if (tile_smem <= 200u * 1024u && cudaGetDevice(&dev) == cudaSuccess &&
+    int dev = 0, sms = 0, per_sm = 0, smem_sm = 0;
+    uint32_t stages = 2;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess)
+      stages = ys::tile_auto_stages(a.matrix.tile_cap[0], a.matrix.entry_cap[0], (size_t)smem_sm);
+    tile_smem = ys::tile_smem_bytes(a.matrix.tile_cap[0], a.matrix.entry_cap[0], stages);
+    if (tile_smem <= 200u * 1024u &&
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
         cudaFuncSetAttribute(ys::pcg_spmv_dot_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem) ==
             cudaSuccess &&
@@ -395,7 +399,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       tiled = true;
       P.tiled = ys::TiledSet{a.matrix.values32[0], a.matrix.row_ptr[0], a.matrix.entry_block[0],
                              a.matrix.entry_col[0], a.matrix.row_block[0], P.nv, a.matrix.tile_cap[0],
-                             a.matrix.entry_cap[0]};
+                             a.matrix.entry_cap[0], stages};
     }
   }
   P.partials = w; w += (uint64_t)ys::kRowLanes * (grid + 2);

@@ -278,25 +278,28 @@ int32_t ys_spmv_tile_plan(const uint32_t* positions, uint32_t nu, const uint32_t
 
 int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr, const uint32_t* entry_block,
                            const uint32_t* entry_col, const uint32_t* row_block, uint32_t tile_cap,
-                           uint32_t entry_cap, uint32_t num_vars, const float* x32, double* y, int32_t beta,
-                           uint32_t* stage_status, void* stream) {
+                           uint32_t entry_cap, uint32_t stages, uint32_t num_vars, const float* x32, double* y,
+                           int32_t beta, uint32_t* stage_status, void* stream) {
+  YS_REQUIRE(stages == 0 || (stages >= 2 && stages <= ys::kMaxStages), YS_ERR_INVALID, "stages: 0 (auto) or 2..4");
   YS_REQUIRE(values32 && x32 && row_block && tile_cap > 0 && entry_cap > 0 && (entry_cap & 3u) == 0,
              YS_ERR_INVALID, "null argument or no tile plan");
   YS_REQUIRE((reinterpret_cast<uintptr_t>(x32) & 15) == 0 && (reinterpret_cast<uintptr_t>(values32) & 15) == 0,
              YS_ERR_INVALID, "values32 and x32 must be 16-byte aligned");
   if (num_vars == 0) return YS_OK;
-  const size_t smem = ys::tile_smem_bytes(tile_cap, entry_cap);
-  YS_REQUIRE(smem <= 200u * 1024u, YS_ERR_CAPACITY, "a tile's blocks exceed the shared-memory stage");
-  YS_CUDA_TRY(cudaFuncSetAttribute(ys::spmv3_x32_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int dev = 0, sms = 0, per_sm = 0;
+  int dev = 0, sms = 0, per_sm = 0, smem_sm = 0;
   YS_CUDA_TRY(cudaGetDevice(&dev));
   YS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  YS_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  if (stages == 0) stages = ys::tile_auto_stages(tile_cap, entry_cap, (size_t)smem_sm);
+  const size_t smem = ys::tile_smem_bytes(tile_cap, entry_cap, stages);
+  YS_REQUIRE(smem <= 200u * 1024u, YS_ERR_CAPACITY, "a tile's blocks exceed the shared-memory stage");
+  YS_CUDA_TRY(cudaFuncSetAttribute(ys::spmv3_x32_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   YS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ys::spmv3_x32_tiled_kernel, ys::kTileThreads,
                                                             smem));
   YS_REQUIRE(per_sm > 0, YS_ERR_CAPACITY, "tiled SpMV does not fit on an SM");
   const uint32_t ntiles = (num_vars + ys::kTileRows - 1) / ys::kTileRows;
   const unsigned grid = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
-  ys::TiledSet T{values32, row_ptr, entry_block, entry_col, row_block, num_vars, tile_cap, entry_cap};
+  ys::TiledSet T{values32, row_ptr, entry_block, entry_col, row_block, num_vars, tile_cap, entry_cap, stages};
   ys::spmv3_x32_tiled_kernel<<<grid, ys::kTileThreads, smem, (cudaStream_t)stream>>>(
       T, reinterpret_cast<const float4*>(x32), y, beta, stage_status);
   YS_CHECK_LAUNCH();

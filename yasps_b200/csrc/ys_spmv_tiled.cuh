@@ -1,5 +1,6 @@
 // Tiled symmetric 3x3-block SpMV with FP32 blocks staged in shared memory by
-// bulk copies (cp.async.bulk + mbarrier, double-buffered, persistent CTAs).
+// bulk copies (cp.async.bulk + mbarrier, a ring of stage buffers, persistent
+// CTAs).
 //
 // In the reference's storage every off-diagonal block is stored once (upper)
 // and used twice: by its row (B x_c) and, transposed, by its column
@@ -40,6 +41,7 @@ struct TiledSet {
   uint32_t nv;
   uint32_t tile_cap;           // most blocks in one tile
   uint32_t entry_cap;          // most plan entries of one tile, 4-aligned range
+  uint32_t stages;             // stage buffers in shared memory (2 .. kMaxStages)
 };
 
 // Words of row_ptr / row_block staged per tile: rows r0 .. r0 + kTileRows
@@ -191,37 +193,52 @@ __device__ __forceinline__ void tile_row_staged(const TiledSet& T, const TileSta
   y2 = (double)a2;
 }
 
-// Shared memory of a tiled launch: two stage buffers.
-inline size_t tile_smem_bytes(uint32_t tile_cap, uint32_t entry_cap) {
-  return 2 * tile_stage_bytes(tile_cap, entry_cap);
+// Stage buffers of a tiled launch (2 .. kMaxStages) and their shared memory.
+constexpr uint32_t kMaxStages = 4;
+inline size_t tile_smem_bytes(uint32_t tile_cap, uint32_t entry_cap, uint32_t stages) {
+  return (size_t)stages * tile_stage_bytes(tile_cap, entry_cap);
 }
 
-// Runs every tile t = blockIdx.x + k gridDim.x of the set through the
-// double-buffered stage; out(i, valid, lane, y0, y1, y2) receives each row
-// (all lanes call it, lane 0 of a row group owns the result).  A bulk-copy
-// wait that runs out sets *err and the CTA reads global memory from then on
-// through the row-plan gather (the same values and order: the result stays
-// exact).
+// Stage count of a launch: the most stages (up to kMaxStages) that still let
+// two CTAs share an SM, so that several tiles are in flight per SM while the
+// others compute; at least two.
+inline uint32_t tile_auto_stages(uint32_t tile_cap, uint32_t entry_cap, size_t smem_per_sm) {
+  const size_t one = tile_stage_bytes(tile_cap, entry_cap);
+  uint32_t s = kMaxStages;
+  while (s > 2 && 2 * (s * one + 1024) > smem_per_sm) --s;
+  return s;
+}
+
+// Runs every tile t = blockIdx.x + k gridDim.x of the set through a ring of
+// `stages` stage buffers (tile k is staged in buffer k % stages, up to
+// stages - 1 tiles ahead of the one being computed);
+// out(i, valid, lane, y0, y1, y2) receives each row (all lanes call it, lane
+// 0 of a row group owns the result).  A bulk-copy wait that runs out sets
+// *err and the CTA reads global memory from then on through the row-plan
+// gather (the same values and order: the result stays exact).
 template <class Out>
-__device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4* __restrict__ x32,
-                                                unsigned* err, Out&& out) {
+__device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4* __restrict__ x32, unsigned* err,
+                                                Out&& out) {
+  const uint32_t stages = T.stages;
   extern __shared__ float4 tile_stage4[];
   float* stage_base = reinterpret_cast<float*>(tile_stage4);
   const uint64_t buf_floats = tile_stage_bytes(T.tile_cap, T.entry_cap) / 4;
-  __shared__ uint64_t bars[2];
+  __shared__ uint64_t bars[kMaxStages];
   __shared__ int dead;
   const uint32_t ntiles = (T.nv + kTileRows - 1) / kTileRows;
   if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (uint32_t b = 0; b < stages; ++b) mbar_init(&bars[b], 1);
     mbar_fence_init();
     dead = 0;
   }
   __syncthreads();
-  uint32_t issued[2] = {0u, 0u};  // phases issued per buffer (thread 0)
-  // thread 0: stage tile `t` into buffer `buf`: its blocks, its plan entries
-  // (a 16-byte aligned range) and its row pointers, one mbarrier phase
-  auto issue = [&](uint32_t t, int buf) {
+  uint32_t issued = 0;  // tiles issued by this CTA (thread 0)
+  // thread 0: stage this CTA's tile number `q` (t = blockIdx.x + q gridDim.x)
+  // into buffer q % stages: its blocks, its plan entries (a 16-byte aligned
+  // range) and its row pointers, one mbarrier phase
+  auto issue = [&]() {
+    const uint32_t t = blockIdx.x + issued * gridDim.x;
+    const uint32_t buf = issued % stages;
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
     const uint32_t b0 = __ldg(T.row_block + r0), b1 = __ldg(T.row_block + r1);
     const uint32_t e0a = __ldg(T.row_ptr + r0) & ~3u, e1a = (__ldg(T.row_ptr + r1) + 3u) & ~3u;
@@ -229,6 +246,7 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     const uint32_t vb = (b1 - b0) * kTileSlotBytes, eb = (e1a - e0a) * 4u, rb = ((r1 - r0 + 4u) & ~3u) * 4u;
     float* dst = stage_base + buf * buf_floats;
     const TileStage S = stage_view(T, dst, r0, b0, e0a);
+    fence_proxy_async_smem();
     mbar_arrive_expect_tx(&bars[buf], vb + 2 * eb + 2 * rb);
     if (vb) bulk_copy_g2s(dst, T.values32 + (uint64_t)kFp32BlockStride * b0, vb, &bars[buf]);
     if (eb) {
@@ -237,27 +255,25 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     }
     bulk_copy_g2s((void*)S.rptr, T.row_ptr + r0, rb, &bars[buf]);
     bulk_copy_g2s((void*)S.rblock, T.row_block + r0, rb, &bars[buf]);
-    ++issued[buf];
+    ++issued;
   };
-  if (threadIdx.x == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
-  uint32_t k = 0;
+  const uint32_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (threadIdx.x == 0)
+    while (issued < mine && issued + 1 < stages) issue();
   constexpr uint32_t kRowsPerPass = kTileThreads / kRowLanes;
-  constexpr uint32_t kPasses = kTileRows / kRowsPerPass;
-  static_assert(kPasses == 2, "two rows a thread");
+  static_assert(kTileRows == 2 * kRowsPerPass, "two rows a thread");
   const int lane = (int)(threadIdx.x % kRowLanes);
-  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
-    const int buf = (int)(k & 1);
-    const uint32_t next = t + gridDim.x;
-    if (threadIdx.x == 0 && next < ntiles && !dead) {
-      fence_proxy_async_smem();
-      issue(next, buf ^ 1);
-    }
+  for (uint32_t k = 0; k < mine; ++k) {
+    const uint32_t t = blockIdx.x + k * gridDim.x;
+    const uint32_t buf = k % stages;
+    // buffer (k + stages - 1) % stages was last read in iteration k - 1
+    if (threadIdx.x == 0 && issued < mine && !dead) issue();
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
     const uint32_t iA = r0 + threadIdx.x / kRowLanes, iB = iA + kRowsPerPass;
     double yA[3], yB[3];
-    // the k-th tile is the (k >> 1)-th phase of its buffer
+    // tile k is the (k / stages)-th phase of its buffer
     bool staged = !dead;
-    if (staged && !mbar_wait_bounded(&bars[buf], (k >> 1) & 1u)) {
+    if (staged && !mbar_wait_bounded(&bars[buf], (k / stages) & 1u)) {
       staged = false;
       dead = 1;  // no further copies into this CTA's buffers
       atomicOr(err, 1u);
@@ -279,12 +295,11 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     out(iB, iB < r1, lane, yB[0], yB[1], yB[2]);
     __syncthreads();
   }
-  // a CTA that stopped staging waits (bounded) for the last copy it issued
-  // into each buffer before its shared memory goes away
+  // a CTA that stopped staging waits (bounded) for every copy it issued
+  // before its shared memory goes away: the last phase of each buffer
   if (dead && threadIdx.x == 0) {
-#pragma unroll
-    for (int b = 0; b < 2; ++b)
-      if (issued[b]) mbar_wait_bounded(&bars[b], (issued[b] - 1) & 1u);
+    for (uint32_t q = issued > stages ? issued - stages : 0; q < issued; ++q)
+      mbar_wait_bounded(&bars[q % stages], (q / stages) & 1u);
   }
 }
 

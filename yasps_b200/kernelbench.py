@@ -128,6 +128,10 @@ def main():
     snh.evaluate(plan, bs.records, H._grad_records)
     snh.projection_method = 1
 
+  def tiled(stages):
+    L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block),
+           tile_cap, entry_cap, stages, nv, L.ptr(x32), L.ptr(y), 0, None, st)
+
   cases = {
       "snh_eval_only": lambda: snh_eval(0),
       "snh_eval_project": lambda: snh_eval(1),
@@ -140,10 +144,10 @@ def main():
                                   L.ptr(x), L.ptr(y), 0, st),
       "spmv_fp32_x32": lambda: L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv,
                                       L.ptr(x32), L.ptr(y), 0, st),
-      "spmv_fp32_tiled": lambda: L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb),
-                                        L.ptr(ec), L.ptr(row_block), tile_cap, entry_cap, nv, L.ptr(x32), L.ptr(y), 0,
-                                        None,
-                                        st),
+      "spmv_fp32_tiled": lambda: tiled(0),
+      "spmv_fp32_tiled_s2": lambda: tiled(2),
+      "spmv_fp32_tiled_s3": lambda: tiled(3),
+      "spmv_fp32_tiled_s4": lambda: tiled(4),
       "mas_apply": lambda: L.call("ys_mas_apply", mas._mas, L.ptr(x), L.ptr(z), st),
       "gemv": lambda: L.call("ys_mas_gemv", mas._mas, st, None),
       "newton_step": lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
