@@ -124,8 +124,9 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
 
 // Curvature p^T q (grid reduction) and the step length; the last block of
 // the grid decides.
+template <int BLOCK = kPcgBlock>
 __device__ __forceinline__ void spmv_dot_finish(const PcgParams& P, double (&v)[1]) {
-  if (!grid_reduce_last<1>(v, P.partials, P.tickets + 1)) return;
+  if (!grid_reduce_last<1, BLOCK>(v, P.partials, P.tickets + 1)) return;
   if (threadIdx.x != 0) return;
   double* st = P.st;
   const double curv = v[0];
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
 // The SpMV + dot of the FP32 loop over the tile plan: each persistent CTA
 // stages its tiles' blocks into shared memory by bulk copies (see
 // ys_spmv_tiled.cuh); lane 0 of a row group writes q and adds p . q.
-__global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot_tiled(PcgParams P) {
+__global__ void __launch_bounds__(kTileThreads) pcg_spmv_dot_tiled(PcgParams P) {
   double v[1] = {0.0};
   spmv3_tiles_x32(P.tiled, P.p32, P.tickets + 6, [&](uint32_t i, bool valid, int lane, double q0, double q1,
                                                      double q2) {
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot_tiled(PcgParams P) {
     P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
     v[0] += P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
   });
-  spmv_dot_finish(P, v);
+  spmv_dot_finish<kTileThreads>(P, v);
 }
 
 __global__ void __launch_bounds__(kPcgBlock) pcg_update_bj(PcgParams P) {
@@ -391,7 +392,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
         cudaFuncSetAttribute(ys::pcg_spmv_dot_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem) ==
             cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ys::pcg_spmv_dot_tiled, ys::kPcgBlock, tile_smem) ==
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ys::pcg_spmv_dot_tiled, ys::kTileThreads, tile_smem) ==
             cudaSuccess &&
         sms > 0 && per_sm > 0) {
       const unsigned ntiles = (P.nv + ys::kTileRows - 1) / ys::kTileRows;
@@ -450,7 +451,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       cudaGraphNode_t n1 = nullptr, n2 = nullptr, n3 = nullptr;
       void* args1[] = {&P};
       if (tiled)
-        e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot_tiled, grid_tiles, ys::kPcgBlock,
+        e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot_tiled, grid_tiles, ys::kTileThreads,
                            args1, tile_smem);
       else
         e = ys::add_kernel(body, &n1, nullptr, 0,

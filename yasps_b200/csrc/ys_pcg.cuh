@@ -58,14 +58,14 @@ __device__ __forceinline__ double thread_partial_sum(const double* __restrict__ 
   return (a0 + a1) + (a2 + a3);
 }
 
-template <int NV>
+template <int NV, int BLOCK = kPcgBlock>
 __device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* __restrict__ partials,
                                                  unsigned* __restrict__ ticket) {
-  __shared__ double red[kPcgBlock / 32];
+  __shared__ double red[BLOCK / 32];
   __shared__ bool last;
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
-    const double s = block_sum<kPcgBlock>(v[k], red);
+    const double s = block_sum<BLOCK>(v[k], red);
     if (threadIdx.x == 0) partials[(uint64_t)k * gridDim.x + blockIdx.x] = s;
   }
   __threadfence();
@@ -76,7 +76,7 @@ __device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* __rest
   __threadfence();
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
-    v[k] = block_sum<kPcgBlock>(thread_partial_sum(partials + (uint64_t)k * gridDim.x, gridDim.x), red);
+    v[k] = block_sum<BLOCK>(thread_partial_sum(partials + (uint64_t)k * gridDim.x, gridDim.x), red);
   }
   if (threadIdx.x == 0) *ticket = 0u;
   return true;

@@ -25,7 +25,7 @@
 namespace ys {
 
 constexpr uint32_t kTileRows = YS_SPMV_TILE_ROWS;
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = kTileRows * kRowLanes;  // a thread group of kRowLanes a row
 constexpr uint32_t kTileSlotBytes = 4 * kFp32BlockStride;  // one FP32 block slot (48 B)
 // try_wait polls before a CTA stops using shared memory (the copies are a
 // few tens of KB and land within microseconds; the bound only keeps a stuck
@@ -233,6 +233,19 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
   }
   __syncthreads();
   uint32_t issued = 0;  // tiles issued by this CTA (thread 0)
+  const uint32_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // thread 0 loads the bounds of the next tile to issue one issue ahead, so
+  // the copy is not held up by their latency
+  uint32_t nb0 = 0, nb1 = 0, ne0 = 0, ne1 = 0;
+  auto load_bounds = [&](uint32_t q) {
+    if (q >= mine) return;
+    const uint32_t r0 = (blockIdx.x + q * gridDim.x) * kTileRows, r1 = min(r0 + kTileRows, T.nv);
+    nb0 = __ldg(T.row_block + r0);
+    nb1 = __ldg(T.row_block + r1);
+    ne0 = __ldg(T.row_ptr + r0);
+    ne1 = __ldg(T.row_ptr + r1);
+  };
+  if (threadIdx.x == 0) load_bounds(0);
   // thread 0: stage this CTA's tile number `q` (t = blockIdx.x + q gridDim.x)
   // into buffer q % stages: its blocks, its plan entries (a 16-byte aligned
   // range) and its row pointers, one mbarrier phase
@@ -240,8 +253,7 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     const uint32_t t = blockIdx.x + issued * gridDim.x;
     const uint32_t buf = issued % stages;
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
-    const uint32_t b0 = __ldg(T.row_block + r0), b1 = __ldg(T.row_block + r1);
-    const uint32_t e0a = __ldg(T.row_ptr + r0) & ~3u, e1a = (__ldg(T.row_ptr + r1) + 3u) & ~3u;
+    const uint32_t b0 = nb0, b1 = nb1, e0a = ne0 & ~3u, e1a = (ne1 + 3u) & ~3u;
     // rows r0 .. r1 (inclusive) rounded up to 4 words: at most num_vars + 4
     const uint32_t vb = (b1 - b0) * kTileSlotBytes, eb = (e1a - e0a) * 4u, rb = ((r1 - r0 + 4u) & ~3u) * 4u;
     float* dst = stage_base + buf * buf_floats;
@@ -256,12 +268,11 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     bulk_copy_g2s((void*)S.rptr, T.row_ptr + r0, rb, &bars[buf]);
     bulk_copy_g2s((void*)S.rblock, T.row_block + r0, rb, &bars[buf]);
     ++issued;
+    load_bounds(issued);
   };
-  const uint32_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   if (threadIdx.x == 0)
     while (issued < mine && issued + 1 < stages) issue();
-  constexpr uint32_t kRowsPerPass = kTileThreads / kRowLanes;
-  static_assert(kTileRows == 2 * kRowsPerPass, "two rows a thread");
+  static_assert(kTileRows * kRowLanes == kTileThreads, "one row a thread group");
   const int lane = (int)(threadIdx.x % kRowLanes);
   for (uint32_t k = 0; k < mine; ++k) {
     const uint32_t t = blockIdx.x + k * gridDim.x;
@@ -269,8 +280,8 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     // buffer (k + stages - 1) % stages was last read in iteration k - 1
     if (threadIdx.x == 0 && issued < mine && !dead) issue();
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
-    const uint32_t iA = r0 + threadIdx.x / kRowLanes, iB = iA + kRowsPerPass;
-    double yA[3], yB[3];
+    const uint32_t iA = r0 + threadIdx.x / kRowLanes;
+    double yA[3];
     // tile k is the (k / stages)-th phase of its buffer
     bool staged = !dead;
     if (staged && !mbar_wait_bounded(&bars[buf], (k / stages) & 1u)) {
@@ -285,14 +296,11 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
       const uint32_t* rp = rblk - kTileRowWords;
       const TileStage S = stage_view(T, base, r0, rblk[0], rp[0] & ~3u);
       tile_row_staged(T, S, x32, iA, iA < r1, lane, yA[0], yA[1], yA[2]);
-      tile_row_staged(T, S, x32, iB, iB < r1, lane, yB[0], yB[1], yB[2]);
     } else {
       SpmvSet g{nullptr, T.values32, T.row_ptr, T.entry_block, T.entry_col};
       spmv3_group_x32(&g, 1, iA, iA < r1, lane, x32, yA[0], yA[1], yA[2]);
-      spmv3_group_x32(&g, 1, iB, iB < r1, lane, x32, yB[0], yB[1], yB[2]);
     }
     out(iA, iA < r1, lane, yA[0], yA[1], yA[2]);
-    out(iB, iB < r1, lane, yB[0], yB[1], yB[2]);
     __syncthreads();
   }
   // a CTA that stopped staging waits (bounded) for every copy it issued
