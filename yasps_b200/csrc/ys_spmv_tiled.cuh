@@ -26,20 +26,20 @@ namespace ys {
 
 constexpr uint32_t kTileRows = YS_SPMV_TILE_ROWS;
 constexpr int kTileThreads = kTileRows * kRowLanes;  // a thread group of kRowLanes a row
-constexpr uint32_t kTileSlotBytes = 4 * kFp32BlockStride;  // one FP32 block slot (48 B)
+constexpr uint32_t kTileSlotBytes = 4 * kFp32BlockStride;  // one FP32 block (36 B)
 // try_wait polls before a CTA stops using shared memory (the copies are a
 // few tens of KB and land within microseconds; the bound only keeps a stuck
 // copy from hanging the device)
 constexpr uint32_t kTileWaitPolls = 1u << 22;
 
 struct TiledSet {
-  const float* values32;       // 12-float slots, (row, col)-sorted upper blocks
+  const float* values32;       // 9 floats a block, (row, col)-sorted upper blocks
   const uint32_t* row_ptr;     // row plan (ys_spmv_plan_build), num_vars + 4 entries
   const uint32_t* entry_block; // both hold (row_ptr[nv] + 3) & ~3 entries at least
   const uint32_t* entry_col;
   const uint32_t* row_block;   // [nv + 4] first stored block of each row
   uint32_t nv;
-  uint32_t tile_cap;           // most blocks in one tile
+  uint32_t tile_cap;           // most blocks of one tile's 4-block aligned range
   uint32_t entry_cap;          // most plan entries of one tile, 4-aligned range
   uint32_t stages;             // stage buffers in shared memory (2 .. kMaxStages)
 };
@@ -111,16 +111,16 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
+// A staged block: 9 floats, 36-byte stride (an odd word stride, so the lanes
+// of a row group reading consecutive blocks hit distinct banks).
 __device__ __forceinline__ void load_slot(const float* __restrict__ p, float (&b)[9]) {
-  const float4* q = reinterpret_cast<const float4*>(p);
-  const float4 v0 = q[0], v1 = q[1], v2 = q[2];
-  b[0] = v0.x; b[1] = v0.y; b[2] = v0.z; b[3] = v0.w;
-  b[4] = v1.x; b[5] = v1.y; b[6] = v1.z; b[7] = v1.w;
-  b[8] = v2.x;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) b[k] = p[k];
 }
 
 // One staged tile: pointers into a stage buffer and the global ranges they
-// hold (blocks [b0, ...), plan entries [e0a, ...), rows [r0, ...]).
+// hold (blocks [b0, ...) from the 4-aligned block before the tile's first,
+// plan entries [e0a, ...), rows [r0, ...]).
 struct TileStage {
   const float* blocks;
   const uint32_t* cols;
@@ -160,27 +160,23 @@ __device__ __forceinline__ void tile_row_staged(const TiledSet& T, const TileSta
     nt = (e1 - e0) - (S.rblock[k + 1] - ub);  // transposed entries come first
   }
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-  for (uint32_t e = e0 + lane; e < e1; e += 2 * kRowLanes) {
-    const uint32_t f = e + kRowLanes;
-    const bool two = f < e1;
-    const uint32_t g = two ? f : e;
-    const uint32_t kA = e - e0, kB = g - e0;
-    const bool tA = kA < nt, tB = kB < nt;
-    const uint32_t jA = S.cols[e - S.e0a], jB = S.cols[g - S.e0a];
-    const uint32_t bA = tA ? (S.eblocks[e - S.e0a] & 0x7fffffffu) : ub + (kA - nt);
-    const uint32_t bB = tB ? (S.eblocks[g - S.e0a] & 0x7fffffffu) : ub + (kB - nt);
-    float xa[3], xb[3], ba[9], bb[9];
-    load_x(x32, jA, xa);
-    load_x(x32, jB, xb);
-    if (bA >= S.b0) load_slot(S.blocks + (uint64_t)kFp32BlockStride * (bA - S.b0), ba);
-    else load_block(T.values32, bA, ba);
-    if (bB >= S.b0) load_slot(S.blocks + (uint64_t)kFp32BlockStride * (bB - S.b0), bb);
-    else load_block(T.values32, bB, bb);
-    const float wB = two ? 1.f : 0.f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) xb[k] *= wB;
-    block_mac(ba, xa, tA, a0, a1, a2);
-    block_mac(bb, xb, tB, a0, a1, a2);
+  // entries lane, lane + 8, ... in order (the order of the row-plan gather);
+  // the next entry's column and neighbour vector are loaded before this
+  // entry's product, so one gather is always in flight
+  uint32_t e = e0 + lane;
+  float xn[3] = {0.f, 0.f, 0.f};
+  if (e < e1) load_x(x32, S.cols[e - S.e0a], xn);
+#pragma unroll 1
+  for (; e < e1; e += kRowLanes) {
+    const uint32_t kk = e - e0;
+    const bool tr = kk < nt;
+    const uint32_t b = tr ? (S.eblocks[e - S.e0a] & 0x7fffffffu) : ub + (kk - nt);
+    const float xv[3] = {xn[0], xn[1], xn[2]};
+    if (e + kRowLanes < e1) load_x(x32, S.cols[e + kRowLanes - S.e0a], xn);
+    float bv[9];
+    if (b >= S.b0) load_slot(S.blocks + (uint64_t)kFp32BlockStride * (b - S.b0), bv);
+    else load_block(T.values32, b, bv);
+    block_mac(bv, xv, tr, a0, a1, a2);
   }
 #pragma unroll
   for (int o = kRowLanes / 2; o > 0; o >>= 1) {
@@ -199,13 +195,14 @@ inline size_t tile_smem_bytes(uint32_t tile_cap, uint32_t entry_cap, uint32_t st
   return (size_t)stages * tile_stage_bytes(tile_cap, entry_cap);
 }
 
-// Stage count of a launch: the most stages (up to kMaxStages) that still let
-// two CTAs share an SM, so that several tiles are in flight per SM while the
-// others compute; at least two.
+// Stage count of a launch: the kernel is bound by the latency of its
+// gathers, so resident warps come first: the most stages (up to kMaxStages,
+// at least two) that still let the thread limit's worth of CTAs share an SM.
 inline uint32_t tile_auto_stages(uint32_t tile_cap, uint32_t entry_cap, size_t smem_per_sm) {
   const size_t one = tile_stage_bytes(tile_cap, entry_cap);
+  const size_t ctas = 2048 / kTileThreads;
   uint32_t s = kMaxStages;
-  while (s > 2 && 2 * (s * one + 1024) > smem_per_sm) --s;
+  while (s > 2 && ctas * (s * one + 1024) > smem_per_sm) --s;
   return s;
 }
 
@@ -232,28 +229,35 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     dead = 0;
   }
   __syncthreads();
-  uint32_t issued = 0;  // tiles issued by this CTA (thread 0)
   const uint32_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  // thread 0 loads the bounds of the next tile to issue one issue ahead, so
-  // the copy is not held up by their latency
-  uint32_t nb0 = 0, nb1 = 0, ne0 = 0, ne1 = 0;
+  // thread 0's pipeline state lives in shared memory (the other threads need
+  // no registers for it): tiles issued so far, and the bounds of the next
+  // tile to issue, loaded one issue ahead so the copy is not held up by
+  // their latency
+  __shared__ uint32_t issued;
+  __shared__ uint32_t nxt[4];  // row_block[r0], row_block[r1], row_ptr[r0], row_ptr[r1]
   auto load_bounds = [&](uint32_t q) {
     if (q >= mine) return;
     const uint32_t r0 = (blockIdx.x + q * gridDim.x) * kTileRows, r1 = min(r0 + kTileRows, T.nv);
-    nb0 = __ldg(T.row_block + r0);
-    nb1 = __ldg(T.row_block + r1);
-    ne0 = __ldg(T.row_ptr + r0);
-    ne1 = __ldg(T.row_ptr + r1);
+    nxt[0] = __ldg(T.row_block + r0);
+    nxt[1] = __ldg(T.row_block + r1);
+    nxt[2] = __ldg(T.row_ptr + r0);
+    nxt[3] = __ldg(T.row_ptr + r1);
   };
-  if (threadIdx.x == 0) load_bounds(0);
+  if (threadIdx.x == 0) {
+    issued = 0;
+    load_bounds(0);
+  }
   // thread 0: stage this CTA's tile number `q` (t = blockIdx.x + q gridDim.x)
   // into buffer q % stages: its blocks, its plan entries (a 16-byte aligned
   // range) and its row pointers, one mbarrier phase
   auto issue = [&]() {
-    const uint32_t t = blockIdx.x + issued * gridDim.x;
-    const uint32_t buf = issued % stages;
+    const uint32_t q = issued;
+    const uint32_t t = blockIdx.x + q * gridDim.x;
+    const uint32_t buf = q % stages;
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
-    const uint32_t b0 = nb0, b1 = nb1, e0a = ne0 & ~3u, e1a = (ne1 + 3u) & ~3u;
+    // whole 4-block groups (144 bytes) and 4-entry groups: 16-byte aligned
+    const uint32_t b0 = nxt[0] & ~3u, b1 = (nxt[1] + 3u) & ~3u, e0a = nxt[2] & ~3u, e1a = (nxt[3] + 3u) & ~3u;
     // rows r0 .. r1 (inclusive) rounded up to 4 words: at most num_vars + 4
     const uint32_t vb = (b1 - b0) * kTileSlotBytes, eb = (e1a - e0a) * 4u, rb = ((r1 - r0 + 4u) & ~3u) * 4u;
     float* dst = stage_base + buf * buf_floats;
@@ -267,11 +271,12 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     }
     bulk_copy_g2s((void*)S.rptr, T.row_ptr + r0, rb, &bars[buf]);
     bulk_copy_g2s((void*)S.rblock, T.row_block + r0, rb, &bars[buf]);
-    ++issued;
-    load_bounds(issued);
+    issued = q + 1;
+    load_bounds(q + 1);
   };
   if (threadIdx.x == 0)
     while (issued < mine && issued + 1 < stages) issue();
+  __syncthreads();
   static_assert(kTileRows * kRowLanes == kTileThreads, "one row a thread group");
   const int lane = (int)(threadIdx.x % kRowLanes);
   for (uint32_t k = 0; k < mine; ++k) {
@@ -294,7 +299,7 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
       const uint32_t* rblk = reinterpret_cast<const uint32_t*>(base + (uint64_t)kFp32BlockStride * T.tile_cap) +
                              2ull * T.entry_cap + kTileRowWords;
       const uint32_t* rp = rblk - kTileRowWords;
-      const TileStage S = stage_view(T, base, r0, rblk[0], rp[0] & ~3u);
+      const TileStage S = stage_view(T, base, r0, rblk[0] & ~3u, rp[0] & ~3u);
       tile_row_staged(T, S, x32, iA, iA < r1, lane, yA[0], yA[1], yA[2]);
     } else {
       SpmvSet g{nullptr, T.values32, T.row_ptr, T.entry_block, T.entry_col};
@@ -306,7 +311,8 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
   // a CTA that stopped staging waits (bounded) for every copy it issued
   // before its shared memory goes away: the last phase of each buffer
   if (dead && threadIdx.x == 0) {
-    for (uint32_t q = issued > stages ? issued - stages : 0; q < issued; ++q)
+    const uint32_t n = issued;
+    for (uint32_t q = n > stages ? n - stages : 0; q < n; ++q)
       mbar_wait_bounded(&bars[q % stages], (q / stages) & 1u);
   }
 }
