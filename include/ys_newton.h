@@ -407,8 +407,8 @@ int32_t ys_spmv_plan_build(const uint32_t* positions, uint32_t nu, uint32_t num_
 int32_t ys_spmv_plan_workspace_bytes(uint32_t nu, uint32_t num_vars, uint64_t* bytes);
 
 /* y = H x (beta == 0) or y += H x (beta == 1) for a 3x3 symmetric upper
- * block set with FP64 (values, 9 doubles a block) or FP32 (values32, 9
- * floats a block, see ys_assemble3) blocks, one of which is NULL.  Deterministic (row-gather, fixed order).  Replaces `spmv_blocks`
+ * block set with FP64 (values, 9 doubles a block) or FP32 (values32, 12-float
+ * 16-byte aligned slots, see ys_assemble3) blocks, one of which is NULL.  Deterministic (row-gather, fixed order).  Replaces `spmv_blocks`
  * (PKG/matrixAndVector/matrix/matrix.pyx:21-86) and `spmvOffDiagonalBlocks`
  * (PKG/kernel/Solver/solverKernel.pyx:156-215).                            */
 int32_t ys_spmv3(const double* values, const float* values32, const uint32_t* row_ptr,
@@ -473,7 +473,7 @@ typedef struct ys_matrix3 {
   /* up to two 3x3 block sets (static + dynamic), each with an SpMV row plan */
   uint32_t num_sets;
   const double* values[2];
-  const float* values32[2];      /* FP32 blocks, 9 floats each (ys_assemble3)     */
+  const float* values32[2];      /* 12-float block slots (ys_assemble3)           */
   const uint32_t* row_ptr[2];
   const uint32_t* entry_block[2];
   const uint32_t* entry_col[2];
@@ -587,10 +587,9 @@ int32_t ys_mas_gemv(void* handle, void* stream, uint64_t* algorithmic_bytes);
 int32_t ys_gradient_coordinates(const uint32_t* codes, const uint16_t* sizes, uint32_t n, uint32_t K,
                                 uint32_t* grad_outer, uint32_t* coords, uint16_t* dims, void* stream);
 /* ys_assemble specialised for 3x3 blocks.  out32 (when not NULL) receives
- * the FP32 copy packed like the FP64 blocks, 9 floats per block (block u at
- * out32 + 9 u): the layout ys_spmv3 and the PCG read FP32 blocks in.  The
- * FP32 array is 16-byte aligned and holds whole groups of 4 blocks
- * (36 * ceil(nu / 4) floats; the tiled SpMV copies 144-byte groups).      */
+ * the FP32 copy in 16-byte aligned slots of 12 floats per block (block u at
+ * out32 + 12 u, the last 3 floats unused): the layout ys_spmv3, the tiled
+ * SpMV and the PCG read FP32 blocks in.                                   */
 int32_t ys_assemble3(const double* records, const uint32_t* begin, const uint32_t* count, const uint32_t* offset,
                      uint32_t nu, double* out, float* out32, void* stream);
 /* ys_assemble with out offset offset[u * offset_stride] (the gradient passes

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(256) assemble3_kernel(const double* __restrict
   for (uint32_t k = 0; k < c; ++k) acc += rec[(uint64_t)b + 9ull * k + e];
   const uint64_t o = offset[u];
   out[o + e] = acc;
-  if (out32) out32[9ull * u + e] = (float)acc;  // FP32 copy, 9 floats a block
+  if (out32) out32[12ull * u + e] = (float)acc;  // 12-float FP32 block slots
 }
 
 struct DiagLayout {

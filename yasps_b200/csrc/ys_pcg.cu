@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_spmv_dot(PcgParams P) {
 // The SpMV + dot of the FP32 loop over the tile plan: each persistent CTA
 // stages its tiles' blocks into shared memory by bulk copies (see
 // ys_spmv_tiled.cuh); lane 0 of a row group writes q and adds p . q.
-__global__ void __launch_bounds__(kTileThreads) pcg_spmv_dot_tiled(PcgParams P) {
+__global__ void __launch_bounds__(kTileThreads, 3) pcg_spmv_dot_tiled(PcgParams P) {
   double v[1] = {0.0};
   spmv3_tiles_x32(P.tiled, P.p32, P.tickets + 6, [&](uint32_t i, bool valid, int lane, double q0, double q1,
                                                      double q2) {

@@ -97,8 +97,7 @@ __global__ void tile_row_block_kernel(const uint32_t* __restrict__ pos, uint32_t
 
 // Checks that row i's direct plan entries are the blocks row_block[i] ..
 // row_block[i+1] - 1 in order after its transposed entries, and records the
-// largest tile (scratch[0]: mismatch flag, scratch[1]: most blocks of a tile's
-// 4-block aligned range,
+// largest tile (scratch[0]: mismatch flag, scratch[1]: most blocks of a tile,
 // scratch[2]: most plan entries of a tile's 16-byte aligned entry range).
 __global__ void tile_check_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ eblock,
                                   const uint32_t* __restrict__ row_block, uint32_t nv,
@@ -122,7 +121,7 @@ __global__ void tile_check_kernel(const uint32_t* __restrict__ row_ptr, const ui
   }
   if (i % kTileRows == 0) {
     const uint32_t r1 = min(i + kTileRows, nv);
-    atomicMax(scratch + 1, ((row_block[r1] + 3u) & ~3u) - (ub & ~3u));
+    atomicMax(scratch + 1, row_block[r1] - ub);
     atomicMax(scratch + 2, ((row_ptr[r1] + 3u) & ~3u) - (e0 & ~3u));
   }
 }

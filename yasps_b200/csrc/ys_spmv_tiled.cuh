@@ -26,20 +26,20 @@ namespace ys {
 
 constexpr uint32_t kTileRows = YS_SPMV_TILE_ROWS;
 constexpr int kTileThreads = kTileRows * kRowLanes;  // a thread group of kRowLanes a row
-constexpr uint32_t kTileSlotBytes = 4 * kFp32BlockStride;  // one FP32 block (36 B)
+constexpr uint32_t kTileSlotBytes = 4 * kFp32BlockStride;  // one FP32 block slot (48 B)
 // try_wait polls before a CTA stops using shared memory (the copies are a
 // few tens of KB and land within microseconds; the bound only keeps a stuck
 // copy from hanging the device)
 constexpr uint32_t kTileWaitPolls = 1u << 22;
 
 struct TiledSet {
-  const float* values32;       // 9 floats a block, (row, col)-sorted upper blocks
+  const float* values32;       // 12-float slots, (row, col)-sorted upper blocks
   const uint32_t* row_ptr;     // row plan (ys_spmv_plan_build), num_vars + 4 entries
   const uint32_t* entry_block; // both hold (row_ptr[nv] + 3) & ~3 entries at least
   const uint32_t* entry_col;
   const uint32_t* row_block;   // [nv + 4] first stored block of each row
   uint32_t nv;
-  uint32_t tile_cap;           // most blocks of one tile's 4-block aligned range
+  uint32_t tile_cap;           // most blocks of one tile
   uint32_t entry_cap;          // most plan entries of one tile, 4-aligned range
   uint32_t stages;             // stage buffers in shared memory (2 .. kMaxStages)
 };
@@ -111,16 +111,18 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
-// A staged block: 9 floats, 36-byte stride (an odd word stride, so the lanes
-// of a row group reading consecutive blocks hit distinct banks).
+// A staged block slot: three 16-byte shared loads (the 12-word slot stride
+// spreads the 8 lanes of a row group over distinct banks).
 __device__ __forceinline__ void load_slot(const float* __restrict__ p, float (&b)[9]) {
-#pragma unroll
-  for (int k = 0; k < 9; ++k) b[k] = p[k];
+  const float4* q = reinterpret_cast<const float4*>(p);
+  const float4 v0 = q[0], v1 = q[1], v2 = q[2];
+  b[0] = v0.x; b[1] = v0.y; b[2] = v0.z; b[3] = v0.w;
+  b[4] = v1.x; b[5] = v1.y; b[6] = v1.z; b[7] = v1.w;
+  b[8] = v2.x;
 }
 
 // One staged tile: pointers into a stage buffer and the global ranges they
-// hold (blocks [b0, ...) from the 4-aligned block before the tile's first,
-// plan entries [e0a, ...), rows [r0, ...]).
+// hold (blocks [b0, ...), plan entries [e0a, ...), rows [r0, ...]).
 struct TileStage {
   const float* blocks;
   const uint32_t* cols;
@@ -256,8 +258,8 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
     const uint32_t t = blockIdx.x + q * gridDim.x;
     const uint32_t buf = q % stages;
     const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, T.nv);
-    // whole 4-block groups (144 bytes) and 4-entry groups: 16-byte aligned
-    const uint32_t b0 = nxt[0] & ~3u, b1 = (nxt[1] + 3u) & ~3u, e0a = nxt[2] & ~3u, e1a = (nxt[3] + 3u) & ~3u;
+    // block slots are 48 bytes; entries move in 4-entry groups: 16-byte aligned
+    const uint32_t b0 = nxt[0], b1 = nxt[1], e0a = nxt[2] & ~3u, e1a = (nxt[3] + 3u) & ~3u;
     // rows r0 .. r1 (inclusive) rounded up to 4 words: at most num_vars + 4
     const uint32_t vb = (b1 - b0) * kTileSlotBytes, eb = (e1a - e0a) * 4u, rb = ((r1 - r0 + 4u) & ~3u) * 4u;
     float* dst = stage_base + buf * buf_floats;
@@ -299,7 +301,7 @@ __device__ __forceinline__ void spmv3_tiles_x32(const TiledSet& T, const float4*
       const uint32_t* rblk = reinterpret_cast<const uint32_t*>(base + (uint64_t)kFp32BlockStride * T.tile_cap) +
                              2ull * T.entry_cap + kTileRowWords;
       const uint32_t* rp = rblk - kTileRowWords;
-      const TileStage S = stage_view(T, base, r0, rblk[0] & ~3u, rp[0] & ~3u);
+      const TileStage S = stage_view(T, base, r0, rblk[0], rp[0] & ~3u);
       tile_row_staged(T, S, x32, iA, iA < r1, lane, yA[0], yA[1], yA[2]);
     } else {
       SpmvSet g{nullptr, T.values32, T.row_ptr, T.entry_block, T.entry_col};

@@ -56,9 +56,8 @@ class vector:
 
 
 def fp32_slots(num_blocks: int) -> int:
-  """Floats of the FP32 copy of a 3x3 block set: 9 a block, padded to whole
-  groups of 4 blocks (the tiled SpMV copies 144-byte groups)."""
-  return 36 * max((int(num_blocks) + 3) // 4, 1)
+  """Floats of the FP32 copy of a 3x3 block set (16-byte aligned 12-float slots)."""
+  return max(12 * int(num_blocks), 12)
 
 
 class _Term:
@@ -706,9 +705,9 @@ class hessian:
       return
     for bs in self.block_sets:
       nu = bs.pattern.num_unique
-      v = torch.zeros(fp32_slots(nu), dtype=torch.float32, device=_dev())
-      v[:9 * nu] = bs.values[:9 * nu].to(torch.float32)
-      bs.values32 = v
+      v = torch.zeros((max(nu, 1), 12), dtype=torch.float32, device=_dev())
+      v[:nu, :9] = bs.values[:9 * nu].view(nu, 9).to(torch.float32)
+      bs.values32 = v.reshape(-1)
     self.values32_current = True
 
   def spmv_plan(self, bs: _BlockSet):
