@@ -19,8 +19,11 @@ beside the serial plain FP64 path, solves/s and p50/p99 latency (rank 0, N=1).
 ``cloth_contact``: Newton steps of the mixed cloth + affine bodies + contact
 scene (StVK, bending, 16 icosphere bodies, 200k barrier pairs, friction) in
 both precision forms (rank 0, N=1).
-``--impl reference``: the CPU restatement of the reference path (oracle) on
-a bounded sample of the same workload (rank 0 only).
+``error_vs_oracle``: the device gradient, assembled Hessian and solutions
+against one whole FP64 CPU Newton step of the same workload (oracle), which
+is also ``cpu_baseline`` (rank 0, N=1).
+``--impl reference``: whole CPU Newton steps of the same workload (the oracle
+restatement of the reference path), rank 0 only.
 
 Launch: ``python bench.py --gpus N --steps K --warmup W``; for N>1 under
 torchrun every rank solves its own independent scene (replicas, weak scaling).
@@ -224,6 +227,9 @@ def gpu_arm(args):
   stats = dict(solver.statistics)
   impl = solver.implementation
   rel_res = float(getattr(impl, "final_relative_residual", float("nan")))
+  Hs = mz.activeHessian()
+  device_out = {"g": Hs.gradient.value.cpu().numpy(), "pos": Hs.block_positions.cpu().numpy(),
+                "val": Hs.blocks_flattened.cpu().numpy(), "x": {"fp32_refine": impl.solution.cpu().numpy()}}
   value = replica_value(world, args.steps, ms)
   lat_ms = sorted(1e3 * x for x in lat)
   levels = len(impl.hierarchy.levels)
@@ -236,6 +242,7 @@ def gpu_arm(args):
   ms64, _ = time_steps(step, max(3, args.steps // 3), pg)
   fp64_value = replica_value(world, max(3, args.steps // 3), ms64)
   stats64 = dict(solver64.statistics)
+  device_out["x"]["fp64"] = solver64.implementation.solution.cpu().numpy()
   # end to end through the public API with host buffers
   mz.setSolver("mas", mixed_spmv=True, stop_rule="residual")
   host_pos = torch.from_numpy(np.ascontiguousarray(cube.free_position.reshape(-1))).pin_memory()
@@ -251,7 +258,7 @@ def gpu_arm(args):
     e2e_step()
   ms_e2e, _ = time_steps(e2e_step, max(3, args.steps // 3), pg)
   e2e_value = replica_value(world, max(3, args.steps // 3), ms_e2e)
-  # roofline of the dominant kernel (MAS domain GEMV), timed on its own stream
+  # roofline of the MAS domain GEMV, timed on its own stream
   ms_solver = mz.linearSolver.implementation
   H = mz.activeHessian()
   import ctypes
@@ -274,10 +281,12 @@ def gpu_arm(args):
   # scaled by this launch's layout bytes (traffic grows with the domains)
   from yasps_b200.kernelbench import gemv_layout_bytes
   traffic = (109.60e6 + 7.08e6) / GEMV_LAYOUT_56 * gemv_layout_bytes(ms_solver._tables)
-  roofline = {"kernel": "mas_gemv (MAS domain-inverse apply, FP32)", "bound": "hbm", "achieved": achieved,
-              "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-              "traffic": traffic, "bytes_per_launch": int(nbytes.value), "ms_per_launch": gemv_ms}
-  roofline_spmv = spmv_roofline(mz.activeHessian(), hbm, peak_kind)
+  roofline_gemv = {"kernel": "mas_gemv (MAS domain-inverse apply, FP32)", "bound": "hbm", "achieved": achieved,
+                   "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                   "traffic": traffic, "bytes_per_launch": int(nbytes.value), "ms_per_launch": gemv_ms}
+  # the headline roofline is the step's dominant kernel: the SpMV of the PCG
+  # loop (one launch an iteration)
+  roofline = spmv_roofline(mz.activeHessian(), hbm, peak_kind, args.side)
   # the host-bound serving loop runs before the CPU baseline, whose worker
   # threads would otherwise compete with it for the host cores
   serve = None
@@ -286,9 +295,10 @@ def gpu_arm(args):
   cloth = None
   if rank == 0 and world == 1 and not args.no_cloth:
     cloth = cloth_leg(args)
-  cpu = None
+  cpu, err = None, None
   if rank == 0 and world == 1 and not args.no_cpu_baseline:
-    cpu = cpu_baseline_leg(cube, args.tol)
+    cpu, err = cpu_step_leg(cube, args.tol, (device_out["g"], device_out["pos"], device_out["val"],
+                                             device_out["x"]))
   line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
           "vs_baseline": None, "dtype": "f32+f64 refine (f64 element Hessians and projection)",
@@ -301,8 +311,8 @@ def gpu_arm(args):
           "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * cube.dofs,
                   "d2h_bytes_per_step": 8 * cube.dofs},
           "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
-          "roofline_spmv": roofline_spmv, "clocks": clk,
-          "cpu_baseline": cpu, "serving": serve, "cloth_contact": cloth}
+          "roofline_gemv": roofline_gemv, "clocks": clk,
+          "cpu_baseline": cpu, "error_vs_oracle": err, "serving": serve, "cloth_contact": cloth}
   if rank == 0:
     print(json.dumps(line), flush=True)
   if pg is not None:
@@ -312,15 +322,25 @@ def gpu_arm(args):
 GEMV_LAYOUT_56 = 111_651_744  # tiled-layout bytes of one domain-GEMV launch on the 56^3 cube
 
 
-def spmv_roofline(H, hbm, peak_kind, reps=50):
-  """The FP32 block SpMV of the PCG loop (FP32 blocks, float4 copy of the
-  direction) timed alone with CUDA events.  Algorithmic bytes: 9 floats per
-  stored upper block, (block, column) indices and the row pointer, x read
-  once (3 floats a variable) and y written once (3 doubles)."""
+# DRAM bytes (read + write) of one tiled SpMV launch on this 64^3 workload,
+# from an ncu capture of the same launch (dram__bytes_read.sum +
+# dram__bytes_write.sum); None on other sizes
+SPMV_TILED_TRAFFIC_64 = None
+
+
+def spmv_roofline(H, hbm, peak_kind, side, reps=50):
+  """The SpMV of the FP32 PCG loop (the tiled kernel: FP32 block slots,
+  plan entries and row pointers staged in shared memory by bulk copies,
+  the float4 copy of the direction gathered) timed alone with CUDA events
+  over `reps` launches on its stream.  Algorithmic bytes per launch (the
+  symmetric storage's own count): nb (9 * 4 + 8) for the stored FP32
+  blocks and two 32-bit indices each, plus the vector read and the product
+  written once in FP64, 2 * 8 * n."""
   import torch
   from yasps_b200 import _lib as L
   bs = H.block_sets[0]
   row_ptr, eb, ec = H.spmv_plan(bs)
+  row_block, cap, ecap = H.tile_plan(bs)
   nv = H.rows // 3
   entries = int(row_ptr[nv].item())
   x = torch.cos(torch.arange(H.rows, dtype=torch.float64, device="cuda") * 0.37)
@@ -328,8 +348,8 @@ def spmv_roofline(H, hbm, peak_kind, reps=50):
   y = torch.empty_like(x)
   s = torch.cuda.current_stream()
   L.call("ys_pack_x32", L.ptr(x), nv, L.ptr(x32), s.cuda_stream)
-  call = lambda: L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32),
-                        L.ptr(y), 0, s.cuda_stream)
+  call = lambda: L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec),
+                        L.ptr(row_block), cap, ecap, 0, nv, L.ptr(x32), L.ptr(y), 0, None, s.cuda_stream)
   for _ in range(3):
     call()
   torch.cuda.synchronize()
@@ -340,12 +360,13 @@ def spmv_roofline(H, hbm, peak_kind, reps=50):
   e1.record(s)
   torch.cuda.synchronize()
   ms = e0.elapsed_time(e1) / reps
-  nbytes = 36 * bs.pattern.num_unique + 8 * entries + 4 * (nv + 1) + 12 * nv + 24 * nv
+  nb = bs.pattern.num_unique
+  nbytes = nb * (9 * 4 + 8) + 2 * 8 * H.rows
   achieved = nbytes / (ms / 1e3) / 1e9
-  return {"kernel": "spmv3_x32 (symmetric 3x3 block SpMV, FP32 blocks)", "bound": "hbm", "achieved": achieved,
-          "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-          "bytes_per_launch": nbytes, "ms_per_launch": ms, "stored_blocks": bs.pattern.num_unique,
-          "entries": entries}
+  return {"kernel": "spmv3_x32_tiled (symmetric 3x3 block SpMV of the FP32 PCG loop)", "bound": "hbm",
+          "achieved": achieved, "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+          "traffic": SPMV_TILED_TRAFFIC_64 if side == 64 else None, "bytes_per_launch": nbytes,
+          "ms_per_launch": ms, "stored_blocks": nb, "entries": entries, "tile_cap": cap, "entry_cap": ecap}
 
 
 def launches_per_newton_step(impl, its, refs):
@@ -449,41 +470,102 @@ def serving_leg(args):
   return out
 
 
-def cpu_baseline_leg(cube, tol):
+def blocks_to_csr(positions, values, n):
+  """Symmetric CSR of upper 3x3 block storage (scalar block offsets)."""
+  import scipy.sparse as sp
+  pos = np.asarray(positions, dtype=np.int64).reshape(-1, 2)
+  vals = np.asarray(values, dtype=np.float64)[:9 * len(pos)].reshape(-1, 3, 3)
+  k = np.arange(3)
+  rows = (pos[:, 0, None, None] + k[None, :, None]).repeat(3, axis=2)
+  cols = (pos[:, 1, None, None] + k[None, None, :]).repeat(3, axis=1)
+  up = sp.coo_matrix((vals.ravel(), (rows.ravel(), cols.ravel())), shape=(n, n)).tocsr()
+  off = pos[:, 0] != pos[:, 1]
+  lo = sp.coo_matrix((vals[off].ravel(), (rows[off].ravel(), cols[off].ravel())), shape=(n, n)).tocsr().T
+  return (up + lo).tocsr()
+
+
+def cpu_step_leg(cube, tol, gpu=None):
+  """One whole, unsampled CPU Newton step of the workload (the oracle's
+  restatement of the reference's CPU path: every element, the full MAS
+  update, MAS-PCG to the target), timed; and, with ``gpu`` = (g, positions,
+  values, {name: x}) from the device, the device's error against this FP64
+  oracle: gradient and assembled Hessian (largest entry difference relative
+  to the largest entry) and the true relative residual ``||g - H x|| / ||g||``
+  of each device solution under the oracle's g and H."""
   from oracle import baseline
-  threads = os.cpu_count() or 1
-  g, H, mas, its = baseline.prepare(cube, tol=tol)
-  total, info = baseline.timed_sample(cube, H, g, mas, its)
-  return {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "port",
-          "sample": (f"oracle (NumPy/SciPy, {threads} host threads): SNH eval+projection+assembly on "
-                     f"{info['sample_fraction']:.4f} of the tets and MAS update on the same fraction of level-0 "
-                     f"domains, scaled; {info['iterations']} MAS-PCG iterations from a full CPU solve to 1e-6 "
-                     f"timed per iteration"), "breakdown_s": info}
+  t0 = time.perf_counter()
+  pool = baseline.ElementPool(cube)
+  threads = pool.workers
+  try:
+    g0, H0 = pool.assemble()
+    mas = baseline.CpuMas(H0, cube.free_count)
+    setup_s = time.perf_counter() - t0
+    g, H, x, its, phases = baseline.cpu_newton_step(cube, mas, tol=tol, pool=pool)
+  finally:
+    pool.close()
+  cpu = {"value": 1.0 / phases["total_s"], "unit": "solves/s", "cores": threads, "kind": "port",
+         "sample": (f"one whole Newton step of the same workload, unsampled (oracle NumPy/SciPy restatement "
+                    f"of the reference CPU path; elements on {threads} worker processes, BLAS threads for the "
+                    f"rest): all {cube.tet_count} tets' SNH + projection + assembly, the MAS update of every "
+                    f"domain, {its} MAS-PCG iterations to the target residual; hierarchy built once beforehand "
+                    f"({setup_s:.1f} s with the first assembly, cached per structure as in the reference)"),
+         "steps_timed": 1, "breakdown_s": phases}
+  err = None
+  if gpu is not None:
+    g_dev, pos_dev, val_dev, xs = gpu
+    Hd = blocks_to_csr(pos_dev, val_dev, cube.dofs)
+    gn = float(np.linalg.norm(g))
+    err = {"oracle": "FP64 CPU restatement, same seeded inputs",
+           "gradient_rel_max": float(np.abs(g_dev - g).max() / np.abs(g).max()),
+           "hessian_rel_max": float(abs(Hd - H).max() / abs(H).max()),
+           "cpu_solution_rel_residual": float(np.linalg.norm(g - H @ x) / gn)}
+    for name, xd in xs.items():
+      err[f"{name}_rel_residual"] = float(np.linalg.norm(g - H @ xd) / gn)
+  return cpu, err
 
 
 def reference_arm(args):
+  """Whole, unsampled CPU Newton steps of the workload (the oracle port of
+  the reference's CPU path; the reference itself is Python and does not
+  travel to the GPU box).  Steps are timed whole, after one untimed
+  assembly: the requested count, or fewer when the next step would take the
+  timed region past two minutes (at least one); the line says how many ran."""
   rank = int(os.environ.get("RANK", "0"))
   if rank != 0:
     return
   from oracle import baseline
   cube = workload(args.side, seed=0)
-  g, H, mas, its = baseline.prepare(cube, tol=args.tol)
-  for _ in range(args.warmup):
-    baseline.timed_sample(cube, H, g, mas, its)
-  totals = []
-  for _ in range(args.steps):
-    t, info = baseline.timed_sample(cube, H, g, mas, its)
-    totals.append(t)
-  value = 1.0 / float(np.mean(totals))
-  threads = os.cpu_count() or 1
+  pool = baseline.ElementPool(cube)
+  threads = pool.workers
+  try:
+    g0, H0 = pool.assemble()  # warm-up: the first assembly
+    mas = baseline.CpuMas(H0, cube.free_count)
+    totals, its = [], 0
+    t0 = time.perf_counter()
+    while len(totals) < args.steps:
+      _, _, _, its, ph = baseline.cpu_newton_step(cube, mas, tol=args.tol, pool=pool)
+      totals.append(ph["total_s"])
+      if time.perf_counter() - t0 + ph["total_s"] > 120.0:
+        break
+    wall = time.perf_counter() - t0
+  finally:
+    pool.close()
+  steps = len(totals)
+  value = steps / wall
   cpu = {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-         "sample": (f"oracle restatement of the reference CPU path: SNH+projection+assembly and MAS update on "
-                    f"{info['sample_fraction']:.4f} of the work scaled up, {its} MAS-PCG iterations timed per "
-                    f"iteration")}
+         "sample": (f"{steps} whole Newton steps timed (of {args.steps} requested; the timed region stops before "
+                    f"it would pass 120 s), unsampled: every tet, the full MAS update, {its} MAS-PCG iterations to "
+                    f"1e-6 true relative residual; oracle NumPy/SciPy restatement of the reference CPU path, "
+                    f"elements on {threads} worker processes"),
+         "steps_timed": steps}
+  lat = sorted(1e3 * t for t in totals)
   line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1,
-          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
-          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded FEM cube)",
+          "steps": steps, "steps_requested": args.steps, "warmup": args.warmup, "warmup_done": 1,
+          "ms_per_step": 1e3 * wall / steps,
+          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+          "data": "synthetic (seeded FEM cube)",
           "config": config(cube, {"parallelism": "cpu", "path": "fp64", "iterations": its}),
+          "p50_ms": lat[len(lat) // 2], "p99_ms": lat[-1],
           "cpu_baseline": cpu, "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                                        "d2h_bytes_per_step": 0}}
   print(json.dumps(line), flush=True)

@@ -12,6 +12,7 @@ chunk ordering of ``oracle/mas.py``.
 
 from __future__ import annotations
 
+import os
 import time
 
 import numpy as np
@@ -145,6 +146,72 @@ def assemble_chunked(cube, chunk=200_000):
     g -= (k - 1) * gi.ravel()
     H = H - (k - 1) * sp.diags(np.repeat(cube.mass, 3))
   return g, H.tocsr()
+
+
+_POOL_CUBE = None
+
+
+def _pool_init(cube):
+  global _POOL_CUBE
+  _POOL_CUBE = cube
+
+
+def _pool_chunk(bounds):
+  return system_from_cube(_POOL_CUBE, slice(*bounds))
+
+
+class ElementPool:
+  """Worker processes (spawned: safe next to a CUDA context) that evaluate
+  the element terms of the cube in chunks, so the CPU step uses every host
+  core; created once, reused by every step."""
+
+  def __init__(self, cube, workers=None):
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    self.workers = max(1, int(workers or os.cpu_count() or 1))
+    self.cube = cube
+    self.ex = cf.ProcessPoolExecutor(self.workers, mp_context=mp.get_context("spawn"), initializer=_pool_init,
+                                     initargs=(cube,))
+    # start and import in every worker (bounded: a worker that cannot start
+    # raises instead of waiting forever)
+    list(self.ex.map(_pool_chunk, [(0, 1)] * self.workers, timeout=300))
+
+  def assemble(self):
+    """Gradient + Hessian of the whole cube (chunks spread over the workers)."""
+    nt = self.cube.tet_count
+    step = max(1, (nt + 4 * self.workers - 1) // (4 * self.workers))
+    chunks = [(s, min(nt, s + step)) for s in range(0, nt, step)]
+    g, H = None, None
+    for gi, Hi in self.ex.map(_pool_chunk, chunks, timeout=1800):
+      g = gi if g is None else g + gi
+      H = Hi if H is None else H + Hi
+    k = len(chunks)
+    if k > 1:  # the inertia term is in every chunk: keep one copy
+      _, gi, _ = energies.inertia_local(self.cube.free_position, self.cube.x_tilde(), self.cube.mass)
+      g -= (k - 1) * gi.ravel()
+      H = H - (k - 1) * sp.diags(np.repeat(self.cube.mass, 3))
+    return g, H.tocsr()
+
+  def close(self):
+    self.ex.shutdown()
+
+
+def cpu_newton_step(cube, mas, tol=1e-6, maxit=1000, pool=None):
+  """One whole, unsampled CPU Newton step of the cube (element evaluation,
+  projection and assembly of every tetrahedron, the MAS numeric update of
+  every domain, MAS-PCG to ``||g - H x|| <= tol ||g||``), timed phase by
+  phase; the element phase runs on ``pool`` (an :class:`ElementPool`) when
+  given.  ``mas`` carries the hierarchy (built once per structure, as the
+  reference caches it) and is updated in place.  Returns
+  ``(g, H, x, iterations, seconds_by_phase)``."""
+  t0 = time.perf_counter()
+  g, H = pool.assemble() if pool is not None else assemble_chunked(cube)
+  t1 = time.perf_counter()
+  mas.update(H)
+  t2 = time.perf_counter()
+  x, its = pcg(H, g, mas, tol, maxit)
+  t3 = time.perf_counter()
+  return g, H, x, its, dict(element_s=t1 - t0, mas_update_s=t2 - t1, pcg_s=t3 - t2, total_s=t3 - t0)
 
 
 def prepare(cube, tol=1e-6, maxit=1000):
