@@ -369,6 +369,26 @@ def spmv_roofline(H, hbm, peak_kind, side, reps=50):
           "ms_per_launch": ms, "stored_blocks": nb, "entries": entries, "tile_cap": cap, "entry_cap": ecap}
 
 
+def served_oracle_check(done, seed, count=8, max_side=30):
+  """True relative residual ||g - H x|| / ||g|| of a sample of served
+  solutions under g and H assembled by the FP64 oracle from the same request
+  (cube side, material, seeded positions): the `count` requests of smallest
+  side up to `max_side` (the oracle assembles serially)."""
+  import dataclasses
+  from oracle import solvers
+  from tests.oracle_scene import OracleCube
+  from yasps_b200 import scenes
+  pick = sorted((r for r in done if r.side <= max_side), key=lambda r: (r.side, r.tag))[:count]
+  res = []
+  for r in pick:
+    cube = scenes.fem_cube(r.side, noise=0.01, seed=seed * 1000003 + int(r.tag))
+    cube = dataclasses.replace(cube, mu=r.mu, lam=r.lam)
+    ora = OracleCube(cube)
+    res.append(solvers.relative_residual(ora.matvec, ora.gradient, r.solution))
+  return {"oracle": "FP64 CPU assembly of each sampled request", "requests": [int(r.tag) for r in pick],
+          "sides": [int(r.side) for r in pick], "rel_residuals": res, "max_rel_residual": max(res) if res else None}
+
+
 def launches_per_newton_step(impl, its, refs):
   """Kernels of this library launched in one Newton step of the precision form.
 
@@ -424,6 +444,14 @@ def cloth_leg(args):
     st = solver.statistics
     out[name] = {"solves_per_s": 5 / (ms / 1e3), "ms_per_step": ms / 5, "iterations": int(st["iterations"]),
                  "refinements": int(st.get("refinements", 0))}
+    # the solution checked on the host in FP64 against the FP64 system the
+    # device assembled (each element kind of it matches the oracle in the
+    # tests): an independent residual, not the solver's own
+    Hc = mz.activeHessian()
+    A = blocks_to_csr(Hc.block_positions.cpu().numpy(), Hc.blocks_flattened.cpu().numpy(), Hc.rows)
+    g = Hc.gradient.value.cpu().numpy()
+    x = solver.implementation.solution.cpu().numpy()
+    out[name]["host_fp64_rel_residual"] = float(np.linalg.norm(g - A @ x) / np.linalg.norm(g))
   impl = mz.linearSolver.implementation
   out["dof"] = mz.activeHessian().rows
   out["blocks"] = int(mz.activeHessian()._static.pattern.num_unique)
@@ -457,6 +485,7 @@ def serving_leg(args):
   done = srv.run(serving.poisson_fem_stream(count=n, mean_spacing=2e-3, seed=0))
   out["served"] = serving.stream_stats(done)
   out["served"]["max_rel_residual"] = max(r.relative_residual for r in done)
+  out["served"]["error_vs_oracle"] = served_oracle_check(done, seed=0)
   out["served_saturated"] = serving.stream_stats(
       srv.run(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=0)))
   out["serial_fp64"] = serving.stream_stats(
