@@ -307,15 +307,18 @@ typedef struct ys_affine_args {
 int32_t ys_affine_eval(const ys_affine_args* args, void* stream);
 
 /* ---- contact through affine-body vertices --------------------------------
- * The PP / PE / PT / EE barriers of ys_energy_eval over a position union one
- * child of which is the vertices of affine bodies, whose position is the
- * computed x = A_b xbar + t_b (the collision union [soft, abd, container] of
+ * The PP / PE / PT / EE barriers and the four lagged friction kinds of
+ * ys_energy_eval over a position union one child of which is the vertices of
+ * affine bodies, whose position is the computed x = A_b xbar + t_b (the
+ * collision union [soft, abd, container] of
  * examples/dropping_in_container_mixed/dropping_in_container.py:344, and
- * :270 for the position).  The reference differentiates such a pair with
- * respect to the leaves of every vertex (a free position, or the A and t of
- * its body), merges repeated leaves (one body's A and t seen from several
- * vertices), and projects the compressed local Hessian, up to 24x24
- * (hessianKernelFullProject.pyx:95-139).
+ * :270 for the position).  The map from the leaves (a free position, or the
+ * A and t of a vertex's body) to the pair's vertex positions is linear, so
+ * the reference projects the Hessian with respect to the vertex positions
+ * (3V x 3V) and maps it to the leaves, J^T proj(H) J, merging repeated
+ * leaves (one body's A and t seen from several vertices)
+ * (PKG/differentiator/differentiator.pyx:795-799; the reference's test
+ * expectation tests/differentiator/test_hessian_sparsity_permutation_gpu.py:269).
  *
  * Codes (ys_coupled_indices): K = 4 slots per vertex, slot stride 1; a plain
  * vertex fills its first slot (target position code, 1 for a non-target
@@ -324,30 +327,23 @@ int32_t ys_affine_eval(const ys_affine_args* args, void* stream);
  * (wrt_start_A + 3 (3b + r) + 2) and t (wrt_start_t + 3b + 2).  Compression,
  * coordinates and the pattern then work unchanged (A as three 3-DoF rows).
  *
- * Evaluation (ys_coupled_energy_eval): the barrier's value, gradient and
- * Hessian in the 3V vertex coordinates, then the chain rule through the
- * linear map Jhat (vertex coordinates <- compressed leaves).  Projection of
- * Hc = Jhat^T H Jhat: with M = Jhat Jhat^T = m (x) I3, m the VxV Gram matrix
- * of [xbar; 1] over the vertices of one body (1 on a plain vertex), and
- * L = chol(m) (x) I3, Hc has the nonzero spectrum of S = L^T H L and its
- * eigenvectors are Jhat^T L^-T u for S u = lambda u.  So S (3V x 3V) takes
- * the PSD test and the negative-mode projection, and the change S' - S goes
- * back as H' = H + L^-T (S' - S) L^-1 before the merge: the projected
- * compressed Hessian of the reference, from a 12x12 eigenproblem at most.
- * The PSD short-circuit tolerance applies to S's diagonal (the reference's
- * to Hc's).  Elements without an affine vertex take the plain path exactly.
- * Body vertices of one element must be affinely independent (m positive
- * definite); an element that is not sets *status to its index + 1 (first
- * one wins) and is written unprojected.                                   */
+ * Evaluation (ys_coupled_energy_eval): the energy's value, gradient and
+ * Hessian in the 3V vertex coordinates, the PSD test and negative-mode
+ * projection of that Hessian, then the chain rule through the linear map
+ * Jhat (vertex coordinates <- compressed leaves), written merged per leaf.
+ * Friction kinds read base.rest (the old positions of the union's vertices,
+ * same child layout) and base.params (9 lagged values per element).  An
+ * element naming a vertex outside the union or a body beyond num_bodies sets
+ * *status to its index + 1 (first one wins) and is skipped.              */
 typedef struct ys_coupled_args {
-  ys_energy_args base;          /* kind PP/PE/PT/EE; base.position child `affine_child` unused */
+  ys_energy_args base;          /* barrier or friction kind; base.position child `affine_child` unused */
   uint32_t affine_child;        /* union child of the affine-body vertices                   */
   const uint32_t* vertex_body;  /* [affine vertices] body of each                            */
   const double* rest;           /* [affine vertices x 3] body-frame rest position xbar      */
   const double* affine;         /* [num_bodies x 9] A per body, row-major                    */
   const double* translation;    /* [num_bodies x 3] t per body                               */
   uint32_t num_bodies;
-  int32_t* status;              /* [1] or NULL: first element (+1) with dependent body vertices */
+  int32_t* status;              /* [1] or NULL: first element (+1) with an invalid vertex    */
 } ys_coupled_args;
 
 int32_t ys_coupled_indices(const uint32_t* connectivity, uint32_t n, uint32_t arity, uint32_t num_children,

@@ -56,15 +56,44 @@ def _squared_distance(kind, x):
   return float(np.dot(x[2] - x[0], b) ** 2 / np.dot(b, b))
 
 
-def scene(s, method):
+FRICTION = {"pp": 11, "pe": 9, "pt": 8, "ee": 10}
+
+
+def add_friction(s, seed=0):
+  """Lagged friction over the same pairs: union positions at the start of
+  the step a small seeded move away, the lagged data of each pair from them
+  (the oracle's restatement of the reference's friction helpers)."""
+  from oracle import vertex_energies as ve
+  rng = np.random.default_rng(100 + seed)
+  allpos = union_positions(s)
+  last = allpos + rng.uniform(-2e-3, 2e-3, allpos.shape)
+  lagged = {}
+  for key, conn in s["pairs"].items():
+    lagged[key] = np.stack([ve.LAGGED[FRICTION[key]](last[c.astype(np.int64)], s["dhat"], s["kappa"])
+                            for c in conn])
+  s["friction"] = dict(last=last, fdhat=1e-6, rate=0.3, lagged=lagged)
+  return s
+
+
+def union_positions(s):
+  return np.concatenate([s["cloth"], s["bodies"].positions(), s["container"]])
+
+
+def scene(s, method, separate_hessian_jacobian=False):
   from yasps_b200 import scenes
+  fr = None
+  if "friction" in s:
+    f = s["friction"]
+    fr = dict(last=f["last"], fdhat=f["fdhat"], rate=f["rate"])
+    fr.update({k: (s["pairs"][k], f["lagged"][k]) for k in s["pairs"]})
   return scenes.contact_with_bodies_scene(s["cloth"], s["bodies"], s["container"], s["pairs"], s["dhat"],
-                                          s["kappa"], projection_method=method)
+                                          s["kappa"], projection_method=method, friction=fr,
+                                          separate_hessian_jacobian=separate_hessian_jacobian)
 
 
 def oracle_assembly(s, method):
-  """(dense H, gradient, energy total) of the barrier terms, targets
-  [cloth, A (three rows a body), t]."""
+  """(dense H, gradient, energy total) of the barrier terms (and the friction
+  terms when the scene has them), targets [cloth, A (three rows a body), t]."""
   cloth, bodies, container = s["cloth"], s["bodies"], s["container"]
   nc, nv, nb = len(cloth), len(bodies.rest), bodies.num_bodies
   start_a, start_t = 3 * nc, 3 * nc + 9 * nb
@@ -72,8 +101,13 @@ def oracle_assembly(s, method):
   A = bodies.affine
   terms = []
   energy = 0.0
-  for key, arity in (("pp", 2), ("pe", 3), ("pt", 4), ("ee", 4)):
+  kinds = [(key, arity, KIND[key]) for key, arity in (("pp", 2), ("pe", 3), ("pt", 4), ("ee", 4))]
+  if "friction" in s:
+    kinds += [(key, arity, FRICTION[key]) for key, arity in (("pp", 2), ("pe", 3), ("pt", 4), ("ee", 4))]
+  last = s["friction"]["last"] if "friction" in s else None
+  for key, arity, ekind in kinds:
     conn = s["pairs"][key].astype(np.int64)
+    fric = ekind in FRICTION.values()
     K = 4 * arity
     codes_t = np.zeros((len(conn), K), dtype=np.int64)
     sizes_t = np.zeros((len(conn), K), dtype=np.int64)
@@ -101,8 +135,14 @@ def oracle_assembly(s, method):
           codes.extend([1, 0, 0, 0])
         else:
           codes.extend([start_a + 3 * (3 * i + r) + 2 for r in range(3)] + [start_t + 3 * i + 2])
-      en, codes_c, sizes_c, g_c, h_c = cc.local_compressed(KIND[key], verts, np.asarray(codes),
-                                                           (s["dhat"], s["kappa"]), method)
+      if fric:
+        f = s["friction"]
+        en, codes_c, sizes_c, g_c, h_c = cc.local_compressed(ekind, verts, np.asarray(codes),
+                                                             (f["fdhat"], 0.01, f["rate"]), method,
+                                                             lagged=f["lagged"][key][e], rest=last[row])
+      else:
+        en, codes_c, sizes_c, g_c, h_c = cc.local_compressed(ekind, verts, np.asarray(codes),
+                                                             (s["dhat"], s["kappa"]), method)
       energy += en
       codes_t[e], sizes_t[e] = codes_c, sizes_c
       g_t[e, :g_c.size] = g_c

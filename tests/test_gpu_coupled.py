@@ -1,9 +1,8 @@
 """Barrier contact through affine-body vertices on the GPU against the oracle.
 
-The device evaluates each pair in vertex coordinates, projects ``L^T H L``
-and applies the chain rule to the body leaves; the oracle differentiates in
-the leaves, merges repeated ones and projects the merged matrix whole (up to
-24x24).  Compared: dense assembled matrix and gradient at 1e-12 relative to
+The device and the oracle evaluate each pair in vertex coordinates, project
+that Hessian (the reference's inner projection for a linear map from the
+leaves) and apply the chain rule to the body leaves, merging repeated ones.  Compared: dense assembled matrix and gradient at 1e-12 relative to
 the largest entry, energy total at 1e-12 relative; the rerun is
 bit-identical; a solve of the full scene (with inertia and orthogonality)
 through MAS reaches the stated true relative residual.
@@ -43,6 +42,29 @@ def test_coupled_assembly_matches_oracle(method):
   assert rel(H.gradient.value.cpu().numpy(), grad) <= 1e-12
   assert rel(_dense(H), dense) <= 1e-12
   assert abs(sc.computeTotalEnergy() - energy) <= 1e-12 * abs(energy)
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_coupled_friction_matches_oracle(method):
+  """Lagged friction of the four kinds through affine-body vertices (the
+  old positions through the same union), beside the barriers."""
+  s = cs.add_friction(cs.make(seed=3))
+  sc, _ = cs.scene(s, method)
+  H = sc.minimizer.computeNumericValue()
+  dense, grad, energy = cs.oracle_assembly(s, method)
+  assert rel(H.gradient.value.cpu().numpy(), grad) <= 1e-12
+  assert rel(_dense(H), dense) <= 1e-12
+  assert abs(sc.computeTotalEnergy() - energy) <= 1e-12 * abs(energy)
+
+
+def test_separate_hessian_jacobian_flag_gives_the_same_matrix():
+  """addEnergy(separate_hessian_jacobian=True) (the reference's explicit
+  J-block evaluation of J^T H J) assembles the same values bit for bit."""
+  s = cs.add_friction(cs.make(seed=3))
+  sc, _ = cs.scene(s, 2)
+  first = sc.minimizer.computeNumericValue().blocks_flattened.clone()
+  sc2, _ = cs.scene(s, 2, separate_hessian_jacobian=True)
+  assert bool((sc2.minimizer.computeNumericValue().blocks_flattened == first).all())
 
 
 def test_coupled_projection_is_exercised_and_reruns_bit_identical():

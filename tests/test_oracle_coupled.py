@@ -1,13 +1,13 @@
 """Contact through affine-body vertices, on the CPU.
 
-The reference projects the compressed local Hessian of a pair (leaves of
-plain vertices and of the bodies of abd vertices, repeated leaves merged) as
-a whole, up to 24x24.  The device projects ``S = L^T H L`` (3V x 3V, L from
-the Gram matrix of the element's body vertices) instead.  These tests check
-on random elements that both routes give the same compressed matrix, that
-the chain rule through ``x = A xbar + t`` matches autograd in the leaves,
-and that the projection is exercised.  Tolerance: 1e-11 relative to the
-largest entry.
+The reference projects the Hessian of a pair with respect to its vertex
+positions (3V x 3V) and maps it to the leaves (plain positions, body A rows
+and t) through the linear Jacobian of x = A xbar + t, merging repeated
+leaves: ``J^T proj(H) J``.  These tests check on random elements that the
+oracle's unprojected result equals autograd in the leaves (the chain rule,
+merged), that the projected one is ``J^T proj(H) J`` and positive
+semidefinite, and that the projection is exercised.  Tolerance: 1e-11
+relative to the largest entry.
 """
 
 import numpy as np
@@ -64,9 +64,58 @@ LAYOUTS = [
 ]
 
 
+def _leaf_autograd(kind, verts, codes, params):
+  """Gradient and Hessian by autograd directly in the leaves, repeated
+  leaves merged (sum of their rows and columns)."""
+  import torch
+  fn = ve.KINDS[kind]
+  slots = []
+  for v, d in enumerate(verts):
+    for s in range(4):
+      k = 4 * v + s
+      if codes[k] == 0:
+        continue
+      val = d[1] if d[0] == "p" else (d[1][3 * s:3 * s + 3] if s < 3 else d[2])
+      slots.append((k, np.asarray(val, dtype=np.float64)))
+  where = {k: i for i, (k, _) in enumerate(slots)}
+
+  def f(z):
+    xs = []
+    for v, d in enumerate(verts):
+      if d[0] == "p":
+        i = where[4 * v]
+        xs.append(z[3 * i:3 * i + 3])
+      else:
+        xbar = torch.tensor(np.asarray(d[3], dtype=np.float64))
+        rows = [z[3 * where[4 * v + r]:3 * where[4 * v + r] + 3] for r in range(3)]
+        tt = z[3 * where[4 * v + 3]:3 * where[4 * v + 3] + 3]
+        xs.append(torch.stack([torch.dot(rows[r], xbar) + tt[r] for r in range(3)]))
+    x = torch.stack(xs)
+    return fn(x, torch.zeros_like(x), params)
+
+  z0 = torch.tensor(np.concatenate([v for _, v in slots]))
+  g = torch.autograd.functional.jacobian(f, z0).numpy()
+  h = torch.autograd.functional.hessian(f, z0).numpy()
+  first, owner, keep = {}, [], []
+  for k, _ in slots:
+    c = int(codes[k])
+    if c >= 2 and c in first:
+      owner.append(first[c])
+      continue
+    if c >= 2:
+      first[c] = len(keep)
+    owner.append(len(keep))
+    keep.append(k)
+  P = np.zeros((3 * len(slots), 3 * len(keep)))
+  for i, o in enumerate(owner):
+    P[3 * i:3 * i + 3, 3 * o:3 * o + 3] = np.eye(3)
+  return P.T @ g, P.T @ h @ P
+
+
 @pytest.mark.parametrize("kind,layout", LAYOUTS)
 @pytest.mark.parametrize("method", [1, 2])
-def test_gram_route_matches_the_merged_projection(kind, layout, method):
+def test_inner_projection_through_the_leaf_jacobian(kind, layout, method):
+  from oracle import projection
   rng = np.random.default_rng(7 + 13 * kind + len(layout) + 101 * method)
   projected = 0
   for trial in range(6):
@@ -80,11 +129,12 @@ def test_gram_route_matches_the_merged_projection(kind, layout, method):
     e, codes_c, sizes_c, g_c, h_c = cc.local_compressed(kind, verts, codes, params, method)
     J = cc.jacobian(verts, codes)
     assert abs(e - e0[0]) <= 1e-13 * abs(e0[0])
-    assert rel(J.T @ g_x[0], g_c) <= 1e-11
+    g_leaf, h_leaf = _leaf_autograd(kind, verts, codes, params)
+    assert rel(g_c, g_leaf) <= 1e-11
     _, _, _, _, h_raw = cc.local_compressed(kind, verts, codes, params, 0)
-    assert rel(J.T @ h_x[0] @ J, h_raw) <= 1e-11
-    via = J.T @ cc.projected_via_gram(h_x[0], verts, method) @ J
-    assert rel(via, h_c) <= 1e-11
+    assert rel(h_raw, h_leaf) <= 1e-11
+    assert rel(h_c, J.T @ projection.project_spd(h_x[0], method) @ J) <= 1e-11
+    assert np.linalg.eigvalsh(0.5 * (h_c + h_c.T)).min() >= -1e-9 * np.abs(h_c).max()
     projected += int(rel(h_c, h_raw) > 1e-9)
   assert projected >= 1, "no element reached the projection"
 

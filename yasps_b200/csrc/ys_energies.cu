@@ -739,97 +739,6 @@ __device__ __forceinline__ void coupled_jt_vec(const CoupledVertex& cv, int s, c
   }
 }
 
-// Projection of the compressed Hessian through S = L^T H L (see the header):
-// h (packed upper, vertex coordinates) becomes H + L^-T (S' - S) L^-1.
-// Returns false when the body vertices' Gram matrix is not positive definite.
-template <int V>
-__device__ __forceinline__ bool coupled_project(double (&h)[3 * V * (3 * V + 1) / 2], const CoupledVertex (&cv)[V],
-                                                int method, double* stash) {
-  constexpr int N = 3 * V, H = N * (N + 1) / 2;
-  double L[V][V], Li[V][V];
-#pragma unroll
-  for (int i = 0; i < V; ++i)
-#pragma unroll
-    for (int j = 0; j < V; ++j) L[i][j] = Li[i][j] = 0.0;
-  // Cholesky of the Gram matrix m (m_ij = xbar_i . xbar_j + 1 within one body)
-#pragma unroll
-  for (int j = 0; j < V; ++j) {
-#pragma unroll
-    for (int i = j; i < V; ++i) {
-      double m;
-      if (i == j)
-        m = cv[i].body == kNoBody ? 1.0
-                                  : cv[i].xbar[0] * cv[i].xbar[0] + cv[i].xbar[1] * cv[i].xbar[1] +
-                                        cv[i].xbar[2] * cv[i].xbar[2] + 1.0;
-      else
-        m = (cv[i].body != kNoBody && cv[i].body == cv[j].body)
-                ? cv[i].xbar[0] * cv[j].xbar[0] + cv[i].xbar[1] * cv[j].xbar[1] + cv[i].xbar[2] * cv[j].xbar[2] + 1.0
-                : 0.0;
-      const double m0 = m;
-#pragma unroll
-      for (int k = 0; k < j; ++k) m -= L[i][k] * L[j][k];
-      if (i == j) {
-        if (!(m > 1e-12 * m0)) return false;
-        L[j][j] = sqrt(m);
-      } else {
-        L[i][j] = m / L[j][j];
-      }
-    }
-  }
-  // L^-1 (lower triangular)
-#pragma unroll
-  for (int i = 0; i < V; ++i) {
-    Li[i][i] = 1.0 / L[i][i];
-#pragma unroll
-    for (int j = 0; j < i; ++j) {
-      double acc = 0.0;
-#pragma unroll
-      for (int k = j; k < i; ++k) acc += L[i][k] * Li[k][j];
-      Li[i][j] = -acc * Li[i][i];
-    }
-  }
-  // S = L^T H L, entry (3v+k, 3w+l) = sum_{p>=v, q>=w} L[p][v] L[q][w] H(3p+k, 3q+l)
-  double sm[H];
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = i; j < N; ++j) {
-      const int v = i / 3, k = i % 3, w = j / 3, l = j % 3;
-      double acc = 0.0;
-#pragma unroll
-      for (int p = v; p < V; ++p)
-#pragma unroll
-        for (int q = w; q < V; ++q) acc += L[p][v] * L[q][w] * h[sym<N>(3 * p + k, 3 * q + l)];
-      sm[utri<N>(i, j)] = acc;
-    }
-  double s[H];  // packed lower copy for the PSD test
-#pragma unroll
-  for (int rr = 0; rr < N; ++rr)
-#pragma unroll
-    for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = sm[utri<N>(c, rr)];
-  if (psd_test_packed<N>(s)) return true;
-  double d[H];
-#pragma unroll
-  for (int i = 0; i < H; ++i) d[i] = sm[i];
-  project_negative_modes<N>(sm, method, stash, blockDim.x);
-#pragma unroll
-  for (int i = 0; i < H; ++i) d[i] = sm[i] - d[i];
-  // H += L^-T D L^-1, entry (3p+k, 3q+l) += sum_{v>=p, w>=q} Li[v][p] Li[w][q] D(3v+k, 3w+l)
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = i; j < N; ++j) {
-      const int p = i / 3, k = i % 3, q = j / 3, l = j % 3;
-      double acc = 0.0;
-#pragma unroll
-      for (int v = p; v < V; ++v)
-#pragma unroll
-        for (int w = q; w < V; ++w) acc += Li[v][p] * Li[w][q] * d[sym<N>(3 * v + k, 3 * w + l)];
-      h[utri<N>(i, j)] += acc;
-    }
-  return true;
-}
-
 // Records of the compressed Hessian: target slots merged by code in
 // first-occurrence order (the coordinates' order), block (gi, gj) =
 // sum over slots k in gi, l in gj of J_k^T H(v_k, v_l) J_l, transposed when
@@ -896,11 +805,13 @@ __global__ void __launch_bounds__(kEnergyThreads) coupled_kernel(const ys_couple
   CoupledVertex cv[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
-    if (!load_coupled_point(a, a.base.conn[(uint64_t)t * V + v], x.p[v], cv[v])) {
+    const uint32_t id = a.base.conn[(uint64_t)t * V + v];
+    if (!load_coupled_point(a, id, x.p[v], cv[v])) {
       if (a.status) atomicCAS(a.status, 0, (int32_t)(t + 1));
       return;
     }
-    r.p[v][0] = r.p[v][1] = r.p[v][2] = 0.0;
+    if (a.base.rest.num_children) load_point(a.base.rest, id, r.p[v]);  // friction: old positions
+    else r.p[v][0] = r.p[v][1] = r.p[v][2] = 0.0;
   }
   const HD<N> e = E::template eval<N>(a.base, t, x, r);
   if (a.base.energy) a.base.energy[t] = e.v;
@@ -921,21 +832,18 @@ __global__ void __launch_bounds__(kEnergyThreads) coupled_kernel(const ys_couple
   double h[HD<N>::H];
 #pragma unroll
   for (int i = 0; i < HD<N>::H; ++i) h[i] = e.h[i];
+  // The leaves map linearly to the vertex positions, so the Hessian with
+  // respect to the positions is projected (the inner projection of the
+  // reference, PKG/differentiator/differentiator.pyx:795-799) and then mapped
+  // to the leaves by coupled_records.
   if (a.base.projection_method >= 1) {
-    bool any = false;
+    double s[HD<N>::H];
 #pragma unroll
-    for (int v = 0; v < V; ++v) any |= cv[v].body != kNoBody;
-    if (!any) {
-      double s[HD<N>::H];
+    for (int rr = 0; rr < N; ++rr)
 #pragma unroll
-      for (int rr = 0; rr < N; ++rr)
-#pragma unroll
-        for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = h[utri<N>(c, rr)];
-      if (!psd_test_packed<N>(s))
-        project_negative_modes<N>(h, a.base.projection_method, energy_stash + threadIdx.x, blockDim.x);
-    } else if (!coupled_project<V>(h, cv, a.base.projection_method, energy_stash + threadIdx.x)) {
-      if (a.status) atomicCAS(a.status, 0, (int32_t)(t + 1));
-    }
+      for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = h[utri<N>(c, rr)];
+    if (!psd_test_packed<N>(s))
+      project_negative_modes<N>(h, a.base.projection_method, energy_stash + threadIdx.x, blockDim.x);
   }
   coupled_records<V>(code, cv, a.base.plan.coord_outer[t], a.base.plan.record, a.base.block_records, h);
 }
@@ -949,12 +857,14 @@ __global__ void __launch_bounds__(128) coupled_value_kernel(const ys_coupled_arg
   CoupledVertex cv[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
-    if (!load_coupled_point(a, a.base.conn[(uint64_t)t * V + v], x.p[v], cv[v])) {
+    const uint32_t id = a.base.conn[(uint64_t)t * V + v];
+    if (!load_coupled_point(a, id, x.p[v], cv[v])) {
       if (a.status) atomicCAS(a.status, 0, (int32_t)(t + 1));
       a.base.energy[t] = 0.0;
       return;
     }
-    r.p[v][0] = r.p[v][1] = r.p[v][2] = 0.0;
+    if (a.base.rest.num_children) load_point(a.base.rest, id, r.p[v]);
+    else r.p[v][0] = r.p[v][1] = r.p[v][2] = 0.0;
   }
   a.base.energy[t] = E::template eval<0>(a.base, t, x, r).v;
 }
@@ -1095,14 +1005,24 @@ int32_t ys_coupled_energy_eval(const ys_coupled_args* args, void* stream) {
              "affine bodies needed");
   if (a.base.num_elements == 0) return YS_OK;
   cudaStream_t s = (cudaStream_t)stream;
+  const bool friction = a.base.kind >= YS_ENERGY_FRICTION_PT && a.base.kind <= YS_ENERGY_FRICTION_PP;
+  YS_REQUIRE(!friction || (a.base.rest.num_children >= 1 && a.base.params && a.base.param_stride >= 9),
+             YS_ERR_INVALID, "friction needs the old positions and 9 lagged parameters per element");
+  YS_REQUIRE(a.base.rest.num_children == 0 ||
+                 a.base.rest.prefix[a.base.rest.num_children] >= a.base.position.prefix[a.base.position.num_children],
+             YS_ERR_INVALID, "old positions must cover the position union");
   switch (a.base.kind) {
     case YS_ENERGY_POINT_POINT: return ys::launch_coupled<ys::PointPoint>(a, s);
     case YS_ENERGY_POINT_EDGE: return ys::launch_coupled<ys::PointEdge>(a, s);
     case YS_ENERGY_POINT_TRIANGLE: return ys::launch_coupled<ys::PointTriangle>(a, s);
     case YS_ENERGY_EDGE_EDGE: return ys::launch_coupled<ys::EdgeEdge>(a, s);
+    case YS_ENERGY_FRICTION_PT: return ys::launch_coupled<ys::FrictionPT>(a, s);
+    case YS_ENERGY_FRICTION_PE: return ys::launch_coupled<ys::FrictionPE>(a, s);
+    case YS_ENERGY_FRICTION_EE: return ys::launch_coupled<ys::FrictionEE>(a, s);
+    case YS_ENERGY_FRICTION_PP: return ys::launch_coupled<ys::FrictionPP>(a, s);
     default: break;
   }
-  YS_REQUIRE(false, YS_ERR_INVALID, "coupled evaluation takes the PP, PE, PT and EE barriers");
+  YS_REQUIRE(false, YS_ERR_INVALID, "coupled evaluation takes the contact barriers and the lagged friction kinds");
 }
 
 }  // extern "C"

@@ -131,8 +131,9 @@ class _Term:
       if len(idx) > 1:
         raise ValueError("a position union may hold one primitive of affine-body vertices")
       if idx:
-        if self.expr.code not in (1, 2, 3, 4):
-          raise ValueError(f"{type(self.expr).__name__}: only the PP/PE/PT/EE barriers take affine-body vertices")
+        if self.expr.code not in (1, 2, 3, 4, 8, 9, 10, 11):
+          raise ValueError(f"{type(self.expr).__name__}: only the contact barriers and the lagged friction kinds "
+                           "take affine-body vertices")
         ap = leaves[idx[0]].expr
         vb = ap.conn.value.reshape(-1)
         if vb.numel() and int(vb.max().item()) >= ap.bodies.numInstances:
@@ -571,8 +572,8 @@ class hessian:
       st = torch.cat(statuses).cpu()
       if bool((st != 0).any()):
         k = int((st != 0).nonzero()[0, 0])
-        raise ValueError(f"contact with affine bodies: element {int(st[k]) - 1} of a barrier term has affinely "
-                         "dependent body vertices (degenerate Gram matrix)")
+        raise ValueError(f"contact with affine bodies: element {int(st[k]) - 1} of a term names a vertex "
+                         "outside the position union or a body beyond the body primitive")
     for bs in (self._static, self._dynamic):
       self._assemble(bs)
     self.gradient.value.zero_()

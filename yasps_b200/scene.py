@@ -51,7 +51,14 @@ class minimizer:
   def addEnergy(self, e, targets=(), projection_method=1, dynamic_instances=False, **flags):
     if e.operator != ENERGY:
       raise ValueError("minimizer.addEnergy: the attribute must be an energy")
-    unsupported = {k: v for k, v in flags.items() if v and k in ("gradient_only", "separate_hessian_jacobian", "lto")}
+    # separate_hessian_jacobian: the reference then evaluates J^T H J from
+    # explicit Jacobian blocks instead of a symbolic expansion; the matrix is
+    # the same (for a linear map from the targets the inner Hessian is
+    # projected either way, PKG/differentiator/differentiator.pyx:795-799;
+    # for a nonlinear one the flag is ignored, PKG/matrixAndVector/matrix/
+    # hessian.pyx:905).  Every element kernel here already forms J^T H J from
+    # explicit blocks, so the flag is accepted and changes nothing.
+    unsupported = {k: v for k, v in flags.items() if v and k in ("gradient_only", "lto")}
     if unsupported:
       raise NotImplementedError(f"minimizer.addEnergy: unsupported options {sorted(unsupported)}")
     if any(r.energy is e for r in self.requests + self.requests_dynamic):

@@ -661,15 +661,22 @@ BARRIER_PAIRS = (("pp", 2), ("pe", 3), ("pt", 4), ("ee", 4))
 
 def contact_with_bodies_scene(cloth_position, bodies: AffineBodies, container, pairs, dhat: float, kappa: float,
                               projection_method: int = 2, cloth_mass=None, dt: float = 0.01,
-                              name: str = "contact_with_bodies"):
+                              name: str = "contact_with_bodies", friction=None,
+                              separate_hessian_jacobian: bool = False):
   """Barrier pairs over the collision union ``[cloth, abd vertices, container]``
   (``examples/dropping_in_container_mixed/dropping_in_container.py:344-405``):
   the abd vertices sit at ``A xbar + t`` of their bodies, the container is
   DATA, the targets are ``[cloth position, affine_matrices, translations]``.
   ``pairs`` maps ``pp/pe/pt/ee`` to union-index connectivities.  With
   ``cloth_mass`` the scene also carries the inertia of the cloth and body
-  vertices and the bodies' orthogonality energy (a solvable system)."""
-  from .energies import edge_edge, inertia, point_edge, point_point, point_triangle
+  vertices and the bodies' orthogonality energy (a solvable system).
+  ``friction`` (optional) adds lagged friction over the same union
+  (``examples/dropping_in_container/dropping_in_container.py:248-290``): a dict
+  with ``last`` (the union's positions at the start of the step, one row a
+  union vertex), ``fdhat``, ``rate``, and per kind ``pp/pe/pt/ee`` a pair of
+  (union connectivity, lagged [n, 9])."""
+  from .energies import (edge_edge, friction_edge_edge, friction_point_edge, friction_point_point,
+                         friction_point_triangle, inertia, point_edge, point_point, point_triangle)
   from .scene import scene as make_scene
   sc = make_scene(name)
   m = sc.addMesh("collision_mesh")
@@ -691,7 +698,29 @@ def contact_with_bodies_scene(cloth_position, bodies: AffineBodies, container, p
     c = p.addConnectivity(key + "2v", allv, np.asarray(conn, dtype=np.uint32), arity)
     x = p.addAttribute("positions", through=c, source=apos)
     sc.addEnergy(p.addAttribute("barrier", computed_attribute=makers[key](x, dhat, kappa)),
-                 projection_method=projection_method)
+                 projection_method=projection_method, separate_hessian_jacobian=separate_hessian_jacobian)
+  if friction is not None:
+    last = np.asarray(friction["last"], dtype=np.float64).reshape(-1, 3)
+    nc, nv = len(cloth_position), len(bodies.rest)
+    for prim, part in ((cloth, last[:nc]), (verts, last[nc:nc + nv]), (cont, last[nc + nv:])):
+      a = prim.addConstant("contact_last_position", rows=3, cols=1)
+      a.updateValue(part)
+    alast = allv.addAttribute("contact_last_position")
+    fmakers = {"pp": friction_point_point, "pe": friction_point_edge, "pt": friction_point_triangle,
+               "ee": friction_edge_edge}
+    for key, arity in BARRIER_PAIRS:
+      if key not in friction:
+        continue
+      conn, lagged = friction[key]
+      p = m.addPrimitive("friction_" + key, numInstances=len(conn))
+      c = p.addConnectivity(key + "f2v", allv, np.asarray(conn, dtype=np.uint32), arity)
+      x = p.addAttribute("positions", through=c, source=apos)
+      xl = p.addAttribute("last_positions", through=c, source=alast)
+      lag = p.addConstant("lagged", rows=9, cols=1)
+      lag.updateValue(np.asarray(lagged, dtype=np.float64))
+      sc.addEnergy(p.addAttribute("friction", computed_attribute=fmakers[key](x, xl, friction["fdhat"], dt,
+                                                                              friction["rate"], lag)),
+                   projection_method=projection_method, separate_hessian_jacobian=separate_hessian_jacobian)
   if cloth_mass is not None:
     old = cloth.addConstant("old_position", rows=3, cols=1)
     old.updateValue(cloth_position)
