@@ -38,9 +38,7 @@ def oracle_assembly(cube, bodies, projection_method=1):
   body_codes = lambda b: np.stack([start_a + 9 * b + 2, start_t + 3 * b + 2], axis=1)
   body_sizes = lambda m: np.tile(np.array([9, 3]), (m, 1))
   rest_t = bodies.rest[bodies.tets.astype(np.int64)].reshape(-1, 12)
-  e_as, g, h = ae.grad_hess(ae.snh, q[tb], rest_t, (bodies.mu, bodies.lam, cube.dt))
-  if projection_method >= 1:
-    h = projection.project_spd(h, projection_method)
+  e_as, g, h = ae.snh_projected(q[tb], rest_t, (bodies.mu, bodies.lam, cube.dt), projection_method)
   terms.append((body_codes(tb), body_sizes(tb.size), g, h))
   x_before = bodies.positions()
   data = np.concatenate([bodies.rest, x_before, bodies.velocity, bodies.mass[:, None]], axis=1)

@@ -16,6 +16,8 @@
 // second-order forward-mode differentiation (ys_ad.cuh); the local Hessian
 // is projected like the SNH one (LDL^T PSD test, then the negative modes) and
 // scattered with the NoProject merge rules into pattern records.
+#include <type_traits>
+
 #include "ys_ad.cuh"
 #include "ys_common.cuh"
 
@@ -506,33 +508,39 @@ struct AffineInertia {
   }
 };
 
-// Stable Neo-Hookean (helpers.py:129-136) of a tetrahedron of one body:
-// positions xbar_k A^T + t, F rows x_{k} - x_0, TB rows xbar_k - xbar_0,
-// IB = (TB^T)^-1, vol = det(TB^T) / 6, FI = F^T IB.
+// Stable Neo-Hookean (stable_neo_hookean_modified, helpers.py:129-136) of a
+// tetrahedron of one body: positions xbar_k A^T + t, F rows x_k - x_0 (the
+// edge matrix), TB rows xbar_k - xbar_0, IB = (TB^T)^-1, vol = det(TB^T) / 6,
+// FI = F^T IB.  The energy's argument in the reference is F (the deformation
+// gradient attribute of dropping_in_container_mixed/dropping_in_container.py:
+// 306-320), a linear function of A, so the reference projects the 9x9
+// Hessian with respect to F and maps it to the body coordinates
+// (PKG/differentiator/differentiator.pyx:795-799): eval<N> gives the energy
+// over the 9 entries of F (N = 9, input 3m + i = F[m][i]) or its value (N = 0);
+// the affine kernel projects and maps (affine_snh_to_body).
 struct AffineSnh {
   static constexpr int A = 4;
-  template <int N>
-  __device__ static HD<N> eval(const ys_affine_args& a, uint32_t e, const AffineBody& b) {
+  static constexpr bool kInnerF = true;
+  // rest edges ed[m] = xbar_{m+1} - xbar_0 and IB of element e
+  __device__ static void rest_frame(const ys_affine_args& a, uint32_t e, double (&ed)[3][3], double (&ib)[3][3],
+                                    double& det, double (&xb)[4][3]) {
     const uint4 tv = reinterpret_cast<const uint4*>(a.tets)[e];
-    double xb[4][3];
     load_rest3(a.rest, tv.x, xb[0]);
     load_rest3(a.rest, tv.y, xb[1]);
     load_rest3(a.rest, tv.z, xb[2]);
     load_rest3(a.rest, tv.w, xb[3]);
-    double ed[3][3];
 #pragma unroll
     for (int m = 0; m < 3; ++m)
 #pragma unroll
       for (int c = 0; c < 3; ++c) ed[m][c] = xb[m + 1][c] - xb[0][c];
     // (TB^T)^-1 rows: (e1 x e2, e2 x e0, e0 x e1) / det
-    double ib[3][3];
     const double k0[3] = {ed[1][1] * ed[2][2] - ed[1][2] * ed[2][1], ed[1][2] * ed[2][0] - ed[1][0] * ed[2][2],
                           ed[1][0] * ed[2][1] - ed[1][1] * ed[2][0]};
     const double k1[3] = {ed[2][1] * ed[0][2] - ed[2][2] * ed[0][1], ed[2][2] * ed[0][0] - ed[2][0] * ed[0][2],
                           ed[2][0] * ed[0][1] - ed[2][1] * ed[0][0]};
     const double k2[3] = {ed[0][1] * ed[1][2] - ed[0][2] * ed[1][1], ed[0][2] * ed[1][0] - ed[0][0] * ed[1][2],
                           ed[0][0] * ed[1][1] - ed[0][1] * ed[1][0]};
-    const double det = ed[0][0] * k0[0] + ed[0][1] * k0[1] + ed[0][2] * k0[2];
+    det = ed[0][0] * k0[0] + ed[0][1] * k0[1] + ed[0][2] * k0[2];
     const double inv = 1.0 / det;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -540,26 +548,27 @@ struct AffineSnh {
       ib[1][c] = k1[c] * inv;
       ib[2][c] = k2[c] * inv;
     }
-    // Positions, then FI = F^T IB.  FI is linear in A: dFI_ij / dA_ic = M_cj
-    // with M = TB^T IB (the identity up to rounding) and dFI / dt = 0, so
-    // its entries are built as linear HD numbers.
+  }
+
+  template <int N>
+  __device__ static HD<N> eval(const ys_affine_args& a, uint32_t e, const AffineBody& b) {
+    double ed[3][3], ib[3][3], det, xb[4][3];
+    rest_frame(a, e, ed, ib, det, xb);
     double xs[4][3];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
       for (int r = 0; r < 3; ++r) xs[k][r] = b.a[r][0] * xb[k][0] + b.a[r][1] * xb[k][1] + b.a[r][2] * xb[k][2] + b.t[r];
-    HD<N> fi[3][3];
+    HD<N> f[3][3];  // F[m][i] = x_{m+1, i} - x_{0, i}
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) f[m][i] = hd_var<N>(xs[m + 1][i] - xs[0][i], 3 * m + i);
+    HD<N> fi[3][3];  // FI = F^T IB
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        fi[i][j] = hd_const<N>(ib[0][j] * (xs[1][i] - xs[0][i]) + ib[1][j] * (xs[2][i] - xs[0][i]) +
-                               ib[2][j] * (xs[3][i] - xs[0][i]));
-        if constexpr (N >= 12) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) fi[i][j].g[3 * i + c] = ed[0][c] * ib[0][j] + ed[1][c] * ib[1][j] + ed[2][c] * ib[2][j];
-        }
-      }
+      for (int j = 0; j < 3; ++j) fi[i][j] = ib[0][j] * f[0][i] + ib[1][j] * f[1][i] + ib[2][j] * f[2][i];
     HD<N> ic = hd_const<N>(0.0);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -575,6 +584,39 @@ struct AffineSnh {
     return (det / 6.0 * a.dt * a.dt) * psi;
   }
 };
+
+// The F-space energy of a body tetrahedron mapped to its body coordinates
+// (A row-major at 0..8, t at 9..11; F does not depend on t):
+// dF[m][i] / dA[r][c] = delta_ir ed[m][c], so g_A[r][c] = sum_m ed[m][c]
+// g_F[m][r] and H_A = J^T H_F J.
+__device__ __forceinline__ void affine_snh_to_body(const HD<9>& ef, const double (&ed)[3][3], HD<12>& q) {
+  q.v = ef.v;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) acc += ed[m][c] * ef.g[3 * m + r];
+      q.g[3 * r + c] = acc;
+    }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) q.g[9 + r] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 12; ++i)
+#pragma unroll
+    for (int j = i; j < 12; ++j) {
+      double acc = 0.0;
+      if (i < 9 && j < 9) {
+        const int r = i / 3, c = i % 3, r2 = j / 3, c2 = j % 3;
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int m2 = 0; m2 < 3; ++m2) acc += ed[m][c] * ed[m2][c2] * ef.h[sym<9>(3 * m + r, 3 * m2 + r2)];
+      }
+      q.h[utri<12>(i, j)] = acc;
+    }
+}
 
 // Body of element e; false (element skipped) when an index is out of range.
 __device__ __forceinline__ bool load_affine_body(const ys_affine_args& a, uint32_t e, AffineBody& b) {
@@ -593,6 +635,11 @@ __device__ __forceinline__ bool load_affine_body(const ys_affine_args& a, uint32
   return true;
 }
 
+template <class E, class = void>
+struct InnerF : std::false_type {};
+template <class E>
+struct InnerF<E, std::void_t<decltype(E::kInnerF)>> : std::bool_constant<E::kInnerF> {};
+
 template <class E>
 __global__ void __launch_bounds__(kEnergyThreads) affine_kernel(const ys_affine_args a) {
   constexpr int A = E::A, N = 3 * A;
@@ -601,8 +648,29 @@ __global__ void __launch_bounds__(kEnergyThreads) affine_kernel(const ys_affine_
   if (e >= a.num_elements) return;
   AffineBody b;
   if (!load_affine_body(a, e, b)) return;
-  const HD<N> en = E::template eval<N>(a, e, b);
-  finish_element<A>(a, e, en, energy_stash + threadIdx.x);
+  if constexpr (InnerF<E>::value) {
+    // project the Hessian in F (9x9), then map it to the body coordinates
+    HD<9> ef = E::template eval<9>(a, e, b);
+    if (a.projection_method >= 1) {
+      double s[HD<9>::H];
+#pragma unroll
+      for (int rr = 0; rr < 9; ++rr)
+#pragma unroll
+        for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = ef.h[utri<9>(c, rr)];
+      if (!psd_test_packed<9>(s)) project_negative_modes<9>(ef.h, a.projection_method, energy_stash + threadIdx.x,
+                                                            blockDim.x);
+    }
+    double ed[3][3], ib[3][3], det, xb[4][3];
+    E::rest_frame(a, e, ed, ib, det, xb);
+    HD<N> en;
+    affine_snh_to_body(ef, ed, en);
+    ys_affine_args plain = a;
+    plain.projection_method = 0;  // projected already
+    finish_element<A>(plain, e, en, energy_stash + threadIdx.x);
+  } else {
+    const HD<N> en = E::template eval<N>(a, e, b);
+    finish_element<A>(a, e, en, energy_stash + threadIdx.x);
+  }
 }
 
 template <class E>
