@@ -14,7 +14,7 @@ followed by the translation t (``:243``).
 * :func:`snh` -- ``stable_neo_hookean_modified`` (``helpers.py:129-136``) on
   the tet positions ``xbar A^T + t`` (``dropping_in_container.py:280-320``,
   ``:370``); :func:`snh_projected` with the reference's projection (in the
-  deformation gradient F, then mapped to the body coordinates).
+  vertex positions, then mapped to the body coordinates).
 
 :func:`grad_hess` batches the gradient and Hessian over elements.
 """
@@ -67,52 +67,30 @@ def snh(q, data, params):
   return vol * (0.5 * mu * (ic - 3.0) - 0.5 * mu * torch.log(i3) + 0.5 * lam * ((j - alpha) * (j - alpha))) * dt * dt
 
 
-def snh_of_edges(f, rest, mu, lam, dt):
-  """``stable_neo_hookean_modified`` (``helpers.py:129-136``) of the edge
-  matrix ``f`` (rows x_k - x_0) of a tetrahedron with body-frame rest
-  positions ``rest`` [4, 3]."""
-  torch = _t()
-  tb = torch.stack([rest[1] - rest[0], rest[2] - rest[0], rest[3] - rest[0]])
-  ib = torch.linalg.inv(tb.T)
-  vol = torch.linalg.det(tb.T) / 6.0
-  fi = f.T @ ib
-  j = torch.linalg.det(fi)
-  ic = torch.trace(fi.T @ fi)
-  alpha = 1.0 + 0.75 * mu / lam
-  return vol * (0.5 * mu * (ic - 3.0) - 0.5 * mu * torch.log(ic + 1.0) + 0.5 * lam * ((j - alpha) * (j - alpha))) \
-      * dt * dt
-
-
 def snh_projected(q, rest, params, method):
   """Energies, gradients [n, 12] and Hessians [n, 12, 12] of the affine SNH in
-  the body coordinates with the reference's projection: its energy argument
-  is the deformation-gradient attribute F (the edge matrix, linear in A:
-  ``dropping_in_container_mixed/dropping_in_container.py:306-320``), so the
-  9x9 Hessian with respect to F is projected and mapped by J = dF/dq
+  the body coordinates with the reference's projection: the energy's
+  argument is the tetrahedron's gathered vertex positions ``xbar A^T + t``,
+  linear in the body coordinates, so the 12x12 Hessian with respect to the
+  positions is projected and mapped by J = dx/dq
   (``PKG/differentiator/differentiator.pyx:795-799``)."""
-  from . import projection
-  torch = _t()
+  from . import energies, projection
   q = np.asarray(q, dtype=np.float64)
   rest = np.asarray(rest, dtype=np.float64).reshape(len(q), 4, 3)
   mu, lam, dt = params
-  n = len(q)
-  e, g, h = np.zeros(n), np.zeros((n, 12)), np.zeros((n, 12, 12))
-  for k in range(n):
-    a = q[k, :9].reshape(3, 3)
-    r = torch.tensor(rest[k])
-    ed = rest[k, 1:] - rest[k, 0]
-    f0 = torch.tensor(ed @ a.T)  # rows A (xbar_m - xbar_0)
-    fn = lambda v: snh_of_edges(v.reshape(3, 3), r, mu, lam, dt)
-    e[k] = float(fn(f0.reshape(-1)))
-    gf = torch.autograd.functional.jacobian(fn, f0.reshape(-1)).numpy()
-    hf = torch.autograd.functional.hessian(fn, f0.reshape(-1)).numpy()
-    hf = projection.project_spd(0.5 * (hf + hf.T), method)
-    J = np.zeros((9, 12))  # F[m][i] = sum_c A[i][c] ed[m][c]
-    for m in range(3):
-      for i in range(3):
-        J[3 * m + i, 3 * i:3 * i + 3] = ed[m]
-    g[k] = J.T @ gf
-    h[k] = J.T @ hf @ J
+  a = q[:, :9].reshape(-1, 3, 3)
+  t = q[:, 9:12]
+  x = np.einsum("nkc,nrc->nkr", rest, a) + t[:, None, :]
+  e, gx, hx = energies.snh_from_rest(x, rest, mu, lam, dt)
+  if method >= 1:
+    hx = projection.project_spd(hx, method)
+  J = np.zeros((len(q), 12, 12))  # row 3k + r: xbar_k at columns 3r .. 3r + 2, 1 at 9 + r
+  for k in range(4):
+    for r in range(3):
+      J[:, 3 * k + r, 3 * r:3 * r + 3] = rest[:, k]
+      J[:, 3 * k + r, 9 + r] = 1.0
+  g = np.einsum("nij,ni->nj", J, gx)
+  h = np.einsum("nia,nij,njb->nab", J, hx, J)
   return e, g, h
 
 

@@ -508,20 +508,19 @@ struct AffineInertia {
   }
 };
 
-// Stable Neo-Hookean (stable_neo_hookean_modified, helpers.py:129-136) of a
-// tetrahedron of one body: positions xbar_k A^T + t, F rows x_k - x_0 (the
-// edge matrix), TB rows xbar_k - xbar_0, IB = (TB^T)^-1, vol = det(TB^T) / 6,
-// FI = F^T IB.  The energy's argument in the reference is F (the deformation
-// gradient attribute of dropping_in_container_mixed/dropping_in_container.py:
-// 306-320), a linear function of A, so the reference projects the 9x9
-// Hessian with respect to F and maps it to the body coordinates
+// Stable Neo-Hookean (helpers.py:102-127) of a tetrahedron of one body whose
+// vertices sit at x_k = A xbar_k + t: F rows x_k - x_0 (the edge matrix), TB
+// rows xbar_k - xbar_0, IB = (TB^T)^-1, vol = det(TB^T) / 6, FI = F^T IB.
+// The energy's argument is the gathered vertex positions, a linear function
+// of the body's A and t, so the reference projects the 12x12 Hessian with
+// respect to those positions and maps it to the body coordinates
 // (PKG/differentiator/differentiator.pyx:795-799): eval<N> gives the energy
-// over the 9 entries of F (N = 9, input 3m + i = F[m][i]) or its value (N = 0);
-// the affine kernel projects and maps (affine_snh_to_body).
+// over the 12 position coordinates (N = 12, input 3k + r = x_k[r]) or its
+// value (N = 0); the affine kernel projects and maps (affine_positions_to_body).
 struct AffineSnh {
   static constexpr int A = 4;
-  static constexpr bool kInnerF = true;
-  // rest edges ed[m] = xbar_{m+1} - xbar_0 and IB of element e
+  static constexpr bool kInnerPositions = true;
+  // body-frame rest positions xbar, rest edges, IB and det(TB^T) of element e
   __device__ static void rest_frame(const ys_affine_args& a, uint32_t e, double (&ed)[3][3], double (&ib)[3][3],
                                     double& det, double (&xb)[4][3]) {
     const uint4 tv = reinterpret_cast<const uint4*>(a.tets)[e];
@@ -554,21 +553,18 @@ struct AffineSnh {
   __device__ static HD<N> eval(const ys_affine_args& a, uint32_t e, const AffineBody& b) {
     double ed[3][3], ib[3][3], det, xb[4][3];
     rest_frame(a, e, ed, ib, det, xb);
-    double xs[4][3];
+    HD<N> x[4][3];  // positions A xbar_k + t as the inputs
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
-      for (int r = 0; r < 3; ++r) xs[k][r] = b.a[r][0] * xb[k][0] + b.a[r][1] * xb[k][1] + b.a[r][2] * xb[k][2] + b.t[r];
-    HD<N> f[3][3];  // F[m][i] = x_{m+1, i} - x_{0, i}
-#pragma unroll
-    for (int m = 0; m < 3; ++m)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) f[m][i] = hd_var<N>(xs[m + 1][i] - xs[0][i], 3 * m + i);
-    HD<N> fi[3][3];  // FI = F^T IB
+      for (int r = 0; r < 3; ++r)
+        x[k][r] = hd_var<N>(b.a[r][0] * xb[k][0] + b.a[r][1] * xb[k][1] + b.a[r][2] * xb[k][2] + b.t[r], 3 * k + r);
+    HD<N> fi[3][3];  // FI = F^T IB, F[m][i] = x_{m+1}[i] - x_0[i]
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) fi[i][j] = ib[0][j] * f[0][i] + ib[1][j] * f[1][i] + ib[2][j] * f[2][i];
+      for (int j = 0; j < 3; ++j)
+        fi[i][j] = ib[0][j] * (x[1][i] - x[0][i]) + ib[1][j] * (x[2][i] - x[0][i]) + ib[2][j] * (x[3][i] - x[0][i]);
     HD<N> ic = hd_const<N>(0.0);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -585,35 +581,42 @@ struct AffineSnh {
   }
 };
 
-// The F-space energy of a body tetrahedron mapped to its body coordinates
-// (A row-major at 0..8, t at 9..11; F does not depend on t):
-// dF[m][i] / dA[r][c] = delta_ir ed[m][c], so g_A[r][c] = sum_m ed[m][c]
-// g_F[m][r] and H_A = J^T H_F J.
-__device__ __forceinline__ void affine_snh_to_body(const HD<9>& ef, const double (&ed)[3][3], HD<12>& q) {
-  q.v = ef.v;
+// The position-space energy of a body tetrahedron mapped to its body
+// coordinates (A row-major at 0..8, t at 9..11): x_k[r] = sum_c A[r][c]
+// xbar_k[c] + t[r], so J = dx/dq holds xbar_k at (3k + r, 3r .. 3r + 2) and 1
+// at (3k + r, 9 + r); g_q = J^T g_x, H_q = J^T H_x J.
+__device__ __forceinline__ double affine_jac(const double (&xb)[4][3], int k, int r, int j) {
+  if (j < 9) return (j / 3 == r) ? xb[k][j % 3] : 0.0;
+  return (j - 9 == r) ? 1.0 : 0.0;
+}
+
+__device__ __forceinline__ void affine_positions_to_body(const HD<12>& ex, const double (&xb)[4][3], HD<12>& q) {
+  q.v = ex.v;
 #pragma unroll
-  for (int r = 0; r < 3; ++r)
+  for (int j = 0; j < 12; ++j) {
+    double acc = 0.0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double acc = 0.0;
+    for (int k = 0; k < 4; ++k)
 #pragma unroll
-      for (int m = 0; m < 3; ++m) acc += ed[m][c] * ef.g[3 * m + r];
-      q.g[3 * r + c] = acc;
-    }
-#pragma unroll
-  for (int r = 0; r < 3; ++r) q.g[9 + r] = 0.0;
+      for (int r = 0; r < 3; ++r) acc += affine_jac(xb, k, r, j) * ex.g[3 * k + r];
+    q.g[j] = acc;
+  }
 #pragma unroll
   for (int i = 0; i < 12; ++i)
 #pragma unroll
     for (int j = i; j < 12; ++j) {
       double acc = 0.0;
-      if (i < 9 && j < 9) {
-        const int r = i / 3, c = i % 3, r2 = j / 3, c2 = j % 3;
 #pragma unroll
-        for (int m = 0; m < 3; ++m)
+      for (int k = 0; k < 4; ++k)
 #pragma unroll
-          for (int m2 = 0; m2 < 3; ++m2) acc += ed[m][c] * ed[m2][c2] * ef.h[sym<9>(3 * m + r, 3 * m2 + r2)];
-      }
+        for (int r = 0; r < 3; ++r) {
+          const double ji = affine_jac(xb, k, r, i);
+          if (ji == 0.0) continue;
+#pragma unroll
+          for (int k2 = 0; k2 < 4; ++k2)
+#pragma unroll
+            for (int r2 = 0; r2 < 3; ++r2) acc += ji * ex.h[sym<12>(3 * k + r, 3 * k2 + r2)] * affine_jac(xb, k2, r2, j);
+        }
       q.h[utri<12>(i, j)] = acc;
     }
 }
@@ -636,9 +639,9 @@ __device__ __forceinline__ bool load_affine_body(const ys_affine_args& a, uint32
 }
 
 template <class E, class = void>
-struct InnerF : std::false_type {};
+struct InnerPositions : std::false_type {};
 template <class E>
-struct InnerF<E, std::void_t<decltype(E::kInnerF)>> : std::bool_constant<E::kInnerF> {};
+struct InnerPositions<E, std::void_t<decltype(E::kInnerPositions)>> : std::bool_constant<E::kInnerPositions> {};
 
 template <class E>
 __global__ void __launch_bounds__(kEnergyThreads) affine_kernel(const ys_affine_args a) {
@@ -648,22 +651,23 @@ __global__ void __launch_bounds__(kEnergyThreads) affine_kernel(const ys_affine_
   if (e >= a.num_elements) return;
   AffineBody b;
   if (!load_affine_body(a, e, b)) return;
-  if constexpr (InnerF<E>::value) {
-    // project the Hessian in F (9x9), then map it to the body coordinates
-    HD<9> ef = E::template eval<9>(a, e, b);
+  if constexpr (InnerPositions<E>::value) {
+    // project the Hessian in the vertex positions (12x12), then map it to
+    // the body coordinates
+    HD<12> ex = E::template eval<12>(a, e, b);
     if (a.projection_method >= 1) {
-      double s[HD<9>::H];
+      double s[HD<12>::H];
 #pragma unroll
-      for (int rr = 0; rr < 9; ++rr)
+      for (int rr = 0; rr < 12; ++rr)
 #pragma unroll
-        for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = ef.h[utri<9>(c, rr)];
-      if (!psd_test_packed<9>(s)) project_negative_modes<9>(ef.h, a.projection_method, energy_stash + threadIdx.x,
-                                                            blockDim.x);
+        for (int c = 0; c <= rr; ++c) s[tri(rr, c)] = ex.h[utri<12>(c, rr)];
+      if (!psd_test_packed<12>(s))
+        project_negative_modes<12>(ex.h, a.projection_method, energy_stash + threadIdx.x, blockDim.x);
     }
     double ed[3][3], ib[3][3], det, xb[4][3];
     E::rest_frame(a, e, ed, ib, det, xb);
     HD<N> en;
-    affine_snh_to_body(ef, ed, en);
+    affine_positions_to_body(ex, xb, en);
     ys_affine_args plain = a;
     plain.projection_method = 0;  // projected already
     finish_element<A>(plain, e, en, energy_stash + threadIdx.x);

@@ -674,15 +674,109 @@ class hessian:
       L.call("ys_assemble", L.ptr(bs.records), L.ptr(p.record_begin), L.ptr(p.record_count), L.ptr(p.value_offset),
              L.ptr(p.dims), p.num_unique, L.ptr(bs.values), L.ptr(v32), s)
 
+  # -- reference layout of wide (9-DoF) targets -------------------------------------
+  @property
+  def wide_targets(self) -> bool:
+    """True when a target is wider than 3 (the 9-DoF ``affine_matrices``)."""
+    return any(w.size != 3 for w in self.__wrt)
+
+  def _reference_view(self, bs: _BlockSet):
+    """The block set in the reference's layout, for scenes with 9-DoF
+    targets: internally the affine matrix of a body is three 3-DoF rows (so
+    the SpMV, the MAS hierarchy and the FP32 copy see 3x3 blocks only); the
+    reference keeps one 9-DoF slot (``dropping_in_container.py:241-243``), so
+    its pattern has 9x9 / 9x3 / 3x9 / 3x3 categories sorted by (h, w, row,
+    col) (``coordinateCompressionKernel.pyx:34-53``).  The view re-runs the
+    compression, coordinates and pattern build on the slot codes with each
+    body's three A-row slots folded into one slot of size 9 (the other two
+    become padding), which gives the reference's positions, dims, category
+    counts and starts, and lookups; its values are gathered from the 3x3
+    blocks.  Returns ``(pattern, value map)`` cached per pattern."""
+    import ctypes
+    torch = _torch()
+    p = bs.pattern
+    cached = getattr(bs, "ref_view", None)
+    if cached is not None and cached[0] is p:
+      return cached[1], cached[2]
+    s = L.stream_ptr()
+    a_ranges = [(self.wrt_start_indices[k], self.wrt_start_indices[k + 1]) for k, w in enumerate(self.__wrt)
+                if w.size == 9]
+    info, total = [], 0
+    for d in bs.infos:
+      t = d["term"]
+      n, K = t.n, d["K"]
+      codes = d["codes"][:n * K].to(torch.int64).clone()
+      sizes = d["sizes"][:n * K].to(torch.int64).clone()
+      for a0, a1 in a_ranges:
+        off = codes - 2 - a0
+        inside = (codes >= 2) & (off >= 0) & (codes - 2 < a1)
+        row = torch.div(off, 3, rounding_mode="floor")
+        body = torch.div(row, 3, rounding_mode="floor")
+        first = inside & (row % 3 == 0)
+        codes = torch.where(first, a0 + 9 * body + 2, torch.where(inside, torch.zeros_like(codes), codes))
+        sizes = torch.where(first, torch.full_like(sizes, 9), torch.where(inside, torch.zeros_like(sizes), sizes))
+      codes = codes.to(torch.int32).contiguous()
+      sizes = sizes.to(torch.int16).contiguous()
+      perm = torch.empty(max(n * K, 1), dtype=torch.int16, device=_dev())
+      outer = torch.empty(n + 1, dtype=torch.int32, device=_dev())
+      L.call("ys_compress_indices", L.ptr(codes), L.ptr(sizes), n, K, L.ptr(perm), None, L.ptr(outer), s)
+      m = int(outer[n].item()) if n else 0
+      info.append((codes, sizes, perm, outer, n, K, m, total))
+      total += m
+    coords = torch.empty(max(2 * total, 2), dtype=torch.int32, device=_dev())
+    dims = torch.empty(max(2 * total, 2), dtype=torch.int16, device=_dev())
+    for codes, sizes, perm, outer, n, K, m, off in info:
+      if m:
+        L.call("ys_compute_coordinates", L.ptr(codes), L.ptr(perm), L.ptr(sizes), L.ptr(outer), n, K,
+               coords.data_ptr() + 8 * off, dims.data_ptr() + 4 * off, s)
+    ref = _Pattern(coords, dims, total)
+    # value map: every reference entry (R + a, C + b) from the 3x3 block that
+    # holds it in the internal upper storage (transposed below the diagonal)
+    nu, N = ref.num_unique, self.rows
+    pos = ref.positions[:2 * nu].view(nu, 2).to(torch.int64)
+    dm = ref.dims[:2 * nu].view(nu, 2).to(torch.int64)
+    voff = ref.value_offset[:nu].to(torch.int64)
+    hw = dm[:, 0] * dm[:, 1]
+    blk = torch.repeat_interleave(torch.arange(nu, device=_dev()), hw)
+    local = torch.arange(int(hw.sum().item()), device=_dev()) - torch.repeat_interleave(torch.cumsum(hw, 0) - hw, hw)
+    a_ = torch.div(local, dm[blk, 1], rounding_mode="floor")
+    b_ = local % dm[blk, 1]
+    r, c = pos[blk, 0] + a_, pos[blk, 1] + b_
+    lo, hi = torch.minimum(r, c), torch.maximum(r, c)
+    swap = r > c
+    ipos = p.positions[:2 * p.num_unique].view(-1, 2).to(torch.int64)
+    keys = ipos[:, 0] * N + ipos[:, 1]
+    want = (lo - lo % 3) * N + (hi - hi % 3)
+    ib = torch.searchsorted(keys, want)
+    ib = torch.clamp(ib, max=max(p.num_unique - 1, 0))
+    if not bool((keys[ib] == want).all()):
+      raise RuntimeError("hessian: reference layout names a block the internal pattern does not hold")
+    er = torch.where(swap, c % 3, r % 3)
+    ec = torch.where(swap, r % 3, c % 3)
+    src = p.value_offset[:p.num_unique].to(torch.int64)[ib] + 3 * er + ec
+    dst = voff[blk] + local
+    vmap = torch.empty(max(ref.total_values, 1), dtype=torch.int64, device=_dev())
+    vmap[dst] = src
+    bs.ref_view = (p, ref, vmap)
+    return ref, vmap
+
   # -- reference attribute surface ---------------------------------------------------
   def _set_attr(self, bs, name):
     p = bs.pattern if bs is not None else None
+    if p is not None and p.num_unique and self.wide_targets:
+      ref, vmap = self._reference_view(bs)
+      if name == "values":
+        return bs.values[vmap[:max(ref.total_values, 1)]]
+      if name == "lookups":
+        return ref.lookup[:ref.m]
+      return {"positions": ref.positions[:2 * ref.num_unique], "starts": ref.category_starts,
+              "counts": ref.category_counts, "dims": ref.category_dims}[name]
     if p is None or p.num_unique == 0:
       return {"values": _torch().zeros(1, dtype=_torch().float64, device=_dev()),
               "positions": _torch().zeros(2, dtype=_torch().int32, device=_dev()), "starts": [],
-              "counts": [], "dims": []}[name]
+              "counts": [], "dims": [], "lookups": _torch().zeros(0, dtype=_torch().int32, device=_dev())}[name]
     return {"values": bs.values, "positions": p.positions[:2 * p.num_unique], "starts": p.category_starts,
-            "counts": p.category_counts, "dims": p.category_dims}[name]
+            "counts": p.category_counts, "dims": p.category_dims, "lookups": p.lookup[:p.m]}[name]
 
   blocks_flattened = property(lambda self: self._set_attr(self._static, "values"))
   block_positions = property(lambda self: self._set_attr(self._static, "positions"))
@@ -694,6 +788,10 @@ class hessian:
   blocks_start_indices_dynamic = property(lambda self: self._set_attr(self._dynamic, "starts"))
   block_counts_dynamic = property(lambda self: self._set_attr(self._dynamic, "counts"))
   block_dimensions_dynamic = property(lambda self: self._set_attr(self._dynamic, "dims"))
+  # occurrence -> value offset of every element block, flattened over the
+  # terms in order (the reference's lookup arrays, hessian.pyx:782-808)
+  lookups = property(lambda self: self._set_attr(self._static, "lookups"))
+  lookups_dynamic = property(lambda self: self._set_attr(self._dynamic, "lookups"))
 
   @property
   def block_sets(self):
