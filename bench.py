@@ -448,7 +448,8 @@ def cloth_leg(args):
     # device assembled (each element kind of it matches the oracle in the
     # tests): an independent residual, not the solver's own
     Hc = mz.activeHessian()
-    A = blocks_to_csr(Hc.block_positions.cpu().numpy(), Hc.blocks_flattened.cpu().numpy(), Hc.rows)
+    pos3, val3 = Hc.blocks3()
+    A = blocks_to_csr(pos3.cpu().numpy(), val3.cpu().numpy(), Hc.rows)
     g = Hc.gradient.value.cpu().numpy()
     x = solver.implementation.solution.cpu().numpy()
     out[name]["host_fp64_rel_residual"] = float(np.linalg.norm(g - A @ x) / np.linalg.norm(g))

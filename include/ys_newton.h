@@ -495,6 +495,15 @@ typedef struct ys_pcg_args {
   double* solution;             /* [n] in: initial guess unless zero_initial_guess */
   int32_t zero_initial_guess;
   double* workspace;            /* ys_pcg_workspace_doubles(n) doubles             */
+  /* Block-Jacobi with targets wider than 3 (a 9-DoF affine matrix is three
+   * 3-DoF variables whose 9x9 diagonal block is inverted whole,
+   * diagonalBlockInverseKernel.pyx:40-215): jacobi_group[i] = first variable
+   * of i's group | (group size << 30), group size 1 or 3, and
+   * jacobi_inverse holds per variable the 3 x 9 row strip of its group's
+   * inverse (27 doubles, row-major, columns of the group's variables in
+   * order).  NULL: every group is one variable and jacobi_inverse holds 3x3
+   * blocks (9 doubles a variable).                                         */
+  const uint32_t* jacobi_group;
 } ys_pcg_args;
 
 /* With YS_PREC_MAS a finite non-positive curvature p^T H p (rounding on an

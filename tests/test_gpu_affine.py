@@ -23,13 +23,20 @@ def rel(a, b):
 
 
 def _dense(H):
+  """Dense matrix from the public block attributes (any block categories)."""
   pos = H.block_positions.cpu().numpy().astype(np.int64).reshape(-1, 2)
-  vals = H.blocks_flattened.cpu().numpy()[:9 * pos.shape[0]].reshape(-1, 3, 3)
+  vals = H.blocks_flattened.cpu().numpy()
+  dims = np.asarray(H.block_dimensions, dtype=np.int64).reshape(-1, 2)
   d = np.zeros((H.rows, H.rows))
-  for (r, c), b in zip(pos, vals):
-    d[r:r + 3, c:c + 3] += b
-    if r != c:
-      d[c:c + 3, r:r + 3] += b.T
+  k = 0
+  for (h, w), cnt, start in zip(dims, H.block_counts, H.blocks_start_indices):
+    for j in range(cnt):
+      r, c = pos[k]
+      b = vals[start + j * h * w:start + (j + 1) * h * w].reshape(h, w)
+      d[r:r + h, c:c + w] += b
+      if r != c:
+        d[c:c + w, r:r + h] += b.T
+      k += 1
   return d
 
 
@@ -45,13 +52,33 @@ def _scene(method, seed=1, nb=3, m=3):
 def test_affine_assembly_matches_oracle(method):
   cube, bodies, sc, _ = _scene(method)
   H = sc.minimizer.computeNumericValue()
-  dense, grad, diag, energy, _ = oracle_assembly(cube, bodies, projection_method=method)
-  assert H.block_dimensions == [3, 3]
+  dense, grad, diag, energy, pat = oracle_assembly(cube, bodies, projection_method=method)
   assert rel(H.gradient.value.cpu().numpy(), grad) <= 1e-12
   assert rel(_dense(H), dense) <= 1e-12
   assert rel(H.diagonal_blocks.cpu().numpy(), diag) <= 1e-12
   assert rel(H.diagonal.cpu().numpy(), np.diag(dense)) <= 1e-12
   assert abs(sc.computeTotalEnergy() - energy) <= 1e-12 * abs(energy)
+
+
+def test_affine_reference_layout_bit_exact():
+  """The public block attributes of a scene with 9-DoF affine targets carry
+  the reference's layout: categories (9x9, 9x3, 3x9, 3x3 ...) in (h, w, row,
+  col) order, block positions, category counts and value starts, and the
+  lookup of every element block, bit-exact against the oracle pattern built
+  with 9-DoF slots; the values at 1e-12."""
+  cube, bodies, sc, _ = _scene(1)
+  H = sc.minimizer.computeNumericValue()
+  _, _, _, _, pat = oracle_assembly(cube, bodies, projection_method=1)
+  pos = H.block_positions.cpu().numpy().astype(np.int64).reshape(-1, 2)
+  assert np.array_equal(pos, pat.positions)
+  assert H.block_dimensions == pat.category_dims.reshape(-1).tolist()
+  assert sorted(set(map(tuple, pat.category_dims.tolist()))) >= [(3, 3), (3, 9), (9, 3), (9, 9)]
+  assert H.block_counts == pat.category_counts.tolist()
+  assert H.blocks_start_indices == pat.category_starts.tolist()
+  assert np.array_equal(H.lookups.cpu().numpy().astype(np.int64), np.concatenate(pat.lookups))
+  # values: the same matrix through both layouts
+  dense, *_ = oracle_assembly(cube, bodies, projection_method=1)
+  assert rel(_dense(H), dense) <= 1e-12
 
 
 def test_affine_projection_is_exercised():
@@ -81,3 +108,25 @@ def test_affine_bodies_reject_mixed_tets():
   sc, _ = scenes.affine_scene(cube, bodies)
   with pytest.raises(ValueError, match="one body"):
     sc.minimizer.computeNumericValue()
+
+
+def test_affine_scene_block_jacobi_with_9x9_blocks():
+  """Block-Jacobi PCG with the 9x9 diagonal blocks of the affine matrices
+  (pseudo-inverted whole, diagonalBlockInverseKernel.pyx:40-215) and 3x3
+  blocks elsewhere, against the oracle's block-Jacobi PCG on the same
+  system: the reference's return code within one iteration and the solution
+  at the reference's squared preconditioned stopping rule."""
+  cube, bodies, sc, _ = _scene(1, seed=2, nb=4)
+  sc.minimizer.setSolver("jacobian")
+  H = sc.minimizer.computeNumericValue()
+  dense, grad, diag, _, pat = oracle_assembly(cube, bodies, projection_method=1)
+  nf, nb = cube.free_count, bodies.num_bodies
+  counts, sizes = [nf, nb, nb], [3, 9, 3]
+  inv = solvers.diagonal_inverse(diag, counts, sizes)
+  ref = solvers.jacobi_pcg(lambda v: dense @ v, grad, inv, counts, sizes, 1e-14, 4000)
+  code = sc.minimizer.linearSolver.computeSolution(H, H.gradient, None, tolerance=1e-14, maxIterations=4000,
+                                                   zero_initial_guess=True)
+  assert ref.status > 0 and abs(code - ref.status) <= 1
+  x = sc.minimizer.linearSolver.solution.cpu().numpy()
+  assert solvers.relative_residual(lambda v: dense @ v, grad, x) <= 10 * solvers.relative_residual(
+      lambda v: dense @ v, grad, ref.solution) + 1e-9

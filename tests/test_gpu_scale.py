@@ -96,7 +96,8 @@ def test_cloth_with_bodies_precision_form():
     mz.setSolver("mas", mixed_spmv=mixed, stop_rule="residual")
     mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=5000)
     Hc = mz.activeHessian()
-    A = blocks_to_csr(Hc.block_positions.cpu().numpy(), Hc.blocks_flattened.cpu().numpy(), Hc.rows)
+    pos3, val3 = Hc.blocks3()
+    A = blocks_to_csr(pos3.cpu().numpy(), val3.cpu().numpy(), Hc.rows)
     g = Hc.gradient.value.cpu().numpy()
     x = mz.linearSolver.implementation.solution.cpu().numpy()
     assert np.linalg.norm(g - A @ x) <= 1e-6 * np.linalg.norm(g)

@@ -94,7 +94,7 @@ class Matrix3(C.Structure):
 class PcgArgs(C.Structure):
   _fields_ = [("matrix", Matrix3), ("precision", i32), ("preconditioner", i32), ("jacobi_inverse", vp), ("mas", vp),
               ("stop_rule", i32), ("tolerance", f64), ("max_iterations", u32), ("rhs", vp), ("solution", vp),
-              ("zero_initial_guess", i32), ("workspace", vp)]
+              ("zero_initial_guess", i32), ("workspace", vp), ("jacobi_group", vp)]
 
 
 class PcgResult(C.Structure):

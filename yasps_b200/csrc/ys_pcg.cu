@@ -41,6 +41,7 @@ struct PcgParams {
   int zero_guess;
   int restart_on_curvature;  // MAS: a non-positive curvature restarts from M^-1 r (zero step, beta = 0)
   TiledSet tiled;            // tile plan of the FP32 set (pcg_spmv_dot_tiled)
+  const uint32_t* jgroup;    // block-Jacobi groups (first var | size << 30) or null: 3x3 blocks
   double tolerance;
   uint32_t max_it;
   cudaGraphConditionalHandle cond;
@@ -56,6 +57,64 @@ __device__ __forceinline__ void jacobi3(const double* __restrict__ inv, uint32_t
 
 __device__ __forceinline__ bool stop_reached(const PcgParams& P, double delta_new, double rr) {
   return P.stop_rule == YS_STOP_RESIDUAL ? rr <= P.st[kTolAbs] : delta_new <= P.st[kTolAbs];
+}
+
+// Start of the solve from the initial reductions v = (r.z, r.r, g.g,
+// g.M^-1 g) (thread 0 of the last block): the stop threshold and the status.
+__device__ __forceinline__ void pcg_init_finish(const PcgParams& P, const double (&v)[4]) {
+  double* st = P.st;
+  const double delta_new = v[0];
+  const double delta0 = P.zero_guess ? v[0] : v[3];
+  st[kDeltaNew] = delta_new;
+  st[kDelta0] = delta0;
+  st[kRR] = v[1];
+  st[kRR0] = v[1];
+  st[kGG] = v[2];
+  st[kIter] = 0.0;
+  st[kAlpha] = 0.0;
+  st[kBeta] = 0.0;
+  st[kBarrierFail] = 0.0;
+  st[kRestart] = 0.0;
+  int status = kContinue;
+  double tol;
+  if (P.stop_rule == YS_STOP_RESIDUAL) {
+    tol = P.st[kTolParam] * P.st[kTolParam] * v[2];
+    if (!(isfinite(v[1]) && isfinite(v[2]))) status = kInvalidInit;
+    else if (v[1] <= tol) status = kConverged;
+    else if (!(isfinite(delta_new) && delta_new > 0.0)) status = kInvalidInit;
+  } else {
+    // solverKernel.pyx:588-604
+    tol = P.st[kTolParam] * delta0;
+    if (!(isfinite(delta0) && delta0 >= 0.0 && isfinite(delta_new) && delta_new >= 0.0)) status = kInvalidInit;
+    else if (!(isfinite(tol) && tol >= 0.0)) status = kInvalidInit;
+    else if (delta_new <= tol) status = kConverged;
+  }
+  if (status == kContinue && P.st[kMaxItParam] < 1.0) status = kMaxIter;
+  st[kTolAbs] = tol;
+  st[kStatus] = (double)status;
+  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+}
+
+// Iteration bookkeeping from v = (r.z, r.r) (thread 0 of the last block).
+__device__ __forceinline__ void pcg_update_finish(const PcgParams& P, const double (&v)[2]) {
+  double* st = P.st;
+  const double delta_new = v[0], delta_old = st[kDeltaOld];
+  const double it = st[kIter] + 1.0;
+  st[kIter] = it;
+  st[kDeltaNew] = delta_new;
+  st[kRR] = v[1];
+  int status = kContinue;
+  // finishCgIteration (solverKernel.pyx:420-438)
+  if (!isfinite(delta_new) || delta_new < 0.0 || !isfinite(delta_old) || delta_old <= 0.0) {
+    st[kBeta] = 0.0;
+    status = kNonSpd;
+  } else {
+    st[kBeta] = delta_new / delta_old;
+    if (stop_reached(P, delta_new, v[1])) status = kConverged;
+    else if (it >= P.st[kMaxItParam]) status = kMaxIter;
+  }
+  st[kStatus] = (double)status;
+  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
 }
 
 // Initial residual, preconditioned residual and the stop threshold.
@@ -89,37 +148,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_init_bj(PcgParams P) {
   }
   if (!grid_reduce_last<4>(v, P.partials, P.tickets)) return;
   if (threadIdx.x != 0) return;
-  double* st = P.st;
-  const double delta_new = v[0];
-  const double delta0 = P.zero_guess ? v[0] : v[3];
-  st[kDeltaNew] = delta_new;
-  st[kDelta0] = delta0;
-  st[kRR] = v[1];
-  st[kRR0] = v[1];
-  st[kGG] = v[2];
-  st[kIter] = 0.0;
-  st[kAlpha] = 0.0;
-  st[kBeta] = 0.0;
-  st[kBarrierFail] = 0.0;
-  st[kRestart] = 0.0;
-  int status = kContinue;
-  double tol;
-  if (P.stop_rule == YS_STOP_RESIDUAL) {
-    tol = P.st[kTolParam] * P.st[kTolParam] * v[2];
-    if (!(isfinite(v[1]) && isfinite(v[2]))) status = kInvalidInit;
-    else if (v[1] <= tol) status = kConverged;
-    else if (!(isfinite(delta_new) && delta_new > 0.0)) status = kInvalidInit;
-  } else {
-    // solverKernel.pyx:588-604
-    tol = P.st[kTolParam] * delta0;
-    if (!(isfinite(delta0) && delta0 >= 0.0 && isfinite(delta_new) && delta_new >= 0.0)) status = kInvalidInit;
-    else if (!(isfinite(tol) && tol >= 0.0)) status = kInvalidInit;
-    else if (delta_new <= tol) status = kConverged;
-  }
-  if (status == kContinue && P.st[kMaxItParam] < 1.0) status = kMaxIter;
-  st[kTolAbs] = tol;
-  st[kStatus] = (double)status;
-  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+  pcg_init_finish(P, v);
 }
 
 // Curvature p^T q (grid reduction) and the step length; the last block of
@@ -212,24 +241,106 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_update_bj(PcgParams P) {
   }
   if (!grid_reduce_last<2>(v, P.partials, P.tickets + 2)) return;
   if (threadIdx.x != 0 || !live) return;
-  double* st = P.st;
-  const double delta_new = v[0], delta_old = st[kDeltaOld];
-  const double it = st[kIter] + 1.0;
-  st[kIter] = it;
-  st[kDeltaNew] = delta_new;
-  st[kRR] = v[1];
-  int status = kContinue;
-  // finishCgIteration (solverKernel.pyx:420-438)
-  if (!isfinite(delta_new) || delta_new < 0.0 || !isfinite(delta_old) || delta_old <= 0.0) {
-    st[kBeta] = 0.0;
-    status = kNonSpd;
-  } else {
-    st[kBeta] = delta_new / delta_old;
-    if (stop_reached(P, delta_new, v[1])) status = kConverged;
-    else if (it >= P.st[kMaxItParam]) status = kMaxIter;
+  pcg_update_finish(P, v);
+}
+
+// ---- block-Jacobi over variable groups ----------------------------------------
+// A target wider than 3 (the 9-DoF affine matrix of a body, stored as three
+// 3-DoF rows) has one diagonal block of 9x9 whose pseudo-inverse couples its
+// three rows (diagonalBlockInverseKernel.pyx:40-215 inverts per attribute
+// block).  With jgroup, jinv holds for every 3-DoF variable the 3 x 9 strip of
+// its group's inverse (27 doubles, row-major; columns of the group's
+// variables in order) and jgroup[i] = first variable of i's group | (group
+// size << 30).  The thread of a group's first variable updates the whole
+// group, so every z of the group sees the group's new residual.
+constexpr uint32_t kGroupShift = 30;
+
+__device__ __forceinline__ void group_apply(const double* __restrict__ jinv, uint32_t g, int gs, const double* rr,
+                                            double* zz) {
+  for (int s = 0; s < gs; ++s) {
+    const double* strip = jinv + 27ull * (g + s);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double acc = 0.0;
+      for (int t = 0; t < 3 * gs; ++t) acc += strip[9 * k + t] * rr[t];
+      zz[3 * s + k] = acc;
+    }
   }
-  st[kStatus] = (double)status;
-  cudaGraphSetConditional(P.cond, status == kContinue ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kPcgBlock) pcg_init_bjw(PcgParams P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};  // r.z, r.r, g.g, g.M^-1 g
+  if (i < P.nv && (P.jgroup[i] & ((1u << kGroupShift) - 1)) == i) {
+    const int gs = (int)(P.jgroup[i] >> kGroupShift);
+    double gg[9], rr[9], zz[9], yy[9];
+    for (int s = 0; s < gs; ++s) {
+      const uint32_t j = i + s;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) gg[3 * s + k] = rr[3 * s + k] = P.rhs[3ull * j + k];
+      if (P.zero_guess) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) P.x[3ull * j + k] = 0.0;
+      } else {
+        double h0, h1, h2;
+        spmv3_row(P.sets, P.nsets, P.fp32, j, P.x, h0, h1, h2);
+        rr[3 * s] -= h0; rr[3 * s + 1] -= h1; rr[3 * s + 2] -= h2;
+      }
+    }
+    group_apply(P.jinv, i, gs, rr, zz);
+    if (!P.zero_guess) group_apply(P.jinv, i, gs, gg, yy);
+    for (int s = 0; s < gs; ++s) {
+      const uint32_t j = i + s;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int q = 3 * s + k;
+        P.r[3ull * j + k] = rr[q];
+        P.z[3ull * j + k] = zz[q];
+        P.p[3ull * j + k] = zz[q];
+        v[0] += rr[q] * zz[q];
+        v[1] += rr[q] * rr[q];
+        v[2] += gg[q] * gg[q];
+        if (!P.zero_guess) v[3] += gg[q] * yy[q];
+      }
+      if (P.p32) P.p32[j] = make_float4((float)zz[3 * s], (float)zz[3 * s + 1], (float)zz[3 * s + 2], 0.0f);
+    }
+  }
+  if (!grid_reduce_last<4>(v, P.partials, P.tickets)) return;
+  if (threadIdx.x != 0) return;
+  pcg_init_finish(P, v);
+}
+
+__global__ void __launch_bounds__(kPcgBlock) pcg_update_bjw(PcgParams P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = P.st[kStatus] == (double)kContinue;
+  double v[2] = {0.0, 0.0};
+  if (i < P.nv && live && (P.jgroup[i] & ((1u << kGroupShift) - 1)) == i) {
+    const int gs = (int)(P.jgroup[i] >> kGroupShift);
+    const double alpha = P.st[kAlpha];
+    double rr[9], zz[9];
+    for (int s = 0; s < gs; ++s) {
+      const uint32_t j = i + s;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        P.x[3ull * j + k] = P.x[3ull * j + k] + P.p[3ull * j + k] * alpha;
+        rr[3 * s + k] = P.r[3ull * j + k] - P.q[3ull * j + k] * alpha;
+        P.r[3ull * j + k] = rr[3 * s + k];
+      }
+    }
+    group_apply(P.jinv, i, gs, rr, zz);
+    for (int s = 0; s < gs; ++s) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int q = 3 * s + k;
+        P.z[3ull * (i + s) + k] = zz[q];
+        v[0] += rr[q] * zz[q];
+        v[1] += rr[q] * rr[q];
+      }
+    }
+  }
+  if (!grid_reduce_last<2>(v, P.partials, P.tickets + 2)) return;
+  if (threadIdx.x != 0 || !live) return;
+  pcg_update_finish(P, v);
 }
 
 __global__ void __launch_bounds__(kPcgBlock) pcg_direction(PcgParams P) {
@@ -406,6 +517,7 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   P.partials = w; w += (uint64_t)ys::kRowLanes * (grid + 2);
   P.tickets = reinterpret_cast<unsigned*>(w);
   P.jinv = a.jacobi_inverse;
+  P.jgroup = a.jacobi_group;
   P.stop_rule = a.stop_rule;
   P.zero_guess = a.zero_initial_guess;
   P.restart_on_curvature = a.preconditioner == YS_PREC_MAS;
@@ -432,7 +544,9 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   if (e == cudaSuccess) {
     if (a.preconditioner == YS_PREC_BLOCK_JACOBI) {
       void* args0[] = {&P};
-      e = ys::add_kernel(h->graph, &init, &reset, 1, (const void*)ys::pcg_init_bj, grid, ys::kPcgBlock, args0);
+      e = ys::add_kernel(h->graph, &init, &reset, 1,
+                         P.jgroup ? (const void*)ys::pcg_init_bjw : (const void*)ys::pcg_init_bj, grid, ys::kPcgBlock,
+                         args0);
     } else {
       e = ys::mas_add_init_nodes(a.mas, h->graph, &reset, 1, &init, P.nv, P.rhs, P.x, P.r, P.p, P.p32, P.q, P.z, P.st, P.partials,
                                  P.tickets, P.sets, P.nsets, P.fp32, P.stop_rule, P.zero_guess, P.tolerance, P.max_it,
@@ -459,7 +573,9 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
                            grid_rows, ys::kPcgBlock, args1);
       if (e == cudaSuccess) {
         if (a.preconditioner == YS_PREC_BLOCK_JACOBI) {
-          e = ys::add_kernel(body, &n2, &n1, 1, (const void*)ys::pcg_update_bj, grid, ys::kPcgBlock, args1);
+          e = ys::add_kernel(body, &n2, &n1, 1,
+                             P.jgroup ? (const void*)ys::pcg_update_bjw : (const void*)ys::pcg_update_bj, grid,
+                             ys::kPcgBlock, args1);
         } else {
           e = ys::mas_add_update_nodes(a.mas, body, &n1, 1, &n2, &h->mas);
         }

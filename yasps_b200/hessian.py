@@ -793,6 +793,13 @@ class hessian:
   lookups = property(lambda self: self._set_attr(self._static, "lookups"))
   lookups_dynamic = property(lambda self: self._set_attr(self._dynamic, "lookups"))
 
+  def blocks3(self):
+    """``(positions [2 nu], values [9 nu])`` of the static set in the internal
+    3x3 storage the device kernels run on (the public attributes give the
+    reference's layout, which differs for 9-DoF targets)."""
+    p = self._static.pattern
+    return p.positions[:2 * p.num_unique], self._static.values[:9 * p.num_unique]
+
   @property
   def block_sets(self):
     return [bs for bs in (self._static, self._dynamic) if bs.pattern is not None and bs.pattern.num_unique]

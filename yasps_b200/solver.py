@@ -88,7 +88,7 @@ class _PcgBase:
       self._work = torch.zeros(int(L.load().ys_pcg_workspace_doubles(n)), dtype=torch.float64, device=_dev())
       self._cache.release()
 
-  def _run_pcg(self, H, rhs, x, fp32, prec_kind, jinv, mas_handle, tol, maxit, zero_guess, stop_rule):
+  def _run_pcg(self, H, rhs, x, fp32, prec_kind, jinv, mas_handle, tol, maxit, zero_guess, stop_rule, jgroup=None):
     """One device PCG solve into ``x``; returns the ys_pcg_result."""
     # the graph holds every device pointer of the matrix: a rebuilt pattern
     # (dynamic terms) gives new row plans and must give a new graph
@@ -96,7 +96,7 @@ class _PcgBase:
                   tuple(0 if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else t) for t in H.tile_plan(bs))
                   for bs in H.block_sets)
     key = (id(H), H.rows, rhs.data_ptr(), x.data_ptr(), fp32, prec_kind, None if jinv is None else jinv.data_ptr(),
-           mas_handle, bool(zero_guess), stop_rule,
+           mas_handle, bool(zero_guess), stop_rule, None if jgroup is None else jgroup.data_ptr(),
            tuple(bs.values.data_ptr() for bs in H.block_sets),
            tuple(0 if bs.values32 is None else bs.values32.data_ptr() for bs in H.block_sets), plans)
 
@@ -114,6 +114,7 @@ class _PcgBase:
       args.solution = L.ptr(x)
       args.zero_initial_guess = 1 if zero_guess else 0
       args.workspace = L.ptr(self._work)
+      args.jacobi_group = L.ptr(jgroup)
       h = ctypes.c_void_p()
       L.call("ys_pcg_create", ctypes.byref(args), ctypes.byref(h))
       return h, args
@@ -199,9 +200,8 @@ class jacobianPCGSolver(_PcgBase):
       raise ValueError("jacobianPCGSolver.computeSolution: right_hand_side size must match the Hessian size.")
     torch = _torch()
     H = active_hessian
-    if any(w.size != 3 for w in H.wrt):
-      raise NotImplementedError("the device block-Jacobi PCG inverts 3x3 variable blocks; scenes with 9-DoF "
-                                "affine attributes are solved with the MAS solver")
+    if any(w.size not in (3, 9) for w in H.wrt):
+      raise NotImplementedError("the device block-Jacobi PCG takes 3- and 9-DoF targets")
     if self._jinv is None or self._jinv.numel() != H.diagonal_blocks.numel():
       self._jinv = torch.zeros_like(H.diagonal_blocks)
     nat = len(H.wrt)
@@ -209,14 +209,49 @@ class jacobianPCGSolver(_PcgBase):
     L.call("ys_invert_diagonal_blocks", L.ptr(H.diagonal_blocks), L.ptr(self._jinv), nat,
            arr(H.diagonal_blocks_start_cpu[:nat]), arr([w.correspondance.numInstances for w in H.wrt]),
            arr([w.size for w in H.wrt]), L.stream_ptr())
+    jinv, jgroup = self._jinv, None
+    if any(w.size == 9 for w in H.wrt):
+      jinv, jgroup = self._group_strips(H)
     if not zero_initial_guess:
       self._solution.copy_(_as_tensor(initial_guess))
-    res = self._run_pcg(H, rhs, self._solution, False, L.YS_PREC_BLOCK_JACOBI, self._jinv, None, tolerance,
-                        maxIterations, zero_initial_guess, self.stop_rule)
+    res = self._run_pcg(H, rhs, self._solution, False, L.YS_PREC_BLOCK_JACOBI, jinv, None, tolerance,
+                        maxIterations, zero_initial_guess, self.stop_rule, jgroup)
     self._statistics = {"solver": "jacobian", "converged": res.status >= 0, "iterations": int(res.iterations),
                         "result": int(res.status), "solve_seconds": time.perf_counter() - t0,
                         "matrix_size": int(H.rows), "tolerance": float(tolerance)}
     return int(res.status)
+
+
+  def _group_strips(self, H):
+    """Per 3-DoF variable, the 3 x 9 row strip of its attribute block's
+    pseudo-inverse and its group word (first variable | size << 30): a
+    3-DoF target is a group of one, a 9-DoF target (the affine matrix of a
+    body, three internal 3-DoF rows) a group of three."""
+    torch = _torch()
+    nv = H.rows // 3
+    key = (nv, tuple((w.size, w.correspondance.numInstances) for w in H.wrt))
+    if getattr(self, "_strip_key", None) != key:
+      self._strips = torch.zeros((nv, 3, 9), dtype=torch.float64, device=_dev())
+      grp = np.zeros(nv, dtype=np.int64)
+      for k, w in enumerate(H.wrt):
+        v0, cnt = H.gradient_segments_start_cpu[k] // 3, w.correspondance.numInstances
+        if w.size == 3:
+          ids = v0 + np.arange(cnt)
+          grp[ids] = ids | (1 << 30)
+        else:
+          first = v0 + 3 * np.arange(cnt)
+          grp[v0:v0 + 3 * cnt] = np.repeat(first, 3) | (3 << 30)
+      self._jgroup = torch.from_numpy(grp.astype(np.uint32).view(np.int32)).to(_dev())
+      self._strip_key = key
+    strips = self._strips
+    for k, w in enumerate(H.wrt):
+      v0, cnt = H.gradient_segments_start_cpu[k] // 3, w.correspondance.numInstances
+      d0 = H.diagonal_blocks_start_cpu[k]
+      if w.size == 3:
+        strips[v0:v0 + cnt, :, :3] = self._jinv[d0:d0 + 9 * cnt].view(cnt, 3, 3)
+      else:
+        strips[v0:v0 + 3 * cnt] = self._jinv[d0:d0 + 81 * cnt].view(cnt, 3, 3, 9).reshape(3 * cnt, 3, 9)
+    return strips.view(-1), self._jgroup
 
 
 class masSolver(_PcgBase):
