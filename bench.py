@@ -60,6 +60,9 @@ def parse():
   p.add_argument("--no-cloth", action="store_true", help="skip the cloth + contact leg")
   p.add_argument("--serving-requests", type=int, default=512,
                  help="requests of the serving stream (0: skip the serving leg)")
+  p.add_argument("--workload", default="fem64", choices=["fem64", "mixed-serving"],
+                 help="fem64: the headline line; mixed-serving: only the mixed serving stream (64 cloth + "
+                      "affine-body + contact scenes beside 8 FEM cubes of 126^3 vertices, 150 GB budget)")
   return p.parse_args()
 
 
@@ -459,6 +462,82 @@ def cloth_leg(args):
   return out
 
 
+def mixed_serving_leg(args):
+  """The mixed serving stream: 64 cloth + affine-body + contact scenes (cloth
+  side U{64..256}, 2..16 icosphere bodies, 10k..200k barrier pairs, each its
+  own topology) interleaved with 8 FEM cubes of 126^3 vertices (E=1e6,
+  nu=0.45, noise +-0.005), Poisson arrivals (mean gap 2 ms) and all at once,
+  a 150 GB admission budget; the precision form served beside the serial
+  plain FP64 path.  Errors: every solution's true relative residual under the
+  device FP64 system, and under the FP64 oracle's system for a sample (the
+  three smallest and the largest cloth scene, one FEM cube)."""
+  import torch
+  from oracle import baseline, cloth_scene
+  from yasps_b200 import scenes, serving
+  wl = serving.mixed_workload(seed=0)
+  srv = serving.NewtonServer(max_slots=len(wl.order), passes=8, memory_budget=150e9, tolerance=args.tol,
+                             max_iterations=5000)
+  t0 = time.perf_counter()
+  for spec in wl.scenes:
+    srv.add_topology(serving.cloth_scene_topology(spec))
+  srv.register([sp.key for sp in wl.scenes], slots_per_side=1)
+  srv.register([wl.fem_side], slots_per_side=len(wl.fem))
+  t_register = time.perf_counter() - t0
+  hbm, peak_kind = peaks()
+  fem_topo = srv.topology(wl.fem_side)
+  big = max(wl.scenes, key=lambda sp: sp.side)
+  spmv = {"fem_126": spmv_roofline(fem_topo.H, hbm, peak_kind, wl.fem_side),
+          "cloth_largest": spmv_roofline(srv.topology(big.key).H, hbm, peak_kind, big.side)}
+  for v in spmv.values():
+    v["traffic"] = None
+  # warm-up: the stream once each way (CUDA graphs of the size buckets, the
+  # FP64 solver state of every topology)
+  srv.run(wl.requests(srv))
+  srv.solve_serial_fp64(wl.requests(srv))
+  clocks = Clocks(torch.cuda.current_device())
+  clocks.start()
+  created = srv.slots_created
+  done = srv.run(wl.requests(srv))
+  out = {"workload": (f"{len(wl.scenes)} cloth + affine-body + contact scenes (cloth side U{{64..256}}, 2..16 "
+                      f"icosphere bodies of 2,562 vertices, 10k..200k barrier pairs, lagged PT friction; each "
+                      f"its own topology) interleaved with {len(wl.fem)} SNH FEM cubes of {wl.fem_side}^3 vertices "
+                      f"({(wl.fem_side - 1) ** 3 * 6:,} tets, E=1e6, nu=0.45, noise +-0.005); Poisson arrivals "
+                      "(mean gap 2 ms) and all at once; 150 GB admission budget; solve to 1e-6 true relative "
+                      "residual"),
+         "register_topologies_s": t_register,
+         "cloth_vertices": int(sum(sp.side ** 2 for sp in wl.scenes)),
+         "fem_dof_each": int(fem_topo.n)}
+  out["served"] = serving.stream_stats(done)
+  out["served_saturated"] = serving.stream_stats(srv.run(wl.requests(srv, all_at_once=True)))
+  out["serial_fp64"] = serving.stream_stats(srv.solve_serial_fp64(wl.requests(srv)))
+  out["serial_fp64_saturated"] = serving.stream_stats(srv.solve_serial_fp64(wl.requests(srv, all_at_once=True)))
+  out["clocks"] = clocks.stop()
+  out["slots_created_while_timed"] = srv.slots_created - created
+  out["resident_slot_gb"] = srv.resident_bytes / 1e9
+  out["max_allocated_gb"] = torch.cuda.max_memory_allocated() / 1e9
+  out["spmv_roofline"] = spmv
+  # errors: device FP64 residual of every solution, oracle residual of a sample
+  out["served"]["max_rel_residual"] = max(r.relative_residual for r in done)
+  by_tag = {r.tag: r for r in done}
+  cloth_tags = sorted((k for k, (kind, _) in enumerate(wl.order) if kind == "cloth"),
+                      key=lambda k: wl.scenes[wl.order[k][1]].side)
+  sample = cloth_tags[:3] + cloth_tags[-1:]
+  oracle = {"oracle": "FP64 CPU restatement (matrix-free g and H x of each sampled request)", "cloth": {}}
+  for k in sample:
+    sp = wl.scenes[wl.order[k][1]]
+    cc = srv.topology(sp.key).cloth
+    oracle["cloth"][f"side{sp.side}_bodies{sp.bodies}_pairs{sp.pairs}"] = cloth_scene.relative_residual(
+        cc, by_tag[k].solution)
+  fem_tag = next(k for k, (kind, _) in enumerate(wl.order) if kind == "fem")
+  f = wl.fem[wl.order[fem_tag][1]]
+  cube = scenes.fem_cube(wl.fem_side, young=f["young"], poisson=f["poisson"], noise=f["noise"], seed=f["seed"])
+  oracle[f"fem_{wl.fem_side}"] = baseline.relative_residual_pooled(cube, by_tag[fem_tag].solution)
+  oracle["max_rel_residual"] = max(list(oracle["cloth"].values()) + [oracle[f"fem_{wl.fem_side}"]])
+  out["served"]["error_vs_oracle"] = oracle
+  srv.close()
+  return out
+
+
 def serving_leg(args):
   """Serving form on a seeded Poisson stream of FEM Newton steps (one GPU):
   continuous batching (FP32+refine) beside the serial plain FP64 path."""
@@ -601,10 +680,29 @@ def reference_arm(args):
   print(json.dumps(line), flush=True)
 
 
+def mixed_arm(args):
+  """``--workload mixed-serving``: the mixed serving stream alone (rank 0 of
+  one GPU), one JSON line whose value is the served stream's solves/s."""
+  import torch
+  if int(os.environ.get("WORLD_SIZE", "1")) > 1 and int(os.environ.get("RANK", "0")) != 0:
+    return
+  torch.cuda.set_device(0)
+  out = mixed_serving_leg(args)
+  line = {"metric": METRIC, "value": out["served"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+          "dtype": "f32+f64 refine (f64 element Hessians, projection and barrier terms)",
+          "data": "synthetic (seeded cloth, body and FEM scenes, no external data)",
+          "config": {"workload": out["workload"], "parallelism": "one GPU, continuous batching"},
+          "p50_ms": out["served"]["p50_ms"], "p99_ms": out["served"]["p99_ms"], "mixed_serving": out}
+  print(json.dumps(line), flush=True)
+
+
 def main():
   args = parse()
   if args.impl == "reference":
     reference_arm(args)
+  elif args.workload == "mixed-serving":
+    mixed_arm(args)
   else:
     gpu_arm(args)
 

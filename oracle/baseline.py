@@ -248,3 +248,57 @@ def timed_sample(cube, H, g, mas, iterations, sample_fraction=1.0 / 128, pcg_ite
   total = t_elem + t_mas + t_it * iterations
   return total, dict(element_s=t_elem, mas_update_s=t_mas, pcg_iteration_s=t_it, iterations=int(iterations),
                      sample_fraction=sample_fraction)
+
+
+def times_from_cube(cube, v, tet_slice=slice(None)):
+  """Gradient and Hessian product ``H v`` (free DoFs) of the cube's SNH
+  elements in ``tet_slice``, matrix-free (the same element terms and
+  projection as :func:`system_from_cube`; inertia excluded)."""
+  tets = cube.tets.astype(np.int64)[tet_slice]
+  x = cube.positions_all()[tets]
+  r = cube.rest_all()[tets]
+  _, g, h = energies.snh_from_rest(x, r, cube.mu, cube.lam, cube.dt)
+  h = projection.project_spd(h, 1)
+  npin, n = cube.pinned_count, cube.dofs
+  dof = np.where((tets >= npin)[:, :, None], 3 * (tets[:, :, None] - npin) + np.arange(3), -1).reshape(len(tets), 12)
+  m = dof >= 0
+  vl = np.where(m, np.asarray(v)[np.maximum(dof, 0)], 0.0)
+  hv = np.einsum("tij,tj->ti", h, vl)
+  grad, prod = np.zeros(n), np.zeros(n)
+  np.add.at(grad, dof[m], g[m])
+  np.add.at(prod, dof[m], hv[m])
+  return grad, prod
+
+
+_POOL_V = None
+
+
+def _times_init(cube, v):
+  global _POOL_CUBE, _POOL_V
+  _POOL_CUBE, _POOL_V = cube, v
+
+
+def _times_chunk(bounds):
+  return times_from_cube(_POOL_CUBE, _POOL_V, slice(*bounds))
+
+
+def relative_residual_pooled(cube, v, workers=None, chunk=250_000):
+  """``||g - H v|| / ||g||`` of the cube's Newton system at ``v``, element
+  terms matrix-free on spawned worker processes (safe next to a CUDA
+  context), the inertia term added once."""
+  import concurrent.futures as cf
+  import multiprocessing as mp
+  workers = max(1, int(workers or os.cpu_count() or 1))
+  v = np.asarray(v, dtype=np.float64)
+  nt = cube.tet_count
+  chunks = [(s, min(nt, s + chunk)) for s in range(0, nt, chunk)]
+  g, hv = np.zeros(cube.dofs), np.zeros(cube.dofs)
+  with cf.ProcessPoolExecutor(min(workers, len(chunks)), mp_context=mp.get_context("spawn"),
+                              initializer=_times_init, initargs=(cube, v)) as ex:
+    for gi, hi in ex.map(_times_chunk, chunks, timeout=1800):
+      g += gi
+      hv += hi
+  _, gi, _ = energies.inertia_local(cube.free_position, cube.x_tilde(), cube.mass)
+  g += gi.ravel()
+  hv += np.repeat(cube.mass, 3) * v
+  return float(np.linalg.norm(g - hv) / np.linalg.norm(g))

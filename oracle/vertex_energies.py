@@ -118,8 +118,8 @@ def baraff_witkin(x, rest, p):
   f = _membrane_f(x, rest)
   i6 = f[:, 0].dot(f[:, 1])
   i5u, i5v = torch.linalg.norm(f[:, 0]), torch.linalg.norm(f[:, 1])
-  uc = 0.01 if float(i5u.detach()) < 1.0 else 1.0
-  vc = 0.01 if float(i5v.detach()) < 1.0 else 1.0
+  uc = torch.where(i5u < 1.0, 0.01, 1.0)
+  vc = torch.where(i5v < 1.0, 0.01, 1.0)
   stretch = uc * (i5u - 1.0) ** 2 + vc * (i5v - 1.0) ** 2
   return (stretch_s * stretch + shear_s * i6 * i6) * thickness * _rest_area(rest) * dt * dt
 
@@ -146,10 +146,8 @@ def _friction(rel, p, lagged):
   eps = np.sqrt(fdhat) * dt
   fric_dhat = fdhat * dt * dt
   y = torch.sqrt(y2 + 1e-16)
-  if float(y2.detach()) > fric_dhat:
-    phi = y
-  else:
-    phi = eps / 3.0 + y2 / eps - y2 * y / (3.0 * eps * eps)
+  # the branch as a select (both sides finite), so the formula batches
+  phi = torch.where(y2 > fric_dhat, y, eps / 3.0 + y2 / eps - y2 * y / (3.0 * eps * eps))
   return rate * lam * phi
 
 
@@ -256,12 +254,43 @@ FRICTION_KINDS = (8, 9, 10, 11)
 LAGGED = {8: lagged_friction_pt, 9: lagged_friction_pe, 10: lagged_friction_ee, 11: lagged_friction_pp}
 
 
-def energy_grad_hess(kind, x, rest, params, lagged=None):
+def energy_grad_hess(kind, x, rest, params, lagged=None, chunk=16384):
   """Energy [n], gradient [n, 3A] and Hessian [n, 3A, 3A] of ``n`` elements.
 
   ``x``, ``rest``: [n, A, 3]; ``params``: the scalar parameters of the kind;
-  ``lagged``: [n, 9] for friction.
+  ``lagged``: [n, 9] for friction.  The elements are differentiated in
+  batches of ``chunk`` (``torch.func`` over the same formulas as
+  :func:`energy_grad_hess_loop`, which takes them one at a time).
   """
+  torch = _t()
+  from torch.func import grad, hessian, vmap
+  fn = KINDS[kind]
+  x = np.asarray(x, dtype=np.float64)
+  n, arity = x.shape[0], x.shape[1]
+  rest = np.zeros_like(x) if rest is None else np.asarray(rest, dtype=np.float64)
+  lag = np.zeros((n, 9)) if lagged is None else np.asarray(lagged, dtype=np.float64).reshape(n, -1)
+  fric = kind in FRICTION_KINDS
+
+  def f(v, r, lg):
+    xx = v.reshape(arity, 3)
+    return fn(xx, r, params, lg) if fric else fn(xx, r, params)
+
+  e = np.zeros(n)
+  g = np.zeros((n, 3 * arity))
+  h = np.zeros((n, 3 * arity, 3 * arity))
+  for a in range(0, n, chunk):
+    b = min(n, a + chunk)
+    v = torch.from_numpy(np.ascontiguousarray(x[a:b].reshape(b - a, -1)))
+    r = torch.from_numpy(np.ascontiguousarray(rest[a:b]))
+    lg = torch.from_numpy(np.ascontiguousarray(lag[a:b]))
+    e[a:b] = vmap(f)(v, r, lg).numpy()
+    g[a:b] = vmap(grad(f))(v, r, lg).numpy()
+    h[a:b] = vmap(hessian(f))(v, r, lg).numpy()
+  return e, g, 0.5 * (h + np.transpose(h, (0, 2, 1)))
+
+
+def energy_grad_hess_loop(kind, x, rest, params, lagged=None):
+  """:func:`energy_grad_hess` one element at a time (``torch.autograd.functional``)."""
   torch = _t()
   fn = KINDS[kind]
   x = np.asarray(x, dtype=np.float64)

@@ -75,3 +75,38 @@ def test_slots_are_reused_and_budget_bounds_residency(server):
   assert server.resident_bytes <= server.memory_budget
   assert server.resident_bytes >= before
   assert server.launches > 0
+
+
+def test_mixed_stream_of_cloth_scenes_and_fem_cubes():
+  """The mixed serving form at small size: cloth + affine-body + contact
+  scenes (their own topologies) interleaved with FEM cubes, served together;
+  every result meets the residual of its FP64 oracle system and is
+  bit-identical to the same request served alone."""
+  from oracle import cloth_scene
+  wl = serving.mixed_workload(num_scenes=3, num_fem=2, fem_side=10, side_range=(20, 28), body_range=(1, 3),
+                              pair_range=(300, 900), fem_young=1e6, fem_poisson=0.45, fem_noise=0.005,
+                              mean_spacing=5e-4, seed=7)
+  srv = serving.NewtonServer(max_slots=8, passes=4, memory_budget=4e9, max_iterations=5000)
+  try:
+    for spec in wl.scenes:
+      srv.add_topology(serving.cloth_scene_topology(spec))
+    srv.register([s.key for s in wl.scenes] + [wl.fem_side], slots_per_side=1)
+    alone = {}
+    for r in wl.requests(srv):
+      (d,) = srv.run([r])
+      alone[d.tag] = d.solution
+    done = srv.run(wl.requests(srv))
+    assert len(done) == len(wl.order)
+    for r in done:
+      assert r.converged, (r.tag, r.phase)
+      assert np.array_equal(r.solution, alone[r.tag]), r.tag
+      kind, i = wl.order[r.tag]
+      if kind == "cloth":
+        cc = srv.topology(wl.scenes[i].key).cloth
+        assert cloth_scene.relative_residual(cc, r.solution) <= 1e-6
+      else:
+        f = wl.fem[i]
+        case = (wl.fem_side, f["young"], f["poisson"], f["noise"], f["seed"])
+        assert oracle_residual(case, r.solution) <= 1e-6
+  finally:
+    srv.close()

@@ -519,7 +519,7 @@ def cloth_contact(side: int = 256, pairs: int = 200_000, spacing: float = 0.05, 
     bodies, faces = _bodies_over_cloth(rng, n, spacing, dhat, num_bodies, body_subdivisions, body_radius,
                                        body_stiffness, dt)
     body_pt = _body_cloth_pairs(bodies, faces, pos, n, spacing, dhat)
-  npt = pairs // 2 - (0 if body_pt is None else len(body_pt))
+  npt = max(0, pairs // 2 - (0 if body_pt is None else len(body_pt)))
   nee = pairs - pairs // 2
   # PT: a cloth vertex above an obstacle triangle (cloth vertex (i+1, k+1) lies over cell (i, k))
   tri_pick = rng.integers(0, len(otris), size=npt)
@@ -584,21 +584,24 @@ def cloth_contact_scene(cc: ClothContact, projection_method: int = 1):
   allv = body.addPrimitiveUnion("all_vertices", [obst, cloth])
   apos = allv.addAttribute("position")
   aold = allv.addAttribute("old_position")
-  ptp = body.addPrimitive("pt_pairs", numInstances=len(cc.pt))
-  ptc = ptp.addConnectivity("to_vertices", allv, cc.pt, 4)
-  ptx = ptp.addAttribute("x", through=ptc, source=apos)
-  pte = ptp.addAttribute("barrier", computed_attribute=point_triangle(ptx, cc.dhat, cc.kappa))
-  lag = ptp.addConstant("lagged", rows=9, cols=1)
-  lag.updateValue(cc.lagged)
-  ptf = ptp.addAttribute("friction", computed_attribute=friction_point_triangle(
-      ptx, ptp.addAttribute("x_old", through=ptc, source=aold), cc.fdhat, cc.dt, cc.friction, lag))
-  eep = body.addPrimitive("ee_pairs", numInstances=len(cc.ee))
-  eec = eep.addConnectivity("to_vertices", allv, cc.ee, 4)
-  eee = eep.addAttribute("barrier", computed_attribute=edge_edge(
-      eep.addAttribute("x", through=eec, source=apos), cc.dhat, cc.kappa))
+  contact = []
+  if len(cc.pt):
+    ptp = body.addPrimitive("pt_pairs", numInstances=len(cc.pt))
+    ptc = ptp.addConnectivity("to_vertices", allv, cc.pt, 4)
+    ptx = ptp.addAttribute("x", through=ptc, source=apos)
+    lag = ptp.addConstant("lagged", rows=9, cols=1)
+    lag.updateValue(cc.lagged)
+    contact += [ptp.addAttribute("barrier", computed_attribute=point_triangle(ptx, cc.dhat, cc.kappa)),
+                ptp.addAttribute("friction", computed_attribute=friction_point_triangle(
+                    ptx, ptp.addAttribute("x_old", through=ptc, source=aold), cc.fdhat, cc.dt, cc.friction, lag))]
+  if len(cc.ee):
+    eep = body.addPrimitive("ee_pairs", numInstances=len(cc.ee))
+    eec = eep.addConnectivity("to_vertices", allv, cc.ee, 4)
+    contact.append(eep.addAttribute("barrier", computed_attribute=edge_edge(
+        eep.addAttribute("x", through=eec, source=apos), cc.dhat, cc.kappa)))
   kin = cloth.addAttribute("inertia", computed_attribute=inertia(old, None, cc.dt, pos, mass,
                                                                  gravity=(0.0, -9.8, 0.0)))
-  for e in (mem, ben, pte, eee, ptf):
+  for e in [mem, ben] + contact:
     sc.addEnergy(e, projection_method=projection_method)
   sc.addEnergy(kin, projection_method=-1)
   if cc.bodies is None:
@@ -607,12 +610,13 @@ def cloth_contact_scene(cc: ClothContact, projection_method: int = 1):
   # affine bodies on the cloth: the collision union [cloth, abd, obstacle]
   # (dropping_in_container.py:344) carries the body-cloth point-triangle pairs
   prims, amat, trans, verts, vpos = _affine_body_attributes(body, cc.bodies)
-  coll = body.addPrimitiveUnion("collision_vertices", [cloth, verts, obst])
-  cpos = coll.addAttribute("position")
-  bpp = body.addPrimitive("body_pt_pairs", numInstances=len(cc.body_pt))
-  bpc = bpp.addConnectivity("to_collision_vertices", coll, cc.body_pt, 4)
-  sc.addEnergy(bpp.addAttribute("barrier", computed_attribute=point_triangle(
-      bpp.addAttribute("x", through=bpc, source=cpos), cc.dhat, cc.kappa)), projection_method=projection_method)
+  if len(cc.body_pt):
+    coll = body.addPrimitiveUnion("collision_vertices", [cloth, verts, obst])
+    cpos = coll.addAttribute("position")
+    bpp = body.addPrimitive("body_pt_pairs", numInstances=len(cc.body_pt))
+    bpc = bpp.addConnectivity("to_collision_vertices", coll, cc.body_pt, 4)
+    sc.addEnergy(bpp.addAttribute("barrier", computed_attribute=point_triangle(
+        bpp.addAttribute("x", through=bpc, source=cpos), cc.dhat, cc.kappa)), projection_method=projection_method)
   _affine_body_energies(sc, cc.bodies, prims, amat, verts, vpos, cc.dt)
   sc.addMinimizeTarget([pos, amat, trans])
   return sc, dict(position=pos, old_position=old, affine_matrices=amat, translations=trans)

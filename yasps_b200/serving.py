@@ -1,11 +1,15 @@
 """Serving form: continuous batching of Newton-step solves on one GPU.
 
-A request is one Newton step of a Stable Neo-Hookean FEM cube (gradient and
-SPD-projected Hessian, then ``H x = g`` to a true relative residual, the step
-``scene.minimizeEnergy`` takes; ``PKG/scene/scene.pyx:155-200``).  Its side
-selects a resident topology: the scene, the BSR pattern, the SpMV plan and
-the MAS hierarchy are built once per side and stay on the device.  Its
-material and positions are its own.  The server
+A request is one Newton step of a resident scene (gradient and SPD-projected
+Hessian, then ``H x = g`` to a true relative residual, the step
+``scene.minimizeEnergy`` takes; ``PKG/scene/scene.pyx:155-200``).  Its
+topology key selects a resident topology: the scene, the BSR pattern, the
+SpMV plan and the MAS hierarchy are built once per topology and stay on the
+device.  Two kinds of topology exist: a Stable Neo-Hookean FEM cube keyed by
+its side (its requests bring their material and positions), and any scene
+with one static 3x3 block set and a MAS hierarchy (the mixed cloth + affine
+body + contact scenes among them), whose requests bring the values of named
+input attributes.  The server
 
 * admits queued requests as slots and HBM free up (a byte budget over every
   resident per-request buffer);
@@ -42,7 +46,11 @@ from .solver import create_mas_handle, mas_numeric_buffers
 
 @dataclass
 class NewtonRequest:
-  """One Newton-step solve: inputs in pinned host memory, results filled in."""
+  """One Newton-step solve: inputs in pinned host memory, results filled in.
+
+  A FEM-cube request carries ``side``, its Lame parameters and positions; a
+  scene request carries ``key`` (its topology) and ``inputs`` (attribute
+  name -> pinned float64 tensor)."""
 
   side: int
   mu: float
@@ -51,6 +59,8 @@ class NewtonRequest:
   pinned_position: object    # pinned float64 tensor [3 * pinned vertices]
   arrival: float = 0.0       # seconds after the start of the stream
   tag: object = None
+  key: object = None         # topology key (the cube side when None)
+  inputs: Optional[dict] = None
   solution: Optional[np.ndarray] = None
   phase: int = L.YS_SERVE_EMPTY
   iterations: int = 0
@@ -62,6 +72,10 @@ class NewtonRequest:
   @property
   def latency(self) -> float:
     return self.t_done - self.arrival
+
+  @property
+  def topology_key(self):
+    return self.side if self.key is None else self.key
 
   @property
   def converged(self) -> bool:
@@ -78,14 +92,30 @@ def fem_request(side: int, young: float, poisson: float, noise: float, seed: int
   return NewtonRequest(side, mu, lam, pin(free), pin(pinned), arrival, tag)
 
 
-class FemTopology:
-  """Resident structure of one cube side: a template scene whose Hessian
-  pattern, SpMV plan and MAS hierarchy every request of this side reuses."""
+def scene_request(key, inputs: dict, arrival: float = 0.0, tag=None) -> NewtonRequest:
+  """A request for the resident scene topology ``key``: ``inputs`` maps
+  input-attribute names to arrays, copied here into pinned host memory."""
+  torch = _torch()
+  pinned = {}
+  for name, v in inputs.items():
+    t = torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64).reshape(-1))
+    pinned[name] = t.pin_memory() if torch.cuda.is_available() else t
+  return NewtonRequest(0, math.nan, math.nan, None, None, arrival, tag, key=key, inputs=pinned)
 
-  def __init__(self, side: int, spacing: float = 0.1, solver_options: Optional[dict] = None):
-    self.side = int(side)
-    cube = scenes.fem_cube(self.side, spacing=spacing, noise=0.0)
-    self.scene, self.handles = scenes.fem_scene(cube)
+
+class SceneTopology:
+  """Resident structure of one scene: its Hessian pattern (one static 3x3
+  block set), SpMV plan and MAS hierarchy, reused by every request of this
+  topology.  ``inputs`` names the attributes a request sets (name ->
+  attribute); the scene's other values stay as built."""
+
+  def __init__(self, key, scene, inputs: Optional[dict] = None, solver_options: Optional[dict] = None):
+    self.key = key
+    self.scene = scene
+    self.input_attributes = dict(inputs or {})
+    self._setup(solver_options)
+
+  def _setup(self, solver_options: Optional[dict]) -> None:
     opts = dict(solver_options or {})
     opts["mixed_spmv"] = True
     self.scene.minimizer.setSolver("mas", **opts)
@@ -98,12 +128,36 @@ class FemTopology:
     self.weights = self.mas_solver.weights_for(len(self.tables.level_node_offset) - 1)
     dev, _ = self.mas_solver._dev_tables
     self.dev_tables = {k: v for k, v in dev.items() if k not in mas_numeric_keys()}
+    if len(H.block_sets) != 1:
+      raise ValueError("SceneTopology: the serving form takes scenes with one static block set")
     bs = H.block_sets[0]
     self.plan = H.spmv_plan(bs)
     self.nvalues = int(bs.values.numel())
     self.nvalues32 = int(bs.values32.numel())
     self.n = int(H.rows)
     self.nv = self.n // 3
+
+  def load_inputs(self, req: NewtonRequest) -> None:
+    """Input attributes of ``req`` into the template (current stream)."""
+    missing = set(self.input_attributes) - set(req.inputs or {})
+    if missing or set(req.inputs or {}) - set(self.input_attributes):
+      raise ValueError(f"SceneTopology {self.key!r}: request inputs {sorted(req.inputs or {})} "
+                       f"differ from {sorted(self.input_attributes)}")
+    for name, value in req.inputs.items():
+      self.input_attributes[name].copyValueFrom(value)
+
+
+class FemTopology(SceneTopology):
+  """Resident structure of one cube side: a template scene whose Hessian
+  pattern, SpMV plan and MAS hierarchy every request of this side reuses."""
+
+  def __init__(self, side: int, spacing: float = 0.1, solver_options: Optional[dict] = None):
+    self.side = int(side)
+    self.key = self.side
+    cube = scenes.fem_cube(self.side, spacing=spacing, noise=0.0)
+    self.scene, self.handles = scenes.fem_scene(cube)
+    self.input_attributes = {}
+    self._setup(solver_options)
     self.mu_att = self.scene["mu"]
     self.lam_att = self.scene["lam"]
 
@@ -182,7 +236,9 @@ class NewtonServer:
   ``max_slots`` solves are in flight at most; ``memory_budget`` bounds the
   bytes of the pooled per-request buffers (admission by HBM footprint);
   ``passes`` PCG passes run per launch between two host checks;
-  ``admission_streams`` streams carry the admission work of different sides.
+  ``admission_streams`` streams carry the admission work of different
+  topologies.  FEM-cube topologies are built on first use; scene topologies
+  are added with ``add_topology``.
   """
 
   def __init__(self, max_slots: int = 64, passes: int = 8, memory_budget: float = 40e9, tolerance: float = 1e-6,
@@ -201,12 +257,14 @@ class NewtonServer:
     L.call("ys_serve_create", self.max_slots, self.passes, ctypes.byref(h))
     self.handle = h
     self._status = (L.ServeSlotStatus * self.max_slots)()
-    # admission work of different sides overlaps on several streams; one side
-    # always uses the same stream (its requests share the template buffers)
+    # admission work of different topologies overlaps on several streams; one
+    # topology always uses the same stream (its requests share the template
+    # buffers)
     self.admit_streams = [torch.cuda.Stream() for _ in range(int(admission_streams))]
+    self._stream_of = {}                          # topology key -> admission stream
     self.solve_stream = torch.cuda.Stream()
-    self.topologies: Dict[int, FemTopology] = {}
-    self._idle = collections.defaultdict(list)   # side -> idle slots
+    self.topologies: Dict[object, SceneTopology] = {}
+    self._idle = collections.defaultdict(list)   # topology key -> idle slots
     self.resident_bytes = 0
     self._free_ids = list(range(self.max_slots - 1, -1, -1))
     self._pending = collections.deque()           # (req, slot, id) admitted, admission work in flight
@@ -219,44 +277,72 @@ class NewtonServer:
     self._launch_events = []
 
   # -- resources ------------------------------------------------------------------
-  def topology(self, side: int) -> FemTopology:
-    topo = self.topologies.get(side)
+  def topology(self, key) -> SceneTopology:
+    """The topology of ``key``; an integer key not yet resident builds the
+    FEM cube of that side."""
+    topo = self.topologies.get(key)
     if topo is None:
-      topo = FemTopology(side, self.spacing, self.solver_options)
-      self.topologies[side] = topo
+      if not isinstance(key, (int, np.integer)):
+        raise KeyError(f"NewtonServer: no topology {key!r} (add scene topologies with add_topology)")
+      topo = FemTopology(int(key), self.spacing, self.solver_options)
+      self.topologies[topo.key] = topo
     return topo
 
-  def register(self, sides, slots_per_side: int = 1) -> None:
-    """Build the topologies of ``sides`` and pool ``slots_per_side`` slots each."""
-    for side in sides:
-      topo = self.topology(int(side))
-      while len(self._idle[topo.side]) < slots_per_side:
+  def add_topology(self, topo: SceneTopology) -> SceneTopology:
+    """Make a prebuilt scene topology resident under ``topo.key``."""
+    if topo.key in self.topologies:
+      raise ValueError(f"NewtonServer.add_topology: topology {topo.key!r} exists")
+    self.topologies[topo.key] = topo
+    return topo
+
+  def register(self, keys, slots_per_side: int = 1) -> None:
+    """Build (FEM sides) or look up the topologies of ``keys`` and pool
+    ``slots_per_side`` slots each."""
+    for key in keys:
+      topo = self.topology(key)
+      while len(self._idle[topo.key]) < slots_per_side:
         slot = self._new_slot(topo)
         if slot is None:
           break
-        self._idle[topo.side].append(slot)
+        self._idle[topo.key].append(slot)
     _torch().cuda.synchronize()
 
-  def _new_slot(self, topo: FemTopology) -> Optional[_Slot]:
+  def _new_slot(self, topo: SceneTopology) -> Optional[_Slot]:
+    need = getattr(topo, "slot_bytes", None)
+    if need is not None and self.resident_bytes + need > self.memory_budget:
+      self._evict_idle(need)
+      if self.resident_bytes + need > self.memory_budget:
+        return None
     self.slots_created += 1
     slot = _Slot(topo)
+    topo.slot_bytes = slot.nbytes
     if self.resident_bytes + slot.nbytes > self.memory_budget:
-      # evict idle slots of other sides until it fits
-      for side in list(self._idle):
-        while self._idle[side] and self.resident_bytes + slot.nbytes > self.memory_budget:
-          old = self._idle[side].pop()
-          self.resident_bytes -= old.nbytes
-          old.release()
+      self._evict_idle(slot.nbytes)
       if self.resident_bytes + slot.nbytes > self.memory_budget:
         slot.release()
         return None
     self.resident_bytes += slot.nbytes
     return slot
 
-  def _take_slot(self, side: int) -> Optional[_Slot]:
-    if self._idle[side]:
-      return self._idle[side].pop()
-    return self._new_slot(self.topology(side))
+  def _evict_idle(self, need: int) -> None:
+    """Release idle pooled slots (of any topology) until ``need`` more bytes fit."""
+    for key in list(self._idle):
+      while self._idle[key] and self.resident_bytes + need > self.memory_budget:
+        old = self._idle[key].pop()
+        self.resident_bytes -= old.nbytes
+        old.release()
+
+  def _take_slot(self, key) -> Optional[_Slot]:
+    if self._idle[key]:
+      return self._idle[key].pop()
+    return self._new_slot(self.topology(key))
+
+  def _admit_stream(self, key):
+    stream = self._stream_of.get(key)
+    if stream is None:
+      stream = self.admit_streams[len(self._stream_of) % len(self.admit_streams)]
+      self._stream_of[key] = stream
+    return stream
 
   def close(self) -> None:
     if self.handle is not None:
@@ -278,12 +364,12 @@ class NewtonServer:
   def _admit_arrivals(self, queue, now):
     torch = _torch()
     while queue and self._free_ids:
-      slot = self._take_slot(queue[0].side)
+      slot = self._take_slot(queue[0].topology_key)
       if slot is None:
         break
       req = queue.popleft()
       t = time.perf_counter()
-      with torch.cuda.stream(self.admit_streams[req.side % len(self.admit_streams)]):
+      with torch.cuda.stream(self._admit_stream(req.topology_key)):
         slot.admit(req)
       self.host_seconds["admit"] += time.perf_counter() - t
       req.t_admit = now
@@ -331,7 +417,7 @@ class NewtonServer:
       req.t_done = t
       L.call("ys_serve_detach", self.handle, sid)
       self._free_ids.append(sid)
-      self._idle[slot.topo.side].append(slot)
+      self._idle[slot.topo.key].append(slot)
       out.append(req)
     return out
 
@@ -373,7 +459,7 @@ class NewtonServer:
         self._pending[0][1].ready.synchronize()
         self.host_seconds["wait_admission"] += time.perf_counter() - t
       elif queue:
-        raise RuntimeError(f"a side-{queue[0].side} request does not fit the memory budget")
+        raise RuntimeError(f"a request of topology {queue[0].topology_key!r} does not fit the memory budget")
       elif i < total:
         wait = reqs[i].arrival - (clock() - t0)
         if wait > 0:
@@ -390,7 +476,7 @@ class NewtonServer:
     for req in reqs:
       while clock() - t0 < req.arrival:
         pass
-      topo = self.topology(req.side)
+      topo = self.topology(req.topology_key)
       solver = topo.mas_solver
       req.t_admit = clock() - t0
       saved = solver.mixed_spmv, solver.stop_rule
@@ -449,3 +535,86 @@ def poisson_fem_stream(count: int = 512, mean_spacing: float = 2e-3, side_range=
     reqs.append(NewtonRequest(side, mu, lam, buf[off:a], buf[a:b], float(arrivals[k]), k))
     off = b
   return reqs
+
+
+# ---- mixed serving: cloth + affine-body + contact scenes beside large FEM cubes -------
+
+@dataclass
+class ClothSceneSpec:
+  """One scene of the cloth-over-obstacle type with affine bodies
+  (``scenes.cloth_contact``): its topology key and generator arguments."""
+
+  key: object
+  side: int
+  bodies: int
+  pairs: int
+  seed: int
+
+
+def cloth_scene_topology(spec: ClothSceneSpec, solver_options: Optional[dict] = None) -> SceneTopology:
+  """Build the scene of ``spec`` and make it a serving topology whose
+  requests set the cloth positions, the positions of the last step and the
+  bodies' affine matrices and translations."""
+  cc = scenes.cloth_contact(spec.side, spec.pairs, num_bodies=spec.bodies, seed=spec.seed)
+  sc, handles = scenes.cloth_contact_scene(cc)
+  names = [k for k in ("position", "old_position", "affine_matrices", "translations") if k in handles]
+  topo = SceneTopology(spec.key, sc, {k: handles[k] for k in names}, solver_options)
+  topo.cloth = cc
+  topo.spec = spec
+  return topo
+
+
+def cloth_scene_request(topo: SceneTopology, arrival: float = 0.0, tag=None) -> NewtonRequest:
+  """The Newton step of a cloth-scene topology at its generated state."""
+  cc = topo.cloth
+  inputs = {"position": cc.cloth_position, "old_position": cc.cloth_position}
+  if cc.bodies is not None:
+    inputs.update(affine_matrices=cc.bodies.affine, translations=cc.bodies.translation)
+  return scene_request(topo.key, inputs, arrival, tag)
+
+
+@dataclass
+class MixedWorkload:
+  """A mixed stream: cloth scenes (one request each) interleaved with FEM
+  cube requests of one side; ``order[k]`` names the k-th arrival as
+  ``("cloth", i)`` or ``("fem", j)``."""
+
+  scenes: List[ClothSceneSpec]
+  fem_side: int
+  fem: List[dict]
+  order: List[tuple]
+  arrivals: np.ndarray
+
+  def requests(self, server: "NewtonServer", all_at_once: bool = False) -> List[NewtonRequest]:
+    """Requests in arrival order (the topologies must be resident); with
+    ``all_at_once`` every request arrives at time 0."""
+    out = []
+    for k, (kind, i) in enumerate(self.order):
+      at = 0.0 if all_at_once else float(self.arrivals[k])
+      if kind == "cloth":
+        out.append(cloth_scene_request(server.topology(self.scenes[i].key), at, tag=k))
+      else:
+        f = self.fem[i]
+        out.append(fem_request(self.fem_side, f["young"], f["poisson"], f["noise"], f["seed"], arrival=at, tag=k))
+    return out
+
+
+def mixed_workload(num_scenes: int = 64, num_fem: int = 8, fem_side: int = 126, side_range=(64, 256),
+                   body_range=(2, 16), pair_range=(10_000, 200_000), fem_young: float = 1e6,
+                   fem_poisson: float = 0.45, fem_noise: float = 0.005, mean_spacing: float = 2e-3,
+                   seed: int = 0) -> MixedWorkload:
+  """Seeded mixed stream: ``num_scenes`` cloth scenes with cloth side, body
+  count and contact pair count drawn uniform in their ranges, and
+  ``num_fem`` FEM cubes of ``fem_side``^3 vertices, in a random interleaving
+  with Poisson arrivals of mean gap ``mean_spacing`` s."""
+  rng = np.random.default_rng(seed)
+  specs = [ClothSceneSpec(("cloth", k), int(rng.integers(side_range[0], side_range[1] + 1)),
+                          int(rng.integers(body_range[0], body_range[1] + 1)),
+                          int(rng.integers(pair_range[0], pair_range[1] + 1)), seed * 1000003 + k)
+           for k in range(num_scenes)]
+  fem = [dict(young=fem_young, poisson=fem_poisson, noise=fem_noise, seed=seed * 1000003 + 500 + j)
+         for j in range(num_fem)]
+  order = [("cloth", k) for k in range(num_scenes)] + [("fem", j) for j in range(num_fem)]
+  order = [order[i] for i in rng.permutation(len(order))]
+  gaps = rng.exponential(mean_spacing, len(order)) if mean_spacing > 0 else np.zeros(len(order))
+  return MixedWorkload(specs, int(fem_side), fem, order, np.cumsum(gaps) - gaps[0])
