@@ -250,6 +250,66 @@ typedef struct ys_energy_args {
  * these energies (hessianKernelHost.pyx:27-161).                           */
 int32_t ys_energy_eval(const ys_energy_args* args, void* stream);
 
+/* ---- rectangular second-order Jacobians (PKG/matrixAndVector/matrix/
+ * secondOrderJacobian.pyx, PKG/kernel/Jacobian/secondOrderJacobianKernel*.pyx,
+ * PKG/kernel/Coordinate/secondOrderJacobianIndicesKernel.pyx) -------------
+ * d2E / (d rows d cols) of a scalar energy, rows and columns two target
+ * lists.  The values of an instance come from its unprojected local Hessian
+ * over the energy's arguments (the reference's no-project Jacobian kernel);
+ * every argument carries a row code and a column code (ys_join_union_indices
+ * run once with the row targets and once with the column targets).        */
+
+/* Unprojected local Hessians, packed upper (3A(3A+1)/2 doubles an element,
+ * row-major upper triangle), of the vertex-tuple energies (args->kind, the
+ * position arguments; rest, lagged data and parameters as for
+ * ys_energy_eval, the plan and record fields unused).                      */
+int32_t ys_local_hessians(const ys_energy_args* args, double* out, void* stream);
+/* Same for the SNH tetrahedra (12x12, 78 doubles an element).              */
+int32_t ys_snh_local_hessians(const ys_snh_args* args, double* out, void* stream);
+/* Same for the inertia 1/2 m |x - x_before - dt v - dt^2 g|^2 per vertex
+ * over its arguments (x, x_before) (args = 2) or (x, x_before, v) (args = 3):
+ * m [[I, -I, -dt I], [-I, I, dt I], [-dt I, dt I, dt^2 I]] (helpers.py:
+ * 138-141).  `mass` may be NULL (then mass_value for every vertex).        */
+int32_t ys_inertia_local_hessians(const double* mass, double mass_value, double dt, uint32_t n,
+                                  uint32_t args, double* out, void* stream);
+
+/* Coordinates of the (row target, column target) pairs of every instance:
+ * the distinct row codes >= 2 (first occurrence order) times the distinct
+ * column codes >= 2, row-major, as scalar (row, col) pairs with dims (3, 3).
+ * With coords NULL: coord_outer (n+1) = exclusive counts.  Otherwise
+ * coords [2 m], dims [2 m] at the offsets of coord_outer.  Codes are
+ * [n x K] with the argument a at column a * slot_stride, args <= 8.
+ * Replaces count/generate_rectangular_coordinates
+ * (secondOrderJacobianIndicesKernel.pyx:16-84).                            */
+int32_t ys_rect_coordinates(const uint32_t* row_codes, const uint32_t* col_codes, uint32_t n, uint32_t K,
+                            uint32_t slot_stride, uint32_t args, uint32_t* coord_outer, uint32_t* coords,
+                            uint16_t* dims, void* stream);
+
+/* Records (9 doubles, row-major) of every pair, in the order of
+ * ys_rect_coordinates, at record[coord_outer[t] + k] (the assembly plan of
+ * ys_pattern_build over those coordinates): the sum of the local Hessian's
+ * argument blocks of the pair's row group and column group.  Sum them with
+ * ys_assemble3.  Replaces compute_second_order_jacobian_no_project
+ * (secondOrderJacobianKernel.pyx:86-140).                                  */
+int32_t ys_rect_records(const double* local_hessians, uint32_t args, const uint32_t* row_codes,
+                        const uint32_t* col_codes, uint32_t n, uint32_t K, uint32_t slot_stride,
+                        const uint32_t* coord_outer, const uint32_t* record, double* records, void* stream);
+
+/* Products with the assembled rectangular matrix (unique 3x3 blocks sorted
+ * by (row, col), scalar positions).  ys_rect_plan builds row_ptr
+ * [block_rows + 1], col_ptr [block_cols + 1] and col_order [num_blocks]
+ * (blocks by column, stable); ys_rect_spmv computes y = J x (transpose 0,
+ * y of 3 block_rows) or y = J^T x (transpose 1, y of 3 block_cols), each
+ * output row summed in block order.  Replaces matrix.spmv of
+ * secondOrderJacobian (PKG/matrixAndVector/matrix/matrix.pyx).            */
+int32_t ys_rect_plan_workspace_bytes(uint32_t num_blocks, uint64_t* bytes);
+int32_t ys_rect_plan(const uint32_t* positions, uint32_t num_blocks, uint32_t block_rows, uint32_t block_cols,
+                     uint32_t* row_ptr, uint32_t* col_ptr, uint32_t* col_order, void* workspace,
+                     uint64_t workspace_bytes, void* stream);
+int32_t ys_rect_spmv(const double* values, const uint32_t* positions, const uint32_t* row_ptr,
+                     const uint32_t* col_ptr, const uint32_t* col_order, uint32_t block_rows, uint32_t block_cols,
+                     const double* x, double* y, uint32_t transpose, void* stream);
+
 /* ---- affine (ABD) bodies ------------------------------------------------
  * A body carries a 3x3 affine matrix A (9 DoF, row-major, the reference's
  * `affine_matrices` attribute, examples/dropping_in_container_mixed/

@@ -394,6 +394,51 @@ __global__ void __launch_bounds__(kProjThreads) snh_project_kernel(const ys_snh_
     snh_project_one(a, a.work_list[i], stash, blockDim.x);
 }
 
+// Unprojected 12x12 local Hessian A of every tet (packed upper, 78 doubles),
+// from the same blocks as the records of snh_eval_kernel.
+__global__ void __launch_bounds__(128) snh_local_hessian_kernel(const ys_snh_args a, double* out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  SnhState st;
+  snh_state(a, t, st);
+  V3 u[4], v[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    u[k] = mul(st.f, st.g[k]);
+    v[k] = mul(st.cof, st.g[k]);
+  }
+  double* dst = out + (uint64_t)t * 78;
+#pragma unroll
+  for (int ai = 0; ai < 4; ++ai)
+#pragma unroll
+    for (int bi = ai; bi < 4; ++bi) {
+      double blk[3][3];
+      hess_block(st, st.g[ai], st.g[bi], u[ai], u[bi], v[ai], v[bi], blk);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l)
+          if (3 * ai + k <= 3 * bi + l) dst[utri<12>(3 * ai + k, 3 * bi + l)] = blk[k][l];
+    }
+}
+
+// Local Hessian of the inertia term 1/2 m |x - x_before - dt v - dt^2 g|^2
+// over its arguments (x, x_before[, v]), packed upper: m [[I, -I, -dt I],
+// [-I, I, dt I], [-dt I, dt I, dt^2 I]] (helpers.py:138-141).
+__global__ void inertia_local_hessian_kernel(const double* __restrict__ mass, double mass_value, double dt,
+                                             uint32_t n, int args, double* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double m = mass ? mass[i] : mass_value;
+  const double c[3] = {1.0, -1.0, -dt};
+  const int N = 3 * args;
+  const int H = N * (N + 1) / 2;
+  double* dst = out + (uint64_t)i * H;
+  int q = 0;
+  for (int r = 0; r < N; ++r)
+    for (int col = r; col < N; ++col) dst[q++] = (r % 3 == col % 3) ? m * c[r / 3] * c[col / 3] : 0.0;
+}
+
 __global__ void inertia_kernel(const ys_inertia_args a) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.num_vertices) return;
@@ -476,3 +521,23 @@ int32_t ys_inertia_eval(const ys_inertia_args* args, void* stream) {
 }
 
 }  // extern "C"
+
+extern "C" int32_t ys_snh_local_hessians(const ys_snh_args* args, double* out, void* stream) {
+  YS_REQUIRE(args != nullptr && out != nullptr, YS_ERR_INVALID, "null argument");
+  const ys_snh_args& a = *args;
+  if (a.num_elements == 0) return YS_OK;
+  ys::snh_local_hessian_kernel<<<ys::grid_for(a.num_elements, 128), 128, 0, (cudaStream_t)stream>>>(a, out);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+extern "C" int32_t ys_inertia_local_hessians(const double* mass, double mass_value, double dt, uint32_t n,
+                                             uint32_t args, double* out, void* stream) {
+  YS_REQUIRE(out != nullptr, YS_ERR_INVALID, "null output");
+  YS_REQUIRE(args == 2 || args == 3, YS_ERR_INVALID, "inertia has 2 or 3 arguments");
+  if (n == 0) return YS_OK;
+  ys::inertia_local_hessian_kernel<<<ys::grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(mass, mass_value, dt, n,
+                                                                                           (int)args, out);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}

@@ -417,6 +417,37 @@ __global__ void __launch_bounds__(128) energy_value_kernel(const ys_energy_args 
   a.energy[t] = E::template eval<0>(a, t, x, r).v;
 }
 
+// Unprojected local Hessian of every element with respect to its position
+// arguments, packed upper (HD<3A>::H doubles an element): the input of the
+// rectangular second-order Jacobian, whose reference kernel does not project
+// (PKG/kernel/Jacobian/secondOrderJacobianKernelNoProject.pyx).
+template <class E>
+__global__ void __launch_bounds__(kEnergyThreads) local_hessian_kernel(const ys_energy_args a, double* out) {
+  constexpr int A = E::A, N = 3 * A;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  Pts<A> x, r;
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    const uint32_t id = a.conn[(uint64_t)t * A + k];
+    load_point(a.position, id, x.p[k]);
+    if (a.rest.num_children) load_point(a.rest, id, r.p[k]);
+    else r.p[k][0] = r.p[k][1] = r.p[k][2] = 0.0;
+  }
+  const HD<N> e = E::template eval<N>(a, t, x, r);
+  double* dst = out + (uint64_t)t * HD<N>::H;
+#pragma unroll
+  for (int i = 0; i < HD<N>::H; ++i) dst[i] = e.h[i];
+}
+
+template <class E>
+static int32_t launch_local_hessian(const ys_energy_args& a, double* out, cudaStream_t s) {
+  YS_REQUIRE(a.arity == (uint32_t)E::A, YS_ERR_INVALID, "arity does not match the energy kind");
+  local_hessian_kernel<E><<<grid_for(a.num_elements, kEnergyThreads), kEnergyThreads, 0, s>>>(a, out);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
 template <class E>
 static int32_t launch_energy_value(const ys_energy_args& a, cudaStream_t s) {
   YS_REQUIRE(a.arity == (uint32_t)E::A, YS_ERR_INVALID, "arity does not match the energy kind");
@@ -964,6 +995,39 @@ static int32_t launch_coupled(const ys_coupled_args& a, cudaStream_t s) {
 }  // namespace ys
 
 extern "C" {
+
+int32_t ys_local_hessians(const ys_energy_args* args, double* out, void* stream) {
+  YS_REQUIRE(args != nullptr && out != nullptr, YS_ERR_INVALID, "null argument");
+  const ys_energy_args& a = *args;
+  YS_REQUIRE(a.position.num_children >= 1 && a.position.num_children <= YS_MAX_UNION, YS_ERR_INVALID,
+             "bad position union");
+  YS_REQUIRE(a.rest.num_children <= YS_MAX_UNION, YS_ERR_INVALID, "bad rest union");
+  const bool friction = a.kind == YS_ENERGY_FRICTION_PT || a.kind == YS_ENERGY_FRICTION_PE ||
+                        a.kind == YS_ENERGY_FRICTION_EE || a.kind == YS_ENERGY_FRICTION_PP;
+  const bool needs_rest = a.kind == YS_ENERGY_BENDING || a.kind == YS_ENERGY_BARAFF_WITKIN ||
+                          a.kind == YS_ENERGY_STVK_MEMBRANE || friction;
+  YS_REQUIRE(!needs_rest || a.rest.num_children >= 1, YS_ERR_INVALID, "this energy needs rest positions");
+  YS_REQUIRE(!friction || (a.params && a.param_stride >= 9), YS_ERR_INVALID,
+             "friction needs 9 lagged parameters per element");
+  if (a.num_elements == 0) return YS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (a.kind) {
+    case YS_ENERGY_POINT_POINT: return ys::launch_local_hessian<ys::PointPoint>(a, out, s);
+    case YS_ENERGY_POINT_EDGE: return ys::launch_local_hessian<ys::PointEdge>(a, out, s);
+    case YS_ENERGY_POINT_TRIANGLE: return ys::launch_local_hessian<ys::PointTriangle>(a, out, s);
+    case YS_ENERGY_EDGE_EDGE: return ys::launch_local_hessian<ys::EdgeEdge>(a, out, s);
+    case YS_ENERGY_BENDING: return ys::launch_local_hessian<ys::Bending>(a, out, s);
+    case YS_ENERGY_BARAFF_WITKIN: return ys::launch_local_hessian<ys::BaraffWitkin>(a, out, s);
+    case YS_ENERGY_STVK_MEMBRANE: return ys::launch_local_hessian<ys::StvkMembrane>(a, out, s);
+    case YS_ENERGY_FRICTION_PT: return ys::launch_local_hessian<ys::FrictionPT>(a, out, s);
+    case YS_ENERGY_FRICTION_PE: return ys::launch_local_hessian<ys::FrictionPE>(a, out, s);
+    case YS_ENERGY_FRICTION_EE: return ys::launch_local_hessian<ys::FrictionEE>(a, out, s);
+    case YS_ENERGY_FRICTION_PP: return ys::launch_local_hessian<ys::FrictionPP>(a, out, s);
+    default: break;
+  }
+  ys_set_last_error("unknown energy kind", __FILE__, __LINE__);
+  return YS_ERR_INVALID;
+}
 
 int32_t ys_energy_eval(const ys_energy_args* args, void* stream) {
   YS_REQUIRE(args != nullptr, YS_ERR_INVALID, "null args");

@@ -1,0 +1,284 @@
+// Rectangular second-order Jacobians d2E / (d rows d cols).
+//
+// The reference differentiates a scalar energy once with respect to the row
+// targets and the result with respect to the column targets
+// (PKG/differentiator/differentiator.pyx:367-489), builds the coordinates of
+// every (row slot, column slot) pair of an instance
+// (PKG/kernel/Coordinate/secondOrderJacobianIndicesKernel.pyx:16-84: a pair
+// counts when both slots carry a target code >= 2, row-major over the
+// instance's row slots) and compresses them into unique blocks like a
+// Hessian, without the upper-triangle fold
+// (PKG/matrixAndVector/matrix/secondOrderJacobian.pyx:296-335).  Here the
+// instance's values come from its unprojected local Hessian over the
+// energy's arguments (an argument may carry a row code, a column code, or
+// both), repeated target codes of one instance are merged (first occurrence
+// order), and the blocks are summed in a fixed order by the assembly plan of
+// ys_pattern_build.  The product y = J x or y = J^T x gathers per output
+// block row in block order: deterministic.
+#include <algorithm>
+
+#include <cub/cub.cuh>
+
+#include "ys_common.cuh"
+
+namespace ys {
+
+constexpr int kRectMaxArgs = 8;
+
+__device__ __forceinline__ int rect_groups(const uint32_t* __restrict__ codes, uint32_t t, uint32_t K,
+                                           uint32_t stride, int args, int (&group)[kRectMaxArgs],
+                                           int (&first)[kRectMaxArgs]) {
+  int nfirst = 0;
+  for (int a = 0; a < args; ++a) {
+    const uint32_t c = codes[(uint64_t)t * K + (uint64_t)a * stride];
+    group[a] = -1;
+    if (c < 2) continue;
+    int g = -1;
+    for (int q = 0; q < nfirst; ++q)
+      if (codes[(uint64_t)t * K + (uint64_t)first[q] * stride] == c) g = q;
+    if (g < 0) {
+      first[nfirst] = a;
+      g = nfirst++;
+    }
+    group[a] = g;
+  }
+  return nfirst;
+}
+
+__global__ void rect_count_kernel(const uint32_t* __restrict__ row_codes, const uint32_t* __restrict__ col_codes,
+                                  uint32_t n, uint32_t K, uint32_t stride, int args, uint32_t* __restrict__ count) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int group[kRectMaxArgs], first[kRectMaxArgs];
+  const int nr = rect_groups(row_codes, t, K, stride, args, group, first);
+  const int nc = rect_groups(col_codes, t, K, stride, args, group, first);
+  count[t] = (uint32_t)(nr * nc);
+}
+
+__global__ void rect_coords_kernel(const uint32_t* __restrict__ row_codes, const uint32_t* __restrict__ col_codes,
+                                   uint32_t n, uint32_t K, uint32_t stride, int args,
+                                   const uint32_t* __restrict__ outer, uint32_t* __restrict__ coords,
+                                   uint16_t* __restrict__ dims) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int rg[kRectMaxArgs], rf[kRectMaxArgs], cg[kRectMaxArgs], cf[kRectMaxArgs];
+  const int nr = rect_groups(row_codes, t, K, stride, args, rg, rf);
+  const int nc = rect_groups(col_codes, t, K, stride, args, cg, cf);
+  uint32_t o = outer[t];
+  for (int i = 0; i < nr; ++i)
+    for (int j = 0; j < nc; ++j, ++o) {
+      coords[2ull * o] = row_codes[(uint64_t)t * K + (uint64_t)rf[i] * stride] - 2u;
+      coords[2ull * o + 1] = col_codes[(uint64_t)t * K + (uint64_t)cf[j] * stride] - 2u;
+      dims[2ull * o] = 3;
+      dims[2ull * o + 1] = 3;
+    }
+}
+
+// Records of one instance: for every (row group, column group) the sum of
+// its argument blocks of the packed upper local Hessian.
+__global__ void rect_records_kernel(const double* __restrict__ local_h, int args,
+                                    const uint32_t* __restrict__ row_codes, const uint32_t* __restrict__ col_codes,
+                                    uint32_t n, uint32_t K, uint32_t stride, const uint32_t* __restrict__ outer,
+                                    const uint32_t* __restrict__ record, double* __restrict__ out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int N = 3 * args;
+  const double* h = local_h + (uint64_t)t * (N * (N + 1) / 2);
+  int rg[kRectMaxArgs], rf[kRectMaxArgs], cg[kRectMaxArgs], cf[kRectMaxArgs];
+  const int nr = rect_groups(row_codes, t, K, stride, args, rg, rf);
+  const int nc = rect_groups(col_codes, t, K, stride, args, cg, cf);
+  // packed upper index of (r, c) for any order
+  auto at = [&](int r, int c) {
+    const int lo = r < c ? r : c, hi = r < c ? c : r;
+    return h[lo * N - lo * (lo - 1) / 2 + (hi - lo)];
+  };
+  uint32_t o = outer[t];
+  for (int i = 0; i < nr; ++i)
+    for (int j = 0; j < nc; ++j, ++o) {
+      double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int a = 0; a < args; ++a) {
+        if (rg[a] != i) continue;
+        for (int b = 0; b < args; ++b) {
+          if (cg[b] != j) continue;
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int l = 0; l < 3; ++l) acc[k][l] += at(3 * a + k, 3 * b + l);
+        }
+      }
+      double* dst = out + record[o];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) dst[3 * k + l] = acc[k][l];
+    }
+}
+
+// First block of every block row (rows sorted): row_ptr[r] = lower bound.
+__global__ void rect_row_ptr_kernel(const uint32_t* __restrict__ positions, uint32_t nb, uint32_t block_rows,
+                                    uint32_t* __restrict__ row_ptr) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > block_rows) return;
+  uint32_t lo = 0, hi = nb;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (positions[2ull * mid] / 3u < r) lo = mid + 1;
+    else hi = mid;
+  }
+  row_ptr[r] = lo;
+}
+
+__global__ void rect_col_ptr_kernel(const uint32_t* __restrict__ keys, uint32_t nb, uint32_t block_cols,
+                                    uint32_t* __restrict__ col_ptr) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > block_cols) return;
+  uint32_t lo = 0, hi = nb;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (keys[mid] < c) lo = mid + 1;
+    else hi = mid;
+  }
+  col_ptr[c] = lo;
+}
+
+__global__ void rect_col_keys_kernel(const uint32_t* __restrict__ positions, uint32_t nb, uint32_t* __restrict__ keys,
+                                     uint32_t* __restrict__ vals) {
+  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nb) return;
+  keys[u] = positions[2ull * u + 1] / 3u;
+  vals[u] = u;
+}
+
+__global__ void rect_spmv_kernel(const double* __restrict__ values, const uint32_t* __restrict__ positions,
+                                 const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ order,
+                                 uint32_t out_rows, int transpose, const double* __restrict__ x,
+                                 double* __restrict__ y) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= out_rows) return;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (uint32_t e = ptr[r]; e < ptr[r + 1]; ++e) {
+    const uint32_t u = order ? order[e] : e;
+    const double* b = values + 9ull * u;
+    if (!transpose) {
+      const double* xv = x + positions[2ull * u + 1];
+      s0 += b[0] * xv[0] + b[1] * xv[1] + b[2] * xv[2];
+      s1 += b[3] * xv[0] + b[4] * xv[1] + b[5] * xv[2];
+      s2 += b[6] * xv[0] + b[7] * xv[1] + b[8] * xv[2];
+    } else {
+      const double* xv = x + positions[2ull * u];
+      s0 += b[0] * xv[0] + b[3] * xv[1] + b[6] * xv[2];
+      s1 += b[1] * xv[0] + b[4] * xv[1] + b[7] * xv[2];
+      s2 += b[2] * xv[0] + b[5] * xv[1] + b[8] * xv[2];
+    }
+  }
+  y[3ull * r] = s0;
+  y[3ull * r + 1] = s1;
+  y[3ull * r + 2] = s2;
+}
+
+}  // namespace ys
+
+extern "C" {
+
+int32_t ys_rect_coordinates(const uint32_t* row_codes, const uint32_t* col_codes, uint32_t n, uint32_t K,
+                            uint32_t slot_stride, uint32_t args, uint32_t* coord_outer, uint32_t* coords,
+                            uint16_t* dims, void* stream) {
+  YS_REQUIRE(row_codes && col_codes && coord_outer, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE(args >= 1 && args <= (uint32_t)ys::kRectMaxArgs, YS_ERR_INVALID, "1..8 arguments an instance");
+  YS_REQUIRE((uint64_t)(args - 1) * slot_stride < K, YS_ERR_INVALID, "slot stride beyond the code row");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (coords == nullptr) {
+    // counts into coord_outer[1..n], then an inclusive scan in place
+    YS_CUDA_TRY(cudaMemsetAsync(coord_outer, 0, sizeof(uint32_t), s));
+    if (n == 0) return YS_OK;
+    ys::rect_count_kernel<<<ys::grid_for(n, 256), 256, 0, s>>>(row_codes, col_codes, n, K, slot_stride, (int)args,
+                                                              coord_outer + 1);
+    YS_CHECK_LAUNCH();
+    size_t tmp = 0;
+    YS_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tmp, coord_outer + 1, coord_outer + 1, (int)n, s));
+    void* d_tmp = nullptr;
+    YS_CUDA_TRY(cudaMallocAsync(&d_tmp, tmp, s));
+    const cudaError_t e = cub::DeviceScan::InclusiveSum(d_tmp, tmp, coord_outer + 1, coord_outer + 1, (int)n, s);
+    cudaFreeAsync(d_tmp, s);
+    YS_CUDA_TRY(e);
+    return YS_OK;
+  }
+  YS_REQUIRE(dims != nullptr, YS_ERR_INVALID, "null dims");
+  if (n == 0) return YS_OK;
+  ys::rect_coords_kernel<<<ys::grid_for(n, 256), 256, 0, s>>>(row_codes, col_codes, n, K, slot_stride, (int)args,
+                                                             coord_outer, coords, dims);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_rect_records(const double* local_hessians, uint32_t args, const uint32_t* row_codes,
+                        const uint32_t* col_codes, uint32_t n, uint32_t K, uint32_t slot_stride,
+                        const uint32_t* coord_outer, const uint32_t* record, double* records, void* stream) {
+  YS_REQUIRE(local_hessians && row_codes && col_codes && coord_outer && record && records, YS_ERR_INVALID,
+             "null argument");
+  YS_REQUIRE(args >= 1 && args <= (uint32_t)ys::kRectMaxArgs, YS_ERR_INVALID, "1..8 arguments an instance");
+  if (n == 0) return YS_OK;
+  ys::rect_records_kernel<<<ys::grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(
+      local_hessians, (int)args, row_codes, col_codes, n, K, slot_stride, coord_outer, record, records);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_rect_plan_workspace_bytes(uint32_t num_blocks, uint64_t* bytes) {
+  YS_REQUIRE(bytes != nullptr, YS_ERR_INVALID, "null output");
+  size_t tmp = 0;
+  const int m = (int)std::max<uint32_t>(num_blocks, 1);
+  YS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                              (const uint32_t*)nullptr, (uint32_t*)nullptr, m));
+  const uint64_t keys = 4ull * m;
+  *bytes = 4 * ((keys + 255) / 256 * 256) + (tmp + 255) / 256 * 256;
+  return YS_OK;
+}
+
+int32_t ys_rect_plan(const uint32_t* positions, uint32_t num_blocks, uint32_t block_rows, uint32_t block_cols,
+                     uint32_t* row_ptr, uint32_t* col_ptr, uint32_t* col_order, void* workspace,
+                     uint64_t workspace_bytes, void* stream) {
+  YS_REQUIRE(row_ptr && col_ptr && col_order, YS_ERR_INVALID, "null output");
+  YS_REQUIRE(num_blocks == 0 || positions, YS_ERR_INVALID, "null positions");
+  uint64_t need = 0;
+  const int32_t rc = ys_rect_plan_workspace_bytes(num_blocks, &need);
+  if (rc != YS_OK) return rc;
+  YS_REQUIRE(workspace && workspace_bytes >= need, YS_ERR_INVALID, "workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  ys::rect_row_ptr_kernel<<<ys::grid_for(block_rows + 1, 256), 256, 0, s>>>(positions, num_blocks, block_rows,
+                                                                            row_ptr);
+  YS_CHECK_LAUNCH();
+  const int m = (int)std::max<uint32_t>(num_blocks, 1);
+  const uint64_t keys = (4ull * m + 255) / 256 * 256;
+  uint8_t* w = static_cast<uint8_t*>(workspace);
+  uint32_t* k_in = reinterpret_cast<uint32_t*>(w);
+  uint32_t* v_in = reinterpret_cast<uint32_t*>(w + keys);
+  uint32_t* k_out = reinterpret_cast<uint32_t*>(w + 2 * keys);
+  void* tmp = w + 4 * keys;
+  size_t tmp_bytes = workspace_bytes - 4 * keys;
+  if (num_blocks) {
+    ys::rect_col_keys_kernel<<<ys::grid_for(num_blocks, 256), 256, 0, s>>>(positions, num_blocks, k_in, v_in);
+    YS_CHECK_LAUNCH();
+    // stable: the blocks of one column stay in block order
+    YS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, col_order, (int)num_blocks, 0,
+                                                32, s));
+  }
+  ys::rect_col_ptr_kernel<<<ys::grid_for(block_cols + 1, 256), 256, 0, s>>>(k_out, num_blocks, block_cols, col_ptr);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_rect_spmv(const double* values, const uint32_t* positions, const uint32_t* row_ptr,
+                     const uint32_t* col_ptr, const uint32_t* col_order, uint32_t block_rows, uint32_t block_cols,
+                     const double* x, double* y, uint32_t transpose, void* stream) {
+  YS_REQUIRE(row_ptr && col_ptr && x && y, YS_ERR_INVALID, "null argument");
+  const uint32_t out_rows = transpose ? block_cols : block_rows;
+  if (out_rows == 0) return YS_OK;
+  ys::rect_spmv_kernel<<<ys::grid_for(out_rows, 128), 128, 0, (cudaStream_t)stream>>>(
+      values, positions, transpose ? col_ptr : row_ptr, transpose ? col_order : nullptr, out_rows, (int)transpose,
+      x, y);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+}  // extern "C"

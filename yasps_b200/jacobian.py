@@ -1,0 +1,384 @@
+"""Rectangular second-order Jacobians and the differentiator front end.
+
+Mirrors ``PKG/matrixAndVector/matrix/secondOrderJacobian.pyx`` (the
+rectangular matrix ``d2E / (d row_wrt d column_wrt)``: ``row_wrt``,
+``column_wrt``, their start indices, ``compute``, ``spmv(x, transpose)``,
+``+`` and the reference's block attributes) and the entry points of
+``PKG/differentiator/differentiator.pyx:174-489``: ``diff2`` with equal
+target lists gives the projected Hessian, with different lists the
+rectangular Jacobian (never projected, as the reference's no-project
+Jacobian kernel); ``diff1`` of scalar energies gives their gradient.
+
+Values on the device through libys_newton.so: the unprojected local
+Hessian of every instance over the energy's arguments
+(``ys_local_hessians``, ``ys_snh_local_hessians``,
+``ys_inertia_local_hessians``), the (row target, column target) pairs of
+every instance (``ys_rect_coordinates``), the unique sort of
+``ys_pattern_build`` (no upper-triangle fold), merged records
+(``ys_rect_records``) summed in a fixed order (``ys_assemble3``), and the
+deterministic products ``ys_rect_spmv``.
+
+An argument of an energy is a row (column) slot when its leaf is one of the
+row (column) targets: for the vertex-tuple energies and the SNH tetrahedra
+the leaves of the position union (so ``row_wrt=[cloth position]``,
+``column_wrt=[obstacle position]`` gives the cloth-obstacle coupling
+blocks), for the inertia term its ``x``, ``x_before`` and ``vel``
+attributes (the adjoint blocks ``d2E / (dx dx_before)`` and
+``d2E / (dx dvel)`` of the reference's differentiable-simulation examples,
+``examples/bunny_dropping_on_ground/bunny_dropping_on_ground.py:333-334``).
+Mixed derivatives through the rest / lagged arguments of an energy (rest
+shapes, the last step's positions of friction) and through affine-body
+vertices are not built.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import List
+
+import numpy as np
+
+from . import _lib as L
+from .graph import AFFINE, attribute, resolve_leaf_children
+from .hessian import _Pattern, _dev, _torch, hessian, vector
+
+
+def _start_indices(targets):
+  starts = [0]
+  for t in targets:
+    starts.append(starts[-1] + t.size * t.correspondance.numInstances)
+  return starts
+
+
+def _validate_targets(targets, name):
+  if not isinstance(targets, list) or len(targets) == 0:
+    raise ValueError(f"secondOrderJacobian.__init__: {name} must be a non-empty list.")
+  seen = set()
+  for t in targets:
+    if not isinstance(t, attribute):
+      raise TypeError(f"secondOrderJacobian.__init__: every {name} item must be an attribute.")
+    if t.isDynamic:
+      raise ValueError(f"secondOrderJacobian.__init__: {name} cannot contain dynamic attributes.")
+    if t.hash in seen:
+      raise ValueError(f"secondOrderJacobian.__init__: {name} contains a duplicate target.")
+    if t.size != 3:
+      raise NotImplementedError(f"secondOrderJacobian: target {t.fullName} is not a 3-vector")
+    seen.add(t.hash)
+  return list(targets)
+
+
+class _RectTerm:
+  """One energy's instances: argument connectivity and leaves, row and
+  column slot codes, and its unprojected local Hessians."""
+
+  def __init__(self, energy: attribute, jac: "secondOrderJacobian"):
+    e = getattr(energy, "expr", None)
+    if e is None:
+      raise ValueError(f"secondOrderJacobian: {energy.fullName} is not a computed energy")
+    self.energy, self.expr, self.jac = energy, e, jac
+    self.prim = energy.correspondance
+    self._cache = {}
+
+  @property
+  def n(self) -> int:
+    return int(self.prim.numInstances)
+
+  def arguments(self):
+    """(connectivity [n, A] int32 into the leaf union, leaves, prefix, A)."""
+    torch = _torch()
+    e, n = self.expr, self.n
+    if e.kind in ("affine_inertia", "affine_snh") or (
+        e.kind == "vertex" and any(l.operator == AFFINE for l in resolve_leaf_children(e.position.source)[0])):
+      raise NotImplementedError("secondOrderJacobian: energies through affine-body vertices are not built")
+    if e.kind in ("snh", "vertex"):
+      leaves, prefix = resolve_leaf_children(e.position.source)
+      return e.position.through.value, leaves, prefix, 4 if e.kind == "snh" else e.arity
+    if e.kind == "inertia":
+      leaves = [e.x, e.x_before] + ([e.vel] if e.vel is not None else [])
+      key = ("inertia_conn", n, len(leaves))
+      if key not in self._cache:
+        i = torch.arange(n, dtype=torch.int64, device=_dev())
+        conn = torch.stack([i + k * n for k in range(len(leaves))], dim=1) if n else \
+            torch.zeros((1, len(leaves)), dtype=torch.int64, device=_dev())
+        self._cache[key] = conn.to(torch.int32).contiguous()
+      return self._cache[key], leaves, [k * n for k in range(len(leaves) + 1)], len(leaves)
+    raise NotImplementedError(f"secondOrderJacobian: energy kind {e.kind!r} is not built")
+
+  def codes(self, targets, starts):
+    torch = _torch()
+    conn, leaves, prefix, A = self.arguments()
+    kinds, wstart = [], []
+    for leaf in leaves:
+      k = next((i for i, t in enumerate(targets) if t is leaf), None)
+      kinds.append(0 if k is None else 2)
+      wstart.append(0 if k is None else int(starts[k]))
+    nc = len(leaves)
+    stride = 2 if nc > 1 else 1
+    K = A * stride
+    n = self.n
+    codes = torch.empty(max(n * K, 1), dtype=torch.int32, device=_dev())
+    sizes = torch.empty(max(n * K, 1), dtype=torch.int16, device=_dev())
+    arr = lambda v, t: (t * len(v))(*v)
+    L.call("ys_join_union_indices", L.ptr(conn), n, A, nc, arr(prefix, L.u32), arr(kinds, L.i32),
+           arr(wstart, L.u32), 3, L.ptr(codes), L.ptr(sizes), L.stream_ptr())
+    return codes, K, stride, A
+
+  def local_hessians(self, out):
+    e, n = self.expr, self.n
+    s = L.stream_ptr()
+    if n == 0:
+      return
+    if e.kind == "inertia":
+      m_kind, m_val = e.mass_p
+      mass = m_val.value if m_kind == "array" else None
+      mass_value = 0.0 if mass is not None else (m_val.scalar() if m_kind == "scene" else float(m_val))
+      dt = e.dt_p[1] if e.dt_p[0] == "value" else e.dt_p[1].scalar()
+      L.call("ys_inertia_local_hessians", L.ptr(mass), float(mass_value), float(dt), n,
+             3 if e.vel is not None else 2, L.ptr(out), s)
+      return
+    from .hessian import _Term
+    from .scene import energyRequest
+    helper = _Term(energyRequest(self.energy, [], -1, False), [], [0])
+    if e.kind == "snh":
+      a = L.SnhArgs()
+      a.position = helper._union3(e.position.source)
+      a.rest = helper._union3(e.rest.source)
+      a.tets = L.ptr(e.position.through.value)
+      a.num_elements = n
+      mu_arr, a.mu_value = helper._param(e.mu_p, n)
+      lam_arr, a.lam_value = helper._param(e.lam_p, n)
+      a.mu, a.lam = L.ptr(mu_arr), L.ptr(lam_arr)
+      a.dt = helper._param(e.dt_p, n)[1]
+      L.call("ys_snh_local_hessians", ctypes.byref(a), L.ptr(out), s)
+      return
+    a = L.EnergyArgs()
+    a.kind = e.code
+    a.position = helper._union3(e.position.source)
+    if e.rest is not None:
+      a.rest = helper._union3(e.rest.source)
+    else:
+      a.rest.num_children = 0
+    a.conn = L.ptr(e.position.through.value)
+    a.arity = e.arity
+    a.num_elements = n
+    if e.per_element is not None:
+      a.params = L.ptr(e.per_element.value)
+      a.param_stride = e.per_element.size
+    for k, p in enumerate(e.params_p):
+      a.values[k] = helper._param(p, n)[1]
+    L.call("ys_local_hessians", ctypes.byref(a), L.ptr(out), s)
+
+
+class secondOrderJacobian:
+  """Rectangular matrix ``d2E / (d row_wrt d column_wrt)`` of a sum of
+  scalar energies (``secondOrderJacobian.pyx:17-52``)."""
+
+  def __init__(self, row_wrt: List[attribute], column_wrt: List[attribute]):
+    self.__row_wrt = _validate_targets(row_wrt, "row_wrt")
+    self.__column_wrt = _validate_targets(column_wrt, "column_wrt")
+    self.__row_start = _start_indices(self.__row_wrt)
+    self.__column_start = _start_indices(self.__column_wrt)
+    self.rows = int(self.__row_start[-1])
+    self.cols = int(self.__column_start[-1])
+    self.sources: List[attribute] = []
+    self.sources_dynamic: List[attribute] = []
+    self._setup = None
+    self.blocks_flattened = None
+    self.block_positions = None
+    self.block_dimensions: List[List[int]] = []
+    self.blocks_start_indices: List[int] = [0]
+    self.block_counts: List[int] = []
+    self.blocks_flattened_dynamic = None
+    self.block_positions_dynamic = None
+    self.block_dimensions_dynamic: List[List[int]] = []
+    self.blocks_start_indices_dynamic: List[int] = [0]
+    self.block_counts_dynamic: List[int] = []
+
+  @property
+  def row_wrt(self):
+    return self.__row_wrt
+
+  @property
+  def column_wrt(self):
+    return self.__column_wrt
+
+  @property
+  def row_start_indices(self):
+    return self.__row_start
+
+  @property
+  def column_start_indices(self):
+    return self.__column_start
+
+  def __add__(self, other: "secondOrderJacobian") -> "secondOrderJacobian":
+    if not isinstance(other, secondOrderJacobian):
+      raise TypeError("secondOrderJacobian.__add__: unsupported operand type(s) for +: 'secondOrderJacobian' and "
+                      f"'{type(other).__name__}'")
+    if len(self.row_wrt) != len(other.row_wrt) or any(a is not b for a, b in zip(self.row_wrt, other.row_wrt)):
+      raise ValueError("secondOrderJacobian.__add__: row_wrt mismatch.")
+    if len(self.column_wrt) != len(other.column_wrt) or any(
+        a is not b for a, b in zip(self.column_wrt, other.column_wrt)):
+      raise ValueError("secondOrderJacobian.__add__: column_wrt mismatch.")
+    out = secondOrderJacobian(self.row_wrt, self.column_wrt)
+    out.sources = self.sources + other.sources
+    out.sources_dynamic = self.sources_dynamic + other.sources_dynamic
+    return out
+
+  # -- structure --------------------------------------------------------------------
+  def _build(self, sources):
+    torch = _torch()
+    s = L.stream_ptr()
+    terms = []
+    total = 0
+    for src in sources:
+      t = _RectTerm(src, self)
+      n = t.n
+      rc, K, stride, A = t.codes(self.__row_wrt, self.__row_start)
+      cc, _, _, _ = t.codes(self.__column_wrt, self.__column_start)
+      outer = torch.empty(n + 1, dtype=torch.int32, device=_dev())
+      L.call("ys_rect_coordinates", L.ptr(rc), L.ptr(cc), n, K, stride, A, L.ptr(outer), None, None, s)
+      m = int(outer[n].item()) if n else 0
+      N = 3 * A
+      local_h = torch.empty(max(n * N * (N + 1) // 2, 1), dtype=torch.float64, device=_dev())
+      terms.append(dict(term=t, rc=rc, cc=cc, K=K, stride=stride, A=A, outer=outer, m=m, off=total,
+                        local_h=local_h))
+      total += m
+    coords = torch.empty(max(2 * total, 2), dtype=torch.int32, device=_dev())
+    dims = torch.empty(max(2 * total, 2), dtype=torch.int16, device=_dev())
+    for d in terms:
+      if d["m"]:
+        L.call("ys_rect_coordinates", L.ptr(d["rc"]), L.ptr(d["cc"]), d["term"].n, d["K"], d["stride"], d["A"],
+               L.ptr(d["outer"]), coords.data_ptr() + 8 * d["off"], dims.data_ptr() + 4 * d["off"], s)
+    pat = _Pattern(coords, dims, total)
+    if pat.num_unique and not pat.all3:
+      raise NotImplementedError("secondOrderJacobian: only 3x3 blocks are built")
+    records = torch.empty(max(pat.total_records, 1), dtype=torch.float64, device=_dev())
+    values = torch.zeros(max(pat.total_values, 1), dtype=torch.float64, device=_dev())
+    # products: row and column pointers over the unique blocks
+    nu = pat.num_unique
+    br, bc = self.rows // 3, self.cols // 3
+    row_ptr = torch.empty(br + 1, dtype=torch.int32, device=_dev())
+    col_ptr = torch.empty(bc + 1, dtype=torch.int32, device=_dev())
+    col_order = torch.empty(max(nu, 1), dtype=torch.int32, device=_dev())
+    ws = L.u64(0)
+    L.call("ys_rect_plan_workspace_bytes", nu, ctypes.byref(ws))
+    work = torch.empty(int(ws.value), dtype=torch.uint8, device=_dev())
+    L.call("ys_rect_plan", L.ptr(pat.positions), nu, br, bc, L.ptr(row_ptr), L.ptr(col_ptr), L.ptr(col_order),
+           L.ptr(work), int(ws.value), s)
+    return dict(terms=terms, pattern=pat, records=records, values=values, plan=(row_ptr, col_ptr, col_order))
+
+  def compute(self):
+    """Evaluate every term and assemble (``secondOrderJacobian.pyx:530-559``;
+    dynamic sources rebuild their pattern on every call)."""
+    torch = _torch()
+    if self.rows % 3 or self.cols % 3:
+      raise NotImplementedError("secondOrderJacobian: targets of 3-vectors only")
+    s = L.stream_ptr()
+    if self._setup is None:
+      self._setup = self._build(self.sources)
+    dyn = self._build(self.sources_dynamic) if self.sources_dynamic else None
+    for part, name in ((self._setup, ""), (dyn, "_dynamic")):
+      if part is None:
+        continue
+      pat = part["pattern"]
+      for d in part["terms"]:
+        t = d["term"]
+        if t.n == 0 or d["m"] == 0:
+          continue
+        t.local_hessians(d["local_h"])
+        L.call("ys_rect_records", L.ptr(d["local_h"]), d["A"], L.ptr(d["rc"]), L.ptr(d["cc"]), t.n, d["K"],
+               d["stride"], L.ptr(d["outer"]), pat.record.data_ptr() + 4 * d["off"], L.ptr(part["records"]), s)
+      if pat.num_unique:
+        L.call("ys_assemble3", L.ptr(part["records"]), L.ptr(pat.record_begin), L.ptr(pat.record_count),
+               L.ptr(pat.value_offset), pat.num_unique, L.ptr(part["values"]), None, s)
+      nu = pat.num_unique
+      setattr(self, "blocks_flattened" + name, part["values"][:pat.total_values] if nu else part["values"][:0])
+      setattr(self, "block_positions" + name, pat.positions[:2 * nu])
+      setattr(self, "block_dimensions" + name, [[3, 3]] if nu else [])
+      setattr(self, "blocks_start_indices" + name, [0, 9 * nu] if nu else [0])
+      setattr(self, "block_counts" + name, [nu] if nu else [])
+    self._dynamic_part = dyn
+    return self
+
+  # -- products -----------------------------------------------------------------------
+  def spmv(self, x: vector, transpose: bool = False) -> vector:
+    """``J x`` (or ``J^T x``) as a new vector (``matrix.pyx:393-408``)."""
+    if not isinstance(x, vector):
+      raise TypeError("matrix.spmv: x must be a vector.")
+    if not isinstance(transpose, (bool, np.bool_)):
+      raise TypeError("matrix.spmv: transpose must be a bool.")
+    n_in, n_out = (self.rows, self.cols) if transpose else (self.cols, self.rows)
+    if x.size != n_in:
+      orientation = "transposed " if transpose else ""
+      raise ValueError(f"matrix.spmv: input vector for {orientation}matrix has size {x.size}, expected {n_in}.")
+    if self._setup is None:
+      raise RuntimeError("secondOrderJacobian.spmv: call compute() first")
+    out = vector(n_out)
+    s = L.stream_ptr()
+    br, bc = self.rows // 3, self.cols // 3
+    parts = [p for p in (self._setup, getattr(self, "_dynamic_part", None)) if p is not None]
+    tmp = vector(n_out)
+    for k, part in enumerate(parts):
+      dst = out if k == 0 else tmp
+      row_ptr, col_ptr, col_order = part["plan"]
+      L.call("ys_rect_spmv", L.ptr(part["values"]), L.ptr(part["pattern"].positions), L.ptr(row_ptr), L.ptr(col_ptr),
+             L.ptr(col_order), br, bc, L.ptr(x.value), L.ptr(dst.value), int(bool(transpose)), s)
+      if k:
+        out.value.add_(tmp.value)
+    return out
+
+
+class gradient(vector):
+  """Gradient of scalar energies with respect to targets, as ``diff1``
+  returns it (``differentiator.pyx:174-239``): ``compute`` evaluates the
+  energies and fills ``value``."""
+
+  def __init__(self, wrt, parent: hessian):
+    self.wrt = list(wrt)
+    self.parent = parent
+    super().__init__(parent.rows)
+
+  def compute(self):
+    self.parent.compute()
+    self.value = self.parent.gradient.value
+    return self
+
+
+class differentiator:
+  """``diff1`` / ``diff2`` (``PKG/differentiator/differentiator.pyx:174-489``)."""
+
+  @staticmethod
+  def _same(a, b):
+    return len(a) == len(b) and all(x is y for x, y in zip(a, b))
+
+  def diff2(self, source, target1, target2, local_targets=(), projection_method=1, save_intermediate=False,
+            separate_hessian_jacobian=False, dynamic_instances=False, grouped_add=False, lto=False):
+    from .scene import energyRequest
+    src = list(source) if isinstance(source, (list, tuple)) else [source]
+    if not src:
+      raise ValueError("differentiator.diff2: source can not be empty.")
+    if self._same(list(target1), list(target2)):
+      reqs = [energyRequest(e, list(local_targets), int(projection_method), bool(dynamic_instances)) for e in src]
+      return hessian(list(target1), [] if dynamic_instances else reqs, reqs if dynamic_instances else [])
+    for e in src:
+      if e.size != 1:
+        raise ValueError("differentiator.__diff2_jacobian_single: source must be a scalar attribute.")
+    jac = secondOrderJacobian(list(target1), list(target2))
+    if dynamic_instances:
+      jac.sources_dynamic = src
+    else:
+      jac.sources = src
+    return jac
+
+  def diff1(self, source, global_targets, local_targets=(), dynamic_instances=False):
+    from .scene import energyRequest
+    src = list(source) if isinstance(source, (list, tuple)) else [source]
+    if not src:
+      raise ValueError("differentiator.diff1: source can not be empty.")
+    if not isinstance(global_targets, list) or not global_targets:
+      raise ValueError("differentiator.diff1: global_targets can not be empty.")
+    if any(e.size != 1 for e in src):
+      raise NotImplementedError("differentiator.diff1: first-order Jacobians of vector-valued sources are not built")
+    reqs = [energyRequest(e, list(local_targets), -1, bool(dynamic_instances)) for e in src]
+    parent = hessian(list(global_targets), [] if dynamic_instances else reqs, reqs if dynamic_instances else [])
+    return gradient(global_targets, parent)
