@@ -549,9 +549,10 @@ def serving_leg(args):
   srv.register(range(8, 49), slots_per_side=3)
   t_register = time.perf_counter() - t0
   srv.run(serving.poisson_fem_stream(count=82, mean_spacing=0.0, seed=99))
-  # steady state: an untimed pass of the two timed streams grows the
-  # per-side slot pools to what they need, so no slot (device allocations,
-  # which synchronise) is created inside the timed streams
+  # steady state: pools sized for the timed streams (no slot, a device
+  # allocation that synchronises, is created inside them) and an untimed
+  # pass of the two timed streams (the CUDA graphs of their size buckets)
+  srv.reserve(serving.poisson_fem_stream(count=n, mean_spacing=2e-3, seed=0))
   srv.run(serving.poisson_fem_stream(count=n, mean_spacing=2e-3, seed=0))
   srv.run(serving.poisson_fem_stream(count=n, mean_spacing=0.0, seed=0))
   srv.solve_serial_fp64(serving.poisson_fem_stream(count=41, mean_spacing=0.0, seed=98))

@@ -307,17 +307,33 @@ class NewtonServer:
         self._idle[topo.key].append(slot)
     _torch().cuda.synchronize()
 
-  def _new_slot(self, topo: SceneTopology) -> Optional[_Slot]:
+  def reserve(self, requests) -> None:
+    """Pool enough slots for ``requests`` (their count per topology, at most
+    ``max_slots`` each) within the memory budget, so serving that stream
+    creates no slot (a device allocation synchronises the device)."""
+    need = collections.Counter(r.topology_key for r in requests)
+    for key, count in need.items():
+      topo = self.topology(key)
+      while len(self._idle[key]) < min(count, self.max_slots):
+        slot = self._new_slot(topo, evict=False)
+        if slot is None:
+          break
+        self._idle[key].append(slot)
+    _torch().cuda.synchronize()
+
+  def _new_slot(self, topo: SceneTopology, evict: bool = True) -> Optional[_Slot]:
     need = getattr(topo, "slot_bytes", None)
     if need is not None and self.resident_bytes + need > self.memory_budget:
-      self._evict_idle(need)
+      if evict:
+        self._evict_idle(need)
       if self.resident_bytes + need > self.memory_budget:
         return None
     self.slots_created += 1
     slot = _Slot(topo)
     topo.slot_bytes = slot.nbytes
     if self.resident_bytes + slot.nbytes > self.memory_budget:
-      self._evict_idle(slot.nbytes)
+      if evict:
+        self._evict_idle(slot.nbytes)
       if self.resident_bytes + slot.nbytes > self.memory_budget:
         slot.release()
         return None
