@@ -118,8 +118,10 @@ def baraff_witkin(x, rest, p):
   f = _membrane_f(x, rest)
   i6 = f[:, 0].dot(f[:, 1])
   i5u, i5v = torch.linalg.norm(f[:, 0]), torch.linalg.norm(f[:, 1])
-  uc = torch.where(i5u < 1.0, 0.01, 1.0)
-  vc = torch.where(i5v < 1.0, 0.01, 1.0)
+  # selects between float64 constants (python scalars would give float32)
+  lo, one = i5u.new_tensor(0.01), i5u.new_tensor(1.0)
+  uc = torch.where(i5u < 1.0, lo, one)
+  vc = torch.where(i5v < 1.0, lo, one)
   stretch = uc * (i5u - 1.0) ** 2 + vc * (i5v - 1.0) ** 2
   return (stretch_s * stretch + shear_s * i6 * i6) * thickness * _rest_area(rest) * dt * dt
 

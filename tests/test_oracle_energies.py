@@ -101,3 +101,22 @@ def test_batched_differentiation_matches_one_element_at_a_time(kind):
   for a, b in zip(batched, single):
     assert np.all(np.isfinite(a))
     assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+
+
+def test_baraff_witkin_select_keeps_float64():
+  """The stretch weights (0.01 below unit stretch, else 1) are float64
+  constants: the energy equals its direct float64 evaluation to rounding
+  (a float32 0.01 would be off by 2e-8 relative)."""
+  import torch
+  rng = np.random.default_rng(3)
+  tri = np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 0.1], [0.1, 0.0, 0.0]])
+  x = tri + rng.uniform(-3e-3, 3e-3, size=(3, 3))
+  rest = tri.copy()
+  p = (2000.0, 1000.0, 1e-3, 0.01)
+  e = float(ve.baraff_witkin(torch.tensor(x), torch.tensor(rest), p))
+  f = ve._membrane_f(torch.tensor(x), torch.tensor(rest)).numpy()
+  u, v = np.linalg.norm(f[:, 0]), np.linalg.norm(f[:, 1])
+  cu, cv = (0.01 if u < 1.0 else 1.0), (0.01 if v < 1.0 else 1.0)
+  area = 0.5 * np.linalg.norm(np.cross(rest[1] - rest[0], rest[2] - rest[0]))
+  ref = (p[0] * (cu * (u - 1.0) ** 2 + cv * (v - 1.0) ** 2) + p[1] * (f[:, 0] @ f[:, 1]) ** 2) * p[2] * area * p[3] ** 2
+  assert abs(e - ref) <= 1e-14 * abs(ref)
