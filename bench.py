@@ -326,9 +326,9 @@ GEMV_LAYOUT_56 = 111_651_744  # tiled-layout bytes of one domain-GEMV launch on 
 
 
 # DRAM bytes (read + write) of one tiled SpMV launch on this 64^3 workload,
-# from an ncu capture of the same launch (dram__bytes_read.sum +
-# dram__bytes_write.sum); None on other sizes
-SPMV_TILED_TRAFFIC_64 = None
+# from an ncu capture of the same launch (dram__bytes.sum.per_second x
+# gpu__time_duration.sum = 3.0907 TB/s x 45.024 us); None on other sizes
+SPMV_TILED_TRAFFIC_64 = 139.16e6
 
 
 def spmv_roofline(H, hbm, peak_kind, side, reps=50):
