@@ -664,7 +664,8 @@ int32_t ys_assemble_strided(const double* records, const uint32_t* begin, const 
                             double* out, void* stream);
 /* FP64 iterative-refinement residual: x += delta (when delta is not NULL),
  * r = rhs - H x with the FP64 blocks of `m`, and ||r||^2, ||rhs||^2 (host
- * norms_host[0..1] when not NULL, synchronising `stream`).  workspace holds
+ * norms_host[0..1] when not NULL, synchronising `stream`).  x NULL stands
+ * for the zero vector (r = rhs, no product; delta must then be NULL).  workspace holds
  * ys_refine_workspace_doubles(num_vars) doubles.  The FP64 audit of the
  * reference's mixed_spmv mode (PKG/solver/mas/solver.py:643-688).           */
 uint64_t ys_refine_workspace_doubles(uint32_t num_vars);

@@ -388,8 +388,9 @@ __global__ void __launch_bounds__(kPcgBlock) refine_residual(RefineParams P) {
   double v[2] = {0.0, 0.0};
   for (uint32_t gb = blockIdx.x; gb < groups; gb += gridDim.x) {  // block-uniform
     const uint32_t i = gb * kRows + threadIdx.x / kRowLanes;
-    double h[3];
-    spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.x, h[0], h[1], h[2]);
+    double h[3] = {0.0, 0.0, 0.0};
+    // x == NULL is the zero vector: r = g without the product
+    if (P.x) spmv3_group(P.sets, P.nsets, false, i, i < P.nv, lane, P.x, h[0], h[1], h[2]);
     if (i < P.nv && lane == 0) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -675,6 +676,7 @@ int32_t ys_refine_residual(const ys_matrix3* m, const double* rhs, double* x, co
   cudaStream_t s = (cudaStream_t)stream;
   const uint32_t nv = m->num_vars;
   const unsigned grid = ys::grid_for(nv, ys::kPcgBlock);
+  YS_REQUIRE(x || !delta, YS_ERR_INVALID, "a correction needs the solution vector");
   if (delta) {
     ys::refine_add<<<grid, ys::kPcgBlock, 0, s>>>(nv, x, delta);
     YS_CHECK_LAUNCH();

@@ -392,7 +392,7 @@ class masSolver(_PcgBase):
     total_its, refinements, status = 0, 0, -4
     # x = 0, r = g (the refinement residual of the zero guess)
     x.zero_()
-    L.call("ys_refine_residual", ctypes.byref(m), L.ptr(rhs), L.ptr(x), None, L.ptr(r), L.ptr(work), norms,
+    L.call("ys_refine_residual", ctypes.byref(m), L.ptr(rhs), None, None, L.ptr(r), L.ptr(work), norms,
            L.stream_ptr())
     gnorm = float(np.sqrt(norms[1]))
     rnorm = float(np.sqrt(norms[0]))
