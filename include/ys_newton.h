@@ -630,6 +630,16 @@ int32_t ys_mas_create(const ys_mas_desc* desc, void** handle);
  * mas/cuda/local_inverse.cu:190-545).  When failed_domains is not NULL the
  * call synchronises and reports singular domains (YS_ERR_SINGULAR_DOMAIN). */
 int32_t ys_mas_numeric_update(void* handle, const double* fine_values, void* stream, int32_t* failed_domains);
+/* FP64 values of the union of two 3x3 block sets on their union pattern
+ * (the MAS fine level of a Hessian with a dynamic contact set): block u is
+ * a[9 a_index[u] ..] + b[9 b_index[u] ..], a negative index meaning no block
+ * of that set; pass the result to ys_mas_numeric_update of a handle whose
+ * fine blocks are the union pattern.  The reference adds the dynamic blocks
+ * into the domain matrices of every level
+ * (PKG/solver/mas/cuda/dynamic_assembly_specialized.cu:81-112,
+ * mas/numeric_assembly.py:64-83 over "both" block sets).                    */
+int32_t ys_mas_union_values(const double* a, const int32_t* a_index, const double* b, const int32_t* b_index,
+                            uint32_t num_blocks, double* out, void* stream);
 /* Singular domains of the last ys_mas_numeric_update on `stream` (which may
  * have been called without failed_domains, so the check can wait for a
  * later synchronisation); synchronises the stream; YS_ERR_SINGULAR_DOMAIN

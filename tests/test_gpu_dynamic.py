@@ -106,3 +106,71 @@ def test_dynamic_pairs_rebuild_their_pattern():
     segs = sc.minimizeEnergy(tolerance=1e-10, maxIterations=5000)
     x = segs[0].cpu().numpy()
     assert np.linalg.norm(exp_h @ x - exp_g) <= 1e-10 * np.linalg.norm(exp_g)
+
+
+def test_mas_with_a_dynamic_contact_set():
+  """MAS over a static and a dynamic block set: the hierarchy is built on the
+  static graph (the reference's default) and the dynamic blocks enter the
+  domain matrices of every level, as the reference's numeric assembly over
+  both sets does (mas/numeric_assembly.py:64-83).  The device MAS apply
+  equals the oracle MAS on the same hierarchy with every block (FP32
+  inverses: 2e-4), and the MAS PCG meets the oracle system's residual, as
+  the pair set changes."""
+  import torch
+  from oracle import mas as omas
+  from yasps_b200 import _lib as L
+  from yasps_b200 import energies as E
+  from yasps_b200.scene import scene as make_scene
+  vs = VertexScene(m=6, seed=8)
+  sc = make_scene("dynamic_contacts_mas")
+  mesh = sc.addMesh("cloth")
+  verts = mesh.addPrimitive("vertices", numInstances=len(vs.x))
+  pos = verts.addAttribute("position", rows=3, cols=1)
+  pos.updateValue(vs.x)
+  rest = verts.addConstant("rest_position", rows=3, cols=1)
+  rest.updateValue(vs.rest)
+  old = verts.addConstant("old_position", rows=3, cols=1)
+  old.updateValue(vs.x_old)
+  mass = verts.addConstant("mass")
+  mass.updateValue(vs.mass)
+  tri = mesh.addPrimitive("tris", numInstances=len(vs.tris))
+  tc = tri.addConnectivity("to_vertices", verts, vs.tris.astype(np.uint32), 3)
+  mem = tri.addAttribute("membrane", computed_attribute=E.baraff_witkin(
+      tri.addAttribute("rest", through=tc, source=rest), tri.addAttribute("x", through=tc, source=pos),
+      *vs.mem_params))
+  pairs = mesh.addPrimitive("pairs", numInstances=len(vs.pt), isDynamic=True)
+  pc = pairs.addConnectivity("to_vertices", verts, vs.pt.astype(np.uint32), 4)
+  bar = pairs.addAttribute("barrier", computed_attribute=E.point_triangle(
+      pairs.addAttribute("x", through=pc, source=pos), vs.dhat, vs.kappa))
+  kin = verts.addAttribute("inertia", computed_attribute=E.inertia(old, None, vs.dt, pos, mass,
+                                                                      gravity=tuple(vs.gravity)))
+  sc.addEnergy(mem, projection_method=1)
+  sc.addEnergy(bar, projection_method=1, dynamic_instances=True)
+  sc.addEnergy(kin, projection_method=-1)
+  sc.addMinimizeTarget([pos])
+  sc.minimizer.setSolver("mas", fine_level_weight=1.0, stop_rule="residual")
+  nv = len(vs.x)
+  for active in (vs.pt, vs.pt[:3], vs.pt[::-1][:4]):
+    pairs.updateNumInstances(len(active))
+    pc.updateConnectivity(active.astype(np.uint32))
+    H = sc.minimizer.computeNumericValue()
+    exp_h, exp_g = oracle_dense(vs, active)
+    ms = sc.minimizer.linearSolver.implementation
+    ms._ensure_hierarchy(H)
+    assert len(H.block_sets) == 2 and ms._union is not None
+    assert ms.numeric_update(H) == 0
+    r = np.cos(np.arange(H.rows) * 0.37)
+    rt = torch.from_numpy(r).cuda()
+    z = torch.zeros_like(rt)
+    L.call("ys_mas_apply", ms._mas, L.ptr(rt), L.ptr(z), L.stream_ptr())
+    spos = H.block_sets[0].pattern
+    sp = spos.positions[:2 * spos.num_unique].cpu().numpy().astype(np.int64).reshape(-1, 2)
+    h = omas.build_hierarchy(np.full(nv, 3), [(a // 3, b // 3) for a, b in sp if a != b])
+    blocks = [(a, b, exp_h[3 * a:3 * a + 3, 3 * b:3 * b + 3]) for a in range(nv) for b in range(a, nv)
+              if np.any(exp_h[3 * a:3 * a + 3, 3 * b:3 * b + 3] != 0.0)]
+    pre = omas.MASPreconditioner(h, omas.level_local_matrices(h, blocks))
+    ref = pre.apply(r)
+    assert np.linalg.norm(z.cpu().numpy() - ref) <= 2e-4 * np.linalg.norm(ref)
+    segs = sc.minimizeEnergy(tolerance=1e-10, maxIterations=5000)
+    x = segs[0].cpu().numpy()
+    assert np.linalg.norm(exp_h @ x - exp_g) <= 1e-10 * np.linalg.norm(exp_g)

@@ -171,6 +171,7 @@ SIGNATURES = {
     "ys_pcg_destroy": (i32, [vp]),
     "ys_mas_create": (i32, [P(MasDesc), P(vp)]),
     "ys_mas_numeric_update": (i32, [vp, vp, vp, P(i32)]),
+    "ys_mas_union_values": (i32, [vp, vp, vp, vp, u32, vp, vp]),
     "ys_mas_apply": (i32, [vp, vp, vp, vp]),
     "ys_mas_destroy": (i32, [vp]),
     "ys_mas_gemv": (i32, [vp, vp, P(u64)]),

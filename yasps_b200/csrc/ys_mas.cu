@@ -68,6 +68,22 @@ __global__ void __launch_bounds__(256) mas_level_blocks(MasDev M, uint32_t begin
   }
 }
 
+// Union of two 3x3 block sets (the static set and the dynamic contact set)
+// on their union pattern: block u = A[a_index[u]] + B[b_index[u]], a
+// negative index standing for no block (one order, deterministic).
+__global__ void union_values_kernel(const double* __restrict__ a, const int32_t* __restrict__ ai,
+                                    const double* __restrict__ b, const int32_t* __restrict__ bi, uint32_t nu,
+                                    double* __restrict__ out) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 9ull * nu) return;
+  const uint32_t u = (uint32_t)(t / 9), e = (uint32_t)(t % 9);
+  const int32_t ia = ai[u], ib = bi[u];
+  double v = 0.0;
+  if (ia >= 0) v = a[9ull * ia + e];
+  if (ib >= 0) v += b[9ull * ib + e];
+  out[t] = v;
+}
+
 // f(integral_constant<int, I>) for I = B .. E-1 (a loop whose index is a
 // compile-time constant in its body).
 template <int B, int E, typename F>
@@ -889,6 +905,16 @@ int32_t ys_mas_create(const ys_mas_desc* d, void** handle) {
     return YS_ERR_CUDA;
   }
   *handle = h;
+  return YS_OK;
+}
+
+int32_t ys_mas_union_values(const double* a, const int32_t* a_index, const double* b, const int32_t* b_index,
+                            uint32_t num_blocks, double* out, void* stream) {
+  YS_REQUIRE(out && a_index && b_index, YS_ERR_INVALID, "null argument");
+  if (num_blocks == 0) return YS_OK;
+  ys::union_values_kernel<<<ys::grid_for(9ull * num_blocks, 256), 256, 0, (cudaStream_t)stream>>>(
+      a, a_index, b, b_index, num_blocks, out);
+  YS_CHECK_LAUNCH();
   return YS_OK;
 }
 

@@ -300,24 +300,50 @@ class masSolver(_PcgBase):
     if self._mas is not None:
       L.call("ys_mas_destroy", self._mas)
     self._mas, self._mas_key, self.hierarchy, self._tables, self._dev_tables = None, None, None, None, None
+    self._hierarchy_key, self._union = None, None
 
   def _ensure_hierarchy(self, H):
+    """The hierarchy is built on the static block set's graph (the reference's
+    default, ``include_dynamic_edges=False``, ``mas/hierarchy.py:158``); with a
+    dynamic (contact) set, the fine level of the numeric update is the union
+    of both sets, so its blocks enter the domain matrices of every level as
+    the reference assembles them (``mas/numeric_assembly.py:64-83``); the
+    tables follow the dynamic pattern."""
     torch = _torch()
     sets = H.block_sets
-    if len(sets) != 1:
-      raise NotImplementedError("the device MAS assembles one static 3x3 block set")
+    if not sets or len(sets) > 2:
+      raise NotImplementedError("the device MAS takes a static and at most one dynamic 3x3 block set")
     bs = sets[0]
-    key = (id(bs.pattern), H.rows)
+    dyn = sets[1] if len(sets) == 2 else None
+    key = (id(bs.pattern), None if dyn is None else id(dyn.pattern), H.rows)
     if key == self._mas_key:
       return
     if self._mas is not None:
       L.call("ys_mas_destroy", self._mas)
       self._mas = None
+    if not all(s.pattern.all3 for s in sets):
+      raise NotImplementedError("the device MAS supports 3x3 blocks (3-DoF variables)")
     pos = bs.pattern.positions[:2 * bs.pattern.num_unique].cpu().numpy().astype(np.int64).reshape(-1, 2)
     nv = H.rows // 3
-    edges = pos[pos[:, 0] != pos[:, 1]] // 3
-    self.hierarchy = mas_hierarchy.build_hierarchy(np.full(nv, 3), edges, self.max_domain_dofs, self.max_levels,
-                                                   self.target_nodes, self.global_coarse_domain)
+    hkey = (id(bs.pattern), H.rows)
+    if getattr(self, "_hierarchy_key", None) != hkey or self.hierarchy is None:
+      edges = pos[pos[:, 0] != pos[:, 1]] // 3
+      self.hierarchy = mas_hierarchy.build_hierarchy(np.full(nv, 3), edges, self.max_domain_dofs, self.max_levels,
+                                                     self.target_nodes, self.global_coarse_domain)
+      self._hierarchy_key = hkey
+    self._union = None
+    if dyn is not None:
+      dpos = dyn.pattern.positions[:2 * dyn.pattern.num_unique].cpu().numpy().astype(np.int64).reshape(-1, 2)
+      n = H.rows
+      keys = np.concatenate([pos[:, 0] * n + pos[:, 1], dpos[:, 0] * n + dpos[:, 1]])
+      uniq, inv = np.unique(keys, return_inverse=True)
+      ia = np.full(uniq.size, -1, dtype=np.int32)
+      ib = np.full(uniq.size, -1, dtype=np.int32)
+      ia[inv[:len(pos)]] = np.arange(len(pos), dtype=np.int32)
+      ib[inv[len(pos):]] = np.arange(len(dpos), dtype=np.int32)
+      pos = np.stack([uniq // n, uniq % n], axis=1)
+      self._union = (torch.from_numpy(ia).to(_dev()), torch.from_numpy(ib).to(_dev()),
+                     torch.zeros(9 * uniq.size, dtype=torch.float64, device=_dev()), int(uniq.size))
     t = mas_hierarchy.build_tables(self.hierarchy, pos)
     self._tables = t
     weights = self.weights_for(len(self.hierarchy.levels))
@@ -331,7 +357,13 @@ class masSolver(_PcgBase):
 
   def numeric_update(self, H, check=True):
     failed = ctypes.c_int32(0)
-    L.call("ys_mas_numeric_update", self._mas, L.ptr(H.block_sets[0].values), L.stream_ptr(),
+    values = H.block_sets[0].values
+    if getattr(self, "_union", None) is not None:
+      ia, ib, out, nu = self._union
+      L.call("ys_mas_union_values", L.ptr(values), L.ptr(ia), L.ptr(H.block_sets[1].values), L.ptr(ib), nu,
+             L.ptr(out), L.stream_ptr())
+      values = out
+    L.call("ys_mas_numeric_update", self._mas, L.ptr(values), L.stream_ptr(),
            ctypes.byref(failed) if check else None)
     return int(failed.value)
 
