@@ -289,11 +289,16 @@ int32_t ys_rect_coordinates(const uint32_t* row_codes, const uint32_t* col_codes
  * ys_rect_coordinates, at record[coord_outer[t] + k] (the assembly plan of
  * ys_pattern_build over those coordinates): the sum of the local Hessian's
  * argument blocks of the pair's row group and column group.  Sum them with
- * ys_assemble3.  Replaces compute_second_order_jacobian_no_project
+ * ys_assemble3.  difference_args = D > 0 (args = 2 D): the local Hessians
+ * cover the first D arguments of an energy of x - x_old only (the lagged
+ * friction kinds), arguments D .. 2D-1 are the step-start positions, and
+ * their blocks are the first ones negated once per step-start side.
+ * Replaces compute_second_order_jacobian_no_project
  * (secondOrderJacobianKernel.pyx:86-140).                                  */
-int32_t ys_rect_records(const double* local_hessians, uint32_t args, const uint32_t* row_codes,
-                        const uint32_t* col_codes, uint32_t n, uint32_t K, uint32_t slot_stride,
-                        const uint32_t* coord_outer, const uint32_t* record, double* records, void* stream);
+int32_t ys_rect_records(const double* local_hessians, uint32_t args, uint32_t difference_args,
+                        const uint32_t* row_codes, const uint32_t* col_codes, uint32_t n, uint32_t K,
+                        uint32_t slot_stride, const uint32_t* coord_outer, const uint32_t* record, double* records,
+                        void* stream);
 
 /* Products with the assembled rectangular matrix (unique 3x3 blocks sorted
  * by (row, col), scalar positions).  ys_rect_plan builds row_ptr

@@ -140,3 +140,55 @@ def test_square_and_gradient_forms():
   assert np.abs(v1.cpu().numpy() - v2.cpu().numpy()).max() <= 1e-13 * np.abs(v1.cpu().numpy()).max()
   g = d.diff1(energies, [h["free_position"]]).compute()
   assert np.abs(g.value.cpu().numpy() - g_scene).max() <= 1e-13 * np.abs(g_scene).max()
+
+
+@pytest.mark.parametrize("kind", [8, 9, 10, 11])
+def test_friction_position_against_step_start_positions(kind):
+  """Lagged friction is a function of x - x_old: d2E/(dx dx_old) is minus the
+  unprojected position Hessian, argument by argument (the oracle's local
+  Hessian folded over the step-start leaves)."""
+  from tests.vertex_scene import VertexScene
+  from yasps_b200 import energies as E
+  from yasps_b200.scene import scene as make_scene
+  vs = VertexScene(m=6, seed=5)
+  conn = {8: vs.pt, 9: vs.pe, 10: vs.ee, 11: vs.pp}[kind]
+  lag = {8: vs.lagged, 9: vs.lagged_pe, 10: vs.lagged_ee, 11: vs.lagged_pp}[kind]
+  sc = make_scene("friction_rect")
+  m = sc.addMesh("m")
+  verts = m.addPrimitive("vertices", numInstances=len(vs.x))
+  pos = verts.addAttribute("position", rows=3, cols=1)
+  pos.updateValue(vs.x)
+  old = verts.addConstant("old_position", rows=3, cols=1)
+  old.updateValue(vs.x_old)
+  prim = m.addPrimitive("pairs", numInstances=len(conn))
+  c = prim.addConnectivity("to_vertices", verts, conn.astype(np.uint32), conn.shape[1])
+  lagged = prim.addConstant("lagged", rows=9, cols=1)
+  lagged.updateValue(lag)
+  fric = {8: E.friction_point_triangle, 9: E.friction_point_edge, 10: E.friction_edge_edge,
+          11: E.friction_point_point}[kind]
+  e = prim.addAttribute("friction", computed_attribute=fric(
+      prim.addAttribute("x", through=c, source=pos), prim.addAttribute("x_old", through=c, source=old),
+      *vs.fric_params, lagged))
+  J = differentiator().diff2([e], [pos], [old]).compute()
+  _, _, h = ve.energy_grad_hess(kind, vs.x[conn], vs.x_old[conn], vs.fric_params, lag)
+  A = conn.shape[1]
+  ext = np.block([[h, -h], [-h, h]])
+  ids = conn.astype(np.int64)
+  zero = np.zeros_like(ids)
+  rc = np.concatenate([2 + 3 * ids, zero], axis=1)
+  ccode = np.concatenate([zero, 2 + 3 * ids], axis=1)
+  assert ext.shape[1] == 6 * A
+  check(J, orj.dense(ext, rc, ccode, J.rows, J.cols), rc, ccode)
+
+
+def test_rest_shape_targets_are_refused():
+  """A mixed derivative through a rest shape (here the SNH rest positions)
+  is not built and raises instead of returning a zero matrix."""
+  cube = scenes.fem_cube(4, noise=0.01, seed=1)
+  sc, h = scenes.fem_scene(cube)
+  snh = next(r.energy for r in sc.minimizer.requests if r.energy.expr.kind == "snh")
+  from yasps_b200.graph import resolve_leaf_children
+  rest_leaf = resolve_leaf_children(snh.expr.rest.source)[0][-1]  # the free vertices' rest positions
+  J = differentiator().diff2([snh], [h["free_position"]], [rest_leaf])
+  with pytest.raises(NotImplementedError):
+    J.compute()

@@ -137,7 +137,7 @@ SIGNATURES = {
     "ys_snh_local_hessians": (i32, [P(SnhArgs), vp, vp]),
     "ys_inertia_local_hessians": (i32, [vp, f64, f64, u32, u32, vp, vp]),
     "ys_rect_coordinates": (i32, [vp, vp, u32, u32, u32, u32, vp, vp, vp, vp]),
-    "ys_rect_records": (i32, [vp, u32, vp, vp, u32, u32, u32, vp, vp, vp, vp]),
+    "ys_rect_records": (i32, [vp, u32, u32, vp, vp, u32, u32, u32, vp, vp, vp, vp]),
     "ys_rect_plan_workspace_bytes": (i32, [u32, P(u64)]),
     "ys_rect_plan": (i32, [vp, u32, u32, u32, vp, vp, vp, vp, u64, vp]),
     "ys_rect_spmv": (i32, [vp, vp, vp, vp, vp, u32, u32, vp, vp, u32, vp]),

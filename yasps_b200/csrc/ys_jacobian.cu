@@ -75,22 +75,32 @@ __global__ void rect_coords_kernel(const uint32_t* __restrict__ row_codes, const
 }
 
 // Records of one instance: for every (row group, column group) the sum of
-// its argument blocks of the packed upper local Hessian.
-__global__ void rect_records_kernel(const double* __restrict__ local_h, int args,
+// its argument blocks of the packed upper local Hessian.  With `diff` > 0
+// the local Hessian covers the first `diff` arguments only and arguments
+// diff .. 2 diff - 1 are the step-start positions of an energy of x - x_old:
+// their blocks are the first ones negated once per step-start side.
+__global__ void rect_records_kernel(const double* __restrict__ local_h, int args, int diff,
                                     const uint32_t* __restrict__ row_codes, const uint32_t* __restrict__ col_codes,
                                     uint32_t n, uint32_t K, uint32_t stride, const uint32_t* __restrict__ outer,
                                     const uint32_t* __restrict__ record, double* __restrict__ out) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const int N = 3 * args;
+  const int hargs = diff > 0 ? diff : args;
+  const int N = 3 * hargs;
   const double* h = local_h + (uint64_t)t * (N * (N + 1) / 2);
   int rg[kRectMaxArgs], rf[kRectMaxArgs], cg[kRectMaxArgs], cf[kRectMaxArgs];
   const int nr = rect_groups(row_codes, t, K, stride, args, rg, rf);
   const int nc = rect_groups(col_codes, t, K, stride, args, cg, cf);
-  // packed upper index of (r, c) for any order
+  // packed upper index of (r, c) for any order, arguments folded onto the
+  // local Hessian's with their sign
   auto at = [&](int r, int c) {
+    double sign = 1.0;
+    if (diff > 0) {
+      if (r >= N) { r -= N; sign = -sign; }
+      if (c >= N) { c -= N; sign = -sign; }
+    }
     const int lo = r < c ? r : c, hi = r < c ? c : r;
-    return h[lo * N - lo * (lo - 1) / 2 + (hi - lo)];
+    return sign * h[lo * N - lo * (lo - 1) / 2 + (hi - lo)];
   };
   uint32_t o = outer[t];
   for (int i = 0; i < nr; ++i)
@@ -211,15 +221,19 @@ int32_t ys_rect_coordinates(const uint32_t* row_codes, const uint32_t* col_codes
   return YS_OK;
 }
 
-int32_t ys_rect_records(const double* local_hessians, uint32_t args, const uint32_t* row_codes,
-                        const uint32_t* col_codes, uint32_t n, uint32_t K, uint32_t slot_stride,
-                        const uint32_t* coord_outer, const uint32_t* record, double* records, void* stream) {
+int32_t ys_rect_records(const double* local_hessians, uint32_t args, uint32_t difference_args,
+                        const uint32_t* row_codes, const uint32_t* col_codes, uint32_t n, uint32_t K,
+                        uint32_t slot_stride, const uint32_t* coord_outer, const uint32_t* record, double* records,
+                        void* stream) {
   YS_REQUIRE(local_hessians && row_codes && col_codes && coord_outer && record && records, YS_ERR_INVALID,
              "null argument");
   YS_REQUIRE(args >= 1 && args <= (uint32_t)ys::kRectMaxArgs, YS_ERR_INVALID, "1..8 arguments an instance");
+  YS_REQUIRE(difference_args == 0 || 2 * difference_args == args, YS_ERR_INVALID,
+             "difference form: args must be twice difference_args");
   if (n == 0) return YS_OK;
   ys::rect_records_kernel<<<ys::grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(
-      local_hessians, (int)args, row_codes, col_codes, n, K, slot_stride, coord_outer, record, records);
+      local_hessians, (int)args, (int)difference_args, row_codes, col_codes, n, K, slot_stride, coord_outer, record,
+      records);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

@@ -25,10 +25,11 @@ the leaves of the position union (so ``row_wrt=[cloth position]``,
 blocks), for the inertia term its ``x``, ``x_before`` and ``vel``
 attributes (the adjoint blocks ``d2E / (dx dx_before)`` and
 ``d2E / (dx dvel)`` of the reference's differentiable-simulation examples,
-``examples/bunny_dropping_on_ground/bunny_dropping_on_ground.py:333-334``).
-Mixed derivatives through the rest / lagged arguments of an energy (rest
-shapes, the last step's positions of friction) and through affine-body
-vertices are not built.
+``examples/bunny_dropping_on_ground/bunny_dropping_on_ground.py:333-334``),
+and for the lagged friction kinds, functions of ``x - x_old``, also the
+leaves of their step-start positions.  Mixed derivatives through the rest
+shapes of the other energies and through affine-body vertices are not
+built (a target among those leaves raises).
 """
 
 from __future__ import annotations
@@ -83,6 +84,20 @@ class _RectTerm:
   def n(self) -> int:
     return int(self.prim.numInstances)
 
+  @property
+  def difference_args(self) -> int:
+    """The lagged friction kinds are functions of x - x_old: their
+    step-start positions are arguments too (``ys_rect_records``'s
+    difference form); 0 for the other energies."""
+    e = self.expr
+    return int(e.arity) if e.kind == "vertex" and e.code in (8, 9, 10, 11) and e.rest is not None else 0
+
+  def rest_leaves(self):
+    """Leaves of the energy's rest / step-start argument (empty without one)."""
+    e = self.expr
+    rest = getattr(e, "rest", None)
+    return resolve_leaf_children(rest.source)[0] if rest is not None else []
+
   def arguments(self):
     """(connectivity [n, A] int32 into the leaf union, leaves, prefix, A)."""
     torch = _torch()
@@ -92,7 +107,21 @@ class _RectTerm:
       raise NotImplementedError("secondOrderJacobian: energies through affine-body vertices are not built")
     if e.kind in ("snh", "vertex"):
       leaves, prefix = resolve_leaf_children(e.position.source)
-      return e.position.through.value, leaves, prefix, 4 if e.kind == "snh" else e.arity
+      A = 4 if e.kind == "snh" else e.arity
+      if not self.difference_args:
+        return e.position.through.value, leaves, prefix, A
+      # [position arguments, step-start arguments] over the union of both
+      # leaf lists
+      rleaves, rprefix = resolve_leaf_children(e.rest.source)
+      if len(leaves) + len(rleaves) > 8:
+        raise NotImplementedError("secondOrderJacobian: more than 8 leaves in the position and step-start unions")
+      key = ("difference_conn", n)
+      if key not in self._cache:
+        c = e.position.through.value.reshape(-1)[:n * A].to(torch.int64).view(n, A) if n else \
+            torch.zeros((1, A), dtype=torch.int64, device=_dev())
+        self._cache[key] = torch.cat([c, c + int(prefix[-1])], dim=1).to(torch.int32).contiguous()
+      return (self._cache[key], list(leaves) + list(rleaves),
+              list(prefix[:-1]) + [int(prefix[-1]) + int(p) for p in rprefix], 2 * A)
     if e.kind == "inertia":
       leaves = [e.x, e.x_before] + ([e.vel] if e.vel is not None else [])
       key = ("inertia_conn", n, len(leaves))
@@ -233,14 +262,20 @@ class secondOrderJacobian:
     for src in sources:
       t = _RectTerm(src, self)
       n = t.n
+      diff = t.difference_args
+      if not diff:
+        rest = t.rest_leaves()
+        if any(any(x is r for r in rest) for x in self.__row_wrt + self.__column_wrt):
+          raise NotImplementedError("secondOrderJacobian: mixed derivatives through the rest argument of "
+                                    f"{type(t.expr).__name__} are not built")
       rc, K, stride, A = t.codes(self.__row_wrt, self.__row_start)
       cc, _, _, _ = t.codes(self.__column_wrt, self.__column_start)
       outer = torch.empty(n + 1, dtype=torch.int32, device=_dev())
       L.call("ys_rect_coordinates", L.ptr(rc), L.ptr(cc), n, K, stride, A, L.ptr(outer), None, None, s)
       m = int(outer[n].item()) if n else 0
-      N = 3 * A
+      N = 3 * (diff if diff else A)
       local_h = torch.empty(max(n * N * (N + 1) // 2, 1), dtype=torch.float64, device=_dev())
-      terms.append(dict(term=t, rc=rc, cc=cc, K=K, stride=stride, A=A, outer=outer, m=m, off=total,
+      terms.append(dict(term=t, rc=rc, cc=cc, K=K, stride=stride, A=A, diff=diff, outer=outer, m=m, off=total,
                         local_h=local_h))
       total += m
     coords = torch.empty(max(2 * total, 2), dtype=torch.int32, device=_dev())
@@ -286,8 +321,8 @@ class secondOrderJacobian:
         if t.n == 0 or d["m"] == 0:
           continue
         t.local_hessians(d["local_h"])
-        L.call("ys_rect_records", L.ptr(d["local_h"]), d["A"], L.ptr(d["rc"]), L.ptr(d["cc"]), t.n, d["K"],
-               d["stride"], L.ptr(d["outer"]), pat.record.data_ptr() + 4 * d["off"], L.ptr(part["records"]), s)
+        L.call("ys_rect_records", L.ptr(d["local_h"]), d["A"], d["diff"], L.ptr(d["rc"]), L.ptr(d["cc"]), t.n,
+               d["K"], d["stride"], L.ptr(d["outer"]), pat.record.data_ptr() + 4 * d["off"], L.ptr(part["records"]), s)
       if pat.num_unique:
         L.call("ys_assemble3", L.ptr(part["records"]), L.ptr(pat.record_begin), L.ptr(pat.record_count),
                L.ptr(pat.value_offset), pat.num_unique, L.ptr(part["values"]), None, s)
