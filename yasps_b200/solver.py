@@ -422,16 +422,18 @@ class masSolver(_PcgBase):
     norms = (L.f64 * 2)()
     target = tolerance if self.stop_rule == "residual" else np.sqrt(tolerance)
     total_its, refinements, status = 0, 0, -4
-    # x = 0, r = g (the refinement residual of the zero guess)
+    # the zero guess's residual is g itself (a device copy, so every inner
+    # solve reads r and keeps one cached graph); the first inner tolerance
+    # needs no norm (||r|| = ||g||), so the first synchronising residual
+    # read comes after the first inner solve
     x.zero_()
-    L.call("ys_refine_residual", ctypes.byref(m), L.ptr(rhs), None, None, L.ptr(r), L.ptr(work), norms,
-           L.stream_ptr())
-    gnorm = float(np.sqrt(norms[1]))
-    rnorm = float(np.sqrt(norms[0]))
-    if rnorm <= target * gnorm:
-      return 0, 0, 0
+    r.copy_(rhs)
+    gnorm = rnorm = None
     for _ in range(self.max_refinements):
-      inner_tol = max(self.refinement_tolerance, 0.5 * target * gnorm / max(rnorm, 1e-300))
+      if rnorm is None:
+        inner_tol = max(self.refinement_tolerance, 0.5 * target)
+      else:
+        inner_tol = max(self.refinement_tolerance, 0.5 * target * gnorm / max(rnorm, 1e-300))
       res = self._run_pcg(H, r, delta, True, L.YS_PREC_MAS, None, self._mas, min(inner_tol, 0.5),
                           max(1, max_iterations - total_its), True, "residual")
       total_its += int(res.iterations)
@@ -439,6 +441,7 @@ class masSolver(_PcgBase):
       L.call("ys_refine_residual", ctypes.byref(m), L.ptr(rhs), L.ptr(x), L.ptr(delta), L.ptr(r), L.ptr(work),
              norms, L.stream_ptr())
       rnorm = float(np.sqrt(norms[0]))
+      gnorm = float(np.sqrt(norms[1]))
       if rnorm <= target * gnorm:
         status = total_its
         break
