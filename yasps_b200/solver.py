@@ -259,7 +259,9 @@ class masSolver(_PcgBase):
 
   def __init__(self, max_domain_dofs=96, max_levels=6, target_nodes_per_partition=32, coarsest_level_weight=2.5,
                fine_level_weight=1.5, level_weights=None, global_coarse_domain=True, mixed_spmv=False,
-               stop_rule="preconditioned", refinement_tolerance=1e-3, max_refinements=8, **unused):
+               stop_rule="preconditioned", refinement_tolerance=1e-3, max_refinements=8,
+               adaptive_fine_level_weight=None, dense_collision_fine_level_weight=3.0,
+               dense_collision_block_ratio=0.1, **unused):
     """Options follow ``MASSolver`` (``PKG/solver/mas/solver.py:89-120``).
 
     Level weights default to the reference's device runtime
@@ -267,6 +269,11 @@ class masSolver(_PcgBase):
     the intermediate levels and ``coarsest_level_weight`` on the coarsest
     (``fine_level_weight=1.0`` gives the CPU reference's weights,
     ``mas/preconditioner.py:32-36``).  ``level_weights`` overrides both.
+    With a dynamic (contact) block set holding at least
+    ``dense_collision_block_ratio`` blocks per fine variable, the fine-level
+    weight is raised to ``dense_collision_fine_level_weight``
+    (``adaptive_fine_level_weight``, on by default unless ``level_weights``
+    is given; ``mas/solver.py:106-182``, ``mas/cuda_runtime.py:2716-2731``).
     """
     super().__init__(stop_rule)
     self.max_domain_dofs = int(max_domain_dofs)
@@ -277,6 +284,15 @@ class masSolver(_PcgBase):
     self.level_weights = None if level_weights is None else tuple(float(w) for w in level_weights)
     self.global_coarse_domain = bool(global_coarse_domain)
     self.mixed_spmv = bool(mixed_spmv)
+    self.adaptive_fine_level_weight = (level_weights is None if adaptive_fine_level_weight is None
+                                       else bool(adaptive_fine_level_weight))
+    if not (np.isfinite(dense_collision_fine_level_weight) and dense_collision_fine_level_weight > 0):
+      raise ValueError("dense collision fine-level weight must be positive")
+    if not (np.isfinite(dense_collision_block_ratio) and dense_collision_block_ratio > 0):
+      raise ValueError("dense collision block ratio must be positive")
+    self.dense_collision_fine_level_weight = float(dense_collision_fine_level_weight)
+    self.dense_collision_block_ratio = float(dense_collision_block_ratio)
+    self.active_fine_level_weight = None
     self.refinement_tolerance = float(refinement_tolerance)
     self.max_refinements = int(max_refinements)
     self.hierarchy = None
@@ -346,7 +362,11 @@ class masSolver(_PcgBase):
                      torch.zeros(9 * uniq.size, dtype=torch.float64, device=_dev()), int(uniq.size))
     t = mas_hierarchy.build_tables(self.hierarchy, pos)
     self._tables = t
-    weights = self.weights_for(len(self.hierarchy.levels))
+    weights = list(self.weights_for(len(self.hierarchy.levels)))
+    dynamic_blocks = 0 if dyn is None else int(dyn.pattern.num_unique)
+    if self.adaptive_fine_level_weight and dynamic_blocks / max(1, nv) >= self.dense_collision_block_ratio:
+      weights[0] = max(weights[0], self.dense_collision_fine_level_weight)
+    self.active_fine_level_weight = weights[0]
     dev = upload_mas_tables(t)
     dev.update(mas_numeric_buffers(t))
     h, keep = create_mas_handle(t, nv, weights, dev)
@@ -403,6 +423,7 @@ class masSolver(_PcgBase):
     self._statistics = {"solver": "mas", "converged": status >= 0, "iterations": its, "refinements": refinements,
                         "result": 0 if status >= 0 else -4, "solve_seconds": time.perf_counter() - t0,
                         "levels": len(self.hierarchy.levels), "domains_per_level": self.hierarchy.domains_per_level,
+                        "fine_level_weight": self.active_fine_level_weight,
                         "matrix_size": int(H.rows), "tolerance": float(tolerance)}
     return 0 if status >= 0 else -4
 
