@@ -111,3 +111,43 @@ def linear_quadratic_local(y, jac, offset, inner, linear, project=None):
   h = inner if project is None else project(inner)
   hess = np.broadcast_to(jac.T @ h @ jac, (y.shape[0], jac.shape[1], jac.shape[1])).copy()
   return energy, grad, hess
+
+
+def snh_hessian_with_rest(x, rest, mu, lam, dt):
+  """Hessians [T, 24, 24] of the Stable Neo-Hookean energy (``helpers.py:116-127``)
+  with respect to the tet's positions and its rest positions together
+  (``[x (12), X (12)]``, argument-major), by torch autograd over the same
+  expression (``FI = F^T IB`` with ``IB`` the inverse of the rest edge
+  matrix, ``vol`` from the rest edges).  The position-position block equals
+  :func:`snh_from_rest`'s Hessian."""
+  import torch
+  from torch.func import hessian, vmap
+  x = torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, 12)))
+  r = torch.from_numpy(np.ascontiguousarray(np.asarray(rest, dtype=np.float64).reshape(-1, 12)))
+  t = x.shape[0]
+  mu = torch.from_numpy(np.broadcast_to(np.asarray(mu, dtype=np.float64), (t,)).copy())
+  lam = torch.from_numpy(np.broadcast_to(np.asarray(lam, dtype=np.float64), (t,)).copy())
+
+  def det3(a):
+    return (a[0, 0] * (a[1, 1] * a[2, 2] - a[1, 2] * a[2, 1]) - a[0, 1] * (a[1, 0] * a[2, 2] - a[1, 2] * a[2, 0])
+            + a[0, 2] * (a[1, 0] * a[2, 1] - a[1, 1] * a[2, 0]))
+
+  def inv3(a):
+    c = torch.stack([torch.linalg.cross(a[:, 1], a[:, 2]), torch.linalg.cross(a[:, 2], a[:, 0]),
+                     torch.linalg.cross(a[:, 0], a[:, 1])])   # rows: the inverse's rows times det
+    return c / det3(a)
+
+  def energy(z, m, l):
+    p, q = z[:12].reshape(4, 3), z[12:].reshape(4, 3)
+    dm = torch.stack([q[1] - q[0], q[2] - q[0], q[3] - q[0]], dim=1)   # columns: rest edges
+    ds = torch.stack([p[1] - p[0], p[2] - p[0], p[3] - p[0]], dim=1)
+    f = ds @ inv3(dm)
+    ic = (f * f).sum()
+    j = det3(f)
+    alpha = 1.0 + 0.75 * m / l
+    vol = det3(dm) / 6.0
+    return vol * (0.5 * m * (ic - 3.0) - 0.5 * m * torch.log(ic + 1.0) + 0.5 * l * (j - alpha) ** 2) * dt * dt
+
+  z = torch.cat([x, r], dim=1)
+  h = vmap(hessian(energy))(z, mu, lam).numpy()
+  return 0.5 * (h + np.transpose(h, (0, 2, 1)))

@@ -181,14 +181,23 @@ def test_friction_position_against_step_start_positions(kind):
   check(J, orj.dense(ext, rc, ccode, J.rows, J.cols), rc, ccode)
 
 
-def test_rest_shape_targets_are_refused():
-  """A mixed derivative through a rest shape (here the SNH rest positions)
-  is not built and raises instead of returning a zero matrix."""
-  cube = scenes.fem_cube(4, noise=0.01, seed=1)
+def test_snh_positions_against_rest_positions():
+  """Shape derivatives d2E/(dx dX) of the SNH tetrahedra (free positions
+  against free rest positions) against the oracle's autograd Hessian over
+  (x, X); rest against rest is not built and raises."""
+  from yasps_b200.graph import resolve_leaf_children
+  cube = scenes.fem_cube(5, noise=0.01, seed=1)
   sc, h = scenes.fem_scene(cube)
   snh = next(r.energy for r in sc.minimizer.requests if r.energy.expr.kind == "snh")
-  from yasps_b200.graph import resolve_leaf_children
-  rest_leaf = resolve_leaf_children(snh.expr.rest.source)[0][-1]  # the free vertices' rest positions
-  J = differentiator().diff2([snh], [h["free_position"]], [rest_leaf])
+  free_rest = resolve_leaf_children(snh.expr.rest.source)[0][-1]  # the free vertices' rest positions
+  J = differentiator().diff2([snh], [h["free_position"]], [free_rest]).compute()
+  tets = cube.tets.astype(np.int64)
+  hl = oe.snh_hessian_with_rest(cube.positions_all()[tets], cube.rest_all()[tets], cube.mu, cube.lam, cube.dt)
+  npin = cube.pinned_count
+  free_code = np.where(tets >= npin, 2 + 3 * (tets - npin), 0)
+  zero = np.zeros_like(free_code)
+  rc = np.concatenate([free_code, zero], axis=1)
+  ccode = np.concatenate([zero, free_code], axis=1)
+  check(J, orj.dense(hl, rc, ccode, J.rows, J.cols), rc, ccode)
   with pytest.raises(NotImplementedError):
-    J.compute()
+    differentiator().diff2([snh], [free_rest], [h["free_position"], free_rest]).compute()

@@ -21,3 +21,26 @@ def test_inertia_blocks_and_merging():
   # x_before and v both mapped to one column target: the blocks add up
   cboth = np.stack([0 * i, 2 + 3 * i, 2 + 3 * i], axis=1)
   assert np.allclose(orj.dense(loc, rc, cboth, 6, 6), np.kron(np.diag(-m * (1 + dt)), np.eye(3)))
+
+
+def test_snh_hessian_with_rest_matches_the_position_hessian():
+  """The (x, X) Hessian's position block is the SNH oracle's Hessian, and its
+  position-rest block is the derivative of the oracle gradient in X
+  (central differences of the closed-form gradient, 1e-6)."""
+  from oracle import energies as oe
+  from yasps_b200 import scenes
+  cube = scenes.fem_cube(3, noise=0.01, seed=2)
+  tets = cube.tets.astype(np.int64)[:5]
+  x, X = cube.positions_all()[tets], cube.rest_all()[tets]
+  h = oe.snh_hessian_with_rest(x, X, cube.mu, cube.lam, cube.dt)
+  _, g, hxx = oe.snh_from_rest(x, X, cube.mu, cube.lam, cube.dt)
+  assert np.abs(h[:, :12, :12] - hxx).max() <= 1e-12 * np.abs(hxx).max()
+  eps = 1e-6
+  for k in range(12):
+    Xp, Xm = X.reshape(-1, 12).copy(), X.reshape(-1, 12).copy()
+    Xp[:, k] += eps
+    Xm[:, k] -= eps
+    gp = oe.snh_from_rest(x, Xp.reshape(-1, 4, 3), cube.mu, cube.lam, cube.dt)[1]
+    gm = oe.snh_from_rest(x, Xm.reshape(-1, 4, 3), cube.mu, cube.lam, cube.dt)[1]
+    fd = (gp - gm) / (2 * eps)
+    assert np.abs(h[:, :12, 12 + k] - fd).max() <= 1e-6 * np.abs(h[:, :12, 12:]).max()

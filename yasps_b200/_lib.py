@@ -135,6 +135,7 @@ SIGNATURES = {
     "ys_energy_eval": (i32, [P(EnergyArgs), vp]),
     "ys_local_hessians": (i32, [P(EnergyArgs), vp, vp]),
     "ys_snh_local_hessians": (i32, [P(SnhArgs), vp, vp]),
+    "ys_snh_rest_local_hessians": (i32, [P(SnhArgs), vp, vp]),
     "ys_inertia_local_hessians": (i32, [vp, f64, f64, u32, u32, vp, vp]),
     "ys_rect_coordinates": (i32, [vp, vp, u32, u32, u32, u32, vp, vp, vp, vp]),
     "ys_rect_records": (i32, [vp, u32, u32, vp, vp, u32, u32, u32, vp, vp, vp, vp]),

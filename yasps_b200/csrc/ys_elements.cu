@@ -422,6 +422,157 @@ __global__ void __launch_bounds__(128) snh_local_hessian_kernel(const ys_snh_arg
     }
 }
 
+// ---- SNH with respect to the rest positions too ----------------------------
+// The position gradient s (c1 F G_k + c3 cof G_k) of the same SNH formulas,
+// differentiated in the rest positions of one vertex at a time by a
+// first-order dual number over its 3 coordinates (the current positions held
+// constant): the position-rest block d(dE/dx)/dX of the tet's Hessian.
+struct D3 {
+  double v, d[3];
+};
+__device__ __forceinline__ D3 d3c(double c) { return D3{c, {0.0, 0.0, 0.0}}; }
+__device__ __forceinline__ D3 operator+(const D3& a, const D3& b) {
+  return D3{a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2]}};
+}
+__device__ __forceinline__ D3 operator-(const D3& a, const D3& b) {
+  return D3{a.v - b.v, {a.d[0] - b.d[0], a.d[1] - b.d[1], a.d[2] - b.d[2]}};
+}
+__device__ __forceinline__ D3 operator*(const D3& a, const D3& b) {
+  return D3{a.v * b.v, {a.d[0] * b.v + a.v * b.d[0], a.d[1] * b.v + a.v * b.d[1], a.d[2] * b.v + a.v * b.d[2]}};
+}
+__device__ __forceinline__ D3 operator*(double s, const D3& a) { return D3{s * a.v, {s * a.d[0], s * a.d[1], s * a.d[2]}}; }
+__device__ __forceinline__ D3 d3_recip(const D3& a) {
+  const double i = 1.0 / a.v, di = -i * i;
+  return D3{i, {di * a.d[0], di * a.d[1], di * a.d[2]}};
+}
+
+// x-X block (12 x 3) of rest vertex `va`: out[3k + c][m] = d(dE/dx_kc)/dX_va,m.
+__device__ void snh_rest_column(const double (&x)[4][3], const double (&X)[4][3], int va, double mu, double lam,
+                                double dt, double (&out)[12][3]) {
+  D3 P[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      P[k][c] = d3c(X[k][c]);
+      if (k == va) P[k][c].d[c] = 1.0;
+    }
+  D3 e[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e[k][c] = P[k + 1][c] - P[0][c];
+  auto crossc = [&](const D3 (&a)[3], const D3 (&b)[3], D3 (&o)[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  D3 k0[3], k1[3], k2[3];
+  crossc(e[1], e[2], k0);
+  crossc(e[2], e[0], k1);
+  crossc(e[0], e[1], k2);
+  const D3 det = e[0][0] * k0[0] + e[0][1] * k0[1] + e[0][2] * k0[2];
+  const D3 inv = d3_recip(det);
+  D3 G[4][3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    G[1][j] = k0[j] * inv;
+    G[2][j] = k1[j] * inv;
+    G[3][j] = k2[j] * inv;
+    G[0][j] = -1.0 * (G[1][j] + G[2][j] + G[3][j]);
+  }
+  D3 F[3][3];  // columns f_j
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      D3 acc = x[0][c] * G[0][j];
+#pragma unroll
+      for (int k = 1; k < 4; ++k) acc = acc + x[k][c] * G[k][j];
+      F[j][c] = acc;
+    }
+  D3 C[3][3];
+  crossc(F[1], F[2], C[0]);
+  crossc(F[2], F[0], C[1]);
+  crossc(F[0], F[1], C[2]);
+  D3 ic = d3c(0.0);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ic = ic + F[j][c] * F[j][c];
+  const D3 J = F[0][0] * C[0][0] + F[0][1] * C[0][1] + F[0][2] * C[0][2];
+  const double alpha = 1.0 + 0.75 * mu / lam;
+  const D3 s = (dt * dt / 6.0) * det;
+  const D3 c1 = mu * (d3c(1.0) - d3_recip(ic + d3c(1.0)));
+  const D3 c3 = lam * (J - d3c(alpha));
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      D3 pf = G[k][0] * F[0][c], pc = G[k][0] * C[0][c];
+#pragma unroll
+      for (int j = 1; j < 3; ++j) {
+        pf = pf + G[k][j] * F[j][c];
+        pc = pc + G[k][j] * C[j][c];
+      }
+      const D3 gx = s * (c1 * pf + c3 * pc);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) out[3 * k + c][m] = gx.d[m];
+    }
+}
+
+// Packed upper 24x24 Hessian over (x, X) of one tet: the x-x block from the
+// SNH blocks, the x-X block by differentiation in X; the X-X block is left
+// zero (rest-rest products are not built: the caller never reads them).
+__global__ void __launch_bounds__(64) snh_rest_local_hessian_kernel(const ys_snh_args a, double* out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  double* dst = out + (uint64_t)t * 300;
+  {
+    SnhState st;
+    snh_state(a, t, st);
+    V3 u[4], v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      u[k] = mul(st.f, st.g[k]);
+      v[k] = mul(st.cof, st.g[k]);
+    }
+#pragma unroll
+    for (int ai = 0; ai < 4; ++ai)
+#pragma unroll
+      for (int bi = ai; bi < 4; ++bi) {
+        double blk[3][3];
+        hess_block(st, st.g[ai], st.g[bi], u[ai], u[bi], v[ai], v[bi], blk);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int l = 0; l < 3; ++l)
+            if (3 * ai + k <= 3 * bi + l) dst[utri<24>(3 * ai + k, 3 * bi + l)] = blk[k][l];
+      }
+  }
+  for (int i = 12; i < 24; ++i)
+    for (int j = i; j < 24; ++j) dst[utri<24>(i, j)] = 0.0;
+  const uint4 tv = reinterpret_cast<const uint4*>(a.tets)[t];
+  const uint32_t id[4] = {tv.x, tv.y, tv.z, tv.w};
+  double x[4][3], X[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const V3 p = load3(a.position, id[k]), r = load3(a.rest, id[k]);
+    x[k][0] = p.x; x[k][1] = p.y; x[k][2] = p.z;
+    X[k][0] = r.x; X[k][1] = r.y; X[k][2] = r.z;
+  }
+  const double mu = a.mu ? a.mu[t] : a.mu_value;
+  const double lam = a.lam ? a.lam[t] : a.lam_value;
+#pragma unroll 1
+  for (int va = 0; va < 4; ++va) {
+    double col[12][3];
+    snh_rest_column(x, X, va, mu, lam, a.dt, col);
+    for (int i = 0; i < 12; ++i)
+#pragma unroll
+      for (int m = 0; m < 3; ++m) dst[utri<24>(i, 12 + 3 * va + m)] = col[i][m];
+  }
+}
+
 // Local Hessian of the inertia term 1/2 m |x - x_before - dt v - dt^2 g|^2
 // over its arguments (x, x_before[, v]), packed upper: m [[I, -I, -dt I],
 // [-I, I, dt I], [-dt I, dt I, dt^2 I]] (helpers.py:138-141).
@@ -538,6 +689,15 @@ extern "C" int32_t ys_inertia_local_hessians(const double* mass, double mass_val
   if (n == 0) return YS_OK;
   ys::inertia_local_hessian_kernel<<<ys::grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(mass, mass_value, dt, n,
                                                                                            (int)args, out);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+extern "C" int32_t ys_snh_rest_local_hessians(const ys_snh_args* args, double* out, void* stream) {
+  YS_REQUIRE(args != nullptr && out != nullptr, YS_ERR_INVALID, "null argument");
+  const ys_snh_args& a = *args;
+  if (a.num_elements == 0) return YS_OK;
+  ys::snh_rest_local_hessian_kernel<<<ys::grid_for(a.num_elements, 64), 64, 0, (cudaStream_t)stream>>>(a, out);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

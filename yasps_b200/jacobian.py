@@ -26,10 +26,12 @@ blocks), for the inertia term its ``x``, ``x_before`` and ``vel``
 attributes (the adjoint blocks ``d2E / (dx dx_before)`` and
 ``d2E / (dx dvel)`` of the reference's differentiable-simulation examples,
 ``examples/bunny_dropping_on_ground/bunny_dropping_on_ground.py:333-334``),
-and for the lagged friction kinds, functions of ``x - x_old``, also the
-leaves of their step-start positions.  Mixed derivatives through the rest
-shapes of the other energies and through affine-body vertices are not
-built (a target among those leaves raises).
+for the lagged friction kinds, functions of ``x - x_old``, also the
+leaves of their step-start positions, and for the SNH tetrahedra the
+leaves of their rest positions against the position leaves (shape
+derivatives ``d2E / (dx dX)``).  Mixed derivatives through the rest shapes
+of the other energies, rest against rest, and through affine-body vertices
+are not built (a target among those leaves raises).
 """
 
 from __future__ import annotations
@@ -92,6 +94,12 @@ class _RectTerm:
     e = self.expr
     return int(e.arity) if e.kind == "vertex" and e.code in (8, 9, 10, 11) and e.rest is not None else 0
 
+  @property
+  def rest_form(self) -> bool:
+    """SNH with a target among its rest leaves: the arguments are the tet's
+    positions and rest positions (``ys_snh_rest_local_hessians``)."""
+    return getattr(self, "_rest_form", False)
+
   def rest_leaves(self):
     """Leaves of the energy's rest / step-start argument (empty without one)."""
     e = self.expr
@@ -108,10 +116,10 @@ class _RectTerm:
     if e.kind in ("snh", "vertex"):
       leaves, prefix = resolve_leaf_children(e.position.source)
       A = 4 if e.kind == "snh" else e.arity
-      if not self.difference_args:
+      if not self.difference_args and not self.rest_form:
         return e.position.through.value, leaves, prefix, A
-      # [position arguments, step-start arguments] over the union of both
-      # leaf lists
+      # [position arguments, step-start (or rest) arguments] over the union
+      # of both leaf lists
       rleaves, rprefix = resolve_leaf_children(e.rest.source)
       if len(leaves) + len(rleaves) > 8:
         raise NotImplementedError("secondOrderJacobian: more than 8 leaves in the position and step-start unions")
@@ -170,6 +178,7 @@ class _RectTerm:
     helper = _Term(energyRequest(self.energy, [], -1, False), [], [0])
     if e.kind == "snh":
       a = L.SnhArgs()
+      entry = "ys_snh_rest_local_hessians" if self.rest_form else "ys_snh_local_hessians"
       a.position = helper._union3(e.position.source)
       a.rest = helper._union3(e.rest.source)
       a.tets = L.ptr(e.position.through.value)
@@ -178,7 +187,7 @@ class _RectTerm:
       lam_arr, a.lam_value = helper._param(e.lam_p, n)
       a.mu, a.lam = L.ptr(mu_arr), L.ptr(lam_arr)
       a.dt = helper._param(e.dt_p, n)[1]
-      L.call("ys_snh_local_hessians", ctypes.byref(a), L.ptr(out), s)
+      L.call(entry, ctypes.byref(a), L.ptr(out), s)
       return
     a = L.EnergyArgs()
     a.kind = e.code
@@ -265,15 +274,19 @@ class secondOrderJacobian:
       diff = t.difference_args
       if not diff:
         rest = t.rest_leaves()
-        if any(any(x is r for r in rest) for x in self.__row_wrt + self.__column_wrt):
+        in_rows = any(any(x is r for r in rest) for x in self.__row_wrt)
+        in_cols = any(any(x is r for r in rest) for x in self.__column_wrt)
+        if (in_rows or in_cols) and (t.expr.kind != "snh" or (in_rows and in_cols)):
           raise NotImplementedError("secondOrderJacobian: mixed derivatives through the rest argument of "
-                                    f"{type(t.expr).__name__} are not built")
+                                    f"{type(t.expr).__name__} are not built"
+                                    + (" (rest against rest)" if t.expr.kind == "snh" else ""))
+        t._rest_form = in_rows or in_cols
       rc, K, stride, A = t.codes(self.__row_wrt, self.__row_start)
       cc, _, _, _ = t.codes(self.__column_wrt, self.__column_start)
       outer = torch.empty(n + 1, dtype=torch.int32, device=_dev())
       L.call("ys_rect_coordinates", L.ptr(rc), L.ptr(cc), n, K, stride, A, L.ptr(outer), None, None, s)
       m = int(outer[n].item()) if n else 0
-      N = 3 * (diff if diff else A)
+      N = 3 * (diff if diff else A)  # the rest form's local Hessian covers all 8 arguments
       local_h = torch.empty(max(n * N * (N + 1) // 2, 1), dtype=torch.float64, device=_dev())
       terms.append(dict(term=t, rc=rc, cc=cc, K=K, stride=stride, A=A, diff=diff, outer=outer, m=m, off=total,
                         local_h=local_h))
