@@ -307,20 +307,42 @@ int32_t ys_rect_records(const double* local_hessians, uint32_t args, uint32_t di
                         uint32_t slot_stride, const uint32_t* coord_outer, const uint32_t* record, double* records,
                         void* stream);
 
-/* Products with the assembled rectangular matrix (unique 3x3 blocks sorted
- * by (row, col), scalar positions).  ys_rect_plan builds row_ptr
- * [block_rows + 1], col_ptr [block_cols + 1] and col_order [num_blocks]
- * (blocks by column, stable); ys_rect_spmv computes y = J x (transpose 0,
- * y of 3 block_rows) or y = J^T x (transpose 1, y of 3 block_cols), each
- * output row summed in block order.  Replaces matrix.spmv of
- * secondOrderJacobian (PKG/matrixAndVector/matrix/matrix.pyx).            */
+/* Material-parameter columns (the reference's diff2(E, [position], [young])
+ * of its material-optimization examples): the derivative of an element's
+ * position gradient in one of its own scalar parameters, per argument,
+ * [n x 3 args] doubles.  SNH: which 0 mu, 1 lambda (the per-tet Lame
+ * arrays of ys_snh_args); inertia: the vertex mass over its 2 or 3
+ * arguments (x, x_before[, v]).                                            */
+int32_t ys_snh_param_jacobian(const ys_snh_args* args, uint32_t which, double* out, void* stream);
+int32_t ys_inertia_mass_jacobian(const ys_inertia_args* args, uint32_t arguments, double* out, void* stream);
+/* Coordinates and records of the parameter columns: one (3 x 1) pair per
+ * distinct row code of element t and column param_start + t (coord_outer
+ * alone when coords is NULL, as ys_rect_coordinates); records are the sums
+ * of the pair's argument derivatives, 3 doubles at record[coord_outer[t] + k]. */
+int32_t ys_rect_param_coordinates(const uint32_t* row_codes, uint32_t n, uint32_t K, uint32_t slot_stride,
+                                  uint32_t args, uint32_t param_start, uint32_t* coord_outer, uint32_t* coords,
+                                  uint16_t* dims, void* stream);
+int32_t ys_rect_param_records(const double* derivatives, uint32_t args, const uint32_t* row_codes, uint32_t n,
+                              uint32_t K, uint32_t slot_stride, const uint32_t* coord_outer, const uint32_t* record,
+                              double* records, void* stream);
+
+/* Products with one category of the assembled rectangular matrix (unique
+ * blocks of 3 rows and col_width = 1 or 3 columns, sorted by (row, col),
+ * scalar positions, 3 col_width values a block).  ys_rect_plan builds
+ * row_ptr [block_rows + 1], col_ptr [block_cols + 1] (block_cols column
+ * units of col_width) and col_order [num_blocks] (blocks by column, stable);
+ * ys_rect_spmv computes y = J x (transpose 0, 3 block_rows outputs) or
+ * y = J^T x (transpose 1, col_width block_cols outputs), each output summed
+ * in block order, written (accumulate 0) or added (1).  Replaces matrix.spmv
+ * of secondOrderJacobian (PKG/matrixAndVector/matrix/matrix.pyx).         */
 int32_t ys_rect_plan_workspace_bytes(uint32_t num_blocks, uint64_t* bytes);
 int32_t ys_rect_plan(const uint32_t* positions, uint32_t num_blocks, uint32_t block_rows, uint32_t block_cols,
-                     uint32_t* row_ptr, uint32_t* col_ptr, uint32_t* col_order, void* workspace,
+                     uint32_t col_width, uint32_t* row_ptr, uint32_t* col_ptr, uint32_t* col_order, void* workspace,
                      uint64_t workspace_bytes, void* stream);
 int32_t ys_rect_spmv(const double* values, const uint32_t* positions, const uint32_t* row_ptr,
                      const uint32_t* col_ptr, const uint32_t* col_order, uint32_t block_rows, uint32_t block_cols,
-                     const double* x, double* y, uint32_t transpose, void* stream);
+                     uint32_t col_width, const double* x, double* y, uint32_t transpose, uint32_t accumulate,
+                     void* stream);
 
 /* ---- affine (ABD) bodies ------------------------------------------------
  * A body carries a 3x3 affine matrix A (9 DoF, row-major, the reference's

@@ -151,3 +151,33 @@ def snh_hessian_with_rest(x, rest, mu, lam, dt):
   z = torch.cat([x, r], dim=1)
   h = vmap(hessian(energy))(z, mu, lam).numpy()
   return 0.5 * (h + np.transpose(h, (0, 2, 1)))
+
+
+def snh_parameter_jacobian(x, rest, mu, lam, dt, which):
+  """d(dE/dx)/d mu (``which`` 0) or d(dE/dx)/d lambda (1) of the Stable
+  Neo-Hookean energy per tet, [T, 12], by torch autograd (forward over
+  reverse) of the same expression as :func:`snh_hessian_with_rest`."""
+  import torch
+  from torch.func import grad, jacfwd, vmap
+  x = torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, 12)))
+  r = torch.from_numpy(np.ascontiguousarray(np.asarray(rest, dtype=np.float64).reshape(-1, 12)))
+  t = x.shape[0]
+  mu = torch.from_numpy(np.broadcast_to(np.asarray(mu, dtype=np.float64), (t,)).copy())
+  lam = torch.from_numpy(np.broadcast_to(np.asarray(lam, dtype=np.float64), (t,)).copy())
+
+  def energy(p12, q12, m, l):
+    p, q = p12.reshape(4, 3), q12.reshape(4, 3)
+    dm = torch.stack([q[1] - q[0], q[2] - q[0], q[3] - q[0]], dim=1)
+    ds = torch.stack([p[1] - p[0], p[2] - p[0], p[3] - p[0]], dim=1)
+    ib = torch.stack([torch.linalg.cross(dm[:, 1], dm[:, 2]), torch.linalg.cross(dm[:, 2], dm[:, 0]),
+                      torch.linalg.cross(dm[:, 0], dm[:, 1])])
+    det = (dm[:, 0] * ib[0]).sum()
+    f = ds @ (ib / det)
+    ic = (f * f).sum()
+    j = (f[:, 0] * torch.linalg.cross(f[:, 1], f[:, 2])).sum()
+    alpha = 1.0 + 0.75 * m / l
+    return det / 6.0 * (0.5 * m * (ic - 3.0) - 0.5 * m * torch.log(ic + 1.0) + 0.5 * l * (j - alpha) ** 2) * dt * dt
+
+  argnum = 2 if which == 0 else 3
+  d = vmap(jacfwd(grad(energy, argnums=0), argnums=argnum))(x, r, mu, lam)
+  return d.numpy()

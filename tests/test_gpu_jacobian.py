@@ -21,11 +21,18 @@ pytestmark = pytest.mark.gpu
 
 
 def device_dense(J):
+  """Dense matrix from the block attributes (categories of (h, w) blocks)."""
   pos = J.block_positions.cpu().numpy().astype(np.int64).reshape(-1, 2)
-  vals = J.blocks_flattened.cpu().numpy().reshape(-1, 3, 3)
+  vals = J.blocks_flattened.cpu().numpy()
   D = np.zeros((J.rows, J.cols))
-  for (r, c), b in zip(pos, vals):
-    D[r:r + 3, c:c + 3] += b
+  b = 0
+  for g, cnt in enumerate(J.block_counts):
+    h, w = J.block_dimensions[2 * g:2 * g + 2]
+    start = J.blocks_start_indices[g]
+    for k in range(cnt):
+      r, c = pos[b + k]
+      D[r:r + h, c:c + w] += vals[start + k * h * w:start + (k + 1) * h * w].reshape(h, w)
+    b += cnt
   return D, pos
 
 
@@ -36,7 +43,8 @@ def expected_positions(row_codes, col_codes):
 
 def check(J, D_oracle, row_codes, col_codes):
   D, pos = device_dense(J)
-  assert np.array_equal(pos, expected_positions(row_codes, col_codes))
+  if row_codes is not None:
+    assert np.array_equal(pos, expected_positions(row_codes, col_codes))
   scale = np.abs(D_oracle).max()
   assert np.abs(D - D_oracle).max() <= 1e-12 * scale
   rng = np.random.default_rng(0)
@@ -201,3 +209,87 @@ def test_snh_positions_against_rest_positions():
   check(J, orj.dense(hl, rc, ccode, J.rows, J.cols), rc, ccode)
   with pytest.raises(NotImplementedError):
     differentiator().diff2([snh], [free_rest], [h["free_position"], free_rest]).compute()
+
+
+def material_scene(side=5):
+  """A FEM cube whose tets carry their own Lame parameters (per-tet
+  attributes), as the reference's material-optimization examples."""
+  from yasps_b200.energies import inertia, stable_neo_hookean
+  from yasps_b200.scene import scene as make_scene
+  cube = scenes.fem_cube(side, noise=0.01, seed=6)
+  rng = np.random.default_rng(1)
+  sc = make_scene("material")
+  body = sc.addMesh("body")
+  pinned = body.addPrimitive("pinned", numInstances=cube.pinned_count)
+  pp = pinned.addAttribute("position", rows=3, cols=1)
+  pp.updateValue(cube.positions_all()[:cube.pinned_count])
+  pr = pinned.addConstant("rest_position", rows=3, cols=1)
+  pr.updateValue(cube.rest_all()[:cube.pinned_count])
+  free = body.addPrimitive("free", numInstances=cube.free_count)
+  fp = free.addAttribute("position", rows=3, cols=1)
+  fp.updateValue(cube.free_position)
+  fr = free.addConstant("rest_position", rows=3, cols=1)
+  fr.updateValue(cube.rest_all()[cube.pinned_count:])
+  last = free.addConstant("last_position", rows=3, cols=1)
+  last.updateValue(cube.free_position + rng.uniform(-1e-3, 1e-3, size=cube.free_position.shape))
+  vel = free.addConstant("velocity", rows=3, cols=1)
+  vel.updateValue(rng.uniform(-0.1, 0.1, size=cube.free_position.shape))
+  mass = free.addConstant("mass")
+  mass.updateValue(cube.mass)
+  verts = body.addPrimitiveUnion("vertices", [pinned, free])
+  tets = body.addPrimitive("tetrahedra", numInstances=cube.tet_count)
+  conn = tets.addConnectivity("to_vertices", verts, cube.tets.astype(np.uint32), 4)
+  mu = tets.addConstant("mu")
+  mu.updateValue(cube.mu * rng.uniform(0.5, 1.5, size=cube.tet_count))
+  lam = tets.addConstant("lam")
+  lam.updateValue(cube.lam * rng.uniform(0.5, 1.5, size=cube.tet_count))
+  snh = tets.addAttribute("snh", computed_attribute=stable_neo_hookean(
+      tets.addAttribute("rest", through=conn, source=verts.addAttribute("rest_position")),
+      tets.addAttribute("x", through=conn, source=verts.addAttribute("position")), mu, lam, cube.dt))
+  kin = free.addAttribute("inertia", computed_attribute=inertia(last, vel, cube.dt, fp, mass,
+                                                                gravity=(0.0, 0.0, -9.8)))
+  return cube, dict(snh=snh, inertia=kin, position=fp, mu=mu, lam=lam, mass=mass, last=last, vel=vel)
+
+
+@pytest.mark.parametrize("which", ["mu", "lam"])
+def test_snh_material_parameter_columns(which):
+  """d2E/(dx d mu) and d2E/(dx d lambda) of SNH tets with per-tet Lame
+  parameters (the reference's diff2(elastic, [position], [young]) of its
+  material-optimization examples, here on the Lame arrays): (3 x 1) blocks
+  against the oracle's autograd derivatives, and the products."""
+  import torch
+  cube, h = material_scene()
+  J = differentiator().diff2([h["snh"]], [h["position"]], [h[which]]).compute()
+  assert J.block_dimensions == [3, 1]
+  tets = cube.tets.astype(np.int64)
+  d = oe.snh_parameter_jacobian(cube.positions_all()[tets], cube.rest_all()[tets],
+                                h["mu"].host_value.reshape(-1), h["lam"].host_value.reshape(-1), cube.dt,
+                                0 if which == "mu" else 1)
+  npin = cube.pinned_count
+  D = np.zeros((J.rows, J.cols))
+  for t in range(len(tets)):
+    for a in range(4):
+      if tets[t, a] >= npin:
+        v = tets[t, a] - npin
+        D[3 * v:3 * v + 3, t] += d[t, 3 * a:3 * a + 3]
+  check(J, D, None, None)
+
+
+def test_inertia_mass_column_beside_a_position_column():
+  """d2E/(dx dm) of the inertia term (x - x~ per vertex, a (3 x 1) block)
+  beside d2E/(dx dx_before) (-m I, 3 x 3) in one Jacobian: two block
+  categories, the scalar columns first, products over both."""
+  cube, h = material_scene()
+  J = differentiator().diff2([h["inertia"]], [h["position"]], [h["mass"], h["last"]]).compute()
+  assert J.block_dimensions == [3, 1, 3, 3]
+  x = cube.free_position
+  last = h["last"].host_value.reshape(-1, 3)
+  vel = h["vel"].host_value.reshape(-1, 3)
+  dt = cube.dt
+  xt = last + vel * dt + np.array([0.0, 0.0, -9.8]) * dt * dt
+  nf = cube.free_count
+  D = np.zeros((J.rows, J.cols))
+  for v in range(nf):
+    D[3 * v:3 * v + 3, v] = x[v] - xt[v]
+    D[3 * v:3 * v + 3, nf + 3 * v:nf + 3 * v + 3] = -cube.mass[v] * np.eye(3)
+  check(J, D, None, None)

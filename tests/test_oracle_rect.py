@@ -44,3 +44,21 @@ def test_snh_hessian_with_rest_matches_the_position_hessian():
     gm = oe.snh_from_rest(x, Xm.reshape(-1, 4, 3), cube.mu, cube.lam, cube.dt)[1]
     fd = (gp - gm) / (2 * eps)
     assert np.abs(h[:, :12, 12 + k] - fd).max() <= 1e-6 * np.abs(h[:, :12, 12:]).max()
+
+
+def test_snh_parameter_jacobian_matches_differences():
+  """The oracle's d(dE/dx)/d mu and d(dE/dx)/d lambda against central
+  differences of the closed-form SNH gradient (1e-6)."""
+  from oracle import energies as oe
+  from yasps_b200 import scenes
+  cube = scenes.fem_cube(3, noise=0.01, seed=2)
+  tets = cube.tets.astype(np.int64)[:6]
+  x, X = cube.positions_all()[tets], cube.rest_all()[tets]
+  for which in (0, 1):
+    d = oe.snh_parameter_jacobian(x, X, cube.mu, cube.lam, cube.dt, which)
+    h = 1e-6 * (cube.mu if which == 0 else cube.lam)
+    args = lambda s: (cube.mu + s, cube.lam) if which == 0 else (cube.mu, cube.lam + s)
+    gp = oe.snh_from_rest(x, X, *args(h), cube.dt)[1]
+    gm = oe.snh_from_rest(x, X, *args(-h), cube.dt)[1]
+    fd = (gp - gm) / (2 * h)
+    assert np.abs(d - fd).max() <= 1e-6 * np.abs(d).max()

@@ -140,8 +140,12 @@ SIGNATURES = {
     "ys_rect_coordinates": (i32, [vp, vp, u32, u32, u32, u32, vp, vp, vp, vp]),
     "ys_rect_records": (i32, [vp, u32, u32, vp, vp, u32, u32, u32, vp, vp, vp, vp]),
     "ys_rect_plan_workspace_bytes": (i32, [u32, P(u64)]),
-    "ys_rect_plan": (i32, [vp, u32, u32, u32, vp, vp, vp, vp, u64, vp]),
-    "ys_rect_spmv": (i32, [vp, vp, vp, vp, vp, u32, u32, vp, vp, u32, vp]),
+    "ys_rect_plan": (i32, [vp, u32, u32, u32, u32, vp, vp, vp, vp, u64, vp]),
+    "ys_rect_spmv": (i32, [vp, vp, vp, vp, vp, u32, u32, u32, vp, vp, u32, u32, vp]),
+    "ys_snh_param_jacobian": (i32, [P(SnhArgs), u32, vp, vp]),
+    "ys_inertia_mass_jacobian": (i32, [P(InertiaArgs), u32, vp, vp]),
+    "ys_rect_param_coordinates": (i32, [vp, u32, u32, u32, u32, u32, vp, vp, vp, vp]),
+    "ys_rect_param_records": (i32, [vp, u32, vp, u32, u32, u32, vp, vp, vp, vp]),
     "ys_affine_eval": (i32, [P(AffineArgs), vp]),
     "ys_coupled_indices": (i32, [vp, u32, u32, u32, P(u32), P(i32), P(u32), u32, vp, u32, i32, u32, i32, u32, vp, vp,
                                  vp]),

@@ -573,6 +573,46 @@ __global__ void __launch_bounds__(64) snh_rest_local_hessian_kernel(const ys_snh
   }
 }
 
+// Derivative of the SNH position gradient s (c1 F G_k + c3 cof G_k) in a
+// per-tet material parameter (which 0: mu, with dc1/dmu = 1 - 1/(IC+1) and
+// dc3/dmu = -3/4 through alpha; 1: lambda, with dc3/dlam = J - 1):
+// out[12 t + 3 k + c].
+__global__ void snh_param_jacobian_kernel(const ys_snh_args a, int which, double* out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  SnhState st;
+  snh_state(a, t, st);
+  const double ic = dot(st.f.c[0], st.f.c[0]) + dot(st.f.c[1], st.f.c[1]) + dot(st.f.c[2], st.f.c[2]);
+  const double J = dot(st.f.c[0], st.cof.c[0]);
+  const double d1 = which == 0 ? 1.0 - 1.0 / (ic + 1.0) : 0.0;
+  const double d3 = which == 0 ? -0.75 : J - 1.0;
+  double* dst = out + 12ull * t;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const V3 gk = st.s * (d1 * mul(st.f, st.g[k]) + d3 * mul(st.cof, st.g[k]));
+    dst[3 * k] = gk.x;
+    dst[3 * k + 1] = gk.y;
+    dst[3 * k + 2] = gk.z;
+  }
+}
+
+// Derivative of the inertia gradient in the vertex's mass, per argument
+// (x, x_before[, v]): x - x~, -(x - x~), -dt (x - x~)  (out[3 args i + 3 a + k]).
+__global__ void inertia_mass_jacobian_kernel(const ys_inertia_args a, int args, double* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.num_vertices) return;
+  const double* x = a.position + 3ull * i;
+  const double* xb = a.x_before + 3ull * i;
+  const double h2 = a.dt * a.dt;
+  const double scale[3] = {1.0, -1.0, -a.dt};
+  double* dst = out + 3ull * args * i;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double d = x[k] - (xb[k] + (a.velocity ? a.velocity[3ull * i + k] * a.dt : 0.0) + a.gravity[k] * h2);
+    for (int q = 0; q < args; ++q) dst[3 * q + k] = scale[q] * d;
+  }
+}
+
 // Local Hessian of the inertia term 1/2 m |x - x_before - dt v - dt^2 g|^2
 // over its arguments (x, x_before[, v]), packed upper: m [[I, -I, -dt I],
 // [-I, I, dt I], [-dt I, dt I, dt^2 I]] (helpers.py:138-141).
@@ -698,6 +738,29 @@ extern "C" int32_t ys_snh_rest_local_hessians(const ys_snh_args* args, double* o
   const ys_snh_args& a = *args;
   if (a.num_elements == 0) return YS_OK;
   ys::snh_rest_local_hessian_kernel<<<ys::grid_for(a.num_elements, 64), 64, 0, (cudaStream_t)stream>>>(a, out);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+extern "C" int32_t ys_snh_param_jacobian(const ys_snh_args* args, uint32_t which, double* out, void* stream) {
+  YS_REQUIRE(args != nullptr && out != nullptr, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE(which <= 1, YS_ERR_INVALID, "which: 0 mu, 1 lambda");
+  const ys_snh_args& a = *args;
+  if (a.num_elements == 0) return YS_OK;
+  ys::snh_param_jacobian_kernel<<<ys::grid_for(a.num_elements, 128), 128, 0, (cudaStream_t)stream>>>(a, (int)which,
+                                                                                                   out);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+extern "C" int32_t ys_inertia_mass_jacobian(const ys_inertia_args* args, uint32_t arguments, double* out,
+                                            void* stream) {
+  YS_REQUIRE(args != nullptr && out != nullptr, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE(arguments == 2 || arguments == 3, YS_ERR_INVALID, "inertia has 2 or 3 arguments");
+  const ys_inertia_args& a = *args;
+  if (a.num_vertices == 0) return YS_OK;
+  ys::inertia_mass_jacobian_kernel<<<ys::grid_for(a.num_vertices, 256), 256, 0, (cudaStream_t)stream>>>(
+      a, (int)arguments, out);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

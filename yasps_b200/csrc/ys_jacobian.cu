@@ -124,6 +124,58 @@ __global__ void rect_records_kernel(const double* __restrict__ local_h, int args
     }
 }
 
+// Columns of a per-element scalar parameter (element t's column is
+// param_start + t): one (3 x 1) pair per row group of the element.
+__global__ void rect_param_count_kernel(const uint32_t* __restrict__ row_codes, uint32_t n, uint32_t K,
+                                        uint32_t stride, int args, uint32_t* __restrict__ count) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int group[kRectMaxArgs], first[kRectMaxArgs];
+  count[t] = (uint32_t)rect_groups(row_codes, t, K, stride, args, group, first);
+}
+
+__global__ void rect_param_coords_kernel(const uint32_t* __restrict__ row_codes, uint32_t n, uint32_t K,
+                                         uint32_t stride, int args, uint32_t param_start,
+                                         const uint32_t* __restrict__ outer, uint32_t* __restrict__ coords,
+                                         uint16_t* __restrict__ dims) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int group[kRectMaxArgs], first[kRectMaxArgs];
+  const int nr = rect_groups(row_codes, t, K, stride, args, group, first);
+  uint32_t o = outer[t];
+  for (int i = 0; i < nr; ++i, ++o) {
+    coords[2ull * o] = row_codes[(uint64_t)t * K + (uint64_t)first[i] * stride] - 2u;
+    coords[2ull * o + 1] = param_start + t;
+    dims[2ull * o] = 3;
+    dims[2ull * o + 1] = 1;
+  }
+}
+
+// Records (3 doubles) of the parameter pairs: per row group, the sum of its
+// arguments' derivatives d[t][3 a .. 3 a + 2].
+__global__ void rect_param_records_kernel(const double* __restrict__ d, int args,
+                                          const uint32_t* __restrict__ row_codes, uint32_t n, uint32_t K,
+                                          uint32_t stride, const uint32_t* __restrict__ outer,
+                                          const uint32_t* __restrict__ record, double* __restrict__ out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int group[kRectMaxArgs], first[kRectMaxArgs];
+  const int nr = rect_groups(row_codes, t, K, stride, args, group, first);
+  const double* src = d + 3ull * args * t;
+  uint32_t o = outer[t];
+  for (int i = 0; i < nr; ++i, ++o) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < args; ++a) {
+      if (group[a] != i) continue;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc[k] += src[3 * a + k];
+    }
+    double* dst = out + record[o];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dst[k] = acc[k];
+  }
+}
+
 // First block of every block row (rows sorted): row_ptr[r] = lower bound.
 __global__ void rect_row_ptr_kernel(const uint32_t* __restrict__ positions, uint32_t nb, uint32_t block_rows,
                                     uint32_t* __restrict__ row_ptr) {
@@ -151,39 +203,45 @@ __global__ void rect_col_ptr_kernel(const uint32_t* __restrict__ keys, uint32_t 
   col_ptr[c] = lo;
 }
 
-__global__ void rect_col_keys_kernel(const uint32_t* __restrict__ positions, uint32_t nb, uint32_t* __restrict__ keys,
-                                     uint32_t* __restrict__ vals) {
+__global__ void rect_col_keys_kernel(const uint32_t* __restrict__ positions, uint32_t nb, uint32_t width,
+                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nb) return;
-  keys[u] = positions[2ull * u + 1] / 3u;
+  keys[u] = positions[2ull * u + 1] / width;
   vals[u] = u;
 }
 
+// Blocks of 3 rows and `width` (1 or 3) columns, values row-major and
+// contiguous (3 width a block).  J x: one thread an output block row, its
+// blocks in order; J^T x: one thread an output column unit, its blocks in the
+// stable column order.  accumulate: y += instead of y =.
 __global__ void rect_spmv_kernel(const double* __restrict__ values, const uint32_t* __restrict__ positions,
                                  const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ order,
-                                 uint32_t out_rows, int transpose, const double* __restrict__ x,
-                                 double* __restrict__ y) {
+                                 uint32_t out_rows, int width, int transpose, int accumulate,
+                                 const double* __restrict__ x, double* __restrict__ y) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= out_rows) return;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (uint32_t e = ptr[r]; e < ptr[r + 1]; ++e) {
+  const uint32_t e0 = ptr[r], e1 = ptr[r + 1];
+  if (transpose && e0 == e1) return;
+  // output rows are block rows of 3; output columns sit at their blocks'
+  // scalar column (a column target need not start at a multiple of 3)
+  const uint64_t base = transpose ? positions[2ull * (order ? order[e0] : e0) + 1] : 3ull * r;
+  double s[3] = {0.0, 0.0, 0.0};
+  for (uint32_t e = e0; e < e1; ++e) {
     const uint32_t u = order ? order[e] : e;
-    const double* b = values + 9ull * u;
+    const double* b = values + 3ull * width * u;
     if (!transpose) {
       const double* xv = x + positions[2ull * u + 1];
-      s0 += b[0] * xv[0] + b[1] * xv[1] + b[2] * xv[2];
-      s1 += b[3] * xv[0] + b[4] * xv[1] + b[5] * xv[2];
-      s2 += b[6] * xv[0] + b[7] * xv[1] + b[8] * xv[2];
+      for (int k = 0; k < 3; ++k)
+        for (int c = 0; c < width; ++c) s[k] += b[k * width + c] * xv[c];
     } else {
       const double* xv = x + positions[2ull * u];
-      s0 += b[0] * xv[0] + b[3] * xv[1] + b[6] * xv[2];
-      s1 += b[1] * xv[0] + b[4] * xv[1] + b[7] * xv[2];
-      s2 += b[2] * xv[0] + b[5] * xv[1] + b[8] * xv[2];
+      for (int c = 0; c < width; ++c) s[c] += b[c] * xv[0] + b[width + c] * xv[1] + b[2 * width + c] * xv[2];
     }
   }
-  y[3ull * r] = s0;
-  y[3ull * r + 1] = s1;
-  y[3ull * r + 2] = s2;
+  const int m = transpose ? width : 3;
+  double* yv = y + base;
+  for (int k = 0; k < m; ++k) yv[k] = accumulate ? yv[k] + s[k] : s[k];
 }
 
 }  // namespace ys
@@ -238,6 +296,48 @@ int32_t ys_rect_records(const double* local_hessians, uint32_t args, uint32_t di
   return YS_OK;
 }
 
+int32_t ys_rect_param_coordinates(const uint32_t* row_codes, uint32_t n, uint32_t K, uint32_t slot_stride,
+                                  uint32_t args, uint32_t param_start, uint32_t* coord_outer, uint32_t* coords,
+                                  uint16_t* dims, void* stream) {
+  YS_REQUIRE(row_codes && coord_outer, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE(args >= 1 && args <= (uint32_t)ys::kRectMaxArgs, YS_ERR_INVALID, "1..8 arguments an instance");
+  YS_REQUIRE((uint64_t)(args - 1) * slot_stride < K, YS_ERR_INVALID, "slot stride beyond the code row");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (coords == nullptr) {
+    YS_CUDA_TRY(cudaMemsetAsync(coord_outer, 0, sizeof(uint32_t), s));
+    if (n == 0) return YS_OK;
+    ys::rect_param_count_kernel<<<ys::grid_for(n, 256), 256, 0, s>>>(row_codes, n, K, slot_stride, (int)args,
+                                                                    coord_outer + 1);
+    YS_CHECK_LAUNCH();
+    size_t tmp = 0;
+    YS_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tmp, coord_outer + 1, coord_outer + 1, (int)n, s));
+    void* d_tmp = nullptr;
+    YS_CUDA_TRY(cudaMallocAsync(&d_tmp, tmp, s));
+    const cudaError_t e = cub::DeviceScan::InclusiveSum(d_tmp, tmp, coord_outer + 1, coord_outer + 1, (int)n, s);
+    cudaFreeAsync(d_tmp, s);
+    YS_CUDA_TRY(e);
+    return YS_OK;
+  }
+  YS_REQUIRE(dims != nullptr, YS_ERR_INVALID, "null dims");
+  if (n == 0) return YS_OK;
+  ys::rect_param_coords_kernel<<<ys::grid_for(n, 256), 256, 0, s>>>(row_codes, n, K, slot_stride, (int)args,
+                                                                   param_start, coord_outer, coords, dims);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_rect_param_records(const double* derivatives, uint32_t args, const uint32_t* row_codes, uint32_t n,
+                              uint32_t K, uint32_t slot_stride, const uint32_t* coord_outer, const uint32_t* record,
+                              double* records, void* stream) {
+  YS_REQUIRE(derivatives && row_codes && coord_outer && record && records, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE(args >= 1 && args <= (uint32_t)ys::kRectMaxArgs, YS_ERR_INVALID, "1..8 arguments an instance");
+  if (n == 0) return YS_OK;
+  ys::rect_param_records_kernel<<<ys::grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(
+      derivatives, (int)args, row_codes, n, K, slot_stride, coord_outer, record, records);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
 int32_t ys_rect_plan_workspace_bytes(uint32_t num_blocks, uint64_t* bytes) {
   YS_REQUIRE(bytes != nullptr, YS_ERR_INVALID, "null output");
   size_t tmp = 0;
@@ -250,9 +350,10 @@ int32_t ys_rect_plan_workspace_bytes(uint32_t num_blocks, uint64_t* bytes) {
 }
 
 int32_t ys_rect_plan(const uint32_t* positions, uint32_t num_blocks, uint32_t block_rows, uint32_t block_cols,
-                     uint32_t* row_ptr, uint32_t* col_ptr, uint32_t* col_order, void* workspace,
+                     uint32_t col_width, uint32_t* row_ptr, uint32_t* col_ptr, uint32_t* col_order, void* workspace,
                      uint64_t workspace_bytes, void* stream) {
   YS_REQUIRE(row_ptr && col_ptr && col_order, YS_ERR_INVALID, "null output");
+  YS_REQUIRE(col_width == 1 || col_width == 3, YS_ERR_INVALID, "blocks 1 or 3 columns wide");
   YS_REQUIRE(num_blocks == 0 || positions, YS_ERR_INVALID, "null positions");
   uint64_t need = 0;
   const int32_t rc = ys_rect_plan_workspace_bytes(num_blocks, &need);
@@ -271,7 +372,8 @@ int32_t ys_rect_plan(const uint32_t* positions, uint32_t num_blocks, uint32_t bl
   void* tmp = w + 4 * keys;
   size_t tmp_bytes = workspace_bytes - 4 * keys;
   if (num_blocks) {
-    ys::rect_col_keys_kernel<<<ys::grid_for(num_blocks, 256), 256, 0, s>>>(positions, num_blocks, k_in, v_in);
+    ys::rect_col_keys_kernel<<<ys::grid_for(num_blocks, 256), 256, 0, s>>>(positions, num_blocks, col_width, k_in,
+                                                                           v_in);
     YS_CHECK_LAUNCH();
     // stable: the blocks of one column stay in block order
     YS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, col_order, (int)num_blocks, 0,
@@ -284,13 +386,15 @@ int32_t ys_rect_plan(const uint32_t* positions, uint32_t num_blocks, uint32_t bl
 
 int32_t ys_rect_spmv(const double* values, const uint32_t* positions, const uint32_t* row_ptr,
                      const uint32_t* col_ptr, const uint32_t* col_order, uint32_t block_rows, uint32_t block_cols,
-                     const double* x, double* y, uint32_t transpose, void* stream) {
+                     uint32_t col_width, const double* x, double* y, uint32_t transpose, uint32_t accumulate,
+                     void* stream) {
   YS_REQUIRE(row_ptr && col_ptr && x && y, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE(col_width == 1 || col_width == 3, YS_ERR_INVALID, "blocks 1 or 3 columns wide");
   const uint32_t out_rows = transpose ? block_cols : block_rows;
   if (out_rows == 0) return YS_OK;
   ys::rect_spmv_kernel<<<ys::grid_for(out_rows, 128), 128, 0, (cudaStream_t)stream>>>(
-      values, positions, transpose ? col_ptr : row_ptr, transpose ? col_order : nullptr, out_rows, (int)transpose,
-      x, y);
+      values, positions, transpose ? col_ptr : row_ptr, transpose ? col_order : nullptr, out_rows, (int)col_width,
+      (int)transpose, (int)accumulate, x, y);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

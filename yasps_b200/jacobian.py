@@ -64,8 +64,8 @@ def _validate_targets(targets, name):
       raise ValueError(f"secondOrderJacobian.__init__: {name} cannot contain dynamic attributes.")
     if t.hash in seen:
       raise ValueError(f"secondOrderJacobian.__init__: {name} contains a duplicate target.")
-    if t.size != 3:
-      raise NotImplementedError(f"secondOrderJacobian: target {t.fullName} is not a 3-vector")
+    if t.size not in (1, 3):
+      raise NotImplementedError(f"secondOrderJacobian: target {t.fullName} is neither a 3-vector nor a scalar")
     seen.add(t.hash)
   return list(targets)
 
@@ -160,6 +160,56 @@ class _RectTerm:
            arr(wstart, L.u32), 3, L.ptr(codes), L.ptr(sizes), L.stream_ptr())
     return codes, K, stride, A
 
+  def parameters(self):
+    """``(which, attribute)`` of the energy's per-element scalar parameters
+    that a Jacobian column can take: the SNH tets' Lame arrays (0 mu,
+    1 lambda) and the inertia vertices' masses (0)."""
+    e = self.expr
+    out = []
+    if e.kind == "snh":
+      for which, p in ((0, e.mu_p), (1, e.lam_p)):
+        if p[0] == "array":
+          out.append((which, p[1]))
+    elif e.kind == "inertia" and e.mass_p[0] == "array":
+      out.append((0, e.mass_p[1]))
+    return out
+
+  def parameter_derivatives(self, which, out):
+    """d(dE/d argument)/d parameter per element, ``[n x 3 args]``."""
+    e, n = self.expr, self.n
+    s = L.stream_ptr()
+    if n == 0:
+      return
+    from .hessian import _Term
+    from .scene import energyRequest
+    helper = _Term(energyRequest(self.energy, [], -1, False), [], [0])
+    if e.kind == "snh":
+      a = self._snh_args(helper)
+      L.call("ys_snh_param_jacobian", ctypes.byref(a), int(which), L.ptr(out), s)
+      return
+    a = L.InertiaArgs()
+    a.position, a.x_before = L.ptr(e.x.value), L.ptr(e.x_before.value)
+    a.velocity = L.ptr(e.vel.value) if e.vel is not None else None
+    a.mass = L.ptr(e.mass_p[1].value)
+    a.dt = e.dt_p[1] if e.dt_p[0] == "value" else e.dt_p[1].scalar()
+    for k in range(3):
+      a.gravity[k] = e.gravity[k]
+    a.num_vertices = n
+    L.call("ys_inertia_mass_jacobian", ctypes.byref(a), 3 if e.vel is not None else 2, L.ptr(out), s)
+
+  def _snh_args(self, helper):
+    e, n = self.expr, self.n
+    a = L.SnhArgs()
+    a.position = helper._union3(e.position.source)
+    a.rest = helper._union3(e.rest.source)
+    a.tets = L.ptr(e.position.through.value)
+    a.num_elements = n
+    mu_arr, a.mu_value = helper._param(e.mu_p, n)
+    lam_arr, a.lam_value = helper._param(e.lam_p, n)
+    a.mu, a.lam = L.ptr(mu_arr), L.ptr(lam_arr)
+    a.dt = helper._param(e.dt_p, n)[1]
+    return a
+
   def local_hessians(self, out):
     e, n = self.expr, self.n
     s = L.stream_ptr()
@@ -177,16 +227,8 @@ class _RectTerm:
     from .scene import energyRequest
     helper = _Term(energyRequest(self.energy, [], -1, False), [], [0])
     if e.kind == "snh":
-      a = L.SnhArgs()
       entry = "ys_snh_rest_local_hessians" if self.rest_form else "ys_snh_local_hessians"
-      a.position = helper._union3(e.position.source)
-      a.rest = helper._union3(e.rest.source)
-      a.tets = L.ptr(e.position.through.value)
-      a.num_elements = n
-      mu_arr, a.mu_value = helper._param(e.mu_p, n)
-      lam_arr, a.lam_value = helper._param(e.lam_p, n)
-      a.mu, a.lam = L.ptr(mu_arr), L.ptr(lam_arr)
-      a.dt = helper._param(e.dt_p, n)[1]
+      a = self._snh_args(helper)
       L.call(entry, ctypes.byref(a), L.ptr(out), s)
       return
     a = L.EnergyArgs()
@@ -281,6 +323,16 @@ class secondOrderJacobian:
                                     f"{type(t.expr).__name__} are not built"
                                     + (" (rest against rest)" if t.expr.kind == "snh" else ""))
         t._rest_form = in_rows or in_cols
+      params = []
+      for which, att in t.parameters():
+        if any(att is x for x in self.__row_wrt):
+          raise NotImplementedError("secondOrderJacobian: parameter rows are not built (take the transposed "
+                                    "target lists and spmv(transpose=True))")
+        k = next((i for i, x in enumerate(self.__column_wrt) if x is att), None)
+        if k is not None:
+          if t.rest_form:
+            raise NotImplementedError("secondOrderJacobian: rest positions and parameters in one Jacobian")
+          params.append((which, int(self.__column_start[k])))
       rc, K, stride, A = t.codes(self.__row_wrt, self.__row_start)
       cc, _, _, _ = t.codes(self.__column_wrt, self.__column_start)
       outer = torch.empty(n + 1, dtype=torch.int32, device=_dev())
@@ -288,39 +340,61 @@ class secondOrderJacobian:
       m = int(outer[n].item()) if n else 0
       N = 3 * (diff if diff else A)  # the rest form's local Hessian covers all 8 arguments
       local_h = torch.empty(max(n * N * (N + 1) // 2, 1), dtype=torch.float64, device=_dev())
-      terms.append(dict(term=t, rc=rc, cc=cc, K=K, stride=stride, A=A, diff=diff, outer=outer, m=m, off=total,
-                        local_h=local_h))
+      d = dict(term=t, rc=rc, cc=cc, K=K, stride=stride, A=A, diff=diff, outer=outer, m=m, off=total,
+               local_h=local_h, params=[])
       total += m
+      for which, start in params:
+        pouter = torch.empty(n + 1, dtype=torch.int32, device=_dev())
+        L.call("ys_rect_param_coordinates", L.ptr(rc), n, K, stride, A, start, L.ptr(pouter), None, None, s)
+        pm = int(pouter[n].item()) if n else 0
+        deriv = torch.empty(max(3 * A * n, 1), dtype=torch.float64, device=_dev())
+        d["params"].append(dict(which=which, start=start, outer=pouter, m=pm, off=total, deriv=deriv))
+        total += pm
+      terms.append(d)
     coords = torch.empty(max(2 * total, 2), dtype=torch.int32, device=_dev())
     dims = torch.empty(max(2 * total, 2), dtype=torch.int16, device=_dev())
     for d in terms:
       if d["m"]:
         L.call("ys_rect_coordinates", L.ptr(d["rc"]), L.ptr(d["cc"]), d["term"].n, d["K"], d["stride"], d["A"],
                L.ptr(d["outer"]), coords.data_ptr() + 8 * d["off"], dims.data_ptr() + 4 * d["off"], s)
+      for q in d["params"]:
+        if q["m"]:
+          L.call("ys_rect_param_coordinates", L.ptr(d["rc"]), d["term"].n, d["K"], d["stride"], d["A"], q["start"],
+                 L.ptr(q["outer"]), coords.data_ptr() + 8 * q["off"], dims.data_ptr() + 4 * q["off"], s)
     pat = _Pattern(coords, dims, total)
-    if pat.num_unique and not pat.all3:
-      raise NotImplementedError("secondOrderJacobian: only 3x3 blocks are built")
     records = torch.empty(max(pat.total_records, 1), dtype=torch.float64, device=_dev())
     values = torch.zeros(max(pat.total_values, 1), dtype=torch.float64, device=_dev())
-    # products: row and column pointers over the unique blocks
-    nu = pat.num_unique
-    br, bc = self.rows // 3, self.cols // 3
-    row_ptr = torch.empty(br + 1, dtype=torch.int32, device=_dev())
-    col_ptr = torch.empty(bc + 1, dtype=torch.int32, device=_dev())
-    col_order = torch.empty(max(nu, 1), dtype=torch.int32, device=_dev())
-    ws = L.u64(0)
-    L.call("ys_rect_plan_workspace_bytes", nu, ctypes.byref(ws))
-    work = torch.empty(int(ws.value), dtype=torch.uint8, device=_dev())
-    L.call("ys_rect_plan", L.ptr(pat.positions), nu, br, bc, L.ptr(row_ptr), L.ptr(col_ptr), L.ptr(col_order),
-           L.ptr(work), int(ws.value), s)
-    return dict(terms=terms, pattern=pat, records=records, values=values, plan=(row_ptr, col_ptr, col_order))
+    # products: row and column pointers of every block category (3 rows,
+    # 1 or 3 columns)
+    plans = []
+    b0 = 0
+    nc = len(pat.category_counts) if pat.num_unique else 0
+    for c in range(nc):
+      h, w = pat.category_dims[2 * c], pat.category_dims[2 * c + 1]
+      nb = pat.category_counts[c]
+      if h != 3 or w not in (1, 3):
+        raise NotImplementedError(f"secondOrderJacobian: {h}x{w} blocks are not built")
+      br, bc = self.rows // 3, self.cols // w
+      row_ptr = torch.empty(br + 1, dtype=torch.int32, device=_dev())
+      col_ptr = torch.empty(bc + 1, dtype=torch.int32, device=_dev())
+      col_order = torch.empty(max(nb, 1), dtype=torch.int32, device=_dev())
+      ws = L.u64(0)
+      L.call("ys_rect_plan_workspace_bytes", nb, ctypes.byref(ws))
+      work = torch.empty(int(ws.value), dtype=torch.uint8, device=_dev())
+      pos = pat.positions.data_ptr() + 8 * b0
+      L.call("ys_rect_plan", pos, nb, br, bc, w, L.ptr(row_ptr), L.ptr(col_ptr), L.ptr(col_order), L.ptr(work),
+             int(ws.value), s)
+      plans.append(dict(width=w, blocks=nb, first=b0, value_start=pat.category_starts[c], row_ptr=row_ptr,
+                        col_ptr=col_ptr, col_order=col_order, block_cols=bc))
+      b0 += nb
+    return dict(terms=terms, pattern=pat, records=records, values=values, plans=plans)
 
   def compute(self):
     """Evaluate every term and assemble (``secondOrderJacobian.pyx:530-559``;
     dynamic sources rebuild their pattern on every call)."""
     torch = _torch()
-    if self.rows % 3 or self.cols % 3:
-      raise NotImplementedError("secondOrderJacobian: targets of 3-vectors only")
+    if any(t.size != 3 for t in self.__row_wrt):
+      raise NotImplementedError("secondOrderJacobian: row targets of 3-vectors only")
     s = L.stream_ptr()
     if self._setup is None:
       self._setup = self._build(self.sources)
@@ -331,20 +405,32 @@ class secondOrderJacobian:
       pat = part["pattern"]
       for d in part["terms"]:
         t = d["term"]
-        if t.n == 0 or d["m"] == 0:
+        if t.n == 0:
           continue
-        t.local_hessians(d["local_h"])
-        L.call("ys_rect_records", L.ptr(d["local_h"]), d["A"], d["diff"], L.ptr(d["rc"]), L.ptr(d["cc"]), t.n,
-               d["K"], d["stride"], L.ptr(d["outer"]), pat.record.data_ptr() + 4 * d["off"], L.ptr(part["records"]), s)
-      if pat.num_unique:
-        L.call("ys_assemble3", L.ptr(part["records"]), L.ptr(pat.record_begin), L.ptr(pat.record_count),
-               L.ptr(pat.value_offset), pat.num_unique, L.ptr(part["values"]), None, s)
+        if d["m"]:
+          t.local_hessians(d["local_h"])
+          L.call("ys_rect_records", L.ptr(d["local_h"]), d["A"], d["diff"], L.ptr(d["rc"]), L.ptr(d["cc"]), t.n,
+                 d["K"], d["stride"], L.ptr(d["outer"]), pat.record.data_ptr() + 4 * d["off"],
+                 L.ptr(part["records"]), s)
+        for q in d["params"]:
+          if not q["m"]:
+            continue
+          t.parameter_derivatives(q["which"], q["deriv"])
+          L.call("ys_rect_param_records", L.ptr(q["deriv"]), d["A"], L.ptr(d["rc"]), t.n, d["K"], d["stride"],
+                 L.ptr(q["outer"]), pat.record.data_ptr() + 4 * q["off"], L.ptr(part["records"]), s)
       nu = pat.num_unique
+      if nu:
+        if pat.all3:
+          L.call("ys_assemble3", L.ptr(part["records"]), L.ptr(pat.record_begin), L.ptr(pat.record_count),
+                 L.ptr(pat.value_offset), nu, L.ptr(part["values"]), None, s)
+        else:
+          L.call("ys_assemble", L.ptr(part["records"]), L.ptr(pat.record_begin), L.ptr(pat.record_count),
+                 L.ptr(pat.value_offset), L.ptr(pat.dims), nu, L.ptr(part["values"]), None, s)
       setattr(self, "blocks_flattened" + name, part["values"][:pat.total_values] if nu else part["values"][:0])
       setattr(self, "block_positions" + name, pat.positions[:2 * nu])
-      setattr(self, "block_dimensions" + name, [[3, 3]] if nu else [])
-      setattr(self, "blocks_start_indices" + name, [0, 9 * nu] if nu else [0])
-      setattr(self, "block_counts" + name, [nu] if nu else [])
+      setattr(self, "block_dimensions" + name, list(pat.category_dims) if nu else [])
+      setattr(self, "blocks_start_indices" + name, list(pat.category_starts) if nu else [0])
+      setattr(self, "block_counts" + name, list(pat.category_counts) if nu else [])
     self._dynamic_part = dyn
     return self
 
@@ -363,16 +449,15 @@ class secondOrderJacobian:
       raise RuntimeError("secondOrderJacobian.spmv: call compute() first")
     out = vector(n_out)
     s = L.stream_ptr()
-    br, bc = self.rows // 3, self.cols // 3
+    br = self.rows // 3
     parts = [p for p in (self._setup, getattr(self, "_dynamic_part", None)) if p is not None]
-    tmp = vector(n_out)
-    for k, part in enumerate(parts):
-      dst = out if k == 0 else tmp
-      row_ptr, col_ptr, col_order = part["plan"]
-      L.call("ys_rect_spmv", L.ptr(part["values"]), L.ptr(part["pattern"].positions), L.ptr(row_ptr), L.ptr(col_ptr),
-             L.ptr(col_order), br, bc, L.ptr(x.value), L.ptr(dst.value), int(bool(transpose)), s)
-      if k:
-        out.value.add_(tmp.value)
+    for part in parts:
+      pat = part["pattern"]
+      for pl in part["plans"]:
+        L.call("ys_rect_spmv", part["values"].data_ptr() + 8 * pl["value_start"],
+               pat.positions.data_ptr() + 8 * pl["first"], L.ptr(pl["row_ptr"]), L.ptr(pl["col_ptr"]),
+               L.ptr(pl["col_order"]), br, pl["block_cols"], pl["width"], L.ptr(x.value), L.ptr(out.value),
+               int(bool(transpose)), 1, s)
     return out
 
 
