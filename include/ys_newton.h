@@ -326,8 +326,19 @@ int32_t ys_rect_param_records(const double* derivatives, uint32_t args, const ui
                               uint32_t K, uint32_t slot_stride, const uint32_t* coord_outer, const uint32_t* record,
                               double* records, void* stream);
 
+/* First-order Jacobian of the affine-body vertex positions x_i = A_b xbar_i
+ * + t_b (firstOrderJacobian.pyx of the reference's diff1 on a vector
+ * source): rows 3 i, a (3 x 9) block in the columns of A (row r holds xbar_i
+ * at 3 r .. 3 r + 2) and a (3 x 3) identity in those of t, per vertex in
+ * that order (a column start < 0 leaves that target out).  With record NULL
+ * it writes the coordinates and dims of the n (or 2 n) occurrences; with
+ * the assembly plan of ys_pattern_build over them, the records.           */
+int32_t ys_affine_position_jacobian(const uint32_t* vertex_body, const double* xbar, uint32_t n,
+                                    int64_t a_column_start, int64_t t_column_start, uint32_t* coords,
+                                    uint16_t* dims, const uint32_t* record, double* records, void* stream);
+
 /* Products with one category of the assembled rectangular matrix (unique
- * blocks of 3 rows and col_width = 1 or 3 columns, sorted by (row, col),
+ * blocks of 3 rows and col_width = 1, 3 or 9 columns, sorted by (row, col),
  * scalar positions, 3 col_width values a block).  ys_rect_plan builds
  * row_ptr [block_rows + 1], col_ptr [block_cols + 1] (block_cols column
  * units of col_width) and col_order [num_blocks] (blocks by column, stable);

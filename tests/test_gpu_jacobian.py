@@ -293,3 +293,28 @@ def test_inertia_mass_column_beside_a_position_column():
     D[3 * v:3 * v + 3, v] = x[v] - xt[v]
     D[3 * v:3 * v + 3, nf + 3 * v:nf + 3 * v + 3] = -cube.mass[v] * np.eye(3)
   check(J, D, None, None)
+
+
+def test_first_order_jacobian_of_affine_vertex_positions():
+  """diff1 of a vector-valued source: the affine-body vertex positions
+  x_i = A_b xbar_i + t_b against the bodies' affine matrices (3 x 9 blocks,
+  row r holding xbar_i) and translations (3 x 3 identities), as the
+  reference's firstOrderJacobian; products in both directions."""
+  from yasps_b200.jacobian import firstOrderJacobian
+  from yasps_b200.scene import scene as make_scene
+  bodies = scenes.affine_bodies(num_bodies=3, m=2, seed=3)
+  sc = make_scene("abd_map")
+  mesh = sc.addMesh("m")
+  _, amat, trans, _, vpos = scenes._affine_body_attributes(mesh, bodies)
+  J = differentiator().diff1(vpos, [amat, trans])
+  assert isinstance(J, firstOrderJacobian)
+  J.compute()
+  assert J.block_dimensions == [3, 3, 3, 9]
+  nv, nb = len(bodies.rest), bodies.num_bodies
+  D = np.zeros((3 * nv, 12 * nb))
+  for i in range(nv):
+    b = int(bodies.vertex_body[i])
+    for r in range(3):
+      D[3 * i + r, 9 * b + 3 * r:9 * b + 3 * r + 3] = bodies.rest[i]
+      D[3 * i + r, 9 * nb + 3 * b + r] = 1.0
+  check(J, D, None, None)

@@ -146,6 +146,7 @@ SIGNATURES = {
     "ys_inertia_mass_jacobian": (i32, [P(InertiaArgs), u32, vp, vp]),
     "ys_rect_param_coordinates": (i32, [vp, u32, u32, u32, u32, u32, vp, vp, vp, vp]),
     "ys_rect_param_records": (i32, [vp, u32, vp, u32, u32, u32, vp, vp, vp, vp]),
+    "ys_affine_position_jacobian": (i32, [vp, vp, u32, C.c_int64, C.c_int64, vp, vp, vp, vp, vp]),
     "ys_affine_eval": (i32, [P(AffineArgs), vp]),
     "ys_coupled_indices": (i32, [vp, u32, u32, u32, P(u32), P(i32), P(u32), u32, vp, u32, i32, u32, i32, u32, vp, vp,
                                  vp]),

@@ -176,6 +176,48 @@ __global__ void rect_param_records_kernel(const double* __restrict__ d, int args
   }
 }
 
+// First-order Jacobian of the affine-body vertex positions x_i = A_b xbar_i
+// + t_b (b the body of vertex i): rows 3 i; the (3 x 9) block of A (row r
+// holds xbar_i at columns 3 r .. 3 r + 2) and the (3 x 3) identity of t,
+// in this order per vertex.
+__global__ void affine_jacobian_coords_kernel(const uint32_t* __restrict__ vertex_body, uint32_t n, int64_t a_col,
+                                              int64_t t_col, uint32_t* __restrict__ coords,
+                                              uint16_t* __restrict__ dims) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t b = vertex_body[i];
+  uint64_t o = (uint64_t)i * ((a_col >= 0) + (t_col >= 0));
+  if (a_col >= 0) {
+    coords[2 * o] = 3u * i;
+    coords[2 * o + 1] = (uint32_t)(a_col + 9ll * b);
+    dims[2 * o] = 3;
+    dims[2 * o + 1] = 9;
+    ++o;
+  }
+  if (t_col >= 0) {
+    coords[2 * o] = 3u * i;
+    coords[2 * o + 1] = (uint32_t)(t_col + 3ll * b);
+    dims[2 * o] = 3;
+    dims[2 * o + 1] = 3;
+  }
+}
+
+__global__ void affine_jacobian_records_kernel(const double* __restrict__ xbar, uint32_t n, int with_a, int with_t,
+                                               const uint32_t* __restrict__ record, double* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t o = (uint64_t)i * (with_a + with_t);
+  if (with_a) {
+    double* dst = out + record[o++];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 9; ++c) dst[9 * r + c] = (c / 3 == r) ? xbar[3ull * i + c % 3] : 0.0;
+  }
+  if (with_t) {
+    double* dst = out + record[o];
+    for (int k = 0; k < 9; ++k) dst[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  }
+}
+
 // First block of every block row (rows sorted): row_ptr[r] = lower bound.
 __global__ void rect_row_ptr_kernel(const uint32_t* __restrict__ positions, uint32_t nb, uint32_t block_rows,
                                     uint32_t* __restrict__ row_ptr) {
@@ -211,7 +253,7 @@ __global__ void rect_col_keys_kernel(const uint32_t* __restrict__ positions, uin
   vals[u] = u;
 }
 
-// Blocks of 3 rows and `width` (1 or 3) columns, values row-major and
+// Blocks of 3 rows and `width` (1, 3 or 9) columns, values row-major and
 // contiguous (3 width a block).  J x: one thread an output block row, its
 // blocks in order; J^T x: one thread an output column unit, its blocks in the
 // stable column order.  accumulate: y += instead of y =.
@@ -226,7 +268,7 @@ __global__ void rect_spmv_kernel(const double* __restrict__ values, const uint32
   // output rows are block rows of 3; output columns sit at their blocks'
   // scalar column (a column target need not start at a multiple of 3)
   const uint64_t base = transpose ? positions[2ull * (order ? order[e0] : e0) + 1] : 3ull * r;
-  double s[3] = {0.0, 0.0, 0.0};
+  double s[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (uint32_t e = e0; e < e1; ++e) {
     const uint32_t u = order ? order[e] : e;
     const double* b = values + 3ull * width * u;
@@ -338,6 +380,25 @@ int32_t ys_rect_param_records(const double* derivatives, uint32_t args, const ui
   return YS_OK;
 }
 
+int32_t ys_affine_position_jacobian(const uint32_t* vertex_body, const double* xbar, uint32_t n,
+                                    int64_t a_column_start, int64_t t_column_start, uint32_t* coords,
+                                    uint16_t* dims, const uint32_t* record, double* records, void* stream) {
+  YS_REQUIRE(a_column_start >= 0 || t_column_start >= 0, YS_ERR_INVALID, "no column target");
+  if (n == 0) return YS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (record == nullptr) {
+    YS_REQUIRE(vertex_body && coords && dims, YS_ERR_INVALID, "null argument");
+    ys::affine_jacobian_coords_kernel<<<ys::grid_for(n, 256), 256, 0, s>>>(vertex_body, n, a_column_start,
+                                                                         t_column_start, coords, dims);
+  } else {
+    YS_REQUIRE(xbar && records, YS_ERR_INVALID, "null argument");
+    ys::affine_jacobian_records_kernel<<<ys::grid_for(n, 256), 256, 0, s>>>(
+        xbar, n, a_column_start >= 0 ? 1 : 0, t_column_start >= 0 ? 1 : 0, record, records);
+  }
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
 int32_t ys_rect_plan_workspace_bytes(uint32_t num_blocks, uint64_t* bytes) {
   YS_REQUIRE(bytes != nullptr, YS_ERR_INVALID, "null output");
   size_t tmp = 0;
@@ -353,7 +414,7 @@ int32_t ys_rect_plan(const uint32_t* positions, uint32_t num_blocks, uint32_t bl
                      uint32_t col_width, uint32_t* row_ptr, uint32_t* col_ptr, uint32_t* col_order, void* workspace,
                      uint64_t workspace_bytes, void* stream) {
   YS_REQUIRE(row_ptr && col_ptr && col_order, YS_ERR_INVALID, "null output");
-  YS_REQUIRE(col_width == 1 || col_width == 3, YS_ERR_INVALID, "blocks 1 or 3 columns wide");
+  YS_REQUIRE(col_width == 1 || col_width == 3 || col_width == 9, YS_ERR_INVALID, "blocks 1, 3 or 9 columns wide");
   YS_REQUIRE(num_blocks == 0 || positions, YS_ERR_INVALID, "null positions");
   uint64_t need = 0;
   const int32_t rc = ys_rect_plan_workspace_bytes(num_blocks, &need);
@@ -389,7 +450,7 @@ int32_t ys_rect_spmv(const double* values, const uint32_t* positions, const uint
                      uint32_t col_width, const double* x, double* y, uint32_t transpose, uint32_t accumulate,
                      void* stream) {
   YS_REQUIRE(row_ptr && col_ptr && x && y, YS_ERR_INVALID, "null argument");
-  YS_REQUIRE(col_width == 1 || col_width == 3, YS_ERR_INVALID, "blocks 1 or 3 columns wide");
+  YS_REQUIRE(col_width == 1 || col_width == 3 || col_width == 9, YS_ERR_INVALID, "blocks 1, 3 or 9 columns wide");
   const uint32_t out_rows = transpose ? block_cols : block_rows;
   if (out_rows == 0) return YS_OK;
   ys::rect_spmv_kernel<<<ys::grid_for(out_rows, 128), 128, 0, (cudaStream_t)stream>>>(

@@ -53,7 +53,7 @@ def _start_indices(targets):
   return starts
 
 
-def _validate_targets(targets, name):
+def _validate_targets(targets, name, sizes=(1, 3)):
   if not isinstance(targets, list) or len(targets) == 0:
     raise ValueError(f"secondOrderJacobian.__init__: {name} must be a non-empty list.")
   seen = set()
@@ -64,8 +64,8 @@ def _validate_targets(targets, name):
       raise ValueError(f"secondOrderJacobian.__init__: {name} cannot contain dynamic attributes.")
     if t.hash in seen:
       raise ValueError(f"secondOrderJacobian.__init__: {name} contains a duplicate target.")
-    if t.size not in (1, 3):
-      raise NotImplementedError(f"secondOrderJacobian: target {t.fullName} is neither a 3-vector nor a scalar")
+    if t.size not in sizes:
+      raise NotImplementedError(f"secondOrderJacobian: target {t.fullName} of size {t.size} is not built")
     seen.add(t.hash)
   return list(targets)
 
@@ -253,9 +253,9 @@ class secondOrderJacobian:
   """Rectangular matrix ``d2E / (d row_wrt d column_wrt)`` of a sum of
   scalar energies (``secondOrderJacobian.pyx:17-52``)."""
 
-  def __init__(self, row_wrt: List[attribute], column_wrt: List[attribute]):
+  def __init__(self, row_wrt: List[attribute], column_wrt: List[attribute], _column_sizes=(1, 3)):
     self.__row_wrt = _validate_targets(row_wrt, "row_wrt")
-    self.__column_wrt = _validate_targets(column_wrt, "column_wrt")
+    self.__column_wrt = _validate_targets(column_wrt, "column_wrt", _column_sizes)
     self.__row_start = _start_indices(self.__row_wrt)
     self.__column_start = _start_indices(self.__column_wrt)
     self.rows = int(self.__row_start[-1])
@@ -364,15 +364,20 @@ class secondOrderJacobian:
     pat = _Pattern(coords, dims, total)
     records = torch.empty(max(pat.total_records, 1), dtype=torch.float64, device=_dev())
     values = torch.zeros(max(pat.total_values, 1), dtype=torch.float64, device=_dev())
-    # products: row and column pointers of every block category (3 rows,
-    # 1 or 3 columns)
+    return dict(terms=terms, pattern=pat, records=records, values=values, plans=self._plans(pat))
+
+  def _plans(self, pat):
+    """Row and column pointers of every block category (3 rows; 1, 3 or 9
+    columns) for the products."""
+    torch = _torch()
+    s = L.stream_ptr()
     plans = []
     b0 = 0
     nc = len(pat.category_counts) if pat.num_unique else 0
     for c in range(nc):
       h, w = pat.category_dims[2 * c], pat.category_dims[2 * c + 1]
       nb = pat.category_counts[c]
-      if h != 3 or w not in (1, 3):
+      if h != 3 or w not in (1, 3, 9):
         raise NotImplementedError(f"secondOrderJacobian: {h}x{w} blocks are not built")
       br, bc = self.rows // 3, self.cols // w
       row_ptr = torch.empty(br + 1, dtype=torch.int32, device=_dev())
@@ -387,7 +392,7 @@ class secondOrderJacobian:
       plans.append(dict(width=w, blocks=nb, first=b0, value_start=pat.category_starts[c], row_ptr=row_ptr,
                         col_ptr=col_ptr, col_order=col_order, block_cols=bc))
       b0 += nb
-    return dict(terms=terms, pattern=pat, records=records, values=values, plans=plans)
+    return plans
 
   def compute(self):
     """Evaluate every term and assemble (``secondOrderJacobian.pyx:530-559``;
@@ -461,6 +466,73 @@ class secondOrderJacobian:
     return out
 
 
+class firstOrderJacobian(secondOrderJacobian):
+  """Sparse first derivative of a vector attribute with respect to targets
+  (``PKG/matrixAndVector/matrix/firstOrderJacobian.pyx:87-117``): rows follow
+  the source's instance-major storage, columns the targets.  Built for the
+  affine-body vertex positions ``x = A xbar + t`` (``affine_position``)
+  against the bodies' ``affine_matrices`` (3 x 9 blocks) and
+  ``translations`` (3 x 3 identities)."""
+
+  def __init__(self, row_source: attribute, wrt: List[attribute]):
+    from .energies import AffinePosition
+    e = getattr(row_source, "expr", None)
+    if not isinstance(e, AffinePosition):
+      raise NotImplementedError("firstOrderJacobian: vector sources other than affine-body vertex positions are "
+                                "not built")
+    if row_source.isDynamic:
+      raise ValueError("firstOrderJacobian.__init__: dynamically sized row sources are not supported because "
+                       "matrix dimensions must remain fixed.")
+    super().__init__([row_source], list(wrt), _column_sizes=(3, 9))
+    self.__row_source = row_source
+    self._map = e
+    starts = self.column_start_indices
+    self._a_col = next((int(starts[k]) for k, t in enumerate(self.column_wrt) if t is e.affine), -1)
+    self._t_col = next((int(starts[k]) for k, t in enumerate(self.column_wrt) if t is e.translation), -1)
+
+  @property
+  def row_source(self):
+    return self.__row_source
+
+  @property
+  def wrt(self):
+    return self.column_wrt
+
+  def compute(self):
+    torch = _torch()
+    s = L.stream_ptr()
+    e = self._map
+    n = int(self.__row_source.correspondance.numInstances)
+    if self._setup is None:
+      per = (self._a_col >= 0) + (self._t_col >= 0)
+      m = n * per
+      coords = torch.empty(max(2 * m, 2), dtype=torch.int32, device=_dev())
+      dims = torch.empty(max(2 * m, 2), dtype=torch.int16, device=_dev())
+      vb = e.conn.value
+      if m:
+        L.call("ys_affine_position_jacobian", L.ptr(vb), None, n, self._a_col, self._t_col, L.ptr(coords),
+               L.ptr(dims), None, None, s)
+      pat = _Pattern(coords, dims, m)
+      records = torch.empty(max(pat.total_records, 1), dtype=torch.float64, device=_dev())
+      values = torch.zeros(max(pat.total_values, 1), dtype=torch.float64, device=_dev())
+      self._setup = dict(terms=[], pattern=pat, records=records, values=values, plans=self._plans(pat), m=m)
+    part = self._setup
+    pat = part["pattern"]
+    if part["m"]:
+      L.call("ys_affine_position_jacobian", None, L.ptr(e.rest.value), n, self._a_col, self._t_col, None, None,
+             L.ptr(pat.record), L.ptr(part["records"]), s)
+      L.call("ys_assemble", L.ptr(part["records"]), L.ptr(pat.record_begin), L.ptr(pat.record_count),
+             L.ptr(pat.value_offset), L.ptr(pat.dims), pat.num_unique, L.ptr(part["values"]), None, s)
+    nu = pat.num_unique
+    self.blocks_flattened = part["values"][:pat.total_values] if nu else part["values"][:0]
+    self.block_positions = pat.positions[:2 * nu]
+    self.block_dimensions = list(pat.category_dims) if nu else []
+    self.blocks_start_indices = list(pat.category_starts) if nu else [0]
+    self.block_counts = list(pat.category_counts) if nu else []
+    self._dynamic_part = None
+    return self
+
+
 class gradient(vector):
   """Gradient of scalar energies with respect to targets, as ``diff1``
   returns it (``differentiator.pyx:174-239``): ``compute`` evaluates the
@@ -510,8 +582,13 @@ class differentiator:
       raise ValueError("differentiator.diff1: source can not be empty.")
     if not isinstance(global_targets, list) or not global_targets:
       raise ValueError("differentiator.diff1: global_targets can not be empty.")
-    if any(e.size != 1 for e in src):
-      raise NotImplementedError("differentiator.diff1: first-order Jacobians of vector-valued sources are not built")
+    vector_valued = [e.size != 1 for e in src]
+    if any(vector_valued):
+      if not all(vector_valued):
+        raise ValueError("differentiator.diff1: scalar and vector-valued sources cannot be mixed in one call.")
+      if len(src) != 1:
+        raise NotImplementedError("differentiator.diff1: one vector-valued source a call")
+      return firstOrderJacobian(src[0], list(global_targets))
     reqs = [energyRequest(e, list(local_targets), -1, bool(dynamic_instances)) for e in src]
     parent = hessian(list(global_targets), [] if dynamic_instances else reqs, reqs if dynamic_instances else [])
     return gradient(global_targets, parent)
