@@ -325,18 +325,19 @@ def gpu_arm(args):
 GEMV_LAYOUT_56 = 111_651_744  # tiled-layout bytes of one domain-GEMV launch on the 56^3 cube
 
 
-# DRAM bytes (read + write) of one tiled SpMV launch on this 64^3 workload,
-# from an ncu capture of the same launch (dram__bytes.sum.per_second x
-# gpu__time_duration.sum = 3.0907 TB/s x 45.024 us); None on other sizes
-SPMV_TILED_TRAFFIC_64 = 139.16e6
+# DRAM bytes (read + write) of one streamed-tile SpMV launch on this 64^3
+# workload, from an ncu capture of the same launch (dram__bytes.sum.per_second
+# x gpu__time_duration.sum = 3.2909 TB/s x 37.984 us); None on other sizes
+SPMV_STREAM_TRAFFIC_64 = 125.00e6
 
 
 def spmv_roofline(H, hbm, peak_kind, side, reps=50):
-  """The SpMV of the FP32 PCG loop (the tiled kernel: FP32 block slots,
-  plan entries and row pointers staged in shared memory by bulk copies,
-  the float4 copy of the direction gathered) timed alone with CUDA events
-  over `reps` launches on its stream.  Algorithmic bytes per launch (the
-  symmetric storage's own count): nb (9 * 4 + 8) for the stored FP32
+  """The SpMV of the FP32 PCG loop timed alone with CUDA events over `reps`
+  launches on its stream: the streamed-tile kernel (each tile's packed FP32
+  blocks, entry words and row offsets staged in shared memory by bulk
+  copies, its distinct neighbour vectors gathered once), or the tiled one
+  for a block set without a streamed plan.  Algorithmic bytes per launch
+  (the symmetric storage's own count): nb (9 * 4 + 8) for the stored FP32
   blocks and two 32-bit indices each, plus the vector read and the product
   written once in FP64, 2 * 8 * n."""
   import torch
@@ -344,6 +345,7 @@ def spmv_roofline(H, hbm, peak_kind, side, reps=50):
   bs = H.block_sets[0]
   row_ptr, eb, ec = H.spmv_plan(bs)
   row_block, cap, ecap = H.tile_plan(bs)
+  sp = H.stream_plan(bs)
   nv = H.rows // 3
   entries = int(row_ptr[nv].item())
   x = torch.cos(torch.arange(H.rows, dtype=torch.float64, device="cuda") * 0.37)
@@ -351,8 +353,15 @@ def spmv_roofline(H, hbm, peak_kind, side, reps=50):
   y = torch.empty_like(x)
   s = torch.cuda.current_stream()
   L.call("ys_pack_x32", L.ptr(x), nv, L.ptr(x32), s.cuda_stream)
-  call = lambda: L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec),
-                        L.ptr(row_block), cap, ecap, 0, nv, L.ptr(x32), L.ptr(y), 0, None, s.cuda_stream)
+  if sp is not None:
+    st = sp.struct()
+    name = "spmv3_x32_stream (streamed-tile symmetric 3x3 block SpMV of the FP32 PCG loop)"
+    call = lambda: L.call("ys_spmv3_x32_streamed", st, L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv,
+                          L.ptr(x32), L.ptr(y), 0, 0, 0, None, s.cuda_stream)
+  else:
+    name = "spmv3_x32_tiled (tiled symmetric 3x3 block SpMV of the FP32 PCG loop)"
+    call = lambda: L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec),
+                          L.ptr(row_block), cap, ecap, 0, nv, L.ptr(x32), L.ptr(y), 0, None, s.cuda_stream)
   for _ in range(3):
     call()
   torch.cuda.synchronize()
@@ -366,10 +375,15 @@ def spmv_roofline(H, hbm, peak_kind, side, reps=50):
   nb = bs.pattern.num_unique
   nbytes = nb * (9 * 4 + 8) + 2 * 8 * H.rows
   achieved = nbytes / (ms / 1e3) / 1e9
-  return {"kernel": "spmv3_x32_tiled (symmetric 3x3 block SpMV of the FP32 PCG loop)", "bound": "hbm",
-          "achieved": achieved, "peak": hbm, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-          "traffic": SPMV_TILED_TRAFFIC_64 if side == 64 else None, "bytes_per_launch": nbytes,
-          "ms_per_launch": ms, "stored_blocks": nb, "entries": entries, "tile_cap": cap, "entry_cap": ecap}
+  out = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_source": peak_kind, "unit": "GB/s",
+         "frac": achieved / hbm,
+         "traffic": SPMV_STREAM_TRAFFIC_64 if (side == 64 and sp is not None) else None,
+         "bytes_per_launch": nbytes, "ms_per_launch": ms, "stored_blocks": nb, "entries": entries}
+  if sp is not None:
+    out.update({"stream_block_cap": sp.block_cap, "stream_entry_cap": sp.entry_cap, "stream_halo_cap": sp.halo_cap})
+  else:
+    out.update({"tile_cap": cap, "entry_cap": ecap})
+  return out
 
 
 def served_oracle_check(done, seed, count=8, max_side=30):

@@ -562,6 +562,66 @@ int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr,
                            uint32_t stages, uint32_t num_vars, const float* x32, double* y,
                            int32_t beta, uint32_t* stage_status, void* stream);
 
+/* Streamed-tile plan of a 3x3 block set (ys_spmv_stream_plan): tiles of
+ * YS_SPMV_TILE_ROWS rows, each with one contiguous run of packed FP32
+ * blocks (its own stored blocks, then the blocks of earlier tiles that its
+ * rows use transposed), one run of entry words and its distinct neighbour
+ * variables.  block_cap == 0: no plan.  No counterpart in the reference.  */
+typedef struct ys_spmv_stream {
+  const float* blocks32;         /* 9 floats a slot, ys_spmv_stream_words slots (ys_spmv_stream_fill) */
+  const uint32_t* desc;          /* 4 words a tile (+ 4 scratch): base, blocks, entries, columns      */
+  const uint32_t* rows;          /* 68 words a tile: row offsets into the entry words, column count  */
+  const uint32_t* words;         /* entry words: column index | block slot << 16 | transposed << 31  */
+  const uint32_t* halo;          /* distinct neighbour variables of each tile, ascending             */
+  uint32_t block_cap;            /* most blocks, entries, distinct columns of a tile (multiples of 4) */
+  uint32_t entry_cap;
+  uint32_t halo_cap;
+} ys_spmv_stream;
+
+/* Slots (and words) each array of a streamed-tile plan needs: num_entries
+ * = row_ptr[num_vars] of the row plan.  No counterpart in the reference.  */
+int32_t ys_spmv_stream_words(uint32_t num_entries, uint32_t num_vars, uint64_t* words);
+
+/* Builds the streamed-tile plan of a 3x3 block set from its row plan and
+ * ys_spmv_tile_plan's row_block: desc [4 * (tiles + 1)] words, rows
+ * [68 * tiles], words / halo / src [capacity_words] (>= ys_spmv_stream_words),
+ * all 16-byte aligned; src[s] = the stored block of stream slot s (or
+ * 0xffffffff).  caps_host[3] = block_cap, entry_cap, halo_cap.  Synchronises
+ * `stream` (set-up, once per pattern).  YS_ERR_CAPACITY when a tile has more
+ * than 4096 entries, 512 distinct columns or 32768 stream slots (the tiled
+ * SpMV then stays the product of the FP32 loop); YS_ERR_INVALID when the
+ * blocks are not (row, col)-sorted along the row plan.  No counterpart in
+ * the reference.                                                          */
+int32_t ys_spmv_stream_plan(const uint32_t* row_ptr, const uint32_t* entry_block,
+                            const uint32_t* entry_col, const uint32_t* row_block, uint32_t num_vars,
+                            uint64_t capacity_words, uint32_t* desc, uint32_t* rows, uint32_t* words,
+                            uint32_t* halo, uint32_t* src, uint32_t* caps_host, void* stream);
+
+/* blocks32[9 s + k] = values32[12 src[s] + k] for every slot s < slots with
+ * a block (zeros elsewhere): the streamed plan's packed FP32 blocks, current
+ * after each update of values32.  slots = ys_spmv_stream_words (a multiple
+ * of 4); src and blocks32 16-byte aligned.  No counterpart in the
+ * reference.                                                              */
+int32_t ys_spmv_stream_fill(const float* values32, const uint32_t* src, uint64_t slots, float* blocks32,
+                            void* stream);
+
+/* ys_spmv3_x32 over a streamed-tile plan: persistent CTAs stage each tile's
+ * packed blocks, entry words, distinct columns and row offsets into shared
+ * memory with bulk copies (cp.async.bulk, mbarrier completion, a ring of
+ * `stages` buffers: 2 or 3, 0 = three when three CTAs still share an SM,
+ * else two) and gather the tile's distinct neighbour vectors once
+ * (cp.async), so every block read is a streamed HBM read and no neighbour is
+ * fetched twice by a tile.  Bit-identical to ys_spmv3_x32.  The row plan
+ * (values32, row_ptr, entry_block, entry_col) is read instead by a CTA whose
+ * copy wait ran out (`stage_status` OR-ed with 1; the result is the same).
+ * max_ctas > 0 caps the grid (tests: several tiles a CTA).  Replaces the
+ * reference's `yasps_mas_specialized_fine_block_spmv`
+ * (PKG/solver/mas/cuda/block_spmv.cu:279-398).                            */
+int32_t ys_spmv3_x32_streamed(const ys_spmv_stream* plan, const float* values32, const uint32_t* row_ptr,
+                              const uint32_t* entry_block, const uint32_t* entry_col, uint32_t num_vars,
+                              const float* x32, double* y, int32_t beta, uint32_t stages,
+                              uint32_t max_ctas, uint32_t* stage_status, void* stream);
+
 /* ---- preconditioned CG ----------------------------------------------------- */
 
 #define YS_PREC_BLOCK_JACOBI 0
@@ -585,6 +645,10 @@ typedef struct ys_matrix3 {
   const uint32_t* row_block[2];
   uint32_t tile_cap[2];
   uint32_t entry_cap[2];
+  /* optional streamed-tile plan of each set (ys_spmv_stream_plan, blocks
+   * current with values32); with one set and FP32 blocks the PCG loop runs
+   * ys_spmv3_x32_streamed in preference to the tiled SpMV.               */
+  ys_spmv_stream stream[2];
 } ys_matrix3;
 
 typedef struct ys_pcg_args {

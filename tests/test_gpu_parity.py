@@ -113,6 +113,7 @@ def test_spmv_fp64_and_fp32(c0):
   assert np.array_equal(y.cpu().numpy(), y32)
   # the tiled SpMV (shared-memory stages by bulk copies) gives the same bits
   check_tiled_spmv(H, x32, y.cpu().numpy())
+  check_streamed_spmv(H, x32, y.cpu().numpy())
 
 
 def check_tiled_spmv(H, x32, expected):
@@ -140,6 +141,91 @@ def check_tiled_spmv(H, x32, expected):
   assert int(status.item()) == 0
 
 
+def check_streamed_spmv(H, x32, expected):
+  """The streamed-tile plan against the row plan (every entry word decodes
+  to its entry's neighbour, block and orientation; the distinct columns of
+  each tile are its entries' columns, ascending) and the streamed SpMV
+  against ``expected`` bit for bit, with the grid capped so that CTAs loop
+  over several tiles."""
+  import torch
+  from yasps_b200 import _lib as L
+  nv = H.rows // 3
+  (bs,) = H.block_sets
+  row_ptr, eb, ec = H.spmv_plan(bs)
+  sp = H.stream_plan(bs)
+  assert sp is not None
+  rp = row_ptr.cpu().numpy().astype(np.int64)[:nv + 1]
+  ebn = eb.cpu().numpy().view(np.uint32).astype(np.int64)
+  ecn = ec.cpu().numpy().astype(np.int64)
+  desc = sp.desc.cpu().numpy().view(np.uint32).astype(np.int64).reshape(-1, 4)
+  rows = sp.rows.cpu().numpy().view(np.uint32).astype(np.int64).reshape(-1, 68)
+  words = sp.words.cpu().numpy().view(np.uint32).astype(np.int64)
+  halo = sp.halo.cpu().numpy().view(np.uint32).astype(np.int64)
+  src = sp.src.cpu().numpy().view(np.uint32).astype(np.int64)
+  R = L.YS_SPMV_TILE_ROWS
+  ntiles = (nv + R - 1) // R
+  for t in range(ntiles):
+    r0, r1 = t * R, min(t * R + R, nv)
+    base, nslots, ne, nh = desc[t]
+    assert base % 4 == 0 and base == (rp[r0] + 4 * t + 3) & ~3 and ne == rp[r1] - rp[r0]
+    assert np.array_equal(rows[t, :r1 - r0 + 1], rp[r0:r1 + 1] - rp[r0]) and rows[t, 65] == nh
+    cols = ecn[rp[r0]:rp[r1]]
+    assert np.array_equal(halo[base:base + nh], np.unique(cols))
+    w = words[base:base + ne]
+    assert np.array_equal(halo[base + (w & 0xffff)], cols)
+    slot = (w >> 16) & 0x7fff
+    assert slot.max() < nslots
+    assert np.array_equal(src[base + slot], ebn[rp[r0]:rp[r1]] & 0x7fffffff)
+    assert np.array_equal(w >> 31, ebn[rp[r0]:rp[r1]] >> 31)
+  assert sp.block_cap == max(((int(d[1]) + 3) & ~3) for d in desc[:ntiles])
+  status = torch.zeros(1, dtype=torch.int32, device="cuda")
+  y = torch.full((H.rows,), np.nan, dtype=torch.float64, device="cuda")
+  st = sp.struct()
+  for stages, max_ctas in ((0, 0), (2, 1), (3, 1), (2, 3), (3, 3), (0, 0)):
+    L.call("ys_spmv3_x32_streamed", st, L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32),
+           L.ptr(y), 0, stages, max_ctas, L.ptr(status), L.stream_ptr())
+    assert np.array_equal(y.cpu().numpy(), expected)
+  # beta = 1 adds to y
+  L.call("ys_spmv3_x32_streamed", st, L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32),
+         L.ptr(y), 1, 0, 0, L.ptr(status), L.stream_ptr())
+  assert np.array_equal(y.cpu().numpy(), expected + expected)
+  assert int(status.item()) == 0
+
+
+def test_streamed_pcg_matches_tiled_pcg_bit_for_bit():
+  """The FP32 MAS-PCG loop over the streamed-tile SpMV and over the tiled
+  SpMV (same products): the same iterations and the same solution bits;
+  the packed blocks follow a new assembly of the values."""
+  import torch
+  from yasps_b200 import _lib as L
+  cube = scenes.fem_cube(16, spacing=0.1, young=1e6, poisson=0.45, noise=0.005, seed=3)
+  sc, _ = build(cube, "mas", mixed_spmv=True, stop_rule="residual")
+  solver = sc.minimizer.linearSolver
+  mas = solver.implementation
+  H = sc.minimizer.computeNumericValue()
+  H.ensure_fp32()
+  (bs,) = H.block_sets
+  solver.computeSolution(H, H.gradient, None, tolerance=1e-6, maxIterations=2000, zero_initial_guess=True)
+  runs = []
+  for use_stream in (True, False, True):
+    if use_stream:
+      bs.stream = None  # rebuilt
+    else:
+      bs.stream = False  # no streamed plan: the tiled SpMV
+    z = torch.zeros(H.rows, dtype=torch.float64, device="cuda")
+    res = mas._run_pcg(H, H.gradient.value, z, True, L.YS_PREC_MAS, None, mas._mas, 1e-30, 30, True, "residual")
+    runs.append((int(res.iterations), z.cpu().numpy().copy()))
+  assert runs[0][0] == runs[1][0] == 30
+  assert np.array_equal(runs[0][1], runs[1][1]) and np.array_equal(runs[0][1], runs[2][1])
+  # new FP32 values (a new version) refresh the packed blocks before use
+  sp = H.stream_plan(bs)
+  before = sp.blocks32.clone()
+  bs.values32.mul_(2.0)
+  H.values32_version += 1
+  assert H.stream_plan(bs) is sp
+  assert torch.equal(sp.blocks32, before * 2.0)
+
+
 def test_tiled_spmv_many_tiles_bit_identical():
   """A 24^3 cube (13,248 free variables, 207 tiles of 64 rows) through the
   tiled SpMV against the row-plan SpMV, bit for bit, and the FP32 loop that
@@ -160,6 +246,7 @@ def test_tiled_spmv_many_tiles_bit_identical():
   L.call("ys_spmv3_x32", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32), L.ptr(y), 0,
          L.stream_ptr())
   check_tiled_spmv(H, x32, y.cpu().numpy())
+  check_streamed_spmv(H, x32, y.cpu().numpy())
   ora = OracleCube(cube)
   segs = sc.minimizeEnergy(tolerance=1e-6, maxIterations=2000)
   assert solvers.relative_residual(ora.matvec, ora.gradient, segs[0].cpu().numpy()) <= 1e-6

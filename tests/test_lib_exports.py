@@ -57,7 +57,7 @@ def test_ctypes_structs_follow_header_field_order():
            "ys_snh_args": _lib.SnhArgs, "ys_inertia_args": _lib.InertiaArgs, "ys_matrix3": _lib.Matrix3,
            "ys_pcg_args": _lib.PcgArgs, "ys_pcg_result": _lib.PcgResult, "ys_mas_desc": _lib.MasDesc,
            "ys_serve_slot_desc": _lib.ServeSlotDesc, "ys_energy_args": _lib.EnergyArgs, "ys_affine_args": _lib.AffineArgs,
-           "ys_coupled_args": _lib.CoupledArgs,
+           "ys_coupled_args": _lib.CoupledArgs, "ys_spmv_stream": _lib.SpmvStream,
            "ys_serve_slot_status": _lib.ServeSlotStatus}
   for cname, cls in pairs.items():
     assert structs[cname] == [f[0] for f in cls._fields_], cname

@@ -85,10 +85,15 @@ class CoupledArgs(C.Structure):
               ("translation", vp), ("num_bodies", u32), ("status", vp)]
 
 
+class SpmvStream(C.Structure):
+  _fields_ = [("blocks32", vp), ("desc", vp), ("rows", vp), ("words", vp), ("halo", vp), ("block_cap", u32),
+              ("entry_cap", u32), ("halo_cap", u32)]
+
+
 class Matrix3(C.Structure):
   _fields_ = [("num_sets", u32), ("values", vp * 2), ("values32", vp * 2), ("row_ptr", vp * 2),
               ("entry_block", vp * 2), ("entry_col", vp * 2), ("num_vars", u32), ("row_block", vp * 2),
-              ("tile_cap", u32 * 2), ("entry_cap", u32 * 2)]
+              ("tile_cap", u32 * 2), ("entry_cap", u32 * 2), ("stream", SpmvStream * 2)]
 
 
 class PcgArgs(C.Structure):
@@ -167,6 +172,10 @@ SIGNATURES = {
     "ys_spmv3_x32": (i32, [vp, vp, vp, vp, u32, vp, vp, i32, vp]),
     "ys_spmv_tile_plan": (i32, [vp, u32, vp, vp, u32, vp, P(u32), P(u32), vp]),
     "ys_spmv3_x32_tiled": (i32, [vp, vp, vp, vp, vp, u32, u32, u32, u32, vp, vp, i32, vp, vp]),
+    "ys_spmv_stream_words": (i32, [u32, u32, P(u64)]),
+    "ys_spmv_stream_plan": (i32, [vp, vp, vp, vp, u32, u64, vp, vp, vp, vp, vp, P(u32), vp]),
+    "ys_spmv_stream_fill": (i32, [vp, vp, u64, vp, vp]),
+    "ys_spmv3_x32_streamed": (i32, [P(SpmvStream), vp, vp, vp, vp, u32, vp, vp, i32, u32, u32, vp, vp]),
     "ys_pcg_workspace_doubles": (u64, [u32]),
     "ys_pcg_create": (i32, [P(PcgArgs), P(vp)]),
     "ys_pcg_run": (i32, [vp, vp, P(PcgResult)]),

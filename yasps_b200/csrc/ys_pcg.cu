@@ -17,7 +17,7 @@
 
 #include "ys_mas.cuh"
 #include "ys_pcg.cuh"
-#include "ys_spmv_tiled.cuh"
+#include "ys_spmv_stream.cuh"
 
 namespace ys {
 
@@ -41,6 +41,7 @@ struct PcgParams {
   int zero_guess;
   int restart_on_curvature;  // MAS: a non-positive curvature restarts from M^-1 r (zero step, beta = 0)
   TiledSet tiled;            // tile plan of the FP32 set (pcg_spmv_dot_tiled)
+  StreamSet streamed;        // streamed-tile plan of the FP32 set (pcg_spmv_dot_streamed)
   const uint32_t* jgroup;    // block-Jacobi groups (first var | size << 30) or null: 3x3 blocks
   double tolerance;
   uint32_t max_it;
@@ -217,6 +218,24 @@ __global__ void __launch_bounds__(kTileThreads, 3) pcg_spmv_dot_tiled(PcgParams 
     P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
     v[0] += P.p[3ull * i] * q0 + P.p[3ull * i + 1] * q1 + P.p[3ull * i + 2] * q2;
   });
+  spmv_dot_finish<kTileThreads>(P, v);
+}
+
+// The same over the streamed-tile plan (see ys_spmv_stream.cuh).
+__global__ void __launch_bounds__(kTileThreads, 2) pcg_spmv_dot_streamed(PcgParams P) {
+  double v[1] = {0.0};
+  double pp[3] = {0.0, 0.0, 0.0};  // p of the row, loaded before its products
+  spmv3_stream_x32(
+      P.streamed, P.p32, P.tickets + 6,
+      [&](uint32_t i, bool valid, int lane) {
+        if (valid && lane == 0)
+          for (int c = 0; c < 3; ++c) pp[c] = P.p[3ull * i + c];
+      },
+      [&](uint32_t i, bool valid, int lane, double q0, double q1, double q2) {
+        if (!valid || lane != 0) return;
+        P.q[3ull * i] = q0; P.q[3ull * i + 1] = q1; P.q[3ull * i + 2] = q2;
+        v[0] += pp[0] * q0 + pp[1] * q1 + pp[2] * q2;
+      });
   spmv_dot_finish<kTileThreads>(P, v);
 }
 
@@ -490,10 +509,30 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
   }
   // the FP32 loop of a single block set with a tile plan runs the tiled
   // SpMV (persistent CTAs, shared-memory stages)
-  bool tiled = false;
+  bool tiled = false, streamed = false;
   size_t tile_smem = 0;
   unsigned grid_tiles = 0;
-  if (P.fp32 && P.nsets == 1 && a.matrix.row_block[0] && a.matrix.tile_cap[0] > 0 && a.matrix.entry_cap[0] > 0) {
+  const ys_spmv_stream& sp = a.matrix.stream[0];
+  if (P.fp32 && P.nsets == 1 && sp.blocks32 && sp.desc && sp.rows && sp.words && sp.halo && sp.block_cap > 0 &&
+      sp.entry_cap > 0 && sp.halo_cap > 0 && sp.halo_cap <= ys::kStreamMaxHalo && sp.block_cap % 4 == 0 &&
+      sp.entry_cap % 4 == 0 && sp.halo_cap % 4 == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    const uint32_t stages = ys::stream_pick_stages((const void*)ys::pcg_spmv_dot_streamed, sp.block_cap,
+                                                   sp.entry_cap, sp.halo_cap, &per_sm);
+    tile_smem = ys::stream_smem_bytes(sp.block_cap, sp.entry_cap, sp.halo_cap, stages ? stages : 2);
+    if (stages && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaFuncSetAttribute(ys::pcg_spmv_dot_streamed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tile_smem) == cudaSuccess &&
+        sms > 0 && per_sm > 0) {
+      const unsigned ntiles = (P.nv + ys::kTileRows - 1) / ys::kTileRows;
+      grid_tiles = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
+      streamed = true;
+      P.streamed = ys::stream_set(sp, P.sets[0], P.nv, stages);
+    }
+  }
+  if (!streamed && P.fp32 && P.nsets == 1 && a.matrix.row_block[0] && a.matrix.tile_cap[0] > 0 &&
+      a.matrix.entry_cap[0] > 0) {
     int dev = 0, sms = 0, per_sm = 0, smem_sm = 0;
     uint32_t stages = 2;
     if (cudaGetDevice(&dev) == cudaSuccess &&
@@ -565,7 +604,10 @@ int32_t ys_pcg_create(const ys_pcg_args* args, void** handle) {
       cudaGraph_t body = cp.conditional.phGraph_out[0];
       cudaGraphNode_t n1 = nullptr, n2 = nullptr, n3 = nullptr;
       void* args1[] = {&P};
-      if (tiled)
+      if (streamed)
+        e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot_streamed, grid_tiles,
+                           ys::kTileThreads, args1, tile_smem);
+      else if (tiled)
         e = ys::add_kernel(body, &n1, nullptr, 0, (const void*)ys::pcg_spmv_dot_tiled, grid_tiles, ys::kTileThreads,
                            args1, tile_smem);
       else

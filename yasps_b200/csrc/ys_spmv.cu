@@ -2,7 +2,7 @@
 #include <cub/cub.cuh>
 
 #include "ys_spmv.cuh"
-#include "ys_spmv_tiled.cuh"
+#include "ys_spmv_stream.cuh"
 
 namespace ys {
 
@@ -144,6 +144,196 @@ __global__ void __launch_bounds__(kTileThreads) spmv3_x32_tiled_kernel(TiledSet 
     y[3ull * i + 1] = y1;
     y[3ull * i + 2] = y2;
   });
+}
+
+// ---- streamed tiles (ys_spmv_stream.cuh) ------------------------------------
+
+// Exclusive block-wide prefix sum over kTileThreads threads; *total gets the sum.
+__device__ __forceinline__ uint32_t tile_scan_exclusive(uint32_t v, uint32_t* wsum, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int w = 0; w < kTileThreads / 32; ++w) {
+      const uint32_t c = wsum[w];
+      wsum[w] = acc;
+      acc += c;
+    }
+    wsum[kTileThreads / 32] = acc;
+  }
+  __syncthreads();
+  const uint32_t r = wsum[warp] + x - v;
+  *total = wsum[kTileThreads / 32];
+  __syncthreads();
+  return r;
+}
+
+// One CTA a tile: the tile's distinct columns (its entry columns sorted in
+// shared memory, duplicates dropped), the cross blocks (transposed entries
+// whose block belongs to an earlier tile) numbered in entry order after the
+// tile's own blocks, and the entry words, row offsets, stream sources and
+// descriptor of the tile.  caps[0] |= 1: a tile has more entries than the
+// sort holds; |= 2: more distinct columns or stream slots than the kernel
+// takes; |= 4: the blocks are not (row, col)-sorted along the row plan.
+// caps[1..3]: the most stream blocks, entries and distinct columns of a
+// tile, each rounded up to a multiple of 4.
+__global__ void __launch_bounds__(kTileThreads) stream_plan_kernel(
+    const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ entry_block,
+    const uint32_t* __restrict__ entry_col, const uint32_t* __restrict__ row_block, uint32_t nv,
+    uint4* __restrict__ desc, uint32_t* __restrict__ rows, uint32_t* __restrict__ words, uint32_t* __restrict__ halo,
+    uint32_t* __restrict__ src, uint32_t* __restrict__ caps) {
+  __shared__ uint32_t key[kStreamMaxEntries];
+  __shared__ uint32_t uniq[kStreamMaxEntries];
+  __shared__ uint32_t wsum[kTileThreads / 32 + 1];
+  constexpr uint32_t kPer = kStreamMaxEntries / kTileThreads;  // consecutive items a thread
+  const uint32_t t = blockIdx.x;
+  const uint32_t r0 = t * kTileRows, r1 = min(r0 + kTileRows, nv);
+  const uint32_t p0 = row_ptr[r0], ne = row_ptr[r1] - p0;
+  const uint32_t base = (p0 + 4u * t + 3u) & ~3u;
+  const uint32_t b0 = row_block[r0], b1 = row_block[r1];
+  // (a tile holds at most one own block per entry: otherwise the plan does
+  // not match the blocks, and nothing is written)
+  if (ne > kStreamMaxEntries || b1 < b0 || b1 - b0 > ne) {
+    if (threadIdx.x == 0) atomicOr(caps, ne > kStreamMaxEntries ? 1u : 4u);
+    return;
+  }
+  const uint32_t own = b1 - b0;
+  uint32_t n = 1;
+  while (n < ne) n <<= 1;
+  for (uint32_t j = threadIdx.x; j < n; j += kTileThreads) key[j] = j < ne ? entry_col[p0 + j] : 0xffffffffu;
+  __syncthreads();
+  for (uint32_t size = 2; size <= n; size <<= 1)
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t j = threadIdx.x; j < n; j += kTileThreads) {
+        const uint32_t q = j ^ stride;
+        if (q > j) {
+          const uint32_t a = key[j], b = key[q];
+          if ((a > b) == ((j & size) == 0)) {
+            key[j] = b;
+            key[q] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  // distinct columns in ascending order
+  const uint32_t j0 = threadIdx.x * kPer;
+  uint32_t cnt = 0;
+  for (uint32_t q = 0; q < kPer; ++q) {
+    const uint32_t j = j0 + q;
+    cnt += (j < ne && (j == 0 || key[j] != key[j - 1])) ? 1u : 0u;
+  }
+  uint32_t nh = 0;
+  uint32_t at = tile_scan_exclusive(cnt, wsum, &nh);
+  for (uint32_t q = 0; q < kPer; ++q) {
+    const uint32_t j = j0 + q;
+    if (j < ne && (j == 0 || key[j] != key[j - 1])) uniq[at++] = key[j];
+  }
+  // cross blocks, numbered in entry order
+  cnt = 0;
+  for (uint32_t q = 0; q < kPer; ++q) {
+    const uint32_t j = j0 + q;
+    if (j < ne) {
+      const uint32_t eb = entry_block[p0 + j];
+      cnt += ((eb >> 31) && (eb & 0x7fffffffu) < b0) ? 1u : 0u;
+    }
+  }
+  uint32_t ncross = 0;
+  uint32_t rank = tile_scan_exclusive(cnt, wsum, &ncross);  // ends with a barrier: uniq is complete
+  const uint32_t nslots = own + ncross;
+  int bad = 0;
+  for (uint32_t q = 0; q < kPer; ++q) {
+    const uint32_t j = j0 + q;
+    if (j >= ne) break;
+    const uint32_t eb = entry_block[p0 + j], col = entry_col[p0 + j];
+    const uint32_t tr = eb >> 31, blk = eb & 0x7fffffffu;
+    const bool cross = tr && blk < b0;
+    if (!cross && (blk < b0 || blk >= b1)) bad = 1;
+    const uint32_t slot = cross ? own + rank++ : blk - b0;
+    uint32_t lo = 0, hi = nh;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (uniq[mid] < col) lo = mid + 1;
+      else hi = mid;
+    }
+    words[base + j] = lo | ((slot & 0x7fffu) << 16) | (tr << 31);
+    if (cross && slot < ne) src[base + slot] = blk;
+  }
+  if (threadIdx.x < 4 && ne + threadIdx.x < round4(ne)) words[base + ne + threadIdx.x] = 0u;
+  for (uint32_t b = b0 + threadIdx.x; b < b1; b += kTileThreads) src[base + (b - b0)] = b;
+  for (uint32_t j = threadIdx.x; j < round4(nh); j += kTileThreads) halo[base + j] = j < nh ? uniq[j] : uniq[0];
+  for (uint32_t k = threadIdx.x; k < kStreamRowWords; k += kTileThreads)
+    rows[(uint64_t)kStreamRowWords * t + k] =
+        k <= kTileRows ? row_ptr[min(r0 + k, r1)] - p0 : (k == kStreamHaloWord ? nh : 0u);
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    desc[t] = make_uint4(base, nslots, ne, nh);
+    if (bad) atomicOr(caps, 4u);
+    if (nh > kStreamMaxHalo || nslots > kStreamMaxSlots) atomicOr(caps, 2u);
+    atomicMax(caps + 1, round4(nslots));
+    atomicMax(caps + 2, round4(ne));
+    atomicMax(caps + 3, round4(nh));
+  }
+}
+
+// stream32[9 s + k] = values32[12 src[s] + k] for every slot with a block,
+// four slots a thread (36 floats: nine 16-byte stores; slots without a block
+// get zeros, which no entry reads).  slots is a multiple of 4.
+__global__ void stream_fill_kernel(const float* __restrict__ values32, const uint32_t* __restrict__ src,
+                                   uint64_t slots, float* __restrict__ stream32) {
+  const uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (4 * q >= slots) return;
+  const uint4 b = reinterpret_cast<const uint4*>(src)[q];
+  const uint32_t bs[4] = {b.x, b.y, b.z, b.w};
+  float v[36];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float w[9];
+    if (bs[k] != kStreamEmpty) {
+      load_block(values32, bs[k], w);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 9; ++j) w[j] = 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) v[9 * k + j] = w[j];
+  }
+  float4* o = reinterpret_cast<float4*>(stream32 + 36ull * q);
+#pragma unroll
+  for (int j = 0; j < 9; ++j) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+}
+
+__device__ unsigned g_stream_stage_status;
+
+__global__ void __launch_bounds__(kTileThreads, 3) spmv3_x32_stream_kernel(StreamSet T, const float4* __restrict__ x32,
+                                                                          double* __restrict__ y, int beta,
+                                                                          unsigned* status) {
+  unsigned* err = status ? status : &g_stream_stage_status;
+  double old[3] = {0.0, 0.0, 0.0};
+  spmv3_stream_x32(
+      T, x32, err,
+      [&](uint32_t i, bool valid, int lane) {
+        if (beta && valid && lane == 0)
+          for (int c = 0; c < 3; ++c) old[c] = y[3ull * i + c];
+      },
+      [&](uint32_t i, bool valid, int lane, double y0, double y1, double y2) {
+        if (!valid || lane != 0) return;
+        if (beta) {
+          y0 += old[0];
+          y1 += old[1];
+          y2 += old[2];
+        }
+        y[3ull * i] = y0;
+        y[3ull * i + 1] = y1;
+        y[3ull * i + 2] = y2;
+      });
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -301,6 +491,97 @@ int32_t ys_spmv3_x32_tiled(const float* values32, const uint32_t* row_ptr, const
   const unsigned grid = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
   ys::TiledSet T{values32, row_ptr, entry_block, entry_col, row_block, num_vars, tile_cap, entry_cap, stages};
   ys::spmv3_x32_tiled_kernel<<<grid, ys::kTileThreads, smem, (cudaStream_t)stream>>>(
+      T, reinterpret_cast<const float4*>(x32), y, beta, stage_status);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+
+int32_t ys_spmv_stream_words(uint32_t num_entries, uint32_t num_vars, uint64_t* words) {
+  YS_REQUIRE(words, YS_ERR_INVALID, "null argument");
+  *words = ys::stream_words(num_entries, num_vars);
+  return YS_OK;
+}
+
+int32_t ys_spmv_stream_plan(const uint32_t* row_ptr, const uint32_t* entry_block, const uint32_t* entry_col,
+                            const uint32_t* row_block, uint32_t num_vars, uint64_t capacity_words, uint32_t* desc,
+                            uint32_t* rows, uint32_t* words, uint32_t* halo, uint32_t* src, uint32_t* caps_host,
+                            void* stream) {
+  YS_REQUIRE(row_ptr && entry_block && entry_col && row_block && desc && rows && words && halo && src && caps_host,
+             YS_ERR_INVALID, "null argument");
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(words) & 15) == 0 && (reinterpret_cast<uintptr_t>(halo) & 15) == 0 &&
+                 (reinterpret_cast<uintptr_t>(rows) & 15) == 0 && (reinterpret_cast<uintptr_t>(desc) & 15) == 0,
+             YS_ERR_INVALID, "desc, rows, words and halo must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  caps_host[0] = caps_host[1] = caps_host[2] = 0;
+  if (num_vars == 0) return YS_OK;
+  uint32_t total = 0;
+  YS_CUDA_TRY(cudaMemcpyAsync(&total, row_ptr + num_vars, 4, cudaMemcpyDeviceToHost, s));
+  YS_CUDA_TRY(cudaStreamSynchronize(s));
+  YS_REQUIRE(capacity_words >= ys::stream_words(total, num_vars), YS_ERR_CAPACITY, "stream plan arrays too small");
+  const uint32_t ntiles = (num_vars + ys::kTileRows - 1) / ys::kTileRows;
+  uint32_t* caps = desc + 4ull * ntiles;  // the descriptor array's last uint4
+  YS_CUDA_TRY(cudaMemsetAsync(caps, 0, 16, s));
+  YS_CUDA_TRY(cudaMemsetAsync(src, 0xff, 4ull * capacity_words, s));
+  ys::stream_plan_kernel<<<ntiles, ys::kTileThreads, 0, s>>>(row_ptr, entry_block, entry_col, row_block, num_vars,
+                                                            reinterpret_cast<uint4*>(desc), rows, words, halo, src,
+                                                            caps);
+  YS_CHECK_LAUNCH();
+  uint32_t h[4] = {0, 0, 0, 0};
+  YS_CUDA_TRY(cudaMemcpyAsync(h, caps, sizeof(h), cudaMemcpyDeviceToHost, s));
+  YS_CUDA_TRY(cudaStreamSynchronize(s));
+  YS_REQUIRE(!(h[0] & 4u), YS_ERR_INVALID, "blocks are not (row, col)-sorted along the row plan");
+  YS_REQUIRE(h[0] == 0, YS_ERR_CAPACITY, "a tile exceeds the streamed SpMV's entry, column or slot limits");
+  caps_host[0] = h[1];
+  caps_host[1] = h[2];
+  caps_host[2] = h[3];
+  return YS_OK;
+}
+
+int32_t ys_spmv_stream_fill(const float* values32, const uint32_t* src, uint64_t slots, float* blocks32,
+                            void* stream) {
+  YS_REQUIRE(values32 && src && blocks32, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(values32) & 15) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0 &&
+                 (reinterpret_cast<uintptr_t>(blocks32) & 15) == 0 && slots % 4 == 0,
+             YS_ERR_INVALID, "values32, src and blocks32 16-byte aligned, slots a multiple of 4");
+  if (slots == 0) return YS_OK;
+  ys::stream_fill_kernel<<<ys::grid_for(slots / 4, 256), 256, 0, (cudaStream_t)stream>>>(values32, src, slots,
+                                                                                      blocks32);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_spmv3_x32_streamed(const ys_spmv_stream* plan, const float* values32, const uint32_t* row_ptr,
+                              const uint32_t* entry_block, const uint32_t* entry_col, uint32_t num_vars,
+                              const float* x32, double* y, int32_t beta, uint32_t stages, uint32_t max_ctas,
+                              uint32_t* stage_status, void* stream) {
+  YS_REQUIRE(plan && values32 && x32 && row_ptr && entry_block && entry_col, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(x32) & 15) == 0 && (reinterpret_cast<uintptr_t>(values32) & 15) == 0,
+             YS_ERR_INVALID, "values32 and x32 must be 16-byte aligned");
+  if (num_vars == 0) return YS_OK;
+  YS_REQUIRE(plan->blocks32 && plan->desc && plan->rows && plan->words && plan->halo && plan->block_cap % 4 == 0 &&
+                 plan->entry_cap % 4 == 0 && plan->halo_cap % 4 == 0 && plan->halo_cap <= ys::kStreamMaxHalo,
+             YS_ERR_INVALID, "no stream plan");
+  YS_REQUIRE(stages == 0 || stages == 2 || stages == 3, YS_ERR_INVALID, "stages: 0 (auto), 2 or 3");
+  int dev = 0, sms = 0, per_sm = 0;
+  YS_CUDA_TRY(cudaGetDevice(&dev));
+  YS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (stages == 0)
+    stages = ys::stream_pick_stages((const void*)ys::spmv3_x32_stream_kernel, plan->block_cap, plan->entry_cap,
+                                    plan->halo_cap, &per_sm);
+  YS_REQUIRE(stages != 0, YS_ERR_CAPACITY, "a tile's stream exceeds the shared-memory stages");
+  const size_t smem = ys::stream_smem_bytes(plan->block_cap, plan->entry_cap, plan->halo_cap, stages);
+  YS_REQUIRE(smem <= 220u * 1024u, YS_ERR_CAPACITY, "a tile's stream exceeds the shared-memory stages");
+  YS_CUDA_TRY(cudaFuncSetAttribute(ys::spmv3_x32_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  YS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ys::spmv3_x32_stream_kernel, ys::kTileThreads,
+                                                            smem));
+  YS_REQUIRE(per_sm > 0, YS_ERR_CAPACITY, "streamed SpMV does not fit on an SM");
+  const uint32_t ntiles = (num_vars + ys::kTileRows - 1) / ys::kTileRows;
+  unsigned grid = std::min<unsigned>(ntiles, (unsigned)(sms * per_sm));
+  if (max_ctas) grid = std::min<unsigned>(grid, max_ctas);
+  ys::StreamSet T =
+      ys::stream_set(*plan, ys::SpmvSet{nullptr, values32, row_ptr, entry_block, entry_col}, num_vars, stages);
+  ys::spmv3_x32_stream_kernel<<<grid, ys::kTileThreads, smem, (cudaStream_t)stream>>>(
       T, reinterpret_cast<const float4*>(x32), y, beta, stage_status);
   YS_CHECK_LAUNCH();
   return YS_OK;

@@ -403,6 +403,27 @@ class _Pattern:
     self.all3 = nc == 1 and self.category_dims == [3, 3]
 
 
+class _StreamPlan:
+  """Device arrays of a streamed-tile SpMV plan (``ys_spmv_stream_plan``)
+  and the packed FP32 blocks it streams (``ys_spmv_stream_fill``)."""
+
+  def __init__(self, desc, rows, words, halo, src, blocks32, caps, slots):
+    self.desc, self.rows, self.words, self.halo, self.src, self.blocks32 = desc, rows, words, halo, src, blocks32
+    self.block_cap, self.entry_cap, self.halo_cap = caps
+    self.slots = slots
+    self.filled = None  # values32 version the blocks were packed from
+
+  def struct(self):
+    st = L.SpmvStream()
+    st.blocks32, st.desc, st.rows = L.ptr(self.blocks32), L.ptr(self.desc), L.ptr(self.rows)
+    st.words, st.halo = L.ptr(self.words), L.ptr(self.halo)
+    st.block_cap, st.entry_cap, st.halo_cap = self.block_cap, self.entry_cap, self.halo_cap
+    return st
+
+  def pointers(self):
+    return (self.blocks32.data_ptr(), self.desc.data_ptr(), self.words.data_ptr())
+
+
 class _BlockSet:
   def __init__(self):
     self.terms: List[_Term] = []
@@ -413,6 +434,7 @@ class _BlockSet:
     self.infos = []
     self.spmv = None  # (row_ptr, entry_block, entry_col)
     self.tiles = None  # (row_block, tile capacity) of the tiled SpMV, or (None, 0)
+    self.stream = None  # _StreamPlan of the streamed-tile SpMV, False when the set has none
 
 
 class hessian:
@@ -439,6 +461,9 @@ class hessian:
     self.want_diagonal = False
     self._diag_stale = True
     self.values32_current = False
+    # bumped whenever the FP32 block values change (the streamed SpMV's
+    # packed copy is refreshed from them before the next FP32 solve)
+    self.values32_version = 0
     self.gradient: Optional[vector] = None
     self._diagonal = None
     self._diagonal_blocks = None
@@ -585,6 +610,7 @@ class hessian:
     if self.want_diagonal:
       self._extract_diagonal()
     self.values32_current = self.want_fp32
+    self.values32_version += 1
     return self
 
   def term_energies(self):
@@ -815,6 +841,7 @@ class hessian:
       v[:nu, :9] = bs.values[:9 * nu].view(nu, 9).to(torch.float32)
       bs.values32 = v.reshape(-1)
     self.values32_current = True
+    self.values32_version += 1
 
   def spmv_plan(self, bs: _BlockSet):
     """Row plan of a 3x3 block set for the deterministic SpMV."""
@@ -837,6 +864,7 @@ class hessian:
            L.ptr(eb), L.ptr(ec), L.stream_ptr())
     bs.spmv = (row_ptr, eb, ec)
     bs.tiles = None
+    bs.stream = None
     return bs.spmv
 
   def tile_plan(self, bs: _BlockSet):
@@ -855,6 +883,44 @@ class hessian:
                   ok=(L.YS_OK, L.YS_ERR_INVALID))
       bs.tiles = (row_block, int(cap.value), int(ecap.value)) if rc == L.YS_OK else (None, 0, 0)
     return bs.tiles
+
+  def stream_plan(self, bs: _BlockSet):
+    """The streamed-tile SpMV plan of a 3x3 block set with FP32 values
+    (``ys_spmv_stream_plan``), its packed blocks current with the FP32
+    values; None when the set has no FP32 values or no such plan (a tile
+    beyond the plan's limits: the tiled SpMV stays in use)."""
+    import ctypes
+    torch = _torch()
+    if bs.values32 is None:
+      return None
+    row_ptr, eb, ec = self.spmv_plan(bs)
+    row_block, cap, _ = self.tile_plan(bs)
+    if bs.stream is None:
+      bs.stream = False
+      if row_block is not None and cap > 0:
+        nv = self.rows // 3
+        entries = int(row_ptr[nv].item())
+        words = L.u64(0)
+        L.call("ys_spmv_stream_words", entries, nv, ctypes.byref(words))
+        nw = int(words.value)
+        ntiles = (nv + L.YS_SPMV_TILE_ROWS - 1) // L.YS_SPMV_TILE_ROWS
+        i32 = lambda k: torch.zeros(k, dtype=torch.int32, device=_dev())
+        desc, rows, wd, halo, src = i32(4 * (ntiles + 1)), i32(68 * ntiles), i32(nw), i32(nw), i32(nw)
+        caps = (L.u32 * 3)()
+        rc = L.call("ys_spmv_stream_plan", L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block), nv, nw,
+                    L.ptr(desc), L.ptr(rows), L.ptr(wd), L.ptr(halo), L.ptr(src), caps, L.stream_ptr(),
+                    ok=(L.YS_OK, L.YS_ERR_CAPACITY))
+        if rc == L.YS_OK:
+          blocks32 = torch.zeros(9 * nw, dtype=torch.float32, device=_dev())
+          bs.stream = _StreamPlan(desc, rows, wd, halo, src, blocks32, tuple(int(c) for c in caps), nw)
+    sp = bs.stream
+    if not sp:
+      return None
+    if sp.filled != (self.values32_version, bs.values32.data_ptr()):
+      L.call("ys_spmv_stream_fill", L.ptr(bs.values32), L.ptr(sp.src), sp.slots, L.ptr(sp.blocks32),
+             L.stream_ptr())
+      sp.filled = (self.values32_version, bs.values32.data_ptr())
+    return sp
 
   def spmv(self, direction: vector, transpose: bool = False, fp32: bool = False) -> vector:
     """``H x`` (symmetric, so ``transpose`` gives the same product)."""
@@ -880,5 +946,8 @@ class hessian:
       m.row_ptr[k], m.entry_block[k], m.entry_col[k] = L.ptr(row_ptr), L.ptr(eb), L.ptr(ec)
       row_block, cap, ecap = self.tile_plan(bs)
       m.row_block[k], m.tile_cap[k], m.entry_cap[k] = L.ptr(row_block), cap, ecap
+      sp = self.stream_plan(bs)
+      if sp is not None:
+        m.stream[k] = sp.struct()
     m.num_vars = self.rows // 3
     return m

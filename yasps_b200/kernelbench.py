@@ -132,6 +132,21 @@ def main():
     L.call("ys_spmv3_x32_tiled", L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block),
            tile_cap, entry_cap, stages, nv, L.ptr(x32), L.ptr(y), 0, None, st)
 
+  sp = H.stream_plan(bs)
+  sps = sp.struct() if sp is not None else None
+
+  def streamed(stages):
+    L.call("ys_spmv3_x32_streamed", sps, L.ptr(bs.values32), L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), nv, L.ptr(x32),
+           L.ptr(y), 0, stages, 0, None, st)
+
+  def pcg_without_stream():
+    keep = bs.stream
+    bs.stream = False
+    try:
+      mas._run_pcg(H, H.gradient.value, z, True, L.YS_PREC_MAS, None, mas._mas, 1e-30, 50, True, "residual")
+    finally:
+      bs.stream = keep
+
   cases = {
       "snh_eval_only": lambda: snh_eval(0),
       "snh_eval_project": lambda: snh_eval(1),
@@ -148,12 +163,19 @@ def main():
       "spmv_fp32_tiled_s2": lambda: tiled(2),
       "spmv_fp32_tiled_s3": lambda: tiled(3),
       "spmv_fp32_tiled_s4": lambda: tiled(4),
+      "spmv_fp32_stream": lambda: streamed(0),
+      "spmv_fp32_stream_s2": lambda: streamed(2),
+      "spmv_fp32_stream_s3": lambda: streamed(3),
+      "stream_fill": lambda: L.call("ys_spmv_stream_fill", L.ptr(bs.values32), L.ptr(sp.src), sp.slots,
+                                    L.ptr(sp.blocks32), st),
       "mas_apply": lambda: L.call("ys_mas_apply", mas._mas, L.ptr(x), L.ptr(z), st),
       "gemv": lambda: L.call("ys_mas_gemv", mas._mas, st, None),
       "newton_step": lambda: mz.computeHessianAndGradient(tolerance=1e-6, maxIterations=2000),
       # 50 MAS-PCG iterations (unreachable tolerance) from one graph launch
       "pcg50_fp32": lambda: mas._run_pcg(H, H.gradient.value, z, True, L.YS_PREC_MAS, None, mas._mas, 1e-30, 50,
                                          True, "residual"),
+      # the same loop over the tiled SpMV (no streamed-tile plan)
+      "pcg50_fp32_tiled": lambda: pcg_without_stream(),
       "pcg50_fp64": lambda: mas._run_pcg(H, H.gradient.value, z, False, L.YS_PREC_MAS, None, mas._mas, 1e-30, 50,
                                          True, "residual"),
   }
@@ -166,7 +188,7 @@ def main():
          "gemv_alg_bytes": int(nbytes.value), "gemv_layout_bytes": gemv_layout_bytes(mas._tables),
          "non_psd": int(snh._const_cache[("work", snh.n)][1].item()), "pcg": mz.linearSolver.statistics}
   for name, fn in cases.items():
-    if args.kernel in ("all", name):
+    if args.kernel == "all" or name in args.kernel.split(","):
       out[name + "_ms"] = _time(fn, args.reps if name != "newton_step" else max(2, args.reps // 5))
   print(json.dumps(out))
 

@@ -92,9 +92,13 @@ class _PcgBase:
     """One device PCG solve into ``x``; returns the ys_pcg_result."""
     # the graph holds every device pointer of the matrix: a rebuilt pattern
     # (dynamic terms) gives new row plans and must give a new graph
+    # (an FP32 solve first refreshes the streamed SpMV's packed blocks from
+    # the current FP32 values; the graph holds the plan's pointers)
+    streams = [H.stream_plan(bs) if fp32 else None for bs in H.block_sets]
     plans = tuple(tuple(t.data_ptr() for t in H.spmv_plan(bs)) + (bs.pattern.num_unique,) +
-                  tuple(0 if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else t) for t in H.tile_plan(bs))
-                  for bs in H.block_sets)
+                  tuple(0 if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else t) for t in H.tile_plan(bs)) +
+                  (sp.pointers() if sp is not None else ())
+                  for bs, sp in zip(H.block_sets, streams))
     key = (id(H), H.rows, rhs.data_ptr(), x.data_ptr(), fp32, prec_kind, None if jinv is None else jinv.data_ptr(),
            mas_handle, bool(zero_guess), stop_rule, None if jgroup is None else jgroup.data_ptr(),
            tuple(bs.values.data_ptr() for bs in H.block_sets),
