@@ -194,8 +194,9 @@ def check_streamed_spmv(H, x32, expected):
 
 def test_streamed_pcg_matches_tiled_pcg_bit_for_bit():
   """The FP32 MAS-PCG loop over the streamed-tile SpMV and over the tiled
-  SpMV (same products): the same iterations and the same solution bits;
-  the packed blocks follow a new assembly of the values."""
+  SpMV (same products; one tile a CTA in both grids here, so the curvature
+  sums group alike): the same iterations and the same solution bits; the
+  packed blocks follow new FP32 values."""
   import torch
   from yasps_b200 import _lib as L
   cube = scenes.fem_cube(16, spacing=0.1, young=1e6, poisson=0.45, noise=0.005, seed=3)
