@@ -586,6 +586,8 @@ int32_t ys_spmv_stream_words(uint32_t num_entries, uint32_t num_vars, uint64_t* 
  * ys_spmv_tile_plan's row_block: desc [4 * (tiles + 1)] words, rows
  * [68 * tiles], words / halo / src [capacity_words] (>= ys_spmv_stream_words),
  * all 16-byte aligned; src[s] = the stored block of stream slot s (or
+ * 0xffffffff); slot_of [2 * num_blocks] (8-byte aligned) = each stored
+ * block's slot in its row's tile and its cross slot in a later tile (or
  * 0xffffffff).  caps_host[3] = block_cap, entry_cap, halo_cap.  Synchronises
  * `stream` (set-up, once per pattern).  YS_ERR_CAPACITY when a tile has more
  * than 4096 entries, 512 distinct columns or 32768 stream slots (the tiled
@@ -595,7 +597,17 @@ int32_t ys_spmv_stream_words(uint32_t num_entries, uint32_t num_vars, uint64_t* 
 int32_t ys_spmv_stream_plan(const uint32_t* row_ptr, const uint32_t* entry_block,
                             const uint32_t* entry_col, const uint32_t* row_block, uint32_t num_vars,
                             uint64_t capacity_words, uint32_t* desc, uint32_t* rows, uint32_t* words,
-                            uint32_t* halo, uint32_t* src, uint32_t* caps_host, void* stream);
+                            uint32_t* halo, uint32_t* src, uint32_t num_blocks, uint32_t* slot_of,
+                            uint32_t* caps_host, void* stream);
+
+/* ys_assemble3 that also writes every block's FP32 values into the streamed
+ * plan's packed blocks (blocks32 of ys_spmv_stream_fill) at its own slot
+ * slot_of[2 b] and, when a later tile uses it transposed, at slot_of[2 b + 1]:
+ * the fill after the assembly is then not needed.  No counterpart in the
+ * reference.                                                              */
+int32_t ys_assemble3_streamed(const double* records, const uint32_t* begin, const uint32_t* count,
+                              const uint32_t* offset, uint32_t nu, double* out, float* out32,
+                              const uint32_t* slot_of, float* blocks32, void* stream);
 
 /* blocks32[9 s + k] = values32[12 src[s] + k] for every slot s < slots with
  * a block (zeros elsewhere): the streamed plan's packed FP32 blocks, current

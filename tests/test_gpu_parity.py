@@ -218,8 +218,15 @@ def test_streamed_pcg_matches_tiled_pcg_bit_for_bit():
     runs.append((int(res.iterations), z.cpu().numpy().copy()))
   assert runs[0][0] == runs[1][0] == 30
   assert np.array_equal(runs[0][1], runs[1][1]) and np.array_equal(runs[0][1], runs[2][1])
-  # new FP32 values (a new version) refresh the packed blocks before use
+  # a new assembly writes the packed blocks itself: the same as a fill
+  assert sc.minimizer.computeNumericValue() is H
   sp = H.stream_plan(bs)
+  assert sp.filled == (H.values32_version, bs.values32.data_ptr())
+  want = torch.zeros_like(sp.blocks32)
+  L.call("ys_spmv_stream_fill", L.ptr(bs.values32), L.ptr(sp.src), sp.slots, L.ptr(want), L.stream_ptr())
+  used = (sp.src != -1).repeat_interleave(9)
+  assert torch.equal(sp.blocks32[used], want[used])
+  # new FP32 values (a new version) refresh the packed blocks before use
   before = sp.blocks32.clone()
   bs.values32.mul_(2.0)
   H.values32_version += 1

@@ -173,7 +173,8 @@ SIGNATURES = {
     "ys_spmv_tile_plan": (i32, [vp, u32, vp, vp, u32, vp, P(u32), P(u32), vp]),
     "ys_spmv3_x32_tiled": (i32, [vp, vp, vp, vp, vp, u32, u32, u32, u32, vp, vp, i32, vp, vp]),
     "ys_spmv_stream_words": (i32, [u32, u32, P(u64)]),
-    "ys_spmv_stream_plan": (i32, [vp, vp, vp, vp, u32, u64, vp, vp, vp, vp, vp, P(u32), vp]),
+    "ys_spmv_stream_plan": (i32, [vp, vp, vp, vp, u32, u64, vp, vp, vp, vp, vp, u32, vp, P(u32), vp]),
+    "ys_assemble3_streamed": (i32, [vp, vp, vp, vp, u32, vp, vp, vp, vp, vp]),
     "ys_spmv_stream_fill": (i32, [vp, vp, u64, vp, vp]),
     "ys_spmv3_x32_streamed": (i32, [P(SpmvStream), vp, vp, vp, vp, u32, vp, vp, i32, u32, u32, vp, vp]),
     "ys_pcg_workspace_doubles": (u64, [u32]),

@@ -67,7 +67,9 @@ __global__ void __launch_bounds__(256) assemble3_kernel(const double* __restrict
                                                         const uint32_t* __restrict__ begin,
                                                         const uint32_t* __restrict__ count,
                                                         const uint32_t* __restrict__ offset, uint32_t nu,
-                                                        double* __restrict__ out, float* __restrict__ out32) {
+                                                        double* __restrict__ out, float* __restrict__ out32,
+                                                        const uint2* __restrict__ slot_of,
+                                                        float* __restrict__ blocks32) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t u = warp * 3 + lane / 9;
@@ -79,6 +81,13 @@ __global__ void __launch_bounds__(256) assemble3_kernel(const double* __restrict
   const uint64_t o = offset[u];
   out[o + e] = acc;
   if (out32) out32[12ull * u + e] = (float)acc;  // 12-float FP32 block slots
+  if (blocks32) {
+    // the streamed SpMV's packed copies: the block's slot in its row's tile
+    // and, for a block used transposed by a later tile, its slot there
+    const uint2 sl = slot_of[u];
+    blocks32[9ull * sl.x + e] = (float)acc;
+    if (sl.y != 0xffffffffu) blocks32[9ull * sl.y + e] = (float)acc;
+  }
 }
 
 struct DiagLayout {
@@ -210,7 +219,21 @@ int32_t ys_assemble3(const double* records, const uint32_t* begin, const uint32_
   if (nu == 0) return YS_OK;
   const uint64_t warps = (nu + 2) / 3;
   ys::assemble3_kernel<<<ys::grid_for(warps * 32, 256), 256, 0, (cudaStream_t)stream>>>(records, begin, count, offset,
-                                                                                        nu, out, out32);
+                                                                                        nu, out, out32, nullptr,
+                                                                                        nullptr);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
+
+int32_t ys_assemble3_streamed(const double* records, const uint32_t* begin, const uint32_t* count,
+                              const uint32_t* offset, uint32_t nu, double* out, float* out32, const uint32_t* slot_of,
+                              float* blocks32, void* stream) {
+  YS_REQUIRE(slot_of && blocks32, YS_ERR_INVALID, "null argument");
+  YS_REQUIRE((reinterpret_cast<uintptr_t>(slot_of) & 7) == 0, YS_ERR_INVALID, "slot_of must be 8-byte aligned");
+  if (nu == 0) return YS_OK;
+  const uint64_t warps = (nu + 2) / 3;
+  ys::assemble3_kernel<<<ys::grid_for(warps * 32, 256), 256, 0, (cudaStream_t)stream>>>(
+      records, begin, count, offset, nu, out, out32, reinterpret_cast<const uint2*>(slot_of), blocks32);
   YS_CHECK_LAUNCH();
   return YS_OK;
 }

@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kTileThreads) stream_plan_kernel(
     const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ entry_block,
     const uint32_t* __restrict__ entry_col, const uint32_t* __restrict__ row_block, uint32_t nv,
     uint4* __restrict__ desc, uint32_t* __restrict__ rows, uint32_t* __restrict__ words, uint32_t* __restrict__ halo,
-    uint32_t* __restrict__ src, uint32_t* __restrict__ caps) {
+    uint32_t* __restrict__ src, uint32_t* __restrict__ slot_of, uint32_t* __restrict__ caps) {
   __shared__ uint32_t key[kStreamMaxEntries];
   __shared__ uint32_t uniq[kStreamMaxEntries];
   __shared__ uint32_t wsum[kTileThreads / 32 + 1];
@@ -264,10 +264,16 @@ __global__ void __launch_bounds__(kTileThreads) stream_plan_kernel(
       else hi = mid;
     }
     words[base + j] = lo | ((slot & 0x7fffu) << 16) | (tr << 31);
-    if (cross && slot < ne) src[base + slot] = blk;
+    if (cross && slot < ne) {
+      src[base + slot] = blk;
+      slot_of[2ull * blk + 1] = base + slot;  // a block is used transposed by one row only
+    }
   }
   if (threadIdx.x < 4 && ne + threadIdx.x < round4(ne)) words[base + ne + threadIdx.x] = 0u;
-  for (uint32_t b = b0 + threadIdx.x; b < b1; b += kTileThreads) src[base + (b - b0)] = b;
+  for (uint32_t b = b0 + threadIdx.x; b < b1; b += kTileThreads) {
+    src[base + (b - b0)] = b;
+    slot_of[2ull * b] = base + (b - b0);
+  }
   for (uint32_t j = threadIdx.x; j < round4(nh); j += kTileThreads) halo[base + j] = j < nh ? uniq[j] : uniq[0];
   for (uint32_t k = threadIdx.x; k < kStreamRowWords; k += kTileThreads)
     rows[(uint64_t)kStreamRowWords * t + k] =
@@ -505,9 +511,10 @@ int32_t ys_spmv_stream_words(uint32_t num_entries, uint32_t num_vars, uint64_t* 
 
 int32_t ys_spmv_stream_plan(const uint32_t* row_ptr, const uint32_t* entry_block, const uint32_t* entry_col,
                             const uint32_t* row_block, uint32_t num_vars, uint64_t capacity_words, uint32_t* desc,
-                            uint32_t* rows, uint32_t* words, uint32_t* halo, uint32_t* src, uint32_t* caps_host,
-                            void* stream) {
-  YS_REQUIRE(row_ptr && entry_block && entry_col && row_block && desc && rows && words && halo && src && caps_host,
+                            uint32_t* rows, uint32_t* words, uint32_t* halo, uint32_t* src, uint32_t num_blocks,
+                            uint32_t* slot_of, uint32_t* caps_host, void* stream) {
+  YS_REQUIRE(row_ptr && entry_block && entry_col && row_block && desc && rows && words && halo && src && slot_of &&
+                 caps_host,
              YS_ERR_INVALID, "null argument");
   YS_REQUIRE((reinterpret_cast<uintptr_t>(words) & 15) == 0 && (reinterpret_cast<uintptr_t>(halo) & 15) == 0 &&
                  (reinterpret_cast<uintptr_t>(rows) & 15) == 0 && (reinterpret_cast<uintptr_t>(desc) & 15) == 0,
@@ -523,9 +530,10 @@ int32_t ys_spmv_stream_plan(const uint32_t* row_ptr, const uint32_t* entry_block
   uint32_t* caps = desc + 4ull * ntiles;  // the descriptor array's last uint4
   YS_CUDA_TRY(cudaMemsetAsync(caps, 0, 16, s));
   YS_CUDA_TRY(cudaMemsetAsync(src, 0xff, 4ull * capacity_words, s));
+  YS_CUDA_TRY(cudaMemsetAsync(slot_of, 0xff, 8ull * num_blocks, s));
   ys::stream_plan_kernel<<<ntiles, ys::kTileThreads, 0, s>>>(row_ptr, entry_block, entry_col, row_block, num_vars,
                                                             reinterpret_cast<uint4*>(desc), rows, words, halo, src,
-                                                            caps);
+                                                            slot_of, caps);
   YS_CHECK_LAUNCH();
   uint32_t h[4] = {0, 0, 0, 0};
   YS_CUDA_TRY(cudaMemcpyAsync(h, caps, sizeof(h), cudaMemcpyDeviceToHost, s));

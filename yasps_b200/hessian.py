@@ -407,8 +407,9 @@ class _StreamPlan:
   """Device arrays of a streamed-tile SpMV plan (``ys_spmv_stream_plan``)
   and the packed FP32 blocks it streams (``ys_spmv_stream_fill``)."""
 
-  def __init__(self, desc, rows, words, halo, src, blocks32, caps, slots):
+  def __init__(self, desc, rows, words, halo, src, slot_of, blocks32, caps, slots):
     self.desc, self.rows, self.words, self.halo, self.src, self.blocks32 = desc, rows, words, halo, src, blocks32
+    self.slot_of = slot_of  # each stored block's own and cross slot (the streamed assembly writes both)
     self.block_cap, self.entry_cap, self.halo_cap = caps
     self.slots = slots
     self.filled = None  # values32 version the blocks were packed from
@@ -435,6 +436,7 @@ class _BlockSet:
     self.spmv = None  # (row_ptr, entry_block, entry_col)
     self.tiles = None  # (row_block, tile capacity) of the tiled SpMV, or (None, 0)
     self.stream = None  # _StreamPlan of the streamed-tile SpMV, False when the set has none
+    self.stream_written = False  # the last assembly wrote the packed blocks too
 
 
 class hessian:
@@ -541,7 +543,11 @@ class hessian:
       bs.values = torch.zeros(max(bs.pattern.total_values, 1), dtype=torch.float64, device=_dev())
     bs.values32 = None
     bs.infos = infos
+    # every plan of the old pattern goes with it
     bs.spmv = None
+    bs.tiles = None
+    bs.stream = None
+    bs.stream_written = False
 
   def _term_plan(self, d, bs):
     p = L.TermPlan()
@@ -611,6 +617,10 @@ class hessian:
       self._extract_diagonal()
     self.values32_current = self.want_fp32
     self.values32_version += 1
+    for bs in (self._static, self._dynamic):
+      if bs.stream and bs.stream_written:
+        bs.stream.filled = (self.values32_version, bs.values32.data_ptr())
+      bs.stream_written = False
     return self
 
   def term_energies(self):
@@ -693,7 +703,15 @@ class hessian:
       if bs.values32 is None or bs.values32.numel() < n32:
         bs.values32 = torch.zeros(n32, dtype=torch.float32, device=_dev())
       v32 = bs.values32
-    if p.all3:
+    sp = bs.stream
+    if (p.all3 and sp and v32 is not None and bs.spmv is not None and
+        sp.slot_of.numel() == 2 * p.num_unique):
+      # the streamed SpMV's packed blocks are written by the assembly itself
+      L.call("ys_assemble3_streamed", L.ptr(bs.records), L.ptr(p.record_begin), L.ptr(p.record_count),
+             L.ptr(p.value_offset), p.num_unique, L.ptr(bs.values), L.ptr(v32), L.ptr(sp.slot_of),
+             L.ptr(sp.blocks32), s)
+      bs.stream_written = True
+    elif p.all3:
       L.call("ys_assemble3", L.ptr(bs.records), L.ptr(p.record_begin), L.ptr(p.record_count), L.ptr(p.value_offset),
              p.num_unique, L.ptr(bs.values), L.ptr(v32), s)
     else:
@@ -907,12 +925,14 @@ class hessian:
         i32 = lambda k: torch.zeros(k, dtype=torch.int32, device=_dev())
         desc, rows, wd, halo, src = i32(4 * (ntiles + 1)), i32(68 * ntiles), i32(nw), i32(nw), i32(nw)
         caps = (L.u32 * 3)()
+        nu = bs.pattern.num_unique
+        slot_of = i32(2 * nu)
         rc = L.call("ys_spmv_stream_plan", L.ptr(row_ptr), L.ptr(eb), L.ptr(ec), L.ptr(row_block), nv, nw,
-                    L.ptr(desc), L.ptr(rows), L.ptr(wd), L.ptr(halo), L.ptr(src), caps, L.stream_ptr(),
-                    ok=(L.YS_OK, L.YS_ERR_CAPACITY))
+                    L.ptr(desc), L.ptr(rows), L.ptr(wd), L.ptr(halo), L.ptr(src), nu, L.ptr(slot_of), caps,
+                    L.stream_ptr(), ok=(L.YS_OK, L.YS_ERR_CAPACITY))
         if rc == L.YS_OK:
           blocks32 = torch.zeros(9 * nw, dtype=torch.float32, device=_dev())
-          bs.stream = _StreamPlan(desc, rows, wd, halo, src, blocks32, tuple(int(c) for c in caps), nw)
+          bs.stream = _StreamPlan(desc, rows, wd, halo, src, slot_of, blocks32, tuple(int(c) for c in caps), nw)
     sp = bs.stream
     if not sp:
       return None
@@ -946,7 +966,8 @@ class hessian:
       m.row_ptr[k], m.entry_block[k], m.entry_col[k] = L.ptr(row_ptr), L.ptr(eb), L.ptr(ec)
       row_block, cap, ecap = self.tile_plan(bs)
       m.row_block[k], m.tile_cap[k], m.entry_cap[k] = L.ptr(row_block), cap, ecap
-      sp = self.stream_plan(bs)
+      # (the PCG runs the streamed SpMV for a single block set only)
+      sp = self.stream_plan(bs) if len(sets) == 1 else None
       if sp is not None:
         m.stream[k] = sp.struct()
     m.num_vars = self.rows // 3

@@ -94,7 +94,7 @@ class _PcgBase:
     # (dynamic terms) gives new row plans and must give a new graph
     # (an FP32 solve first refreshes the streamed SpMV's packed blocks from
     # the current FP32 values; the graph holds the plan's pointers)
-    streams = [H.stream_plan(bs) if fp32 else None for bs in H.block_sets]
+    streams = [H.stream_plan(bs) if fp32 and len(H.block_sets) == 1 else None for bs in H.block_sets]
     plans = tuple(tuple(t.data_ptr() for t in H.spmv_plan(bs)) + (bs.pattern.num_unique,) +
                   tuple(0 if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else t) for t in H.tile_plan(bs)) +
                   (sp.pointers() if sp is not None else ())
