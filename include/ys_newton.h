@@ -270,8 +270,9 @@ int32_t ys_snh_local_hessians(const ys_snh_args* args, double* out, void* stream
  * [x0..x3, X0..X3] (24x24 packed upper, 300 doubles an element): the x-x
  * block as ys_snh_local_hessians, the x-X block the derivative of the
  * position gradient in the rest positions (first-order dual numbers over
- * one rest vertex at a time); the X-X block is written as zero (rest-rest
- * Jacobians are not built).                                               */
+ * one rest vertex at a time), the X-X block the energy's second derivatives
+ * in the rest positions (hyper-dual numbers over two rest vertices at a
+ * time, 10 pairs a tet).                                                  */
 int32_t ys_snh_rest_local_hessians(const ys_snh_args* args, double* out, void* stream);
 /* Same for the inertia 1/2 m |x - x_before - dt v - dt^2 g|^2 per vertex
  * over its arguments (x, x_before) (args = 2) or (x, x_before, v) (args = 3):

@@ -191,8 +191,9 @@ def test_friction_position_against_step_start_positions(kind):
 
 def test_snh_positions_against_rest_positions():
   """Shape derivatives d2E/(dx dX) of the SNH tetrahedra (free positions
-  against free rest positions) against the oracle's autograd Hessian over
-  (x, X); rest against rest is not built and raises."""
+  against free rest positions), and rest positions against both (the
+  rest-rest blocks d2E/dX2 among them), against the oracle's autograd
+  Hessian over (x, X)."""
   from yasps_b200.graph import resolve_leaf_children
   cube = scenes.fem_cube(5, noise=0.01, seed=1)
   sc, h = scenes.fem_scene(cube)
@@ -207,8 +208,14 @@ def test_snh_positions_against_rest_positions():
   rc = np.concatenate([free_code, zero], axis=1)
   ccode = np.concatenate([zero, free_code], axis=1)
   check(J, orj.dense(hl, rc, ccode, J.rows, J.cols), rc, ccode)
-  with pytest.raises(NotImplementedError):
-    differentiator().diff2([snh], [free_rest], [h["free_position"], free_rest]).compute()
+  # rows: rest positions; columns: positions, then rest positions
+  J2 = differentiator().diff2([snh], [free_rest], [h["free_position"], free_rest]).compute()
+  nfree = cube.free_count
+  rest_code = np.where(tets >= npin, 2 + 3 * (tets - npin + nfree), 0)
+  rc2 = np.concatenate([zero, free_code], axis=1)
+  cc2 = np.concatenate([free_code, rest_code], axis=1)
+  assert J2.rows == 3 * nfree and J2.cols == 6 * nfree
+  check(J2, orj.dense(hl, rc2, cc2, J2.rows, J2.cols), rc2, cc2)
 
 
 def material_scene(side=5):

@@ -521,9 +521,157 @@ __device__ void snh_rest_column(const double (&x)[4][3], const double (&X)[4][3]
     }
 }
 
+// Hyper-dual number over two sets of 3 directions (the rest coordinates of
+// vertex va, set a, and of vertex vb, set b): value, first derivatives in
+// each set and the mixed second derivatives d2/(dX_va dX_vb).
+struct H33 {
+  double v, a[3], b[3], ab[3][3];
+};
+__device__ __forceinline__ H33 h33c(double c) {
+  H33 r;
+  r.v = c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = r.b[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = 0.0;
+  }
+  return r;
+}
+__device__ __forceinline__ H33 operator+(const H33& f, const H33& g) {
+  H33 r;
+  r.v = f.v + g.v;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = f.a[i] + g.a[i];
+    r.b[i] = f.b[i] + g.b[i];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = f.ab[i][j] + g.ab[i][j];
+  }
+  return r;
+}
+__device__ __forceinline__ H33 operator*(double s, const H33& f) {
+  H33 r;
+  r.v = s * f.v;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = s * f.a[i];
+    r.b[i] = s * f.b[i];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = s * f.ab[i][j];
+  }
+  return r;
+}
+__device__ __forceinline__ H33 operator-(const H33& f, const H33& g) { return f + (-1.0) * g; }
+__device__ __forceinline__ H33 operator*(const H33& f, const H33& g) {
+  H33 r;
+  r.v = f.v * g.v;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = f.a[i] * g.v + f.v * g.a[i];
+    r.b[i] = f.b[i] * g.v + f.v * g.b[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      r.ab[i][j] = f.ab[i][j] * g.v + f.v * g.ab[i][j] + f.a[i] * g.b[j] + g.a[i] * f.b[j];
+  return r;
+}
+// h(f) from h(f.v), h'(f.v), h''(f.v)
+__device__ __forceinline__ H33 h33_apply(const H33& f, double h, double dh, double d2h) {
+  H33 r;
+  r.v = h;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = dh * f.a[i];
+    r.b[i] = dh * f.b[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = dh * f.ab[i][j] + d2h * f.a[i] * f.b[j];
+  return r;
+}
+__device__ __forceinline__ H33 h33_recip(const H33& f) {
+  const double i = 1.0 / f.v;
+  return h33_apply(f, i, -i * i, 2.0 * i * i * i);
+}
+__device__ __forceinline__ H33 h33_log(const H33& f) {
+  const double i = 1.0 / f.v;
+  return h33_apply(f, log(f.v), i, -i * i);
+}
+
+// Rest-rest block (3 x 3) of rest vertices va, vb: out[i][j] =
+// d2E/(dX_va,i dX_vb,j), the SNH energy of the tet (the formula of
+// snh_state) evaluated in hyper-dual numbers over the rest positions, the
+// current positions held constant.
+__device__ __noinline__ void snh_rest_rest_block(const double (&x)[4][3], const double (&X)[4][3], int va, int vb,
+                                                 double mu, double lam, double dt, double (&out)[3][3]) {
+  H33 P[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      P[k][c] = h33c(X[k][c]);
+      if (k == va) P[k][c].a[c] = 1.0;
+      if (k == vb) P[k][c].b[c] = 1.0;
+    }
+  H33 e[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e[k][c] = P[k + 1][c] - P[0][c];
+  auto crossc = [&](const H33 (&a)[3], const H33 (&b)[3], H33 (&o)[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  H33 k0[3], k1[3], k2[3];
+  crossc(e[1], e[2], k0);
+  crossc(e[2], e[0], k1);
+  crossc(e[0], e[1], k2);
+  const H33 det = e[0][0] * k0[0] + e[0][1] * k0[1] + e[0][2] * k0[2];
+  const H33 inv = h33_recip(det);
+  H33 G[4][3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    G[1][j] = k0[j] * inv;
+    G[2][j] = k1[j] * inv;
+    G[3][j] = k2[j] * inv;
+    G[0][j] = (-1.0) * (G[1][j] + G[2][j] + G[3][j]);
+  }
+  H33 F[3][3];  // columns f_j
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      H33 acc = x[0][c] * G[0][j];
+#pragma unroll
+      for (int k = 1; k < 4; ++k) acc = acc + x[k][c] * G[k][j];
+      F[j][c] = acc;
+    }
+  H33 c0[3];
+  crossc(F[1], F[2], c0);
+  H33 ic = h33c(0.0);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ic = ic + F[j][c] * F[j][c];
+  const H33 J = F[0][0] * c0[0] + F[0][1] * c0[1] + F[0][2] * c0[2];
+  const double alpha = 1.0 + 0.75 * mu / lam;
+  const H33 jm = J - h33c(alpha);
+  const H33 psi = (0.5 * mu) * (ic - h33c(3.0)) - (0.5 * mu) * h33_log(ic + h33c(1.0)) + (0.5 * lam) * (jm * jm);
+  const H33 E = ((dt * dt / 6.0) * det) * psi;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) out[i][j] = E.ab[i][j];
+}
+
 // Packed upper 24x24 Hessian over (x, X) of one tet: the x-x block from the
-// SNH blocks, the x-X block by differentiation in X; the X-X block is left
-// zero (rest-rest products are not built: the caller never reads them).
+// SNH blocks, the x-X block by differentiation of the position gradient in
+// X, the X-X block by hyper-dual evaluation of the energy.
 __global__ void __launch_bounds__(64) snh_rest_local_hessian_kernel(const ys_snh_args a, double* out) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.num_elements) return;
@@ -550,8 +698,6 @@ __global__ void __launch_bounds__(64) snh_rest_local_hessian_kernel(const ys_snh
             if (3 * ai + k <= 3 * bi + l) dst[utri<24>(3 * ai + k, 3 * bi + l)] = blk[k][l];
       }
   }
-  for (int i = 12; i < 24; ++i)
-    for (int j = i; j < 24; ++j) dst[utri<24>(i, j)] = 0.0;
   const uint4 tv = reinterpret_cast<const uint4*>(a.tets)[t];
   const uint32_t id[4] = {tv.x, tv.y, tv.z, tv.w};
   double x[4][3], X[4][3];
@@ -571,6 +717,16 @@ __global__ void __launch_bounds__(64) snh_rest_local_hessian_kernel(const ys_snh
 #pragma unroll
       for (int m = 0; m < 3; ++m) dst[utri<24>(i, 12 + 3 * va + m)] = col[i][m];
   }
+#pragma unroll 1
+  for (int va = 0; va < 4; ++va)
+#pragma unroll 1
+    for (int vb = va; vb < 4; ++vb) {
+      double blk[3][3];
+      snh_rest_rest_block(x, X, va, vb, mu, lam, a.dt, blk);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          if (3 * va + i <= 3 * vb + j) dst[utri<24>(12 + 3 * va + i, 12 + 3 * vb + j)] = blk[i][j];
+    }
 }
 
 // Derivative of the SNH position gradient s (c1 F G_k + c3 cof G_k) in a

@@ -29,9 +29,10 @@ attributes (the adjoint blocks ``d2E / (dx dx_before)`` and
 for the lagged friction kinds, functions of ``x - x_old``, also the
 leaves of their step-start positions, and for the SNH tetrahedra the
 leaves of their rest positions against the position leaves (shape
-derivatives ``d2E / (dx dX)``).  Mixed derivatives through the rest shapes
-of the other energies, rest against rest, and through affine-body vertices
-are not built (a target among those leaves raises).
+derivatives ``d2E / (dx dX)``) and against each other (``d2E / dX2``).
+Mixed derivatives through the rest shapes of the other energies and
+through affine-body vertices are not built (a target among those leaves
+raises).
 """
 
 from __future__ import annotations
@@ -318,10 +319,9 @@ class secondOrderJacobian:
         rest = t.rest_leaves()
         in_rows = any(any(x is r for r in rest) for x in self.__row_wrt)
         in_cols = any(any(x is r for r in rest) for x in self.__column_wrt)
-        if (in_rows or in_cols) and (t.expr.kind != "snh" or (in_rows and in_cols)):
+        if (in_rows or in_cols) and t.expr.kind != "snh":
           raise NotImplementedError("secondOrderJacobian: mixed derivatives through the rest argument of "
-                                    f"{type(t.expr).__name__} are not built"
-                                    + (" (rest against rest)" if t.expr.kind == "snh" else ""))
+                                    f"{type(t.expr).__name__} are not built")
         t._rest_form = in_rows or in_cols
       params = []
       for which, att in t.parameters():
