@@ -264,6 +264,15 @@ int32_t ys_energy_eval(const ys_energy_args* args, void* stream);
  * position arguments; rest, lagged data and parameters as for
  * ys_energy_eval, the plan and record fields unused).                      */
 int32_t ys_local_hessians(const ys_energy_args* args, double* out, void* stream);
+
+/* Unprojected local Hessians over the positions and the rest positions of
+ * the cloth energies (YS_ENERGY_BENDING, _BARAFF_WITKIN, _STVK_MEMBRANE):
+ * arguments [x0 .. x(A-1), X0 .. X(A-1)], packed upper (6A)x(6A), the rest
+ * quantities (rest frame, rest dihedral, rest edge length and area)
+ * differentiated with the positions.  One hyper-dual evaluation of the
+ * energy a vertex pair (3x3 block).  No counterpart kernel in the reference
+ * (its differentiator forms these derivatives symbolically).              */
+int32_t ys_rest_local_hessians(const ys_energy_args* args, double* out, void* stream);
 /* Same for the SNH tetrahedra (12x12, 78 doubles an element).              */
 int32_t ys_snh_local_hessians(const ys_snh_args* args, double* out, void* stream);
 /* SNH over the positions and the rest positions of the tet, arguments

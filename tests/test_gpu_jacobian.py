@@ -325,3 +325,52 @@ def test_first_order_jacobian_of_affine_vertex_positions():
       D[3 * i + r, 9 * b + 3 * r:9 * b + 3 * r + 3] = bodies.rest[i]
       D[3 * i + r, 9 * nb + 3 * b + r] = 1.0
   check(J, D, None, None)
+
+
+def cloth_rest_local(kind, x, rest, conn, params):
+  """Oracle local Hessians [n, 6A, 6A] of a cloth energy over (positions,
+  rest positions) of each element, by autograd through the oracle's rest
+  frame / rest dihedral."""
+  import torch
+  fn = {5: ve.bending, 6: ve.baraff_witkin, 7: ve.stvk_membrane}[kind]
+  p = torch.tensor(params, dtype=torch.float64)
+  out = []
+  for q in conn:
+    A = len(q)
+    z0 = torch.tensor(np.concatenate([x[q], rest[q]]).ravel(), dtype=torch.float64)
+    H = torch.autograd.functional.hessian(lambda z: fn(z[:3 * A].view(A, 3), z[3 * A:].view(A, 3), p), z0)
+    out.append(H.numpy())
+  return np.stack(out)
+
+
+@pytest.mark.parametrize("membrane", ["baraff_witkin", "stvk"])
+def test_cloth_energies_against_rest_positions(membrane):
+  """Shape derivatives of the cloth energies through their rest quantities
+  (rest frame and area of the membranes, rest dihedral and edge length of
+  the bending): positions against rest positions per energy, and rest
+  positions against both for the sum of the two, against autograd of the
+  oracle formulas."""
+  from tests.vertex_scene import VertexScene
+  from yasps_b200.graph import resolve_leaf_children
+  vs = VertexScene(m=5, seed=3, membrane=membrane)
+  sc = vs.build()
+  pos = sc.minimizer.wrt[0]
+  es = {r.energy.expr.code: r.energy for r in sc.minimizer.requests
+        if r.energy.expr.kind == "vertex" and r.energy.expr.code in (5, 6, 7)}
+  rest = resolve_leaf_children(next(iter(es.values())).expr.rest.source)[0][-1]
+  terms = {kind: (conn, params) for kind, conn, params, aux, _ in vs.terms() if kind in (5, 6, 7)}
+  n3 = vs.n
+  total = np.zeros((n3, 2 * n3))
+  for kind, e in es.items():
+    conn, params = terms[kind]
+    hl = cloth_rest_local(kind, vs.x, vs.rest, conn, params)
+    code = 2 + 3 * conn.astype(np.int64)
+    zero = np.zeros_like(code)
+    rc, cc = np.concatenate([code, zero], axis=1), np.concatenate([zero, code], axis=1)
+    J = differentiator().diff2([e], [pos], [rest]).compute()
+    check(J, orj.dense(hl, rc, cc, J.rows, J.cols), rc, cc)
+    cc2 = np.concatenate([code, code + n3], axis=1)
+    total += orj.dense(hl, np.concatenate([zero, code], axis=1), cc2, n3, 2 * n3)
+  J2 = differentiator().diff2(list(es.values()), [rest], [pos, rest]).compute()
+  assert J2.rows == n3 and J2.cols == 2 * n3
+  check(J2, total, None, None)

@@ -139,6 +139,7 @@ SIGNATURES = {
     "ys_inertia_eval": (i32, [P(InertiaArgs), vp]),
     "ys_energy_eval": (i32, [P(EnergyArgs), vp]),
     "ys_local_hessians": (i32, [P(EnergyArgs), vp, vp]),
+    "ys_rest_local_hessians": (i32, [P(EnergyArgs), vp, vp]),
     "ys_snh_local_hessians": (i32, [P(SnhArgs), vp, vp]),
     "ys_snh_rest_local_hessians": (i32, [P(SnhArgs), vp, vp]),
     "ys_inertia_local_hessians": (i32, [vp, f64, f64, u32, u32, vp, vp]),

@@ -226,4 +226,128 @@ __device__ __forceinline__ HD<N> norm(const HV<N>& a) {
   return hd_sqrt(dot(a, a));
 }
 
+// ---- hyper-dual numbers over two sets of 3 directions ----------------------
+// H33 carries a value, its first derivatives in two sets of 3 inputs (set a:
+// the coordinates of one vertex, set b: those of another, or the same) and
+// the mixed second derivatives d2/(da db): one 3x3 block of a Hessian per
+// evaluation.  Rules as for HD, with a.g b.g^T split into the two sets:
+//   (f g).ab = f.ab g + f g.ab + f.a g.b^T + g.a f.b^T
+//   h(f).ab  = h' f.ab + h'' f.a f.b^T
+struct H33 {
+  double v, a[3], b[3], ab[3][3];
+};
+__device__ __forceinline__ H33 h33c(double c) {
+  H33 r;
+  r.v = c;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = r.b[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = 0.0;
+  }
+  return r;
+}
+__device__ __forceinline__ H33 operator+(const H33& f, const H33& g) {
+  H33 r;
+  r.v = f.v + g.v;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = f.a[i] + g.a[i];
+    r.b[i] = f.b[i] + g.b[i];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = f.ab[i][j] + g.ab[i][j];
+  }
+  return r;
+}
+__device__ __forceinline__ H33 operator*(double s, const H33& f) {
+  H33 r;
+  r.v = s * f.v;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = s * f.a[i];
+    r.b[i] = s * f.b[i];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = s * f.ab[i][j];
+  }
+  return r;
+}
+__device__ __forceinline__ H33 operator-(const H33& f, const H33& g) { return f + (-1.0) * g; }
+__device__ __forceinline__ H33 operator*(const H33& f, const H33& g) {
+  H33 r;
+  r.v = f.v * g.v;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = f.a[i] * g.v + f.v * g.a[i];
+    r.b[i] = f.b[i] * g.v + f.v * g.b[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      r.ab[i][j] = f.ab[i][j] * g.v + f.v * g.ab[i][j] + f.a[i] * g.b[j] + g.a[i] * f.b[j];
+  return r;
+}
+// h(f) from h(f.v), h'(f.v), h''(f.v)
+__device__ __forceinline__ H33 h33_apply(const H33& f, double h, double dh, double d2h) {
+  H33 r;
+  r.v = h;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = dh * f.a[i];
+    r.b[i] = dh * f.b[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.ab[i][j] = dh * f.ab[i][j] + d2h * f.a[i] * f.b[j];
+  return r;
+}
+__device__ __forceinline__ H33 h33_recip(const H33& f) {
+  const double i = 1.0 / f.v;
+  return h33_apply(f, i, -i * i, 2.0 * i * i * i);
+}
+__device__ __forceinline__ H33 h33_log(const H33& f) {
+  const double i = 1.0 / f.v;
+  return h33_apply(f, log(f.v), i, -i * i);
+}
+
+
+__device__ __forceinline__ H33 operator+(const H33& f, double c) {
+  H33 r = f;
+  r.v += c;
+  return r;
+}
+__device__ __forceinline__ H33 operator-(const H33& f, double c) {
+  H33 r = f;
+  r.v -= c;
+  return r;
+}
+__device__ __forceinline__ H33 operator/(const H33& f, const H33& g) { return f * h33_recip(g); }
+__device__ __forceinline__ H33 h33_sqrt(const H33& f) {
+  const double s = sqrt(f.v);
+  return h33_apply(f, s, 0.5 / s, -0.25 / (s * f.v));
+}
+// atan2(y, x), the second-derivative terms of hd_atan2
+__device__ __forceinline__ H33 h33_atan2(const H33& y, const H33& x) {
+  const double r2 = x.v * x.v + y.v * y.v;
+  const double ir = 1.0 / r2, ir2 = ir * ir;
+  const double fy = x.v * ir, fx = -y.v * ir;
+  const double fyy = -2.0 * x.v * y.v * ir2, fxx = 2.0 * x.v * y.v * ir2;
+  const double fxy = (y.v * y.v - x.v * x.v) * ir2;
+  H33 r;
+  r.v = atan2(y.v, x.v);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    r.a[i] = fy * y.a[i] + fx * x.a[i];
+    r.b[i] = fy * y.b[i] + fx * x.b[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      r.ab[i][j] = fy * y.ab[i][j] + fx * x.ab[i][j] + fyy * y.a[i] * y.b[j] + fxx * x.a[i] * x.b[j] +
+                   fxy * (x.a[i] * y.b[j] + y.a[i] * x.b[j]);
+  return r;
+}
+
 }  // namespace ys

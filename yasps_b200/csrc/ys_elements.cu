@@ -22,6 +22,7 @@
 // A, runs the PSD test and writes records for the PSD tets; tets that need the
 // eigen-solve are compacted into a work list and finished by
 // `snh_project_kernel`, so the expensive path runs without divergence.
+#include "ys_ad.cuh"
 #include "ys_common.cuh"
 #include "ys_eigen.cuh"
 
@@ -519,87 +520,6 @@ __device__ void snh_rest_column(const double (&x)[4][3], const double (&X)[4][3]
 #pragma unroll
       for (int m = 0; m < 3; ++m) out[3 * k + c][m] = gx.d[m];
     }
-}
-
-// Hyper-dual number over two sets of 3 directions (the rest coordinates of
-// vertex va, set a, and of vertex vb, set b): value, first derivatives in
-// each set and the mixed second derivatives d2/(dX_va dX_vb).
-struct H33 {
-  double v, a[3], b[3], ab[3][3];
-};
-__device__ __forceinline__ H33 h33c(double c) {
-  H33 r;
-  r.v = c;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    r.a[i] = r.b[i] = 0.0;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) r.ab[i][j] = 0.0;
-  }
-  return r;
-}
-__device__ __forceinline__ H33 operator+(const H33& f, const H33& g) {
-  H33 r;
-  r.v = f.v + g.v;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    r.a[i] = f.a[i] + g.a[i];
-    r.b[i] = f.b[i] + g.b[i];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) r.ab[i][j] = f.ab[i][j] + g.ab[i][j];
-  }
-  return r;
-}
-__device__ __forceinline__ H33 operator*(double s, const H33& f) {
-  H33 r;
-  r.v = s * f.v;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    r.a[i] = s * f.a[i];
-    r.b[i] = s * f.b[i];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) r.ab[i][j] = s * f.ab[i][j];
-  }
-  return r;
-}
-__device__ __forceinline__ H33 operator-(const H33& f, const H33& g) { return f + (-1.0) * g; }
-__device__ __forceinline__ H33 operator*(const H33& f, const H33& g) {
-  H33 r;
-  r.v = f.v * g.v;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    r.a[i] = f.a[i] * g.v + f.v * g.a[i];
-    r.b[i] = f.b[i] * g.v + f.v * g.b[i];
-  }
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-      r.ab[i][j] = f.ab[i][j] * g.v + f.v * g.ab[i][j] + f.a[i] * g.b[j] + g.a[i] * f.b[j];
-  return r;
-}
-// h(f) from h(f.v), h'(f.v), h''(f.v)
-__device__ __forceinline__ H33 h33_apply(const H33& f, double h, double dh, double d2h) {
-  H33 r;
-  r.v = h;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    r.a[i] = dh * f.a[i];
-    r.b[i] = dh * f.b[i];
-  }
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) r.ab[i][j] = dh * f.ab[i][j] + d2h * f.a[i] * f.b[j];
-  return r;
-}
-__device__ __forceinline__ H33 h33_recip(const H33& f) {
-  const double i = 1.0 / f.v;
-  return h33_apply(f, i, -i * i, 2.0 * i * i * i);
-}
-__device__ __forceinline__ H33 h33_log(const H33& f) {
-  const double i = 1.0 / f.v;
-  return h33_apply(f, log(f.v), i, -i * i);
 }
 
 // Rest-rest block (3 x 3) of rest vertices va, vb: out[i][j] =

@@ -219,6 +219,138 @@ struct StvkMembrane {
   }
 };
 
+// ---- the cloth energies over positions and rest positions ------------------
+// The same formulas as Bending, BaraffWitkin and StvkMembrane (and their rest
+// quantities rest_frame and dihedral), written over H33 numbers so that both
+// the positions and the rest positions are inputs: one evaluation gives the
+// 3x3 block of d2E between two of the element's 2A vertices (positions 0 ..
+// A-1, rest positions A .. 2A-1).
+struct HV33 {
+  H33 x, y, z;
+};
+__device__ __forceinline__ HV33 operator-(const HV33& u, const HV33& v) { return {u.x - v.x, u.y - v.y, u.z - v.z}; }
+__device__ __forceinline__ HV33 operator+(const HV33& u, const HV33& v) { return {u.x + v.x, u.y + v.y, u.z + v.z}; }
+__device__ __forceinline__ HV33 scale(const H33& s, const HV33& v) { return {s * v.x, s * v.y, s * v.z}; }
+__device__ __forceinline__ H33 dot(const HV33& u, const HV33& v) { return u.x * v.x + u.y * v.y + u.z * v.z; }
+__device__ __forceinline__ HV33 cross(const HV33& u, const HV33& v) {
+  return {u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
+}
+__device__ __forceinline__ H33 norm(const HV33& u) { return h33_sqrt(dot(u, u)); }
+
+__device__ __noinline__ H33 dihedral33(const HV33& q0, const HV33& q1, const HV33& q2, const HV33& q3) {
+  const HV33 n0 = cross(q0 - q2, q1 - q2);
+  const HV33 n1 = cross(q1 - q3, q0 - q3);
+  const HV33 axis = q1 - q0;
+  const H33 num = dot(cross(n0, n1), axis) / norm(axis);
+  const H33 den = dot(n0, n1) + norm(n0) * norm(n1);
+  return 2.0 * h33_atan2(num, den);
+}
+
+// rest_frame: rotate the rest normal onto +y, keep (x, z); M^-1 and the area
+__device__ __noinline__ void rest_frame33(const HV33 (&r)[3], H33 (&minv)[2][2], H33& area) {
+  const HV33 nn = cross(r[1] - r[0], r[2] - r[0]);
+  const H33 nl = norm(nn);
+  area = 0.5 * nl;
+  const HV33 n = scale(h33_recip(nl), nn);
+  // vec = (-n_z, 0, n_x), cos = n_y: rows 0 and 2 of I + [vec]x + [vec]x^2 / (1 + cos)
+  const H33 ic = h33_recip(n.y + 1.0);
+  const H33 nx2 = n.x * n.x, nz2 = n.z * n.z, nxz = n.x * n.z;
+  // [vec]x = [[0, -n_x, 0], [n_x, 0, n_z], [0, -n_z, 0]];
+  // [vec]x^2 = [[-n_x^2, 0, -n_x n_z], [0, -n_x^2 - n_z^2, 0], [-n_x n_z, 0, -n_z^2]]
+  const H33 r00 = (-1.0 * nx2) * ic + 1.0, r01 = -1.0 * n.x, r02 = (-1.0 * nxz) * ic;
+  const H33 r20 = (-1.0 * nxz) * ic, r21 = -1.0 * n.z, r22 = (-1.0 * nz2) * ic + 1.0;
+  H33 uv[3][2];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    uv[q][0] = r00 * r[q].x + r01 * r[q].y + r02 * r[q].z;
+    uv[q][1] = r20 * r[q].x + r21 * r[q].y + r22 * r[q].z;
+  }
+  const H33 m00 = uv[1][0] - uv[0][0], m01 = uv[2][0] - uv[0][0];
+  const H33 m10 = uv[1][1] - uv[0][1], m11 = uv[2][1] - uv[0][1];
+  const H33 idet = h33_recip(m00 * m11 - m01 * m10);
+  minv[0][0] = m11 * idet;
+  minv[0][1] = (-1.0 * m01) * idet;
+  minv[1][0] = (-1.0 * m10) * idet;
+  minv[1][1] = m00 * idet;
+}
+
+__device__ __forceinline__ void membrane_f33(const HV33 (&x)[3], const H33 (&minv)[2][2], HV33& f0, HV33& f1) {
+  const HV33 x10 = x[1] - x[0], x20 = x[2] - x[0];
+  f0 = scale(minv[0][0], x10) + scale(minv[1][0], x20);
+  f1 = scale(minv[0][1], x10) + scale(minv[1][1], x20);
+}
+
+__device__ __noinline__ H33 cloth_energy33(const ys_energy_args& a, const HV33 (&q)[4], const HV33 (&p)[4]) {
+  if (a.kind == YS_ENERGY_BENDING) {
+    const H33 theta = dihedral33(q[0], q[1], q[2], q[3]);
+    const H33 theta0 = dihedral33(p[0], p[1], p[2], p[3]);
+    const H33 d = theta - theta0;
+    const double dt = a.values[1];
+    return (a.values[0] * dt * dt) * (norm(p[1] - p[0]) * (d * d));
+  }
+  const HV33 qx[3] = {q[0], q[1], q[2]}, px[3] = {p[0], p[1], p[2]};
+  H33 minv[2][2], area;
+  rest_frame33(px, minv, area);
+  HV33 f0, f1;
+  membrane_f33(qx, minv, f0, f1);
+  const double dt = a.values[3];
+  if (a.kind == YS_ENERGY_BARAFF_WITKIN) {
+    const H33 sh = dot(f0, f1);
+    const H33 i5u = norm(f0), i5v = norm(f1);
+    const double uc = i5u.v < 1.0 ? 0.01 : 1.0, vc = i5v.v < 1.0 ? 0.01 : 1.0;
+    const H33 du = i5u - 1.0, dv = i5v - 1.0;
+    const H33 stretch = uc * (du * du) + vc * (dv * dv);
+    return (a.values[2] * dt * dt) * (area * (a.values[0] * stretch + a.values[1] * (sh * sh)));
+  }
+  const H33 e00 = 0.5 * (dot(f0, f0) - 1.0), e11 = 0.5 * (dot(f1, f1) - 1.0), e01 = 0.5 * dot(f0, f1);
+  const H33 tr = e00 + e11;
+  const H33 psi = a.values[0] * (e00 * e00 + e11 * e11 + 2.0 * (e01 * e01)) + (0.5 * a.values[1]) * (tr * tr);
+  return (a.values[2] * dt * dt) * (area * psi);
+}
+
+// Unprojected local Hessian over (positions, rest positions) of every
+// element, packed upper (6A)x(6A): one H33 evaluation a vertex pair.
+template <int A>
+__global__ void __launch_bounds__(64) rest_local_hessian_kernel(const ys_energy_args a, double* out) {
+  constexpr int M = 2 * A, N = 3 * M;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.num_elements) return;
+  double v[M][3];
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    const uint32_t id = a.conn[(uint64_t)t * A + k];
+    load_point(a.position, id, v[k]);
+    load_point(a.rest, id, v[A + k]);
+  }
+  double* dst = out + (uint64_t)t * (N * (N + 1) / 2);
+#pragma unroll 1
+  for (int va = 0; va < M; ++va)
+#pragma unroll 1
+    for (int vb = va; vb < M; ++vb) {
+      HV33 w[M];
+#pragma unroll
+      for (int k = 0; k < M; ++k) {
+        H33* c[3] = {&w[k].x, &w[k].y, &w[k].z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          *c[d] = h33c(v[k][d]);
+          if (k == va) c[d]->a[d] = 1.0;
+          if (k == vb) c[d]->b[d] = 1.0;
+        }
+      }
+      HV33 q[4], p[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        q[k] = w[k < A ? k : 0];
+        p[k] = w[k < A ? A + k : A];
+      }
+      const H33 e = cloth_energy33(a, q, p);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          if (3 * va + i <= 3 * vb + j) dst[utri<N>(3 * va + i, 3 * vb + j)] = e.ab[i][j];
+    }
+}
+
 // Lagged friction (friction_helpers.py:12-66): with the lagged tangent
 // basis (q[2..4], q[5..7]) and lambda_last_h (q[8]), phi of the tangential
 // relative displacement y = |(t0.rel, t1.rel)| (smoothed below sqrt(fDhat) dt)
@@ -995,6 +1127,27 @@ static int32_t launch_coupled(const ys_coupled_args& a, cudaStream_t s) {
 }  // namespace ys
 
 extern "C" {
+
+int32_t ys_rest_local_hessians(const ys_energy_args* args, double* out, void* stream) {
+  YS_REQUIRE(args != nullptr && out != nullptr, YS_ERR_INVALID, "null argument");
+  const ys_energy_args& a = *args;
+  YS_REQUIRE(a.position.num_children >= 1 && a.position.num_children <= YS_MAX_UNION, YS_ERR_INVALID,
+             "bad position union");
+  YS_REQUIRE(a.rest.num_children >= 1 && a.rest.num_children <= YS_MAX_UNION, YS_ERR_INVALID,
+             "the rest form needs rest positions");
+  const int A = a.kind == YS_ENERGY_BENDING ? 4
+                : (a.kind == YS_ENERGY_BARAFF_WITKIN || a.kind == YS_ENERGY_STVK_MEMBRANE) ? 3 : 0;
+  YS_REQUIRE(A != 0, YS_ERR_INVALID, "rest-position derivatives: bending, Baraff-Witkin and StVK membranes only");
+  YS_REQUIRE(a.arity == (uint32_t)A, YS_ERR_INVALID, "arity does not match the energy kind");
+  if (a.num_elements == 0) return YS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (A == 4)
+    ys::rest_local_hessian_kernel<4><<<ys::grid_for(a.num_elements, 64), 64, 0, s>>>(a, out);
+  else
+    ys::rest_local_hessian_kernel<3><<<ys::grid_for(a.num_elements, 64), 64, 0, s>>>(a, out);
+  YS_CHECK_LAUNCH();
+  return YS_OK;
+}
 
 int32_t ys_local_hessians(const ys_energy_args* args, double* out, void* stream) {
   YS_REQUIRE(args != nullptr && out != nullptr, YS_ERR_INVALID, "null argument");

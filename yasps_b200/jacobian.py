@@ -29,10 +29,11 @@ attributes (the adjoint blocks ``d2E / (dx dx_before)`` and
 for the lagged friction kinds, functions of ``x - x_old``, also the
 leaves of their step-start positions, and for the SNH tetrahedra the
 leaves of their rest positions against the position leaves (shape
-derivatives ``d2E / (dx dX)``) and against each other (``d2E / dX2``).
-Mixed derivatives through the rest shapes of the other energies and
-through affine-body vertices are not built (a target among those leaves
-raises).
+derivatives ``d2E / (dx dX)``) and against each other (``d2E / dX2``);
+the same for the cloth energies (bending, Baraff-Witkin and StVK
+membranes) through their rest frames.  Mixed derivatives through the rest
+argument of the other energies and through affine-body vertices are not
+built (a target among those leaves raises).
 """
 
 from __future__ import annotations
@@ -97,8 +98,9 @@ class _RectTerm:
 
   @property
   def rest_form(self) -> bool:
-    """SNH with a target among its rest leaves: the arguments are the tet's
-    positions and rest positions (``ys_snh_rest_local_hessians``)."""
+    """SNH or a cloth energy (bending, Baraff-Witkin, StVK) with a target
+    among its rest leaves: the arguments are the element's positions and rest
+    positions (``ys_snh_rest_local_hessians``, ``ys_rest_local_hessians``)."""
     return getattr(self, "_rest_form", False)
 
   def rest_leaves(self):
@@ -247,7 +249,7 @@ class _RectTerm:
       a.param_stride = e.per_element.size
     for k, p in enumerate(e.params_p):
       a.values[k] = helper._param(p, n)[1]
-    L.call("ys_local_hessians", ctypes.byref(a), L.ptr(out), s)
+    L.call("ys_rest_local_hessians" if self.rest_form else "ys_local_hessians", ctypes.byref(a), L.ptr(out), s)
 
 
 class secondOrderJacobian:
@@ -319,7 +321,8 @@ class secondOrderJacobian:
         rest = t.rest_leaves()
         in_rows = any(any(x is r for r in rest) for x in self.__row_wrt)
         in_cols = any(any(x is r for r in rest) for x in self.__column_wrt)
-        if (in_rows or in_cols) and t.expr.kind != "snh":
+        rest_kinds = t.expr.kind == "snh" or (t.expr.kind == "vertex" and t.expr.code in (5, 6, 7))
+        if (in_rows or in_cols) and not rest_kinds:
           raise NotImplementedError("secondOrderJacobian: mixed derivatives through the rest argument of "
                                     f"{type(t.expr).__name__} are not built")
         t._rest_form = in_rows or in_cols
